@@ -1,0 +1,372 @@
+#!/usr/bin/env python3
+"""Benchmark of the diffuse benchmark path: closest + shadow rays per second (Grays/s) on B200, one JSON line.
+
+Workloads (synthetic box-field scenes standing in for the reference's unreleased 116,855-triangle scene):
+  frame512  117,002 triangles, 512 x 512, 256 spp, depth 4, batch 256 (one wavefront pass), CUDA-graph frame  [default]
+  frame720  the same at 1280 x 720
+  frame256  12,290 triangles, 256 x 256, 16 spp, depth 4, batch 16
+  trace16m  117,002 triangles, 2^24 incoherent rays traced closest-hit and any-hit
+A step is one frame (frame*) or one closest + one any-hit pass over the batch (trace16m). `value` counts the rays of
+all ranks over the max over ranks of the device-timed steps (CUDA events on the renderer's stream). `e2e` is the same
+metric through the C ABI with host buffers: each frame's accumulation buffer (trace16m: rays in, hits out) crosses
+PCIe inside the timed region. Multi-GPU runs are independent replicas (weak scaling): the path needs no exchange.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload frame512] [--impl ours|reference]
+"""
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "frame512": dict(scene="boxes117k", w=512, h=512, spp=256, batch=256, bounces=4),
+    "frame720": dict(scene="boxes117k", w=1280, h=720, spp=256, batch=256, bounces=4),
+    "frame256": dict(scene="boxes12k", w=256, h=256, spp=16, batch=16, bounces=4),
+    "trace16m": dict(scene="boxes117k", rays=1 << 24),
+}
+STATE_BYTES = 40          # path state per queued ray: (o, id) + (d, T.r) + (T.g, T.b); shadow entries the same size
+LAYOUT_NAMES = {2: "bvh2", 4: "bvh4", 8: "cwbvh"}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons while the timed region runs."""
+    Q = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, dev_id):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200", "-i", dev_id],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate(); self.p.wait(timeout=10); self.f.flush(); self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1])); mx.append(float(c[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0")); local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def reference_lib():
+    import ctypes as C
+    path = os.path.join(ROOT, "oracle", "_ref", "libcwpref.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    L.ref_render_cpu.restype = C.c_double
+    L.ref_render_cpu.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p, C.c_int]
+    L.ref_trace.restype = C.c_double
+    L.ref_trace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_int]
+    return L
+
+
+def cpu_frame_sample(cwp, wl, mesh, bvh, variant, seconds=12.0):
+    """The frame on the host cores: the reference's own host code (oracle/_ref) when built, else the oracle port.
+    Pixels are taken as a contiguous band from the middle of the image, grown until about `seconds` of work."""
+    import ctypes as C
+    import numpy as np
+    p = cwp.frame_params(mesh, wl["w"], wl["h"], bounces=wl["bounces"])
+    threads = os.cpu_count() or 1
+    L = reference_lib()
+    alb = np.ascontiguousarray(bvh.albedo, np.float32)
+    N = wl["w"] * wl["h"]
+    npix, spent, rays = 64, 0.0, 0
+    while True:
+        pix0 = N // 2 - npix // 2
+        acc = np.zeros((N, 4), np.float32); cnt = np.zeros(2, np.int64)
+        if L is not None:
+            kind = "reference"
+            sec = L.ref_render_cpu(C.addressof(p), variant, 1, bvh.nodes.ctypes.data, bvh.woop.ctypes.data, bvh.tris.ctypes.data, alb.ctypes.data,
+                                   wl["bounces"], wl["spp"], 0, pix0, pix0 + npix, acc.ctypes.data, cnt.ctypes.data, threads)
+        else:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            from conftest import Oracle
+            kind, threads = "port", 1
+            t0 = time.perf_counter()
+            acc, cnt = Oracle().render(p, variant, 1, bvh, wl["bounces"], wl["spp"], 0, pix0, pix0 + npix)
+            sec = time.perf_counter() - t0
+        rays = int(cnt.sum()); spent = sec
+        if sec >= seconds / 4 or npix >= N:
+            break
+        npix = min(N, int(npix * max(2.0, min(16.0, seconds / 4 / max(sec, 1e-3)))))
+    return dict(value=rays / spent / 1e9, unit="Grays/s", cores=threads, kind=kind,
+                sample=f"{npix} pixels x {wl['spp']} spp of the {wl['w']}x{wl['h']} frame ({rays} closest+shadow rays in {spent:.2f} s)")
+
+
+def cpu_trace_sample(cwp, bvh, variant, o, d, seconds=12.0):
+    import numpy as np
+    L = reference_lib(); threads = os.cpu_count() or 1
+    n, spent = 1 << 14, 0.0
+    while True:
+        hits = np.zeros((n, 4), np.float32); occ = np.zeros(n, np.int32)
+        if L is not None:
+            kind = "reference"
+            spent = L.ref_trace(variant, 0, 1, bvh.nodes.ctypes.data, bvh.woop.ctypes.data, o[:n].ctypes.data, d[:n].ctypes.data, n, hits.ctypes.data, None, threads)
+            spent += L.ref_trace(variant, 1, 1, bvh.nodes.ctypes.data, bvh.woop.ctypes.data, o[:n].ctypes.data, d[:n].ctypes.data, n, None, occ.ctypes.data, threads)
+        else:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            from conftest import Oracle
+            kind, threads = "port", 1
+            t0 = time.perf_counter(); orc = Oracle()
+            orc.trace(variant, 1, False, bvh.nodes, bvh.woop, o[:n], d[:n]); orc.trace(variant, 1, True, bvh.nodes, bvh.woop, o[:n], d[:n])
+            spent = time.perf_counter() - t0
+        if spent >= seconds / 4 or n >= len(o):
+            break
+        n = min(len(o), int(n * max(2.0, min(16.0, seconds / 4 / max(spent, 1e-3)))))
+    return dict(value=2 * n / spent / 1e9, unit="Grays/s", cores=threads, kind=kind,
+                sample=f"{n} of the {len(o)} incoherent rays, closest-hit and any-hit ({2 * n} rays in {spent:.2f} s)")
+
+
+def run_reference(args, wl, rank):
+    """--impl reference: the reference's CPU implementation of the path on this host's cores (rank 0 only)."""
+    if rank != 0:
+        return
+    cwp = importlib.import_module("cuda-wavefront-pathtracer_b200")
+    variant = args.variant
+    mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=16)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        if "rays" in wl:
+            # rays from the oracle-free generator need a tracer: use the reference's own host traversal
+            L = reference_lib()
+            import numpy as np
+            p = cwp.frame_params(mesh, 512, 512)
+
+            def tr(o, d):
+                h = np.zeros((len(o), 4), np.float32)
+                L.ref_trace(variant, 0, 1, bvh.nodes.ctypes.data, bvh.woop.ctypes.data, o.ctypes.data, d.ctypes.data, len(o), h.ctypes.data, None, 0)
+                return h
+            if i == 0:
+                ro, rd = cwp.incoherent_rays(1 << 20, p, bvh.tris, tr, seed=41)
+            cb = cpu_trace_sample(cwp, bvh, variant, ro, rd, seconds=args.ref_seconds)
+        else:
+            cb = cpu_frame_sample(cwp, wl, mesh, bvh, variant, seconds=args.ref_seconds)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    print(json.dumps({"impl": "reference", "metric": "closest+shadow rays per second" if "rays" not in wl else "closest+any rays per second",
+                      "value": v, "unit": "Grays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                      "config": {"workload": args.workload, **{k: wl[k] for k in wl}, "layout": LAYOUT_NAMES[variant], "tri": "woop"},
+                      "cpu_baseline": cb, "e2e": {"value": v, "unit": "Grays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="frame512", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", type=int, default=8, choices=[2, 4, 8])
+    ap.add_argument("--bins", type=int, default=32)
+    ap.add_argument("--graph", type=int, default=1)
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    wl = dict(WORKLOADS[args.workload])
+    if args.batch:
+        wl["batch"] = args.batch
+    ws, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, wl, rank)
+        return
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    cwp = importlib.import_module("cuda-wavefront-pathtracer_b200")
+    variant = args.variant
+    mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=args.bins)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce(x, op):
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    props = torch.cuda.get_device_properties(local)
+    try:
+        dev_id = "GPU-" + str(props.uuid)
+    except Exception:
+        dev_id = str(local)
+    hbm_peak, peak_kind = peaks()
+    out = {"metric": "", "value": 0.0, "unit": "Grays/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 0.0,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
+    import torch.distributed as tdist
+    if "rays" not in wl:
+        # ------------------------------------------------------------------ frames
+        w, h, spp, K, B = wl["w"], wl["h"], wl["spp"], wl["batch"], wl["bounces"]
+        p = cwp.frame_params(mesh, w, h, bounces=B)
+        r = cwp.Renderer()
+        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1)
+        for _ in range(args.warmup):
+            r.render(spp)
+        depths = B + 2
+        rays = shadow = 0.0; ms = 0.0
+        c_tot = np.zeros(depths); s_tot = np.zeros(depths); tms = np.zeros(depths); sms = np.zeros(depths)
+        clk = Clocks(dev_id)
+        barrier()
+        for _ in range(args.steps):
+            st = r.render(spp)
+            rays += st.rays; shadow += st.shadow_rays; ms += st.frame_ms
+            c, s, tm, sm = r.depth_stats()
+            c_tot += c; s_tot += s; tms += tm; sms += sm
+        barrier()
+        clocks = clk.stop()
+        max_ms = reduce(ms, tdist.ReduceOp.MAX if ws > 1 else None)
+        all_rays = reduce(rays + shadow, tdist.ReduceOp.SUM if ws > 1 else None)
+        value = all_rays / (max_ms * 1e-3) / 1e9
+        # end to end through the C ABI with host buffers: frame + read of the accumulation buffer into pinned memory
+        host = torch.empty((w * h, 4), dtype=torch.float32, pin_memory=True)
+        barrier(); t0 = time.perf_counter(); e_rays = 0.0
+        for _ in range(args.steps):
+            st = r.render(spp)
+            cwp._check(cwp.lib().cwp_renderer_read_accum(r._h, host.data_ptr()))
+            e_rays += st.rays + st.shadow_rays
+        barrier(); e_s = time.perf_counter() - t0
+        e_s = reduce(e_s, tdist.ReduceOp.MAX if ws > 1 else None)
+        e_rays = reduce(e_rays, tdist.ReduceOp.SUM if ws > 1 else None)
+        # roofline of the dominant kernel (HBM: algorithmic path-state bytes per launch / its event-timed duration)
+        tr_bytes = sum(STATE_BYTES * ((c_tot[d] if d > 0 else 0) + (c_tot[d + 1] if d + 1 < depths else 0) + s_tot[d]) for d in range(depths))
+        sh_bytes = sum(STATE_BYTES * s_tot[d] for d in range(depths))
+        dom = "k_trace_shade" if tms.sum() >= sms.sum() else "k_shadow"
+        b, t = (tr_bytes, tms.sum()) if dom == "k_trace_shade" else (sh_bytes, sms.sum())
+        achieved = b / (t * 1e-3) / 1e9 if t > 0 else 0.0
+        out.update(metric="closest+shadow rays per second, diffuse frame", value=value, ms_per_step=max_ms / args.steps,
+                   config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles, box field seed 1)", "resolution": f"{w}x{h}",
+                           "spp": spp, "batch": K, "depth": B, "layout": LAYOUT_NAMES[variant], "sah_bins": args.bins, "tri": "woop",
+                           "graph": args.graph, "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
+                           "rays_per_frame": (rays + shadow) / args.steps, "closest_per_frame": rays / args.steps, "shadow_per_frame": shadow / args.steps,
+                           "rays_per_sample": (rays + shadow) / args.steps / (w * h * spp), "trace_shade_ms": float(tms.sum() / args.steps),
+                           "shadow_ms": float(sms.sum() / args.steps)},
+                   clocks=clocks,
+                   e2e={"value": e_rays / e_s / 1e9, "unit": "Grays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": w * h * 16,
+                        "note": "scene uploaded once at init; each step renders and reads the w*h float4 accumulation buffer back into pinned host memory"},
+                   gpu_launches=args.steps * (spp // K) * (2 + 2 * depths),
+                   roofline={"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                             "peak_kind": peak_kind, "traffic": None,
+                             "algorithmic": f"{STATE_BYTES} B of path state per queued ray read and per continuation/shadow ray written"})
+        r.close()
+    else:
+        # ------------------------------------------------------------------ ray batches
+        n = wl["rays"]
+        acc = cwp.Accel(bvh, tri=1, device=local)
+        p = cwp.frame_params(mesh, 512, 512)
+        st = torch.cuda.current_stream()
+
+        def tr(o, d):
+            to, td = torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()
+            hh = torch.empty((len(o), 4), dtype=torch.float32, device="cuda")
+            acc.trace_closest(to.data_ptr(), td.data_ptr(), hh.data_ptr(), len(o), st.cuda_stream)
+            torch.cuda.synchronize()
+            return hh.cpu().numpy()
+        o, d = cwp.incoherent_rays(n, p, bvh.tris, tr, seed=41)
+        do, dd = torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()
+        hits = torch.empty((n, 4), dtype=torch.float32, device="cuda"); occ = torch.empty(n, dtype=torch.int32, device="cuda")
+        for _ in range(args.warmup):
+            acc.trace_closest(do.data_ptr(), dd.data_ptr(), hits.data_ptr(), n, st.cuda_stream)
+            acc.trace_any(do.data_ptr(), dd.data_ptr(), occ.data_ptr(), n, st.cuda_stream)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps)]
+        clk = Clocks(dev_id)
+        barrier()
+        for i in range(args.steps):
+            ev[3 * i].record(st)
+            acc.trace_closest(do.data_ptr(), dd.data_ptr(), hits.data_ptr(), n, st.cuda_stream)
+            ev[3 * i + 1].record(st)
+            acc.trace_any(do.data_ptr(), dd.data_ptr(), occ.data_ptr(), n, st.cuda_stream)
+            ev[3 * i + 2].record(st)
+        barrier()
+        clocks = clk.stop()
+        acc.status()
+        c_ms = sum(ev[3 * i].elapsed_time(ev[3 * i + 1]) for i in range(args.steps))
+        a_ms = sum(ev[3 * i + 1].elapsed_time(ev[3 * i + 2]) for i in range(args.steps))
+        max_ms = reduce(c_ms + a_ms, tdist.ReduceOp.MAX if ws > 1 else None)
+        value = 2 * n * args.steps * ws / (max_ms * 1e-3) / 1e9
+        # e2e: pinned host rays in, hits / occluders out, every step
+        ho = torch.from_numpy(o).pin_memory(); hd = torch.from_numpy(d).pin_memory()
+        hh = torch.empty((n, 4), dtype=torch.float32, pin_memory=True); hoc = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        barrier(); t0 = time.perf_counter()
+        import ctypes as C
+        for _ in range(args.steps):
+            cwp._check(cwp.lib().cwp_trace_closest_host(acc._h, ho.data_ptr(), hd.data_ptr(), hh.data_ptr(), n, None))
+            cwp._check(cwp.lib().cwp_trace_any_host(acc._h, ho.data_ptr(), hd.data_ptr(), hoc.data_ptr(), n, None))
+        barrier(); e_s = reduce(time.perf_counter() - t0, tdist.ReduceOp.MAX if ws > 1 else None)
+        dom_ms, dom_b, dom = (c_ms, 48.0, "k_trace_closest") if c_ms >= a_ms else (a_ms, 36.0, "k_trace_any")
+        achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
+        out.update(metric="closest+any rays per second, incoherent ray batch", value=value, ms_per_step=max_ms / args.steps,
+                   config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles)", "rays": n, "layout": LAYOUT_NAMES[variant],
+                           "sah_bins": args.bins, "tri": "woop", "l2": f"ray batch {n * 32 / 1e9:.2f} GB > L2 (126 MB)",
+                           "closest_ms": c_ms / args.steps, "any_ms": a_ms / args.steps},
+                   clocks=clocks,
+                   e2e={"value": 2 * n * args.steps * ws / e_s / 1e9, "unit": "Grays/s", "h2d_bytes_per_step": 2 * 2 * n * 16, "d2h_bytes_per_step": n * 16 + n * 4},
+                   gpu_launches=2 * args.steps,
+                   roofline={"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                             "peak_kind": peak_kind, "traffic": None,
+                             "algorithmic": "closest: 32 B ray in + 16 B hit out; any: 32 B in + 4 B out"})
+        acc.close()
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        if "rays" not in wl:
+            out["cpu_baseline"] = cpu_frame_sample(cwp, wl, mesh, bvh, variant)
+        else:
+            out["cpu_baseline"] = cpu_trace_sample(cwp, bvh, variant, o, d)
+    if ws > 1:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

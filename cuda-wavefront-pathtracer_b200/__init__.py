@@ -1,0 +1,349 @@
+"""B200 wavefront path tracer - Python binding of the C ABI (include/cwp_b200.h, libcwpb200.so).
+
+The classes mirror the reference's C++ interface: ``Mesh`` (scene/mesh.h, io/mesh_loader.h), ``Bvh`` (BVHBuilder +
+BVH2Flat / BVH4Flat / CWBVH + packTriangles / packWoop), ``Accel`` (device scene + trav<V,ANY,TRI> over ray batches)
+and ``Renderer`` (WavefrontRenderer). Errors raise ``CwpError`` carrying the library's status code and message.
+There is no CPU fallback: every compute call goes through the CUDA library, and importing fails loudly when
+libcwpb200.so has not been built.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcwpb200.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_TRAVERSAL, ERR_IO = range(7)
+LAYOUT_BVH2, LAYOUT_BVH4, LAYOUT_CWBVH = 2, 4, 8
+TRI_MT, TRI_WOOP = 0, 1
+FILTER_TABLE = 64
+
+
+class CwpError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cwp error {code}: {msg}")
+        self.code = code
+
+
+class MeshView(C.Structure):
+    _fields_ = [("verts", C.POINTER(C.c_float)), ("n_verts", C.c_int64), ("faces", C.POINTER(C.c_int32)), ("n_tris", C.c_int64),
+                ("face_mat", C.POINTER(C.c_int32)), ("normals", C.POINTER(C.c_float)), ("albedo", C.POINTER(C.c_float)), ("n_albedo", C.c_int32)]
+
+
+class BuildOptions(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("bins", C.c_int32), ("leaf", C.c_int32), ("collapse", C.c_int32), ("threads", C.c_int32)]
+
+
+class BvhData(C.Structure):
+    _fields_ = [("nodes", C.POINTER(C.c_float)), ("n_node_float4", C.c_int64), ("node_stride", C.c_int32),
+                ("order", C.POINTER(C.c_int32)), ("n_tris", C.c_int64), ("tris", C.POINTER(C.c_float)), ("nrm", C.POINTER(C.c_float)),
+                ("woop", C.POINTER(C.c_float)), ("max_depth", C.c_int32), ("max_leaf_tris", C.c_int32), ("sah", C.c_double), ("build_ms", C.c_double)]
+
+
+class SceneBuffers(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("n_node_float4", C.c_int64), ("node_stride", C.c_int32), ("tris", C.c_void_p), ("n_tris", C.c_int64),
+                ("nrm", C.c_void_p), ("woop", C.c_void_p), ("albedo", C.c_void_p), ("n_albedo", C.c_int32)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("ax", C.c_float * 3), ("ay", C.c_float * 3), ("az", C.c_float * 3),
+                ("fx", C.c_float), ("fy", C.c_float), ("px", C.c_float), ("py", C.c_float), ("w", C.c_int32), ("h", C.c_int32),
+                ("lens_r", C.c_float), ("focus_d", C.c_float)]
+
+
+class Params(C.Structure):
+    _fields_ = [("cam", Camera), ("sun_to", C.c_float * 3), ("sun_e", C.c_float * 3), ("sky", C.c_float * 3), ("sun_cos", C.c_float),
+                ("max_b", C.c_int32), ("seed", C.c_uint32), ("eps", C.c_float), ("near_clip", C.c_float), ("has_n", C.c_int32),
+                ("filter_bh", C.c_int32), ("ftab", C.c_float * (FILTER_TABLE + 1))]
+
+
+class RenderOptions(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("tri", C.c_int32), ("batch", C.c_int32), ("bounces", C.c_int32), ("graph", C.c_int32),
+                ("block", C.c_int32), ("device", C.c_int32), ("profile", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+
+class FrameStats(C.Structure):
+    _fields_ = [("rays", C.c_double), ("shadow_rays", C.c_double), ("trace_ms", C.c_double), ("frame_ms", C.c_double)]
+
+
+class RendererInfo(C.Structure):
+    _fields_ = [("vram_mb", C.c_double), ("tlas_ms", C.c_double), ("pt_blocks", C.c_int32), ("n_sm", C.c_int32), ("gpu_name", C.c_char * 256)]
+
+
+# every exported symbol of the C ABI with its ctypes signature (restype, argtypes)
+SIGNATURES = {
+    "cwp_last_error": (C.c_char_p, []),
+    "cwp_version": (C.c_int32, []),
+    "cwp_mesh_box_field": (C.c_int, [C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "cwp_mesh_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "cwp_mesh_from_view": (C.c_int, [C.POINTER(MeshView), C.POINTER(C.c_void_p)]),
+    "cwp_mesh_view_of": (C.c_int, [C.c_void_p, C.POINTER(MeshView)]),
+    "cwp_mesh_write_ply": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "cwp_mesh_free": (None, [C.c_void_p]),
+    "cwp_bvh_build": (C.c_int, [C.c_void_p, C.POINTER(BuildOptions), C.POINTER(C.c_void_p)]),
+    "cwp_bvh_data_of": (C.c_int, [C.c_void_p, C.POINTER(BvhData)]),
+    "cwp_bvh_free": (None, [C.c_void_p]),
+    "cwp_accel_create": (C.c_int, [C.POINTER(SceneBuffers), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "cwp_accel_destroy": (None, [C.c_void_p]),
+    "cwp_trace_closest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    "cwp_trace_any": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    "cwp_trace_closest_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_float)]),
+    "cwp_trace_any_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_float)]),
+    "cwp_accel_status": (C.c_int, [C.c_void_p]),
+    "cwp_renderer_create": (C.c_int, [C.POINTER(C.c_void_p)]),
+    "cwp_renderer_init": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(SceneBuffers), C.POINTER(RenderOptions)]),
+    "cwp_renderer_render": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(FrameStats), C.c_int32, C.c_int32]),
+    "cwp_renderer_read_accum": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cwp_renderer_accum_device": (C.c_void_p, [C.c_void_p]),
+    "cwp_renderer_set_params": (C.c_int, [C.c_void_p, C.POINTER(Params)]),
+    "cwp_renderer_set_materials": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "cwp_renderer_info_of": (C.c_int, [C.c_void_p, C.POINTER(RendererInfo)]),
+    "cwp_renderer_depth_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "cwp_renderer_destroy": (None, [C.c_void_p]),
+    "cwp_camera_look_at": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
+    "cwp_camera_from_c2w": (C.c_int, [C.POINTER(C.c_float), C.c_float, C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
+    "cwp_params_defaults": (C.c_int, [C.POINTER(Params)]),
+    "cwp_params_finish": (C.c_int, [C.POINTER(Params), C.c_float, C.c_float, C.c_float]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library; raises if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is not built: run `make -C {_HERE}` (or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != OK:
+        raise CwpError(rc, lib().cwp_last_error().decode(errors="replace"))
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+class Mesh:
+    """Indexed triangle mesh owned by the library (vertices, faces, material ids, albedo table)."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def box_field(cls, n_boxes, seed=1):
+        h = C.c_void_p()
+        _check(lib().cwp_mesh_box_field(n_boxes, seed, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def load(cls, path):
+        h = C.c_void_p()
+        _check(lib().cwp_mesh_load(str(path).encode(), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_arrays(cls, verts, faces, face_mat=None, albedo=None, normals=None):
+        verts = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        faces = np.ascontiguousarray(faces, np.int32).reshape(-1, 3)
+        v = MeshView()
+        v.verts, v.n_verts, v.faces, v.n_tris = _fptr(verts), len(verts), _iptr(faces), len(faces)
+        keep = [verts, faces]
+        if face_mat is not None:
+            fm = np.ascontiguousarray(face_mat, np.int32); keep.append(fm); v.face_mat = _iptr(fm)
+        if normals is not None:
+            nr = np.ascontiguousarray(normals, np.float32); keep.append(nr); v.normals = _fptr(nr)
+        if albedo is not None:
+            al = np.ascontiguousarray(albedo, np.float32).reshape(-1, 3); keep.append(al); v.albedo = _fptr(al); v.n_albedo = len(al)
+        h = C.c_void_p()
+        _check(lib().cwp_mesh_from_view(C.byref(v), C.byref(h)))
+        return cls(h.value)
+
+    def arrays(self):
+        """(verts [n,3] float32, faces [m,3] int32, face_mat [m] int32, albedo [k,3] float32) copies."""
+        v = MeshView()
+        _check(lib().cwp_mesh_view_of(self._h, C.byref(v)))
+        verts = np.ctypeslib.as_array(v.verts, (v.n_verts, 3)).copy()
+        faces = np.ctypeslib.as_array(v.faces, (v.n_tris, 3)).copy()
+        fm = np.ctypeslib.as_array(v.face_mat, (v.n_tris,)).copy() if v.face_mat else np.zeros(v.n_tris, np.int32)
+        alb = np.ctypeslib.as_array(v.albedo, (v.n_albedo, 3)).copy()
+        return verts, faces, fm, alb
+
+    @property
+    def n_tris(self):
+        v = MeshView(); _check(lib().cwp_mesh_view_of(self._h, C.byref(v))); return v.n_tris
+
+    def write_ply(self, path):
+        _check(lib().cwp_mesh_write_ply(self._h, str(path).encode()))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.cwp_mesh_free(self._h); self._h = C.c_void_p()
+
+
+class Bvh:
+    """Host BVH build result: GPU node array, leaf order, packed triangles and Woop rows (numpy copies)."""
+
+    def __init__(self, mesh, variant=LAYOUT_BVH2, bins=16, leaf=4, collapse=0, threads=0):
+        o = BuildOptions(variant, bins, leaf, collapse, threads)
+        h = C.c_void_p()
+        _check(lib().cwp_bvh_build(mesh._h, C.byref(o), C.byref(h)))
+        try:
+            d = BvhData(); _check(lib().cwp_bvh_data_of(h, C.byref(d)))
+            self.variant, self.stride = variant, d.node_stride
+            self.nodes = np.ctypeslib.as_array(d.nodes, (d.n_node_float4, 4)).copy()
+            self.order = np.ctypeslib.as_array(d.order, (d.n_tris,)).copy()
+            self.tris = np.ctypeslib.as_array(d.tris, (d.n_tris * 3, 4)).copy()
+            self.woop = np.ctypeslib.as_array(d.woop, (d.n_tris * 3, 4)).copy()
+            self.nrm = np.ctypeslib.as_array(d.nrm, (d.n_tris * 3, 4)).copy() if d.nrm else None
+            self.max_depth, self.max_leaf_tris, self.sah, self.build_ms = d.max_depth, d.max_leaf_tris, d.sah, d.build_ms
+        finally:
+            lib().cwp_bvh_free(h)
+        _, _, _, self.albedo = mesh.arrays()
+
+    @property
+    def n_nodes(self):
+        return len(self.nodes) // self.stride
+
+    def scene_buffers(self):
+        """SceneBuffers pointing at this object's arrays (valid while it lives)."""
+        s = SceneBuffers()
+        s.nodes, s.n_node_float4, s.node_stride = self.nodes.ctypes.data, len(self.nodes), self.stride
+        s.tris, s.n_tris = self.tris.ctypes.data, len(self.order)
+        s.nrm = self.nrm.ctypes.data if self.nrm is not None else None
+        s.woop = self.woop.ctypes.data
+        self._alb = np.ascontiguousarray(self.albedo, np.float32)
+        s.albedo, s.n_albedo = self._alb.ctypes.data, len(self._alb)
+        return s
+
+
+class Accel:
+    """Device copy of a scene for ray batches (closest-hit and any-hit)."""
+
+    def __init__(self, bvh, tri=TRI_WOOP, device=0):
+        self._keep = bvh
+        h = C.c_void_p()
+        s = bvh.scene_buffers()
+        _check(lib().cwp_accel_create(C.byref(s), tri, device, C.byref(h)))
+        self._h = h
+
+    def trace_closest(self, d_o, d_d, d_hits, n, stream=None):
+        """Device pointers (ints, e.g. torch data_ptr()); stream = cudaStream_t as int or None."""
+        _check(lib().cwp_trace_closest(self._h, d_o, d_d, d_hits, n, stream))
+
+    def trace_any(self, d_o, d_d, d_occ, n, stream=None):
+        _check(lib().cwp_trace_any(self._h, d_o, d_d, d_occ, n, stream))
+
+    def trace_closest_host(self, o, d):
+        o = np.ascontiguousarray(o, np.float32); d = np.ascontiguousarray(d, np.float32)
+        hits = np.empty((len(o), 4), np.float32); ms = C.c_float()
+        _check(lib().cwp_trace_closest_host(self._h, o.ctypes.data, d.ctypes.data, hits.ctypes.data, len(o), C.byref(ms)))
+        return hits, ms.value
+
+    def trace_any_host(self, o, d):
+        o = np.ascontiguousarray(o, np.float32); d = np.ascontiguousarray(d, np.float32)
+        occ = np.empty(len(o), np.int32); ms = C.c_float()
+        _check(lib().cwp_trace_any_host(self._h, o.ctypes.data, d.ctypes.data, occ.ctypes.data, len(o), C.byref(ms)))
+        return occ, ms.value
+
+    def status(self):
+        _check(lib().cwp_accel_status(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().cwp_accel_destroy(self._h); self._h = C.c_void_p()
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+
+def camera_look_at(pos, target, up, hfov_deg, w, h):
+    c = Camera()
+    f3 = C.c_float * 3
+    _check(lib().cwp_camera_look_at(f3(*pos), f3(*target), f3(*up), hfov_deg, w, h, C.byref(c)))
+    return c
+
+
+def params_defaults():
+    p = Params()
+    _check(lib().cwp_params_defaults(C.byref(p)))
+    return p
+
+
+def params_finish(p, sun_angle_deg, eps_scale, extent):
+    _check(lib().cwp_params_finish(C.byref(p), sun_angle_deg, eps_scale, extent))
+    return p
+
+
+class Renderer:
+    """WavefrontRenderer: init(params, bvh, options) -> render(spp) -> accum sums (w*h float4)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(lib().cwp_renderer_create(C.byref(h)))
+        self._h = h
+
+    def init(self, params, bvh, variant, tri=TRI_WOOP, batch=16, bounces=4, graph=1, device=0, profile=0):
+        self._params, self._bvh = params, bvh
+        o = RenderOptions(); o.variant, o.tri, o.batch, o.bounces, o.graph, o.device, o.profile = variant, tri, batch, bounces, graph, device, profile
+        self.depths = bounces + 2
+        s = bvh.scene_buffers()
+        _check(lib().cwp_renderer_init(self._h, C.byref(params), C.byref(s), C.byref(o)))
+        self.w, self.h = params.cam.w, params.cam.h
+
+    def render(self, spp, s_base=0, clear=True):
+        st = FrameStats()
+        _check(lib().cwp_renderer_render(self._h, spp, C.byref(st), s_base, 1 if clear else 0))
+        return st
+
+    def read_accum(self):
+        a = np.empty((self.h * self.w, 4), np.float32)
+        _check(lib().cwp_renderer_read_accum(self._h, a.ctypes.data))
+        return a
+
+    def accum_device(self):
+        return lib().cwp_renderer_accum_device(self._h)
+
+    def set_params(self, p):
+        self._params = p
+        _check(lib().cwp_renderer_set_params(self._h, C.byref(p)))
+
+    def set_materials(self, albedo):
+        a = np.ascontiguousarray(albedo, np.float32).reshape(-1, 3)
+        _check(lib().cwp_renderer_set_materials(self._h, a.ctypes.data, len(a)))
+
+    def depth_stats(self):
+        """Per-depth (closest rays, shadow rays, trace+shade ms, shadow ms) of the last frame."""
+        n = self.depths
+        c = np.zeros(n, np.int64); s = np.zeros(n, np.int64); tm = np.zeros(n, np.float32); sm = np.zeros(n, np.float32)
+        _check(lib().cwp_renderer_depth_stats(self._h, c.ctypes.data, s.ctypes.data, tm.ctypes.data, sm.ctypes.data, n))
+        return c, s, tm, sm
+
+    def info(self):
+        i = RendererInfo(); _check(lib().cwp_renderer_info_of(self._h, C.byref(i))); return i
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().cwp_renderer_destroy(self._h); self._h = C.c_void_p()
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+
+from . import imageio  # noqa: E402,F401
+from .workloads import *  # noqa: E402,F401,F403  (scene / camera / lighting presets of the benchmark configs)

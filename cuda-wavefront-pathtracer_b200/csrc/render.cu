@@ -1,0 +1,469 @@
+// render.cu - wavefront path tracer for the diffuse (Lambert + sun + constant sky) path on sm_100a.
+//
+// Per pass of K samples per pixel, for depth = 0 .. bounces + 1:
+//   k_trace_shade<depth 0>: camera ray generated in-kernel from the path index (no raygen pass, no state read),
+//   k_trace_shade<depth > 0>: compacted path state read with coalesced 16-byte loads,
+//   both: closest-hit traversal, then shading: miss -> sky; hit at depth <= bounces -> sun next-event estimation into
+//   the shadow queue and a cosine continuation into the next depth's queue, both appended by one atomic per warp
+//   (ballot + popc) so that every warp writes a contiguous run;
+//   k_shadow: any-hit traversal of the shadow queue, unoccluded contributions added with one float4 atomic each.
+// The semantics are those of the reference's legacy path (render/wavefront.cu:42-58 raygen, 94-136 shadeOne,
+// 684-741 frame loop): same sample streams (pixel, sample, depth, dimension), same per-vertex decisions, so frames
+// agree sample by sample with the reference's up to rounding.
+// All traversal kernels are persistent (grid = resident blocks) with per-warp dynamic fetching of 32 paths, and read
+// their queue lengths from device memory, so a whole frame is captured once as a CUDA graph and replayed.
+#include "scene_dev.h"
+#include "trav.cuh"
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace cwpb {
+
+// path state (structure of arrays, one element per path in the queue):
+//   s0 = (origin, path id bits), s1 = (direction, throughput.r), s2 = (throughput.g, throughput.b)
+// shadow queue: h0 = (origin, pixel bits), h1 = (direction, contribution.r), h2 = (contribution.g, contribution.b)
+struct Queues {
+    float4* s0[2]; float4* s1[2]; float2* s2[2];
+    float4* h0; float4* h1; float2* h2;
+};
+
+// per-depth counters, 4 ints each: [0] queue length, [1] shadow queue length, [2] trace fetch, [3] shadow fetch
+struct KArgs {
+    const float4* nodes; const float4* tv; const float4* tris; const float4* nrm; const float3* albedo;
+    Queues q; float4* accum; int* cnt; int* err;
+    int nk, N, sBase, depth;
+};
+
+__device__ __forceinline__ float rnd(const cwp_params& P, unsigned pix, unsigned smp, unsigned depth, unsigned dim) { return sample01(pix, smp, depth, dim, P.seed); }
+__device__ __forceinline__ float3 v3(const float* a) { return f3(a[0], a[1], a[2]); }
+__device__ __forceinline__ unsigned lanemask_lt() { unsigned m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
+
+// one atomic per warp: returns this lane's slot in a contiguous run reserved for the lanes with want set
+__device__ __forceinline__ int warp_append(int* counter, bool want) {
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (!m) return -1;
+    const int leader = __ffs(m) - 1, lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return want ? base + __popc(m & lanemask_lt()) : -1;
+}
+
+__device__ __forceinline__ void accum_add(float4* accum, int pix, float3 c) { atomicAdd(accum + pix, make_float4(c.x, c.y, c.z, 0.f)); }
+
+// camera ray of path i (wavefront.cu:42-58): pixel i mod N, sample sBase + i / N
+__device__ __forceinline__ void camera_ray(const cwp_params& P, int i, int N, int sBase, float3& o, float3& d, int& pix, unsigned& smp) {
+    pix = i % N; smp = (unsigned)(sBase + i / N);
+    const cwp_camera& C = P.cam;
+    const int x = pix % C.w, y = pix / C.w;
+    const float u0 = rnd(P, pix, smp, 0, 0), u1 = rnd(P, pix, smp, 0, 1);
+    float jx, jy;
+    if (P.filter_bh) { jx = table_lookup(P.ftab, CWP_FILTER_TABLE, u0); jy = table_lookup(P.ftab, CWP_FILTER_TABLE, u1); }
+    else { jx = u0 - 0.5f; jy = u1 - 0.5f; }
+    const float dx = (x + 0.5f + jx - C.px) / C.fx, dy = -(y + 0.5f + jy - C.py) / C.fy;
+    const float3 ax = v3(C.ax), ay = v3(C.ay), az = v3(C.az), pos = v3(C.pos);
+    d = normalize(ax * dx + ay * dy - az);
+    o = pos;
+    if (C.lens_r > 0.f) {
+        float lx, ly; disk_map(rnd(P, pix, smp, 0, 2), rnd(P, pix, smp, 0, 3), lx, ly);
+        const float3 pf = pos + (ax * dx + ay * dy - az) * C.focus_d;
+        o = pos + ax * (lx * C.lens_r) + ay * (ly * C.lens_r);
+        d = normalize(pf - o);
+    }
+}
+
+template <int V, int TRI, bool PRIMARY>
+__global__ void __launch_bounds__(128, 8) k_trace_shade(const __grid_constant__ KArgs a, const __grid_constant__ cwp_params P) {
+    int* const c = a.cnt + 4 * a.depth;
+    int* const cNext = c + 4;
+    const int n = PRIMARY ? a.nk : c[0];
+    const int lane = threadIdx.x & 31, rd = a.depth & 1, wr = rd ^ 1;
+    const unsigned depthRng = (unsigned)a.depth + 1u;
+    const bool canBounce = a.depth <= P.max_b;
+    int err = 0;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(c + 2, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const int k = base + lane;
+        const bool valid = k < n;
+        float3 o = f3(0.f, 0.f, 0.f), d = f3(0.f, 0.f, 1.f), T = f3(1.f, 1.f, 1.f);
+        int id = 0, pix = 0; unsigned smp = 0; float tmin = 0.f;
+        if (valid) {
+            if (PRIMARY) { id = k; camera_ray(P, k, a.N, a.sBase, o, d, pix, smp); tmin = P.near_clip; }
+            else {
+                const float4 s0 = __ldcs(a.q.s0[rd] + k), s1 = __ldcs(a.q.s1[rd] + k); const float2 s2 = __ldcs(a.q.s2[rd] + k);
+                o = xyz(s0); d = xyz(s1); T = f3(s1.w, s2.x, s2.y); id = __float_as_int(s0.w);
+                pix = id % a.N; smp = (unsigned)(a.sBase + id / a.N);
+            }
+        }
+        float t = 1e30f, hu = 0.f, hv = 0.f; int tri = -1;
+        if (valid) trace_ray<V, false, TRI>(a.nodes, a.tv, o, d, tmin, t, tri, hu, hv, 0, err);
+        bool wantShadow = false, wantCont = false;
+        float3 po = o, l = d, contrib = T, nd = d;
+        if (valid) {
+            if (tri < 0) accum_add(a.accum, pix, T * v3(P.sky));
+            else if (canBounce) {
+                const float3 p = o + d * t;
+                const float4 b = __ldg(a.tris + 3 * tri + 1), cc = __ldg(a.tris + 3 * tri + 2);
+                float3 ng = normalize(cross(xyz(b), xyz(cc))), ns = ng;
+                if (P.has_n && a.nrm) {
+                    const float3 n0 = xyz(__ldg(a.nrm + 3 * tri)), n1 = xyz(__ldg(a.nrm + 3 * tri + 1)), n2 = xyz(__ldg(a.nrm + 3 * tri + 2));
+                    const float3 nn = n0 * (1.f - hu - hv) + n1 * hu + n2 * hv; const float ln = length(nn);
+                    if (ln > 0.f) ns = nn * (1.f / ln);
+                    if (dot(ns, ng) < 0.f) ns = -ns;
+                }
+                if (dot(ng, d) > 0.f) { ng = -ng; ns = -ns; }
+                const float3 alb = a.albedo[__float_as_int(b.w)];
+                po = p + ng * P.eps;
+                // sun next-event estimation: uniform direction in the sun's cone, Lambert BRDF alb / pi
+                l = cone_dir(v3(P.sun_to), P.sun_cos, rnd(P, pix, smp, depthRng, 2), rnd(P, pix, smp, depthRng, 3));
+                const float cl = dot(ns, l);
+                if (cl > 0.f && dot(ng, l) > 0.f) { contrib = T * alb * v3(P.sun_e) * (cl * CWPB_INV_PI); wantShadow = true; }
+                // continuation: cosine-weighted about the shading normal, throughput *= albedo
+                nd = cosine_dir(ns, rnd(P, pix, smp, depthRng, 0), rnd(P, pix, smp, depthRng, 1));
+                if (dot(nd, ng) > 0.f) { T = T * alb; wantCont = true; }
+            }
+        }
+        const int sp = warp_append(c + 1, wantShadow);
+        if (sp >= 0) {
+            __stcs(a.q.h0 + sp, f4(po, __int_as_float(pix)));
+            __stcs(a.q.h1 + sp, f4(l, contrib.x));
+            __stcs(a.q.h2 + sp, make_float2(contrib.y, contrib.z));
+        }
+        const int cp = warp_append(cNext, wantCont);
+        if (cp >= 0) {
+            __stcs(a.q.s0[wr] + cp, f4(po, __int_as_float(id)));
+            __stcs(a.q.s1[wr] + cp, f4(nd, T.x));
+            __stcs(a.q.s2[wr] + cp, make_float2(T.y, T.z));
+        }
+    }
+    if (err) atomicOr(a.err, err);
+}
+
+template <int V, int TRI>
+__global__ void __launch_bounds__(128, 8) k_shadow(const __grid_constant__ KArgs a) {
+    int* const c = a.cnt + 4 * a.depth;
+    const int n = c[1];
+    const int lane = threadIdx.x & 31;
+    int err = 0;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(c + 3, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const int k = base + lane;
+        if (k < n) {
+            const float4 h0 = __ldcs(a.q.h0 + k), h1 = __ldcs(a.q.h1 + k); const float2 h2 = __ldcs(a.q.h2 + k);
+            float t = 1e30f, u, v; int tri = -1;
+            if (!trace_ray<V, true, TRI>(a.nodes, a.tv, xyz(h0), xyz(h1), 0.f, t, tri, u, v, 0, err))
+                accum_add(a.accum, __float_as_int(h0.w), f3(h1.w, h2.x, h2.y));
+        }
+    }
+    if (err) atomicOr(a.err, err);
+}
+
+// pass set-up: depth-0 queue length = nk; everything else zero
+__global__ void k_pass_begin(int* cnt, int nInts, int nk) {
+    for (int i = threadIdx.x; i < nInts; i += blockDim.x) cnt[i] = i == 0 ? nk : 0;
+}
+// per-depth ray totals of a pass: tot[2 d] += queue length, tot[2 d + 1] += shadow queue length
+__global__ void k_pass_end(const int* cnt, int depths, unsigned long long* tot) {
+    for (int d = threadIdx.x; d < depths; d += blockDim.x) { tot[2 * d] += (unsigned)cnt[4 * d]; tot[2 * d + 1] += (unsigned)cnt[4 * d + 1]; }
+}
+
+}  // namespace cwpb
+
+using namespace cwpb;
+
+struct cwp_renderer {
+    cwp_params P{}; cwp_render_options O{};
+    DeviceScene scene;
+    int N = 0, K = 1, depths = 0; long long nk = 0; bool ready = false;
+    Queues q{};
+    float4* accum = nullptr; int* cnt = nullptr; int* err = nullptr; unsigned long long* tot = nullptr;   // tot: 2 per depth
+    std::vector<unsigned long long> htot;                 // last frame's per-depth totals
+    std::vector<cudaEvent_t> ev; int evPasses = 0;        // profiling: 4 events per (pass, depth)
+    std::vector<float> traceMs, shadowMs;                 // last frame's per-depth kernel times
+    int* hcnt = nullptr;   // pinned copy of the counters (host loop)
+    cudaStream_t st = nullptr; cudaEvent_t f0 = nullptr, f1 = nullptr;
+    cudaGraphExec_t gexec = nullptr; int gSpp = -1, gBase = 0;
+    int gridTrace = 0, gridTrace0 = 0, gridShadow = 0, nSM = 0;
+    std::vector<void*> allocs;
+    double vramMB = 0; std::string gpuName;
+};
+
+namespace {
+
+template <int V, int TRI> int occupancy_of(int& bt0, int& bt, int& bs) {
+    CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt0, k_trace_shade<V, TRI, true>, 128, 0));
+    CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace_shade<V, TRI, false>, 128, 0));
+    CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shadow<V, TRI>, 128, 0));
+    return CWP_OK;
+}
+
+// ev: 4 events (trace start/end, shadow start/end) or nullptr
+template <int V, int TRI> void launch_depth(cwp_renderer* r, KArgs a, int gt0, int gt, int gs, cudaEvent_t* ev) {
+    if (ev) cudaEventRecord(ev[0], r->st);
+    if (a.depth == 0) k_trace_shade<V, TRI, true><<<gt0, 128, 0, r->st>>>(a, r->P);
+    else k_trace_shade<V, TRI, false><<<gt, 128, 0, r->st>>>(a, r->P);
+    if (ev) { cudaEventRecord(ev[1], r->st); cudaEventRecord(ev[2], r->st); }
+    k_shadow<V, TRI><<<gs, 128, 0, r->st>>>(a);
+    if (ev) cudaEventRecord(ev[3], r->st);
+}
+
+KArgs base_args(cwp_renderer* r) {
+    KArgs a{};
+    a.nodes = r->scene.nodes; a.tv = r->scene.leafData(); a.tris = r->scene.tris; a.nrm = r->scene.nrm; a.albedo = r->scene.albedo;
+    a.q = r->q; a.accum = r->accum; a.cnt = r->cnt; a.err = r->err; a.nk = (int)r->nk; a.N = r->N;
+    return a;
+}
+
+void dispatch_depth(cwp_renderer* r, KArgs a, int gt0, int gt, int gs, int pass) {
+    const int V = r->scene.variant, T = r->scene.tri;
+    cudaEvent_t* ev = r->O.profile ? &r->ev[((size_t)pass * r->depths + a.depth) * 4] : nullptr;
+    if (V == 2) { if (T) launch_depth<2, 1>(r, a, gt0, gt, gs, ev); else launch_depth<2, 0>(r, a, gt0, gt, gs, ev); }
+    else if (V == 4) { if (T) launch_depth<4, 1>(r, a, gt0, gt, gs, ev); else launch_depth<4, 0>(r, a, gt0, gt, gs, ev); }
+    else { if (T) launch_depth<8, 1>(r, a, gt0, gt, gs, ev); else launch_depth<8, 0>(r, a, gt0, gt, gs, ev); }
+}
+
+// profiling events for `passes` passes (created on first need, kept)
+int ensure_events(cwp_renderer* r, int passes) {
+    const size_t need = (size_t)passes * r->depths * 4;
+    while (r->ev.size() < need) { cudaEvent_t e; CWPB_CUDA(cudaEventCreate(&e)); r->ev.push_back(e); }
+    r->evPasses = passes;
+    return CWP_OK;
+}
+
+// all passes of a frame with device-side queue lengths and persistent grids (the captured sequence)
+int enqueue_passes(cwp_renderer* r, int spp, int sBase) {
+    const int nInts = 4 * (r->depths + 1);
+    for (int s = sBase, pass = 0; s < sBase + spp; s += r->K, pass++) {
+        k_pass_begin<<<1, 128, 0, r->st>>>(r->cnt, nInts, (int)r->nk);
+        KArgs a = base_args(r); a.sBase = s;
+        for (int d = 0; d < r->depths; d++) { a.depth = d; dispatch_depth(r, a, r->gridTrace0, r->gridTrace, r->gridShadow, pass); }
+        k_pass_end<<<1, 32, 0, r->st>>>(r->cnt, r->depths, r->tot);
+    }
+    CWPB_CUDA(cudaGetLastError());
+    return CWP_OK;
+}
+
+void release(cwp_renderer* r) {
+    if (r->st) cudaStreamSynchronize(r->st);
+    for (cudaEvent_t e : r->ev) cudaEventDestroy(e);
+    r->ev.clear(); r->evPasses = 0;
+    if (r->gexec) cudaGraphExecDestroy(r->gexec);
+    r->gexec = nullptr; r->gSpp = -1;
+    for (void* p : r->allocs) cudaFree(p);
+    r->allocs.clear();
+    if (r->hcnt) cudaFreeHost(r->hcnt);
+    r->hcnt = nullptr;
+    free_scene(r->scene);
+    r->ready = false;
+}
+
+}  // namespace
+
+extern "C" int cwp_renderer_create(cwp_renderer** out) {
+    CWPB_CHECK(out, CWP_ERR_INVALID, "out is NULL");
+    *out = new cwp_renderer();
+    return CWP_OK;
+}
+
+extern "C" void cwp_renderer_destroy(cwp_renderer* r) {
+    if (!r) return;
+    cudaSetDevice(r->O.device);
+    release(r);
+    if (r->st) cudaStreamDestroy(r->st);
+    if (r->f0) cudaEventDestroy(r->f0);
+    if (r->f1) cudaEventDestroy(r->f1);
+    delete r;
+}
+
+extern "C" int cwp_renderer_init(cwp_renderer* r, const cwp_params* p, const cwp_scene_buffers* s, const cwp_render_options* o) {
+    CWPB_CHECK(r && p && s && o, CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(p->cam.w > 0 && p->cam.h > 0, CWP_ERR_INVALID, "image size %dx%d", p->cam.w, p->cam.h);
+    CWPB_CHECK(o->batch >= 1, CWP_ERR_INVALID, "batch must be >= 1");
+    CWPB_CHECK(o->bounces >= 0 && o->bounces <= 1000, CWP_ERR_INVALID, "bounces out of range");
+    CWPB_CHECK(p->max_b <= o->bounces, CWP_ERR_INVALID, "params max_b %d exceeds the initialised bounce limit %d", p->max_b, o->bounces);
+    const long long nk = (long long)p->cam.w * p->cam.h * o->batch;
+    CWPB_CHECK(nk < (1ll << 31), CWP_ERR_INVALID, "w*h*batch = %lld paths in flight exceeds 2^31", nk);
+    CWPB_CUDA(cudaSetDevice(o->device));
+    release(r);
+    size_t free0 = 0, total = 0;
+    CWPB_CUDA(cudaMemGetInfo(&free0, &total));
+    if (int rc = upload_scene(s, o->tri, o->device, r->scene)) return rc;
+    CWPB_CHECK(r->scene.variant == o->variant, CWP_ERR_INVALID, "options.variant %d does not match the node stride (layout %d)", o->variant, r->scene.variant);
+    r->P = *p; r->O = *o;
+    r->N = p->cam.w * p->cam.h; r->K = o->batch; r->nk = nk; r->depths = o->bounces + 2;
+    if (!r->st) { CWPB_CUDA(cudaStreamCreateWithFlags(&r->st, cudaStreamNonBlocking)); CWPB_CUDA(cudaEventCreate(&r->f0)); CWPB_CUDA(cudaEventCreate(&r->f1)); }
+    auto alloc = [&](void** dst, size_t bytes) -> int {
+        cudaError_t e = cudaMalloc(dst, bytes);
+        if (e != cudaSuccess) { release(r); return set_error(CWP_ERR_NOMEM, "cannot allocate %.1f MB of path state: %s", bytes / 1e6, cudaGetErrorString(e)); }
+        r->allocs.push_back(*dst); return CWP_OK;
+    };
+    const size_t NK = (size_t)nk;
+    int rc = 0;
+    for (int b = 0; b < 2 && !rc; b++) {
+        rc = alloc((void**)&r->q.s0[b], NK * 16); if (!rc) rc = alloc((void**)&r->q.s1[b], NK * 16); if (!rc) rc = alloc((void**)&r->q.s2[b], NK * 8);
+    }
+    if (!rc) rc = alloc((void**)&r->q.h0, NK * 16);
+    if (!rc) rc = alloc((void**)&r->q.h1, NK * 16);
+    if (!rc) rc = alloc((void**)&r->q.h2, NK * 8);
+    if (!rc) rc = alloc((void**)&r->accum, (size_t)r->N * 16);
+    if (!rc) rc = alloc((void**)&r->cnt, (size_t)4 * (r->depths + 1) * sizeof(int));
+    if (!rc) rc = alloc((void**)&r->err, sizeof(int));
+    if (!rc) rc = alloc((void**)&r->tot, 2 * (size_t)r->depths * sizeof(unsigned long long));
+    if (rc) return rc;
+    CWPB_CUDA(cudaMallocHost(&r->hcnt, (size_t)4 * (r->depths + 1) * sizeof(int)));
+    CWPB_CUDA(cudaMemset(r->err, 0, sizeof(int)));
+    CWPB_CUDA(cudaMemset(r->accum, 0, (size_t)r->N * 16));
+    size_t free1 = 0; CWPB_CUDA(cudaMemGetInfo(&free1, &total));
+    r->vramMB = (double)(free0 - free1) / 1048576.0;
+    cudaDeviceProp prop; CWPB_CUDA(cudaGetDeviceProperties(&prop, o->device));
+    r->gpuName = prop.name; r->nSM = prop.multiProcessorCount;
+    int bt0 = 0, bt = 0, bs = 0;
+    const int V = r->scene.variant, T = r->scene.tri;
+    if (V == 2) rc = T ? occupancy_of<2, 1>(bt0, bt, bs) : occupancy_of<2, 0>(bt0, bt, bs);
+    else if (V == 4) rc = T ? occupancy_of<4, 1>(bt0, bt, bs) : occupancy_of<4, 0>(bt0, bt, bs);
+    else rc = T ? occupancy_of<8, 1>(bt0, bt, bs) : occupancy_of<8, 0>(bt0, bt, bs);
+    if (rc) return rc;
+    r->gridTrace0 = bt0 * r->nSM; r->gridTrace = bt * r->nSM; r->gridShadow = bs * r->nSM;
+    r->ready = true;
+    return CWP_OK;
+}
+
+extern "C" int cwp_renderer_render(cwp_renderer* r, int32_t spp, cwp_frame_stats* st, int32_t sBase, int32_t clear) {
+    CWPB_CHECK(r && st, CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(r->ready, CWP_ERR_STATE, "render before a successful init");
+    CWPB_CHECK(spp > 0 && spp % r->K == 0, CWP_ERR_INVALID, "spp %d must be a positive multiple of batch %d", spp, r->K);
+    CWPB_CHECK(sBase >= 0, CWP_ERR_INVALID, "negative sample base");
+    CWPB_CUDA(cudaSetDevice(r->O.device));
+    *st = cwp_frame_stats{};
+    if (clear) CWPB_CUDA(cudaMemsetAsync(r->accum, 0, (size_t)r->N * 16, r->st));
+    CWPB_CUDA(cudaMemsetAsync(r->tot, 0, 2 * (size_t)r->depths * sizeof(unsigned long long), r->st));
+    const int passes = spp / r->K;
+    if (r->O.profile && r->evPasses < passes) {
+        if (r->gexec) { CWPB_CUDA(cudaGraphExecDestroy(r->gexec)); r->gexec = nullptr; r->gSpp = -1; }   // events are captured nodes
+        if (int rc = ensure_events(r, passes)) return rc;
+    }
+    CWPB_CUDA(cudaEventRecord(r->f0, r->st));
+    if (r->O.graph) {
+        if (!r->gexec || r->gSpp != spp || r->gBase != sBase) {   // the sample range is part of the captured launches
+            if (r->gexec) { CWPB_CUDA(cudaGraphExecDestroy(r->gexec)); r->gexec = nullptr; }
+            cudaGraph_t g;
+            CWPB_CUDA(cudaStreamBeginCapture(r->st, cudaStreamCaptureModeThreadLocal));
+            int rc = enqueue_passes(r, spp, sBase);
+            cudaError_t e = cudaStreamEndCapture(r->st, &g);
+            if (rc) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
+            CWPB_CUDA(e);
+            e = cudaGraphInstantiate(&r->gexec, g, 0);
+            cudaGraphDestroy(g);
+            CWPB_CUDA(e);
+            r->gSpp = spp; r->gBase = sBase;
+        }
+        CWPB_CUDA(cudaGraphLaunch(r->gexec, r->st));
+    } else {
+        // host loop: exact grids from the queue lengths read back after each depth (one sync per bounce)
+        const int nInts = 4 * (r->depths + 1);
+        for (int s = sBase, pass = 0; s < sBase + spp; s += r->K, pass++) {
+            k_pass_begin<<<1, 128, 0, r->st>>>(r->cnt, nInts, (int)r->nk);
+            KArgs a = base_args(r); a.sBase = s;
+            int n = (int)r->nk;
+            if (r->O.profile) for (int d = 0; d < r->depths; d++) for (int j = 0; j < 4; j++) CWPB_CUDA(cudaEventRecord(r->ev[((size_t)pass * r->depths + d) * 4 + j], r->st));
+            for (int d = 0; d < r->depths && n > 0; d++) {
+                a.depth = d;
+                const int need = (n + 127) / 128;
+                const int gt = need < r->gridTrace ? need : r->gridTrace, gt0 = need < r->gridTrace0 ? need : r->gridTrace0;
+                dispatch_depth(r, a, gt0, gt, r->gridShadow, pass);
+                CWPB_CUDA(cudaMemcpyAsync(r->hcnt, r->cnt, (size_t)nInts * sizeof(int), cudaMemcpyDeviceToHost, r->st));
+                CWPB_CUDA(cudaStreamSynchronize(r->st));
+                n = r->hcnt[4 * (d + 1)];
+            }
+            k_pass_end<<<1, 32, 0, r->st>>>(r->cnt, r->depths, r->tot);
+        }
+        CWPB_CUDA(cudaGetLastError());
+    }
+    CWPB_CUDA(cudaEventRecord(r->f1, r->st));
+    CWPB_CUDA(cudaEventSynchronize(r->f1));
+    float ms = 0.f; CWPB_CUDA(cudaEventElapsedTime(&ms, r->f0, r->f1));
+    int herr = 0;
+    r->htot.assign(2 * (size_t)r->depths, 0);
+    CWPB_CUDA(cudaMemcpy(r->htot.data(), r->tot, r->htot.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    CWPB_CUDA(cudaMemcpy(&herr, r->err, sizeof(int), cudaMemcpyDeviceToHost));
+    double rays = 0, shadow = 0;
+    for (int d = 0; d < r->depths; d++) { rays += (double)r->htot[2 * d]; shadow += (double)r->htot[2 * d + 1]; }
+    st->frame_ms = ms; st->trace_ms = ms; st->rays = rays; st->shadow_rays = shadow;
+    r->traceMs.assign(r->depths, 0.f); r->shadowMs.assign(r->depths, 0.f);
+    if (r->O.profile) {
+        for (int pass = 0; pass < passes; pass++)
+            for (int d = 0; d < r->depths; d++) {
+                cudaEvent_t* e = &r->ev[((size_t)pass * r->depths + d) * 4]; float a = 0.f, b = 0.f;
+                CWPB_CUDA(cudaEventElapsedTime(&a, e[0], e[1])); CWPB_CUDA(cudaEventElapsedTime(&b, e[2], e[3]));
+                r->traceMs[d] += a; r->shadowMs[d] += b;
+            }
+        double t = 0; for (int d = 0; d < r->depths; d++) t += r->traceMs[d] + r->shadowMs[d];
+        st->trace_ms = t;
+    }
+    if (herr) { cudaMemset(r->err, 0, sizeof(int)); return set_error(CWP_ERR_TRAVERSAL, "traversal stopped early on some rays (status 0x%x)", herr); }
+    return CWP_OK;
+}
+
+extern "C" int cwp_renderer_read_accum(const cwp_renderer* r, float* dst) {
+    CWPB_CHECK(r && dst, CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(r->ready, CWP_ERR_STATE, "read before a successful init");
+    CWPB_CUDA(cudaSetDevice(r->O.device));
+    CWPB_CUDA(cudaStreamSynchronize(r->st));
+    CWPB_CUDA(cudaMemcpy(dst, r->accum, (size_t)r->N * 16, cudaMemcpyDeviceToHost));
+    return CWP_OK;
+}
+
+extern "C" const void* cwp_renderer_accum_device(const cwp_renderer* r) { return r ? r->accum : nullptr; }
+
+extern "C" int cwp_renderer_set_params(cwp_renderer* r, const cwp_params* p) {
+    CWPB_CHECK(r && p, CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(r->ready, CWP_ERR_STATE, "set_params before a successful init");
+    CWPB_CHECK(p->cam.w == r->P.cam.w && p->cam.h == r->P.cam.h, CWP_ERR_INVALID, "image size cannot change after init");
+    CWPB_CHECK(p->max_b <= r->O.bounces, CWP_ERR_INVALID, "max_b %d exceeds the initialised bounce limit %d", p->max_b, r->O.bounces);
+    CWPB_CUDA(cudaSetDevice(r->O.device));
+    CWPB_CUDA(cudaStreamSynchronize(r->st));
+    r->P = *p;
+    if (r->gexec) { CWPB_CUDA(cudaGraphExecDestroy(r->gexec)); r->gexec = nullptr; r->gSpp = -1; }   // parameters are baked into the graph
+    return CWP_OK;
+}
+
+extern "C" int cwp_renderer_set_materials(cwp_renderer* r, const float* albedo, int32_t n) {
+    CWPB_CHECK(r && albedo, CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(r->ready, CWP_ERR_STATE, "set_materials before a successful init");
+    CWPB_CHECK(n == r->scene.nAlbedo, CWP_ERR_INVALID, "material count %d differs from the initialised %d", n, r->scene.nAlbedo);
+    CWPB_CUDA(cudaSetDevice(r->O.device));
+    CWPB_CUDA(cudaStreamSynchronize(r->st));
+    std::vector<float3> a(n);
+    for (int i = 0; i < n; i++) a[i] = make_float3(albedo[3 * i], albedo[3 * i + 1], albedo[3 * i + 2]);
+    CWPB_CUDA(cudaMemcpy(r->scene.albedo, a.data(), n * sizeof(float3), cudaMemcpyHostToDevice));
+    return CWP_OK;
+}
+
+extern "C" int cwp_renderer_depth_stats(const cwp_renderer* r, int64_t* closest, int64_t* shadow, float* trace_ms, float* shadow_ms, int32_t n) {
+    CWPB_CHECK(r, CWP_ERR_INVALID, "NULL renderer");
+    CWPB_CHECK(n >= 0, CWP_ERR_INVALID, "negative depth count");
+    for (int d = 0; d < n; d++) {
+        const bool have = d < r->depths && r->htot.size() == 2 * (size_t)r->depths;
+        if (closest) closest[d] = have ? (int64_t)r->htot[2 * d] : 0;
+        if (shadow) shadow[d] = have ? (int64_t)r->htot[2 * d + 1] : 0;
+        if (trace_ms) trace_ms[d] = d < (int)r->traceMs.size() ? r->traceMs[d] : 0.f;
+        if (shadow_ms) shadow_ms[d] = d < (int)r->shadowMs.size() ? r->shadowMs[d] : 0.f;
+    }
+    return CWP_OK;
+}
+
+extern "C" int cwp_renderer_info_of(const cwp_renderer* r, cwp_renderer_info* out) {
+    CWPB_CHECK(r && out, CWP_ERR_INVALID, "NULL argument");
+    memset(out, 0, sizeof *out);
+    out->vram_mb = r->vramMB; out->tlas_ms = 0; out->pt_blocks = r->gridTrace; out->n_sm = r->nSM;
+    snprintf(out->gpu_name, sizeof out->gpu_name, "%s", r->gpuName.c_str());
+    return CWP_OK;
+}

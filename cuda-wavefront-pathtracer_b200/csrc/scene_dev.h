@@ -1,0 +1,25 @@
+// scene_dev.h - device copy of a scene's nodes and triangles, shared by the ray-batch and renderer entry points.
+#pragma once
+#include "runtime.h"
+#include <cstdint>
+
+namespace cwpb {
+
+struct DeviceScene {
+    int device = 0, variant = 2, tri = 1;
+    float4* nodes = nullptr; int64_t nNodes = 0;     // nodes in units of one node (stride float4 each)
+    float4* tris = nullptr; int64_t nTris = 0;       // (v0, id), (e1, mat), (e2, 0)
+    float4* woop = nullptr;                          // Woop rows or nullptr
+    float4* nrm = nullptr;                           // per-corner normals or nullptr
+    float3* albedo = nullptr; int nAlbedo = 0;
+    size_t bytes = 0;
+    const float4* leafData() const { return tri == 1 ? woop : tris; }
+};
+
+// Checks every child and leaf reference of the node array against the buffer sizes (so that no traversal can read
+// out of bounds), then uploads. variant comes from the node stride (4 -> BVH2, 8 -> BVH4, 5 -> CWBVH).
+int upload_scene(const cwp_scene_buffers* s, int tri, int device, DeviceScene& out);
+void free_scene(DeviceScene& s);
+int validate_nodes(const float* nodes, int64_t nF4, int stride, int64_t nTris, int* variantOut);
+
+}  // namespace cwpb

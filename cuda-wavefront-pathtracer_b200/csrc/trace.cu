@@ -1,0 +1,226 @@
+// trace.cu - device scene upload/validation and the standalone closest-hit / any-hit ray-batch kernels.
+#include "scene_dev.h"
+#include "trav.cuh"
+#include <cstring>
+#include <vector>
+
+namespace cwpb {
+
+// ---------------- validation + upload ----------------
+int validate_nodes(const float* nodes, int64_t nF4, int stride, int64_t nTris, int* variantOut) {
+    CWPB_CHECK(nodes && nF4 > 0, CWP_ERR_INVALID, "empty node array");
+    CWPB_CHECK(stride == 4 || stride == 5 || stride == 8, CWP_ERR_INVALID, "node stride %d is not 4 (BVH2), 8 (BVH4) or 5 (CWBVH)", stride);
+    CWPB_CHECK(nF4 % stride == 0, CWP_ERR_INVALID, "node array of %lld float4 is not a multiple of the stride %d", (long long)nF4, stride);
+    const int64_t nNodes = nF4 / stride;
+    const int32_t* w = reinterpret_cast<const int32_t*>(nodes);
+    auto leafOk = [&](int64_t first, int64_t cnt) { return first >= 0 && cnt > 0 && first + cnt <= nTris; };
+    if (stride == 4 || stride == 8) {
+        const int width = stride == 4 ? 2 : 4;
+        for (int64_t n = 0; n < nNodes; n++) {
+            const int32_t* m = w + n * stride * 4 + (stride == 4 ? 12 : 24);
+            for (int j = 0; j < width; j++) {
+                int32_t c = m[j], k = m[j + (stride == 4 ? 2 : 4)];
+                bool ok = k > 0 ? leafOk(c, k) : (k == 0 && (c == -1 || (c >= 0 && c < nNodes)));
+                CWPB_CHECK(ok, CWP_ERR_INVALID, "node %lld child %d: reference (%d, %d) out of range (%lld nodes, %lld triangles)", (long long)n, j, c, k, (long long)nNodes, (long long)nTris);
+            }
+        }
+        *variantOut = stride == 4 ? 2 : 4;
+    } else {
+        for (int64_t n = 0; n < nNodes; n++) {
+            const int32_t* q = w + n * 20;
+            uint32_t ew = (uint32_t)q[3], imask = ew >> 24; int32_t childBase = q[4], triBase = q[5];
+            int nInt = __builtin_popcount(imask);
+            CWPB_CHECK(nInt == 0 || (childBase >= 0 && (int64_t)childBase + nInt <= nNodes), CWP_ERR_INVALID, "CWBVH node %lld: children [%d, +%d) out of range", (long long)n, childBase, nInt);
+            for (int s = 0; s < 8; s++) {
+                uint32_t m = ((uint32_t)q[6 + s / 4] >> (8 * (s & 3))) & 255u;
+                if (m & 0x80u) {
+                    int64_t first = (int64_t)triBase + (m & 31u), cnt = ((m >> 5) & 3u) + 1;
+                    CWPB_CHECK(leafOk(first, cnt), CWP_ERR_INVALID, "CWBVH node %lld slot %d: leaf [%lld, +%lld) out of range", (long long)n, s, (long long)first, (long long)cnt);
+                } else if (m) {
+                    CWPB_CHECK(imask & (1u << s), CWP_ERR_INVALID, "CWBVH node %lld slot %d: internal child without imask bit", (long long)n, s);
+                }
+            }
+        }
+        *variantOut = 8;
+    }
+    return CWP_OK;
+}
+
+void free_scene(DeviceScene& s) {
+    if (s.nodes || s.tris || s.woop || s.nrm || s.albedo) cudaSetDevice(s.device);
+    cudaFree(s.nodes); cudaFree(s.tris); cudaFree(s.woop); cudaFree(s.nrm); cudaFree(s.albedo);
+    s = DeviceScene();
+}
+
+int upload_scene(const cwp_scene_buffers* s, int tri, int device, DeviceScene& out) {
+    CWPB_CHECK(s, CWP_ERR_INVALID, "scene buffers are NULL");
+    CWPB_CHECK(tri == 0 || tri == 1, CWP_ERR_INVALID, "tri must be 0 (Moller-Trumbore) or 1 (Woop)");
+    CWPB_CHECK(s->tris && s->n_tris > 0, CWP_ERR_INVALID, "scene has no triangles");
+    CWPB_CHECK(tri == 0 || s->woop, CWP_ERR_INVALID, "Woop triangle test requested without Woop rows");
+    int variant = 2;
+    if (int rc = validate_nodes(s->nodes, s->n_node_float4, s->node_stride, s->n_tris, &variant)) return rc;
+    free_scene(out);
+    out.device = device; out.variant = variant; out.tri = tri;
+    out.nNodes = s->n_node_float4 / s->node_stride; out.nTris = s->n_tris;
+    CWPB_CUDA(cudaSetDevice(device));
+    auto up = [&](void** dst, const void* src, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(dst, bytes); if (e != cudaSuccess) return e;
+        out.bytes += bytes; return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    };
+    cudaError_t e = up((void**)&out.nodes, s->nodes, (size_t)s->n_node_float4 * 16);
+    if (e == cudaSuccess) e = up((void**)&out.tris, s->tris, (size_t)s->n_tris * 48);
+    if (e == cudaSuccess && s->woop) e = up((void**)&out.woop, s->woop, (size_t)s->n_tris * 48);
+    if (e == cudaSuccess && s->nrm) e = up((void**)&out.nrm, s->nrm, (size_t)s->n_tris * 48);
+    if (e == cudaSuccess) {
+        std::vector<float3> alb;
+        for (int i = 0; i < s->n_albedo; i++) alb.push_back(make_float3(s->albedo[3 * i], s->albedo[3 * i + 1], s->albedo[3 * i + 2]));
+        if (alb.empty()) alb.push_back(make_float3(0.8f, 0.8f, 0.8f));
+        out.nAlbedo = (int)alb.size();
+        e = up((void**)&out.albedo, alb.data(), alb.size() * sizeof(float3));
+    }
+    if (e != cudaSuccess) { free_scene(out); return set_error(e == cudaErrorMemoryAllocation ? CWP_ERR_NOMEM : CWP_ERR_CUDA, "scene upload: %s", cudaGetErrorString(e)); }
+    // every material id referenced by a triangle must have an albedo entry
+    const int32_t* tw = reinterpret_cast<const int32_t*>(s->tris);
+    for (int64_t t = 0; t < s->n_tris; t++) {
+        int32_t mat = tw[t * 12 + 7];
+        if (mat < 0 || mat >= out.nAlbedo) { free_scene(out); return set_error(CWP_ERR_INVALID, "triangle %lld: material %d has no albedo entry", (long long)t, mat); }
+    }
+    return CWP_OK;
+}
+
+// ---------------- ray-batch kernels ----------------
+static constexpr int kBatchBlock = 128;
+
+template <int V, int TRI>
+__global__ void __launch_bounds__(kBatchBlock) k_trace_closest(const float4* __restrict__ nodes, const float4* __restrict__ tv, const float4* __restrict__ ro,
+                                                               const float4* __restrict__ rd, float4* __restrict__ hits, long long n, int* err) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 O = __ldcs(ro + i), D = __ldcs(rd + i);
+    float t = D.w, u = 0.f, v = 0.f; int tri = -1, e = 0;
+    trace_ray<V, false, TRI>(nodes, tv, xyz(O), xyz(D), O.w, t, tri, u, v, 0, e);
+    __stcs(hits + i, make_float4(t, u, v, __int_as_float(tri)));
+    if (e) atomicOr(err, e);
+}
+
+template <int V, int TRI>
+__global__ void __launch_bounds__(kBatchBlock) k_trace_any(const float4* __restrict__ nodes, const float4* __restrict__ tv, const float4* __restrict__ ro,
+                                                           const float4* __restrict__ rd, int* __restrict__ occ, long long n, int* err) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 O = __ldcs(ro + i), D = __ldcs(rd + i);
+    float t = D.w, u = 0.f, v = 0.f; int tri = -1, e = 0;
+    trace_ray<V, true, TRI>(nodes, tv, xyz(O), xyz(D), O.w, t, tri, u, v, 0, e);
+    __stcs(occ + i, tri);
+    if (e) atomicOr(err, e);
+}
+
+template <bool ANY>
+static int launch_batch(const DeviceScene& s, const float4* o, const float4* d, void* out, long long n, int* err, cudaStream_t st) {
+    if (n <= 0) return CWP_OK;
+    const unsigned grid = (unsigned)((n + kBatchBlock - 1) / kBatchBlock);
+    const float4* tv = s.leafData();
+#define CWPB_L(VV, TT) do { if (ANY) k_trace_any<VV, TT><<<grid, kBatchBlock, 0, st>>>(s.nodes, tv, o, d, (int*)out, n, err); \
+                            else k_trace_closest<VV, TT><<<grid, kBatchBlock, 0, st>>>(s.nodes, tv, o, d, (float4*)out, n, err); } while (0)
+    if (s.variant == 2) { if (s.tri) CWPB_L(2, 1); else CWPB_L(2, 0); }
+    else if (s.variant == 4) { if (s.tri) CWPB_L(4, 1); else CWPB_L(4, 0); }
+    else { if (s.tri) CWPB_L(8, 1); else CWPB_L(8, 0); }
+#undef CWPB_L
+    CWPB_CUDA(cudaGetLastError());
+    return CWP_OK;
+}
+
+}  // namespace cwpb
+
+using namespace cwpb;
+
+struct cwp_accel {
+    DeviceScene scene;
+    int* err = nullptr;                 // device traversal status bits
+    cudaStream_t st = nullptr;          // stream of the host-buffer entry points
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float4 *bo = nullptr, *bd = nullptr; void* bh = nullptr; size_t cap = 0;   // staging for host-buffer calls
+};
+
+extern "C" int cwp_accel_create(const cwp_scene_buffers* s, int32_t tri, int32_t device, cwp_accel** out) {
+    CWPB_CHECK(out, CWP_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    cwp_accel* a = new cwp_accel();
+    int rc = upload_scene(s, tri, device, a->scene);
+    if (rc) { delete a; return rc; }
+    cudaError_t e = cudaMalloc(&a->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(a->err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&a->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&a->e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&a->e1);
+    if (e != cudaSuccess) { cwp_accel_destroy(a); return set_error(CWP_ERR_CUDA, "accel setup: %s", cudaGetErrorString(e)); }
+    *out = a;
+    return CWP_OK;
+}
+
+extern "C" void cwp_accel_destroy(cwp_accel* a) {
+    if (!a) return;
+    cudaSetDevice(a->scene.device);
+    if (a->st) cudaStreamSynchronize(a->st);
+    cudaFree(a->err); cudaFree(a->bo); cudaFree(a->bd); cudaFree(a->bh);
+    if (a->st) cudaStreamDestroy(a->st);
+    if (a->e0) cudaEventDestroy(a->e0);
+    if (a->e1) cudaEventDestroy(a->e1);
+    free_scene(a->scene);
+    delete a;
+}
+
+extern "C" int cwp_trace_closest(cwp_accel* a, const float* o, const float* d, float* hits, int64_t n, void* stream) {
+    CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
+    CWPB_CHECK(n >= 0, CWP_ERR_INVALID, "negative ray count");
+    CWPB_CHECK(n == 0 || (o && d && hits), CWP_ERR_INVALID, "NULL ray or hit buffer");
+    CWPB_CUDA(cudaSetDevice(a->scene.device));
+    return launch_batch<false>(a->scene, (const float4*)o, (const float4*)d, hits, n, a->err, (cudaStream_t)stream);
+}
+
+extern "C" int cwp_trace_any(cwp_accel* a, const float* o, const float* d, int32_t* occ, int64_t n, void* stream) {
+    CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
+    CWPB_CHECK(n >= 0, CWP_ERR_INVALID, "negative ray count");
+    CWPB_CHECK(n == 0 || (o && d && occ), CWP_ERR_INVALID, "NULL ray or result buffer");
+    CWPB_CUDA(cudaSetDevice(a->scene.device));
+    return launch_batch<true>(a->scene, (const float4*)o, (const float4*)d, occ, n, a->err, (cudaStream_t)stream);
+}
+
+template <bool ANY>
+static int host_call(cwp_accel* a, const float* o, const float* d, void* res, int64_t n, float* ms) {
+    CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
+    CWPB_CHECK(n >= 0, CWP_ERR_INVALID, "negative ray count");
+    CWPB_CHECK(n == 0 || (o && d && res), CWP_ERR_INVALID, "NULL host buffer");
+    if (ms) *ms = 0.f;
+    if (n == 0) return CWP_OK;
+    CWPB_CUDA(cudaSetDevice(a->scene.device));
+    const size_t resBytes = ANY ? 4 : 16;
+    if ((size_t)n > a->cap) {
+        cudaFree(a->bo); cudaFree(a->bd); cudaFree(a->bh); a->bo = a->bd = nullptr; a->bh = nullptr; a->cap = 0;
+        CWPB_CUDA(cudaMalloc(&a->bo, (size_t)n * 16)); CWPB_CUDA(cudaMalloc(&a->bd, (size_t)n * 16)); CWPB_CUDA(cudaMalloc(&a->bh, (size_t)n * 16));
+        a->cap = (size_t)n;
+    }
+    CWPB_CUDA(cudaEventRecord(a->e0, a->st));
+    CWPB_CUDA(cudaMemcpyAsync(a->bo, o, (size_t)n * 16, cudaMemcpyHostToDevice, a->st));
+    CWPB_CUDA(cudaMemcpyAsync(a->bd, d, (size_t)n * 16, cudaMemcpyHostToDevice, a->st));
+    if (int rc = launch_batch<ANY>(a->scene, a->bo, a->bd, a->bh, n, a->err, a->st)) return rc;
+    CWPB_CUDA(cudaMemcpyAsync(res, a->bh, (size_t)n * resBytes, cudaMemcpyDeviceToHost, a->st));
+    CWPB_CUDA(cudaEventRecord(a->e1, a->st));
+    CWPB_CUDA(cudaEventSynchronize(a->e1));
+    if (ms) CWPB_CUDA(cudaEventElapsedTime(ms, a->e0, a->e1));
+    return CWP_OK;
+}
+
+extern "C" int cwp_trace_closest_host(cwp_accel* a, const float* o, const float* d, float* hits, int64_t n, float* ms) { return host_call<false>(a, o, d, hits, n, ms); }
+extern "C" int cwp_trace_any_host(cwp_accel* a, const float* o, const float* d, int32_t* occ, int64_t n, float* ms) { return host_call<true>(a, o, d, occ, n, ms); }
+
+extern "C" int cwp_accel_status(cwp_accel* a) {
+    CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
+    CWPB_CUDA(cudaSetDevice(a->scene.device));
+    CWPB_CUDA(cudaDeviceSynchronize());
+    int h = 0;
+    CWPB_CUDA(cudaMemcpy(&h, a->err, sizeof(int), cudaMemcpyDeviceToHost));
+    CWPB_CUDA(cudaMemset(a->err, 0, sizeof(int)));
+    CWPB_CHECK(h == 0, CWP_ERR_TRAVERSAL, "traversal stopped early on some rays (status bits 0x%x: 1 = stack bound, 2 = visit budget)", h);
+    return CWP_OK;
+}

@@ -1,0 +1,179 @@
+/* cwp_b200.h - C ABI of the B200 wavefront path tracer (libcwpb200.so).
+ *
+ * Every entry point returns CWP_OK (0) or an error code; cwp_last_error() gives the message of the last failure on
+ * the calling thread. No entry point exits the process. Handles are not thread-safe: use one handle per host thread
+ * (the reference renderer has the same single-thread rule). Device pointers are CUDA global-memory addresses on the
+ * handle's device; host pointers are ordinary process memory. All float4 arrays are 16-byte aligned, x y z w.
+ *
+ * Each declaration names the reference interface it replaces (file:line in YJLi-new/cuda-wavefront-pathtracer).
+ */
+#ifndef CWP_B200_H
+#define CWP_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CWP_OK 0
+#define CWP_ERR_INVALID 1      /* bad argument or malformed buffer */
+#define CWP_ERR_CUDA 2         /* CUDA runtime error */
+#define CWP_ERR_NOMEM 3        /* device or host allocation failed, or admission refused */
+#define CWP_ERR_STATE 4        /* call out of order (e.g. render before init) */
+#define CWP_ERR_TRAVERSAL 5    /* a ray hit the traversal stack bound or visit budget (malformed or too deep BVH) */
+#define CWP_ERR_IO 6           /* file unreadable / unwritable */
+
+#define CWP_LAYOUT_BVH2 2
+#define CWP_LAYOUT_BVH4 4
+#define CWP_LAYOUT_CWBVH 8
+#define CWP_TRI_MT 0           /* Moller-Trumbore on (v0, e1, e2) */
+#define CWP_TRI_WOOP 1         /* Woop unit-triangle rows */
+#define CWP_FILTER_TABLE 64
+
+const char* cwp_last_error(void);
+int32_t cwp_version(void);
+
+/* ------------------------------------------------------------------------------------------------------------------
+ * Meshes and the synthetic box field. Replaces Mesh (scene/mesh.h:9-26), loadMesh/loadOBJ/loadPLY
+ * (io/mesh_loader.h:6-8); the box field has no reference counterpart (the reference's synthetic scene is a sphere
+ * grid, scene/synthetic.cpp:6-48).
+ * ------------------------------------------------------------------------------------------------------------------ */
+typedef struct cwp_mesh cwp_mesh;
+typedef struct cwp_mesh_view {
+    const float* verts; int64_t n_verts;       /* 3 floats per vertex */
+    const int32_t* faces; int64_t n_tris;      /* 3 vertex indices per triangle */
+    const int32_t* face_mat;                   /* material id per triangle or NULL */
+    const float* normals;                      /* 3 floats per vertex or NULL */
+    const float* albedo; int32_t n_albedo;     /* 3 floats per material */
+} cwp_mesh_view;
+
+int cwp_mesh_box_field(int32_t n_boxes, uint64_t seed, cwp_mesh** out);
+int cwp_mesh_load(const char* path, cwp_mesh** out);
+int cwp_mesh_from_view(const cwp_mesh_view* v, cwp_mesh** out);
+int cwp_mesh_view_of(const cwp_mesh* m, cwp_mesh_view* out);
+int cwp_mesh_write_ply(const cwp_mesh* m, const char* path);
+void cwp_mesh_free(cwp_mesh* m);
+
+/* ------------------------------------------------------------------------------------------------------------------
+ * Host BVH construction. Replaces BVHBuilder::build (accel/bvh_builder.cpp:5-68), BVH2Flat/BVH4Flat/BVH8Flat::build
+ * (accel/bvh_layouts.cpp:24,57,97), CWBVH::build (accel/bvh_tools.cpp:75), sahCost (bvh_tools.cpp:40),
+ * packTriangles / packWoop (accel/tri_pack.cpp:6,18) and the layout step of setupScene (app/scene_setup.cpp:190-222).
+ * Output encodings are byte-identical to the reference's at bins = 16.
+ * ------------------------------------------------------------------------------------------------------------------ */
+typedef struct cwp_build_options {
+    int32_t variant;    /* CWP_LAYOUT_* */
+    int32_t bins;       /* SAH bins per axis, 2..256 (reference: 16) */
+    int32_t leaf;       /* max triangles per leaf (reference --leaf, default 4; CWBVH SAH collapse builds from leaf 1) */
+    int32_t collapse;   /* CWBVH: 0 SAH dynamic programme, 1 greedy */
+    int32_t threads;    /* host threads, 0 = all */
+} cwp_build_options;
+
+typedef struct cwp_bvh cwp_bvh;
+typedef struct cwp_bvh_data {
+    const float* nodes; int64_t n_node_float4; int32_t node_stride;   /* 4 (BVH2), 8 (BVH4) or 5 (CWBVH) float4 per node */
+    const int32_t* order; int64_t n_tris;                              /* leaf order of the mesh triangles */
+    const float* tris;                                                 /* 3 float4 per triangle, leaf order */
+    const float* nrm;                                                  /* 3 float4 per triangle or NULL */
+    const float* woop;                                                 /* 3 float4 per triangle */
+    int32_t max_depth, max_leaf_tris;
+    double sah, build_ms;
+} cwp_bvh_data;
+
+int cwp_bvh_build(const cwp_mesh* m, const cwp_build_options* opt, cwp_bvh** out);
+int cwp_bvh_data_of(const cwp_bvh* b, cwp_bvh_data* out);   /* pointers stay valid until cwp_bvh_free */
+void cwp_bvh_free(cwp_bvh* b);
+
+/* ------------------------------------------------------------------------------------------------------------------
+ * Device scene + standalone ray batches. Replaces the device traversal trav<V,ANY,TRI> (accel/traverse.cuh:155-160)
+ * as used by traceOne / shadowOne (render/wavefront.cu:61-72); the batch entry point itself is new.
+ * Rays: o = (ox, oy, oz, tmin), d = (dx, dy, dz, tmax) float4 arrays. Closest hits: float4 (t, u, v, tri bits) with
+ * tri = leaf-order triangle index or -1 (t = tmax on a miss). Any-hit: int32 index of the first occluder found or -1.
+ * ------------------------------------------------------------------------------------------------------------------ */
+typedef struct cwp_scene_buffers {
+    const float* nodes; int64_t n_node_float4; int32_t node_stride;
+    const float* tris; int64_t n_tris;
+    const float* nrm;       /* or NULL */
+    const float* woop;      /* or NULL (required for CWP_TRI_WOOP) */
+    const float* albedo; int32_t n_albedo;
+} cwp_scene_buffers;
+
+typedef struct cwp_accel cwp_accel;
+int cwp_accel_create(const cwp_scene_buffers* s, int32_t tri, int32_t device, cwp_accel** out);
+void cwp_accel_destroy(cwp_accel* a);
+/* stream: a cudaStream_t or NULL (legacy default stream); asynchronous with respect to the host */
+int cwp_trace_closest(cwp_accel* a, const float* d_o, const float* d_d, float* d_hits, int64_t n, void* stream);
+int cwp_trace_any(cwp_accel* a, const float* d_o, const float* d_d, int32_t* d_occluder, int64_t n, void* stream);
+/* host buffers; copies in, traces, copies out, synchronises; *ms = device time of the whole call (may be NULL) */
+int cwp_trace_closest_host(cwp_accel* a, const float* o, const float* d, float* hits, int64_t n, float* ms);
+int cwp_trace_any_host(cwp_accel* a, const float* o, const float* d, int32_t* occluder, int64_t n, float* ms);
+/* traversal status of the calls since the last query (CWP_OK or CWP_ERR_TRAVERSAL); clears it */
+int cwp_accel_status(cwp_accel* a);
+
+/* ------------------------------------------------------------------------------------------------------------------
+ * Wavefront renderer. Replaces class WavefrontRenderer (render/renderer.h:47-93): init (wavefront.cu:469-502),
+ * render (wavefront.cu:684-741 legacy loop, 644-680 graph frame), readAccum / accumDevice (renderer.h:58-59),
+ * setParams / setMaterials (wavefront.cu:744-752), introspection (renderer.h:69). Params mirrors render/params.h:8-16,
+ * RenderOptions renderer.h:11-28, FrameStats renderer.h:45. The accumulation buffer holds w*h float4 radiance sums.
+ * ------------------------------------------------------------------------------------------------------------------ */
+typedef struct cwp_camera {
+    float pos[3], ax[3], ay[3], az[3];   /* camera looks down -az, +ay up (scene/camera.h:7) */
+    float fx, fy, px, py;
+    int32_t w, h;
+    float lens_r, focus_d;
+} cwp_camera;
+
+typedef struct cwp_params {
+    cwp_camera cam;
+    float sun_to[3], sun_e[3], sky[3];
+    float sun_cos;                       /* cos of the sun's angular radius */
+    int32_t max_b; uint32_t seed;
+    float eps, near_clip;
+    int32_t has_n, filter_bh;
+    float ftab[CWP_FILTER_TABLE + 1];    /* pixel-filter inverse CDF (used when filter_bh) */
+} cwp_params;
+
+typedef struct cwp_render_options {
+    int32_t variant;      /* CWP_LAYOUT_* of the scene's nodes */
+    int32_t tri;          /* CWP_TRI_* */
+    int32_t batch;        /* samples per pixel in flight per wavefront pass */
+    int32_t bounces;      /* max bounce depth (camera hit = 0) */
+    int32_t graph;        /* 1: each frame is one CUDA graph with device-side queue counts; 0: host loop */
+    int32_t block;        /* threads per block of the traversal kernels (0 = 128) */
+    int32_t device;       /* CUDA device ordinal */
+    int32_t profile;      /* 1: CUDA event pair around every kernel launch (also inside the graph), see cwp_renderer_depth_stats */
+    int32_t reserved[4];
+} cwp_render_options;
+
+typedef struct cwp_frame_stats { double rays, shadow_rays, trace_ms, frame_ms; } cwp_frame_stats;
+typedef struct cwp_renderer_info { double vram_mb, tlas_ms; int32_t pt_blocks, n_sm; char gpu_name[256]; } cwp_renderer_info;
+
+typedef struct cwp_renderer cwp_renderer;
+int cwp_renderer_create(cwp_renderer** out);
+int cwp_renderer_init(cwp_renderer* r, const cwp_params* p, const cwp_scene_buffers* s, const cwp_render_options* o);
+int cwp_renderer_render(cwp_renderer* r, int32_t spp, cwp_frame_stats* st, int32_t s_base, int32_t clear);
+int cwp_renderer_read_accum(const cwp_renderer* r, float* dst);      /* w*h*4 floats */
+const void* cwp_renderer_accum_device(const cwp_renderer* r);
+int cwp_renderer_set_params(cwp_renderer* r, const cwp_params* p);
+int cwp_renderer_set_materials(cwp_renderer* r, const float* albedo, int32_t n);
+int cwp_renderer_info_of(const cwp_renderer* r, cwp_renderer_info* out);
+/* Per-depth figures of the last frame, summed over its passes, for d < n_depths = bounces + 2: closest[d] / shadow[d]
+ * = rays traced at depth d (queue lengths); trace_ms[d] / shadow_ms[d] = device time of the depth-d trace+shade and
+ * shadow kernels (needs options.profile = 1, else zeros). Any pointer may be NULL. (The reference reports these
+ * only as frame totals: FrameStats, renderer.h:45, and t_trace_ms from event pairs, wavefront.cu:700-709.) */
+int cwp_renderer_depth_stats(const cwp_renderer* r, int64_t* closest, int64_t* shadow, float* trace_ms, float* shadow_ms, int32_t n_depths);
+void cwp_renderer_destroy(cwp_renderer* r);
+
+/* ------------------------------------------------------------------------------------------------------------------
+ * Camera and parameter helpers. Replace lookAtC2W / focalFromHfov / makeCamera (scene/camera.cpp:7-23) and the
+ * Params filling of setupScene (app/scene_setup.cpp:175-185, Lighting defaults scene/lighting.h:7-13).
+ * ------------------------------------------------------------------------------------------------------------------ */
+int cwp_camera_look_at(const float pos[3], const float target[3], const float up[3], float hfov_deg, int32_t w, int32_t h, cwp_camera* out);
+int cwp_camera_from_c2w(const float c2w[16], float fx, float fy, int32_t w, int32_t h, cwp_camera* out);
+/* defaults of the reference CLI: sun (0.3,-0.5,0.8) at 3 W/m^2, 0.526 deg, sky 0.3, seed 1000, box filter off */
+int cwp_params_defaults(cwp_params* p);
+int cwp_params_finish(cwp_params* p, float sun_angle_deg, float eps_scale, float scene_extent);   /* normalises sun_to, fills sun_cos, eps, ftab */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

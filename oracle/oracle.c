@@ -1,0 +1,541 @@
+/* oracle.c - TEST INFRASTRUCTURE ONLY: a scalar CPU restatement of the reference path tracer's algorithms for the
+ * diffuse benchmark path (YJLi-new/cuda-wavefront-pathtracer). It is the checker the parity tests compare the CUDA
+ * library against; nothing in the product links or calls it.
+ *
+ * Parity pin: tests/test_oracle_pin.py checks every function here against the reference's own code compiled from
+ * its sources (oracle/_ref, recipe oracle/Makefile) and against the committed fixtures in tests/golden/ that the
+ * reference produced (tests/golden/make_golden.py).
+ *
+ * Arithmetic: compiled with -ffp-contract=off; fused multiply-adds only where written as fmaf(), at the same places
+ * as the CUDA kernels (so traversal results agree bit for bit with them). Where the reference's host build rounds
+ * differently (it has no fused operations), only exact ties can resolve differently.
+ *
+ * Contents (reference file:line each follows):
+ *   sample hash and warps ........ core/rng.h:6-12, core/sampling.h:13-52
+ *   binned-SAH BVH2 build ........ accel/bvh_builder.cpp:5-68 (bin count as a parameter; the reference fixes 16)
+ *   BVH2 layout .................. accel/bvh_layouts.cpp:6-30
+ *   CWBVH SAH collapse ........... accel/bvh_tools.cpp:46-168
+ *   triangle / Woop packing ...... accel/tri_pack.cpp:6-38
+ *   traversal (BVH2, CWBVH) ...... accel/traverse.cuh:10-70, 112-152
+ *   camera ray + legacy shading .. render/wavefront.cu:42-58, 94-136, frame loop 684-741
+ *   FP64 watertight reference .... not in the reference (precision-form oracle; Woop, Benthin & Wald, JCGT 2013)
+ */
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct { float x, y, z; } V3;
+typedef struct { float x, y, z, w; } V4;
+
+static V3 v3(float x, float y, float z) { V3 r = { x, y, z }; return r; }
+static V3 add(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static V3 sub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static V3 neg(V3 a) { return v3(-a.x, -a.y, -a.z); }
+static V3 mulv(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static V3 muls(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+static float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static V3 cross3(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static V3 normz(V3 a) { float l = sqrtf(dot3(a, a)); return l > 0.f ? muls(a, 1.0f / l) : a; }
+static V3 xyz4(V4 a) { return v3(a.x, a.y, a.z); }
+static float fdot(V3 a, V3 b) { return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)); }
+static float frow(V4 r, V3 a) { return fmaf(a.z, r.z, fmaf(a.y, r.y, fmaf(a.x, r.x, r.w))); }
+static int fi(float f) { int i; memcpy(&i, &f, 4); return i; }
+static unsigned fu(float f) { unsigned u; memcpy(&u, &f, 4); return u; }
+static float iff(int i) { float f; memcpy(&f, &i, 4); return f; }
+static float uf(unsigned u) { float f; memcpy(&f, &u, 4); return f; }
+
+/* ------------------------------------------------------------------ sample hash + warps (core/rng.h, sampling.h) */
+static unsigned hash32(unsigned x) { x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16; return x; }
+float orc_rng(unsigned pix, unsigned smp, unsigned depth, unsigned dim, unsigned seed) {
+    unsigned h = hash32(pix * 0x9E3779B1U ^ hash32(smp * 0x85EBCA77U ^ hash32((depth * 8u + dim) * 0xC2B2AE3DU ^ seed)));
+    return (float)(h >> 8) * (1.0f / 16777216.0f);
+}
+static void onb(V3 n, V3* t, V3* b) {
+    float s = n.z >= 0.f ? 1.f : -1.f; float a = -1.f / (s + n.z); float c = n.x * n.y * a;
+    *t = v3(1.f + s * n.x * n.x * a, s * c, -s * n.x); *b = v3(c, s + n.y * n.y * a, -n.y);
+}
+static V3 cos_hemi(V3 n, float u0, float u1) {
+    float r = sqrtf(u0), ph = 6.2831853f * u1; V3 t, b; onb(n, &t, &b);
+    return normz(add(add(muls(t, r * cosf(ph)), muls(b, r * sinf(ph))), muls(n, sqrtf(fmaxf(0.f, 1.f - u0)))));
+}
+static V3 cone_dir(V3 axis, float cosMax, float u0, float u1) {
+    float cz = 1.f - u0 * (1.f - cosMax); float sz = sqrtf(fmaxf(0.f, 1.f - cz * cz)); float ph = 6.2831853f * u1;
+    V3 t, b; onb(axis, &t, &b);
+    return normz(add(add(muls(axis, cz), muls(t, sz * cosf(ph))), muls(b, sz * sinf(ph))));
+}
+static float table_lookup(const float* tab, int n, float u) {
+    float f = u * n; int k = (int)f; k = k < n - 1 ? k : n - 1; float t = f - k; return tab[k] * (1.f - t) + tab[k + 1] * t;
+}
+
+/* ------------------------------------------------------------------ binned-SAH BVH2 (bvh_builder.cpp:5-68) */
+typedef struct { V3 lo, hi; } Box;
+static Box box_empty(void) { Box b; b.lo = v3(FLT_MAX, FLT_MAX, FLT_MAX); b.hi = v3(-FLT_MAX, -FLT_MAX, -FLT_MAX); return b; }
+static void grow_p(Box* b, V3 p) { b->lo = v3(fminf(b->lo.x, p.x), fminf(b->lo.y, p.y), fminf(b->lo.z, p.z)); b->hi = v3(fmaxf(b->hi.x, p.x), fmaxf(b->hi.y, p.y), fmaxf(b->hi.z, p.z)); }
+static void grow_b(Box* b, const Box* c) {
+    b->lo = v3(fminf(b->lo.x, c->lo.x), fminf(b->lo.y, c->lo.y), fminf(b->lo.z, c->lo.z));
+    b->hi = v3(fmaxf(b->hi.x, c->hi.x), fmaxf(b->hi.y, c->hi.y), fmaxf(b->hi.z, c->hi.z));
+}
+static float box_area(const Box* b) { if (b->hi.x < b->lo.x) return 0.f; V3 d = sub(b->hi, b->lo); return 2.f * (d.x * d.y + d.y * d.z + d.z * d.x); }
+static float comp(V3 v, int a) { return a == 0 ? v.x : a == 1 ? v.y : v.z; }
+
+typedef struct { Box box; int left, right, first, count; } Node;
+typedef struct {
+    const float* v; const int* f; int nb, leafMax;
+    Box* tb; V3* cent; int* idx;
+    Node* nodes; int nNodes, cap; int maxDepth;
+} Build;
+
+static int push_node(Build* B) {
+    if (B->nNodes == B->cap) { B->cap = B->cap ? 2 * B->cap : 1024; B->nodes = (Node*)realloc(B->nodes, sizeof(Node) * B->cap); }
+    Node* n = &B->nodes[B->nNodes]; n->box = box_empty(); n->left = n->right = -1; n->first = n->count = 0;
+    return B->nNodes++;
+}
+static int bin_of(float c, float lo, float scale, int nb) { int b = (int)((c - lo) * scale); return b < 0 ? 0 : b > nb - 1 ? nb - 1 : b; }
+
+/* in-place two-sided partition: scan from the left for an element failing the predicate and from the right for one
+ * satisfying it, swap, repeat (the classic bidirectional partition, same permutation as the C++ library's) */
+static int partition(Build* B, int begin, int end, int axis, float lo, float scale, int bestBin) {
+    int first = begin, last = end;
+    for (;;) {
+        for (;;) { if (first == last) return first; if (bin_of(comp(B->cent[B->idx[first]], axis), lo, scale, B->nb) <= bestBin) first++; else break; }
+        last--;
+        for (;;) { if (first == last) return first; if (!(bin_of(comp(B->cent[B->idx[last]], axis), lo, scale, B->nb) <= bestBin)) last--; else break; }
+        { int t = B->idx[first]; B->idx[first] = B->idx[last]; B->idx[last] = t; }
+        first++;
+    }
+}
+
+static int rec(Build* B, int begin, int end, int depth) {
+    int id = push_node(B), n = end - begin, i, axis, b;
+    if (depth > B->maxDepth) B->maxDepth = depth;
+    Box box = box_empty(), cb = box_empty();
+    for (i = begin; i < end; i++) { grow_b(&box, &B->tb[B->idx[i]]); grow_p(&cb, B->cent[B->idx[i]]); }
+    B->nodes[id].box = box;
+    if (n <= B->leafMax || depth >= 62) { B->nodes[id].first = begin; B->nodes[id].count = n; return id; }
+    const int NB = B->nb;
+    float bestCost = FLT_MAX; int bestAxis = -1, bestBin = -1;
+    V3 ext = sub(cb.hi, cb.lo);
+    Box* bb = (Box*)malloc(sizeof(Box) * NB); int* bc = (int*)malloc(sizeof(int) * NB);
+    float* rA = (float*)malloc(sizeof(float) * NB); int* rC = (int*)malloc(sizeof(int) * NB);
+    for (axis = 0; axis < 3; axis++) {
+        float lo = comp(cb.lo, axis), e = comp(ext, axis);
+        if (e <= 1e-12f) continue;
+        float scale = NB / e;
+        for (b = 0; b < NB; b++) { bb[b] = box_empty(); bc[b] = 0; }
+        for (i = begin; i < end; i++) { int k = bin_of(comp(B->cent[B->idx[i]], axis), lo, scale, NB); grow_b(&bb[k], &B->tb[B->idx[i]]); bc[k]++; }
+        Box acc = box_empty(); int cnt = 0;
+        for (b = NB - 1; b > 0; b--) { grow_b(&acc, &bb[b]); cnt += bc[b]; rA[b] = box_area(&acc); rC[b] = cnt; }
+        Box lacc = box_empty(); int lcnt = 0;
+        for (b = 0; b < NB - 1; b++) {
+            grow_b(&lacc, &bb[b]); lcnt += bc[b];
+            if (lcnt == 0 || rC[b + 1] == 0) continue;
+            float cost = box_area(&lacc) * lcnt + rA[b + 1] * rC[b + 1];
+            if (cost < bestCost) { bestCost = cost; bestAxis = axis; bestBin = b; }
+        }
+    }
+    free(bb); free(bc); free(rA); free(rC);
+    int mid;
+    if (bestAxis < 0) mid = (begin + end) / 2;
+    else {
+        float lo = comp(cb.lo, bestAxis), e = comp(ext, bestAxis), scale = NB / e;
+        mid = partition(B, begin, end, bestAxis, lo, scale, bestBin);
+        if (mid == begin || mid == end) mid = (begin + end) / 2;
+    }
+    int l = rec(B, begin, mid, depth + 1), r = rec(B, mid, end, depth + 1);
+    B->nodes[id].left = l; B->nodes[id].right = r;
+    return id;
+}
+
+static V3 vert(const float* v, int i) { return v3(v[3 * i], v[3 * i + 1], v[3 * i + 2]); }
+
+static void sah_build(Build* B, const float* v, const int* f, int nt, int nb, int leafMax) {
+    memset(B, 0, sizeof *B);
+    B->v = v; B->f = f; B->nb = nb; B->leafMax = leafMax;
+    B->tb = (Box*)malloc(sizeof(Box) * (nt > 0 ? nt : 1)); B->cent = (V3*)malloc(sizeof(V3) * (nt > 0 ? nt : 1)); B->idx = (int*)malloc(sizeof(int) * (nt > 0 ? nt : 1));
+    for (int i = 0; i < nt; i++) {
+        Box b = box_empty(); grow_p(&b, vert(v, f[3 * i])); grow_p(&b, vert(v, f[3 * i + 1])); grow_p(&b, vert(v, f[3 * i + 2]));
+        B->tb[i] = b; B->cent[i] = muls(add(b.lo, b.hi), 0.5f); B->idx[i] = i;
+    }
+    rec(B, 0, nt, 0);
+}
+static void build_free(Build* B) { free(B->tb); free(B->cent); free(B->idx); free(B->nodes); }
+
+/* ------------------------------------------------------------------ BVH2 layout (bvh_layouts.cpp:6-30) */
+typedef struct { V4* a; int n, cap; } V4Vec;
+static void v4_resize(V4Vec* s, int n) { if (n > s->cap) { while (s->cap < n) s->cap = s->cap ? 2 * s->cap : 1024; s->a = (V4*)realloc(s->a, sizeof(V4) * s->cap); } s->n = n; }
+static V4 mk4(float x, float y, float z, float w) { V4 r = { x, y, z, w }; return r; }
+static const float kEmpty = 3e37f;
+
+static int emit2(const Build* B, int bn, V4Vec* out) {
+    const Node* nd = &B->nodes[bn];
+    int id = out->n / 4; v4_resize(out, out->n + 4);
+    int ch[2] = { nd->left, nd->right }, c[2], k[2]; Box bx[2];
+    for (int j = 0; j < 2; j++) {
+        if (ch[j] < 0) { c[j] = -1; k[j] = 0; bx[j].lo = bx[j].hi = v3(kEmpty, kEmpty, kEmpty); continue; }
+        const Node* cn = &B->nodes[ch[j]]; bx[j] = cn->box;
+        if (cn->count > 0) { c[j] = cn->first; k[j] = cn->count; } else { k[j] = 0; c[j] = emit2(B, ch[j], out); }
+    }
+    V4* n = &out->a[id * 4];
+    n[0] = mk4(bx[0].lo.x, bx[0].hi.x, bx[0].lo.y, bx[0].hi.y);
+    n[1] = mk4(bx[1].lo.x, bx[1].hi.x, bx[1].lo.y, bx[1].hi.y);
+    n[2] = mk4(bx[0].lo.z, bx[0].hi.z, bx[1].lo.z, bx[1].hi.z);
+    n[3] = mk4(iff(c[0]), iff(c[1]), iff(k[0]), iff(k[1]));
+    return id;
+}
+static void wrap_root(Build* B) { int r = push_node(B); B->nodes[r].box = B->nodes[0].box; B->nodes[r].left = 0; B->nodes[r].right = -1; }
+
+/* ------------------------------------------------------------------ CWBVH collapse (bvh_tools.cpp:46-168) */
+enum { LEAF = 0, NODEC = 1, PREV = 2, DIST = 10 };
+typedef struct { Box* box; int *L, *R, *first, *cnt, *p; float* C; unsigned char *D, *K8; int n, cap; const int* prim; } CW;
+static void cw_push(CW* w) {
+    if (w->n == w->cap) {
+        w->cap = w->cap ? 2 * w->cap : 1024;
+        w->box = (Box*)realloc(w->box, sizeof(Box) * w->cap); w->L = (int*)realloc(w->L, 4 * w->cap); w->R = (int*)realloc(w->R, 4 * w->cap);
+        w->first = (int*)realloc(w->first, 4 * w->cap); w->cnt = (int*)realloc(w->cnt, 4 * w->cap);
+    }
+    w->n++;
+}
+static int cw_isleaf(const CW* w, int n) { return w->L[n] < 0 || w->D[(size_t)n * 8 + 1] == LEAF; }
+typedef struct { int* a; int n, cap; } IVec;
+static void ipush(IVec* s, int x) { if (s->n == s->cap) { s->cap = s->cap ? 2 * s->cap : 64; s->a = (int*)realloc(s->a, 4 * s->cap); } s->a[s->n++] = x; }
+static void cw_roots(const CW* w, int n, int i, IVec* out) {
+    for (;;) {
+        if (i == 1) { ipush(out, n); return; }
+        unsigned char d = w->D[(size_t)n * 8 + i];
+        if (d == PREV) { i--; continue; }
+        int k = d - DIST; cw_roots(w, w->L[n], k, out); cw_roots(w, w->R[n], i - k, out); return;
+    }
+}
+static void cw_prims(const CW* w, int n, IVec* out) {
+    IVec st = { 0 }; ipush(&st, n);
+    while (st.n) { int h = st.a[--st.n]; if (w->L[h] < 0) { for (int t = 0; t < w->cnt[h]; t++) ipush(out, w->prim[w->first[h] + t]); } else { ipush(&st, w->R[h]); ipush(&st, w->L[h]); } }
+    free(st.a);
+}
+static int expo8(float ext, float lo, float hi) {
+    if (!(ext > 0.f)) return -100;
+    int e = (int)ceilf(log2f(ext / 255.f)); if (e < -100) e = -100;
+    while (lo + 255.f * ldexpf(1.f, e) < hi) e++;
+    return e;
+}
+static int qz(float v, float o, float sc, int up) { float f = (v - o) / sc; int i = up ? (int)ceilf(f) : (int)floorf(f); return i < 0 ? 0 : i > 255 ? 255 : i; }
+static unsigned pack4(const int* q, int b) { return (unsigned)q[b] | ((unsigned)q[b + 1] << 8) | ((unsigned)q[b + 2] << 16) | ((unsigned)q[b + 3] << 24); }
+
+static double cw_build(const Build* B, V4Vec* nodes, IVec* order) {
+    const int pMax = 3; const float cNode = 1.f, cPrim = 0.3f, INF = 3e38f;
+    CW w; memset(&w, 0, sizeof w); w.prim = B->idx;
+    for (int i = 0; i < B->nNodes; i++) {
+        cw_push(&w); const Node* b = &B->nodes[i]; int lf = b->count > 0;
+        w.box[i] = b->box; w.L[i] = lf ? -1 : b->left; w.R[i] = lf ? -1 : b->right; w.first[i] = b->first; w.cnt[i] = lf ? b->count : 0;
+    }
+    for (int i = 0; i < w.n; i++) {
+        if (w.L[i] >= 0 || w.cnt[i] <= pMax) continue;
+        int h = w.cnt[i] / 2, a = w.n; Box bx = w.box[i];
+        cw_push(&w); cw_push(&w);
+        w.box[a] = bx; w.box[a + 1] = bx; w.L[a] = w.L[a + 1] = w.R[a] = w.R[a + 1] = -1;
+        w.first[a] = w.first[i]; w.cnt[a] = h; w.first[a + 1] = w.first[i] + h; w.cnt[a + 1] = w.cnt[i] - h;
+        w.L[i] = a; w.R[i] = a + 1; w.cnt[i] = 0;
+    }
+    const int N = w.n;
+    w.C = (float*)calloc((size_t)N * 8, 4); w.D = (unsigned char*)calloc((size_t)N * 8, 1); w.K8 = (unsigned char*)malloc(N); w.p = (int*)calloc(N, 4);
+    memset(w.K8, 1, N);
+    for (int n = N - 1; n >= 0; n--) {
+        float A = box_area(&w.box[n]); float* c = &w.C[(size_t)n * 8]; unsigned char* d = &w.D[(size_t)n * 8];
+        if (w.L[n] < 0) { w.p[n] = w.cnt[n]; float cl = A * w.p[n] * cPrim; for (int i = 1; i < 8; i++) { c[i] = cl; d[i] = i == 1 ? LEAF : PREV; } continue; }
+        int l = w.L[n], r = w.R[n]; w.p[n] = w.p[l] + w.p[r];
+        const float* cl = &w.C[(size_t)l * 8]; const float* cr = &w.C[(size_t)r * 8];
+        float dist[9]; int dk[9];
+        for (int j = 2; j <= 8; j++) { dist[j] = INF; dk[j] = 1; for (int k = 1; k < j; k++) { float x = cl[k] + cr[j - k]; if (x < dist[j]) { dist[j] = x; dk[j] = k; } } }
+        float cLeaf = w.p[n] <= pMax ? A * w.p[n] * cPrim : INF, cInt = dist[8] + A * cNode;
+        if (cLeaf <= cInt) { c[1] = cLeaf; d[1] = LEAF; } else { c[1] = cInt; d[1] = NODEC; }
+        w.K8[n] = (unsigned char)dk[8];
+        for (int i = 2; i < 8; i++) { if (dist[i] < c[i - 1]) { c[i] = dist[i]; d[i] = (unsigned char)(DIST + dk[i]); } else { c[i] = c[i - 1]; d[i] = PREV; } }
+    }
+    const float Ar = box_area(&w.box[0]); const int rootLeaf = cw_isleaf(&w, 0); double sah;
+    if (rootLeaf) sah = Ar > 0 ? (Ar * w.p[0] * cPrim + Ar * cNode) / Ar : 0;
+    else { float d8 = INF; for (int k = 1; k < 8; k++) { float x = w.C[(size_t)w.L[0] * 8 + k] + w.C[(size_t)w.R[0] * 8 + 8 - k]; d8 = x < d8 ? x : d8; } sah = Ar > 0 ? (d8 + Ar * cNode) / Ar : 0; }
+    /* emission: LIFO job stack, children of a node contiguous */
+    typedef struct { int bn, out, asLeaf; } Job;
+    Job* jobs = (Job*)malloc(sizeof(Job) * (N + 8)); int nj = 0;
+    nodes->n = 0; v4_resize(nodes, 5); order->n = 0;
+    jobs[nj].bn = 0; jobs[nj].out = 0; jobs[nj].asLeaf = rootLeaf; nj++;
+    IVec ch = { 0 }, pr = { 0 };
+    while (nj) {
+        Job jb = jobs[--nj]; int n = jb.bn;
+        ch.n = 0;
+        if (jb.asLeaf) ipush(&ch, n); else { cw_roots(&w, w.L[n], w.K8[n], &ch); cw_roots(&w, w.R[n], 8 - w.K8[n], &ch); }
+        Box box = w.box[n]; V3 pc = muls(add(box.lo, box.hi), 0.5f);
+        int slot[8], used[8] = { 0 }; float cost[8][8];
+        for (int s = 0; s < 8; s++) slot[s] = -1;
+        for (int c = 0; c < ch.n; c++) {
+            V3 cc = sub(muls(add(w.box[ch.a[c]].lo, w.box[ch.a[c]].hi), 0.5f), pc);
+            for (int s = 0; s < 8; s++) cost[c][s] = -(cc.x * (s & 1 ? -1.f : 1.f) + cc.y * (s & 2 ? -1.f : 1.f) + cc.z * (s & 4 ? -1.f : 1.f));
+        }
+        for (int it = 0; it < ch.n; it++) {
+            float bc = INF; int bi = -1, bs = -1;
+            for (int c = 0; c < ch.n; c++) if (!used[c]) for (int s = 0; s < 8; s++) if (slot[s] < 0 && cost[c][s] < bc) { bc = cost[c][s]; bi = c; bs = s; }
+            if (bi < 0) for (int c = 0; c < ch.n && bi < 0; c++) if (!used[c]) for (int s = 0; s < 8; s++) if (slot[s] < 0) { bi = c; bs = s; break; }
+            used[bi] = 1; slot[bs] = ch.a[bi];
+        }
+        V3 ext = sub(box.hi, box.lo);
+        int ex = expo8(ext.x, box.lo.x, box.hi.x), ey = expo8(ext.y, box.lo.y, box.hi.y), ez = expo8(ext.z, box.lo.z, box.hi.z);
+        float sx = ldexpf(1.f, ex), sy = ldexpf(1.f, ey), sz = ldexpf(1.f, ez);
+        int q[6][8], meta[8], isLeafC[8]; int triBase = order->n, nInt = 0; unsigned imask = 0;
+        for (int s = 0; s < 8; s++) {
+            for (int a = 0; a < 6; a++) q[a][s] = 0;
+            meta[s] = 0; isLeafC[s] = 0;
+            int cn = slot[s]; if (cn < 0) continue;
+            Box cb = w.box[cn];
+            q[0][s] = qz(cb.lo.x, box.lo.x, sx, 0); q[3][s] = qz(cb.hi.x, box.lo.x, sx, 1);
+            q[1][s] = qz(cb.lo.y, box.lo.y, sy, 0); q[4][s] = qz(cb.hi.y, box.lo.y, sy, 1);
+            q[2][s] = qz(cb.lo.z, box.lo.z, sz, 0); q[5][s] = qz(cb.hi.z, box.lo.z, sz, 1);
+            if (jb.asLeaf || cw_isleaf(&w, cn)) {
+                pr.n = 0; cw_prims(&w, cn, &pr);
+                int off = order->n - triBase;
+                for (int t = 0; t < pr.n; t++) ipush(order, pr.a[t]);
+                meta[s] = 0x80 | ((pr.n - 1) << 5) | off; isLeafC[s] = 1;
+            } else { meta[s] = 0x40; imask |= 1u << s; nInt++; }
+        }
+        int childBase = nodes->n / 5;
+        v4_resize(nodes, nodes->n + 5 * nInt);
+        V4* o = &nodes->a[jb.out * 5];
+        unsigned ew = (unsigned)(ex + 127) | ((unsigned)(ey + 127) << 8) | ((unsigned)(ez + 127) << 16) | (imask << 24);
+        o[0] = mk4(box.lo.x, box.lo.y, box.lo.z, uf(ew));
+        o[1] = mk4(iff(childBase), iff(triBase), uf(pack4(meta, 0)), uf(pack4(meta, 4)));
+        unsigned u[12]; for (int a = 0; a < 6; a++) { u[2 * a] = pack4(q[a], 0); u[2 * a + 1] = pack4(q[a], 4); }
+        for (int j = 0; j < 3; j++) o[2 + j] = mk4(uf(u[4 * j]), uf(u[4 * j + 1]), uf(u[4 * j + 2]), uf(u[4 * j + 3]));
+        int ord = 0;
+        for (int s = 0; s < 8; s++) if (slot[s] >= 0 && !isLeafC[s]) { jobs[nj].bn = slot[s]; jobs[nj].out = childBase + ord; jobs[nj].asLeaf = 0; nj++; ord++; }
+    }
+    free(jobs); free(ch.a); free(pr.a);
+    free(w.box); free(w.L); free(w.R); free(w.first); free(w.cnt); free(w.p); free(w.C); free(w.D); free(w.K8);
+    return sah;
+}
+
+/* ------------------------------------------------------------------ public build entry point
+ * variant 2: BVH2 from leaves <= leafMax; variant 8: CWBVH by the SAH collapse from single-triangle leaves.
+ * nodes_out capacity: variant 2 -> 4 (nt + 1) float4, variant 8 -> 5 (2 nt) float4. order_out: nt ints.
+ * Returns the node count in float4 units (or -1), fills *max_depth. */
+long orc_build(const float* v, const int* f, int nt, int bins, int leafMax, int variant, float* nodes_out, long cap_f4, int* order_out, int* max_depth, double* sah) {
+    Build B; V4Vec nodes = { 0 }; IVec order = { 0 }; long n = -1;
+    if (nt <= 0 || bins < 2) return -1;
+    sah_build(&B, v, f, nt, bins, variant == 8 ? 1 : leafMax);
+    *max_depth = B.maxDepth;
+    if (variant == 2) {
+        if (B.nodes[0].count > 0) { wrap_root(&B); emit2(&B, B.nNodes - 1, &nodes); } else emit2(&B, 0, &nodes);
+        for (int i = 0; i < nt; i++) order_out[i] = B.idx[i];
+        *sah = 0;
+    } else {
+        *sah = cw_build(&B, &nodes, &order);
+        for (int i = 0; i < order.n && i < nt; i++) order_out[i] = order.a[i];
+    }
+    if (nodes.n <= cap_f4) { memcpy(nodes_out, nodes.a, sizeof(V4) * nodes.n); n = nodes.n; }
+    free(nodes.a); free(order.a); build_free(&B);
+    return n;
+}
+
+/* triangles in leaf order (tri_pack.cpp:6-16) and Woop rows (tri_pack.cpp:18-38) */
+void orc_pack(const float* v, const int* f, const int* fm, const int* order, int n, float* tris, float* woop) {
+    for (int k = 0; k < n; k++) {
+        int t = order[k]; V3 v0 = vert(v, f[3 * t]), e1 = sub(vert(v, f[3 * t + 1]), v0), e2 = sub(vert(v, f[3 * t + 2]), v0), nn = cross3(e1, e2);
+        int mat = fm ? fm[t] : 0;
+        float* o = tris + 12 * (size_t)k;
+        o[0] = v0.x; o[1] = v0.y; o[2] = v0.z; o[3] = iff(t); o[4] = e1.x; o[5] = e1.y; o[6] = e1.z; o[7] = iff(mat); o[8] = e2.x; o[9] = e2.y; o[10] = e2.z; o[11] = 0.f;
+        double a[3][3] = { { e1.x, e2.x, nn.x }, { e1.y, e2.y, nn.y }, { e1.z, e2.z, nn.z } };
+        double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) + a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+        double m[3][3] = { { 0 } };
+        if (!(fabs(det) < 1e-300)) {
+            double id = 1.0 / det;
+            m[0][0] = (a[1][1] * a[2][2] - a[1][2] * a[2][1]) * id; m[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) * id; m[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) * id;
+            m[1][0] = (a[1][2] * a[2][0] - a[1][0] * a[2][2]) * id; m[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) * id; m[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) * id;
+            m[2][0] = (a[1][0] * a[2][1] - a[1][1] * a[2][0]) * id; m[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) * id; m[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) * id;
+        }
+        float* w = woop + 12 * (size_t)k;
+        for (int r = 0; r < 3; r++) {
+            double tt = -(m[r][0] * v0.x + m[r][1] * v0.y + m[r][2] * v0.z);
+            w[4 * r] = (float)m[r][0]; w[4 * r + 1] = (float)m[r][1]; w[4 * r + 2] = (float)m[r][2]; w[4 * r + 3] = (float)tt;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ traversal (traverse.cuh) */
+static int leaf_hit(const V4* tv, int first, int cnt, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv) {
+    for (int t = first; t < first + cnt; t++) {
+        if (tri == 0) {
+            V3 v0 = xyz4(tv[3 * t]), e1 = xyz4(tv[3 * t + 1]), e2 = xyz4(tv[3 * t + 2]);
+            V3 pv = v3(fmaf(d.y, e2.z, -d.z * e2.y), fmaf(d.z, e2.x, -d.x * e2.z), fmaf(d.x, e2.y, -d.y * e2.x));
+            float det = fdot(e1, pv);
+            if (fabsf(det) < 1e-12f) continue;
+            float inv = 1.f / det; V3 tq = sub(o, v0); float u = fdot(tq, pv) * inv;
+            if (u < 0.f || u > 1.f) continue;
+            V3 qv = v3(fmaf(tq.y, e1.z, -tq.z * e1.y), fmaf(tq.z, e1.x, -tq.x * e1.z), fmaf(tq.x, e1.y, -tq.y * e1.x));
+            float vv = fdot(d, qv) * inv;
+            if (vv < 0.f || u + vv > 1.f) continue;
+            float tt = fdot(e2, qv) * inv;
+            if (tt > tmin && tt < *hitT) { *hitT = tt; *hitTri = t; *hu = u; *hv = vv; if (any) return 1; }
+        } else {
+            V4 r2 = tv[3 * t + 2];
+            float Oz = frow(r2, o), Dz = fdot(d, xyz4(r2)), tt = -Oz / Dz;
+            if (tt > tmin && tt < *hitT) {
+                V4 r0 = tv[3 * t];
+                float u = fmaf(tt, fdot(d, xyz4(r0)), frow(r0, o));
+                if (u >= 0.f && u <= 1.f) {
+                    V4 r1 = tv[3 * t + 1];
+                    float vv = fmaf(tt, fdot(d, xyz4(r1)), frow(r1, o));
+                    if (vv >= 0.f && u + vv <= 1.f) { *hitT = tt; *hitTri = t; *hu = u; *hv = vv; if (any) return 1; }
+                }
+            }
+        }
+    }
+    return 0;
+}
+static float safe_rcp(float x) { return 1.f / (fabsf(x) > 1e-20f ? x : copysignf(1e-20f, x)); }
+
+/* visit counters (for the algorithmic-bytes figures) */
+typedef struct { long long nodes, tris; } Stats;
+static int leaf_hit_s(const V4* tv, int first, int cnt, V3 o, V3 d, float tmin, int any, int tri, float* T, int* I, float* U, float* W, Stats* st) {
+    if (st) { /* count tests the same way the loop runs them */
+        int before = *I; float bt = *T; (void)before; (void)bt;
+        int r = 0;
+        for (int t = first; t < first + cnt; t++) { st->tris++; if (leaf_hit(tv, t, 1, o, d, tmin, any, tri, T, I, U, W)) { r = 1; if (any) break; } }
+        return r;
+    }
+    return leaf_hit(tv, first, cnt, o, d, tmin, any, tri, T, I, U, W);
+}
+
+static int trav2(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv, Stats* st) {
+    int stack[64], sp = 0, node = 0;
+    const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z), ox = -o.x * idx, oy = -o.y * idy, oz = -o.z * idz;
+    for (;;) {
+        if (st) st->nodes++;
+        const V4 n0 = nodes[4 * node], n1 = nodes[4 * node + 1], nz = nodes[4 * node + 2], mt = nodes[4 * node + 3];
+        int c0 = fi(mt.x), c1 = fi(mt.y), k0 = fi(mt.z), k1 = fi(mt.w);
+        float a0 = fmaf(n0.x, idx, ox), a1 = fmaf(n0.y, idx, ox), a2 = fmaf(n0.z, idy, oy), a3 = fmaf(n0.w, idy, oy), a4 = fmaf(nz.x, idz, oz), a5 = fmaf(nz.y, idz, oz);
+        float b0 = fmaf(n1.x, idx, ox), b1 = fmaf(n1.y, idx, ox), b2 = fmaf(n1.z, idy, oy), b3 = fmaf(n1.w, idy, oy), b4 = fmaf(nz.z, idz, oz), b5 = fmaf(nz.w, idz, oz);
+        float t0n = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
+        float t0f = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), *hitT));
+        float t1n = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
+        float t1f = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), *hitT));
+        int h0 = t0n <= t0f, h1 = t1n <= t1f;
+        if (h0 && k0 > 0) { if (leaf_hit_s(tv, c0, k0, o, d, tmin, any, tri, hitT, hitTri, hu, hv, st) && any) return 1; h0 = 0; }
+        if (h1 && k1 > 0) { if (leaf_hit_s(tv, c1, k1, o, d, tmin, any, tri, hitT, hitTri, hu, hv, st) && any) return 1; h1 = 0; }
+        if (!h0 && !h1) { if (sp == 0) break; node = stack[--sp]; }
+        else if (h0 && h1) { if (t1n < t0n) { int t = c0; c0 = c1; c1 = t; } if (sp == 64) return -1; stack[sp++] = c1; node = c0; }
+        else node = h0 ? c0 : c1;
+    }
+    return *hitTri >= 0;
+}
+
+static unsigned byte_of(unsigned w, int s) { return (w >> (8 * (s & 3))) & 255u; }
+static int trav8(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv, Stats* st) {
+    unsigned stk[40][2]; int sp = 0, node = 0;
+    const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z);
+    const unsigned oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
+    unsigned cb = 0, im = 0, hm = 0;
+    for (;;) {
+        if (st) st->nodes++;
+        const V4* nb = nodes + 5 * node;
+        V4 f0 = nb[0], f1 = nb[1], f2 = nb[2], f3 = nb[3], f4 = nb[4];
+        unsigned ew = fu(f0.w);
+        float sx = uf((ew & 255u) << 23) * idx, sy = uf(((ew >> 8) & 255u) << 23) * idy, sz = uf(((ew >> 16) & 255u) << 23) * idz;
+        float ox = (f0.x - o.x) * idx, oy = (f0.y - o.y) * idy, oz = (f0.z - o.z) * idz;
+        unsigned imask = ew >> 24, m0 = fu(f1.z), m1 = fu(f1.w); int childBase = fi(f1.x), triBase = fi(f1.y);
+        unsigned q[12] = { fu(f2.x), fu(f2.y), fu(f2.z), fu(f2.w), fu(f3.x), fu(f3.y), fu(f3.z), fu(f3.w), fu(f4.x), fu(f4.y), fu(f4.z), fu(f4.w) };
+        unsigned hits = 0;
+        for (int s = 0; s < 8; s++) {
+            unsigned m = byte_of(s < 4 ? m0 : m1, s); int hi = s < 4 ? 0 : 1;
+            if (m == 0) continue;
+            float x0 = fmaf((float)byte_of(q[0 + hi], s), sx, ox), x1 = fmaf((float)byte_of(q[6 + hi], s), sx, ox);
+            float y0 = fmaf((float)byte_of(q[2 + hi], s), sy, oy), y1 = fmaf((float)byte_of(q[8 + hi], s), sy, oy);
+            float z0 = fmaf((float)byte_of(q[4 + hi], s), sz, oz), z1 = fmaf((float)byte_of(q[10 + hi], s), sz, oz);
+            float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+            float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), *hitT));
+            if (tn <= tf) {
+                if (m & 0x80u) { if (leaf_hit_s(tv, triBase + (int)(m & 31u), (int)((m >> 5) & 3u) + 1, o, d, tmin, any, tri, hitT, hitTri, hu, hv, st) && any) return 1; }
+                else hits |= 1u << (s ^ oct);
+            }
+        }
+        if (hits) { if (hm) { if (sp == 40) return -1; stk[sp][0] = cb; stk[sp][1] = (im << 8) | hm; sp++; } cb = (unsigned)childBase; im = imask; hm = hits; }
+        while (hm == 0) { if (sp == 0) return *hitTri >= 0; sp--; cb = stk[sp][0]; im = stk[sp][1] >> 8; hm = stk[sp][1] & 255u; }
+        unsigned k = (unsigned)__builtin_ctz(hm); hm &= hm - 1; unsigned slot = k ^ oct;
+        node = (int)cb + __builtin_popcount(im & ((1u << slot) - 1u));
+    }
+}
+
+/* ray batch: o/d float4 (tmin / tmax in w). Closest: hits float4 (t, u, v, tri bits). Any: occ = first occluder or -1.
+ * stats (may be NULL): [0] node visits, [1] triangle tests summed over the batch. Returns the number of rays that hit
+ * a stack bound. */
+long orc_trace(int variant, int tri, int any, const float* nodes, const float* tv, const float* ro, const float* rd, long n, float* hits, int* occ, long long* stats) {
+    long bad = 0; Stats st = { 0, 0 };
+    for (long i = 0; i < n; i++) {
+        V3 o = v3(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]), d = v3(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]);
+        float tmin = ro[4 * i + 3], t = rd[4 * i + 3], u = 0.f, vv = 0.f; int h = -1, r;
+        if (variant == 2) r = trav2((const V4*)nodes, (const V4*)tv, o, d, tmin, any, tri, &t, &h, &u, &vv, stats ? &st : NULL);
+        else r = trav8((const V4*)nodes, (const V4*)tv, o, d, tmin, any, tri, &t, &h, &u, &vv, stats ? &st : NULL);
+        if (r < 0) bad++;
+        if (any) occ[i] = h;
+        else { hits[4 * i] = t; hits[4 * i + 1] = u; hits[4 * i + 2] = vv; hits[4 * i + 3] = iff(h); }
+    }
+    if (stats) { stats[0] = st.nodes; stats[1] = st.tris; }
+    return bad;
+}
+
+/* ------------------------------------------------------------------ legacy diffuse frame (wavefront.cu:42-136) */
+typedef struct {
+    float pos[3], ax[3], ay[3], az[3]; float fx, fy, px, py; int w, h; float lens_r, focus_d;
+    float sun_to[3], sun_e[3], sky[3]; float sun_cos; int max_b; unsigned seed; float eps, near_clip; int has_n, filter_bh; float ftab[65];
+} OrcParams;   /* same layout as cwp_params of the library's C ABI */
+
+static V3 a3(const float* a) { return v3(a[0], a[1], a[2]); }
+
+/* Renders samples [s_base, s_base + spp) of pixels [pix0, pix1) with `bounces` as the frame's depth limit
+ * (depths 0 .. bounces + 1 are traced) and adds radiance sums to accum (float4 per pixel). Each path is traced
+ * to completion before the next; the per-vertex decisions and sample dimensions are those of the wavefront loop.
+ * ray_counts (may be NULL): [0] closest rays, [1] shadow rays. */
+void orc_render(const OrcParams* P, int variant, int tri, const float* nodes, const float* tv, const float* tris, const float* albedo,
+                int bounces, int spp, int s_base, int pix0, int pix1, float* accum, long long* ray_counts) {
+    const int N = P->w * P->h, depths = bounces + 2;
+    long long nc = 0, ns = 0;
+    for (int pix = pix0; pix < pix1; pix++) {
+        const int x = pix % P->w, y = pix / P->w;
+        for (int smp = s_base; smp < s_base + spp; smp++) {
+            float u0 = orc_rng(pix, smp, 0, 0, P->seed), u1 = orc_rng(pix, smp, 0, 1, P->seed), jx, jy;
+            if (P->filter_bh) { jx = table_lookup(P->ftab, 64, u0); jy = table_lookup(P->ftab, 64, u1); } else { jx = u0 - 0.5f; jy = u1 - 0.5f; }
+            float dx = (x + 0.5f + jx - P->px) / P->fx, dy = -(y + 0.5f + jy - P->py) / P->fy;
+            V3 d = normz(sub(add(muls(a3(P->ax), dx), muls(a3(P->ay), dy)), a3(P->az))), o = a3(P->pos), T = v3(1.f, 1.f, 1.f);
+            float tmin = P->near_clip;
+            for (int depth = 0; depth < depths; depth++) {
+                nc++;
+                float t = 1e30f, u = 0.f, vv = 0.f; int h = -1;
+                if (variant == 2) trav2((const V4*)nodes, (const V4*)tv, o, d, tmin, 0, tri, &t, &h, &u, &vv, NULL);
+                else trav8((const V4*)nodes, (const V4*)tv, o, d, tmin, 0, tri, &t, &h, &u, &vv, NULL);
+                if (h < 0) { V3 c = mulv(T, a3(P->sky)); accum[4 * pix] += c.x; accum[4 * pix + 1] += c.y; accum[4 * pix + 2] += c.z; break; }
+                if (depth > P->max_b) break;
+                V3 p = add(o, muls(d, t));
+                const float* tb = tris + 12 * (size_t)h;
+                V3 e1 = v3(tb[4], tb[5], tb[6]), e2 = v3(tb[8], tb[9], tb[10]);
+                V3 ng = normz(cross3(e1, e2)), nsh = ng;
+                if (dot3(ng, d) > 0.f) { ng = neg(ng); nsh = neg(nsh); }
+                int mat = fi(tb[7]); V3 alb = a3(albedo + 3 * mat);
+                V3 po = add(p, muls(ng, P->eps));
+                const unsigned dr = (unsigned)depth + 1u;
+                V3 l = cone_dir(a3(P->sun_to), P->sun_cos, orc_rng(pix, smp, dr, 2, P->seed), orc_rng(pix, smp, dr, 3, P->seed));
+                float cl = dot3(nsh, l);
+                if (cl > 0.f && dot3(ng, l) > 0.f) {
+                    V3 contrib = muls(mulv(mulv(T, alb), a3(P->sun_e)), cl * 0.31830989f);
+                    ns++;
+                    float st = 1e30f, su, sv; int sh = -1, occ;
+                    if (variant == 2) occ = trav2((const V4*)nodes, (const V4*)tv, po, l, 0.f, 1, tri, &st, &sh, &su, &sv, NULL);
+                    else occ = trav8((const V4*)nodes, (const V4*)tv, po, l, 0.f, 1, tri, &st, &sh, &su, &sv, NULL);
+                    if (occ == 0) { accum[4 * pix] += contrib.x; accum[4 * pix + 1] += contrib.y; accum[4 * pix + 2] += contrib.z; }
+                }
+                V3 nd = cos_hemi(nsh, orc_rng(pix, smp, dr, 0, P->seed), orc_rng(pix, smp, dr, 1, P->seed));
+                if (dot3(nd, ng) <= 0.f) break;
+                T = mulv(T, alb); o = po; d = nd; tmin = 0.f;
+            }
+        }
+    }
+    (void)N;
+    if (ray_counts) { ray_counts[0] += nc; ray_counts[1] += ns; }
+}

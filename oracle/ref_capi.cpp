@@ -1,0 +1,162 @@
+// ref_capi.cpp - TEST INFRASTRUCTURE ONLY: a C wrapper around the reference's own host code, compiled from the
+// reference's sources by oracle/Makefile into oracle/_ref/libcwpref.so. Used to pin the oracle and the library
+// against the reference (byte-identical BVH buffers, same traversal results) and as the timed CPU baseline.
+//   builder / layouts ... accel/bvh_builder.cpp, accel/bvh_layouts.cpp, accel/bvh_tools.cpp, accel/tri_pack.cpp
+//   traversal ........... accel/traverse.cuh trav<V, ANY, TRI> compiled as host C++ through ref_shim.h
+// The harness (threads, argument marshalling) is ours; the arithmetic is the reference's.
+#include "ref_shim.h"
+#include "accel/bvh_builder.h"
+#include "accel/bvh_layouts.h"
+#include "accel/bvh_tools.h"
+#include "accel/tri_pack.h"
+#include "accel/traverse.cuh"
+#include "core/rng.h"
+#include "core/sampling.h"
+#include <algorithm>
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+static Mesh to_mesh(const float* v, long nv, const int* f, const int* fm, long nt) {
+    Mesh m;
+    for (long i = 0; i < nv; i++) m.v.push_back(make_float3(v[3 * i], v[3 * i + 1], v[3 * i + 2]));
+    for (long i = 0; i < nt; i++) { m.f.push_back(make_int3(f[3 * i], f[3 * i + 1], f[3 * i + 2])); m.fm.push_back(fm ? fm[i] : 0); }
+    m.kd.push_back(make_float3(0.8f, 0.8f, 0.8f));
+    return m;
+}
+
+// Builds like setupScene's layout step (app/scene_setup.cpp:190-222): variant 2 / 4 / 8, collapse 0 = SAH (CWBVH,
+// built from leaf-1 trees), 1 = greedy BVH8. Writes nodes (float4s, up to cap_f4), leaf order, packed triangles and
+// Woop rows (3 float4 per triangle each). Returns the node count in float4 units, or -1 if cap_f4 is too small.
+extern "C" long ref_build(const float* v, long nv, const int* f, const int* fm, long nt, int variant, int leaf, int collapse,
+                          float* nodes_out, long cap_f4, int* order_out, float* tris_out, float* woop_out, int* max_depth, double* sah, double* build_ms) {
+    Mesh m = to_mesh(v, nv, f, fm, nt);
+    auto t0 = std::chrono::steady_clock::now();
+    const bool cw = variant == 8 && collapse == 0;
+    BVHBuilder B; B.leafMax = cw ? 1 : (variant == 8 && leaf > 4) ? 4 : leaf; B.build(m);
+    std::vector<float4> nodes; std::vector<int> order;
+    if (variant == 2) { *sah = sahCost(B, 1, 1); BVH2Flat F; F.build(B); nodes.swap(F.nodes); order = B.idx; }
+    else if (variant == 4) { *sah = sahCost(B, 1, 1); BVH4Flat F; F.build(B); nodes.swap(F.nodes); order = B.idx; }
+    else if (cw) { CWBVH C; C.build(B); nodes.swap(C.nodes); order.swap(C.order); *sah = C.sah; }
+    else { *sah = sahCost(B, 1, 1); BVH8Flat F; F.build(B); nodes.swap(F.nodes); order.swap(F.order); }
+    *build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    *max_depth = B.maxDepth;
+    if ((long)nodes.size() > cap_f4) return -1;
+    memcpy(nodes_out, nodes.data(), nodes.size() * 16);
+    memcpy(order_out, order.data(), order.size() * 4);
+    std::vector<float4> tris, nrm, woop;
+    packTriangles(m, order, tris, nrm); packWoop(m, order, woop);
+    memcpy(tris_out, tris.data(), tris.size() * 16); memcpy(woop_out, woop.data(), woop.size() * 16);
+    return (long)nodes.size();
+}
+
+// The reference's binned-SAH build alone (single thread, as the reference runs it), for the CPU-baseline timing.
+extern "C" double ref_build_ms(const float* v, long nv, const int* f, long nt, int leaf) {
+    Mesh m = to_mesh(v, nv, f, nullptr, nt);
+    auto t0 = std::chrono::steady_clock::now();
+    BVHBuilder B; B.leafMax = leaf; B.build(m);
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+template <int V, bool ANY, int TRI>
+static void run(const float4* nodes, const float4* tv, const float4* ro, const float4* rd, float4* hits, int* occ, long b, long e) {
+    for (long i = b; i < e; i++) {
+        float4 O = ro[i], D = rd[i]; float t = D.w, u = 0.f, vv = 0.f; int tri = -1;
+        trav<V, ANY, TRI>(nodes, tv, xyz(O), xyz(D), O.w, t, tri, u, vv);
+        if (ANY) occ[i] = tri; else hits[i] = make_float4(t, u, vv, __int_as_float(tri));
+    }
+}
+
+// The reference's traversal over a ray batch on `threads` host threads (0 = all): closest hits as float4 (t, u, v,
+// tri bits) like traceOne (render/wavefront.cu:62-66), any-hit as the first occluder index or -1. Returns seconds.
+extern "C" double ref_trace(int variant, int any, int tri, const float* nodes, const float* tv, const float* ro, const float* rd, long n, float* hits, int* occ, int threads) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    auto fn = [&](long b, long e) {
+        const float4 *N = (const float4*)nodes, *T = (const float4*)tv, *O = (const float4*)ro, *D = (const float4*)rd; float4* H = (float4*)hits;
+#define REF_RUN(VV) do { if (any) { if (tri) run<VV, true, 1>(N, T, O, D, H, occ, b, e); else run<VV, true, 0>(N, T, O, D, H, occ, b, e); } \
+                         else { if (tri) run<VV, false, 1>(N, T, O, D, H, occ, b, e); else run<VV, false, 0>(N, T, O, D, H, occ, b, e); } } while (0)
+        if (variant == 2) REF_RUN(2); else if (variant == 4) REF_RUN(4); else REF_RUN(8);
+#undef REF_RUN
+    };
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> ts;
+    for (int k = 0; k < threads; k++) ts.emplace_back(fn, n * k / threads, n * (k + 1) / threads);
+    for (auto& t : ts) t.join();
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// The legacy diffuse frame on host threads, for the CPU baseline of the frame metric. The reference has no CPU
+// renderer (its shading runs only as CUDA kernels), so this harness strings together the reference's own
+// host-compilable code - rng4 (core/rng.h), sampleUniformCone / sampleCosineHemisphere / onb (core/sampling.h), the
+// float3 helpers (core/vec.h) and trav<V, ANY, TRI> (accel/traverse.cuh) - with the per-vertex logic of k_raygen and
+// shadeOne (render/wavefront.cu:42-58, 94-136) restated around them. Paths are traced one after another per thread.
+// P points at a cwp_params-layout struct (include/cwp_b200.h). Pixels [pix0, pix1), samples [s_base, s_base + spp);
+// returns seconds, adds radiance sums to accum (float4 per pixel) and ray counts to counts[0..1].
+struct RefParams {
+    float pos[3], ax[3], ay[3], az[3]; float fx, fy, px, py; int w, h; float lens_r, focus_d;
+    float sun_to[3], sun_e[3], sky[3]; float sun_cos; int max_b; unsigned seed; float eps, near_clip; int has_n, filter_bh; float ftab[65];
+};
+
+template <int V, int TRI>
+static void ref_paths(const RefParams& P, const float4* nodes, const float4* tv, const float4* tris, const float3* albedo, int bounces,
+                      int spp, int sBase, long pix0, long pix1, float* accum, long long* nClosest, long long* nShadow) {
+    const float3 ax = make_float3(P.ax[0], P.ax[1], P.ax[2]), ay = make_float3(P.ay[0], P.ay[1], P.ay[2]), az = make_float3(P.az[0], P.az[1], P.az[2]);
+    const float3 pos = make_float3(P.pos[0], P.pos[1], P.pos[2]), sunTo = make_float3(P.sun_to[0], P.sun_to[1], P.sun_to[2]);
+    const float3 sunE = make_float3(P.sun_e[0], P.sun_e[1], P.sun_e[2]), sky = make_float3(P.sky[0], P.sky[1], P.sky[2]);
+    const int depths = bounces + 2;
+    for (long pix = pix0; pix < pix1; pix++) {
+        const int x = (int)(pix % P.w), y = (int)(pix / P.w);
+        for (int smp = sBase; smp < sBase + spp; smp++) {
+            float u0 = rng4(pix, smp, 0, 0, P.seed), u1 = rng4(pix, smp, 0, 1, P.seed), jx, jy;
+            if (P.filter_bh) { jx = sampleTable(P.ftab, 64, u0); jy = sampleTable(P.ftab, 64, u1); } else { jx = u0 - 0.5f; jy = u1 - 0.5f; }
+            float dx = (x + 0.5f + jx - P.px) / P.fx, dy = -(y + 0.5f + jy - P.py) / P.fy;
+            float3 d = normalize(ax * dx + ay * dy - az), o = pos, T = make_float3(1.f, 1.f, 1.f); float tmin = P.near_clip;
+            for (int depth = 0; depth < depths; depth++) {
+                (*nClosest)++;
+                float t = 1e30f, u = 0.f, v = 0.f; int tri = -1;
+                trav<V, false, TRI>(nodes, tv, o, d, tmin, t, tri, u, v);
+                if (tri < 0) { float3 c = T * sky; accum[4 * pix] += c.x; accum[4 * pix + 1] += c.y; accum[4 * pix + 2] += c.z; break; }
+                if (depth > P.max_b) break;
+                float3 p = o + d * t; float4 b = tris[3 * tri + 1], c4 = tris[3 * tri + 2];
+                float3 ng = normalize(cross(xyz(b), xyz(c4))), ns = ng;
+                if (dot(ng, d) > 0.f) { ng = -ng; ns = -ns; }
+                float3 alb = albedo[__float_as_int(b.w)];
+                float3 po = p + ng * P.eps;
+                float3 l = sampleUniformCone(sunTo, P.sun_cos, rng4(pix, smp, depth + 1, 2, P.seed), rng4(pix, smp, depth + 1, 3, P.seed));
+                float cl = dot(ns, l);
+                if (cl > 0.f && dot(ng, l) > 0.f) {
+                    float3 contrib = T * alb * sunE * (cl * CWP_INV_PI); (*nShadow)++;
+                    float st = 1e30f, su, sv; int stri = -1;
+                    if (!trav<V, true, TRI>(nodes, tv, po, l, 0.f, st, stri, su, sv)) { accum[4 * pix] += contrib.x; accum[4 * pix + 1] += contrib.y; accum[4 * pix + 2] += contrib.z; }
+                }
+                float3 nd = sampleCosineHemisphere(ns, rng4(pix, smp, depth + 1, 0, P.seed), rng4(pix, smp, depth + 1, 1, P.seed));
+                if (dot(nd, ng) <= 0.f) break;
+                T = T * alb; o = po; d = nd; tmin = 0.f;
+            }
+        }
+    }
+}
+
+extern "C" double ref_render_cpu(const void* params, int variant, int tri, const float* nodes, const float* tv, const float* tris, const float* albedo,
+                                 int bounces, int spp, int s_base, long pix0, long pix1, float* accum, long long* counts, int threads) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    const RefParams& P = *(const RefParams*)params;
+    std::vector<long long> nc(threads, 0), ns(threads, 0);
+    auto fn = [&](int k) {
+        long b = pix0 + (pix1 - pix0) * k / threads, e = pix0 + (pix1 - pix0) * (k + 1) / threads;
+        const float4 *N = (const float4*)nodes, *T = (const float4*)tv, *TR = (const float4*)tris; const float3* A = (const float3*)albedo;
+        if (variant == 2) { if (tri) ref_paths<2, 1>(P, N, T, TR, A, bounces, spp, s_base, b, e, accum, &nc[k], &ns[k]); else ref_paths<2, 0>(P, N, T, TR, A, bounces, spp, s_base, b, e, accum, &nc[k], &ns[k]); }
+        else if (variant == 4) { if (tri) ref_paths<4, 1>(P, N, T, TR, A, bounces, spp, s_base, b, e, accum, &nc[k], &ns[k]); else ref_paths<4, 0>(P, N, T, TR, A, bounces, spp, s_base, b, e, accum, &nc[k], &ns[k]); }
+        else { if (tri) ref_paths<8, 1>(P, N, T, TR, A, bounces, spp, s_base, b, e, accum, &nc[k], &ns[k]); else ref_paths<8, 0>(P, N, T, TR, A, bounces, spp, s_base, b, e, accum, &nc[k], &ns[k]); }
+    };
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> ts;
+    for (int k = 0; k < threads; k++) ts.emplace_back(fn, k);
+    for (auto& t : ts) t.join();
+    double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (int k = 0; k < threads; k++) { counts[0] += nc[k]; counts[1] += ns[k]; }
+    return sec;
+}

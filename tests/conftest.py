@@ -1,0 +1,163 @@
+"""Shared fixtures: the library under test, the oracle (test infrastructure) and, where built, the reference's own
+code compiled from its sources (oracle/_ref)."""
+import ctypes as C
+import importlib
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); run with -m gpu")
+
+
+def has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def cwp():
+    return importlib.import_module("cuda-wavefront-pathtracer_b200")
+
+
+def _load_oracle():
+    path = os.path.join(ROOT, "oracle", "liboracle.so")
+    if not os.path.exists(path):
+        import subprocess
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=True, capture_output=True)
+    L = C.CDLL(path)
+    L.orc_build.restype = C.c_long
+    L.orc_build.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.orc_pack.restype = None
+    L.orc_pack.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.orc_trace.restype = C.c_long
+    L.orc_trace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_render.restype = None
+    L.orc_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    L.orc_rng.restype = C.c_float
+    L.orc_rng.argtypes = [C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint]
+    return L
+
+
+class Oracle:
+    """Thin numpy wrapper around liboracle.so."""
+
+    def __init__(self):
+        self.L = _load_oracle()
+
+    def build(self, verts, faces, bins=16, leaf=4, variant=2):
+        nt = len(faces)
+        cap = 5 * 2 * nt + 64
+        nodes = np.zeros((cap, 4), np.float32); order = np.zeros(nt, np.int32)
+        md = C.c_int(); sah = C.c_double()
+        v = np.ascontiguousarray(verts, np.float32); f = np.ascontiguousarray(faces, np.int32)
+        n = self.L.orc_build(v.ctypes.data, f.ctypes.data, nt, bins, leaf, variant, nodes.ctypes.data, cap, order.ctypes.data, C.byref(md), C.byref(sah))
+        assert n > 0
+        return nodes[:n].copy(), order, md.value, sah.value
+
+    def pack(self, verts, faces, fm, order):
+        n = len(order)
+        tris = np.zeros((3 * n, 4), np.float32); woop = np.zeros((3 * n, 4), np.float32)
+        v = np.ascontiguousarray(verts, np.float32); f = np.ascontiguousarray(faces, np.int32); fm = np.ascontiguousarray(fm, np.int32)
+        o = np.ascontiguousarray(order, np.int32)
+        self.L.orc_pack(v.ctypes.data, f.ctypes.data, fm.ctypes.data, o.ctypes.data, n, tris.ctypes.data, woop.ctypes.data)
+        return tris, woop
+
+    def trace(self, variant, tri, any_hit, nodes, tv, o, d, stats=False):
+        n = len(o)
+        hits = np.zeros((n, 4), np.float32); occ = np.zeros(n, np.int32); st = np.zeros(2, np.int64)
+        bad = self.L.orc_trace(variant, tri, 1 if any_hit else 0, np.ascontiguousarray(nodes).ctypes.data, np.ascontiguousarray(tv).ctypes.data,
+                               np.ascontiguousarray(o).ctypes.data, np.ascontiguousarray(d).ctypes.data, n, hits.ctypes.data, occ.ctypes.data,
+                               st.ctypes.data if stats else None)
+        assert bad == 0
+        res = occ if any_hit else hits
+        return (res, st) if stats else res
+
+    def render(self, params, variant, tri, bvh, bounces, spp, s_base=0, pix0=0, pix1=None):
+        w, h = params.cam.w, params.cam.h
+        acc = np.zeros((w * h, 4), np.float32); rc = np.zeros(2, np.int64)
+        tv = bvh.woop if tri == 1 else bvh.tris
+        alb = np.ascontiguousarray(bvh.albedo, np.float32)
+        self.L.orc_render(C.addressof(params), variant, tri, bvh.nodes.ctypes.data, tv.ctypes.data, bvh.tris.ctypes.data, alb.ctypes.data,
+                          bounces, spp, s_base, pix0, w * h if pix1 is None else pix1, acc.ctypes.data, rc.ctypes.data)
+        return acc, rc
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    return Oracle()
+
+
+class Ref:
+    """The reference's own host code (oracle/_ref/libcwpref.so)."""
+
+    def __init__(self, path):
+        L = C.CDLL(path)
+        L.ref_build.restype = C.c_long
+        L.ref_build.argtypes = [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ref_trace.restype = C.c_double
+        L.ref_trace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_int]
+        self.L = L
+
+    def build(self, verts, faces, fm, variant=2, leaf=4, collapse=0):
+        nt = len(faces); cap = 5 * 2 * nt + 64
+        nodes = np.zeros((cap, 4), np.float32); order = np.zeros(nt, np.int32)
+        tris = np.zeros((3 * nt, 4), np.float32); woop = np.zeros((3 * nt, 4), np.float32)
+        md = C.c_int(); sah = C.c_double(); ms = C.c_double()
+        v = np.ascontiguousarray(verts, np.float32); f = np.ascontiguousarray(faces, np.int32); m = np.ascontiguousarray(fm, np.int32)
+        n = self.L.ref_build(v.ctypes.data, len(v), f.ctypes.data, m.ctypes.data, nt, variant, leaf, collapse, nodes.ctypes.data, cap,
+                             order.ctypes.data, tris.ctypes.data, woop.ctypes.data, C.byref(md), C.byref(sah), C.byref(ms))
+        assert n > 0
+        return dict(nodes=nodes[:n].copy(), order=order, tris=tris, woop=woop, max_depth=md.value, sah=sah.value)
+
+    def trace(self, variant, tri, any_hit, nodes, tv, o, d, threads=0):
+        n = len(o)
+        hits = np.zeros((n, 4), np.float32); occ = np.zeros(n, np.int32)
+        self.L.ref_trace(variant, 1 if any_hit else 0, tri, np.ascontiguousarray(nodes).ctypes.data, np.ascontiguousarray(tv).ctypes.data,
+                         np.ascontiguousarray(o).ctypes.data, np.ascontiguousarray(d).ctypes.data, n, hits.ctypes.data, occ.ctypes.data, threads)
+        return occ if any_hit else hits
+
+
+@pytest.fixture(scope="session")
+def ref():
+    path = os.path.join(REF_DIR, "libcwpref.so")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref not built (needs the reference sources; see oracle/Makefile)")
+    return Ref(path)
+
+
+@pytest.fixture(scope="session")
+def gpu():
+    if not has_gpu():
+        pytest.skip("no CUDA GPU")
+    import torch
+    torch.cuda.init()
+    return torch
+
+
+def golden(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def tie_or_equal(h_a, h_b, rel=1e-6):
+    """Per-ray classification of two closest-hit float4 arrays: (same id, tie, lost). A tie is two hits whose
+    distances agree within rel * t; lost is hit vs miss or different hits at different distances."""
+    ia, ib = h_a[:, 3].view(np.int32), h_b[:, 3].view(np.int32)
+    same = ia == ib
+    both = (ia >= 0) & (ib >= 0)
+    ta, tb = h_a[:, 0].astype(np.float64), h_b[:, 0].astype(np.float64)
+    tie = ~same & both & (np.abs(ta - tb) <= rel * np.maximum(np.abs(ta), np.abs(tb)))
+    lost = ~same & ~tie
+    return same, tie, lost

@@ -1,0 +1,151 @@
+"""Ray-batch traversal on the GPU through the C ABI (cwp_trace_closest / cwp_trace_any) against the oracle (bit for
+bit: same fused arithmetic) and against the reference's own traversal (IDs equal except exact ties, |dt| <= 1e-6 t):
+its host build via oracle/_ref and its device build via oracle/_ref/libcwpref_gpu.so on identical batches."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REF_DIR, golden, tie_or_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def gpu_trace(torch, accel, o, d, any_hit=False):
+    to, td = dev(torch, o), dev(torch, d)
+    n = len(o)
+    if any_hit:
+        out = torch.empty(n, dtype=torch.int32, device="cuda")
+        accel.trace_any(to.data_ptr(), td.data_ptr(), out.data_ptr(), n)
+    else:
+        out = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        accel.trace_closest(to.data_ptr(), td.data_ptr(), out.data_ptr(), n)
+    torch.cuda.synchronize()
+    accel.status()
+    return out.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def g():
+    return golden("boxes64.npz")
+
+
+@pytest.mark.parametrize("name,variant", [("bvh2", 2), ("cwbvh", 8)])
+@pytest.mark.parametrize("tri", [1, 0])
+def test_fixture_batch_bitexact_vs_oracle(gpu, cwp, oracle, g, name, variant, tri):
+    mesh = cwp.Mesh.from_arrays(g["verts"], g["faces"], g["face_mat"])
+    bvh = cwp.Bvh(mesh, variant=variant, bins=16, leaf=4)
+    acc = cwp.Accel(bvh, tri=tri)
+    o, d = g["rays_o"], g["rays_d"]
+    tv = bvh.woop if tri else bvh.tris
+    h = gpu_trace(gpu, acc, o, d)
+    assert np.array_equal(h.view(np.uint32), oracle.trace(variant, tri, False, bvh.nodes, tv, o, d).view(np.uint32))
+    occ = gpu_trace(gpu, acc, o, d, any_hit=True)
+    assert np.array_equal(occ, oracle.trace(variant, tri, True, bvh.nodes, tv, o, d))
+    # and against what the reference produced for the same batch
+    same, tie, lost = tie_or_equal(h, g[f"{name}_t{tri}_closest"])
+    assert lost.sum() == 0
+    assert np.array_equal(occ >= 0, g[f"{name}_t{tri}_any"] >= 0)
+
+
+@pytest.mark.parametrize("variant", [2, 4, 8])
+def test_incoherent_12k_bitexact_vs_oracle(gpu, cwp, oracle, variant):
+    mesh, bvh = cwp.scene("boxes12k", variant=variant, bins=32)
+    acc = cwp.Accel(bvh, tri=1)
+    p = cwp.frame_params(mesh, 256, 256)
+    o, d = cwp.incoherent_rays(65536, p, bvh.tris, lambda o, d: gpu_trace(gpu, acc, o, d), seed=21)
+    h = gpu_trace(gpu, acc, o, d)
+    if variant != 4:
+        ho = oracle.trace(variant, 1, False, bvh.nodes, bvh.woop, o, d)
+        assert np.array_equal(h.view(np.uint32), ho.view(np.uint32))
+        assert np.array_equal(gpu_trace(gpu, acc, o, d, True), oracle.trace(variant, 1, True, bvh.nodes, bvh.woop, o, d))
+    else:   # BVH4 (no oracle form): the same original triangles as BVH2, up to ties
+        _, b2 = cwp.scene("boxes12k", variant=2, bins=32)
+        h2 = gpu_trace(gpu, cwp.Accel(b2, tri=1), o, d)
+        same, tie, lost = tie_or_equal(with_mesh_ids(bvh, h), with_mesh_ids(b2, h2))
+        assert lost.sum() == 0
+
+
+def with_mesh_ids(bvh, hits):
+    """hits with the leaf-order triangle index replaced by the mesh triangle id stored in tris[3k].w"""
+    h = hits.copy(); t = h[:, 3].view(np.int32)
+    ids = np.where(t >= 0, bvh.tris[3 * np.maximum(t, 0), 3].view(np.int32), -1).astype(np.int32)
+    h[:, 3] = ids.view(np.float32)
+    return h
+
+
+def test_vs_reference_gpu_traversal_117k(gpu, cwp):
+    path = os.path.join(REF_DIR, "libcwpref_gpu.so")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref/libcwpref_gpu.so not built")
+    L = C.CDLL(path)
+    L.ref_gpu_trace.restype = C.c_int
+    L.ref_gpu_trace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]
+    for variant in (2, 8):
+        mesh, bvh = cwp.scene("boxes117k", variant=variant, bins=16)
+        acc = cwp.Accel(bvh, tri=1)
+        p = cwp.frame_params(mesh, 512, 512)
+        o, d = cwp.incoherent_rays(1 << 20, p, bvh.tris, lambda o, d: gpu_trace(gpu, acc, o, d), seed=31)
+        h = gpu_trace(gpu, acc, o, d)
+        occ = gpu_trace(gpu, acc, o, d, True)
+        nodes, woop, to, td = dev(gpu, bvh.nodes), dev(gpu, bvh.woop), dev(gpu, o), dev(gpu, d)
+        rh = gpu.empty((len(o), 4), dtype=gpu.float32, device="cuda"); ro = gpu.empty(len(o), dtype=gpu.int32, device="cuda")
+        assert L.ref_gpu_trace(variant, 0, 1, nodes.data_ptr(), woop.data_ptr(), to.data_ptr(), td.data_ptr(), len(o), rh.data_ptr(), None, None) == 0
+        assert L.ref_gpu_trace(variant, 1, 1, nodes.data_ptr(), woop.data_ptr(), to.data_ptr(), td.data_ptr(), len(o), None, ro.data_ptr(), None) == 0
+        gpu.cuda.synchronize()
+        same, tie, lost = tie_or_equal(h, rh.cpu().numpy())
+        # the reference's device build uses approximate division (--use_fast_math): only ties and grazing rays may differ
+        assert lost.sum() <= len(o) * 2e-5, (variant, int(lost.sum()), int(tie.sum()))
+        agree = np.mean((occ >= 0) == (ro.cpu().numpy() >= 0))
+        assert agree >= 1 - 2e-5, agree
+
+
+def test_edge_cases(gpu, cwp, oracle):
+    mesh, bvh = cwp.scene("boxes12k", variant=8, bins=16)
+    acc = cwp.Accel(bvh, tri=1)
+    # n = 0 is a no-op
+    acc.trace_closest(0, 0, 0, 0)
+    # axis-parallel directions (reciprocal of 0), tmax shorter than any hit, tmin > tmax, origins inside boxes
+    o = np.array([[0, 0, 10, 0], [0.5, 0.5, 10, 0], [0, 0, 10, 0], [0, 0, 10, 20], [3, -2, 0.05, 0], [0, 0, -1, 0]], np.float32)
+    d = np.array([[0, 0, -1, 1e30], [0, 0, -1, 1e30], [0, 0, -1, 1e-3], [0, 0, -1, 1], [1, 0, 0, 1e30], [0, 0, 1, 1e30]], np.float32)
+    h = gpu_trace(gpu, acc, o, d)
+    ho = oracle.trace(8, 1, False, bvh.nodes, bvh.woop, o, d)
+    assert np.array_equal(h.view(np.uint32), ho.view(np.uint32))
+    assert h[2, 3].view(np.int32) == -1 and h[2, 0] == np.float32(1e-3)   # miss keeps t = tmax
+    assert h[3, 3].view(np.int32) == -1
+    assert h[0, 3].view(np.int32) >= 0 and h[5, 3].view(np.int32) >= 0    # from below the ground: hits its underside
+
+
+def test_host_entry_points_match_device(gpu, cwp):
+    mesh, bvh = cwp.scene("boxes12k", variant=2, bins=16)
+    acc = cwp.Accel(bvh, tri=1)
+    p = cwp.frame_params(mesh, 128, 128)
+    o, d = cwp.camera_rays(p, 5000, seed=2)
+    hh, ms = acc.trace_closest_host(o, d)
+    assert ms > 0
+    assert np.array_equal(hh.view(np.uint32), gpu_trace(gpu, acc, o, d).view(np.uint32))
+    occ, _ = acc.trace_any_host(o, d)
+    assert np.array_equal(occ, gpu_trace(gpu, acc, o, d, True))
+
+
+def test_full_size_batch_properties(gpu, cwp, oracle):
+    """16M incoherent rays on the 117k-triangle scene: any-hit and closest-hit agree on occlusion for every ray, and a
+    seeded 100k subset is bit-identical to the oracle."""
+    mesh, bvh = cwp.scene("boxes117k", variant=8, bins=32)
+    acc = cwp.Accel(bvh, tri=1)
+    p = cwp.frame_params(mesh, 512, 512)
+    n = 1 << 24
+    o, d = cwp.incoherent_rays(n, p, bvh.tris, lambda o, d: gpu_trace(gpu, acc, o, d), seed=41)
+    h = gpu_trace(gpu, acc, o, d)
+    occ = gpu_trace(gpu, acc, o, d, True)
+    hit = h[:, 3].view(np.int32) >= 0
+    assert np.array_equal(hit, occ >= 0)
+    assert 0.2 < hit.mean() < 0.9
+    sub = np.random.default_rng(0).choice(n, 100000, replace=False)
+    ho = oracle.trace(8, 1, False, bvh.nodes, bvh.woop, o[sub], d[sub])
+    assert np.array_equal(h[sub].view(np.uint32), ho.view(np.uint32))
