@@ -203,10 +203,16 @@ def main():
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
+    ap.add_argument("--spp", type=int, default=0, help="override the frame's samples per pixel (profiling cases)")
+    ap.add_argument("--rays", type=int, default=0, help="override the batch size of trace16m (profiling cases)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.batch:
         wl["batch"] = args.batch
+    if args.spp and "spp" in wl:
+        wl["spp"] = args.spp
+    if args.rays and "rays" in wl:
+        wl["rays"] = args.rays
     ws, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, wl, rank)
@@ -258,11 +264,13 @@ def main():
         c_tot = np.zeros(depths); s_tot = np.zeros(depths); tms = np.zeros(depths); sms = np.zeros(depths)
         clk = Clocks(dev_id)
         barrier()
+        torch.cuda.nvtx.range_push("timed")
         for _ in range(args.steps):
             st = r.render(spp)
             rays += st.rays; shadow += st.shadow_rays; ms += st.frame_ms
             c, s, tm, sm = r.depth_stats()
             c_tot += c; s_tot += s; tms += tm; sms += sm
+        torch.cuda.nvtx.range_pop()
         barrier()
         clocks = clk.stop()
         max_ms = reduce(ms, tdist.ReduceOp.MAX if ws > 1 else None)
@@ -321,12 +329,14 @@ def main():
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps)]
         clk = Clocks(dev_id)
         barrier()
+        torch.cuda.nvtx.range_push("timed")
         for i in range(args.steps):
             ev[3 * i].record(st)
             acc.trace_closest(do.data_ptr(), dd.data_ptr(), hits.data_ptr(), n, st.cuda_stream)
             ev[3 * i + 1].record(st)
             acc.trace_any(do.data_ptr(), dd.data_ptr(), occ.data_ptr(), n, st.cuda_stream)
             ev[3 * i + 2].record(st)
+        torch.cuda.nvtx.range_pop()
         barrier()
         clocks = clk.stop()
         acc.status()

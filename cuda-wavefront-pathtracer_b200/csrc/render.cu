@@ -207,12 +207,13 @@ template <int V, int TRI> int occupancy_of(int& bt0, int& bt, int& bs) {
 
 // ev: 4 events (trace start/end, shadow start/end) or nullptr
 template <int V, int TRI> void launch_depth(cwp_renderer* r, KArgs a, int gt0, int gt, int gs, cudaEvent_t* ev) {
-    if (ev) cudaEventRecord(ev[0], r->st);
+    // external records: inside a stream capture they become event-record nodes of the graph
+    if (ev) cudaEventRecordWithFlags(ev[0], r->st, cudaEventRecordExternal);
     if (a.depth == 0) k_trace_shade<V, TRI, true><<<gt0, 128, 0, r->st>>>(a, r->P);
     else k_trace_shade<V, TRI, false><<<gt, 128, 0, r->st>>>(a, r->P);
-    if (ev) { cudaEventRecord(ev[1], r->st); cudaEventRecord(ev[2], r->st); }
+    if (ev) { cudaEventRecordWithFlags(ev[1], r->st, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], r->st, cudaEventRecordExternal); }
     k_shadow<V, TRI><<<gs, 128, 0, r->st>>>(a);
-    if (ev) cudaEventRecord(ev[3], r->st);
+    if (ev) cudaEventRecordWithFlags(ev[3], r->st, cudaEventRecordExternal);
 }
 
 KArgs base_args(cwp_renderer* r) {

@@ -86,17 +86,19 @@ def test_renderer_errors(gpu, cwp):
 
 def test_psnr_vs_reference_pt(gpu, cwp, tmp_path):
     """The reference's own renderer (built from its sources for sm_100) and ours on identical scene files, camera,
-    lighting and seed: >= 50 dB in tone-mapped sRGB (same sample streams, so far above the two-render noise floor)."""
+    lighting and seed at 256 spp: >= 50 dB in tone-mapped sRGB. The sample streams are the same, but the reference's
+    --use_fast_math build rounds directions differently, so paths decorrelate after a bounce or two and the agreement
+    is set by Monte Carlo noise (about 38 dB at 16 spp, 55 dB at 256 spp), which is why the bound is taken at 256 spp."""
     pt = os.path.join(REF_DIR, "pt")
     if not os.path.exists(pt):
         pytest.skip("oracle/_ref/pt not built")
     mesh, bvh = cwp.scene("boxes12k", variant=2, bins=16)
-    w, h, spp = 256, 256, 16
+    w, h, spp = 256, 256, 256
     p = cwp.frame_params(mesh, w, h)
-    args = cwp.reference_inputs(mesh, p, str(tmp_path), w, h, spp, 16)
+    args = cwp.reference_inputs(mesh, p, str(tmp_path), w, h, spp, 256)
     out = str(tmp_path / "ref")
     subprocess.run([pt] + args + ["--out", out, "--reps", "1", "--warm", "0"], check=True, capture_output=True, timeout=300)
     ref_img = cwp.imageio.read_pfm(out + ".pfm")
-    _, _, st, acc = render(cwp, mesh, bvh, w, h, spp, 16, 2)
+    _, _, st, acc = render(cwp, mesh, bvh, w, h, spp, 256, 2)
     ours = cwp.imageio.accum_to_image(acc, w, h, spp)
     assert cwp.imageio.psnr(ours, ref_img) >= 50.0
