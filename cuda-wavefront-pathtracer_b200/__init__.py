@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libcwpb200.so")
+LIB_PATH = os.environ.get("CWPB_LIB") or os.path.join(_HERE, "libcwpb200.so")   # CWPB_LIB: load another build of the library
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_TRAVERSAL, ERR_IO = range(7)
 LAYOUT_BVH2, LAYOUT_BVH4, LAYOUT_CWBVH = 2, 4, 8

@@ -74,8 +74,12 @@ __device__ __forceinline__ void camera_ray(const cwp_params& P, int i, int N, in
     }
 }
 
+#ifndef CWPB_TRACE_MINB
+#define CWPB_TRACE_MINB 8   // resident 128-thread blocks per SM the traversal kernels are compiled for
+#endif
+
 template <int V, int TRI, bool PRIMARY>
-__global__ void __launch_bounds__(128, 8) k_trace_shade(const __grid_constant__ KArgs a, const __grid_constant__ cwp_params P) {
+__global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade(const __grid_constant__ KArgs a, const __grid_constant__ cwp_params P) {
     int* const c = a.cnt + 4 * a.depth;
     int* const cNext = c + 4;
     const int n = PRIMARY ? a.nk : c[0];
@@ -90,18 +94,20 @@ __global__ void __launch_bounds__(128, 8) k_trace_shade(const __grid_constant__ 
         if (base >= n) break;
         const int k = base + lane;
         const bool valid = k < n;
-        float3 o = f3(0.f, 0.f, 0.f), d = f3(0.f, 0.f, 1.f), T = f3(1.f, 1.f, 1.f);
-        int id = 0, pix = 0; unsigned smp = 0; float tmin = 0.f;
+        // only the ray is live across the traversal; throughput and path id are read (or recomputed) afterwards
+        float3 o = f3(0.f, 0.f, 0.f), d = f3(0.f, 0.f, 1.f);
+        int pix = 0; unsigned smp = 0; float tmin = 0.f;
         if (valid) {
-            if (PRIMARY) { id = k; camera_ray(P, k, a.N, a.sBase, o, d, pix, smp); tmin = P.near_clip; }
-            else {
-                const float4 s0 = __ldcs(a.q.s0[rd] + k), s1 = __ldcs(a.q.s1[rd] + k); const float2 s2 = __ldcs(a.q.s2[rd] + k);
-                o = xyz(s0); d = xyz(s1); T = f3(s1.w, s2.x, s2.y); id = __float_as_int(s0.w);
-                pix = id % a.N; smp = (unsigned)(a.sBase + id / a.N);
-            }
+            if (PRIMARY) { camera_ray(P, k, a.N, a.sBase, o, d, pix, smp); tmin = P.near_clip; }
+            else { const float4 s0 = __ldcs(a.q.s0[rd] + k), s1 = __ldcs(a.q.s1[rd] + k); o = xyz(s0); d = xyz(s1); }
         }
         float t = 1e30f, hu = 0.f, hv = 0.f; int tri = -1;
         if (valid) trace_ray<V, false, TRI>(a.nodes, a.tv, o, d, tmin, t, tri, hu, hv, 0, err);
+        float3 T = f3(1.f, 1.f, 1.f); int id = k;
+        if (valid && !PRIMARY) {
+            id = __float_as_int(__ldg(&a.q.s0[rd][k].w)); const float tr = __ldg(&a.q.s1[rd][k].w); const float2 s2 = __ldcs(a.q.s2[rd] + k);
+            T = f3(tr, s2.x, s2.y); pix = id % a.N; smp = (unsigned)(a.sBase + id / a.N);
+        }
         bool wantShadow = false, wantCont = false;
         float3 po = o, l = d, contrib = T, nd = d;
         if (valid) {
@@ -145,7 +151,7 @@ __global__ void __launch_bounds__(128, 8) k_trace_shade(const __grid_constant__ 
 }
 
 template <int V, int TRI>
-__global__ void __launch_bounds__(128, 8) k_shadow(const __grid_constant__ KArgs a) {
+__global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow(const __grid_constant__ KArgs a) {
     int* const c = a.cnt + 4 * a.depth;
     const int n = c[1];
     const int lane = threadIdx.x & 31;

@@ -3,8 +3,11 @@
 //
 // Traversal order, tie rules and leaf handling are those of the reference's device traversal (accel/traverse.cuh):
 // strict tmin < t < hitT (the first triangle found at a given t wins), nearer-child-first BVH2 descent, BVH4 children
-// sorted by entry distance, CWBVH children visited in ray-octant order with leaves tested during the node visit. So
-// for the same ray the same triangle is reported, except at exact ties that rounding may break differently.
+// sorted by entry distance, CWBVH children visited in ray-octant order with the node's hit leaves tested in slot order
+// before descending. So for the same ray the same triangle is reported, except at exact ties that rounding may break
+// differently. (The CWBVH node visit runs its eight slab tests before its leaf tests, where the reference interleaves
+// them; leaf order and descent order are unchanged, so only boxes that a closer hit would have culled a little earlier
+// are visited and rejected one level lower.)
 //
 // Implementation for sm_100a: nodes and triangles are read with 16-byte read-only loads (ld.global.nc.v4), every
 // slab/plane evaluation is one explicit FMA, the short stack lives in registers/local memory, and each traversal
@@ -136,6 +139,11 @@ __device__ __forceinline__ bool trav_bvh4(const float4* __restrict__ nodes, cons
 
 // ---------------- CWBVH ----------------
 __device__ __forceinline__ unsigned byte_of(unsigned w, int s) { return (w >> (8 * (s & 3))) & 255u; }
+// Byte s of w as an exact float without an int->float conversion (those run on the quarter-rate XU pipe): the byte
+// permute builds the bit pattern 0x4B0000bb, which is the float 2^23 + b, and the subtraction is exact.
+__device__ __forceinline__ float qbyte(unsigned w, int s) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | (unsigned)(s & 3))) - 8388608.0f;
+}
 
 template <bool ANY, int TRI>
 __device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
@@ -143,6 +151,10 @@ __device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, con
     uint2 stack[kStack8]; int sp = 0, budget = kVisitBudget;
     const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z);
     const unsigned oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
+    // per axis, the plane a ray enters first: the low bound when the reciprocal is positive, else the high bound.
+    // Selecting it replaces the min/max of each (low, high) pair and gives the same values: the fused affine map
+    // q * s + o is monotonic in q for either sign of s.
+    const bool fx = idx < 0.f, fy = idy < 0.f, fz = idz < 0.f;
     unsigned cb = 0, im = 0, hm = 0; int node = root;
     while (true) {
         if (--budget < 0) { err |= kTravBudget; return hitTri >= 0; }
@@ -153,23 +165,34 @@ __device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, con
         const float ox = (f0.x - o.x) * idx, oy = (f0.y - o.y) * idy, oz = (f0.z - o.z) * idz;
         const unsigned imask = ew >> 24, m0 = __float_as_uint(f1.z), m1 = __float_as_uint(f1.w);
         const int childBase = __float_as_int(f1.x), triBase = __float_as_int(f1.y);
-        const unsigned qlx0 = __float_as_uint(f2.x), qlx1 = __float_as_uint(f2.y), qly0 = __float_as_uint(f2.z), qly1 = __float_as_uint(f2.w);
-        const unsigned qlz0 = __float_as_uint(f3_.x), qlz1 = __float_as_uint(f3_.y), qhx0 = __float_as_uint(f3_.z), qhx1 = __float_as_uint(f3_.w);
-        const unsigned qhy0 = __float_as_uint(f4_.x), qhy1 = __float_as_uint(f4_.y), qhz0 = __float_as_uint(f4_.z), qhz1 = __float_as_uint(f4_.w);
-        unsigned hits = 0;
+        // quantised bounds: lo x (f2.x, f2.y), lo y (f2.z, f2.w), lo z (f3.x, f3.y), hi x (f3.z, f3.w), hi y (f4.x, f4.y), hi z (f4.z, f4.w)
+        const unsigned nx0 = __float_as_uint(fx ? f3_.z : f2.x), nx1 = __float_as_uint(fx ? f3_.w : f2.y), px0 = __float_as_uint(fx ? f2.x : f3_.z), px1 = __float_as_uint(fx ? f2.y : f3_.w);
+        const unsigned ny0 = __float_as_uint(fy ? f4_.x : f2.z), ny1 = __float_as_uint(fy ? f4_.y : f2.w), py0 = __float_as_uint(fy ? f2.z : f4_.x), py1 = __float_as_uint(fy ? f2.w : f4_.y);
+        const unsigned nz0 = __float_as_uint(fz ? f4_.z : f3_.x), nz1 = __float_as_uint(fz ? f4_.w : f3_.y), pz0 = __float_as_uint(fz ? f3_.x : f4_.z), pz1 = __float_as_uint(fz ? f3_.y : f4_.w);
+        // all eight slab tests first (predicated, no branches), then the hit leaves in slot order
+        unsigned boxHit = 0;
 #pragma unroll
         for (int s = 0; s < 8; s++) {
+            const float xn = fmaf(qbyte(s < 4 ? nx0 : nx1, s), sx, ox), xf = fmaf(qbyte(s < 4 ? px0 : px1, s), sx, ox);
+            const float yn = fmaf(qbyte(s < 4 ? ny0 : ny1, s), sy, oy), yf = fmaf(qbyte(s < 4 ? py0 : py1, s), sy, oy);
+            const float zn = fmaf(qbyte(s < 4 ? nz0 : nz1, s), sz, oz), zf = fmaf(qbyte(s < 4 ? pz0 : pz1, s), sz, oz);
+            const float tn = fmaxf(fmaxf(xn, yn), fmaxf(zn, tmin));
+            const float tf = fminf(fminf(xf, yf), fminf(zf, hitT));
+            boxHit |= (tn <= tf ? 1u : 0u) << s;
+        }
+        // leaf slots: meta bit 7 of each byte
+        const unsigned leafMask = ((m0 >> 7) & 1u) | ((m0 >> 14) & 2u) | ((m0 >> 21) & 4u) | ((m0 >> 28) & 8u) |
+                                  ((m1 >> 3) & 16u) | ((m1 >> 10) & 32u) | ((m1 >> 17) & 64u) | ((m1 >> 24) & 128u);
+        unsigned leafHit = boxHit & leafMask;
+        // internal children hit, re-indexed to octant order (slot s -> bit s ^ oct)
+        unsigned hits = boxHit & imask;
+        if (oct & 1u) hits = ((hits & 0x55u) << 1) | ((hits & 0xAAu) >> 1);
+        if (oct & 2u) hits = ((hits & 0x33u) << 2) | ((hits & 0xCCu) >> 2);
+        if (oct & 4u) hits = ((hits & 0x0Fu) << 4) | ((hits & 0xF0u) >> 4);
+        while (leafHit) {
+            const int s = __ffs(leafHit) - 1; leafHit &= leafHit - 1;
             const unsigned m = byte_of(s < 4 ? m0 : m1, s);
-            if (m == 0) continue;
-            float x0 = fmaf((float)byte_of(s < 4 ? qlx0 : qlx1, s), sx, ox), x1 = fmaf((float)byte_of(s < 4 ? qhx0 : qhx1, s), sx, ox);
-            float y0 = fmaf((float)byte_of(s < 4 ? qly0 : qly1, s), sy, oy), y1 = fmaf((float)byte_of(s < 4 ? qhy0 : qhy1, s), sy, oy);
-            float z0 = fmaf((float)byte_of(s < 4 ? qlz0 : qlz1, s), sz, oz), z1 = fmaf((float)byte_of(s < 4 ? qhz0 : qhz1, s), sz, oz);
-            float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-            float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), hitT));
-            if (tn <= tf) {
-                if (m & 0x80u) { if (leaf_hit<ANY, TRI>(tv, triBase + (int)(m & 31u), (int)((m >> 5) & 3u) + 1, o, d, tmin, hitT, hitTri, hu, hv) && ANY) return true; }
-                else hits |= 1u << (s ^ oct);
-            }
+            if (leaf_hit<ANY, TRI>(tv, triBase + (int)(m & 31u), (int)((m >> 5) & 3u) + 1, o, d, tmin, hitT, hitTri, hu, hv) && ANY) return true;
         }
         if (hits) {
             if (hm) { if (sp == kStack8) { err |= kTravOverflow; return hitTri >= 0; } stack[sp++] = make_uint2(cb, (im << 8) | hm); }

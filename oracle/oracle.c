@@ -16,7 +16,8 @@
  *   BVH2 layout .................. accel/bvh_layouts.cpp:6-30
  *   CWBVH SAH collapse ........... accel/bvh_tools.cpp:46-168
  *   triangle / Woop packing ...... accel/tri_pack.cpp:6-38
- *   traversal (BVH2, CWBVH) ...... accel/traverse.cuh:10-70, 112-152
+ *   traversal (BVH2, CWBVH) ...... accel/traverse.cuh:10-70, 112-152 (a CWBVH node's slab tests all run before its
+ *                                  leaf tests, in slot order; descent order as the reference)
  *   camera ray + legacy shading .. render/wavefront.cu:42-58, 94-136, frame loop 684-741
  *   FP64 watertight reference .... not in the reference (precision-form oracle; Woop, Benthin & Wald, JCGT 2013)
  */
@@ -442,7 +443,8 @@ static int trav8(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any,
         float ox = (f0.x - o.x) * idx, oy = (f0.y - o.y) * idy, oz = (f0.z - o.z) * idz;
         unsigned imask = ew >> 24, m0 = fu(f1.z), m1 = fu(f1.w); int childBase = fi(f1.x), triBase = fi(f1.y);
         unsigned q[12] = { fu(f2.x), fu(f2.y), fu(f2.z), fu(f2.w), fu(f3.x), fu(f3.y), fu(f3.z), fu(f3.w), fu(f4.x), fu(f4.y), fu(f4.z), fu(f4.w) };
-        unsigned hits = 0;
+        /* the eight slab tests first, then the hit leaves in slot order, then descent (the library's node visit) */
+        unsigned hits = 0, leafHit = 0;
         for (int s = 0; s < 8; s++) {
             unsigned m = byte_of(s < 4 ? m0 : m1, s); int hi = s < 4 ? 0 : 1;
             if (m == 0) continue;
@@ -451,10 +453,11 @@ static int trav8(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any,
             float z0 = fmaf((float)byte_of(q[4 + hi], s), sz, oz), z1 = fmaf((float)byte_of(q[10 + hi], s), sz, oz);
             float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
             float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), *hitT));
-            if (tn <= tf) {
-                if (m & 0x80u) { if (leaf_hit_s(tv, triBase + (int)(m & 31u), (int)((m >> 5) & 3u) + 1, o, d, tmin, any, tri, hitT, hitTri, hu, hv, st) && any) return 1; }
-                else hits |= 1u << (s ^ oct);
-            }
+            if (tn <= tf) { if (m & 0x80u) leafHit |= 1u << s; else hits |= 1u << (s ^ oct); }
+        }
+        for (int s = 0; s < 8; s++) if (leafHit & (1u << s)) {
+            unsigned m = byte_of(s < 4 ? m0 : m1, s);
+            if (leaf_hit_s(tv, triBase + (int)(m & 31u), (int)((m >> 5) & 3u) + 1, o, d, tmin, any, tri, hitT, hitTri, hu, hv, st) && any) return 1;
         }
         if (hits) { if (hm) { if (sp == 40) return -1; stk[sp][0] = cb; stk[sp][1] = (im << 8) | hm; sp++; } cb = (unsigned)childBase; im = imask; hm = hits; }
         while (hm == 0) { if (sp == 0) return *hitTri >= 0; sp--; cb = stk[sp][0]; im = stk[sp][1] >> 8; hm = stk[sp][1] & 255u; }
