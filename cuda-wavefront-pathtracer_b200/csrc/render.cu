@@ -53,10 +53,19 @@ __device__ __forceinline__ int warp_append(int* counter, bool want) {
 
 __device__ __forceinline__ void accum_add(float4* accum, int pix, float3 c) { atomicAdd(accum + pix, make_float4(c.x, c.y, c.z, 0.f)); }
 
-// camera ray of path i (wavefront.cu:42-58): pixel i mod N, sample sBase + i / N
+// Pixel of path i: path i is sample sBase + i / N of pixel tile_pixel(i mod N). When the image is a whole number of
+// 8 x 4 tiles, consecutive paths walk the pixels tile by tile, so a warp's 32 camera rays cover one 8 x 4 block
+// (coherent traversal); otherwise row-major. Either way every (pixel, sample) pair is rendered exactly once.
+__device__ __forceinline__ int tile_pixel(int j, int w, int h) {
+    if ((w & 7) | (h & 3)) return j;
+    const int t = j >> 5, r = j & 31, tilesX = w >> 3;
+    return ((t / tilesX) * 4 + (r >> 3)) * w + (t % tilesX) * 8 + (r & 7);
+}
+
+// camera ray of path i (wavefront.cu:42-58): pixel tile_pixel(i mod N), sample sBase + i / N
 __device__ __forceinline__ void camera_ray(const cwp_params& P, int i, int N, int sBase, float3& o, float3& d, int& pix, unsigned& smp) {
-    pix = i % N; smp = (unsigned)(sBase + i / N);
     const cwp_camera& C = P.cam;
+    pix = tile_pixel(i % N, C.w, C.h); smp = (unsigned)(sBase + i / N);
     const int x = pix % C.w, y = pix / C.w;
     const float u0 = rnd(P, pix, smp, 0, 0), u1 = rnd(P, pix, smp, 0, 1);
     float jx, jy;
@@ -106,7 +115,7 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade(const __gr
         float3 T = f3(1.f, 1.f, 1.f); int id = k;
         if (valid && !PRIMARY) {
             id = __float_as_int(__ldg(&a.q.s0[rd][k].w)); const float tr = __ldg(&a.q.s1[rd][k].w); const float2 s2 = __ldcs(a.q.s2[rd] + k);
-            T = f3(tr, s2.x, s2.y); pix = id % a.N; smp = (unsigned)(a.sBase + id / a.N);
+            T = f3(tr, s2.x, s2.y); pix = tile_pixel(id % a.N, P.cam.w, P.cam.h); smp = (unsigned)(a.sBase + id / a.N);
         }
         bool wantShadow = false, wantCont = false;
         float3 po = o, l = d, contrib = T, nd = d;
