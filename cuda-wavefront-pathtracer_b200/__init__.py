@@ -63,6 +63,10 @@ class RenderOptions(C.Structure):
                 ("block", C.c_int32), ("device", C.c_int32), ("profile", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
+class DeviceScene(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("tris", C.c_void_p), ("woop", C.c_void_p), ("nrm", C.c_void_p), ("albedo", C.c_void_p)]
+
+
 class FrameStats(C.Structure):
     _fields_ = [("rays", C.c_double), ("shadow_rays", C.c_double), ("trace_ms", C.c_double), ("frame_ms", C.c_double)]
 
@@ -101,6 +105,8 @@ SIGNATURES = {
     "cwp_renderer_info_of": (C.c_int, [C.c_void_p, C.POINTER(RendererInfo)]),
     "cwp_renderer_depth_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
     "cwp_renderer_destroy": (None, [C.c_void_p]),
+    "cwp_render_noalloc": (C.c_int, [C.POINTER(Params), C.POINTER(DeviceScene), C.POINTER(RenderOptions), C.c_int32, C.c_int32, C.c_int32,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]),
     "cwp_camera_look_at": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_camera_from_c2w": (C.c_int, [C.POINTER(C.c_float), C.c_float, C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_params_defaults": (C.c_int, [C.POINTER(Params)]),

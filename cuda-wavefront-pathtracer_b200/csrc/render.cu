@@ -483,3 +483,107 @@ extern "C" int cwp_renderer_info_of(const cwp_renderer* r, cwp_renderer_info* ou
     snprintf(out->gpu_name, sizeof out->gpu_name, "%s", r->gpuName.c_str());
     return CWP_OK;
 }
+
+// ---------------------------------------------------------------------------------------------------------------
+// Rendering without any allocation. Some callers cannot call cudaMalloc: a plugin inside a host application that owns
+// the GPU's memory budget, a serving loop that must not stall on cudaMalloc / cudaFree (both can synchronise the
+// device), or code that must not fail on an allocation in the middle of a frame. cwp_render_noalloc gives them the
+// frame of cwp_renderer_render with every scratch buffer (path state, shadow queue, counters) in the fixed array
+// below, which every GPU that loads this library holds until the process exits. The caller passes the scene and the
+// accumulation buffer as device pointers.
+namespace cwpb {
+
+static constexpr long long kNoAllocMaxPaths = 262144;     // w * h * batch of one pass
+static constexpr int kNoAllocMaxBounces = 62;
+static constexpr size_t kNoAllocStateBytes = (size_t)kNoAllocMaxPaths * (2 * (16 + 16 + 8) + (16 + 16 + 8));
+static constexpr size_t kNoAllocCountBytes = 256 * ((4 * (kNoAllocMaxBounces + 3) * sizeof(int) + 255) / 256);
+static constexpr size_t kNoAllocTotBytes = 256 * ((2 * (kNoAllocMaxBounces + 2) * sizeof(unsigned long long) + 255) / 256);
+static constexpr size_t kNoAllocBytes = kNoAllocStateBytes + kNoAllocCountBytes + kNoAllocTotBytes + 256;
+
+// the scratch: 31.5 MB of path state and queues, then the counters, per-depth ray totals and the status word
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+struct NoAllocDevice { unsigned char* base = nullptr; int gridTrace0 = 0, gridTrace = 0, gridShadow = 0; };
+
+// device address of the scratch on the current device, looked up once per device (host code cannot use the symbol
+// itself: on the host it names a stand-in, not device memory)
+static int noalloc_setup(int dev, NoAllocDevice& out) {
+    static NoAllocDevice table[64];
+    static bool ready[64] = { false };
+    CWPB_CHECK(dev >= 0 && dev < 64, CWP_ERR_INVALID, "device ordinal %d out of range", dev);
+    if (!ready[dev]) {
+        void* p = nullptr;
+        CWPB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        NoAllocDevice d; d.base = (unsigned char*)p;
+        int nSM = 0; CWPB_CUDA(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev));
+        int bt0 = 0, bt = 0, bs = 0;
+        // occupancy of the Woop / CWBVH kernels bounds every variant's grid (all share the launch bounds)
+        if (int rc = occupancy_of<8, 1>(bt0, bt, bs)) return rc;
+        d.gridTrace0 = bt0 * nSM; d.gridTrace = bt * nSM; d.gridShadow = bs * nSM;
+        table[dev] = d; ready[dev] = true;
+    }
+    out = table[dev];
+    return CWP_OK;
+}
+
+}  // namespace cwpb
+
+extern "C" int cwp_render_noalloc(const cwp_params* p, const cwp_device_scene* s, const cwp_render_options* o, int32_t spp, int32_t s_base,
+                                  int32_t clear, float* d_accum, int64_t* h_rays, void* stream) {
+    CWPB_CHECK(p && s && o && d_accum, CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(s->nodes && s->tris && s->albedo && (o->tri == 0 || s->woop), CWP_ERR_INVALID, "scene buffers missing");
+    CWPB_CHECK(o->variant == 2 || o->variant == 4 || o->variant == 8, CWP_ERR_INVALID, "variant %d is not 2, 4 or 8", o->variant);
+    CWPB_CHECK(o->tri == 0 || o->tri == 1, CWP_ERR_INVALID, "tri must be 0 or 1");
+    CWPB_CHECK(p->cam.w > 0 && p->cam.h > 0 && o->batch >= 1, CWP_ERR_INVALID, "bad image size or batch");
+    const long long nk = (long long)p->cam.w * p->cam.h * o->batch;
+    CWPB_CHECK(nk <= kNoAllocMaxPaths, CWP_ERR_INVALID, "w*h*batch = %lld paths exceeds the no-allocation limit of %lld per pass (use a smaller batch, or cwp_renderer_*)", nk, kNoAllocMaxPaths);
+    CWPB_CHECK(o->bounces >= 0 && o->bounces <= kNoAllocMaxBounces, CWP_ERR_INVALID, "bounces %d outside [0, %d] of the no-allocation path", o->bounces, kNoAllocMaxBounces);
+    CWPB_CHECK(p->max_b <= o->bounces, CWP_ERR_INVALID, "params max_b %d exceeds bounces %d", p->max_b, o->bounces);
+    CWPB_CHECK(spp > 0 && spp % o->batch == 0 && s_base >= 0, CWP_ERR_INVALID, "spp %d must be a positive multiple of batch %d", spp, o->batch);
+    int dev = 0; CWPB_CUDA(cudaGetDevice(&dev));
+    NoAllocDevice na; if (int rc = noalloc_setup(dev, na)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t NK = (size_t)kNoAllocMaxPaths;
+    unsigned char* b = na.base;
+    Queues q{};
+    for (int k = 0; k < 2; k++) { q.s0[k] = (float4*)b; b += NK * 16; q.s1[k] = (float4*)b; b += NK * 16; q.s2[k] = (float2*)b; b += NK * 8; }
+    q.h0 = (float4*)b; b += NK * 16; q.h1 = (float4*)b; b += NK * 16; q.h2 = (float2*)b; b += NK * 8;
+    int* cnt = (int*)b; b += kNoAllocCountBytes;
+    unsigned long long* tot = (unsigned long long*)b; b += kNoAllocTotBytes;
+    int* err = (int*)b;
+    const int depths = o->bounces + 2, N = p->cam.w * p->cam.h;
+    // the scratch keeps the previous call's contents: totals and status start at zero, counters are reset per pass
+    CWPB_CUDA(cudaMemsetAsync(tot, 0, 2 * (size_t)depths * sizeof(unsigned long long), st));
+    CWPB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    if (clear) CWPB_CUDA(cudaMemsetAsync(d_accum, 0, (size_t)N * 16, st));
+    KArgs a{};
+    a.nodes = (const float4*)s->nodes; a.tv = (const float4*)(o->tri ? s->woop : s->tris); a.tris = (const float4*)s->tris;
+    a.nrm = (const float4*)s->nrm; a.albedo = (const float3*)s->albedo;
+    a.q = q; a.accum = (float4*)d_accum; a.cnt = cnt; a.err = err; a.nk = (int)nk; a.N = N;
+    for (int sb = s_base; sb < s_base + spp; sb += o->batch) {
+        k_pass_begin<<<1, 128, 0, st>>>(cnt, 4 * (depths + 1), (int)nk);
+        a.sBase = sb;
+        for (int d = 0; d < depths; d++) {
+            a.depth = d;
+#define CWPB_NA(VV, TT) do { if (d == 0) k_trace_shade<VV, TT, true><<<na.gridTrace0, 128, 0, st>>>(a, *p); \
+                             else k_trace_shade<VV, TT, false><<<na.gridTrace, 128, 0, st>>>(a, *p); \
+                             k_shadow<VV, TT><<<na.gridShadow, 128, 0, st>>>(a); } while (0)
+            if (o->variant == 2) { if (o->tri) CWPB_NA(2, 1); else CWPB_NA(2, 0); }
+            else if (o->variant == 4) { if (o->tri) CWPB_NA(4, 1); else CWPB_NA(4, 0); }
+            else { if (o->tri) CWPB_NA(8, 1); else CWPB_NA(8, 0); }
+#undef CWPB_NA
+        }
+        k_pass_end<<<1, 32, 0, st>>>(cnt, depths, tot);
+    }
+    CWPB_CUDA(cudaGetLastError());
+    if (h_rays) {   // optional: wait for the frame and report (closest, shadow) ray totals and the traversal status
+        unsigned long long ht[2 * (kNoAllocMaxBounces + 2)]; int herr = 0;
+        CWPB_CUDA(cudaMemcpyAsync(ht, tot, 2 * (size_t)depths * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        CWPB_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CWPB_CUDA(cudaStreamSynchronize(st));
+        h_rays[0] = h_rays[1] = 0;
+        for (int d = 0; d < depths; d++) { h_rays[0] += (int64_t)ht[2 * d]; h_rays[1] += (int64_t)ht[2 * d + 1]; }
+        CWPB_CHECK(herr == 0, CWP_ERR_TRAVERSAL, "traversal stopped early on some rays (status 0x%x)", herr);
+    }
+    return CWP_OK;
+}

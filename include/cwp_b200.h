@@ -164,6 +164,26 @@ int cwp_renderer_depth_stats(const cwp_renderer* r, int64_t* closest, int64_t* s
 void cwp_renderer_destroy(cwp_renderer* r);
 
 /* ------------------------------------------------------------------------------------------------------------------
+ * Rendering without allocation. No counterpart in the reference. For callers that cannot call cudaMalloc - a plugin
+ * whose host application owns the GPU's memory budget, a serving loop that must not stall on cudaMalloc / cudaFree
+ * (both may synchronise the device), code that must not fail on an allocation mid-frame - this renders the same frame
+ * as cwp_renderer_render into the caller's accumulation buffer, with every scratch buffer in a fixed 31.5 MB device
+ * array inside the library that each GPU loading the library holds until process exit. Limits: w*h*batch <= 262144
+ * paths per pass, bounces <= 62. The scene pointers are device copies of buffers that cwp_bvh_build produced (or that
+ * cwp_accel_create would accept); they are not re-validated here. The first call on a device looks up the array's
+ * device address (do it before any stream capture on that device). All calls share the array: calls whose work
+ * overlaps on the GPU (other streams, other host threads) race and must be serialised by the caller. Launches are
+ * stream-ordered on `stream`; when h_rays is not NULL the call waits for the frame and stores the closest and shadow
+ * ray totals there (and reports traversal errors).
+ * ------------------------------------------------------------------------------------------------------------------ */
+typedef struct cwp_device_scene {
+    const float* nodes; const float* tris; const float* woop; const float* nrm;   /* device pointers; woop / nrm may be NULL */
+    const float* albedo;                                                          /* device, 3 floats per material */
+} cwp_device_scene;
+int cwp_render_noalloc(const cwp_params* p, const cwp_device_scene* s, const cwp_render_options* o, int32_t spp, int32_t s_base,
+                       int32_t clear, float* d_accum, int64_t* h_rays, void* stream);
+
+/* ------------------------------------------------------------------------------------------------------------------
  * Camera and parameter helpers. Replace lookAtC2W / focalFromHfov / makeCamera (scene/camera.cpp:7-23) and the
  * Params filling of setupScene (app/scene_setup.cpp:175-185, Lighting defaults scene/lighting.h:7-13).
  * ------------------------------------------------------------------------------------------------------------------ */
