@@ -205,6 +205,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--spp", type=int, default=0, help="override the frame's samples per pixel (profiling cases)")
     ap.add_argument("--rays", type=int, default=0, help="override the batch size of trace16m (profiling cases)")
+    ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.batch:
@@ -256,7 +257,7 @@ def main():
         w, h, spp, K, B = wl["w"], wl["h"], wl["spp"], wl["batch"], wl["bounces"]
         p = cwp.frame_params(mesh, w, h, bounces=B)
         r = cwp.Renderer()
-        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1)
+        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1, traversal=args.traversal)
         for _ in range(args.warmup):
             r.render(spp)
         depths = B + 2
@@ -295,7 +296,7 @@ def main():
         out.update(metric="closest+shadow rays per second, diffuse frame", value=value, ms_per_step=max_ms / args.steps,
                    config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles, box field seed 1)", "resolution": f"{w}x{h}",
                            "spp": spp, "batch": K, "depth": B, "layout": LAYOUT_NAMES[variant], "sah_bins": args.bins, "tri": "woop",
-                           "graph": args.graph, "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
+                           "graph": args.graph, "traversal": ["auto", "refill", "batch"][args.traversal], "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
                            "rays_per_frame": (rays + shadow) / args.steps, "closest_per_frame": rays / args.steps, "shadow_per_frame": shadow / args.steps,
                            "rays_per_sample": (rays + shadow) / args.steps / (w * h * spp), "trace_shade_ms": float(tms.sum() / args.steps),
                            "shadow_ms": float(sms.sum() / args.steps)},
@@ -311,6 +312,7 @@ def main():
         # ------------------------------------------------------------------ ray batches
         n = wl["rays"]
         acc = cwp.Accel(bvh, tri=1, device=local)
+        acc.set_traversal(args.traversal)
         p = cwp.frame_params(mesh, 512, 512)
         st = torch.cuda.current_stream()
 
@@ -357,7 +359,7 @@ def main():
         achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
         out.update(metric="closest+any rays per second, incoherent ray batch", value=value, ms_per_step=max_ms / args.steps,
                    config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles)", "rays": n, "layout": LAYOUT_NAMES[variant],
-                           "sah_bins": args.bins, "tri": "woop", "l2": f"ray batch {n * 32 / 1e9:.2f} GB > L2 (126 MB)",
+                           "sah_bins": args.bins, "tri": "woop", "traversal": ["auto", "refill", "batch"][args.traversal], "l2": f"ray batch {n * 32 / 1e9:.2f} GB > L2 (126 MB)",
                            "closest_ms": c_ms / args.steps, "any_ms": a_ms / args.steps},
                    clocks=clocks,
                    e2e={"value": 2 * n * args.steps * ws / e_s / 1e9, "unit": "Grays/s", "h2d_bytes_per_step": 2 * 2 * n * 16, "d2h_bytes_per_step": n * 16 + n * 4},

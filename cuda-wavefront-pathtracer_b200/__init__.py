@@ -60,7 +60,8 @@ class Params(C.Structure):
 
 class RenderOptions(C.Structure):
     _fields_ = [("variant", C.c_int32), ("tri", C.c_int32), ("batch", C.c_int32), ("bounces", C.c_int32), ("graph", C.c_int32),
-                ("block", C.c_int32), ("device", C.c_int32), ("profile", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("block", C.c_int32), ("device", C.c_int32), ("profile", C.c_int32), ("traversal", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 class DeviceScene(C.Structure):
@@ -95,6 +96,7 @@ SIGNATURES = {
     "cwp_trace_closest_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_float)]),
     "cwp_trace_any_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_float)]),
     "cwp_accel_status": (C.c_int, [C.c_void_p]),
+    "cwp_accel_set_traversal": (C.c_int, [C.c_void_p, C.c_int32]),
     "cwp_renderer_create": (C.c_int, [C.POINTER(C.c_void_p)]),
     "cwp_renderer_init": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(SceneBuffers), C.POINTER(RenderOptions)]),
     "cwp_renderer_render": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(FrameStats), C.c_int32, C.c_int32]),
@@ -268,6 +270,10 @@ class Accel:
     def status(self):
         _check(lib().cwp_accel_status(self._h))
 
+    def set_traversal(self, mode):
+        """0 auto (persistent refill for BVH2 / CWBVH), 1 refill, 2 one ray per thread"""
+        _check(lib().cwp_accel_set_traversal(self._h, mode))
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             lib().cwp_accel_destroy(self._h); self._h = C.c_void_p()
@@ -303,9 +309,10 @@ class Renderer:
         _check(lib().cwp_renderer_create(C.byref(h)))
         self._h = h
 
-    def init(self, params, bvh, variant, tri=TRI_WOOP, batch=16, bounces=4, graph=1, device=0, profile=0):
+    def init(self, params, bvh, variant, tri=TRI_WOOP, batch=16, bounces=4, graph=1, device=0, profile=0, traversal=0):
         self._params, self._bvh = params, bvh
         o = RenderOptions(); o.variant, o.tri, o.batch, o.bounces, o.graph, o.device, o.profile = variant, tri, batch, bounces, graph, device, profile
+        o.traversal = traversal
         self.depths = bounces + 2
         s = bvh.scene_buffers()
         _check(lib().cwp_renderer_init(self._h, C.byref(params), C.byref(s), C.byref(o)))

@@ -87,14 +87,76 @@ __device__ __forceinline__ void camera_ray(const cwp_params& P, int i, int N, in
 #define CWPB_TRACE_MINB 8   // resident 128-thread blocks per SM the traversal kernels are compiled for
 #endif
 
+// Shading of path k after its closest-hit traversal (wavefront.cu:94-136): miss -> sky; hit at depth <= bounces ->
+// sun next-event estimation (shadow queue) and cosine continuation (next depth's queue). Throughput and path id are
+// read (or, for camera rays, recomputed) here, so that only the ray is live across the traversal. Every lane of the
+// warp must call it (the appends are warp-wide); lanes with valid = false take part without a path.
+template <bool PRIMARY>
+__device__ __forceinline__ void shade_path(const KArgs& a, const cwp_params& P, bool valid, int k, float3 o, float3 d, float t, int tri, float hu, float hv) {
+    int* const c = a.cnt + 4 * a.depth;
+    const int rd = a.depth & 1, wr = rd ^ 1;
+    const unsigned depthRng = (unsigned)a.depth + 1u;
+    float3 T = f3(1.f, 1.f, 1.f); int id = k, pix = 0; unsigned smp = 0;
+    if (valid) {
+        if (!PRIMARY) {
+            id = __float_as_int(__ldg(&a.q.s0[rd][k].w)); const float tr = __ldg(&a.q.s1[rd][k].w); const float2 s2 = __ldcs(a.q.s2[rd] + k);
+            T = f3(tr, s2.x, s2.y);
+        }
+        pix = tile_pixel(id % a.N, P.cam.w, P.cam.h); smp = (unsigned)(a.sBase + id / a.N);
+    }
+    bool wantShadow = false, wantCont = false;
+    float3 po = o, l = d, contrib = T, nd = d;
+    if (valid) {
+        if (tri < 0) accum_add(a.accum, pix, T * v3(P.sky));
+        else if (a.depth <= P.max_b) {
+            const float3 p = o + d * t;
+            const float4 b = __ldg(a.tris + 3 * tri + 1), cc = __ldg(a.tris + 3 * tri + 2);
+            float3 ng = normalize(cross(xyz(b), xyz(cc))), ns = ng;
+            if (P.has_n && a.nrm) {
+                const float3 n0 = xyz(__ldg(a.nrm + 3 * tri)), n1 = xyz(__ldg(a.nrm + 3 * tri + 1)), n2 = xyz(__ldg(a.nrm + 3 * tri + 2));
+                const float3 nn = n0 * (1.f - hu - hv) + n1 * hu + n2 * hv; const float ln = length(nn);
+                if (ln > 0.f) ns = nn * (1.f / ln);
+                if (dot(ns, ng) < 0.f) ns = -ns;
+            }
+            if (dot(ng, d) > 0.f) { ng = -ng; ns = -ns; }
+            const float3 alb = a.albedo[__float_as_int(b.w)];
+            po = p + ng * P.eps;
+            // sun next-event estimation: uniform direction in the sun's cone, Lambert BRDF alb / pi
+            l = cone_dir(v3(P.sun_to), P.sun_cos, rnd(P, pix, smp, depthRng, 2), rnd(P, pix, smp, depthRng, 3));
+            const float cl = dot(ns, l);
+            if (cl > 0.f && dot(ng, l) > 0.f) { contrib = T * alb * v3(P.sun_e) * (cl * CWPB_INV_PI); wantShadow = true; }
+            // continuation: cosine-weighted about the shading normal, throughput *= albedo
+            nd = cosine_dir(ns, rnd(P, pix, smp, depthRng, 0), rnd(P, pix, smp, depthRng, 1));
+            if (dot(nd, ng) > 0.f) { T = T * alb; wantCont = true; }
+        }
+    }
+    const int sp = warp_append(c + 1, wantShadow);
+    if (sp >= 0) {
+        __stcs(a.q.h0 + sp, f4(po, __int_as_float(pix)));
+        __stcs(a.q.h1 + sp, f4(l, contrib.x));
+        __stcs(a.q.h2 + sp, make_float2(contrib.y, contrib.z));
+    }
+    const int cp = warp_append(c + 4, wantCont);
+    if (cp >= 0) {
+        __stcs(a.q.s0[wr] + cp, f4(po, __int_as_float(id)));
+        __stcs(a.q.s1[wr] + cp, f4(nd, T.x));
+        __stcs(a.q.s2[wr] + cp, make_float2(T.y, T.z));
+    }
+}
+
+// the ray of path k at this depth: camera ray (depth 0) or the queued continuation
+template <bool PRIMARY>
+__device__ __forceinline__ void path_ray(const KArgs& a, const cwp_params& P, int k, float3& o, float3& d, float& tmin) {
+    if (PRIMARY) { int pix; unsigned smp; camera_ray(P, k, a.N, a.sBase, o, d, pix, smp); tmin = P.near_clip; }
+    else { const int rd = a.depth & 1; const float4 s0 = __ldcs(a.q.s0[rd] + k), s1 = __ldcs(a.q.s1[rd] + k); o = xyz(s0); d = xyz(s1); tmin = 0.f; }
+}
+
+// one warp fetch of 32 queue entries at a time, each ray traversed to completion, then the 32 shaded together
 template <int V, int TRI, bool PRIMARY>
 __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade(const __grid_constant__ KArgs a, const __grid_constant__ cwp_params P) {
     int* const c = a.cnt + 4 * a.depth;
-    int* const cNext = c + 4;
     const int n = PRIMARY ? a.nk : c[0];
-    const int lane = threadIdx.x & 31, rd = a.depth & 1, wr = rd ^ 1;
-    const unsigned depthRng = (unsigned)a.depth + 1u;
-    const bool canBounce = a.depth <= P.max_b;
+    const int lane = threadIdx.x & 31;
     int err = 0;
     for (;;) {
         int base = 0;
@@ -103,57 +165,90 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade(const __gr
         if (base >= n) break;
         const int k = base + lane;
         const bool valid = k < n;
-        // only the ray is live across the traversal; throughput and path id are read (or recomputed) afterwards
-        float3 o = f3(0.f, 0.f, 0.f), d = f3(0.f, 0.f, 1.f);
-        int pix = 0; unsigned smp = 0; float tmin = 0.f;
-        if (valid) {
-            if (PRIMARY) { camera_ray(P, k, a.N, a.sBase, o, d, pix, smp); tmin = P.near_clip; }
-            else { const float4 s0 = __ldcs(a.q.s0[rd] + k), s1 = __ldcs(a.q.s1[rd] + k); o = xyz(s0); d = xyz(s1); }
-        }
+        float3 o = f3(0.f, 0.f, 0.f), d = f3(0.f, 0.f, 1.f); float tmin = 0.f;
+        if (valid) path_ray<PRIMARY>(a, P, k, o, d, tmin);
         float t = 1e30f, hu = 0.f, hv = 0.f; int tri = -1;
         if (valid) trace_ray<V, false, TRI>(a.nodes, a.tv, o, d, tmin, t, tri, hu, hv, 0, err);
-        float3 T = f3(1.f, 1.f, 1.f); int id = k;
-        if (valid && !PRIMARY) {
-            id = __float_as_int(__ldg(&a.q.s0[rd][k].w)); const float tr = __ldg(&a.q.s1[rd][k].w); const float2 s2 = __ldcs(a.q.s2[rd] + k);
-            T = f3(tr, s2.x, s2.y); pix = tile_pixel(id % a.N, P.cam.w, P.cam.h); smp = (unsigned)(a.sBase + id / a.N);
+        shade_path<PRIMARY>(a, P, valid, k, o, d, t, tri, hu, hv);
+    }
+    if (err) atomicOr(a.err, err);
+}
+
+#ifndef CWPB_REFILL
+#define CWPB_REFILL 12   // a warp refetches rays once this many of its lanes are idle
+#endif
+
+// Persistent traversal with dynamic refill (Aila & Laine 2009): every lane holds one ray's traversal state and
+// advances it one node visit per step; once CWPB_REFILL lanes have finished, the warp shades those paths together,
+// hands their lanes new queue entries with one atomic, and resumes. Lanes stay busy instead of waiting for the slowest
+// ray of a 32-ray batch.
+template <int V, int TRI, bool PRIMARY>
+__global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade_rf(const __grid_constant__ KArgs a, const __grid_constant__ cwp_params P) {
+    int* const c = a.cnt + 4 * a.depth;
+    const int n = PRIMARY ? a.nk : c[0];
+    const int lane = threadIdx.x & 31;
+    int err = 0;
+    TravState<V, false, TRI> ray; typename TravState<V, false, TRI>::Stack stack;
+    int k = -1; bool fin = false, drained = false;
+    for (;;) {
+        if (__any_sync(0xffffffffu, fin)) {
+            shade_path<PRIMARY>(a, P, fin, k, ray.o, ray.d, ray.hitT, ray.hitTri, ray.hu, ray.hv);
+            if (fin) { k = -1; fin = false; }
         }
-        bool wantShadow = false, wantCont = false;
-        float3 po = o, l = d, contrib = T, nd = d;
-        if (valid) {
-            if (tri < 0) accum_add(a.accum, pix, T * v3(P.sky));
-            else if (canBounce) {
-                const float3 p = o + d * t;
-                const float4 b = __ldg(a.tris + 3 * tri + 1), cc = __ldg(a.tris + 3 * tri + 2);
-                float3 ng = normalize(cross(xyz(b), xyz(cc))), ns = ng;
-                if (P.has_n && a.nrm) {
-                    const float3 n0 = xyz(__ldg(a.nrm + 3 * tri)), n1 = xyz(__ldg(a.nrm + 3 * tri + 1)), n2 = xyz(__ldg(a.nrm + 3 * tri + 2));
-                    const float3 nn = n0 * (1.f - hu - hv) + n1 * hu + n2 * hv; const float ln = length(nn);
-                    if (ln > 0.f) ns = nn * (1.f / ln);
-                    if (dot(ns, ng) < 0.f) ns = -ns;
-                }
-                if (dot(ng, d) > 0.f) { ng = -ng; ns = -ns; }
-                const float3 alb = a.albedo[__float_as_int(b.w)];
-                po = p + ng * P.eps;
-                // sun next-event estimation: uniform direction in the sun's cone, Lambert BRDF alb / pi
-                l = cone_dir(v3(P.sun_to), P.sun_cos, rnd(P, pix, smp, depthRng, 2), rnd(P, pix, smp, depthRng, 3));
-                const float cl = dot(ns, l);
-                if (cl > 0.f && dot(ng, l) > 0.f) { contrib = T * alb * v3(P.sun_e) * (cl * CWPB_INV_PI); wantShadow = true; }
-                // continuation: cosine-weighted about the shading normal, throughput *= albedo
-                nd = cosine_dir(ns, rnd(P, pix, smp, depthRng, 0), rnd(P, pix, smp, depthRng, 1));
-                if (dot(nd, ng) > 0.f) { T = T * alb; wantCont = true; }
+        if (!drained) {
+            const bool need = k < 0;
+            const unsigned nm = __ballot_sync(0xffffffffu, need);
+            if (nm) {
+                const int leader = __ffs(nm) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(c + 2, __popc(nm));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                const int kk = base + __popc(nm & lanemask_lt());
+                if (need && kk < n) { k = kk; float3 o, d; float tmin; path_ray<PRIMARY>(a, P, k, o, d, tmin); ray.begin(o, d, tmin, 1e30f, 0); }
+                drained = __any_sync(0xffffffffu, need && kk >= n);   // the queue is empty from here on
             }
         }
-        const int sp = warp_append(c + 1, wantShadow);
-        if (sp >= 0) {
-            __stcs(a.q.h0 + sp, f4(po, __int_as_float(pix)));
-            __stcs(a.q.h1 + sp, f4(l, contrib.x));
-            __stcs(a.q.h2 + sp, make_float2(contrib.y, contrib.z));
+        if (!__any_sync(0xffffffffu, k >= 0)) break;
+        for (;;) {
+            if (k >= 0 && !fin) fin = ray.step(a.nodes, a.tv, stack, err);
+            const unsigned busy = __ballot_sync(0xffffffffu, k >= 0 && !fin);
+            if (!busy || (!drained && 32 - __popc(busy) >= CWPB_REFILL)) break;
         }
-        const int cp = warp_append(cNext, wantCont);
-        if (cp >= 0) {
-            __stcs(a.q.s0[wr] + cp, f4(po, __int_as_float(id)));
-            __stcs(a.q.s1[wr] + cp, f4(nd, T.x));
-            __stcs(a.q.s2[wr] + cp, make_float2(T.y, T.z));
+    }
+    if (err) atomicOr(a.err, err);
+}
+
+template <int V, int TRI>
+__global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow_rf(const __grid_constant__ KArgs a) {
+    int* const c = a.cnt + 4 * a.depth;
+    const int n = c[1];
+    const int lane = threadIdx.x & 31;
+    int err = 0;
+    TravState<V, true, TRI> ray; typename TravState<V, true, TRI>::Stack stack;
+    int k = -1; bool fin = false, drained = false;
+    for (;;) {
+        if (fin) {
+            if (ray.hitTri < 0) { const float4 h0 = __ldg(a.q.h0 + k), h1 = __ldg(a.q.h1 + k); const float2 h2 = __ldcs(a.q.h2 + k); accum_add(a.accum, __float_as_int(h0.w), f3(h1.w, h2.x, h2.y)); }
+            k = -1; fin = false;
+        }
+        if (!drained) {
+            const bool need = k < 0;
+            const unsigned nm = __ballot_sync(0xffffffffu, need);
+            if (nm) {
+                const int leader = __ffs(nm) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(c + 3, __popc(nm));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                const int kk = base + __popc(nm & lanemask_lt());
+                if (need && kk < n) { k = kk; const float4 h0 = __ldg(a.q.h0 + k), h1 = __ldg(a.q.h1 + k); ray.begin(xyz(h0), xyz(h1), 0.f, 1e30f, 0); }
+                drained = __any_sync(0xffffffffu, need && kk >= n);
+            }
+        }
+        if (!__any_sync(0xffffffffu, k >= 0)) break;
+        for (;;) {
+            if (k >= 0 && !fin) fin = ray.step(a.nodes, a.tv, stack, err);
+            const unsigned busy = __ballot_sync(0xffffffffu, k >= 0 && !fin);
+            if (!busy || (!drained && 32 - __popc(busy) >= CWPB_REFILL)) break;
         }
     }
     if (err) atomicOr(a.err, err);
@@ -206,14 +301,22 @@ struct cwp_renderer {
     int* hcnt = nullptr;   // pinned copy of the counters (host loop)
     cudaStream_t st = nullptr; cudaEvent_t f0 = nullptr, f1 = nullptr;
     cudaGraphExec_t gexec = nullptr; int gSpp = -1, gBase = 0;
-    int gridTrace = 0, gridTrace0 = 0, gridShadow = 0, nSM = 0;
+    int gridTrace = 0, gridTrace0 = 0, gridShadow = 0, nSM = 0; bool refill = false;
     std::vector<void*> allocs;
     double vramMB = 0; std::string gpuName;
 };
 
 namespace {
 
-template <int V, int TRI> int occupancy_of(int& bt0, int& bt, int& bs) {
+template <int V, int TRI> int occupancy_of(int& bt0, int& bt, int& bs, bool refill = false) {
+    if constexpr (V != 4) {
+        if (refill) {
+            CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt0, k_trace_shade_rf<V, TRI, true>, 128, 0));
+            CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace_shade_rf<V, TRI, false>, 128, 0));
+            CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shadow_rf<V, TRI>, 128, 0));
+            return CWP_OK;
+        }
+    }
     CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt0, k_trace_shade<V, TRI, true>, 128, 0));
     CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace_shade<V, TRI, false>, 128, 0));
     CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shadow<V, TRI>, 128, 0));
@@ -223,11 +326,22 @@ template <int V, int TRI> int occupancy_of(int& bt0, int& bt, int& bs) {
 // ev: 4 events (trace start/end, shadow start/end) or nullptr
 template <int V, int TRI> void launch_depth(cwp_renderer* r, KArgs a, int gt0, int gt, int gs, cudaEvent_t* ev) {
     // external records: inside a stream capture they become event-record nodes of the graph
+    bool rf = false;
+    if constexpr (V != 4) rf = r->refill;
     if (ev) cudaEventRecordWithFlags(ev[0], r->st, cudaEventRecordExternal);
-    if (a.depth == 0) k_trace_shade<V, TRI, true><<<gt0, 128, 0, r->st>>>(a, r->P);
-    else k_trace_shade<V, TRI, false><<<gt, 128, 0, r->st>>>(a, r->P);
+    if constexpr (V != 4) {
+        if (rf) {
+            if (a.depth == 0) k_trace_shade_rf<V, TRI, true><<<gt0, 128, 0, r->st>>>(a, r->P);
+            else k_trace_shade_rf<V, TRI, false><<<gt, 128, 0, r->st>>>(a, r->P);
+        }
+    }
+    if (!rf) {
+        if (a.depth == 0) k_trace_shade<V, TRI, true><<<gt0, 128, 0, r->st>>>(a, r->P);
+        else k_trace_shade<V, TRI, false><<<gt, 128, 0, r->st>>>(a, r->P);
+    }
     if (ev) { cudaEventRecordWithFlags(ev[1], r->st, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], r->st, cudaEventRecordExternal); }
-    k_shadow<V, TRI><<<gs, 128, 0, r->st>>>(a);
+    if constexpr (V != 4) { if (rf) k_shadow_rf<V, TRI><<<gs, 128, 0, r->st>>>(a); }
+    if (!rf) k_shadow<V, TRI><<<gs, 128, 0, r->st>>>(a);
     if (ev) cudaEventRecordWithFlags(ev[3], r->st, cudaEventRecordExternal);
 }
 
@@ -343,9 +457,12 @@ extern "C" int cwp_renderer_init(cwp_renderer* r, const cwp_params* p, const cwp
     r->gpuName = prop.name; r->nSM = prop.multiProcessorCount;
     int bt0 = 0, bt = 0, bs = 0;
     const int V = r->scene.variant, T = r->scene.tri;
-    if (V == 2) rc = T ? occupancy_of<2, 1>(bt0, bt, bs) : occupancy_of<2, 0>(bt0, bt, bs);
+    CWPB_CHECK(o->traversal >= 0 && o->traversal <= 2, CWP_ERR_INVALID, "traversal %d is not 0, 1 or 2", o->traversal);
+    CWPB_CHECK(!(o->traversal == 1 && V == 4), CWP_ERR_INVALID, "refill traversal is available for BVH2 and CWBVH, not BVH4");
+    r->refill = V != 4 && o->traversal != 2;
+    if (V == 2) rc = T ? occupancy_of<2, 1>(bt0, bt, bs, r->refill) : occupancy_of<2, 0>(bt0, bt, bs, r->refill);
     else if (V == 4) rc = T ? occupancy_of<4, 1>(bt0, bt, bs) : occupancy_of<4, 0>(bt0, bt, bs);
-    else rc = T ? occupancy_of<8, 1>(bt0, bt, bs) : occupancy_of<8, 0>(bt0, bt, bs);
+    else rc = T ? occupancy_of<8, 1>(bt0, bt, bs, r->refill) : occupancy_of<8, 0>(bt0, bt, bs, r->refill);
     if (rc) return rc;
     r->gridTrace0 = bt0 * r->nSM; r->gridTrace = bt * r->nSM; r->gridShadow = bs * r->nSM;
     r->ready = true;

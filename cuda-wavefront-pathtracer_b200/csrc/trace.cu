@@ -115,9 +115,60 @@ __global__ void __launch_bounds__(kBatchBlock) k_trace_any(const float4* __restr
     if (e) atomicOr(err, e);
 }
 
+// Persistent variant with dynamic refill: each lane advances its ray one node visit per step and the warp refetches
+// rays (one atomic on *fetch) once kRefillBatch lanes are idle. *fetch must be zero at launch.
+static constexpr int kRefillBatch = 12;
+__device__ __forceinline__ unsigned lane_lt() { unsigned m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
+
+template <int V, int TRI, bool ANY>
+__global__ void __launch_bounds__(kBatchBlock, 8) k_trace_rf(const float4* __restrict__ nodes, const float4* __restrict__ tv, const float4* __restrict__ ro,
+                                                             const float4* __restrict__ rd, float4* __restrict__ hits, int* __restrict__ occ, long long n, int* fetch, int* err) {
+    const int lane = threadIdx.x & 31;
+    int e = 0;
+    TravState<V, ANY, TRI> ray; typename TravState<V, ANY, TRI>::Stack stack;
+    long long k = -1; bool fin = false, drained = false;
+    for (;;) {
+        if (fin) {
+            if (ANY) __stcs(occ + k, ray.hitTri);
+            else __stcs(hits + k, make_float4(ray.hitT, ray.hu, ray.hv, __int_as_float(ray.hitTri)));
+            k = -1; fin = false;
+        }
+        if (!drained) {
+            const bool need = k < 0;
+            const unsigned nm = __ballot_sync(0xffffffffu, need);
+            if (nm) {
+                const int leader = __ffs(nm) - 1;
+                long long base = 0;
+                if (lane == leader) base = atomicAdd((unsigned long long*)fetch, (unsigned long long)__popc(nm));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                const long long kk = base + __popc(nm & lane_lt());
+                if (need && kk < n) { k = kk; const float4 O = __ldcs(ro + k), D = __ldcs(rd + k); ray.begin(xyz(O), xyz(D), O.w, D.w, 0); }
+                drained = __any_sync(0xffffffffu, need && kk >= n);
+            }
+        }
+        if (!__any_sync(0xffffffffu, k >= 0)) break;
+        for (;;) {
+            if (k >= 0 && !fin) fin = ray.step(nodes, tv, stack, e);
+            const unsigned busy = __ballot_sync(0xffffffffu, k >= 0 && !fin);
+            if (!busy || (!drained && 32 - __popc(busy) >= kRefillBatch)) break;
+        }
+    }
+    if (e) atomicOr(err, e);
+}
+
 template <bool ANY>
-static int launch_batch(const DeviceScene& s, const float4* o, const float4* d, void* out, long long n, int* err, cudaStream_t st) {
+static int launch_batch(const DeviceScene& s, const float4* o, const float4* d, void* out, long long n, int* err, cudaStream_t st, int* fetch, int refillGrid) {
     if (n <= 0) return CWP_OK;
+    const float4* tv0 = s.leafData();
+    if (fetch && s.variant != 4) {   // persistent refill kernels (BVH2, CWBVH)
+        CWPB_CUDA(cudaMemsetAsync(fetch, 0, sizeof(unsigned long long), st));
+#define CWPB_R(VV, TT) k_trace_rf<VV, TT, ANY><<<refillGrid, kBatchBlock, 0, st>>>(s.nodes, tv0, o, d, (float4*)out, (int*)out, n, fetch, err)
+        if (s.variant == 2) { if (s.tri) CWPB_R(2, 1); else CWPB_R(2, 0); }
+        else { if (s.tri) CWPB_R(8, 1); else CWPB_R(8, 0); }
+#undef CWPB_R
+        CWPB_CUDA(cudaGetLastError());
+        return CWP_OK;
+    }
     const unsigned grid = (unsigned)((n + kBatchBlock - 1) / kBatchBlock);
     const float4* tv = s.leafData();
 #define CWPB_L(VV, TT) do { if (ANY) k_trace_any<VV, TT><<<grid, kBatchBlock, 0, st>>>(s.nodes, tv, o, d, (int*)out, n, err); \
@@ -137,6 +188,9 @@ using namespace cwpb;
 struct cwp_accel {
     DeviceScene scene;
     int* err = nullptr;                 // device traversal status bits
+    int* fetch = nullptr;               // refill kernels' ray cursor (8 bytes)
+    int refillGrid = 0;                 // resident blocks of the refill kernels
+    bool refill = true;                 // use them (cwp_accel_set_traversal)
     cudaStream_t st = nullptr;          // stream of the host-buffer entry points
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     float4 *bo = nullptr, *bd = nullptr; void* bh = nullptr; size_t cap = 0;   // staging for host-buffer calls
@@ -150,6 +204,15 @@ extern "C" int cwp_accel_create(const cwp_scene_buffers* s, int32_t tri, int32_t
     if (rc) { delete a; return rc; }
     cudaError_t e = cudaMalloc(&a->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(a->err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&a->fetch, sizeof(unsigned long long));
+    if (e == cudaSuccess && a->scene.variant != 4) {
+        int nSM = 0, b = 0;
+        e = cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, device);
+        const bool t = a->scene.tri == 1;
+        if (e == cudaSuccess) e = a->scene.variant == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, t ? k_trace_rf<2, 1, false> : k_trace_rf<2, 0, false>, kBatchBlock, 0)
+                                                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, t ? k_trace_rf<8, 1, false> : k_trace_rf<8, 0, false>, kBatchBlock, 0);
+        a->refillGrid = b * nSM;
+    }
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&a->st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&a->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&a->e1);
@@ -162,7 +225,7 @@ extern "C" void cwp_accel_destroy(cwp_accel* a) {
     if (!a) return;
     cudaSetDevice(a->scene.device);
     if (a->st) cudaStreamSynchronize(a->st);
-    cudaFree(a->err); cudaFree(a->bo); cudaFree(a->bd); cudaFree(a->bh);
+    cudaFree(a->err); cudaFree(a->fetch); cudaFree(a->bo); cudaFree(a->bd); cudaFree(a->bh);
     if (a->st) cudaStreamDestroy(a->st);
     if (a->e0) cudaEventDestroy(a->e0);
     if (a->e1) cudaEventDestroy(a->e1);
@@ -175,7 +238,7 @@ extern "C" int cwp_trace_closest(cwp_accel* a, const float* o, const float* d, f
     CWPB_CHECK(n >= 0, CWP_ERR_INVALID, "negative ray count");
     CWPB_CHECK(n == 0 || (o && d && hits), CWP_ERR_INVALID, "NULL ray or hit buffer");
     CWPB_CUDA(cudaSetDevice(a->scene.device));
-    return launch_batch<false>(a->scene, (const float4*)o, (const float4*)d, hits, n, a->err, (cudaStream_t)stream);
+    return launch_batch<false>(a->scene, (const float4*)o, (const float4*)d, hits, n, a->err, (cudaStream_t)stream, a->refill ? a->fetch : nullptr, a->refillGrid);
 }
 
 extern "C" int cwp_trace_any(cwp_accel* a, const float* o, const float* d, int32_t* occ, int64_t n, void* stream) {
@@ -183,7 +246,7 @@ extern "C" int cwp_trace_any(cwp_accel* a, const float* o, const float* d, int32
     CWPB_CHECK(n >= 0, CWP_ERR_INVALID, "negative ray count");
     CWPB_CHECK(n == 0 || (o && d && occ), CWP_ERR_INVALID, "NULL ray or result buffer");
     CWPB_CUDA(cudaSetDevice(a->scene.device));
-    return launch_batch<true>(a->scene, (const float4*)o, (const float4*)d, occ, n, a->err, (cudaStream_t)stream);
+    return launch_batch<true>(a->scene, (const float4*)o, (const float4*)d, occ, n, a->err, (cudaStream_t)stream, a->refill ? a->fetch : nullptr, a->refillGrid);
 }
 
 template <bool ANY>
@@ -203,7 +266,7 @@ static int host_call(cwp_accel* a, const float* o, const float* d, void* res, in
     CWPB_CUDA(cudaEventRecord(a->e0, a->st));
     CWPB_CUDA(cudaMemcpyAsync(a->bo, o, (size_t)n * 16, cudaMemcpyHostToDevice, a->st));
     CWPB_CUDA(cudaMemcpyAsync(a->bd, d, (size_t)n * 16, cudaMemcpyHostToDevice, a->st));
-    if (int rc = launch_batch<ANY>(a->scene, a->bo, a->bd, a->bh, n, a->err, a->st)) return rc;
+    if (int rc = launch_batch<ANY>(a->scene, a->bo, a->bd, a->bh, n, a->err, a->st, a->refill ? a->fetch : nullptr, a->refillGrid)) return rc;
     CWPB_CUDA(cudaMemcpyAsync(res, a->bh, (size_t)n * resBytes, cudaMemcpyDeviceToHost, a->st));
     CWPB_CUDA(cudaEventRecord(a->e1, a->st));
     CWPB_CUDA(cudaEventSynchronize(a->e1));
@@ -213,6 +276,14 @@ static int host_call(cwp_accel* a, const float* o, const float* d, void* res, in
 
 extern "C" int cwp_trace_closest_host(cwp_accel* a, const float* o, const float* d, float* hits, int64_t n, float* ms) { return host_call<false>(a, o, d, hits, n, ms); }
 extern "C" int cwp_trace_any_host(cwp_accel* a, const float* o, const float* d, int32_t* occ, int64_t n, float* ms) { return host_call<true>(a, o, d, occ, n, ms); }
+
+extern "C" int cwp_accel_set_traversal(cwp_accel* a, int32_t mode) {
+    CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
+    CWPB_CHECK(mode >= 0 && mode <= 2, CWP_ERR_INVALID, "traversal %d is not 0, 1 or 2", mode);
+    CWPB_CHECK(!(mode == 1 && a->scene.variant == 4), CWP_ERR_INVALID, "refill traversal is available for BVH2 and CWBVH, not BVH4");
+    a->refill = mode != 2 && a->scene.variant != 4;
+    return CWP_OK;
+}
 
 extern "C" int cwp_accel_status(cwp_accel* a) {
     CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");

@@ -64,34 +64,55 @@ __device__ __forceinline__ bool leaf_hit(const float4* __restrict__ tv, int firs
     return false;
 }
 
+// ---------------- resumable traversal state ----------------
+// TravState<V, ANY, TRI>: one ray's traversal, advanced one node visit at a time. begin() sets the ray up; step()
+// visits the current node (its slab tests and hit leaves) and picks the next node, returning true when the ray is
+// done (traversal exhausted, an any-hit found, or a bound exceeded). Running step() to completion is the plain
+// while-while traversal; persistent kernels interleave the steps of many rays (render.cu, trace.cu). The traversal
+// stack is the caller's array (TravState<V>::Stack), kept out of the struct so that its scalars stay in registers.
+template <int V, bool ANY, int TRI> struct TravState;
+
 // ---------------- BVH2 ----------------
 template <bool ANY, int TRI>
-__device__ __forceinline__ bool trav_bvh2(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
-                                          float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
-    int stack[kStack2]; int sp = 0, node = root, budget = kVisitBudget;
-    const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z);
-    const float ox = -o.x * idx, oy = -o.y * idy, oz = -o.z * idz;
-    while (true) {
-        if (--budget < 0) { err |= kTravBudget; break; }
+struct TravState<2, ANY, TRI> {
+    typedef int Stack[kStack2];
+    float3 o, d; float idx, idy, idz, ox, oy, oz, tmin, hitT, hu, hv; int hitTri, node, sp, budget;
+
+    __device__ __forceinline__ void begin(float3 o_, float3 d_, float tmin_, float tmax_, int root) {
+        o = o_; d = d_; tmin = tmin_; hitT = tmax_; hu = hv = 0.f; hitTri = -1; node = root; sp = 0; budget = kVisitBudget;
+        idx = safe_rcp(d.x); idy = safe_rcp(d.y); idz = safe_rcp(d.z);
+        ox = -o.x * idx; oy = -o.y * idy; oz = -o.z * idz;
+    }
+    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ tv, Stack& stack, int& err) {
+        if (--budget < 0) { err |= kTravBudget; return true; }
         const float4* nb = nodes + 4 * (size_t)node;
         const float4 n0 = ld4(nb), n1 = ld4(nb + 1), nz = ld4(nb + 2), mt = ld4(nb + 3);
-        int c0 = __float_as_int(mt.x), c1 = __float_as_int(mt.y), k0 = __float_as_int(mt.z), k1 = __float_as_int(mt.w);
-        float a0 = fmaf(n0.x, idx, ox), a1 = fmaf(n0.y, idx, ox), a2 = fmaf(n0.z, idy, oy), a3 = fmaf(n0.w, idy, oy), a4 = fmaf(nz.x, idz, oz), a5 = fmaf(nz.y, idz, oz);
-        float b0 = fmaf(n1.x, idx, ox), b1 = fmaf(n1.y, idx, ox), b2 = fmaf(n1.z, idy, oy), b3 = fmaf(n1.w, idy, oy), b4 = fmaf(nz.z, idz, oz), b5 = fmaf(nz.w, idz, oz);
-        float t0n = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
-        float t0f = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), hitT));
-        float t1n = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
-        float t1f = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), hitT));
+        int c0 = __float_as_int(mt.x), c1 = __float_as_int(mt.y); const int k0 = __float_as_int(mt.z), k1 = __float_as_int(mt.w);
+        const float a0 = fmaf(n0.x, idx, ox), a1 = fmaf(n0.y, idx, ox), a2 = fmaf(n0.z, idy, oy), a3 = fmaf(n0.w, idy, oy), a4 = fmaf(nz.x, idz, oz), a5 = fmaf(nz.y, idz, oz);
+        const float b0 = fmaf(n1.x, idx, ox), b1 = fmaf(n1.y, idx, ox), b2 = fmaf(n1.z, idy, oy), b3 = fmaf(n1.w, idy, oy), b4 = fmaf(nz.z, idz, oz), b5 = fmaf(nz.w, idz, oz);
+        const float t0n = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
+        const float t0f = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), hitT));
+        const float t1n = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
+        const float t1f = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), hitT));
         bool h0 = t0n <= t0f, h1 = t1n <= t1f;
         if (h0 && k0 > 0) { if (leaf_hit<ANY, TRI>(tv, c0, k0, o, d, tmin, hitT, hitTri, hu, hv) && ANY) return true; h0 = false; }
         if (h1 && k1 > 0) { if (leaf_hit<ANY, TRI>(tv, c1, k1, o, d, tmin, hitT, hitTri, hu, hv) && ANY) return true; h1 = false; }
-        if (!h0 && !h1) { if (sp == 0) break; node = stack[--sp]; }
+        if (!h0 && !h1) { if (sp == 0) return true; node = stack[--sp]; }
         else if (h0 && h1) {
-            if (t1n < t0n) { int t = c0; c0 = c1; c1 = t; }
-            if (sp == kStack2) { err |= kTravOverflow; break; }
+            if (t1n < t0n) { const int t = c0; c0 = c1; c1 = t; }
+            if (sp == kStack2) { err |= kTravOverflow; return true; }
             stack[sp++] = c1; node = c0;
         } else node = h0 ? c0 : c1;
+        return false;
     }
+};
+
+template <bool ANY, int TRI>
+__device__ __forceinline__ bool trav_bvh2(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
+                                          float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
+    TravState<2, ANY, TRI> r; typename TravState<2, ANY, TRI>::Stack stack; r.begin(o, d, tmin, hitT, root);
+    while (!r.step(nodes, tv, stack, err)) {}
+    hitT = r.hitT; hitTri = r.hitTri; hu = r.hu; hv = r.hv;
     return hitTri >= 0;
 }
 
@@ -146,18 +167,18 @@ __device__ __forceinline__ float qbyte(unsigned w, int s) {
 }
 
 template <bool ANY, int TRI>
-__device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
-                                           float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
-    uint2 stack[kStack8]; int sp = 0, budget = kVisitBudget;
-    const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z);
-    const unsigned oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
-    // per axis, the plane a ray enters first: the low bound when the reciprocal is positive, else the high bound.
-    // Selecting it replaces the min/max of each (low, high) pair and gives the same values: the fused affine map
-    // q * s + o is monotonic in q for either sign of s.
-    const bool fx = idx < 0.f, fy = idy < 0.f, fz = idz < 0.f;
-    unsigned cb = 0, im = 0, hm = 0; int node = root;
-    while (true) {
-        if (--budget < 0) { err |= kTravBudget; return hitTri >= 0; }
+struct TravState<8, ANY, TRI> {
+    typedef uint2 Stack[kStack8];
+    float3 o, d; float idx, idy, idz, tmin, hitT, hu, hv; int hitTri, node, sp, budget; unsigned oct, cb, im, hm;
+
+    __device__ __forceinline__ void begin(float3 o_, float3 d_, float tmin_, float tmax_, int root) {
+        o = o_; d = d_; tmin = tmin_; hitT = tmax_; hu = hv = 0.f; hitTri = -1; node = root; sp = 0; budget = kVisitBudget;
+        idx = safe_rcp(d.x); idy = safe_rcp(d.y); idz = safe_rcp(d.z);
+        oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
+        cb = im = hm = 0;
+    }
+    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ tv, Stack& stack, int& err) {
+        if (--budget < 0) { err |= kTravBudget; return true; }
         const float4* nb = nodes + 5 * (size_t)node;
         const float4 f0 = ld4(nb), f1 = ld4(nb + 1), f2 = ld4(nb + 2), f3_ = ld4(nb + 3), f4_ = ld4(nb + 4);
         const unsigned ew = __float_as_uint(f0.w);
@@ -165,6 +186,10 @@ __device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, con
         const float ox = (f0.x - o.x) * idx, oy = (f0.y - o.y) * idy, oz = (f0.z - o.z) * idz;
         const unsigned imask = ew >> 24, m0 = __float_as_uint(f1.z), m1 = __float_as_uint(f1.w);
         const int childBase = __float_as_int(f1.x), triBase = __float_as_int(f1.y);
+        // per axis, the plane a ray enters first: the low bound when the reciprocal is positive, else the high bound.
+        // Selecting it replaces the min/max of each (low, high) pair and gives the same values: the fused affine map
+        // q * s + o is monotonic in q for either sign of s.
+        const bool fx = idx < 0.f, fy = idy < 0.f, fz = idz < 0.f;
         // quantised bounds: lo x (f2.x, f2.y), lo y (f2.z, f2.w), lo z (f3.x, f3.y), hi x (f3.z, f3.w), hi y (f4.x, f4.y), hi z (f4.z, f4.w)
         const unsigned nx0 = __float_as_uint(fx ? f3_.z : f2.x), nx1 = __float_as_uint(fx ? f3_.w : f2.y), px0 = __float_as_uint(fx ? f2.x : f3_.z), px1 = __float_as_uint(fx ? f2.y : f3_.w);
         const unsigned ny0 = __float_as_uint(fy ? f4_.x : f2.z), ny1 = __float_as_uint(fy ? f4_.y : f2.w), py0 = __float_as_uint(fy ? f2.z : f4_.x), py1 = __float_as_uint(fy ? f2.w : f4_.y);
@@ -176,8 +201,12 @@ __device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, con
             const float xn = fmaf(qbyte(s < 4 ? nx0 : nx1, s), sx, ox), xf = fmaf(qbyte(s < 4 ? px0 : px1, s), sx, ox);
             const float yn = fmaf(qbyte(s < 4 ? ny0 : ny1, s), sy, oy), yf = fmaf(qbyte(s < 4 ? py0 : py1, s), sy, oy);
             const float zn = fmaf(qbyte(s < 4 ? nz0 : nz1, s), sz, oz), zf = fmaf(qbyte(s < 4 ? pz0 : pz1, s), sz, oz);
-            const float tn = fmaxf(fmaxf(xn, yn), fmaxf(zn, tmin));
-            const float tf = fminf(fminf(xf, yf), fminf(zf, hitT));
+            // entry = max(xn, yn, zn, tmin), exit = min(xf, yf, zf, hitT) selected with 3-input integer min/max on the
+            // float bits: for values >= +0 the integer order is the float order, entry >= tmin >= +0, and any negative
+            // candidate for the exit makes the float comparison below fail whichever negative value is picked - so
+            // the hit decision is the one the float min/max gives.
+            const float tn = __int_as_float(__vimax3_s32(__float_as_int(xn), __float_as_int(yn), max(__float_as_int(zn), __float_as_int(tmin))));
+            const float tf = __int_as_float(__vimin3_s32(__float_as_int(xf), __float_as_int(yf), min(__float_as_int(zf), __float_as_int(hitT))));
             boxHit |= (tn <= tf ? 1u : 0u) << s;
         }
         // leaf slots: meta bit 7 of each byte
@@ -195,13 +224,23 @@ __device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, con
             if (leaf_hit<ANY, TRI>(tv, triBase + (int)(m & 31u), (int)((m >> 5) & 3u) + 1, o, d, tmin, hitT, hitTri, hu, hv) && ANY) return true;
         }
         if (hits) {
-            if (hm) { if (sp == kStack8) { err |= kTravOverflow; return hitTri >= 0; } stack[sp++] = make_uint2(cb, (im << 8) | hm); }
+            if (hm) { if (sp == kStack8) { err |= kTravOverflow; return true; } stack[sp++] = make_uint2(cb, (im << 8) | hm); }
             cb = (unsigned)childBase; im = imask; hm = hits;
         }
-        while (hm == 0) { if (sp == 0) return hitTri >= 0; uint2 e = stack[--sp]; cb = e.x; im = e.y >> 8; hm = e.y & 255u; }
+        while (hm == 0) { if (sp == 0) return true; const uint2 e = stack[--sp]; cb = e.x; im = e.y >> 8; hm = e.y & 255u; }
         const unsigned k = __ffs(hm) - 1; hm &= hm - 1; const unsigned slot = k ^ oct;
         node = (int)cb + __popc(im & ((1u << slot) - 1u));
+        return false;
     }
+};
+
+template <bool ANY, int TRI>
+__device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
+                                           float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
+    TravState<8, ANY, TRI> r; typename TravState<8, ANY, TRI>::Stack stack; r.begin(o, d, tmin, hitT, root);
+    while (!r.step(nodes, tv, stack, err)) {}
+    hitT = r.hitT; hitTri = r.hitTri; hu = r.hu; hv = r.hv;
+    return hitTri >= 0;
 }
 
 template <int V, bool ANY, int TRI>
