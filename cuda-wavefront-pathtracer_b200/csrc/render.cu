@@ -301,7 +301,7 @@ struct cwp_renderer {
     int* hcnt = nullptr;   // pinned copy of the counters (host loop)
     cudaStream_t st = nullptr; cudaEvent_t f0 = nullptr, f1 = nullptr;
     cudaGraphExec_t gexec = nullptr; int gSpp = -1, gBase = 0;
-    int gridTrace = 0, gridTrace0 = 0, gridShadow = 0, nSM = 0; bool refill = false;
+    int gridTrace = 0, gridTrace0 = 0, gridShadow = 0, nSM = 0; bool refill = false, refillShadow = false;
     std::vector<void*> allocs;
     double vramMB = 0; std::string gpuName;
 };
@@ -326,8 +326,8 @@ template <int V, int TRI> int occupancy_of(int& bt0, int& bt, int& bs, bool refi
 // ev: 4 events (trace start/end, shadow start/end) or nullptr
 template <int V, int TRI> void launch_depth(cwp_renderer* r, KArgs a, int gt0, int gt, int gs, cudaEvent_t* ev) {
     // external records: inside a stream capture they become event-record nodes of the graph
-    bool rf = false;
-    if constexpr (V != 4) rf = r->refill;
+    bool rf = false, rfShadow = false;
+    if constexpr (V != 4) { rf = r->refill; rfShadow = r->refillShadow; }
     if (ev) cudaEventRecordWithFlags(ev[0], r->st, cudaEventRecordExternal);
     if constexpr (V != 4) {
         if (rf) {
@@ -340,8 +340,8 @@ template <int V, int TRI> void launch_depth(cwp_renderer* r, KArgs a, int gt0, i
         else k_trace_shade<V, TRI, false><<<gt, 128, 0, r->st>>>(a, r->P);
     }
     if (ev) { cudaEventRecordWithFlags(ev[1], r->st, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], r->st, cudaEventRecordExternal); }
-    if constexpr (V != 4) { if (rf) k_shadow_rf<V, TRI><<<gs, 128, 0, r->st>>>(a); }
-    if (!rf) k_shadow<V, TRI><<<gs, 128, 0, r->st>>>(a);
+    if constexpr (V != 4) { if (rfShadow) k_shadow_rf<V, TRI><<<gs, 128, 0, r->st>>>(a); }
+    if (!rfShadow) k_shadow<V, TRI><<<gs, 128, 0, r->st>>>(a);
     if (ev) cudaEventRecordWithFlags(ev[3], r->st, cudaEventRecordExternal);
 }
 
@@ -459,10 +459,20 @@ extern "C" int cwp_renderer_init(cwp_renderer* r, const cwp_params* p, const cwp
     const int V = r->scene.variant, T = r->scene.tri;
     CWPB_CHECK(o->traversal >= 0 && o->traversal <= 2, CWP_ERR_INVALID, "traversal %d is not 0, 1 or 2", o->traversal);
     CWPB_CHECK(!(o->traversal == 1 && V == 4), CWP_ERR_INVALID, "refill traversal is available for BVH2 and CWBVH, not BVH4");
-    r->refill = V != 4 && o->traversal != 2;
-    if (V == 2) rc = T ? occupancy_of<2, 1>(bt0, bt, bs, r->refill) : occupancy_of<2, 0>(bt0, bt, bs, r->refill);
-    else if (V == 4) rc = T ? occupancy_of<4, 1>(bt0, bt, bs) : occupancy_of<4, 0>(bt0, bt, bs);
-    else rc = T ? occupancy_of<8, 1>(bt0, bt, bs, r->refill) : occupancy_of<8, 0>(bt0, bt, bs, r->refill);
+    // auto (measured on B200, 117k-triangle box field): refill pays for CWBVH closest-hit traversal; the shadow pass
+    // (coherent rays towards the sun) and BVH2 (bound by dependent node-fetch latency) run faster per 32-ray batch
+    r->refill = o->traversal == 1 || (o->traversal == 0 && V == 8);
+    r->refillShadow = o->traversal == 1;
+    int b0 = 0, b1 = 0;
+    if (V == 2) rc = T ? occupancy_of<2, 1>(bt0, bt, b0, r->refill) : occupancy_of<2, 0>(bt0, bt, b0, r->refill);
+    else if (V == 4) rc = T ? occupancy_of<4, 1>(bt0, bt, b0) : occupancy_of<4, 0>(bt0, bt, b0);
+    else rc = T ? occupancy_of<8, 1>(bt0, bt, b0, r->refill) : occupancy_of<8, 0>(bt0, bt, b0, r->refill);
+    if (rc) return rc;
+    int d0 = 0, d1 = 0;   // shadow grid from the shadow kernel actually used
+    if (V == 2) rc = T ? occupancy_of<2, 1>(d0, d1, bs, r->refillShadow) : occupancy_of<2, 0>(d0, d1, bs, r->refillShadow);
+    else if (V == 4) rc = T ? occupancy_of<4, 1>(d0, d1, bs) : occupancy_of<4, 0>(d0, d1, bs);
+    else rc = T ? occupancy_of<8, 1>(d0, d1, bs, r->refillShadow) : occupancy_of<8, 0>(d0, d1, bs, r->refillShadow);
+    (void)b1;
     if (rc) return rc;
     r->gridTrace0 = bt0 * r->nSM; r->gridTrace = bt * r->nSM; r->gridShadow = bs * r->nSM;
     r->ready = true;

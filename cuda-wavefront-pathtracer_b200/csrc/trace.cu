@@ -190,7 +190,7 @@ struct cwp_accel {
     int* err = nullptr;                 // device traversal status bits
     int* fetch = nullptr;               // refill kernels' ray cursor (8 bytes)
     int refillGrid = 0;                 // resident blocks of the refill kernels
-    bool refill = true;                 // use them (cwp_accel_set_traversal)
+    bool refill = true;                 // use them (cwp_accel_set_traversal; set at creation by the automatic rule)
     cudaStream_t st = nullptr;          // stream of the host-buffer entry points
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     float4 *bo = nullptr, *bd = nullptr; void* bh = nullptr; size_t cap = 0;   // staging for host-buffer calls
@@ -217,6 +217,7 @@ extern "C" int cwp_accel_create(const cwp_scene_buffers* s, int32_t tri, int32_t
     if (e == cudaSuccess) e = cudaEventCreate(&a->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&a->e1);
     if (e != cudaSuccess) { cwp_accel_destroy(a); return set_error(CWP_ERR_CUDA, "accel setup: %s", cudaGetErrorString(e)); }
+    a->refill = a->scene.variant == 8;
     *out = a;
     return CWP_OK;
 }
@@ -281,7 +282,8 @@ extern "C" int cwp_accel_set_traversal(cwp_accel* a, int32_t mode) {
     CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
     CWPB_CHECK(mode >= 0 && mode <= 2, CWP_ERR_INVALID, "traversal %d is not 0, 1 or 2", mode);
     CWPB_CHECK(!(mode == 1 && a->scene.variant == 4), CWP_ERR_INVALID, "refill traversal is available for BVH2 and CWBVH, not BVH4");
-    a->refill = mode != 2 && a->scene.variant != 4;
+    // auto: refill for CWBVH (measured faster on incoherent batches), one ray per thread for BVH2 and BVH4
+    a->refill = mode == 1 || (mode == 0 && a->scene.variant == 8);
     return CWP_OK;
 }
 

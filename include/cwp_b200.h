@@ -108,7 +108,7 @@ int cwp_trace_closest_host(cwp_accel* a, const float* o, const float* d, float* 
 int cwp_trace_any_host(cwp_accel* a, const float* o, const float* d, int32_t* occluder, int64_t n, float* ms);
 /* traversal status of the calls since the last query (CWP_OK or CWP_ERR_TRAVERSAL); clears it */
 int cwp_accel_status(cwp_accel* a);
-/* kernel form of the batch calls: 0 auto (persistent refill for BVH2 / CWBVH), 1 refill, 2 one ray per thread */
+/* kernel form of the batch calls: 0 auto (persistent refill for CWBVH), 1 refill (BVH2 / CWBVH), 2 one ray per thread */
 int cwp_accel_set_traversal(cwp_accel* a, int32_t mode);
 
 /* ------------------------------------------------------------------------------------------------------------------
@@ -143,7 +143,7 @@ typedef struct cwp_render_options {
     int32_t block;        /* threads per block of the traversal kernels (0 = 128) */
     int32_t device;       /* CUDA device ordinal */
     int32_t profile;      /* 1: CUDA event pair around every kernel launch (also inside the graph), see cwp_renderer_depth_stats */
-    int32_t traversal;    /* 0 auto (refill for BVH2 / CWBVH), 1 persistent lanes with dynamic refill, 2 one 32-ray fetch per warp */
+    int32_t traversal;    /* 0 auto (refill for CWBVH closest-hit), 1 persistent lanes with dynamic refill everywhere, 2 one 32-ray fetch per warp */
     int32_t reserved[3];
 } cwp_render_options;
 
