@@ -6,6 +6,8 @@ Workloads (synthetic box-field scenes standing in for the reference's unreleased
   frame720  the same at 1280 x 720
   frame256  12,290 triangles, 256 x 256, 16 spp, depth 4, batch 16
   trace16m  117,002 triangles, 2^24 incoherent rays traced closest-hit and any-hit
+  precision1m  12,290 triangles, 2^20 incoherent rays, precision form (f16 conservative slabs + watertight FP32
+            triangles) closest + any, checked against the FP64 oracle (lost hits, ties, max relative t error)
 A step is one frame (frame*) or one closest + one any-hit pass over the batch (trace16m). `value` counts the rays of
 all ranks over the max over ranks of the device-timed steps (CUDA events on the renderer's stream). `e2e` is the same
 metric through the C ABI with host buffers: each frame's accumulation buffer (trace16m: rays in, hits out) crosses
@@ -32,6 +34,7 @@ WORKLOADS = {
     "frame720": dict(scene="boxes117k", w=1280, h=720, spp=256, batch=256, bounces=4),
     "frame256": dict(scene="boxes12k", w=256, h=256, spp=16, batch=16, bounces=4),
     "trace16m": dict(scene="boxes117k", rays=1 << 24),
+    "precision1m": dict(scene="boxes12k", rays=1 << 20, precision=True),
 }
 STATE_BYTES = 40          # path state per queued ray: (o, id) + (d, T.r) + (T.g, T.b); shadow entries the same size
 LAYOUT_NAMES = {2: "bvh2", 4: "bvh4", 8: "cwbvh"}
@@ -205,6 +208,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--spp", type=int, default=0, help="override the frame's samples per pixel (profiling cases)")
     ap.add_argument("--rays", type=int, default=0, help="override the batch size of trace16m (profiling cases)")
+    ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
@@ -214,6 +218,8 @@ def main():
         wl["spp"] = args.spp
     if args.rays and "rays" in wl:
         wl["rays"] = args.rays
+    if args.precision and "rays" in wl:
+        wl["precision"] = True
     ws, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, wl, rank)
@@ -325,6 +331,18 @@ def main():
         o, d = cwp.incoherent_rays(n, p, bvh.tris, tr, seed=41)
         do, dd = torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()
         hits = torch.empty((n, 4), dtype=torch.float32, device="cuda"); occ = torch.empty(n, dtype=torch.int32, device="cuda")
+        plain = None
+        if wl.get("precision"):
+            # the plain form on the same batch (the "vs plain" figure), then switch to the precision form
+            for _ in range(2):
+                acc.trace_closest(do.data_ptr(), dd.data_ptr(), hits.data_ptr(), n, st.cuda_stream); acc.trace_any(do.data_ptr(), dd.data_ptr(), occ.data_ptr(), n, st.cuda_stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(args.steps):
+                acc.trace_closest(do.data_ptr(), dd.data_ptr(), hits.data_ptr(), n, st.cuda_stream); acc.trace_any(do.data_ptr(), dd.data_ptr(), occ.data_ptr(), n, st.cuda_stream)
+            e1.record(st); torch.cuda.synchronize()
+            plain = 2 * n * args.steps / (e0.elapsed_time(e1) * 1e-3) / 1e9
+            acc.set_precision(1)
         for _ in range(args.warmup):
             acc.trace_closest(do.data_ptr(), dd.data_ptr(), hits.data_ptr(), n, st.cuda_stream)
             acc.trace_any(do.data_ptr(), dd.data_ptr(), occ.data_ptr(), n, st.cuda_stream)
@@ -356,9 +374,23 @@ def main():
             cwp._check(cwp.lib().cwp_trace_any_host(acc._h, ho.data_ptr(), hd.data_ptr(), hoc.data_ptr(), n, None))
         barrier(); e_s = reduce(time.perf_counter() - t0, tdist.ReduceOp.MAX if ws > 1 else None)
         dom_ms, dom_b, dom = (c_ms, 48.0, "k_trace_closest") if c_ms >= a_ms else (a_ms, 36.0, "k_trace_any")
+        check = {}
+        if wl.get("precision"):
+            # FP64 oracle on the same batch: lost hits (must be 0), ties, max relative t error of the closest hits
+            acc.trace_closest(do.data_ptr(), dd.data_ptr(), hits.data_ptr(), n, st.cuda_stream)
+            t64 = torch.empty(n, dtype=torch.float64, device="cuda"); i64 = torch.empty(n, dtype=torch.int32, device="cuda")
+            acc.trace_fp64(do.data_ptr(), dd.data_ptr(), t64.data_ptr(), i64.data_ptr(), n, stream=st.cuda_stream)
+            torch.cuda.synchronize()
+            h = hits.cpu().numpy(); t64n = t64.cpu().numpy(); i64n = i64.cpu().numpy(); ih = h[:, 3].view(np.int32)
+            rel = np.abs(h[:, 0].astype(np.float64) - t64n) / np.maximum(t64n, 1e-30)
+            both = (i64n >= 0) & (ih >= 0); same = both & (ih == i64n)
+            check = {"fp64_rays": n, "lost_hits": int(np.sum((i64n >= 0) & (ih < 0)) + np.sum(both & (ih != i64n) & (rel > 1e-6))),
+                     "tie_mismatches": int(np.sum(both & (ih != i64n) & (rel <= 1e-6))), "max_rel_t_error": float(rel[same].max()) if same.any() else 0.0,
+                     "plain_grays_s": plain, "vs_plain": value / plain if plain else None}
         achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
         out.update(metric="closest+any rays per second, incoherent ray batch", value=value, ms_per_step=max_ms / args.steps,
-                   config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles)", "rays": n, "layout": LAYOUT_NAMES[variant],
+                   config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles)", "rays": n,
+                           "layout": LAYOUT_NAMES[variant] + (" precision form (f16 conservative slabs, watertight fp32 triangles)" if wl.get("precision") else ""), **check,
                            "sah_bins": args.bins, "tri": "woop", "traversal": ["auto", "refill", "batch"][args.traversal], "l2": f"ray batch {n * 32 / 1e9:.2f} GB > L2 (126 MB)",
                            "closest_ms": c_ms / args.steps, "any_ms": a_ms / args.steps},
                    clocks=clocks,

@@ -38,12 +38,13 @@ class BuildOptions(C.Structure):
 class BvhData(C.Structure):
     _fields_ = [("nodes", C.POINTER(C.c_float)), ("n_node_float4", C.c_int64), ("node_stride", C.c_int32),
                 ("order", C.POINTER(C.c_int32)), ("n_tris", C.c_int64), ("tris", C.POINTER(C.c_float)), ("nrm", C.POINTER(C.c_float)),
-                ("woop", C.POINTER(C.c_float)), ("max_depth", C.c_int32), ("max_leaf_tris", C.c_int32), ("sah", C.c_double), ("build_ms", C.c_double)]
+                ("woop", C.POINTER(C.c_float)), ("max_depth", C.c_int32), ("max_leaf_tris", C.c_int32), ("sah", C.c_double), ("build_ms", C.c_double),
+                ("verts", C.POINTER(C.c_float))]
 
 
 class SceneBuffers(C.Structure):
     _fields_ = [("nodes", C.c_void_p), ("n_node_float4", C.c_int64), ("node_stride", C.c_int32), ("tris", C.c_void_p), ("n_tris", C.c_int64),
-                ("nrm", C.c_void_p), ("woop", C.c_void_p), ("albedo", C.c_void_p), ("n_albedo", C.c_int32)]
+                ("nrm", C.c_void_p), ("woop", C.c_void_p), ("albedo", C.c_void_p), ("n_albedo", C.c_int32), ("verts", C.c_void_p)]
 
 
 class Camera(C.Structure):
@@ -97,6 +98,8 @@ SIGNATURES = {
     "cwp_trace_any_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_float)]),
     "cwp_accel_status": (C.c_int, [C.c_void_p]),
     "cwp_accel_set_traversal": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cwp_accel_set_precision": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cwp_trace_fp64": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "cwp_renderer_create": (C.c_int, [C.POINTER(C.c_void_p)]),
     "cwp_renderer_init": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(SceneBuffers), C.POINTER(RenderOptions)]),
     "cwp_renderer_render": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(FrameStats), C.c_int32, C.c_int32]),
@@ -216,6 +219,7 @@ class Bvh:
             self.order = np.ctypeslib.as_array(d.order, (d.n_tris,)).copy()
             self.tris = np.ctypeslib.as_array(d.tris, (d.n_tris * 3, 4)).copy()
             self.woop = np.ctypeslib.as_array(d.woop, (d.n_tris * 3, 4)).copy()
+            self.verts = np.ctypeslib.as_array(d.verts, (d.n_tris * 3, 4)).copy()
             self.nrm = np.ctypeslib.as_array(d.nrm, (d.n_tris * 3, 4)).copy() if d.nrm else None
             self.max_depth, self.max_leaf_tris, self.sah, self.build_ms = d.max_depth, d.max_leaf_tris, d.sah, d.build_ms
         finally:
@@ -233,6 +237,7 @@ class Bvh:
         s.tris, s.n_tris = self.tris.ctypes.data, len(self.order)
         s.nrm = self.nrm.ctypes.data if self.nrm is not None else None
         s.woop = self.woop.ctypes.data
+        s.verts = self.verts.ctypes.data
         self._alb = np.ascontiguousarray(self.albedo, np.float32)
         s.albedo, s.n_albedo = self._alb.ctypes.data, len(self._alb)
         return s
@@ -269,6 +274,13 @@ class Accel:
 
     def status(self):
         _check(lib().cwp_accel_status(self._h))
+
+    def set_precision(self, mode):
+        """0 plain path, 1 precision form (f16 conservative slabs + watertight FP32 triangles)"""
+        _check(lib().cwp_accel_set_precision(self._h, mode))
+
+    def trace_fp64(self, d_o, d_d, d_t, d_tri, n, any_hit=False, stream=None):
+        _check(lib().cwp_trace_fp64(self._h, 1 if any_hit else 0, d_o, d_d, d_t, d_tri, n, stream))
 
     def set_traversal(self, mode):
         """0 auto (persistent refill for BVH2 / CWBVH), 1 refill, 2 one ray per thread"""

@@ -73,7 +73,7 @@ extern "C" void cwp_mesh_free(cwp_mesh* h) { delete h; }
 
 // ---------------- host BVH ----------------
 struct cwp_bvh {
-    std::vector<float4> nodes, tris, nrm, woop; std::vector<int> order;
+    std::vector<float4> nodes, tris, nrm, woop, verts; std::vector<int> order;
     int stride = 4, maxDepth = 0, maxLeafTris = 0; double sah = 0, ms = 0;
 };
 
@@ -107,6 +107,7 @@ extern "C" int cwp_bvh_build(const cwp_mesh* h, const cwp_build_options* o, cwp_
     if (o->variant != 8) { int mx = 0; for (const BNode& n : B.nodes) if (n.leaf()) mx = n.count > mx ? n.count : mx; r->maxLeafTris = mx; }
     pack_tris(m, r->order, r->tris, r->nrm);
     pack_woop(m, r->order, r->woop);
+    pack_verts(m, r->order, r->verts);
     r->ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (o->variant != 8 && B.maxDepth > 63) { delete r; return set_error(CWP_ERR_INVALID, "BVH depth %d exceeds the traversal stack (64)", B.maxDepth); }
     *out = r; return CWP_OK;
@@ -118,6 +119,7 @@ extern "C" int cwp_bvh_data_of(const cwp_bvh* b, cwp_bvh_data* out) {
     out->order = b->order.data(); out->n_tris = (int64_t)b->order.size();
     out->tris = (const float*)b->tris.data(); out->nrm = b->nrm.empty() ? nullptr : (const float*)b->nrm.data(); out->woop = (const float*)b->woop.data();
     out->max_depth = b->maxDepth; out->max_leaf_tris = b->maxLeafTris; out->sah = b->sah; out->build_ms = b->ms;
+    out->verts = (const float*)b->verts.data();
     return CWP_OK;
 }
 

@@ -484,4 +484,12 @@ void pack_woop(const Mesh& m, const std::vector<int>& order, std::vector<float4>
     }
 }
 
+void pack_verts(const Mesh& m, const std::vector<int>& order, std::vector<float4>& v) {
+    const size_t n = order.size(); v.resize(3 * n);
+    for (size_t k = 0; k < n; k++) {
+        const int* f = &m.f[3 * (size_t)order[k]];
+        for (int c = 0; c < 3; c++) v[3 * k + c] = f4(m.vert(f[c]), 0.f);
+    }
+}
+
 }  // namespace cwpb

@@ -65,5 +65,8 @@ int append_bvh8(std::vector<float4>& all, const std::vector<float4>& blas, int t
 
 void pack_tris(const Mesh& m, const std::vector<int>& order, std::vector<float4>& tris, std::vector<float4>& nrm);
 void pack_woop(const Mesh& m, const std::vector<int>& order, std::vector<float4>& w);
+// exact corner positions in leaf order, (v0, 0), (v1, 0), (v2, 0): the watertight triangle test needs the shared
+// vertices of neighbouring triangles bit for bit (v0 + e1 would be rounded)
+void pack_verts(const Mesh& m, const std::vector<int>& order, std::vector<float4>& v);
 
 }  // namespace cwpb

@@ -11,9 +11,11 @@ struct DeviceScene {
     float4* tris = nullptr; int64_t nTris = 0;       // (v0, id), (e1, mat), (e2, 0)
     float4* woop = nullptr;                          // Woop rows or nullptr
     float4* nrm = nullptr;                           // per-corner normals or nullptr
+    float4* verts = nullptr;                         // exact corners (precision form) or nullptr
+    bool precise = false;                            // ray batches use the precision form (FP16 slabs + watertight)
     float3* albedo = nullptr; int nAlbedo = 0;
     size_t bytes = 0;
-    const float4* leafData() const { return tri == 1 ? woop : tris; }
+    const float4* leafData() const { return precise ? verts : tri == 1 ? woop : tris; }
 };
 
 // Checks every child and leaf reference of the node array against the buffer sizes (so that no traversal can read

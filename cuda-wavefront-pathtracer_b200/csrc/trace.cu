@@ -47,8 +47,8 @@ int validate_nodes(const float* nodes, int64_t nF4, int stride, int64_t nTris, i
 }
 
 void free_scene(DeviceScene& s) {
-    if (s.nodes || s.tris || s.woop || s.nrm || s.albedo) cudaSetDevice(s.device);
-    cudaFree(s.nodes); cudaFree(s.tris); cudaFree(s.woop); cudaFree(s.nrm); cudaFree(s.albedo);
+    if (s.nodes || s.tris || s.woop || s.nrm || s.albedo || s.verts) cudaSetDevice(s.device);
+    cudaFree(s.nodes); cudaFree(s.tris); cudaFree(s.woop); cudaFree(s.nrm); cudaFree(s.albedo); cudaFree(s.verts);
     s = DeviceScene();
 }
 
@@ -71,6 +71,7 @@ int upload_scene(const cwp_scene_buffers* s, int tri, int device, DeviceScene& o
     if (e == cudaSuccess) e = up((void**)&out.tris, s->tris, (size_t)s->n_tris * 48);
     if (e == cudaSuccess && s->woop) e = up((void**)&out.woop, s->woop, (size_t)s->n_tris * 48);
     if (e == cudaSuccess && s->nrm) e = up((void**)&out.nrm, s->nrm, (size_t)s->n_tris * 48);
+    if (e == cudaSuccess && s->verts) e = up((void**)&out.verts, s->verts, (size_t)s->n_tris * 48);
     if (e == cudaSuccess) {
         std::vector<float3> alb;
         for (int i = 0; i < s->n_albedo; i++) alb.push_back(make_float3(s->albedo[3 * i], s->albedo[3 * i + 1], s->albedo[3 * i + 2]));
@@ -160,10 +161,11 @@ template <bool ANY>
 static int launch_batch(const DeviceScene& s, const float4* o, const float4* d, void* out, long long n, int* err, cudaStream_t st, int* fetch, int refillGrid) {
     if (n <= 0) return CWP_OK;
     const float4* tv0 = s.leafData();
-    if (fetch && s.variant != 4) {   // persistent refill kernels (BVH2, CWBVH)
+    if (fetch && s.variant != 4) {   // persistent refill kernels (BVH2, CWBVH, precision form)
         CWPB_CUDA(cudaMemsetAsync(fetch, 0, sizeof(unsigned long long), st));
 #define CWPB_R(VV, TT) k_trace_rf<VV, TT, ANY><<<refillGrid, kBatchBlock, 0, st>>>(s.nodes, tv0, o, d, (float4*)out, (int*)out, n, fetch, err)
-        if (s.variant == 2) { if (s.tri) CWPB_R(2, 1); else CWPB_R(2, 0); }
+        if (s.precise) CWPB_R(16, 1);
+        else if (s.variant == 2) { if (s.tri) CWPB_R(2, 1); else CWPB_R(2, 0); }
         else { if (s.tri) CWPB_R(8, 1); else CWPB_R(8, 0); }
 #undef CWPB_R
         CWPB_CUDA(cudaGetLastError());
@@ -173,12 +175,26 @@ static int launch_batch(const DeviceScene& s, const float4* o, const float4* d, 
     const float4* tv = s.leafData();
 #define CWPB_L(VV, TT) do { if (ANY) k_trace_any<VV, TT><<<grid, kBatchBlock, 0, st>>>(s.nodes, tv, o, d, (int*)out, n, err); \
                             else k_trace_closest<VV, TT><<<grid, kBatchBlock, 0, st>>>(s.nodes, tv, o, d, (float4*)out, n, err); } while (0)
-    if (s.variant == 2) { if (s.tri) CWPB_L(2, 1); else CWPB_L(2, 0); }
+    if (s.precise) CWPB_L(16, 1);
+    else if (s.variant == 2) { if (s.tri) CWPB_L(2, 1); else CWPB_L(2, 0); }
     else if (s.variant == 4) { if (s.tri) CWPB_L(4, 1); else CWPB_L(4, 0); }
     else { if (s.tri) CWPB_L(8, 1); else CWPB_L(8, 0); }
 #undef CWPB_L
     CWPB_CUDA(cudaGetLastError());
     return CWP_OK;
+}
+
+// FP64 reference traversal of a ray batch (the precision form's oracle): t in double, leaf-order triangle or -1
+template <bool ANY>
+__global__ void __launch_bounds__(kBatchBlock) k_trace_fp64(const float4* __restrict__ nodes, const float4* __restrict__ verts, const float4* __restrict__ ro,
+                                                            const float4* __restrict__ rd, double* __restrict__ tOut, int* __restrict__ triOut, long long n, int* err) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 O = ro[i], D = rd[i];
+    double t = D.w; int tri = -1, e = 0;
+    trav_fp64<ANY>(nodes, verts, make_double3(O.x, O.y, O.z), make_double3(D.x, D.y, D.z), (double)O.w, t, tri, e);
+    tOut[i] = t; triOut[i] = tri;
+    if (e) atomicOr(err, e);
 }
 
 }  // namespace cwpb
@@ -284,6 +300,35 @@ extern "C" int cwp_accel_set_traversal(cwp_accel* a, int32_t mode) {
     CWPB_CHECK(!(mode == 1 && a->scene.variant == 4), CWP_ERR_INVALID, "refill traversal is available for BVH2 and CWBVH, not BVH4");
     // auto: refill for CWBVH (measured faster on incoherent batches), one ray per thread for BVH2 and BVH4
     a->refill = mode == 1 || (mode == 0 && a->scene.variant == 8);
+    return CWP_OK;
+}
+
+extern "C" int cwp_accel_set_precision(cwp_accel* a, int32_t mode) {
+    CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
+    CWPB_CHECK(mode == 0 || mode == 1, CWP_ERR_INVALID, "precision mode %d is not 0 (plain) or 1 (precision form)", mode);
+    CWPB_CHECK(mode == 0 || (a->scene.variant == 8 && a->scene.verts), CWP_ERR_INVALID, "the precision form needs a CWBVH and the exact corner buffer (cwp_scene_buffers.verts)");
+    a->scene.precise = mode == 1;
+    if (a->scene.precise) {
+        int nSM = 0, b = 0;
+        CWPB_CUDA(cudaSetDevice(a->scene.device));
+        CWPB_CUDA(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, a->scene.device));
+        CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace_rf<16, 1, false>, kBatchBlock, 0));
+        a->refillGrid = b * nSM;
+    }
+    return CWP_OK;
+}
+
+extern "C" int cwp_trace_fp64(cwp_accel* a, int32_t any_hit, const float* d_o, const float* d_d, double* d_t, int32_t* d_tri, int64_t n, void* stream) {
+    CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
+    CWPB_CHECK(n >= 0, CWP_ERR_INVALID, "negative ray count");
+    CWPB_CHECK(a->scene.variant == 8 && a->scene.verts, CWP_ERR_INVALID, "the FP64 traversal needs a CWBVH and the exact corner buffer");
+    if (n == 0) return CWP_OK;
+    CWPB_CHECK(d_o && d_d && d_t && d_tri, CWP_ERR_INVALID, "NULL buffer");
+    CWPB_CUDA(cudaSetDevice(a->scene.device));
+    const unsigned grid = (unsigned)((n + kBatchBlock - 1) / kBatchBlock);
+    if (any_hit) k_trace_fp64<true><<<grid, kBatchBlock, 0, (cudaStream_t)stream>>>(a->scene.nodes, a->scene.verts, (const float4*)d_o, (const float4*)d_d, d_t, d_tri, n, a->err);
+    else k_trace_fp64<false><<<grid, kBatchBlock, 0, (cudaStream_t)stream>>>(a->scene.nodes, a->scene.verts, (const float4*)d_o, (const float4*)d_d, d_t, d_tri, n, a->err);
+    CWPB_CUDA(cudaGetLastError());
     return CWP_OK;
 }
 

@@ -15,6 +15,7 @@
 // instead of running out of bounds or forever.
 #pragma once
 #include "vecmath.h"
+#include <cuda_fp16.h>
 
 namespace cwpb {
 
@@ -243,11 +244,215 @@ __device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, con
     return hitTri >= 0;
 }
 
+
+// ---------------- precision form: FP16 conservative slabs + watertight FP32 triangles ----------------
+// Box test: the CWBVH's 8-bit child planes q (0..255) sit at t = A + q B per axis, A = (node origin - ray origin) / d,
+// B = 2^e / d. The test runs in f16x2, two children per instruction: a byte permute builds the halves 1024 + q, so
+// t = A' + (1024 + q) B with A' = A - 1024 B. The per-node bases are rounded outward in f32 -> f16 (down for the planes
+// a ray enters, up for those it leaves) after widening by m = (|A| + 2048 |B|) / 512 + 1e-4, which bounds the rounding
+// of B to f16 (<= 2^-11 |B| per unit of 1024 + q <= 1279) and of the f16 fused multiply-add (<= 2^-11 of a result
+// <= |A| + 2303 |B|), with an absolute term for f16 subnormals; an axis whose values could leave the f16 range is left
+// unconstrained. So every box the ray meets in exact arithmetic passes - the test is conservative.
+// Triangle test: watertight ray/triangle intersection (Woop, Benthin & Wald, JCGT 2013): shear to the ray's dominant
+// axis, edge functions from the exact shared corner positions (no fused operations, so a shared edge gives the same
+// value with opposite sign in both triangles), double-precision recomputation when an edge function is exactly zero.
+// With the conservative box test no hit inside [tmin, tmax] can be lost.
+struct WtRay { int kx, ky, kz; float sx, sy, sz; };
+__device__ __forceinline__ float comp3(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+__device__ __forceinline__ WtRay wt_setup(float3 d) {
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    WtRay r; r.kz = ax >= ay ? (ax >= az ? 0 : 2) : (ay >= az ? 1 : 2);
+    r.kx = r.kz == 2 ? 0 : r.kz + 1; r.ky = r.kx == 2 ? 0 : r.kx + 1;
+    if (comp3(d, r.kz) < 0.f) { const int t = r.kx; r.kx = r.ky; r.ky = t; }   // keep the winding
+    const float dz = comp3(d, r.kz);
+    r.sx = comp3(d, r.kx) / dz; r.sy = comp3(d, r.ky) / dz; r.sz = 1.f / dz;
+    return r;
+}
+
+template <bool ANY>
+__device__ __forceinline__ bool wt_leaf(const float4* __restrict__ vt, int first, int cnt, float3 o, const WtRay& r, float tmin,
+                                        float& hitT, int& hitTri, float& hu, float& hv) {
+    for (int t = first; t < first + cnt; t++) {
+        const float3 A = xyz(ld4(vt + 3 * t)) - o, B = xyz(ld4(vt + 3 * t + 1)) - o, C = xyz(ld4(vt + 3 * t + 2)) - o;
+        const float Az = comp3(A, r.kz), Bz = comp3(B, r.kz), Cz = comp3(C, r.kz);
+        const float Ax = comp3(A, r.kx) - r.sx * Az, Ay = comp3(A, r.ky) - r.sy * Az;
+        const float Bx = comp3(B, r.kx) - r.sx * Bz, By = comp3(B, r.ky) - r.sy * Bz;
+        const float Cx = comp3(C, r.kx) - r.sx * Cz, Cy = comp3(C, r.ky) - r.sy * Cz;
+        float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+        if (U == 0.f || V == 0.f || W == 0.f) {   // products of floats are exact in double: the signs become exact
+            U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+            V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+            W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+        }
+        if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) continue;
+        const float det = U + V + W;
+        if (det == 0.f) continue;
+        const float T = U * (r.sz * Az) + V * (r.sz * Bz) + W * (r.sz * Cz);
+        const float tt = T / det;
+        if (!(tt > tmin && tt < hitT)) continue;
+        hitT = tt; hitTri = t; hu = V / det; hv = W / det;
+        if (ANY) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ __half2 h2_of_bits(unsigned u) { __half2 h; memcpy(&h, &u, 4); return h; }
+
+// outward-rounded f16 bases of one axis (see above); an axis outside the f16 range is left unconstrained
+__device__ __forceinline__ void h16_axis(float A, float B, __half2& lo2, __half2& hi2, __half2& b2) {
+    const float m = (fabsf(A) + 2048.f * fabsf(B)) * (1.f / 512.f) + 1e-4f, Ap = A - 1024.f * B;   // + 1e-4: f16 subnormal spacing
+    if (fabsf(B) * 1279.f < 30000.f && fabsf(Ap) + m < 30000.f) {
+        const __half lo = __float2half_rd(Ap - m), hi = __float2half_ru(Ap + m), b = __float2half_rn(B);
+        lo2 = __halves2half2(lo, lo); hi2 = __halves2half2(hi, hi); b2 = __halves2half2(b, b);
+    } else {
+        lo2 = h2_of_bits(0xFC00FC00u); hi2 = h2_of_bits(0x7C007C00u); b2 = h2_of_bits(0u);   // -inf, +inf, 0
+    }
+}
+
+template <bool ANY, int TRI>
+struct TravState<16, ANY, TRI> {
+    typedef uint2 Stack[kStack8];
+    float3 o, d; float idx, idy, idz, tmin, hitT, hu, hv; int hitTri, node, sp, budget; unsigned oct, cb, im, hm; WtRay wt;
+
+    __device__ __forceinline__ void begin(float3 o_, float3 d_, float tmin_, float tmax_, int root) {
+        o = o_; d = d_; tmin = tmin_; hitT = tmax_; hu = hv = 0.f; hitTri = -1; node = root; sp = 0; budget = kVisitBudget;
+        idx = safe_rcp(d.x); idy = safe_rcp(d.y); idz = safe_rcp(d.z);
+        oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
+        cb = im = hm = 0; wt = wt_setup(d);
+    }
+    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ vt, Stack& stack, int& err) {
+        if (--budget < 0) { err |= kTravBudget; return true; }
+        const float4* nb = nodes + 5 * (size_t)node;
+        const float4 f0 = ld4(nb), f1 = ld4(nb + 1), f2 = ld4(nb + 2), f3_ = ld4(nb + 3), f4_ = ld4(nb + 4);
+        const unsigned ew = __float_as_uint(f0.w);
+        const unsigned imask = ew >> 24, m0 = __float_as_uint(f1.z), m1 = __float_as_uint(f1.w);
+        const int childBase = __float_as_int(f1.x), triBase = __float_as_int(f1.y);
+        __half2 xlo, xhi, xb, ylo, yhi, yb, zlo, zhi, zb;
+        h16_axis((f0.x - o.x) * idx, __uint_as_float((ew & 255u) << 23) * idx, xlo, xhi, xb);
+        h16_axis((f0.y - o.y) * idy, __uint_as_float(((ew >> 8) & 255u) << 23) * idy, ylo, yhi, yb);
+        h16_axis((f0.z - o.z) * idz, __uint_as_float(((ew >> 16) & 255u) << 23) * idz, zlo, zhi, zb);
+        const bool fx = idx < 0.f, fy = idy < 0.f, fz = idz < 0.f;
+        const unsigned nx0 = __float_as_uint(fx ? f3_.z : f2.x), nx1 = __float_as_uint(fx ? f3_.w : f2.y), px0 = __float_as_uint(fx ? f2.x : f3_.z), px1 = __float_as_uint(fx ? f2.y : f3_.w);
+        const unsigned ny0 = __float_as_uint(fy ? f4_.x : f2.z), ny1 = __float_as_uint(fy ? f4_.y : f2.w), py0 = __float_as_uint(fy ? f2.z : f4_.x), py1 = __float_as_uint(fy ? f2.w : f4_.y);
+        const unsigned nz0 = __float_as_uint(fz ? f4_.z : f3_.x), nz1 = __float_as_uint(fz ? f4_.w : f3_.y), pz0 = __float_as_uint(fz ? f3_.x : f4_.z), pz1 = __float_as_uint(fz ? f3_.y : f4_.w);
+        const __half tmn = __float2half_rd(tmin), tmx = __float2half_ru(hitT);
+        const __half2 tmin2 = __halves2half2(tmn, tmn), tmax2 = __halves2half2(tmx, tmx);
+        unsigned boxHit = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const unsigned sel = (j & 1) ? 0x4342u : 0x4140u;   // bytes (2j, 2j+1) of the word, each under 0x64: halves 1024 + q
+            const __half2 xn = __hfma2(h2_of_bits(__byte_perm(j < 2 ? nx0 : nx1, 0x64646464u, sel)), xb, xlo);
+            const __half2 xf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? px0 : px1, 0x64646464u, sel)), xb, xhi);
+            const __half2 yn = __hfma2(h2_of_bits(__byte_perm(j < 2 ? ny0 : ny1, 0x64646464u, sel)), yb, ylo);
+            const __half2 yf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? py0 : py1, 0x64646464u, sel)), yb, yhi);
+            const __half2 zn = __hfma2(h2_of_bits(__byte_perm(j < 2 ? nz0 : nz1, 0x64646464u, sel)), zb, zlo);
+            const __half2 zf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? pz0 : pz1, 0x64646464u, sel)), zb, zhi);
+            const __half2 tn = __hmax2(__hmax2(xn, yn), __hmax2(zn, tmin2));
+            const __half2 tf = __hmin2(__hmin2(xf, yf), __hmin2(zf, tmax2));
+            const unsigned m = __hle2_mask(tn, tf);
+            boxHit |= ((m & 1u) << (2 * j)) | (((m >> 16) & 1u) << (2 * j + 1));
+        }
+        const unsigned leafMask = ((m0 >> 7) & 1u) | ((m0 >> 14) & 2u) | ((m0 >> 21) & 4u) | ((m0 >> 28) & 8u) |
+                                  ((m1 >> 3) & 16u) | ((m1 >> 10) & 32u) | ((m1 >> 17) & 64u) | ((m1 >> 24) & 128u);
+        unsigned leafHit = boxHit & leafMask;
+        unsigned hits = boxHit & imask;
+        if (oct & 1u) hits = ((hits & 0x55u) << 1) | ((hits & 0xAAu) >> 1);
+        if (oct & 2u) hits = ((hits & 0x33u) << 2) | ((hits & 0xCCu) >> 2);
+        if (oct & 4u) hits = ((hits & 0x0Fu) << 4) | ((hits & 0xF0u) >> 4);
+        while (leafHit) {
+            const int s = __ffs(leafHit) - 1; leafHit &= leafHit - 1;
+            const unsigned m = byte_of(s < 4 ? m0 : m1, s);
+            if (wt_leaf<ANY>(vt, triBase + (int)(m & 31u), (int)((m >> 5) & 3u) + 1, o, wt, tmin, hitT, hitTri, hu, hv) && ANY) return true;
+        }
+        if (hits) {
+            if (hm) { if (sp == kStack8) { err |= kTravOverflow; return true; } stack[sp++] = make_uint2(cb, (im << 8) | hm); }
+            cb = (unsigned)childBase; im = imask; hm = hits;
+        }
+        while (hm == 0) { if (sp == 0) return true; const uint2 e = stack[--sp]; cb = e.x; im = e.y >> 8; hm = e.y & 255u; }
+        const unsigned k = __ffs(hm) - 1; hm &= hm - 1; const unsigned slot = k ^ oct;
+        node = (int)cb + __popc(im & ((1u << slot) - 1u));
+        return false;
+    }
+};
+
+// ---------------- FP64 reference traversal (the precision form's oracle) ----------------
+// CWBVH nodes decoded exactly in double (origin + q 2^e), slab test in double widened by 1e-12 relative, watertight
+// triangle test in double on the exact corners. Finds the closest hit in (tmin, tmax) to double accuracy.
+__device__ __forceinline__ double dcomp(double3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+template <bool ANY>
+__device__ __forceinline__ bool trav_fp64(const float4* __restrict__ nodes, const float4* __restrict__ vt, double3 o, double3 d, double tmin,
+                                          double& hitT, int& hitTri, int& err) {
+    uint2 stack[kStack8]; int sp = 0, budget = kVisitBudget, node = 0;
+    const double ix = 1.0 / (fabs(d.x) > 1e-300 ? d.x : copysign(1e-300, d.x)), iy = 1.0 / (fabs(d.y) > 1e-300 ? d.y : copysign(1e-300, d.y)),
+                 iz = 1.0 / (fabs(d.z) > 1e-300 ? d.z : copysign(1e-300, d.z));
+    const double ad[3] = { fabs(d.x), fabs(d.y), fabs(d.z) };
+    int kz = ad[0] >= ad[1] ? (ad[0] >= ad[2] ? 0 : 2) : (ad[1] >= ad[2] ? 1 : 2), kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
+    if (dcomp(d, kz) < 0.0) { const int t = kx; kx = ky; ky = t; }
+    const double sx = dcomp(d, kx) / dcomp(d, kz), sy = dcomp(d, ky) / dcomp(d, kz), sz = 1.0 / dcomp(d, kz);
+    unsigned cb = 0, im = 0, hm = 0;
+    while (true) {
+        if (--budget < 0) { err |= kTravBudget; return hitTri >= 0; }
+        const float4* nb = nodes + 5 * (size_t)node;
+        const float4 f0 = ld4(nb), f1 = ld4(nb + 1);
+        const unsigned ew = __float_as_uint(f0.w), imask = ew >> 24, m0 = __float_as_uint(f1.z), m1 = __float_as_uint(f1.w);
+        const int childBase = __float_as_int(f1.x), triBase = __float_as_int(f1.y);
+        const double ex = (double)__uint_as_float((ew & 255u) << 23), ey = (double)__uint_as_float(((ew >> 8) & 255u) << 23), ez = (double)__uint_as_float(((ew >> 16) & 255u) << 23);
+        const unsigned* q = reinterpret_cast<const unsigned*>(nb + 2);
+        unsigned boxHit = 0;
+        for (int s = 0; s < 8; s++) {
+            const int w = s < 4 ? 0 : 1;
+            const double lx = (double)f0.x + byte_of(__ldg(q + 0 + w), s) * ex, ly = (double)f0.y + byte_of(__ldg(q + 2 + w), s) * ey, lz = (double)f0.z + byte_of(__ldg(q + 4 + w), s) * ez;
+            const double hx = (double)f0.x + byte_of(__ldg(q + 6 + w), s) * ex, hy = (double)f0.y + byte_of(__ldg(q + 8 + w), s) * ey, hz = (double)f0.z + byte_of(__ldg(q + 10 + w), s) * ez;
+            const double x0 = (lx - o.x) * ix, x1 = (hx - o.x) * ix, y0 = (ly - o.y) * iy, y1 = (hy - o.y) * iy, z0 = (lz - o.z) * iz, z1 = (hz - o.z) * iz;
+            const double tn = fmax(fmax(fmin(x0, x1), fmin(y0, y1)), fmax(fmin(z0, z1), tmin));
+            const double tf = fmin(fmin(fmax(x0, x1), fmax(y0, y1)), fmin(fmax(z0, z1), hitT));
+            if (tn - 1e-12 * fabs(tn) <= tf + 1e-12 * fabs(tf)) boxHit |= 1u << s;
+        }
+        for (int s = 0; s < 8; s++) {
+            if (!(boxHit & (1u << s))) continue;
+            const unsigned m = byte_of(s < 4 ? m0 : m1, s);
+            if (!(m & 0x80u)) continue;
+            for (int t = triBase + (int)(m & 31u), e = t + (int)((m >> 5) & 3u) + 1; t < e; t++) {
+                const float4 a = ld4(vt + 3 * t), b = ld4(vt + 3 * t + 1), c = ld4(vt + 3 * t + 2);
+                const double3 A = make_double3(a.x - o.x, a.y - o.y, a.z - o.z), B = make_double3(b.x - o.x, b.y - o.y, b.z - o.z), C = make_double3(c.x - o.x, c.y - o.y, c.z - o.z);
+                const double Az = dcomp(A, kz), Bz = dcomp(B, kz), Cz = dcomp(C, kz);
+                const double Ax = dcomp(A, kx) - sx * Az, Ay = dcomp(A, ky) - sy * Az, Bx = dcomp(B, kx) - sx * Bz, By = dcomp(B, ky) - sy * Bz;
+                const double Cx = dcomp(C, kx) - sx * Cz, Cy = dcomp(C, ky) - sy * Cz;
+                const double U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+                if ((U < 0.0 || V < 0.0 || W < 0.0) && (U > 0.0 || V > 0.0 || W > 0.0)) continue;
+                const double det = U + V + W;
+                if (det == 0.0) continue;
+                const double tt = (U * (sz * Az) + V * (sz * Bz) + W * (sz * Cz)) / det;
+                if (tt > tmin && tt < hitT) { hitT = tt; hitTri = t; if (ANY) return true; }
+            }
+        }
+        unsigned hits = boxHit & imask;
+        const unsigned oct = (d.x > 0.0 ? 1u : 0u) | (d.y > 0.0 ? 2u : 0u) | (d.z > 0.0 ? 4u : 0u);
+        unsigned ho = 0;
+        for (int s = 0; s < 8; s++) if (hits & (1u << s)) ho |= 1u << (s ^ oct);
+        if (ho) {
+            if (hm) { if (sp == kStack8) { err |= kTravOverflow; return hitTri >= 0; } stack[sp++] = make_uint2(cb, (im << 8) | hm); }
+            cb = (unsigned)childBase; im = imask; hm = ho;
+        }
+        while (hm == 0) { if (sp == 0) return hitTri >= 0; const uint2 e = stack[--sp]; cb = e.x; im = e.y >> 8; hm = e.y & 255u; }
+        const unsigned k = __ffs(hm) - 1; hm &= hm - 1;
+        node = (int)cb + __popc(im & ((1u << (k ^ oct)) - 1u));
+    }
+}
+
 template <int V, bool ANY, int TRI>
 __device__ __forceinline__ bool trace_ray(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
                                           float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
     if (V == 2) return trav_bvh2<ANY, TRI>(nodes, tv, o, d, tmin, hitT, hitTri, hu, hv, root, err);
     if (V == 4) return trav_bvh4<ANY, TRI>(nodes, tv, o, d, tmin, hitT, hitTri, hu, hv, root, err);
+    if (V == 16) {   // precision form: tv = exact corners
+        TravState<16, ANY, TRI> r; typename TravState<16, ANY, TRI>::Stack stack; r.begin(o, d, tmin, hitT, root);
+        while (!r.step(nodes, tv, stack, err)) {}
+        hitT = r.hitT; hitTri = r.hitTri; hu = r.hu; hv = r.hv;
+        return hitTri >= 0;
+    }
     return trav_cwbvh<ANY, TRI>(nodes, tv, o, d, tmin, hitT, hitTri, hu, hv, root, err);
 }
 

@@ -77,6 +77,7 @@ typedef struct cwp_bvh_data {
     const float* woop;                                                 /* 3 float4 per triangle */
     int32_t max_depth, max_leaf_tris;
     double sah, build_ms;
+    const float* verts;                                                /* 3 float4 per triangle: exact corners v0, v1, v2 */
 } cwp_bvh_data;
 
 int cwp_bvh_build(const cwp_mesh* m, const cwp_build_options* opt, cwp_bvh** out);
@@ -95,6 +96,7 @@ typedef struct cwp_scene_buffers {
     const float* nrm;       /* or NULL */
     const float* woop;      /* or NULL (required for CWP_TRI_WOOP) */
     const float* albedo; int32_t n_albedo;
+    const float* verts;     /* exact corners, 3 float4 per triangle, or NULL (required by the precision form) */
 } cwp_scene_buffers;
 
 typedef struct cwp_accel cwp_accel;
@@ -110,6 +112,15 @@ int cwp_trace_any_host(cwp_accel* a, const float* o, const float* d, int32_t* oc
 int cwp_accel_status(cwp_accel* a);
 /* kernel form of the batch calls: 0 auto (persistent refill for CWBVH), 1 refill (BVH2 / CWBVH), 2 one ray per thread */
 int cwp_accel_set_traversal(cwp_accel* a, int32_t mode);
+
+/* Precision form (no counterpart in the reference): mode 1 makes the batch calls traverse the CWBVH with f16x2 slab
+ * tests over its 8-bit child boxes, rounded outward so that they are conservative, and decide hits with a watertight
+ * FP32 triangle test on the exact corners (cwp_scene_buffers.verts) - no hit inside [tmin, tmax] is lost. Mode 0 is the
+ * plain path (FP32 slabs, the reference's triangle tests). Hits use the same leaf-order indices. */
+int cwp_accel_set_precision(cwp_accel* a, int32_t mode);
+/* FP64 traversal of the same CWBVH and exact corners (the precision form's oracle): t in double (tmax on a miss) and
+ * the leaf-order triangle (-1 on a miss); any_hit stops at the first occluder. Device buffers, stream-ordered. */
+int cwp_trace_fp64(cwp_accel* a, int32_t any_hit, const float* d_o, const float* d_d, double* d_t, int32_t* d_tri, int64_t n, void* stream);
 
 /* ------------------------------------------------------------------------------------------------------------------
  * Wavefront renderer. Replaces class WavefrontRenderer (render/renderer.h:47-93): init (wavefront.cu:469-502),

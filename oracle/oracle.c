@@ -542,3 +542,77 @@ void orc_render(const OrcParams* P, int variant, int tri, const float* nodes, co
     (void)N;
     if (ray_counts) { ray_counts[0] += nc; ray_counts[1] += ns; }
 }
+
+/* ------------------------------------------------------------------ FP64 watertight reference (precision form)
+ * Not in the reference. Restates the watertight ray/triangle test (Woop, Benthin & Wald, JCGT 2013) in double over the
+ * exact corners (verts: 3 float4 per leaf-order triangle), driven either by the CWBVH (nodes != NULL: child boxes
+ * decoded exactly in double, slab test widened by 1e-12 relative) or by brute force over all n_tris triangles
+ * (nodes == NULL). t_out = closest t in (tmin, tmax) (tmax on a miss), tri_out = leaf-order triangle or -1. */
+static double dcomp3(const double* v, int k) { return v[k]; }
+static int wt64(const float* vt, int t, const double* o, int kx, int ky, int kz, double sx, double sy, double sz, double tmin, double* hitT) {
+    const float* a = vt + 12 * (size_t)t; const float* b = a + 4; const float* c = a + 8;
+    double A[3] = { a[0] - o[0], a[1] - o[1], a[2] - o[2] }, B[3] = { b[0] - o[0], b[1] - o[1], b[2] - o[2] }, C[3] = { c[0] - o[0], c[1] - o[1], c[2] - o[2] };
+    double Az = dcomp3(A, kz), Bz = dcomp3(B, kz), Cz = dcomp3(C, kz);
+    double Ax = A[kx] - sx * Az, Ay = A[ky] - sy * Az, Bx = B[kx] - sx * Bz, By = B[ky] - sy * Bz, Cx = C[kx] - sx * Cz, Cy = C[ky] - sy * Cz;
+    double U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if ((U < 0.0 || V < 0.0 || W < 0.0) && (U > 0.0 || V > 0.0 || W > 0.0)) return 0;
+    double det = U + V + W;
+    if (det == 0.0) return 0;
+    double tt = (U * (sz * Az) + V * (sz * Bz) + W * (sz * Cz)) / det;
+    if (tt > tmin && tt < *hitT) { *hitT = tt; return 1; }
+    return 0;
+}
+long orc_trace_fp64(const float* nodes, const float* vt, int n_tris, const float* ro, const float* rd, long n, int any, double* t_out, int* tri_out) {
+    for (long i = 0; i < n; i++) {
+        const double o[3] = { ro[4 * i], ro[4 * i + 1], ro[4 * i + 2] }, d[3] = { rd[4 * i], rd[4 * i + 1], rd[4 * i + 2] };
+        const double tmin = ro[4 * i + 3]; double hitT = rd[4 * i + 3]; int hit = -1;
+        const double ad[3] = { fabs(d[0]), fabs(d[1]), fabs(d[2]) };
+        int kz = ad[0] >= ad[1] ? (ad[0] >= ad[2] ? 0 : 2) : (ad[1] >= ad[2] ? 1 : 2), kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
+        if (d[kz] < 0.0) { int t = kx; kx = ky; ky = t; }
+        const double sx = d[kx] / d[kz], sy = d[ky] / d[kz], sz = 1.0 / d[kz];
+        if (!nodes) {
+            for (int t = 0; t < n_tris; t++) if (wt64(vt, t, o, kx, ky, kz, sx, sy, sz, tmin, &hitT)) { hit = t; if (any) break; }
+        } else {
+            const double inv[3] = { 1.0 / (fabs(d[0]) > 1e-300 ? d[0] : copysign(1e-300, d[0])), 1.0 / (fabs(d[1]) > 1e-300 ? d[1] : copysign(1e-300, d[1])),
+                                    1.0 / (fabs(d[2]) > 1e-300 ? d[2] : copysign(1e-300, d[2])) };
+            const unsigned oct = (d[0] > 0.0 ? 1u : 0u) | (d[1] > 0.0 ? 2u : 0u) | (d[2] > 0.0 ? 4u : 0u);
+            unsigned stk[40][2]; int sp = 0, node = 0, done = 0; unsigned cb = 0, im = 0, hm = 0;
+            while (!done) {
+                const V4* nb = (const V4*)nodes + 5 * node;
+                unsigned ew = fu(nb[0].w), imask = ew >> 24, m0 = fu(nb[1].z), m1 = fu(nb[1].w);
+                int childBase = fi(nb[1].x), triBase = fi(nb[1].y);
+                double e[3] = { uf((ew & 255u) << 23), uf(((ew >> 8) & 255u) << 23), uf(((ew >> 16) & 255u) << 23) };
+                double org[3] = { nb[0].x, nb[0].y, nb[0].z };
+                const unsigned* q = (const unsigned*)(nb + 2);
+                unsigned boxHit = 0;
+                for (int s = 0; s < 8; s++) {
+                    int w = s < 4 ? 0 : 1; double lo[3], hi[3], tn = tmin, tf = hitT;
+                    for (int ax = 0; ax < 3; ax++) {
+                        lo[ax] = org[ax] + byte_of(q[2 * ax + w], s) * e[ax]; hi[ax] = org[ax] + byte_of(q[6 + 2 * ax + w], s) * e[ax];
+                    }
+                    double x0 = (lo[0] - o[0]) * inv[0], x1 = (hi[0] - o[0]) * inv[0], y0 = (lo[1] - o[1]) * inv[1], y1 = (hi[1] - o[1]) * inv[1], z0 = (lo[2] - o[2]) * inv[2], z1 = (hi[2] - o[2]) * inv[2];
+                    tn = fmax(fmax(fmin(x0, x1), fmin(y0, y1)), fmax(fmin(z0, z1), tmin));
+                    tf = fmin(fmin(fmax(x0, x1), fmax(y0, y1)), fmin(fmax(z0, z1), hitT));
+                    if (tn - 1e-12 * fabs(tn) <= tf + 1e-12 * fabs(tf)) boxHit |= 1u << s;
+                }
+                for (int s = 0; s < 8 && !done; s++) {
+                    if (!(boxHit & (1u << s))) continue;
+                    unsigned m = byte_of(s < 4 ? m0 : m1, s);
+                    if (!(m & 0x80u)) continue;
+                    for (int t = triBase + (int)(m & 31u), e2 = t + (int)((m >> 5) & 3u) + 1; t < e2; t++)
+                        if (wt64(vt, t, o, kx, ky, kz, sx, sy, sz, tmin, &hitT)) { hit = t; if (any) { done = 1; break; } }
+                }
+                if (done) break;
+                unsigned hits = boxHit & imask, ho = 0;
+                for (int s = 0; s < 8; s++) if (hits & (1u << s)) ho |= 1u << (s ^ oct);
+                if (ho) { if (hm) { if (sp == 40) return -1; stk[sp][0] = cb; stk[sp][1] = (im << 8) | hm; sp++; } cb = (unsigned)childBase; im = imask; hm = ho; }
+                while (hm == 0) { if (sp == 0) { done = 1; break; } sp--; cb = stk[sp][0]; im = stk[sp][1] >> 8; hm = stk[sp][1] & 255u; }
+                if (done) break;
+                unsigned k = (unsigned)__builtin_ctz(hm); hm &= hm - 1;
+                node = (int)cb + __builtin_popcount(im & ((1u << (k ^ oct)) - 1u));
+            }
+        }
+        t_out[i] = hitT; tri_out[i] = hit;
+    }
+    return 0;
+}

@@ -45,6 +45,8 @@ def _load_oracle():
     L.orc_trace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_render.restype = None
     L.orc_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    L.orc_trace_fp64.restype = C.c_long
+    L.orc_trace_fp64.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p]
     L.orc_rng.restype = C.c_float
     L.orc_rng.argtypes = [C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint]
     return L
@@ -83,6 +85,15 @@ class Oracle:
         assert bad == 0
         res = occ if any_hit else hits
         return (res, st) if stats else res
+
+    def trace_fp64(self, nodes, verts, o, d, any_hit=False, brute=False):
+        """FP64 watertight closest (or first) hit: (t float64, leaf-order tri int32); nodes = CWBVH or brute force."""
+        n = len(o); t = np.zeros(n, np.float64); tri = np.zeros(n, np.int32)
+        vt = np.ascontiguousarray(verts, np.float32)
+        r = self.L.orc_trace_fp64(None if brute else np.ascontiguousarray(nodes).ctypes.data, vt.ctypes.data, len(vt) // 3,
+                                  np.ascontiguousarray(o).ctypes.data, np.ascontiguousarray(d).ctypes.data, n, 1 if any_hit else 0, t.ctypes.data, tri.ctypes.data)
+        assert r == 0
+        return t, tri
 
     def render(self, params, variant, tri, bvh, bounces, spp, s_base=0, pix0=0, pix1=None):
         w, h = params.cam.w, params.cam.h

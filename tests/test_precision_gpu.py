@@ -1,0 +1,104 @@
+"""Precision form on the GPU (config 1's 12,290-triangle scene): f16x2 conservative slab tests over the CWBVH's 8-bit
+child boxes plus the watertight FP32 triangle test. Checked against the FP64 oracle on the GPU (itself bit-identical
+to the oracle's host restatement): no lost hits, ties only among equal distances, t within 1e-5 relative; an
+adversarial batch aimed at shared edges and corners finds no gap."""
+import numpy as np
+import pytest
+
+from conftest import tie_or_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def run(torch, acc, o, d, any_hit=False):
+    to, td = dev(torch, o), dev(torch, d); n = len(o)
+    if any_hit:
+        out = torch.empty(n, dtype=torch.int32, device="cuda"); acc.trace_any(to.data_ptr(), td.data_ptr(), out.data_ptr(), n)
+    else:
+        out = torch.empty((n, 4), dtype=torch.float32, device="cuda"); acc.trace_closest(to.data_ptr(), td.data_ptr(), out.data_ptr(), n)
+    torch.cuda.synchronize(); acc.status()
+    return out.cpu().numpy()
+
+
+def run64(torch, acc, o, d, any_hit=False):
+    to, td = dev(torch, o), dev(torch, d); n = len(o)
+    t = torch.empty(n, dtype=torch.float64, device="cuda"); tri = torch.empty(n, dtype=torch.int32, device="cuda")
+    acc.trace_fp64(to.data_ptr(), td.data_ptr(), t.data_ptr(), tri.data_ptr(), n, any_hit=any_hit)
+    torch.cuda.synchronize(); acc.status()
+    return t.cpu().numpy(), tri.cpu().numpy()
+
+
+def compare(h, t64, i64):
+    """(lost, ties, max relative t error) of float hits against the FP64 closest hits"""
+    ih = h[:, 3].view(np.int32)
+    lost = int(np.sum((i64 >= 0) & (ih < 0)))
+    both = (i64 >= 0) & (ih >= 0)
+    diff = both & (ih != i64)
+    rel = np.abs(h[:, 0].astype(np.float64) - t64) / np.maximum(t64, 1e-30)
+    ties = int(np.sum(diff & (rel <= 1e-6)))
+    far = int(np.sum(diff & (rel > 1e-6)))
+    same = both & (ih == i64)
+    return lost + far, ties, float(rel[same].max()) if same.any() else 0.0
+
+
+@pytest.fixture(scope="module")
+def scene12k(cwp):
+    return cwp.scene("boxes12k", variant=8, bins=32)
+
+
+def test_fp64_gpu_matches_host_oracle(gpu, cwp, oracle, scene12k):
+    mesh, bvh = scene12k
+    acc = cwp.Accel(bvh, tri=1)
+    p = cwp.frame_params(mesh, 256, 256)
+    o, d = cwp.incoherent_rays(20000, p, bvh.tris, lambda o, d: run(gpu, acc, o, d), seed=13)
+    t, i = run64(gpu, acc, o, d)
+    th, ih = oracle.trace_fp64(bvh.nodes, bvh.verts, o, d)
+    assert np.array_equal(i, ih) and np.array_equal(t, th)
+
+
+def test_precision_form_loses_no_hit_1m(gpu, cwp, scene12k):
+    mesh, bvh = scene12k
+    acc = cwp.Accel(bvh, tri=1)
+    p = cwp.frame_params(mesh, 256, 256)
+    o, d = cwp.incoherent_rays(1 << 20, p, bvh.tris, lambda o, d: run(gpu, acc, o, d), seed=17)
+    t64, i64 = run64(gpu, acc, o, d)
+    acc.set_precision(1)
+    h = run(gpu, acc, o, d)
+    lost, ties, maxrel = compare(h, t64, i64)
+    assert lost == 0, lost
+    assert ties <= 1e-4 * len(o)
+    assert maxrel <= 1e-5, maxrel
+    occ = run(gpu, acc, o, d, any_hit=True)
+    _, o64 = run64(gpu, acc, o, d, any_hit=True)
+    assert np.array_equal(occ >= 0, o64 >= 0)
+
+
+def test_watertight_on_shared_edges_and_corners(gpu, cwp, scene12k):
+    """Rays from above aimed exactly at corner positions and edge midpoints of the mesh: the precision form hits
+    whenever the FP64 oracle does (no ray slips between neighbouring triangles)."""
+    mesh, bvh = scene12k
+    v, f, _, _ = mesh.arrays()
+    rng = np.random.default_rng(5)
+    pick = rng.choice(len(f), 20000)
+    tri = v[f[pick]]
+    targets = np.concatenate([tri[:, 0], 0.5 * (tri[:, 0] + tri[:, 1]), 0.5 * (tri[:, 1] + tri[:, 2])]).astype(np.float32)
+    dirs = rng.normal(size=targets.shape).astype(np.float32); dirs[:, 2] = -np.abs(dirs[:, 2]) - 0.2
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    o = np.zeros((len(targets), 4), np.float32); o[:, :3] = targets - 30.0 * dirs
+    d = np.zeros((len(targets), 4), np.float32); d[:, :3] = dirs; d[:, 3] = 1e30
+    acc = cwp.Accel(bvh, tri=1)
+    t64, i64 = run64(gpu, acc, o, d)
+    acc.set_precision(1)
+    lost, ties, _ = compare(run(gpu, acc, o, d), t64, i64)
+    assert lost == 0, lost
+
+
+def test_precision_requires_cwbvh_and_corners(gpu, cwp):
+    _, b2 = cwp.scene("boxes12k", variant=2, bins=16)
+    acc = cwp.Accel(b2, tri=1)
+    with pytest.raises(cwp.CwpError):
+        acc.set_precision(1)
