@@ -382,10 +382,14 @@ def main():
             acc.trace_fp64(do.data_ptr(), dd.data_ptr(), t64.data_ptr(), i64.data_ptr(), n, stream=st.cuda_stream)
             torch.cuda.synchronize()
             h = hits.cpu().numpy(); t64n = t64.cpu().numpy(); i64n = i64.cpu().numpy(); ih = h[:, 3].view(np.int32)
-            rel = np.abs(h[:, 0].astype(np.float64) - t64n) / np.maximum(t64n, 1e-30)
-            both = (i64n >= 0) & (ih >= 0); same = both & (ih == i64n)
-            check = {"fp64_rays": n, "lost_hits": int(np.sum((i64n >= 0) & (ih < 0)) + np.sum(both & (ih != i64n) & (rel > 1e-6))),
-                     "tie_mismatches": int(np.sum(both & (ih != i64n) & (rel <= 1e-6))), "max_rel_t_error": float(rel[same].max()) if same.any() else 0.0,
+            ext = float(np.ptp(mesh.arrays()[0], axis=0).max())
+            pc = importlib.import_module("cuda-wavefront-pathtracer_b200.precision_check")
+            c = pc.classify_vs_fp64(h, t64n, i64n, ext, o=o, d=d, verts=bvh.verts)
+            ex = c["extra_mask"]
+            excess = pc.edge_excess(o[ex], d[ex], bvh.verts, h[ex, 3].view(np.int32)) if ex.any() else np.zeros(1)
+            check = {"fp64_rays": n, "lost_hits": c["lost"], "tie_mismatches": c["tie"], "extra_hits": c["extra"],
+                     "extra_hits_max_edge_excess": float(excess.max()),
+                     "max_t_error": c["max_t_error"], "t_error_unit": "max(t, scene extent)",
                      "plain_grays_s": plain, "vs_plain": value / plain if plain else None}
         achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
         out.update(metric="closest+any rays per second, incoherent ray batch", value=value, ms_per_step=max_ms / args.steps,

@@ -307,14 +307,13 @@ extern "C" int cwp_accel_set_precision(cwp_accel* a, int32_t mode) {
     CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
     CWPB_CHECK(mode == 0 || mode == 1, CWP_ERR_INVALID, "precision mode %d is not 0 (plain) or 1 (precision form)", mode);
     CWPB_CHECK(mode == 0 || (a->scene.variant == 8 && a->scene.verts), CWP_ERR_INVALID, "the precision form needs a CWBVH and the exact corner buffer (cwp_scene_buffers.verts)");
+    int nSM = 0, b = 0;
+    CWPB_CUDA(cudaSetDevice(a->scene.device));
+    CWPB_CUDA(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, a->scene.device));
+    if (mode == 1) CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace_rf<16, 1, false>, kBatchBlock, 0));
+    else CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, a->scene.tri == 1 ? k_trace_rf<8, 1, false> : k_trace_rf<8, 0, false>, kBatchBlock, 0));
     a->scene.precise = mode == 1;
-    if (a->scene.precise) {
-        int nSM = 0, b = 0;
-        CWPB_CUDA(cudaSetDevice(a->scene.device));
-        CWPB_CUDA(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, a->scene.device));
-        CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace_rf<16, 1, false>, kBatchBlock, 0));
-        a->refillGrid = b * nSM;
-    }
+    a->refillGrid = b * nSM;
     return CWP_OK;
 }
 

@@ -251,14 +251,20 @@ __device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, con
 // t = A' + (1024 + q) B with A' = A - 1024 B. The per-node bases are rounded outward in f32 -> f16 (down for the planes
 // a ray enters, up for those it leaves) after widening by m = (|A| + 2048 |B|) / 512 + 1e-4, which bounds the rounding
 // of B to f16 (<= 2^-11 |B| per unit of 1024 + q <= 1279) and of the f16 fused multiply-add (<= 2^-11 of a result
-// <= |A| + 2303 |B|), with an absolute term for f16 subnormals; an axis whose values could leave the f16 range is left
-// unconstrained. So every box the ray meets in exact arithmetic passes - the test is conservative.
+// <= |A| + 2303 |B|), with an absolute term for f16 subnormals. So every box the ray meets in exact arithmetic passes.
+// A node with an axis whose plane distances could leave the f16 range (a direction component near zero makes B large)
+// runs its eight slab tests in FP32 instead, widened by 2^-20 (|A| + 256 |B|), which bounds the FP32 rounding of A, B
+// and the fused decode (about 6 ulps); an axis with non-finite A or B is left unconstrained there.
 // Triangle test: watertight ray/triangle intersection (Woop, Benthin & Wald, JCGT 2013): shear to the ray's dominant
 // axis, edge functions from the exact shared corner positions (no fused operations, so a shared edge gives the same
-// value with opposite sign in both triangles), double-precision recomputation when an edge function is exactly zero.
-// With the conservative box test no hit inside [tmin, tmax] can be lost.
+// value with opposite sign in both triangles). An edge function counts as negative or positive only beyond its FP32
+// rounding bound e = 1e-6 (Sx Sy' + Sy Sx') (Sx = |P_kx| + |sx P_kz| bounds a sheared coordinate, 1e-6 is about 17
+// ulps against the 10 that the shear, the products and the difference can accumulate), so a ray that exact (or FP64)
+// arithmetic puts inside a triangle is never rejected: no hit inside [tmin, tmax] can be lost. Rays within the bound
+// of an edge may report the neighbouring triangle or a silhouette hit that exact arithmetic just misses.
 struct WtRay { int kx, ky, kz; float sx, sy, sz; };
 __device__ __forceinline__ float comp3(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+static constexpr float kEdgeRel = 1e-6f, kEdgeAbs = 1e-30f;
 
 __device__ __forceinline__ WtRay wt_setup(float3 d) {
     const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
@@ -276,16 +282,15 @@ __device__ __forceinline__ bool wt_leaf(const float4* __restrict__ vt, int first
     for (int t = first; t < first + cnt; t++) {
         const float3 A = xyz(ld4(vt + 3 * t)) - o, B = xyz(ld4(vt + 3 * t + 1)) - o, C = xyz(ld4(vt + 3 * t + 2)) - o;
         const float Az = comp3(A, r.kz), Bz = comp3(B, r.kz), Cz = comp3(C, r.kz);
-        const float Ax = comp3(A, r.kx) - r.sx * Az, Ay = comp3(A, r.ky) - r.sy * Az;
-        const float Bx = comp3(B, r.kx) - r.sx * Bz, By = comp3(B, r.ky) - r.sy * Bz;
-        const float Cx = comp3(C, r.kx) - r.sx * Cz, Cy = comp3(C, r.ky) - r.sy * Cz;
-        float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
-        if (U == 0.f || V == 0.f || W == 0.f) {   // products of floats are exact in double: the signs become exact
-            U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
-            V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
-            W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
-        }
-        if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) continue;
+        const float Akx = comp3(A, r.kx), Aky = comp3(A, r.ky), Bkx = comp3(B, r.kx), Bky = comp3(B, r.ky), Ckx = comp3(C, r.kx), Cky = comp3(C, r.ky);
+        const float pAx = r.sx * Az, pAy = r.sy * Az, pBx = r.sx * Bz, pBy = r.sy * Bz, pCx = r.sx * Cz, pCy = r.sy * Cz;
+        const float Ax = Akx - pAx, Ay = Aky - pAy, Bx = Bkx - pBx, By = Bky - pBy, Cx = Ckx - pCx, Cy = Cky - pCy;
+        const float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+        const float SAx = fabsf(Akx) + fabsf(pAx), SAy = fabsf(Aky) + fabsf(pAy), SBx = fabsf(Bkx) + fabsf(pBx), SBy = fabsf(Bky) + fabsf(pBy);
+        const float SCx = fabsf(Ckx) + fabsf(pCx), SCy = fabsf(Cky) + fabsf(pCy);
+        const float eU = kEdgeRel * (SCx * SBy + SCy * SBx) + kEdgeAbs, eV = kEdgeRel * (SAx * SCy + SAy * SCx) + kEdgeAbs;
+        const float eW = kEdgeRel * (SBx * SAy + SBy * SAx) + kEdgeAbs;
+        if ((U < -eU || V < -eV || W < -eW) && (U > eU || V > eV || W > eW)) continue;
         const float det = U + V + W;
         if (det == 0.f) continue;
         const float T = U * (r.sz * Az) + V * (r.sz * Bz) + W * (r.sz * Cz);
@@ -299,15 +304,23 @@ __device__ __forceinline__ bool wt_leaf(const float4* __restrict__ vt, int first
 
 __device__ __forceinline__ __half2 h2_of_bits(unsigned u) { __half2 h; memcpy(&h, &u, 4); return h; }
 
-// outward-rounded f16 bases of one axis (see above); an axis outside the f16 range is left unconstrained
-__device__ __forceinline__ void h16_axis(float A, float B, __half2& lo2, __half2& hi2, __half2& b2) {
+// whether an axis's plane distances stay inside the f16 range (see above)
+__device__ __forceinline__ bool h16_ok(float A, float B) {
     const float m = (fabsf(A) + 2048.f * fabsf(B)) * (1.f / 512.f) + 1e-4f, Ap = A - 1024.f * B;   // + 1e-4: f16 subnormal spacing
-    if (fabsf(B) * 1279.f < 30000.f && fabsf(Ap) + m < 30000.f) {
-        const __half lo = __float2half_rd(Ap - m), hi = __float2half_ru(Ap + m), b = __float2half_rn(B);
-        lo2 = __halves2half2(lo, lo); hi2 = __halves2half2(hi, hi); b2 = __halves2half2(b, b);
-    } else {
-        lo2 = h2_of_bits(0xFC00FC00u); hi2 = h2_of_bits(0x7C007C00u); b2 = h2_of_bits(0u);   // -inf, +inf, 0
-    }
+    return fabsf(B) * 1279.f < 30000.f && fabsf(Ap) + m < 30000.f;
+}
+// outward-rounded f16 bases of one axis
+__device__ __forceinline__ void h16_axis(float A, float B, __half2& lo2, __half2& hi2, __half2& b2) {
+    const float m = (fabsf(A) + 2048.f * fabsf(B)) * (1.f / 512.f) + 1e-4f, Ap = A - 1024.f * B;
+    const __half lo = __float2half_rd(Ap - m), hi = __float2half_ru(Ap + m), b = __float2half_rn(B);
+    lo2 = __halves2half2(lo, lo); hi2 = __halves2half2(hi, hi); b2 = __halves2half2(b, b);
+}
+// widened FP32 bases of one axis (nodes outside the f16 range)
+__device__ __forceinline__ void f32_axis(float A, float B, float& lo, float& hi, float& b) {
+    if (fabsf(A) < 1e30f && fabsf(B) < 1e30f) {
+        const float m = (fabsf(A) + 256.f * fabsf(B)) * 9.5367431640625e-7f + 1e-30f;   // 2^-20
+        lo = A - m; hi = A + m; b = B;
+    } else { lo = -INFINITY; hi = INFINITY; b = 0.f; }
 }
 
 template <bool ANY, int TRI>
@@ -328,30 +341,44 @@ struct TravState<16, ANY, TRI> {
         const unsigned ew = __float_as_uint(f0.w);
         const unsigned imask = ew >> 24, m0 = __float_as_uint(f1.z), m1 = __float_as_uint(f1.w);
         const int childBase = __float_as_int(f1.x), triBase = __float_as_int(f1.y);
-        __half2 xlo, xhi, xb, ylo, yhi, yb, zlo, zhi, zb;
-        h16_axis((f0.x - o.x) * idx, __uint_as_float((ew & 255u) << 23) * idx, xlo, xhi, xb);
-        h16_axis((f0.y - o.y) * idy, __uint_as_float(((ew >> 8) & 255u) << 23) * idy, ylo, yhi, yb);
-        h16_axis((f0.z - o.z) * idz, __uint_as_float(((ew >> 16) & 255u) << 23) * idz, zlo, zhi, zb);
+        const float Ax = (f0.x - o.x) * idx, Bx = __uint_as_float((ew & 255u) << 23) * idx;
+        const float Ay = (f0.y - o.y) * idy, By = __uint_as_float(((ew >> 8) & 255u) << 23) * idy;
+        const float Az = (f0.z - o.z) * idz, Bz = __uint_as_float(((ew >> 16) & 255u) << 23) * idz;
         const bool fx = idx < 0.f, fy = idy < 0.f, fz = idz < 0.f;
         const unsigned nx0 = __float_as_uint(fx ? f3_.z : f2.x), nx1 = __float_as_uint(fx ? f3_.w : f2.y), px0 = __float_as_uint(fx ? f2.x : f3_.z), px1 = __float_as_uint(fx ? f2.y : f3_.w);
         const unsigned ny0 = __float_as_uint(fy ? f4_.x : f2.z), ny1 = __float_as_uint(fy ? f4_.y : f2.w), py0 = __float_as_uint(fy ? f2.z : f4_.x), py1 = __float_as_uint(fy ? f2.w : f4_.y);
         const unsigned nz0 = __float_as_uint(fz ? f4_.z : f3_.x), nz1 = __float_as_uint(fz ? f4_.w : f3_.y), pz0 = __float_as_uint(fz ? f3_.x : f4_.z), pz1 = __float_as_uint(fz ? f3_.y : f4_.w);
-        const __half tmn = __float2half_rd(tmin), tmx = __float2half_ru(hitT);
-        const __half2 tmin2 = __halves2half2(tmn, tmn), tmax2 = __halves2half2(tmx, tmx);
         unsigned boxHit = 0;
+        if (h16_ok(Ax, Bx) && h16_ok(Ay, By) && h16_ok(Az, Bz)) {
+            __half2 xlo, xhi, xb, ylo, yhi, yb, zlo, zhi, zb;
+            h16_axis(Ax, Bx, xlo, xhi, xb); h16_axis(Ay, By, ylo, yhi, yb); h16_axis(Az, Bz, zlo, zhi, zb);
+            const __half tmn = __float2half_rd(tmin), tmx = __float2half_ru(hitT);
+            const __half2 tmin2 = __halves2half2(tmn, tmn), tmax2 = __halves2half2(tmx, tmx);
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const unsigned sel = (j & 1) ? 0x4342u : 0x4140u;   // bytes (2j, 2j+1) of the word, each under 0x64: halves 1024 + q
-            const __half2 xn = __hfma2(h2_of_bits(__byte_perm(j < 2 ? nx0 : nx1, 0x64646464u, sel)), xb, xlo);
-            const __half2 xf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? px0 : px1, 0x64646464u, sel)), xb, xhi);
-            const __half2 yn = __hfma2(h2_of_bits(__byte_perm(j < 2 ? ny0 : ny1, 0x64646464u, sel)), yb, ylo);
-            const __half2 yf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? py0 : py1, 0x64646464u, sel)), yb, yhi);
-            const __half2 zn = __hfma2(h2_of_bits(__byte_perm(j < 2 ? nz0 : nz1, 0x64646464u, sel)), zb, zlo);
-            const __half2 zf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? pz0 : pz1, 0x64646464u, sel)), zb, zhi);
-            const __half2 tn = __hmax2(__hmax2(xn, yn), __hmax2(zn, tmin2));
-            const __half2 tf = __hmin2(__hmin2(xf, yf), __hmin2(zf, tmax2));
-            const unsigned m = __hle2_mask(tn, tf);
-            boxHit |= ((m & 1u) << (2 * j)) | (((m >> 16) & 1u) << (2 * j + 1));
+            for (int j = 0; j < 4; j++) {
+                const unsigned sel = (j & 1) ? 0x4342u : 0x4140u;   // bytes (2j, 2j+1) of the word, each under 0x64: halves 1024 + q
+                const __half2 xn = __hfma2(h2_of_bits(__byte_perm(j < 2 ? nx0 : nx1, 0x64646464u, sel)), xb, xlo);
+                const __half2 xf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? px0 : px1, 0x64646464u, sel)), xb, xhi);
+                const __half2 yn = __hfma2(h2_of_bits(__byte_perm(j < 2 ? ny0 : ny1, 0x64646464u, sel)), yb, ylo);
+                const __half2 yf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? py0 : py1, 0x64646464u, sel)), yb, yhi);
+                const __half2 zn = __hfma2(h2_of_bits(__byte_perm(j < 2 ? nz0 : nz1, 0x64646464u, sel)), zb, zlo);
+                const __half2 zf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? pz0 : pz1, 0x64646464u, sel)), zb, zhi);
+                const __half2 tn = __hmax2(__hmax2(xn, yn), __hmax2(zn, tmin2));
+                const __half2 tf = __hmin2(__hmin2(xf, yf), __hmin2(zf, tmax2));
+                const unsigned m = __hle2_mask(tn, tf);
+                boxHit |= ((m & 1u) << (2 * j)) | (((m >> 16) & 1u) << (2 * j + 1));
+            }
+        } else {
+            float xlo, xhi, xb, ylo, yhi, yb, zlo, zhi, zb;
+            f32_axis(Ax, Bx, xlo, xhi, xb); f32_axis(Ay, By, ylo, yhi, yb); f32_axis(Az, Bz, zlo, zhi, zb);
+#pragma unroll
+            for (int s = 0; s < 8; s++) {
+                const float xn = fmaf(qbyte(s < 4 ? nx0 : nx1, s), xb, xlo), xf = fmaf(qbyte(s < 4 ? px0 : px1, s), xb, xhi);
+                const float yn = fmaf(qbyte(s < 4 ? ny0 : ny1, s), yb, ylo), yf = fmaf(qbyte(s < 4 ? py0 : py1, s), yb, yhi);
+                const float zn = fmaf(qbyte(s < 4 ? nz0 : nz1, s), zb, zlo), zf = fmaf(qbyte(s < 4 ? pz0 : pz1, s), zb, zhi);
+                const float tn = fmaxf(fmaxf(xn, yn), fmaxf(zn, tmin)), tf = fminf(fminf(xf, yf), fminf(zf, hitT));
+                boxHit |= (tn <= tf ? 1u : 0u) << s;
+            }
         }
         const unsigned leafMask = ((m0 >> 7) & 1u) | ((m0 >> 14) & 2u) | ((m0 >> 21) & 4u) | ((m0 >> 28) & 8u) |
                                   ((m1 >> 3) & 16u) | ((m1 >> 10) & 32u) | ((m1 >> 17) & 64u) | ((m1 >> 24) & 128u);

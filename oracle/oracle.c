@@ -20,6 +20,8 @@
  *                                  leaf tests, in slot order; descent order as the reference)
  *   camera ray + legacy shading .. render/wavefront.cu:42-58, 94-136, frame loop 684-741
  *   FP64 watertight reference .... not in the reference (precision-form oracle; Woop, Benthin & Wald, JCGT 2013)
+ *   precision form ............... not in the reference (f16x2 conservative slabs + watertight FP32 triangles, the
+ *                                  CUDA precision form restated with exact f16 emulation)
  */
 #include <float.h>
 #include <math.h>
@@ -615,4 +617,140 @@ long orc_trace_fp64(const float* nodes, const float* vt, int n_tris, const float
         t_out[i] = hitT; tri_out[i] = hit;
     }
     return 0;
+}
+
+/* ------------------------------------------------------------------ precision form, restated bit for bit
+ * Not in the reference. The CUDA precision form (f16x2 conservative slab tests over the CWBVH, watertight FP32
+ * triangle test on the exact corners) with every f16 operation emulated exactly: a product of two halves is exact in
+ * double and the sum with a third is exact or far from a rounding midpoint, so rounding the double result once to the
+ * nearest half gives the hardware's fused multiply-add; conversions round down / up / to nearest as the kernel asks.
+ * Closest: hits float4 (t, u, v, tri bits); any: occ = first occluder or -1. stats as orc_trace. */
+static double hround(double x, int mode) { /* mode 0 nearest-even, -1 toward -inf, +1 toward +inf */
+    if (x != x || isinf(x) || x == 0.0) return x;
+    const int neg = x < 0.0; const double a = fabs(x);
+    int e; frexp(a, &e); int ex = e - 1; if (ex < -14) ex = -14;
+    const double qn = ldexp(1.0, ex - 10), k = a / qn, kf = floor(k), r = k - kf;
+    int up;
+    if (mode == 0) up = r > 0.5 || (r == 0.5 && fmod(kf, 2.0) == 1.0);
+    else up = r > 0.0 && ((mode > 0) != neg);
+    double m = (kf + up) * qn;
+    if (m > 65504.0) m = (mode == 0 || up) ? INFINITY : 65504.0;
+    return neg ? -m : m;
+}
+static double hfma(double a, double b, double c) { return hround(a * b + c, 0); }
+double orc_half_round(double x, int mode) { return hround(x, mode); }
+static int h16_ok(float A, float B) {
+    const float m = (fabsf(A) + 2048.f * fabsf(B)) * (1.f / 512.f) + 1e-4f, Ap = A - 1024.f * B;
+    return fabsf(B) * 1279.f < 30000.f && fabsf(Ap) + m < 30000.f;
+}
+static void h16_axis(float A, float B, double* lo, double* hi, double* b) {
+    const float m = (fabsf(A) + 2048.f * fabsf(B)) * (1.f / 512.f) + 1e-4f, Ap = A - 1024.f * B;
+    *lo = hround(Ap - m, -1); *hi = hround(Ap + m, 1); *b = hround(B, 0);
+}
+static void f32_axis(float A, float B, float* lo, float* hi, float* b) {
+    if (fabsf(A) < 1e30f && fabsf(B) < 1e30f) { const float m = (fabsf(A) + 256.f * fabsf(B)) * 9.5367431640625e-7f + 1e-30f; *lo = A - m; *hi = A + m; *b = B; }
+    else { *lo = -INFINITY; *hi = INFINITY; *b = 0.f; }
+}
+typedef struct { int kx, ky, kz; float sx, sy, sz; } WtRay;
+static WtRay wt_setup(V3 d) {
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    WtRay r; r.kz = ax >= ay ? (ax >= az ? 0 : 2) : (ay >= az ? 1 : 2);
+    r.kx = r.kz == 2 ? 0 : r.kz + 1; r.ky = r.kx == 2 ? 0 : r.kx + 1;
+    if (comp(d, r.kz) < 0.f) { int t = r.kx; r.kx = r.ky; r.ky = t; }
+    const float dz = comp(d, r.kz);
+    r.sx = comp(d, r.kx) / dz; r.sy = comp(d, r.ky) / dz; r.sz = 1.f / dz;
+    return r;
+}
+static int wt_leaf(const V4* vt, int first, int cnt, V3 o, const WtRay* r, float tmin, int any, float* hitT, int* hitTri, float* hu, float* hv, Stats* st) {
+    for (int t = first; t < first + cnt; t++) {
+        if (st) st->tris++;
+        const V3 A = sub(xyz4(vt[3 * t]), o), B = sub(xyz4(vt[3 * t + 1]), o), C = sub(xyz4(vt[3 * t + 2]), o);
+        const float Az = comp(A, r->kz), Bz = comp(B, r->kz), Cz = comp(C, r->kz);
+        const float Akx = comp(A, r->kx), Aky = comp(A, r->ky), Bkx = comp(B, r->kx), Bky = comp(B, r->ky), Ckx = comp(C, r->kx), Cky = comp(C, r->ky);
+        const float pAx = r->sx * Az, pAy = r->sy * Az, pBx = r->sx * Bz, pBy = r->sy * Bz, pCx = r->sx * Cz, pCy = r->sy * Cz;
+        const float Ax = Akx - pAx, Ay = Aky - pAy, Bx = Bkx - pBx, By = Bky - pBy, Cx = Ckx - pCx, Cy = Cky - pCy;
+        const float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+        const float SAx = fabsf(Akx) + fabsf(pAx), SAy = fabsf(Aky) + fabsf(pAy), SBx = fabsf(Bkx) + fabsf(pBx), SBy = fabsf(Bky) + fabsf(pBy);
+        const float SCx = fabsf(Ckx) + fabsf(pCx), SCy = fabsf(Cky) + fabsf(pCy);
+        const float eU = 1e-6f * (SCx * SBy + SCy * SBx) + 1e-30f, eV = 1e-6f * (SAx * SCy + SAy * SCx) + 1e-30f, eW = 1e-6f * (SBx * SAy + SBy * SAx) + 1e-30f;
+        if ((U < -eU || V < -eV || W < -eW) && (U > eU || V > eV || W > eW)) continue;
+        const float det = U + V + W;
+        if (det == 0.f) continue;
+        const float T = U * (r->sz * Az) + V * (r->sz * Bz) + W * (r->sz * Cz);
+        const float tt = T / det;
+        if (!(tt > tmin && tt < *hitT)) continue;
+        *hitT = tt; *hitTri = t; *hu = V / det; *hv = W / det;
+        if (any) return 1;
+    }
+    return 0;
+}
+static int trav_prec(const V4* nodes, const V4* vt, V3 o, V3 d, float tmin, int any, float* hitT, int* hitTri, float* hu, float* hv, Stats* st) {
+    unsigned stk[40][2]; int sp = 0, node = 0;
+    const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z);
+    const unsigned oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
+    const WtRay wt = wt_setup(d);
+    unsigned cb = 0, im = 0, hm = 0;
+    for (;;) {
+        if (st) st->nodes++;
+        const V4* nb = nodes + 5 * node;
+        const V4 f0 = nb[0], f1 = nb[1];
+        const unsigned ew = fu(f0.w), imask = ew >> 24, m0 = fu(f1.z), m1 = fu(f1.w);
+        const int childBase = fi(f1.x), triBase = fi(f1.y);
+        const unsigned* q = (const unsigned*)(nb + 2);   /* lo.x[2], lo.y[2], lo.z[2], hi.x[2], hi.y[2], hi.z[2] */
+        const float A[3] = { (f0.x - o.x) * idx, (f0.y - o.y) * idy, (f0.z - o.z) * idz };
+        const float Bq[3] = { uf((ew & 255u) << 23) * idx, uf(((ew >> 8) & 255u) << 23) * idy, uf(((ew >> 16) & 255u) << 23) * idz };
+        const int flip[3] = { idx < 0.f, idy < 0.f, idz < 0.f };
+        unsigned boxHit = 0;
+        if (h16_ok(A[0], Bq[0]) && h16_ok(A[1], Bq[1]) && h16_ok(A[2], Bq[2])) {   /* f16 slabs */
+            double lo[3], hi[3], b[3];
+            for (int ax = 0; ax < 3; ax++) h16_axis(A[ax], Bq[ax], &lo[ax], &hi[ax], &b[ax]);
+            const double tmn = hround(tmin, -1), tmx = hround(*hitT, 1);
+            for (int s = 0; s < 8; s++) {
+                const int w = s < 4 ? 0 : 1; double tn = tmn, tf = tmx;
+                for (int ax = 0; ax < 3; ax++) {
+                    const unsigned qlo = byte_of(q[2 * ax + w], s), qhi = byte_of(q[6 + 2 * ax + w], s);
+                    const double n = hfma(1024.0 + (flip[ax] ? qhi : qlo), b[ax], lo[ax]), f = hfma(1024.0 + (flip[ax] ? qlo : qhi), b[ax], hi[ax]);
+                    tn = fmax(tn, n); tf = fmin(tf, f);
+                }
+                if (tn <= tf) boxHit |= 1u << s;
+            }
+        } else {   /* FP32 slabs, widened */
+            float lo[3], hi[3], b[3];
+            for (int ax = 0; ax < 3; ax++) f32_axis(A[ax], Bq[ax], &lo[ax], &hi[ax], &b[ax]);
+            for (int s = 0; s < 8; s++) {
+                const int w = s < 4 ? 0 : 1; float n3[3], f3[3];
+                for (int ax = 0; ax < 3; ax++) {
+                    const unsigned qlo = byte_of(q[2 * ax + w], s), qhi = byte_of(q[6 + 2 * ax + w], s);
+                    n3[ax] = fmaf((float)(flip[ax] ? qhi : qlo), b[ax], lo[ax]); f3[ax] = fmaf((float)(flip[ax] ? qlo : qhi), b[ax], hi[ax]);
+                }
+                const float tn = fmaxf(fmaxf(n3[0], n3[1]), fmaxf(n3[2], tmin)), tf = fminf(fminf(f3[0], f3[1]), fminf(f3[2], *hitT));
+                if (tn <= tf) boxHit |= 1u << s;
+            }
+        }
+        unsigned hits = 0;
+        for (int s = 0; s < 8; s++) {
+            if (!(boxHit & (1u << s))) continue;
+            const unsigned m = byte_of(s < 4 ? m0 : m1, s);
+            if (m & 0x80u) {
+                if (wt_leaf(vt, triBase + (int)(m & 31u), (int)((m >> 5) & 3u) + 1, o, &wt, tmin, any, hitT, hitTri, hu, hv, st) && any) return 1;
+            }
+        }
+        for (int s = 0; s < 8; s++) if ((boxHit & imask) & (1u << s)) hits |= 1u << (s ^ oct);
+        if (hits) { if (hm) { if (sp == 40) return -1; stk[sp][0] = cb; stk[sp][1] = (im << 8) | hm; sp++; } cb = (unsigned)childBase; im = imask; hm = hits; }
+        while (hm == 0) { if (sp == 0) return *hitTri >= 0; sp--; cb = stk[sp][0]; im = stk[sp][1] >> 8; hm = stk[sp][1] & 255u; }
+        const unsigned k = (unsigned)__builtin_ctz(hm); hm &= hm - 1;
+        node = (int)cb + __builtin_popcount(im & ((1u << (k ^ oct)) - 1u));
+    }
+}
+long orc_trace_prec(const float* nodes, const float* vt, const float* ro, const float* rd, long n, int any, float* hits, int* occ, long long* stats) {
+    long bad = 0; Stats st = { 0, 0 };
+    for (long i = 0; i < n; i++) {
+        const V3 o = v3(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]), d = v3(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]);
+        float t = rd[4 * i + 3], u = 0.f, v = 0.f; int tri = -1;
+        if (trav_prec((const V4*)nodes, (const V4*)vt, o, d, ro[4 * i + 3], any, &t, &tri, &u, &v, stats ? &st : NULL) < 0) bad++;
+        if (any) occ[i] = tri;
+        else { hits[4 * i] = t; hits[4 * i + 1] = u; hits[4 * i + 2] = v; memcpy(&hits[4 * i + 3], &tri, 4); }
+    }
+    if (stats) { stats[0] = st.nodes; stats[1] = st.tris; }
+    return bad;
 }

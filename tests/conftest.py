@@ -47,6 +47,10 @@ def _load_oracle():
     L.orc_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
     L.orc_trace_fp64.restype = C.c_long
     L.orc_trace_fp64.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p]
+    L.orc_trace_prec.restype = C.c_long
+    L.orc_trace_prec.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_half_round.restype = C.c_double
+    L.orc_half_round.argtypes = [C.c_double, C.c_int]
     L.orc_rng.restype = C.c_float
     L.orc_rng.argtypes = [C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint]
     return L
@@ -94,6 +98,18 @@ class Oracle:
                                   np.ascontiguousarray(o).ctypes.data, np.ascontiguousarray(d).ctypes.data, n, 1 if any_hit else 0, t.ctypes.data, tri.ctypes.data)
         assert r == 0
         return t, tri
+
+    def trace_prec(self, nodes, verts, o, d, any_hit=False, stats=False):
+        """The precision form (f16 conservative slabs + watertight FP32 triangles) restated with exact f16 emulation:
+        closest hits float4 (t, u, v, tri bits) or first occluders, bit for bit what the CUDA precision form returns."""
+        n = len(o)
+        hits = np.zeros((n, 4), np.float32); occ = np.zeros(n, np.int32); st = np.zeros(2, np.int64)
+        bad = self.L.orc_trace_prec(np.ascontiguousarray(nodes).ctypes.data, np.ascontiguousarray(verts, np.float32).ctypes.data,
+                                    np.ascontiguousarray(o).ctypes.data, np.ascontiguousarray(d).ctypes.data, n, 1 if any_hit else 0,
+                                    hits.ctypes.data, occ.ctypes.data, st.ctypes.data if stats else None)
+        assert bad == 0
+        res = occ if any_hit else hits
+        return (res, st) if stats else res
 
     def render(self, params, variant, tri, bvh, bounces, spp, s_base=0, pix0=0, pix1=None):
         w, h = params.cam.w, params.cam.h
@@ -156,6 +172,11 @@ def gpu():
     import torch
     torch.cuda.init()
     return torch
+
+
+from importlib import import_module as _im
+_pc = _im("cuda-wavefront-pathtracer_b200.precision_check")
+classify_vs_fp64, wt32, edge_excess = _pc.classify_vs_fp64, _pc.wt32, _pc.edge_excess
 
 
 def golden(name):

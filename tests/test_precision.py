@@ -3,7 +3,7 @@ brute force over every triangle finds (so the conservative double-precision box 
 import numpy as np
 import pytest
 
-from conftest import golden
+from conftest import classify_vs_fp64, edge_excess, golden, wt32
 
 
 def test_fp64_bvh_equals_brute_force_fixture(cwp, oracle):
@@ -31,3 +31,63 @@ def test_exact_corner_buffer(cwp):
     v, f, _, _ = mesh.arrays()
     want = v[f[bvh.order]].reshape(-1, 3)
     assert np.array_equal(bvh.verts[:, :3], want) and np.all(bvh.verts[:, 3] == 0)
+
+
+def test_half_rounding_emulation(oracle):
+    """The oracle's f16 rounding (to nearest even, down, up) agrees with numpy's float16 conversion and brackets every
+    value between adjacent halves, across normal, subnormal and overflowing magnitudes."""
+    rng = np.random.default_rng(2)
+    xs = np.concatenate([rng.normal(size=4000) * 10.0 ** rng.integers(-9, 6, 4000), [0.0, 65504.0, 65519.9, 65520.0, 7e4, -7e4, 2 ** -24, 3 * 2 ** -26, 1025.5, 1026.5]])
+    hr = oracle.L.orc_half_round
+    with np.errstate(over="ignore"):
+        for x in xs:
+            rn, rd, ru = hr(float(x), 0), hr(float(x), -1), hr(float(x), 1)
+            assert rn == float(np.float16(x)) or (np.isinf(rn) and np.isinf(np.float16(x))), x
+            assert rd <= x <= ru, x
+            for r in (rd, ru):
+                assert np.isinf(r) or float(np.float16(r)) == r, x
+            if rd != ru and np.isfinite(rd) and np.isfinite(ru):
+                assert np.nextafter(np.float16(rd), np.float16(np.inf)) == np.float16(ru), x
+
+
+def test_precision_restatement_against_fp64_12k(cwp, oracle):
+    """The precision form restated on the host (f16 conservative slabs, watertight FP32 triangles): no hit the FP64
+    oracle finds is lost, different triangles only at equal distance, t within 1e-6 of max(t, scene extent), and
+    the conservative box test costs at most 1.5x the plain form's node visits."""
+    mesh, bvh = cwp.scene("boxes12k", variant=8, bins=32)
+    p = cwp.frame_params(mesh, 256, 256)
+    o, d = cwp.incoherent_rays(20000, p, bvh.tris, lambda o, d: oracle.trace(8, 1, False, bvh.nodes, bvh.woop, o, d), seed=29)
+    h, st = oracle.trace_prec(bvh.nodes, bvh.verts, o, d, stats=True)
+    _, st_plain = oracle.trace(8, 1, False, bvh.nodes, bvh.woop, o, d, stats=True)
+    t64, i64 = oracle.trace_fp64(bvh.nodes, bvh.verts, o, d)
+    ext = float(np.ptp(mesh.arrays()[0], axis=0).max())
+    c = classify_vs_fp64(h, t64, i64, ext, o=o, d=d, verts=bvh.verts)
+    assert c["lost"] == 0 and c["max_t_error"] <= 1e-6, c
+    ih = h[:, 3].view(np.int32); k = ih >= 0
+    acc, t32 = wt32(o[k], d[k], bvh.verts, ih[k])   # the numpy mirror of the FP32 triangle test agrees bit for bit
+    assert acc.all() and np.array_equal(t32, h[k, 0])
+    ex = c["extra_mask"]
+    assert np.all(edge_excess(o[ex], d[ex], bvh.verts, h[ex, 3].view(np.int32)) <= 1.0)
+    assert st[0] <= 1.5 * st_plain[0]
+    occ = oracle.trace_prec(bvh.nodes, bvh.verts, o, d, any_hit=True)
+    assert np.all(occ[i64 >= 0] >= 0)
+
+
+def test_precision_restatement_corners_and_edges(cwp, oracle):
+    """Rays aimed exactly at corners and edge midpoints: the conservative FP32 edge test never loses a hit that the
+    FP64 oracle finds; the hits FP64 does not report lie within the edge bound of the reported triangle."""
+    mesh, bvh = cwp.scene("boxes12k", variant=8, bins=32)
+    v, f, _, _ = mesh.arrays()
+    rng = np.random.default_rng(5)
+    tri = v[f[rng.choice(len(f), 4000)]]
+    targets = np.concatenate([tri[:, 0], 0.5 * (tri[:, 0] + tri[:, 1]), 0.5 * (tri[:, 1] + tri[:, 2])]).astype(np.float32)
+    dirs = rng.normal(size=targets.shape).astype(np.float32); dirs[:, 2] = -np.abs(dirs[:, 2]) - 0.2
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    o = np.zeros((len(targets), 4), np.float32); o[:, :3] = targets - 30.0 * dirs
+    d = np.zeros((len(targets), 4), np.float32); d[:, :3] = dirs; d[:, 3] = 1e30
+    t64, i64 = oracle.trace_fp64(bvh.nodes, bvh.verts, o, d)
+    h = oracle.trace_prec(bvh.nodes, bvh.verts, o, d)
+    c = classify_vs_fp64(h, t64, i64, float(np.ptp(v, axis=0).max()), o=o, d=d, verts=bvh.verts)
+    assert c["lost"] == 0, c
+    ex = c["extra_mask"]
+    assert np.all(edge_excess(o[ex], d[ex], bvh.verts, h[ex, 3].view(np.int32)) <= 1.0)
