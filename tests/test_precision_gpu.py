@@ -70,7 +70,9 @@ def test_precision_form_loses_no_hit_1m(gpu, cwp, scene12k):
     assert np.all(edge_excess(o[ex], d[ex], bvh.verts, h[ex, 3].view(np.int32)) <= 1.0)
     occ = run(gpu, acc, o, d, any_hit=True)
     _, o64 = run64(gpu, acc, o, d, any_hit=True)
-    assert np.array_equal(occ >= 0, o64 >= 0)
+    assert np.all(occ[o64 >= 0] >= 0)                      # no occluder lost
+    extra = (occ >= 0) & (o64 < 0)                         # occluders within the edge bound of a silhouette
+    assert np.all(edge_excess(o[extra], d[extra], bvh.verts, occ[extra]) <= 1.0)
 
 
 def test_watertight_on_shared_edges_and_corners(gpu, cwp, scene12k):
