@@ -77,6 +77,28 @@ class RendererInfo(C.Structure):
     _fields_ = [("vram_mb", C.c_double), ("tlas_ms", C.c_double), ("pt_blocks", C.c_int32), ("n_sm", C.c_int32), ("gpu_name", C.c_char * 256)]
 
 
+class Instance(C.Structure):
+    _fields_ = [("inv", C.c_float * 12), ("fwd", C.c_float * 12), ("root", C.c_int32), ("mesh", C.c_int32), ("det_sign", C.c_float), ("pad", C.c_int32)]
+
+
+class InstanceDesc(C.Structure):
+    _fields_ = [("mesh", C.c_int32), ("translate", C.c_float * 3), ("translate_per_frame", C.c_float * 3), ("axis", C.c_float * 3),
+                ("angle_deg", C.c_float), ("angle_deg_per_frame", C.c_float), ("scale", C.c_float * 3), ("scale_per_frame", C.c_float * 3)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("device", C.c_int32), ("leaf", C.c_int32), ("widths", C.c_int32), ("reserved", C.c_int32 * 5)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("block", C.c_int32), ("width", C.c_int32), ("fetch", C.c_int32), ("smem_stack", C.c_int32), ("ms", C.c_float), ("reserved", C.c_int32 * 3)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("n_blas", C.c_int32), ("n_scenes", C.c_int32), ("n_tris", C.c_int64), ("n_instances", C.c_int64), ("node_bytes", C.c_int64 * 3),
+                ("blas_build_ms", C.c_double), ("tlas_build_ms", C.c_double), ("blas_hploc_launches", C.c_int32), ("pad", C.c_int32)]
+
+
 # every exported symbol of the C ABI with its ctypes signature (restype, argtypes)
 SIGNATURES = {
     "cwp_last_error": (C.c_char_p, []),
@@ -112,6 +134,21 @@ SIGNATURES = {
     "cwp_renderer_destroy": (None, [C.c_void_p]),
     "cwp_render_noalloc": (C.c_int, [C.POINTER(Params), C.POINTER(DeviceScene), C.POINTER(RenderOptions), C.c_int32, C.c_int32, C.c_int32,
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cwp_xform_invert": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "cwp_xform_animate": (C.c_int, [C.POINTER(InstanceDesc), C.c_int32, C.POINTER(C.c_float)]),
+    "cwp_instance_from_xform": (C.c_int, [C.POINTER(C.c_float), C.c_int32, C.POINTER(Instance)]),
+    "cwp_batch_create": (C.c_int, [C.POINTER(MeshView), C.c_int32, C.POINTER(BatchOptions), C.POINTER(C.c_void_p)]),
+    "cwp_batch_destroy": (None, [C.c_void_p]),
+    "cwp_batch_set_scenes": (C.c_int, [C.c_void_p, C.POINTER(Instance), C.c_int64, C.POINTER(C.c_int32), C.c_int32]),
+    "cwp_batch_trace": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    "cwp_batch_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(BatchTuning)]),
+    "cwp_batch_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
+    "cwp_batch_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
+    "cwp_batch_info_of": (C.c_int, [C.c_void_p, C.POINTER(BatchInfo)]),
+    "cwp_batch_download": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int64), C.c_void_p, C.POINTER(C.c_int64)]),
+    "cwp_batch_blas_root": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "cwp_batch_download_tlas": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64), C.c_void_p, C.c_void_p]),
+    "cwp_batch_status": (C.c_int, [C.c_void_p]),
     "cwp_camera_look_at": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_camera_from_c2w": (C.c_int, [C.POINTER(C.c_float), C.c_float, C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_params_defaults": (C.c_int, [C.POINTER(Params)]),
@@ -368,6 +405,95 @@ class Renderer:
     def __del__(self):
         if _lib is not None:
             self.close()
+
+
+def xform_invert(m):
+    """FP64 inverse of a 3x4 row-major affine map, rounded to float: (inv [12] float32, det sign)."""
+    m = np.ascontiguousarray(m, np.float32).reshape(12)
+    inv = np.zeros(12, np.float32); sg = C.c_float()
+    _check(lib().cwp_xform_invert(_fptr(m), _fptr(inv), C.byref(sg)))
+    return inv, sg.value
+
+
+def xform_animate(mesh, frame=0, translate=(0, 0, 0), axis=(0, 0, 1), angle_deg=0.0, scale=(1, 1, 1),
+                  translate_per_frame=(0, 0, 0), angle_deg_per_frame=0.0, scale_per_frame=(0, 0, 0)):
+    """3x4 object -> world map of an animated instance at a frame (translate . rotate(axis, angle) . scale)."""
+    d = InstanceDesc(mesh, (C.c_float * 3)(*translate), (C.c_float * 3)(*translate_per_frame), (C.c_float * 3)(*axis), angle_deg,
+                     angle_deg_per_frame, (C.c_float * 3)(*scale), (C.c_float * 3)(*scale_per_frame))
+    m = np.zeros(12, np.float32)
+    _check(lib().cwp_xform_animate(C.byref(d), frame, _fptr(m)))
+    return m
+
+
+def instances(xforms, meshes):
+    """Array of cwp_instance records (numpy structured bytes, 112 B each) from 3x4 maps and mesh indices."""
+    xforms = np.ascontiguousarray(xforms, np.float32).reshape(-1, 12)
+    out = (Instance * len(xforms))()
+    for i, (m, k) in enumerate(zip(xforms, meshes)):
+        _check(lib().cwp_instance_from_xform(_fptr(np.ascontiguousarray(m)), int(k), C.byref(out[i])))
+    return out
+
+
+class Batch:
+    """Batched form: many meshes built on the GPU at once (segmented H-PLOC, BVH2 / BVH4 / CWBVH encodings), many
+    two-level scenes, one persistent launch over a scene-tagged ray queue, and the launch-shape autotuner."""
+
+    def __init__(self, meshes, device=0, leaf=4, widths=0):
+        arrs, views = [], (MeshView * len(meshes))()
+        for i, m in enumerate(meshes):
+            v, f, fm, _ = m.arrays() if isinstance(m, Mesh) else m
+            v = np.ascontiguousarray(v, np.float32); f = np.ascontiguousarray(f, np.int32)
+            fm = np.ascontiguousarray(fm if fm is not None else np.zeros(len(f)), np.int32)
+            arrs += [v, f, fm]
+            views[i].verts, views[i].n_verts, views[i].faces, views[i].n_tris, views[i].face_mat = _fptr(v), len(v), _iptr(f), len(f), _iptr(fm)
+        o = BatchOptions(device, leaf, widths)
+        h = C.c_void_p()
+        _check(lib().cwp_batch_create(views, len(meshes), C.byref(o), C.byref(h)))
+        self._h = h
+
+    def set_scenes(self, inst, scene_first):
+        first = np.ascontiguousarray(scene_first, np.int32)
+        _check(lib().cwp_batch_set_scenes(self._h, inst, len(inst), _iptr(first), len(first) - 1))
+
+    def trace(self, d_o, d_d, d_scene, d_hits, d_inst, n, any_hit=False, stream=None):
+        _check(lib().cwp_batch_trace(self._h, 1 if any_hit else 0, d_o, d_d, d_scene, d_hits, d_inst, n, stream))
+
+    def autotune(self, d_o, d_d, d_scene, d_hits, d_inst, n):
+        t = BatchTuning()
+        _check(lib().cwp_batch_autotune(self._h, d_o, d_d, d_scene, d_hits, d_inst, n, C.byref(t)))
+        return t
+
+    def set_tuning(self, block=128, width=8, fetch=12, smem_stack=0):
+        t = BatchTuning(block, width, fetch, smem_stack, 0.0)
+        _check(lib().cwp_batch_set_tuning(self._h, C.byref(t)))
+
+    def tuning(self):
+        t = BatchTuning(); _check(lib().cwp_batch_get_tuning(self._h, C.byref(t))); return t
+
+    def info(self):
+        i = BatchInfo(); _check(lib().cwp_batch_info_of(self._h, C.byref(i))); return i
+
+    def status(self):
+        _check(lib().cwp_batch_status(self._h))
+
+    def download(self, width):
+        """(nodes [k,4] float32, tris [3n,4] float32) of one layout"""
+        nn, nt = C.c_int64(), C.c_int64()
+        _check(lib().cwp_batch_download(self._h, width, None, C.byref(nn), None, C.byref(nt)))
+        nodes = np.zeros((nn.value, 4), np.float32); tris = np.zeros((nt.value, 4), np.float32)
+        _check(lib().cwp_batch_download(self._h, width, nodes.ctypes.data, C.byref(nn), tris.ctypes.data, C.byref(nt)))
+        return nodes, tris
+
+    def download_tlas(self, n_scenes, n_inst):
+        """(tlas nodes [4 n_inst, 4], scene roots [n_scenes], instances as float32 [n_inst, 28])"""
+        nn = C.c_int64()
+        nodes = np.zeros((4 * max(n_inst, 1), 4), np.float32); roots = np.zeros(n_scenes, np.int32); inst = np.zeros((max(n_inst, 1), 28), np.float32)
+        _check(lib().cwp_batch_download_tlas(self._h, nodes.ctypes.data, C.byref(nn), roots.ctypes.data, inst.ctypes.data))
+        return nodes[:nn.value], roots, inst[:n_inst]
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.cwp_batch_destroy(self._h); self._h = C.c_void_p()
 
 
 from . import imageio  # noqa: E402,F401

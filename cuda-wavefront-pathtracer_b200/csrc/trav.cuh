@@ -84,7 +84,8 @@ struct TravState<2, ANY, TRI> {
         idx = safe_rcp(d.x); idy = safe_rcp(d.y); idz = safe_rcp(d.z);
         ox = -o.x * idx; oy = -o.y * idy; oz = -o.z * idz;
     }
-    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ tv, Stack& stack, int& err) {
+    template <class S>
+    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ tv, S& stack, int& err) {
         if (--budget < 0) { err |= kTravBudget; return true; }
         const float4* nb = nodes + 4 * (size_t)node;
         const float4 n0 = ld4(nb), n1 = ld4(nb + 1), nz = ld4(nb + 2), mt = ld4(nb + 3);
@@ -119,14 +120,21 @@ __device__ __forceinline__ bool trav_bvh2(const float4* __restrict__ nodes, cons
 
 // ---------------- BVH4 ----------------
 template <bool ANY, int TRI>
-__device__ __forceinline__ bool trav_bvh4(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
-                                          float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
-    int stack[kStack2]; int sp = 0, node = root, budget = kVisitBudget;
-    const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z);
-    const float ox = -o.x * idx, oy = -o.y * idy, oz = -o.z * idz;
-    const float INF = 3.4e38f;
-    while (true) {
-        if (--budget < 0) { err |= kTravBudget; break; }
+struct TravState<4, ANY, TRI> {
+    typedef int Stack[kStack2];
+    float3 o, d; float idx, idy, idz, ox, oy, oz, tmin, hitT, hu, hv; int hitTri, node, sp, budget;
+
+    __device__ __forceinline__ void begin(float3 o_, float3 d_, float tmin_, float tmax_, int root) {
+        o = o_; d = d_; tmin = tmin_; hitT = tmax_; hu = hv = 0.f; hitTri = -1; node = root; sp = 0; budget = kVisitBudget;
+        idx = safe_rcp(d.x); idy = safe_rcp(d.y); idz = safe_rcp(d.z);
+        ox = -o.x * idx; oy = -o.y * idy; oz = -o.z * idz;
+    }
+    // one node: four slab tests, hit leaves tested in child order, hit inner children sorted by entry distance
+    // (traverse.cuh:74-107), the nearest visited next and the others pushed
+    template <class S>
+    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ tv, S& stack, int& err) {
+        const float INF = 3.4e38f;
+        if (--budget < 0) { err |= kTravBudget; return true; }
         const float4* nb = nodes + 8 * (size_t)node;
         const float4 lx = ld4(nb), hx = ld4(nb + 1), ly = ld4(nb + 2), hy = ld4(nb + 3), lz = ld4(nb + 4), hz = ld4(nb + 5), cf = ld4(nb + 6), kf = ld4(nb + 7);
         float ht[4]; int hc[4];
@@ -136,9 +144,9 @@ __device__ __forceinline__ bool trav_bvh4(const float4* __restrict__ nodes, cons
         const int KK[4] = { __float_as_int(kf.x), __float_as_int(kf.y), __float_as_int(kf.z), __float_as_int(kf.w) };
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            float x0 = fmaf(LX[j], idx, ox), x1 = fmaf(HX[j], idx, ox), y0 = fmaf(LY[j], idy, oy), y1 = fmaf(HY[j], idy, oy), z0 = fmaf(LZ[j], idz, oz), z1 = fmaf(HZ[j], idz, oz);
-            float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-            float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), hitT));
+            const float x0 = fmaf(LX[j], idx, ox), x1 = fmaf(HX[j], idx, ox), y0 = fmaf(LY[j], idy, oy), y1 = fmaf(HY[j], idy, oy), z0 = fmaf(LZ[j], idz, oz), z1 = fmaf(HZ[j], idz, oz);
+            const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+            const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), hitT));
             ht[j] = INF; hc[j] = CC[j];
             if (tn <= tf) {
                 if (KK[j] > 0) { if (leaf_hit<ANY, TRI>(tv, CC[j], KK[j], o, d, tmin, hitT, hitTri, hu, hv) && ANY) return true; }
@@ -149,15 +157,32 @@ __device__ __forceinline__ bool trav_bvh4(const float4* __restrict__ nodes, cons
 #define CWPB_CSWAP(a, b) { if (ht[b] < ht[a]) { float tf_ = ht[a]; ht[a] = ht[b]; ht[b] = tf_; int ti_ = hc[a]; hc[a] = hc[b]; hc[b] = ti_; } }
         CWPB_CSWAP(0, 1) CWPB_CSWAP(2, 3) CWPB_CSWAP(0, 2) CWPB_CSWAP(1, 3) CWPB_CSWAP(1, 2)
 #undef CWPB_CSWAP
-        if (ht[0] == INF) { if (sp == 0) break; node = stack[--sp]; continue; }
-        if (sp + 3 > kStack2) { err |= kTravOverflow; break; }
+        if (ht[0] == INF) { if (sp == 0) return true; node = stack[--sp]; return false; }
+        if (sp + 3 > kStack2) { err |= kTravOverflow; return true; }
         if (ht[3] < INF) stack[sp++] = hc[3];
         if (ht[2] < INF) stack[sp++] = hc[2];
         if (ht[1] < INF) stack[sp++] = hc[1];
         node = hc[0];
+        return false;
     }
+};
+
+template <bool ANY, int TRI>
+__device__ __forceinline__ bool trav_bvh4(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
+                                          float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
+    TravState<4, ANY, TRI> r; typename TravState<4, ANY, TRI>::Stack stack; r.begin(o, d, tmin, hitT, root);
+    while (!r.step(nodes, tv, stack, err)) {}
+    hitT = r.hitT; hitTri = r.hitTri; hu = r.hu; hv = r.hv;
     return hitTri >= 0;
 }
+
+// traversal stack kept in shared memory: entry i of this thread at base[i * stride] (stride = threads per block, so
+// a warp's accesses to one entry hit consecutive words)
+template <class T>
+struct SharedStack {
+    T* base; int stride;
+    __device__ __forceinline__ T& operator[](int i) const { return base[(size_t)i * stride]; }
+};
 
 // ---------------- CWBVH ----------------
 __device__ __forceinline__ unsigned byte_of(unsigned w, int s) { return (w >> (8 * (s & 3))) & 255u; }
@@ -178,7 +203,8 @@ struct TravState<8, ANY, TRI> {
         oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
         cb = im = hm = 0;
     }
-    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ tv, Stack& stack, int& err) {
+    template <class S>
+    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ tv, S& stack, int& err) {
         if (--budget < 0) { err |= kTravBudget; return true; }
         const float4* nb = nodes + 5 * (size_t)node;
         const float4 f0 = ld4(nb), f1 = ld4(nb + 1), f2 = ld4(nb + 2), f3_ = ld4(nb + 3), f4_ = ld4(nb + 4);
@@ -334,7 +360,8 @@ struct TravState<16, ANY, TRI> {
         oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
         cb = im = hm = 0; wt = wt_setup(d);
     }
-    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ vt, Stack& stack, int& err) {
+    template <class S>
+    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ vt, S& stack, int& err) {
         if (--budget < 0) { err |= kTravBudget; return true; }
         const float4* nb = nodes + 5 * (size_t)node;
         const float4 f0 = ld4(nb), f1 = ld4(nb + 1), f2 = ld4(nb + 2), f3_ = ld4(nb + 3), f4_ = ld4(nb + 4);

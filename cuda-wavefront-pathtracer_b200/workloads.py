@@ -28,7 +28,7 @@ SEED = 1000
 EPS_SCALE = 1e-4
 
 __all__ = ["SCENES", "scene", "frame_params", "scene_extent", "camera_rays", "incoherent_rays", "reference_inputs",
-           "HFOV", "SEED", "SUN_TO", "SUN_E", "SUN_ANGLE_RAD", "SKY", "ALBEDO"]
+           "batch_scenes", "batch_rays", "HFOV", "SEED", "SUN_TO", "SUN_E", "SUN_ANGLE_RAD", "SKY", "ALBEDO"]
 
 
 def scene(name_or_boxes, variant=8, bins=32, leaf=4, collapse=0, threads=0):
@@ -127,3 +127,58 @@ def reference_inputs(mesh, p, outdir, w, h, spp, batch, variant="bvh2"):
     return ["--mesh", ply, "--camera", cam, "--lighting", light, "--albedo", str(ALBEDO), str(ALBEDO), str(ALBEDO),
             "--filter", "box", "--hfov", str(HFOV), "--width", str(w), "--height", str(h), "--spp", str(spp), "--bounces", str(p.max_b),
             "--variant", variant, "--tri", "woop", "--fuse", "1", "--batch", str(batch), "--seed", str(p.seed), "--leaf", "4"]
+
+
+def _log_uniform_int(rng, lo, hi):
+    return int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+
+
+def batch_scenes(n_scenes=64, seed=5, tris=(1000, 500000), instances=(1, 4096), blas_per_scene=(1, 8)):
+    """The batched-form workload: n_scenes two-level scenes, each a TLAS over a log-uniform number of instances of
+    1-8 BLAS of its own; every BLAS is a box field of a log-uniform triangle count; every instance a random rigid
+    transform (axis uniform on the sphere, angle uniform in [0, 2 pi), translation uniform in a cube that grows with
+    the cube root of the instance count). Returns (meshes, xforms [n_inst, 12], mesh_of [n_inst], scene_first)."""
+    from . import Mesh
+    rng = np.random.default_rng(seed)
+    meshes, xf, mesh_of, first = [], [], [], [0]
+    for s in range(n_scenes):
+        nb = int(rng.integers(blas_per_scene[0], blas_per_scene[1] + 1))
+        ids = []
+        for _ in range(nb):
+            nt = _log_uniform_int(rng, *tris)
+            ids.append(len(meshes))
+            meshes.append(Mesh.box_field(max(1, (nt - 2) // 12), int(rng.integers(1 << 30))))
+        ni = _log_uniform_int(rng, *instances)
+        half = 20.0 * max(1.0, ni ** (1.0 / 3.0))
+        for _ in range(ni):
+            ax = rng.normal(size=3); ax /= np.linalg.norm(ax)
+            ang = rng.uniform(0, 2 * math.pi); c, sn, k = math.cos(ang), math.sin(ang), 1 - math.cos(ang)
+            x, y, z = ax
+            R = np.array([[c + x * x * k, x * y * k - z * sn, x * z * k + y * sn],
+                          [y * x * k + z * sn, c + y * y * k, y * z * k - x * sn],
+                          [z * x * k - y * sn, z * y * k + x * sn, c + z * z * k]])
+            t = rng.uniform(-half, half, 3)
+            xf.append(np.concatenate([R, t[:, None]], 1).reshape(12))
+            mesh_of.append(ids[int(rng.integers(len(ids)))])
+        first.append(len(xf))
+    return meshes, np.array(xf, np.float32).reshape(-1, 12), np.array(mesh_of, np.int32), np.array(first, np.int32)
+
+
+def batch_rays(xforms, scene_first, rays_per_scene, seed=9, extent=40.0):
+    """Rays of the batched workload, scene-major: origins uniform in each scene's instance-translation box grown by
+    the mesh extent, directions uniform on the sphere, tmin 0, tmax 1e30. Returns (o, d float4, scene int32)."""
+    rng = np.random.default_rng(seed)
+    n_s = len(scene_first) - 1
+    o = np.zeros((n_s * rays_per_scene, 4), np.float32); d = np.zeros_like(o); sc = np.repeat(np.arange(n_s, dtype=np.int32), rays_per_scene)
+    for s in range(n_s):
+        a, b = scene_first[s], scene_first[s + 1]
+        sl = slice(s * rays_per_scene, (s + 1) * rays_per_scene)
+        if b > a:
+            t = xforms[a:b].reshape(-1, 3, 4)[:, :, 3]
+            lo, hi = t.min(0) - extent, t.max(0) + extent
+        else:
+            lo, hi = np.full(3, -extent), np.full(3, extent)
+        o[sl, :3] = rng.uniform(lo, hi, (rays_per_scene, 3))
+        v = rng.normal(size=(rays_per_scene, 3)); v /= np.linalg.norm(v, axis=1, keepdims=True)
+        d[sl, :3] = v; d[sl, 3] = 1e30
+    return o, d, sc

@@ -198,6 +198,99 @@ int cwp_render_noalloc(const cwp_params* p, const cwp_device_scene* s, const cwp
                        int32_t clear, float* d_accum, int64_t* h_rays, void* stream);
 
 /* ------------------------------------------------------------------------------------------------------------------
+ * Instances and two-level scenes (the batched form).
+ * cwp_instance replaces DevInstance (accel/instance.h:7, 112 B: world->object rows, object->world rows, BLAS root,
+ * mesh, det sign); cwp_xform_invert replaces invertXform (scene/instances.cpp:64-79: FP64 adjugate inverse rounded to
+ * fp32); cwp_xform_animate replaces instanceXform (scene/instances.cpp:48-62: translate + axis/angle rotation + scale,
+ * each with a per-frame velocity, composed in FP64).
+ * ------------------------------------------------------------------------------------------------------------------ */
+typedef struct cwp_instance {
+    float inv[12];      /* world -> object, 3 rows of (m0 m1 m2 t) */
+    float fwd[12];      /* object -> world */
+    int32_t root;       /* root node of the instance's BLAS; filled in by cwp_batch_set_scenes */
+    int32_t mesh;       /* BLAS index */
+    float det_sign;     /* sign of det(fwd) */
+    int32_t pad;
+} cwp_instance;
+
+typedef struct cwp_instance_desc {   /* InstanceDesc (scene/instances.h) */
+    int32_t mesh;
+    float translate[3], translate_per_frame[3];
+    float axis[3], angle_deg, angle_deg_per_frame;
+    float scale[3], scale_per_frame[3];
+} cwp_instance_desc;
+
+int cwp_xform_invert(const float m[12], float inv[12], float* det_sign);
+int cwp_xform_animate(const cwp_instance_desc* d, int32_t frame, float m[12]);
+/* fills fwd = m, inv and det_sign from cwp_xform_invert, mesh; root = -1 */
+int cwp_instance_from_xform(const float m[12], int32_t mesh, cwp_instance* out);
+
+/* ------------------------------------------------------------------------------------------------------------------
+ * Batched form: many meshes built on the GPU in one pass, many two-level scenes traced in one persistent launch.
+ * Replaces HplocBuilder (accel/hploc.h:18-41: reserve/build/release, one mesh per build) with a builder that takes
+ * every BLAS at once; hplocToBVH2 (hploc.h:36) and setInstances (render/renderer.h:53, wavefront.cu:570-581: instance
+ * boxes k_inst_boxes, TLAS rebuild) for every scene at once; travInst / StepTrav / persistentTrace
+ * (accel/traverse_inst.cuh:10-159, render/wavefront.cu:403-442) for a ray queue whose rays carry a scene id. The
+ * autotuner has no reference counterpart.
+ * Hits: float4 (t, u, v, tri bits), tri = index into the batch's leaf-order triangle array (its w field of the first
+ * float4 is the triangle's index in its mesh), plus the instance index (into the cwp_batch_set_scenes array) or -1.
+ * ------------------------------------------------------------------------------------------------------------------ */
+typedef struct cwp_batch cwp_batch;
+typedef struct cwp_batch_options {
+    int32_t device;
+    int32_t leaf;           /* max triangles per BVH2 / BVH4 leaf (default 4 when 0); CWBVH leaves hold at most 3 */
+    int32_t widths;         /* bit mask of the layouts to emit: 1 << 2 (BVH2), 1 << 4 (BVH4), 1 << 8 (CWBVH); 0 = all */
+    int32_t reserved[5];
+} cwp_batch_options;
+
+typedef struct cwp_batch_tuning {
+    int32_t block;          /* threads per block, 64..512 */
+    int32_t width;          /* BLAS layout 2, 4 or 8 */
+    int32_t fetch;          /* idle lanes of a warp before it fetches new rays, 1..32 */
+    int32_t smem_stack;     /* 1: BLAS traversal stack in shared memory, 0: in local memory */
+    float ms;               /* autotuner: measured time of the sample (closest + any), else 0 */
+    int32_t reserved[3];
+} cwp_batch_tuning;
+
+typedef struct cwp_batch_info {
+    int32_t n_blas, n_scenes;
+    int64_t n_tris, n_instances;
+    int64_t node_bytes[3];  /* BVH2, BVH4, CWBVH node arrays (0 if not emitted) */
+    double blas_build_ms;   /* GPU time of the BLAS build (bounds, keys, sort, H-PLOC, layouts) */
+    double tlas_build_ms;   /* GPU time of the last cwp_batch_set_scenes (instance boxes, H-PLOC, TLAS layout) */
+    int32_t blas_hploc_launches;   /* H-PLOC kernel launches of the BLAS build (1) */
+    int32_t pad;
+} cwp_batch_info;
+
+/* Builds every BLAS on the device: one bounds pass, one key pass, one segmented radix sort and ONE H-PLOC launch
+ * over all meshes' triangles, then the BVH2 / BVH4 / CWBVH encodings and Moller-Trumbore triangle records. */
+int cwp_batch_create(const cwp_mesh_view* meshes, int32_t n_meshes, const cwp_batch_options* opt, cwp_batch** out);
+void cwp_batch_destroy(cwp_batch* b);
+/* Scenes: scene s owns instances [scene_first[s], scene_first[s + 1]) of inst (n_scenes + 1 entries). Builds every
+ * scene's TLAS (BVH2 over instance world boxes) on the device in one H-PLOC launch; call again each frame when the
+ * transforms move. Synchronous. */
+int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int64_t n_inst, const int32_t* scene_first, int32_t n_scenes);
+/* One persistent launch over a queue of rays tagged with scene ids (d_scene, int32 per ray). any_hit: d_hits may be
+ * NULL and d_inst receives the occluding instance or -1. */
+int cwp_batch_trace(cwp_batch* b, int32_t any_hit, const float* d_o, const float* d_d, const int32_t* d_scene, float* d_hits,
+                    int32_t* d_inst, int64_t n, void* stream);
+/* Times the closest + any-hit trace of the given sample over block size {64, 128, 256, 512}, BLAS width {2, 4, 8},
+ * fetch granularity {1, 2, 4, 8, 16, 32} and stack placement {local, shared}, keeps the fastest and returns it.
+ * d_hits / d_inst are scratch of n entries. */
+int cwp_batch_autotune(cwp_batch* b, const float* d_o, const float* d_d, const int32_t* d_scene, float* d_hits, int32_t* d_inst,
+                       int64_t n, cwp_batch_tuning* best);
+int cwp_batch_set_tuning(cwp_batch* b, const cwp_batch_tuning* t);
+int cwp_batch_get_tuning(const cwp_batch* b, cwp_batch_tuning* t);
+int cwp_batch_info_of(const cwp_batch* b, cwp_batch_info* out);
+/* Host copies for checking: the node array of one layout (width 2, 4 or 8) and the triangle records. Pass NULL
+ * buffers to query the sizes (in float4). */
+int cwp_batch_download(const cwp_batch* b, int32_t width, float* nodes, int64_t* n_node_float4, float* tris, int64_t* n_tri_float4);
+/* root node of mesh m's BLAS in layout width; and the TLAS (BVH2 nodes, root per scene, instances with roots) */
+int cwp_batch_blas_root(const cwp_batch* b, int32_t width, int32_t mesh, int32_t* root);
+int cwp_batch_download_tlas(const cwp_batch* b, float* nodes, int64_t* n_node_float4, int32_t* roots, cwp_instance* inst);
+int cwp_batch_status(cwp_batch* b);   /* synchronises; CWP_ERR_TRAVERSAL if a ray hit a stack bound or the visit budget */
+
+/* ------------------------------------------------------------------------------------------------------------------
  * Camera and parameter helpers. Replace lookAtC2W / focalFromHfov / makeCamera (scene/camera.cpp:7-23) and the
  * Params filling of setupScene (app/scene_setup.cpp:175-185, Lighting defaults scene/lighting.h:7-13).
  * ------------------------------------------------------------------------------------------------------------------ */

@@ -407,8 +407,8 @@ static int leaf_hit_s(const V4* tv, int first, int cnt, V3 o, V3 d, float tmin, 
     return leaf_hit(tv, first, cnt, o, d, tmin, any, tri, T, I, U, W);
 }
 
-static int trav2(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv, Stats* st) {
-    int stack[64], sp = 0, node = 0;
+static int trav2r(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv, Stats* st, int root) {
+    int stack[64], sp = 0, node = root;
     const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z), ox = -o.x * idx, oy = -o.y * idy, oz = -o.z * idz;
     for (;;) {
         if (st) st->nodes++;
@@ -431,8 +431,8 @@ static int trav2(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any,
 }
 
 static unsigned byte_of(unsigned w, int s) { return (w >> (8 * (s & 3))) & 255u; }
-static int trav8(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv, Stats* st) {
-    unsigned stk[40][2]; int sp = 0, node = 0;
+static int trav8r(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv, Stats* st, int root) {
+    unsigned stk[40][2]; int sp = 0, node = root;
     const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z);
     const unsigned oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
     unsigned cb = 0, im = 0, hm = 0;
@@ -468,6 +468,51 @@ static int trav8(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any,
     }
 }
 
+static int trav2(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv, Stats* st) {
+    return trav2r(nodes, tv, o, d, tmin, any, tri, hitT, hitTri, hu, hv, st, 0);
+}
+static int trav8(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv, Stats* st) {
+    return trav8r(nodes, tv, o, d, tmin, any, tri, hitT, hitTri, hu, hv, st, 0);
+}
+/* BVH4 (traverse.cuh:74-107): four slab tests, hit leaves tested in child order, inner children sorted by entry
+ * distance with the five-exchange network, nearest visited next, the others pushed farthest first */
+static int trav4r(const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, int tri, float* hitT, int* hitTri, float* hu, float* hv, Stats* st, int root) {
+    int stack[64], sp = 0, node = root;
+    const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z), ox = -o.x * idx, oy = -o.y * idy, oz = -o.z * idz;
+    const float INF = 3.4e38f;
+    for (;;) {
+        if (st) st->nodes++;
+        const V4* nb = nodes + 8 * node;
+        const float LX[4] = { nb[0].x, nb[0].y, nb[0].z, nb[0].w }, HX[4] = { nb[1].x, nb[1].y, nb[1].z, nb[1].w };
+        const float LY[4] = { nb[2].x, nb[2].y, nb[2].z, nb[2].w }, HY[4] = { nb[3].x, nb[3].y, nb[3].z, nb[3].w };
+        const float LZ[4] = { nb[4].x, nb[4].y, nb[4].z, nb[4].w }, HZ[4] = { nb[5].x, nb[5].y, nb[5].z, nb[5].w };
+        const int CC[4] = { fi(nb[6].x), fi(nb[6].y), fi(nb[6].z), fi(nb[6].w) }, KK[4] = { fi(nb[7].x), fi(nb[7].y), fi(nb[7].z), fi(nb[7].w) };
+        float ht[4]; int hc[4];
+        for (int j = 0; j < 4; j++) {
+            float x0 = fmaf(LX[j], idx, ox), x1 = fmaf(HX[j], idx, ox), y0 = fmaf(LY[j], idy, oy), y1 = fmaf(HY[j], idy, oy), z0 = fmaf(LZ[j], idz, oz), z1 = fmaf(HZ[j], idz, oz);
+            float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+            float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), *hitT));
+            ht[j] = INF; hc[j] = CC[j];
+            if (tn <= tf) {
+                if (KK[j] > 0) { if (leaf_hit_s(tv, CC[j], KK[j], o, d, tmin, any, tri, hitT, hitTri, hu, hv, st) && any) return 1; }
+                else ht[j] = tn;
+            }
+        }
+        static const int net[5][2] = { { 0, 1 }, { 2, 3 }, { 0, 2 }, { 1, 3 }, { 1, 2 } };
+        for (int q = 0; q < 5; q++) {
+            const int a = net[q][0], b = net[q][1];
+            if (ht[b] < ht[a]) { float t = ht[a]; ht[a] = ht[b]; ht[b] = t; int c = hc[a]; hc[a] = hc[b]; hc[b] = c; }
+        }
+        if (ht[0] == INF) { if (sp == 0) break; node = stack[--sp]; continue; }
+        if (sp + 3 > 64) return -1;
+        if (ht[3] < INF) stack[sp++] = hc[3];
+        if (ht[2] < INF) stack[sp++] = hc[2];
+        if (ht[1] < INF) stack[sp++] = hc[1];
+        node = hc[0];
+    }
+    return *hitTri >= 0;
+}
+
 /* ray batch: o/d float4 (tmin / tmax in w). Closest: hits float4 (t, u, v, tri bits). Any: occ = first occluder or -1.
  * stats (may be NULL): [0] node visits, [1] triangle tests summed over the batch. Returns the number of rays that hit
  * a stack bound. */
@@ -477,6 +522,7 @@ long orc_trace(int variant, int tri, int any, const float* nodes, const float* t
         V3 o = v3(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]), d = v3(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]);
         float tmin = ro[4 * i + 3], t = rd[4 * i + 3], u = 0.f, vv = 0.f; int h = -1, r;
         if (variant == 2) r = trav2((const V4*)nodes, (const V4*)tv, o, d, tmin, any, tri, &t, &h, &u, &vv, stats ? &st : NULL);
+        else if (variant == 4) r = trav4r((const V4*)nodes, (const V4*)tv, o, d, tmin, any, tri, &t, &h, &u, &vv, stats ? &st : NULL, 0);
         else r = trav8((const V4*)nodes, (const V4*)tv, o, d, tmin, any, tri, &t, &h, &u, &vv, stats ? &st : NULL);
         if (r < 0) bad++;
         if (any) occ[i] = h;
@@ -752,5 +798,64 @@ long orc_trace_prec(const float* nodes, const float* vt, const float* ro, const 
         else { hits[4 * i] = t; hits[4 * i + 1] = u; hits[4 * i + 2] = v; memcpy(&hits[4 * i + 3], &tri, 4); }
     }
     if (stats) { stats[0] = st.nodes; stats[1] = st.tris; }
+    return bad;
+}
+
+/* ------------------------------------------------------------------ two-level scenes (batched form)
+ * Not a reference function: restates the CUDA batched form's traversal (accel/traverse_inst.cuh:10-41 is its model):
+ * per ray, the TLAS of its scene (BVH2, leaves = one instance, nearer child first, leaves pushed like inner nodes and
+ * entered when they come up), the instance's BLAS (width 2, 4 or 8, root = its mesh) with the ray brought into object
+ * space by the instance's world->object rows (t shared), Moller-Trumbore triangles. inst: 28 floats per instance
+ * (inv rows, fwd rows, root, mesh, det sign, pad as in cwp_instance). Closest: hits float4 + hit instance; any:
+ * first occluder (hits may be NULL) + its instance. Returns the number of rays that hit a stack bound. */
+static int trav_blas(int width, const V4* nodes, const V4* tv, V3 o, V3 d, float tmin, int any, float* t, int* h, float* u, float* v, int root) {
+    if (width == 2) return trav2r(nodes, tv, o, d, tmin, any, 0, t, h, u, v, NULL, root);
+    if (width == 4) return trav4r(nodes, tv, o, d, tmin, any, 0, t, h, u, v, NULL, root);
+    return trav8r(nodes, tv, o, d, tmin, any, 0, t, h, u, v, NULL, root);
+}
+long orc_trace_inst(int width, int any, const float* blas, const float* tris, const float* tlas, const int* scene_root, int n_scenes, const float* inst,
+                    const float* ro, const float* rd, const int* scene_of, long n, float* hits, int* hit_inst) {
+    long bad = 0;
+    const V4* T = (const V4*)tlas;
+    for (long i = 0; i < n; i++) {
+        const V3 o = v3(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]), d = v3(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]);
+        const float tmin = ro[4 * i + 3];
+        float t = rd[4 * i + 3], u = 0.f, v = 0.f; int h = -1, hi = -1, done = 0;
+        const int sc = scene_of[i], root = sc >= 0 && sc < n_scenes ? scene_root[sc] : -1;
+        if (root >= 0) {
+            const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z), ox = -o.x * idx, oy = -o.y * idy, oz = -o.z * idz;
+            int stack[64], sp = 0, next = root;
+            while (!done) {
+                const V4 n0 = T[4 * next], n1 = T[4 * next + 1], nz = T[4 * next + 2], mt = T[4 * next + 3];
+                const int c0 = fi(mt.x), c1 = fi(mt.y), k0 = fi(mt.z), k1 = fi(mt.w);
+                const float a0 = fmaf(n0.x, idx, ox), a1 = fmaf(n0.y, idx, ox), a2 = fmaf(n0.z, idy, oy), a3 = fmaf(n0.w, idy, oy), a4 = fmaf(nz.x, idz, oz), a5 = fmaf(nz.y, idz, oz);
+                const float b0 = fmaf(n1.x, idx, ox), b1 = fmaf(n1.y, idx, ox), b2 = fmaf(n1.z, idy, oy), b3 = fmaf(n1.w, idy, oy), b4 = fmaf(nz.z, idz, oz), b5 = fmaf(nz.w, idz, oz);
+                const float t0n = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
+                const float t0f = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), t));
+                const float t1n = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
+                const float t1f = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), t));
+                const int h0 = c0 >= 0 && t0n <= t0f, h1 = c1 >= 0 && t1n <= t1f;
+                int e0 = k0 > 0 ? ~c0 : c0, e1 = k1 > 0 ? ~c1 : c1, go;
+                if (h0 && h1) { if (t1n < t0n) { int q = e0; e0 = e1; e1 = q; } if (sp == 64) { bad++; break; } stack[sp++] = e1; go = e0; }
+                else if (h0 || h1) go = h0 ? e0 : e1;
+                else { if (sp == 0) break; go = stack[--sp]; }
+                while (go < 0) {   /* an instance: its BLAS in object space, then the next TLAS entry */
+                    const float* I = inst + 28 * (size_t)(~go);
+                    const V3 lo = v3(I[0] * o.x + I[1] * o.y + I[2] * o.z + I[3], I[4] * o.x + I[5] * o.y + I[6] * o.z + I[7], I[8] * o.x + I[9] * o.y + I[10] * o.z + I[11]);
+                    const V3 ld = v3(I[0] * d.x + I[1] * d.y + I[2] * d.z, I[4] * d.x + I[5] * d.y + I[6] * d.z, I[8] * d.x + I[9] * d.y + I[10] * d.z);
+                    int iroot; memcpy(&iroot, &I[24], 4);
+                    float bt = t, bu = 0.f, bv = 0.f; int bh = -1;
+                    if (trav_blas(width, (const V4*)blas, (const V4*)tris, lo, ld, tmin, any, &bt, &bh, &bu, &bv, iroot) < 0) { bad++; done = 1; break; }
+                    if (bh >= 0 && bt < t) { t = bt; h = bh; u = bu; v = bv; hi = ~go; }
+                    if (any && h >= 0) { done = 1; break; }
+                    if (sp == 0) { done = 1; break; }
+                    go = stack[--sp];
+                }
+                if (!done) next = go;
+            }
+        }
+        if (hits) { hits[4 * i] = t; hits[4 * i + 1] = u; hits[4 * i + 2] = v; hits[4 * i + 3] = iff(h); }
+        hit_inst[i] = hi;
+    }
     return bad;
 }

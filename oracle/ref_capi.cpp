@@ -3,6 +3,7 @@
 // against the reference (byte-identical BVH buffers, same traversal results) and as the timed CPU baseline.
 //   builder / layouts ... accel/bvh_builder.cpp, accel/bvh_layouts.cpp, accel/bvh_tools.cpp, accel/tri_pack.cpp
 //   traversal ........... accel/traverse.cuh trav<V, ANY, TRI> compiled as host C++ through ref_shim.h
+//   instance transforms . scene/instances.cpp invertXform / instanceXform (with io/json.cpp, which it links)
 // The harness (threads, argument marshalling) is ours; the arithmetic is the reference's.
 #include "ref_shim.h"
 #include "accel/bvh_builder.h"
@@ -11,6 +12,7 @@
 #include "accel/tri_pack.h"
 #include "accel/traverse.cuh"
 #include "core/rng.h"
+#include "scene/instances.h"
 #include "core/sampling.h"
 #include <algorithm>
 #include <chrono>
@@ -159,4 +161,21 @@ extern "C" double ref_render_cpu(const void* params, int variant, int tri, const
     double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     for (int k = 0; k < threads; k++) { counts[0] += nc[k]; counts[1] += ns[k]; }
     return sec;
+}
+
+// scene/instances.cpp:64-79
+extern "C" void ref_xform_invert(const float* m, float* inv, float* det_sign) {
+    Xform M, I; for (int i = 0; i < 12; i++) M.m[i] = m[i];
+    invertXform(M, I, *det_sign);
+    for (int i = 0; i < 12; i++) inv[i] = I.m[i];
+}
+// scene/instances.cpp:48-62 (parametric instance: translate, axis, angle, scale and their per-frame velocities)
+extern "C" void ref_xform_animate(const float* translate, const float* translate_vel, const float* axis, float angle_deg, float angle_vel,
+                                  const float* scale, const float* scale_vel, int frame, float* m) {
+    InstanceDesc d;
+    d.translate = make_float3(translate[0], translate[1], translate[2]); d.translateVel = make_float3(translate_vel[0], translate_vel[1], translate_vel[2]);
+    d.axis = make_float3(axis[0], axis[1], axis[2]); d.angleDeg = angle_deg; d.angleVel = angle_vel;
+    d.scale = make_float3(scale[0], scale[1], scale[2]); d.scaleVel = make_float3(scale_vel[0], scale_vel[1], scale_vel[2]);
+    const Xform X = instanceXform(d, frame);
+    for (int i = 0; i < 12; i++) m[i] = X.m[i];
 }

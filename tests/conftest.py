@@ -49,6 +49,8 @@ def _load_oracle():
     L.orc_trace_fp64.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p]
     L.orc_trace_prec.restype = C.c_long
     L.orc_trace_prec.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_trace_inst.restype = C.c_long
+    L.orc_trace_inst.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_long, C.c_void_p, C.c_void_p]
     L.orc_half_round.restype = C.c_double
     L.orc_half_round.argtypes = [C.c_double, C.c_int]
     L.orc_rng.restype = C.c_float
@@ -111,6 +113,18 @@ class Oracle:
         res = occ if any_hit else hits
         return (res, st) if stats else res
 
+    def trace_inst(self, width, any_hit, blas, tris, tlas, scene_root, inst, o, d, scene_of):
+        """Two-level traversal of the batched form: (hits float4 [n, 4], hit instance [n])."""
+        n = len(o)
+        hits = np.zeros((n, 4), np.float32); hi = np.zeros(n, np.int32)
+        a = [np.ascontiguousarray(x) for x in (blas, tris, tlas)]
+        sr = np.ascontiguousarray(scene_root, np.int32); ins = np.ascontiguousarray(inst, np.float32); so = np.ascontiguousarray(scene_of, np.int32)
+        bad = self.L.orc_trace_inst(width, 1 if any_hit else 0, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, sr.ctypes.data, len(sr),
+                                    ins.ctypes.data, np.ascontiguousarray(o).ctypes.data, np.ascontiguousarray(d).ctypes.data, so.ctypes.data, n,
+                                    hits.ctypes.data, hi.ctypes.data)
+        assert bad == 0
+        return hits, hi
+
     def render(self, params, variant, tri, bvh, bounces, spp, s_base=0, pix0=0, pix1=None):
         w, h = params.cam.w, params.cam.h
         acc = np.zeros((w * h, 4), np.float32); rc = np.zeros(2, np.int64)
@@ -134,6 +148,10 @@ class Ref:
         L.ref_build.restype = C.c_long
         L.ref_build.argtypes = [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ref_xform_invert.restype = None
+        L.ref_xform_invert.argtypes = [C.POINTER(C.c_float)] * 3
+        L.ref_xform_animate.restype = None
+        L.ref_xform_animate.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_float, C.c_float] + [C.POINTER(C.c_float)] * 2 + [C.c_int, C.POINTER(C.c_float)]
         L.ref_trace.restype = C.c_double
         L.ref_trace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_int]
         self.L = L

@@ -7,6 +7,13 @@ reference sources by oracle/Makefile):
            and Woop rows (16 bins, leaf 4), and the reference traversal's closest hits and any-hit occluders for the
            batch over BVH2 and CWBVH with Woop and Moller-Trumbore triangles
 
+and tests/golden/instances.npz:
+
+  inputs   256 seeded object-to-world maps (rotation x scale x translation, some mirrored, some near-singular) and 64
+           parametric instances (translate / axis / angle / scale with per-frame velocities) at frames 0, 1 and 7
+  outputs  the reference's invertXform inverses and determinant signs and its instanceXform matrices; the reference
+           traversal's closest hits and any-hit occluders over its BVH4 nodes of boxes64 (Woop and Moller-Trumbore)
+
 The fixtures pin the oracle and the library where the reference sources are absent. Run from the repository root:
     python tests/golden/make_golden.py
 """
@@ -44,6 +51,48 @@ def main():
             out[f"{name}_t{tri}_any"] = ref.trace(variant, tri, True, out[f"{name}_nodes"], tv, o, d, threads=1)
     np.savez_compressed(os.path.join(HERE, "boxes64.npz"), **out)
     print("wrote", os.path.join(HERE, "boxes64.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
+    instances(ref, out)
+
+
+def instances(ref, box):
+    import ctypes as C
+    L = ref.L
+    rng = np.random.default_rng(21)
+    mats = []
+    for k in range(256):
+        ax = rng.normal(size=3); ax /= np.linalg.norm(ax); a = rng.uniform(0, 2 * np.pi)
+        K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+        R = np.eye(3) + np.sin(a) * K + (1 - np.cos(a)) * K @ K
+        S = np.diag(np.exp(rng.uniform(-2, 2, 3)) * (np.where(rng.random(3) < 0.1, -1.0, 1.0)))
+        if k % 32 == 5: S[2, 2] = 1e-7   # near-singular
+        mats.append(np.concatenate([R @ S, rng.uniform(-100, 100, (3, 1))], 1).reshape(12))
+    mats = np.array(mats, np.float32)
+    inv = np.zeros_like(mats); det = np.zeros(len(mats), np.float32)
+    fp = C.POINTER(C.c_float)
+    for i in range(len(mats)):
+        L.ref_xform_invert(mats[i].ctypes.data_as(fp), inv[i].ctypes.data_as(fp), det[i:i + 1].ctypes.data_as(fp))
+    n = 64
+    desc = dict(translate=rng.uniform(-50, 50, (n, 3)), translate_vel=rng.uniform(-1, 1, (n, 3)), axis=rng.normal(size=(n, 3)),
+                angle=rng.uniform(-180, 180, n), angle_vel=rng.uniform(-5, 5, n), scale=np.exp(rng.uniform(-1, 1, (n, 3))),
+                scale_vel=rng.uniform(-0.01, 0.01, (n, 3)))
+    desc = {k: np.ascontiguousarray(v, np.float32) for k, v in desc.items()}
+    desc["axis"][0] = 0.0   # zero axis: +z
+    frames = np.array([0, 1, 7], np.int32)
+    anim = np.zeros((n, len(frames), 12), np.float32)
+    for i in range(n):
+        for j, f in enumerate(frames):
+            L.ref_xform_animate(desc["translate"][i].ctypes.data_as(fp), desc["translate_vel"][i].ctypes.data_as(fp), desc["axis"][i].ctypes.data_as(fp),
+                                C.c_float(desc["angle"][i]), C.c_float(desc["angle_vel"][i]), desc["scale"][i].ctypes.data_as(fp),
+                                desc["scale_vel"][i].ctypes.data_as(fp), C.c_int(int(f)), anim[i, j].ctypes.data_as(fp))
+    out = dict(mats=mats, inv=inv, det_sign=det, frames=frames, anim=anim, **{f"desc_{k}": v for k, v in desc.items()})
+    # BVH4 traversal of boxes64 (tris for Moller-Trumbore, woop rows re-packed in the BVH4 leaf order)
+    r = ref.build(box["verts"], box["faces"], box["face_mat"], variant=4, leaf=4, collapse=0)
+    for tri, tv in ((1, r["woop"]), (0, r["tris"])):
+        out[f"bvh4_t{tri}_closest"] = ref.trace(4, tri, False, r["nodes"], tv, box["rays_o"], box["rays_d"], threads=1)
+        out[f"bvh4_t{tri}_any"] = ref.trace(4, tri, True, r["nodes"], tv, box["rays_o"], box["rays_d"], threads=1)
+    out["bvh4_tris"], out["bvh4_woop"] = r["tris"], r["woop"]
+    np.savez_compressed(os.path.join(HERE, "instances.npz"), **out)
+    print("wrote", os.path.join(HERE, "instances.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
 
 
 if __name__ == "__main__":

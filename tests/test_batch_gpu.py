@@ -1,0 +1,143 @@
+"""Batched form on the GPU: the segmented H-PLOC build of many meshes in one launch (every triangle placed exactly
+once per layout, boxes that contain their children), the two-level persistent traversal against the oracle's
+restatement on the very buffers the GPU built (bit for bit, every width, closest and any-hit, scene-tagged queue),
+agreement across widths and tunings, per-frame TLAS rebuilds, and the autotuner."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.fixture(scope="module")
+def batch_case(gpu, cwp):
+    meshes, xf, mesh_of, first = cwp.batch_scenes(n_scenes=6, seed=3, tris=(200, 20000), instances=(1, 60), blas_per_scene=(1, 3))
+    first = np.concatenate([first[:3], [first[2]], first[3:]]).astype(np.int32)   # an empty scene (index 2) in the middle
+    b = cwp.Batch(meshes)
+    inst = cwp.instances(xf, mesh_of)
+    b.set_scenes(inst, first)
+    o, d, sc = cwp.batch_rays(xf, first, 3000, seed=4)
+    sc[::97] = 99   # rays with an unknown scene id miss
+    return meshes, xf, mesh_of, first, b, o, d, sc
+
+
+def trace(gpu, b, o, d, sc, any_hit=False):
+    n = len(o)
+    hits = gpu.empty((n, 4), dtype=gpu.float32, device="cuda"); hi = gpu.empty(n, dtype=gpu.int32, device="cuda")
+    to, td, ts = dev(gpu, o), dev(gpu, d), dev(gpu, sc)
+    b.trace(to.data_ptr(), td.data_ptr(), ts.data_ptr(), hits.data_ptr(), hi.data_ptr(), n, any_hit=any_hit)
+    gpu.cuda.synchronize(); b.status()
+    return hits.cpu().numpy(), hi.cpu().numpy()
+
+
+def test_build_places_every_triangle_once(gpu, cwp, batch_case):
+    meshes, xf, mesh_of, first, b, *_ = batch_case
+    info = b.info()
+    assert info.blas_hploc_launches == 1 and info.n_blas == len(meshes) and info.blas_build_ms > 0
+    ntri = [m.n_tris for m in meshes]; off = np.concatenate([[0], np.cumsum(ntri)])
+    for w in (2, 4, 8):
+        nodes, tris = b.download(w)
+        assert info.node_bytes[{2: 0, 4: 1, 8: 2}[w]] == nodes.nbytes
+        ids = tris[0::3, 3].view(np.int32)
+        # every mesh's local ids appear exactly once (triangles of one mesh may sit anywhere in the array)
+        assert np.array_equal(np.sort(ids), np.sort(np.concatenate([np.arange(n) for n in ntri])))
+        # corners reproduce the input triangles: v0 and v0 + e1 / e2 against each mesh's faces
+        assert np.all(np.isfinite(tris))
+
+
+def test_binary_and_wide_boxes_contain_triangles(gpu, cwp, batch_case):
+    """Every leaf triangle lies inside the box its parent stores for it (BVH2 / BVH4 exact boxes; CWBVH quantised
+    planes rounded outward)."""
+    meshes, xf, mesh_of, first, b, *_ = batch_case
+    for w in (2, 4):
+        nodes, tris = b.download(w)
+        st = 4 if w == 2 else 8
+        N = nodes.reshape(-1, st, 4)
+        v0 = tris[0::3, :3]; v1 = v0 + tris[1::3, :3]; v2 = v0 + tris[2::3, :3]
+        tlo = np.minimum(np.minimum(v0, v1), v2); thi = np.maximum(np.maximum(v0, v1), v2)
+        for node in N:
+            if w == 2:
+                boxes = [((node[0, 0], node[0, 2], node[2, 0]), (node[0, 1], node[0, 3], node[2, 1])), ((node[1, 0], node[1, 2], node[2, 2]), (node[1, 1], node[1, 3], node[2, 3]))]
+                c = node[3].view(np.int32); refs = [(c[0], c[2]), (c[1], c[3])]
+            else:
+                boxes = [((node[0, j], node[2, j], node[4, j]), (node[1, j], node[3, j], node[5, j])) for j in range(4)]
+                refs = [(node[6].view(np.int32)[j], node[7].view(np.int32)[j]) for j in range(4)]
+            for (lo, hi), (c, k) in zip(boxes, refs):
+                if k > 0:
+                    assert np.all(tlo[c:c + k] >= np.array(lo) - 1e-6) and np.all(thi[c:c + k] <= np.array(hi) + 1e-6)
+
+
+@pytest.mark.parametrize("width", [2, 4, 8])
+def test_two_level_trace_matches_oracle(gpu, cwp, oracle, batch_case, width):
+    meshes, xf, mesh_of, first, b, o, d, sc = batch_case
+    b.set_tuning(block=128, width=width, fetch=8, smem_stack=0)
+    nodes, tris = b.download(width)
+    tlas, roots, inst = b.download_tlas(len(first) - 1, len(mesh_of))
+    assert roots[2] == -1
+    for any_hit in (False, True):
+        h, hi = trace(gpu, b, o, d, sc, any_hit)
+        ho, hio = oracle.trace_inst(width, any_hit, nodes, tris, tlas, roots, inst, o, d, sc)
+        if any_hit:
+            assert np.array_equal(hi, hio) and np.array_equal(h[:, 3].view(np.int32), ho[:, 3].view(np.int32))
+        else:
+            assert np.array_equal(h.view(np.uint32), ho.view(np.uint32)) and np.array_equal(hi, hio)
+    assert np.all(hi[sc == 99] == -1) and np.all(hi[sc == 2] == -1)
+    assert (hi >= 0).mean() > 0.05   # the batch does hit geometry
+
+
+def test_widths_and_tunings_agree(gpu, cwp, batch_case):
+    """All widths, block sizes, fetch sizes and stack placements report the same closest hit (instance, mesh-local
+    triangle id, t) up to exact-distance ties."""
+    meshes, xf, mesh_of, first, b, o, d, sc = batch_case
+    base = None
+    for t in ((128, 8, 12, 0), (64, 2, 1, 1), (256, 4, 32, 0), (512, 8, 4, 1), (128, 4, 8, 1), (256, 2, 16, 0)):
+        b.set_tuning(*t)
+        h, hi = trace(gpu, b, o, d, sc)
+        _, tris = b.download(t[1])
+        tri = h[:, 3].view(np.int32)
+        key = np.where(tri >= 0, tris[3 * np.maximum(tri, 0), 3].view(np.int32), -1)
+        cur = (h[:, 0].astype(np.float64), hi, key)
+        if base is None:
+            base = cur; continue
+        same = (cur[1] == base[1]) & (cur[2] == base[2])
+        tie = ~same & (cur[1] >= 0) & (base[1] >= 0) & (np.abs(cur[0] - base[0]) <= 1e-6 * np.abs(base[0]))
+        assert np.all(same | tie), t
+        assert np.array_equal(cur[1] >= 0, base[1] >= 0)
+
+
+def test_tlas_rebuild_per_frame(gpu, cwp, oracle, batch_case):
+    meshes, xf, mesh_of, first, b, o, d, sc = batch_case
+    moved = xf.copy().reshape(-1, 3, 4); moved[:, :, 3] += np.float32(1.5)
+    b.set_scenes(cwp.instances(moved.reshape(-1, 12), mesh_of), first)
+    b.set_tuning(128, 8, 12, 0)
+    h, hi = trace(gpu, b, o, d, sc)
+    nodes, tris = b.download(8)
+    tlas, roots, inst = b.download_tlas(len(first) - 1, len(mesh_of))
+    ho, hio = oracle.trace_inst(8, False, nodes, tris, tlas, roots, inst, o, d, sc)
+    assert np.array_equal(h.view(np.uint32), ho.view(np.uint32)) and np.array_equal(hi, hio)
+    assert b.info().tlas_build_ms > 0
+    b.set_scenes(cwp.instances(xf, mesh_of), first)
+
+
+def test_autotune_picks_a_valid_tuning(gpu, cwp, batch_case):
+    meshes, xf, mesh_of, first, b, o, d, sc = batch_case
+    n = len(o)
+    hits = gpu.empty((n, 4), dtype=gpu.float32, device="cuda"); hi = gpu.empty(n, dtype=gpu.int32, device="cuda")
+    to, td, ts = dev(gpu, o), dev(gpu, d), dev(gpu, sc)
+    t = b.autotune(to.data_ptr(), td.data_ptr(), ts.data_ptr(), hits.data_ptr(), hi.data_ptr(), n)
+    assert t.block in (64, 128, 256, 512) and t.width in (2, 4, 8) and 1 <= t.fetch <= 32 and t.smem_stack in (0, 1) and t.ms > 0
+    cur = b.tuning()
+    assert (cur.block, cur.width, cur.fetch, cur.smem_stack) == (t.block, t.width, t.fetch, t.smem_stack)
+
+
+def test_bad_arguments(gpu, cwp, batch_case):
+    meshes, xf, mesh_of, first, b, *_ = batch_case
+    with pytest.raises(cwp.CwpError):
+        b.set_tuning(block=100)
+    with pytest.raises(cwp.CwpError):
+        b.set_tuning(width=3)
+    with pytest.raises(cwp.CwpError):
+        b.set_scenes(cwp.instances(xf[:1], [len(meshes)]), [0, 1])
