@@ -8,6 +8,9 @@ Workloads (synthetic box-field scenes standing in for the reference's unreleased
   trace16m  117,002 triangles, 2^24 incoherent rays traced closest-hit and any-hit
   precision1m  12,290 triangles, 2^20 incoherent rays, precision form (f16 conservative slabs + watertight FP32
             triangles) closest + any, checked against the FP64 oracle (lost hits, ties, max relative t error)
+  batched64  64 two-level scenes (TLAS over 1-4,096 instances of 1-8 box-field BLAS of 1k-500k triangles each, all
+            BLAS built on the GPU by one H-PLOC launch), 4M rays per scene in one scene-tagged queue, closest + any
+            in one persistent launch each, launch shape chosen by the autotuner
 A step is one frame (frame*) or one closest + one any-hit pass over the batch (trace16m). `value` counts the rays of
 all ranks over the max over ranks of the device-timed steps (CUDA events on the renderer's stream). `e2e` is the same
 metric through the C ABI with host buffers: each frame's accumulation buffer (trace16m: rays in, hits out) crosses
@@ -35,6 +38,7 @@ WORKLOADS = {
     "frame256": dict(scene="boxes12k", w=256, h=256, spp=16, batch=16, bounces=4),
     "trace16m": dict(scene="boxes117k", rays=1 << 24),
     "precision1m": dict(scene="boxes12k", rays=1 << 20, precision=True),
+    "batched64": dict(batched=True, scenes=64, rays_per_scene=4 << 20, tris=(1000, 500000), instances=(1, 4096), blas=(1, 8), seed=5),
 }
 STATE_BYTES = 40          # path state per queued ray: (o, id) + (d, T.r) + (T.g, T.b); shadow entries the same size
 LAYOUT_NAMES = {2: "bvh2", 4: "bvh4", 8: "cwbvh"}
@@ -98,6 +102,9 @@ def reference_lib():
     L.ref_render_cpu.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p, C.c_int]
     L.ref_trace.restype = C.c_double
     L.ref_trace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_int]
+    if hasattr(L, "ref_trace_inst"):
+        L.ref_trace_inst.restype = C.c_double
+        L.ref_trace_inst.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_long, C.c_void_p, C.c_void_p, C.c_int]
     return L
 
 
@@ -193,6 +200,140 @@ def run_reference(args, wl, rank):
                       "cpu_baseline": cb, "e2e": {"value": v, "unit": "Grays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
 
 
+def batched_setup(cwp, wl):
+    meshes, xf, mesh_of, first = cwp.batch_scenes(n_scenes=wl["scenes"], seed=wl["seed"], tris=wl["tris"], instances=wl["instances"], blas_per_scene=wl["blas"])
+    return meshes, xf, mesh_of, first
+
+
+def batched_rays(torch, xf, first, per, seed=9, extent=40.0):
+    """The queue on the device, scene-major: origins uniform in each scene's instance-translation box grown by the
+    mesh extent, directions uniform on the sphere (tmin 0, tmax 1e30), int32 scene id per ray."""
+    import numpy as np
+    n_s = len(first) - 1
+    g = torch.Generator(device="cuda"); g.manual_seed(seed)
+    o = torch.empty((n_s * per, 4), dtype=torch.float32, device="cuda"); d = torch.empty_like(o)
+    for s in range(n_s):
+        a, b = int(first[s]), int(first[s + 1])
+        t = xf[a:b].reshape(-1, 3, 4)[:, :, 3] if b > a else np.zeros((1, 3), np.float32)
+        lo = torch.tensor(t.min(0) - extent, device="cuda"); hi = torch.tensor(t.max(0) + extent, device="cuda")
+        sl = slice(s * per, (s + 1) * per)
+        o[sl, :3] = lo + torch.rand((per, 3), generator=g, device="cuda") * (hi - lo); o[sl, 3] = 0.0
+        v = torch.randn((per, 3), generator=g, device="cuda"); v /= v.norm(dim=1, keepdim=True)
+        d[sl, :3] = v; d[sl, 3] = 1e30
+    sc = torch.arange(n_s, dtype=torch.int32, device="cuda").repeat_interleave(per)
+    return o, d, sc
+
+
+def cpu_batched_sample(b, tuning_width, n_scenes, n_inst, o, d, sc, seconds=12.0):
+    """The reference's two-level traversal (travInst, accel/traverse_inst.cuh, via oracle/_ref) on the host cores over
+    a strided sample of the queue on the GPU-built buffers; the oracle restatement when the reference is absent."""
+    import numpy as np
+    nodes, tris = b.download(tuning_width)
+    tlas, roots, inst = b.download_tlas(n_scenes, n_inst)
+    L = reference_lib(); threads = os.cpu_count() or 1
+    n = 1 << 12
+    while True:
+        step = max(1, len(o) // n)
+        oo = np.ascontiguousarray(o[::step][:n]); dd = np.ascontiguousarray(d[::step][:n]); ss = np.ascontiguousarray(sc[::step][:n])
+        m = len(oo)
+        hits = np.zeros((m, 4), np.float32); hi = np.zeros(m, np.int32)
+        if L is not None and hasattr(L, "ref_trace_inst"):
+            kind = "reference"
+            spent = L.ref_trace_inst(tuning_width, 0, 0, nodes.ctypes.data, tris.ctypes.data, tlas.ctypes.data, roots.ctypes.data, n_scenes, inst.ctypes.data,
+                                     oo.ctypes.data, dd.ctypes.data, ss.ctypes.data, m, hits.ctypes.data, hi.ctypes.data, threads)
+            spent += L.ref_trace_inst(tuning_width, 1, 0, nodes.ctypes.data, tris.ctypes.data, tlas.ctypes.data, roots.ctypes.data, n_scenes, inst.ctypes.data,
+                                      oo.ctypes.data, dd.ctypes.data, ss.ctypes.data, m, None, hi.ctypes.data, threads)
+        else:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            from conftest import Oracle
+            kind, threads = "port", 1
+            orc = Oracle(); t0 = time.perf_counter()
+            orc.trace_inst(tuning_width, False, nodes, tris, tlas, roots, inst, oo, dd, ss); orc.trace_inst(tuning_width, True, nodes, tris, tlas, roots, inst, oo, dd, ss)
+            spent = time.perf_counter() - t0
+        if spent >= seconds / 4 or m >= len(o):
+            break
+        n = min(len(o), int(n * max(2.0, min(16.0, seconds / 4 / max(spent, 1e-3)))))
+    return dict(value=2 * m / spent / 1e9, unit="Grays/s", cores=threads, kind=kind,
+                sample=f"every {step}th ray of the {len(o)}-ray queue ({m} rays, closest-hit and any-hit, {2 * m} rays in {spent:.2f} s)")
+
+
+def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_peak, peak_kind, out):
+    import numpy as np
+    import torch.distributed as tdist
+    t0 = time.perf_counter()
+    meshes, xf, mesh_of, first = batched_setup(cwp, wl)
+    gen_s = time.perf_counter() - t0
+    b = cwp.Batch(meshes, device=torch.cuda.current_device())
+    inst = cwp.instances(xf, mesh_of)
+    b.set_scenes(inst, first)
+    info = b.info()
+    n_s = len(first) - 1
+    per = args.rays if args.rays else wl["rays_per_scene"]
+    o, d, sc = batched_rays(torch, xf, first, per)
+    n = len(o)
+    hits = torch.empty((n, 4), dtype=torch.float32, device="cuda"); hi = torch.empty(n, dtype=torch.int32, device="cuda"); oi = torch.empty(n, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream()
+    # autotuner on a strided sample (every 32nd ray, all scenes represented)
+    samp = torch.arange(0, n, 32, device="cuda")
+    so, sd, ss = o[samp].contiguous(), d[samp].contiguous(), sc[samp].contiguous()
+    sh = torch.empty((len(samp), 4), dtype=torch.float32, device="cuda"); si = torch.empty(len(samp), dtype=torch.int32, device="cuda")
+    t1 = time.perf_counter()
+    tun = b.autotune(so.data_ptr(), sd.data_ptr(), ss.data_ptr(), sh.data_ptr(), si.data_ptr(), len(samp))
+    tune_s = time.perf_counter() - t1
+    del so, sd, ss, sh, si
+
+    def step(ev=None):
+        if ev: ev[0].record(st)
+        b.trace(o.data_ptr(), d.data_ptr(), sc.data_ptr(), hits.data_ptr(), hi.data_ptr(), n, stream=st.cuda_stream)
+        if ev: ev[1].record(st)
+        b.trace(o.data_ptr(), d.data_ptr(), sc.data_ptr(), 0, oi.data_ptr(), n, any_hit=True, stream=st.cuda_stream)
+        if ev: ev[2].record(st)
+    for _ in range(args.warmup):
+        step()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clk = Clocks(dev_id)
+    barrier()
+    torch.cuda.nvtx.range_push("timed")
+    for i in range(args.steps):
+        step(ev[i])
+    torch.cuda.nvtx.range_pop()
+    barrier()
+    clocks = clk.stop()
+    b.status()
+    c_ms = sum(e[0].elapsed_time(e[1]) for e in ev); a_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
+    max_ms = reduce(c_ms + a_ms, tdist.ReduceOp.MAX if ws > 1 else None)
+    value = 2 * n * args.steps * ws / (max_ms * 1e-3) / 1e9
+    hit_rate = float((hi >= 0).float().mean().item())
+    # e2e: pinned host queue in, hits + instances out, every step, through the C ABI
+    ho, hd, hs = o.cpu().pin_memory(), d.cpu().pin_memory(), sc.cpu().pin_memory()
+    hh = torch.empty((n, 4), dtype=torch.float32, pin_memory=True); hhi = torch.empty(n, dtype=torch.int32, pin_memory=True); hoi = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    barrier(); t2 = time.perf_counter()
+    for _ in range(args.steps):
+        o.copy_(ho, non_blocking=True); d.copy_(hd, non_blocking=True); sc.copy_(hs, non_blocking=True)
+        step()
+        hh.copy_(hits, non_blocking=True); hhi.copy_(hi, non_blocking=True); hoi.copy_(oi, non_blocking=True)
+    barrier(); e_s = reduce(time.perf_counter() - t2, tdist.ReduceOp.MAX if ws > 1 else None)
+    dom_ms, dom_b, dom = (c_ms, 56.0, "k_batch_trace (closest)") if c_ms >= a_ms else (a_ms, 40.0, "k_batch_trace (any)")
+    achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
+    out.update(metric="closest+any rays per second, batched two-level scenes", value=value, ms_per_step=max_ms / args.steps,
+               config={"workload": args.workload, "scenes": n_s, "blas": info.n_blas, "tris": int(info.n_tris), "instances": int(info.n_instances),
+                       "rays": n, "rays_per_scene": per, "hit_rate": hit_rate,
+                       "tuning": {"block": tun.block, "width": tun.width, "fetch": tun.fetch, "smem_stack": tun.smem_stack, "sample_ms": tun.ms},
+                       "autotune_s": tune_s, "blas_build_ms": info.blas_build_ms, "blas_hploc_launches": info.blas_hploc_launches,
+                       "tlas_build_ms": info.tlas_build_ms, "node_bytes": {"bvh2": int(info.node_bytes[0]), "bvh4": int(info.node_bytes[1]), "cwbvh": int(info.node_bytes[2])},
+                       "scene_generation_s": gen_s, "l2": f"ray queue {n * 36 / 1e9:.1f} GB > L2 (126 MB)",
+                       "closest_ms": c_ms / args.steps, "any_ms": a_ms / args.steps, "tri": "moller-trumbore"},
+               clocks=clocks,
+               e2e={"value": 2 * n * args.steps * ws / e_s / 1e9, "unit": "Grays/s", "h2d_bytes_per_step": n * 36, "d2h_bytes_per_step": n * 24},
+               gpu_launches=2 * args.steps,
+               roofline={"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic": "closest: 32 B ray + 4 B scene id in, 16 B hit + 4 B instance out; any: 36 B in + 4 B out"})
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        oh, dh, sh_ = o.cpu().numpy(), d.cpu().numpy(), sc.cpu().numpy()
+        out["cpu_baseline"] = cpu_batched_sample(b, tun.width, n_s, len(mesh_of), oh, dh, sh_, seconds=args.ref_seconds)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -207,7 +348,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--spp", type=int, default=0, help="override the frame's samples per pixel (profiling cases)")
-    ap.add_argument("--rays", type=int, default=0, help="override the batch size of trace16m (profiling cases)")
+    ap.add_argument("--rays", type=int, default=0, help="override the batch size of trace16m / rays per scene of batched64 (profiling cases)")
+    ap.add_argument("--scenes", type=int, default=0, help="override the scene count of batched64 (profiling cases)")
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     args = ap.parse_args()
@@ -218,6 +360,8 @@ def main():
         wl["spp"] = args.spp
     if args.rays and "rays" in wl:
         wl["rays"] = args.rays
+    if args.scenes and wl.get("batched"):
+        wl["scenes"] = args.scenes
     if args.precision and "rays" in wl:
         wl["precision"] = True
     ws, rank, local = dist_setup(args)
@@ -233,7 +377,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     cwp = importlib.import_module("cuda-wavefront-pathtracer_b200")
     variant = args.variant
-    mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=args.bins)
+    if not wl.get("batched"):
+        mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=args.bins)
 
     def barrier():
         if ws > 1:
@@ -258,7 +403,9 @@ def main():
     out = {"metric": "", "value": 0.0, "unit": "Grays/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 0.0,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
     import torch.distributed as tdist
-    if "rays" not in wl:
+    if wl.get("batched"):
+        bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_peak, peak_kind, out)
+    elif "rays" not in wl:
         # ------------------------------------------------------------------ frames
         w, h, spp, K, B = wl["w"], wl["h"], wl["spp"], wl["batch"], wl["bounces"]
         p = cwp.frame_params(mesh, w, h, bounces=B)
@@ -404,7 +551,7 @@ def main():
                              "peak_kind": peak_kind, "traffic": None,
                              "algorithmic": "closest: 32 B ray in + 16 B hit out; any: 32 B in + 4 B out"})
         acc.close()
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and not wl.get("batched"):
         if "rays" not in wl:
             out["cpu_baseline"] = cpu_frame_sample(cwp, wl, mesh, bvh, variant)
         else:

@@ -4,6 +4,7 @@
 //   builder / layouts ... accel/bvh_builder.cpp, accel/bvh_layouts.cpp, accel/bvh_tools.cpp, accel/tri_pack.cpp
 //   traversal ........... accel/traverse.cuh trav<V, ANY, TRI> compiled as host C++ through ref_shim.h
 //   instance transforms . scene/instances.cpp invertXform / instanceXform (with io/json.cpp, which it links)
+//   two-level traversal . accel/traverse_inst.cuh travInst<V, ANY, TRI> compiled as host C++ through ref_shim.h
 // The harness (threads, argument marshalling) is ours; the arithmetic is the reference's.
 #include "ref_shim.h"
 #include "accel/bvh_builder.h"
@@ -11,6 +12,7 @@
 #include "accel/bvh_tools.h"
 #include "accel/tri_pack.h"
 #include "accel/traverse.cuh"
+#include "accel/traverse_inst.cuh"
 #include "core/rng.h"
 #include "scene/instances.h"
 #include "core/sampling.h"
@@ -178,4 +180,33 @@ extern "C" void ref_xform_animate(const float* translate, const float* translate
     d.scale = make_float3(scale[0], scale[1], scale[2]); d.scaleVel = make_float3(scale_vel[0], scale_vel[1], scale_vel[2]);
     const Xform X = instanceXform(d, frame);
     for (int i = 0; i < 12; i++) m[i] = X.m[i];
+}
+
+// The reference's two-level traversal (accel/traverse_inst.cuh:10-41) over a scene-tagged ray batch on `threads` host
+// threads: TLAS = BVH2 nodes with instance leaves, roots per scene, DevInstance records (accel/instance.h:7, the same
+// 112-byte layout as cwp_instance), BLAS nodes / triangles with absolute indices. Returns seconds.
+extern "C" double ref_trace_inst(int variant, int any, int tri, const float* blas, const float* tv, const float* tlas, const int* scene_root, int n_scenes,
+                                 const void* inst, const float* ro, const float* rd, const int* scene_of, long n, float* hits, int* hit_inst, int threads) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    auto fn = [&](long b, long e) {
+        const float4 *N = (const float4*)blas, *T = (const float4*)tv, *TL = (const float4*)tlas, *O = (const float4*)ro, *D = (const float4*)rd;
+        const DevInstance* I = (const DevInstance*)inst;
+        for (long i = b; i < e; i++) {
+            const float4 o = O[i], d = D[i]; float t = d.w, u = 0.f, v = 0.f; int h = -1, hi = -1;
+            const int sc = scene_of[i], root = sc >= 0 && sc < n_scenes ? scene_root[sc] : -1;
+            if (root >= 0) {
+#define REF_INST(VV) do { if (any) { if (tri) travInst<VV, true, 1>(TL, root, I, N, T, xyz(o), xyz(d), o.w, t, h, u, v, hi); else travInst<VV, true, 0>(TL, root, I, N, T, xyz(o), xyz(d), o.w, t, h, u, v, hi); } \
+                         else { if (tri) travInst<VV, false, 1>(TL, root, I, N, T, xyz(o), xyz(d), o.w, t, h, u, v, hi); else travInst<VV, false, 0>(TL, root, I, N, T, xyz(o), xyz(d), o.w, t, h, u, v, hi); } } while (0)
+                if (variant == 2) REF_INST(2); else if (variant == 4) REF_INST(4); else REF_INST(8);
+#undef REF_INST
+            }
+            if (hits) { hits[4 * i] = t; hits[4 * i + 1] = u; hits[4 * i + 2] = v; hits[4 * i + 3] = __int_as_float(h); }
+            hit_inst[i] = hi;
+        }
+    };
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> ts;
+    for (int k = 0; k < threads; k++) ts.emplace_back(fn, n * k / threads, n * (k + 1) / threads);
+    for (auto& t : ts) t.join();
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }

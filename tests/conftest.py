@@ -154,6 +154,8 @@ class Ref:
         L.ref_xform_animate.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_float, C.c_float] + [C.POINTER(C.c_float)] * 2 + [C.c_int, C.POINTER(C.c_float)]
         L.ref_trace.restype = C.c_double
         L.ref_trace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_int]
+        L.ref_trace_inst.restype = C.c_double
+        L.ref_trace_inst.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_long, C.c_void_p, C.c_void_p, C.c_int]
         self.L = L
 
     def build(self, verts, faces, fm, variant=2, leaf=4, collapse=0):
@@ -166,6 +168,16 @@ class Ref:
                              order.ctypes.data, tris.ctypes.data, woop.ctypes.data, C.byref(md), C.byref(sah), C.byref(ms))
         assert n > 0
         return dict(nodes=nodes[:n].copy(), order=order, tris=tris, woop=woop, max_depth=md.value, sah=sah.value)
+
+    def trace_inst(self, width, any_hit, blas, tris, tlas, scene_root, inst, o, d, scene_of, threads=0):
+        """The reference's travInst (Moller-Trumbore leaves) over a scene-tagged batch: (hits, hit instance)."""
+        n = len(o)
+        hits = np.zeros((n, 4), np.float32); hi = np.zeros(n, np.int32)
+        a = [np.ascontiguousarray(x) for x in (blas, tris, tlas)]
+        sr = np.ascontiguousarray(scene_root, np.int32); ins = np.ascontiguousarray(inst, np.float32); so = np.ascontiguousarray(scene_of, np.int32)
+        self.L.ref_trace_inst(width, 1 if any_hit else 0, 0, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, sr.ctypes.data, len(sr), ins.ctypes.data,
+                              np.ascontiguousarray(o).ctypes.data, np.ascontiguousarray(d).ctypes.data, so.ctypes.data, n, hits.ctypes.data, hi.ctypes.data, threads)
+        return hits, hi
 
     def trace(self, variant, tri, any_hit, nodes, tv, o, d, threads=0):
         n = len(o)
