@@ -93,7 +93,8 @@ def test_two_level_trace_matches_reference_travinst(gpu, cwp, ref, batch_case, w
     """The reference's own two-level traversal (travInst, compiled from its sources for the host) over the buffers the
     GPU built: the same closest hit (instance, triangle) on every ray up to exact-distance ties (the reference
     enters a TLAS leaf's instances as soon as its node is visited, this traversal when the leaf comes up in
-    nearer-first order), and the same occlusion."""
+    nearer-first order; box bottoms are coplanar with the ground, so rays from below meet many exact ties), and the
+    same occlusion."""
     meshes, xf, mesh_of, first, b, o, d, sc = batch_case
     b.set_tuning(block=128, width=width, fetch=8, smem_stack=0)
     nodes, tris = b.download(width)
@@ -103,7 +104,7 @@ def test_two_level_trace_matches_reference_travinst(gpu, cwp, ref, batch_case, w
     tri, trr = h[:, 3].view(np.int32), hr[:, 3].view(np.int32)
     same = (tri == trr) & (hi == hir)
     tie = ~same & (tri >= 0) & (trr >= 0) & (np.abs(h[:, 0].astype(np.float64) - hr[:, 0]) <= 1e-6 * np.abs(hr[:, 0].astype(np.float64)))
-    assert np.all(same | tie) and tie.mean() < 1e-3
+    assert np.all(same | tie) and tie.mean() < 0.02
     _, oi = trace(gpu, b, o, d, sc, any_hit=True)
     _, oir = ref.trace_inst(width, True, nodes, tris, tlas, roots, inst, o, d, sc)
     assert np.array_equal(oi >= 0, oir >= 0)
