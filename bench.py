@@ -352,6 +352,7 @@ def main():
     ap.add_argument("--scenes", type=int, default=0, help="override the scene count of batched64 (profiling cases)")
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
+    ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.batch:
@@ -410,7 +411,7 @@ def main():
         w, h, spp, K, B = wl["w"], wl["h"], wl["spp"], wl["batch"], wl["bounces"]
         p = cwp.frame_params(mesh, w, h, bounces=B)
         r = cwp.Renderer()
-        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1, traversal=args.traversal)
+        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1, traversal=args.traversal, sort=args.sort)
         for _ in range(args.warmup):
             r.render(spp)
         depths = B + 2
@@ -449,7 +450,7 @@ def main():
         out.update(metric="closest+shadow rays per second, diffuse frame", value=value, ms_per_step=max_ms / args.steps,
                    config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles, box field seed 1)", "resolution": f"{w}x{h}",
                            "spp": spp, "batch": K, "depth": B, "layout": LAYOUT_NAMES[variant], "sah_bins": args.bins, "tri": "woop",
-                           "graph": args.graph, "traversal": ["auto", "refill", "batch"][args.traversal], "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
+                           "graph": args.graph, "traversal": ["auto", "refill", "batch"][args.traversal], "sort": ["off", "octant", "octant+cell"][args.sort], "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
                            "rays_per_frame": (rays + shadow) / args.steps, "closest_per_frame": rays / args.steps, "shadow_per_frame": shadow / args.steps,
                            "rays_per_sample": (rays + shadow) / args.steps / (w * h * spp), "trace_shade_ms": float(tms.sum() / args.steps),
                            "shadow_ms": float(sms.sum() / args.steps)},

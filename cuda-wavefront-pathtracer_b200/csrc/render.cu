@@ -14,6 +14,7 @@
 // their queue lengths from device memory, so a whole frame is captured once as a CUDA graph and replayed.
 #include "scene_dev.h"
 #include "trav.cuh"
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -276,9 +277,57 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow(const __grid_co
     if (err) atomicOr(a.err, err);
 }
 
+// ---------------- continuation regrouping (cwp_render_options.sort) ----------------
+// Before a bounce, the continuation rays are counting-sorted into bins of direction octant (and, for sort = 2, a 4 x 4 x
+// 4 cell of the scene box around their origin), so the rays a warp fetches together descend the tree in the same order.
+// Three light passes over the queue: histogram, exclusive scan of the bins, scatter of the 40-byte entries.
+static constexpr int kSortBins = 512;
+struct SortArgs { const float4* s0; const float4* s1; const float2* s2; float4* t0; float4* t1; float2* t2; const int* n; int* hist; int* cursor;
+                  float3 lo, inv; int mode; };
+__device__ __forceinline__ int sort_key(const SortArgs& a, float4 o, float4 d) {
+    int k = (d.x < 0.f ? 1 : 0) | (d.y < 0.f ? 2 : 0) | (d.z < 0.f ? 4 : 0);
+    if (a.mode == 2) {
+        const int cx = min(max((int)((o.x - a.lo.x) * a.inv.x), 0), 3), cy = min(max((int)((o.y - a.lo.y) * a.inv.y), 0), 3), cz = min(max((int)((o.z - a.lo.z) * a.inv.z), 0), 3);
+        k = (k << 6) | (cz << 4) | (cy << 2) | cx;
+    }
+    return k;
+}
+__global__ void __launch_bounds__(256) k_sort_hist(const SortArgs a) {
+    __shared__ int h[kSortBins];
+    for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const int n = *a.n;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) atomicAdd_block(&h[sort_key(a, __ldcs(a.s0 + k), __ldg(a.s1 + k))], 1);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) if (h[i]) atomicAdd(&a.hist[i], h[i]);
+}
+__global__ void __launch_bounds__(kSortBins) k_sort_scan(const SortArgs a) {
+    __shared__ int v[kSortBins];
+    const int i = threadIdx.x, x = a.hist[i];
+    v[i] = x; __syncthreads();
+    for (int off = 1; off < kSortBins; off <<= 1) { const int y = i >= off ? v[i - off] : 0; __syncthreads(); v[i] += y; __syncthreads(); }
+    a.cursor[i] = v[i] - x;
+}
+__global__ void __launch_bounds__(256) k_sort_scatter(const SortArgs a) {
+    const int n = *a.n, lane = threadIdx.x & 31;
+    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < n; base += gridDim.x * blockDim.x) {
+        const int k = base + lane; const bool ok = k < n;
+        float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = o; float2 t = make_float2(0.f, 0.f);
+        if (ok) { o = __ldcs(a.s0 + k); d = __ldcs(a.s1 + k); t = __ldcs(a.s2 + k); }
+        const int key = ok ? sort_key(a, o, d) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        int pos = 0;
+        if (ok && lane == leader) pos = atomicAdd(&a.cursor[key], __popc(peers));
+        pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(peers & lanemask_lt());
+        if (ok) { __stcs(a.t0 + pos, o); __stcs(a.t1 + pos, d); __stcs(a.t2 + pos, t); }
+    }
+}
+
 // pass set-up: depth-0 queue length = nk; everything else zero
-__global__ void k_pass_begin(int* cnt, int nInts, int nk) {
+__global__ void k_pass_begin(int* cnt, int nInts, int nk, int* bins, int nBins) {
     for (int i = threadIdx.x; i < nInts; i += blockDim.x) cnt[i] = i == 0 ? nk : 0;
+    for (int i = threadIdx.x; i < nBins; i += blockDim.x) bins[i] = 0;
 }
 // per-depth ray totals of a pass: tot[2 d] += queue length, tot[2 d + 1] += shadow queue length
 __global__ void k_pass_end(const int* cnt, int depths, unsigned long long* tot) {
@@ -292,6 +341,8 @@ using namespace cwpb;
 struct cwp_renderer {
     cwp_params P{}; cwp_render_options O{};
     DeviceScene scene;
+    float4 *t0 = nullptr, *t1 = nullptr; float2* t2 = nullptr; int* sortBins = nullptr;   // regrouped continuation queue, bins per depth
+    float3 boxLo{}, boxInv{};
     int N = 0, K = 1, depths = 0; long long nk = 0; bool ready = false;
     Queues q{};
     float4* accum = nullptr; int* cnt = nullptr; int* err = nullptr; unsigned long long* tot = nullptr;   // tot: 2 per depth
@@ -339,6 +390,14 @@ template <int V, int TRI> void launch_depth(cwp_renderer* r, KArgs a, int gt0, i
         if (a.depth == 0) k_trace_shade<V, TRI, true><<<gt0, 128, 0, r->st>>>(a, r->P);
         else k_trace_shade<V, TRI, false><<<gt, 128, 0, r->st>>>(a, r->P);
     }
+    if (r->O.sort && a.depth + 1 < r->depths) {   // regroup the continuations that the next bounce traces
+        const int wr = (a.depth & 1) ^ 1;
+        SortArgs sa{ r->q.s0[wr], r->q.s1[wr], r->q.s2[wr], r->t0, r->t1, r->t2, a.cnt + 4 * (a.depth + 1), r->sortBins + 2 * kSortBins * a.depth,
+                     r->sortBins + 2 * kSortBins * a.depth + kSortBins, r->boxLo, r->boxInv, r->O.sort };
+        k_sort_hist<<<r->nSM * 4, 256, 0, r->st>>>(sa);
+        k_sort_scan<<<1, kSortBins, 0, r->st>>>(sa);
+        k_sort_scatter<<<r->nSM * 8, 256, 0, r->st>>>(sa);
+    }
     if (ev) { cudaEventRecordWithFlags(ev[1], r->st, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], r->st, cudaEventRecordExternal); }
     if constexpr (V != 4) { if (rfShadow) k_shadow_rf<V, TRI><<<gs, 128, 0, r->st>>>(a); }
     if (!rfShadow) k_shadow<V, TRI><<<gs, 128, 0, r->st>>>(a);
@@ -354,6 +413,7 @@ KArgs base_args(cwp_renderer* r) {
 
 void dispatch_depth(cwp_renderer* r, KArgs a, int gt0, int gt, int gs, int pass) {
     const int V = r->scene.variant, T = r->scene.tri;
+    if (r->O.sort && a.depth > 0) { const int rd = a.depth & 1; a.q.s0[rd] = r->t0; a.q.s1[rd] = r->t1; a.q.s2[rd] = r->t2; }
     cudaEvent_t* ev = r->O.profile ? &r->ev[((size_t)pass * r->depths + a.depth) * 4] : nullptr;
     if (V == 2) { if (T) launch_depth<2, 1>(r, a, gt0, gt, gs, ev); else launch_depth<2, 0>(r, a, gt0, gt, gs, ev); }
     else if (V == 4) { if (T) launch_depth<4, 1>(r, a, gt0, gt, gs, ev); else launch_depth<4, 0>(r, a, gt0, gt, gs, ev); }
@@ -372,7 +432,7 @@ int ensure_events(cwp_renderer* r, int passes) {
 int enqueue_passes(cwp_renderer* r, int spp, int sBase) {
     const int nInts = 4 * (r->depths + 1);
     for (int s = sBase, pass = 0; s < sBase + spp; s += r->K, pass++) {
-        k_pass_begin<<<1, 128, 0, r->st>>>(r->cnt, nInts, (int)r->nk);
+        k_pass_begin<<<1, 128, 0, r->st>>>(r->cnt, nInts, (int)r->nk, r->sortBins, r->sortBins ? 2 * kSortBins * r->depths : 0);
         KArgs a = base_args(r); a.sBase = s;
         for (int d = 0; d < r->depths; d++) { a.depth = d; dispatch_depth(r, a, r->gridTrace0, r->gridTrace, r->gridShadow, pass); }
         k_pass_end<<<1, 32, 0, r->st>>>(r->cnt, r->depths, r->tot);
@@ -389,6 +449,7 @@ void release(cwp_renderer* r) {
     r->gexec = nullptr; r->gSpp = -1;
     for (void* p : r->allocs) cudaFree(p);
     r->allocs.clear();
+    r->t0 = r->t1 = nullptr; r->t2 = nullptr; r->sortBins = nullptr;
     if (r->hcnt) cudaFreeHost(r->hcnt);
     r->hcnt = nullptr;
     free_scene(r->scene);
@@ -439,6 +500,20 @@ extern "C" int cwp_renderer_init(cwp_renderer* r, const cwp_params* p, const cwp
     int rc = 0;
     for (int b = 0; b < 2 && !rc; b++) {
         rc = alloc((void**)&r->q.s0[b], NK * 16); if (!rc) rc = alloc((void**)&r->q.s1[b], NK * 16); if (!rc) rc = alloc((void**)&r->q.s2[b], NK * 8);
+    }
+    CWPB_CHECK(o->sort >= 0 && o->sort <= 2, CWP_ERR_INVALID, "sort %d is not 0, 1 or 2", o->sort);
+    if (o->sort) {
+        rc = alloc((void**)&r->t0, NK * 16); if (!rc) rc = alloc((void**)&r->t1, NK * 16); if (!rc) rc = alloc((void**)&r->t2, NK * 8);
+        if (!rc) rc = alloc((void**)&r->sortBins, (size_t)2 * kSortBins * r->depths * sizeof(int));
+        // scene box from the triangles (v0, v0 + e1, v0 + e2) for the origin cells
+        float lo[3] = { 3e38f, 3e38f, 3e38f }, hi[3] = { -3e38f, -3e38f, -3e38f };
+        for (int64_t t = 0; t < s->n_tris && !rc; t++)
+            for (int c = 0; c < 3; c++) {
+                const float* v = s->tris + 12 * t;
+                for (int ax = 0; ax < 3; ax++) { const float x = v[ax] + (c ? s->tris[12 * t + 4 * c + ax] : 0.f); lo[ax] = std::min(lo[ax], x); hi[ax] = std::max(hi[ax], x); }
+            }
+        r->boxLo = f3(lo[0], lo[1], lo[2]);
+        r->boxInv = f3(4.f / std::max(hi[0] - lo[0], 1e-30f), 4.f / std::max(hi[1] - lo[1], 1e-30f), 4.f / std::max(hi[2] - lo[2], 1e-30f));
     }
     if (!rc) rc = alloc((void**)&r->q.h0, NK * 16);
     if (!rc) rc = alloc((void**)&r->q.h1, NK * 16);
@@ -513,7 +588,7 @@ extern "C" int cwp_renderer_render(cwp_renderer* r, int32_t spp, cwp_frame_stats
         // host loop: exact grids from the queue lengths read back after each depth (one sync per bounce)
         const int nInts = 4 * (r->depths + 1);
         for (int s = sBase, pass = 0; s < sBase + spp; s += r->K, pass++) {
-            k_pass_begin<<<1, 128, 0, r->st>>>(r->cnt, nInts, (int)r->nk);
+            k_pass_begin<<<1, 128, 0, r->st>>>(r->cnt, nInts, (int)r->nk, r->sortBins, r->sortBins ? 2 * kSortBins * r->depths : 0);
             KArgs a = base_args(r); a.sBase = s;
             int n = (int)r->nk;
             if (r->O.profile) for (int d = 0; d < r->depths; d++) for (int j = 0; j < 4; j++) CWPB_CUDA(cudaEventRecord(r->ev[((size_t)pass * r->depths + d) * 4 + j], r->st));
@@ -688,7 +763,7 @@ extern "C" int cwp_render_noalloc(const cwp_params* p, const cwp_device_scene* s
     a.nrm = (const float4*)s->nrm; a.albedo = (const float3*)s->albedo;
     a.q = q; a.accum = (float4*)d_accum; a.cnt = cnt; a.err = err; a.nk = (int)nk; a.N = N;
     for (int sb = s_base; sb < s_base + spp; sb += o->batch) {
-        k_pass_begin<<<1, 128, 0, st>>>(cnt, 4 * (depths + 1), (int)nk);
+        k_pass_begin<<<1, 128, 0, st>>>(cnt, 4 * (depths + 1), (int)nk, nullptr, 0);
         a.sBase = sb;
         for (int d = 0; d < depths; d++) {
             a.depth = d;

@@ -45,6 +45,18 @@ def test_graph_and_host_loop_agree(gpu, cwp):
     assert np.allclose(a1, a2, rtol=1e-5, atol=1e-6)                  # only the float-atomic order differs
 
 
+@pytest.mark.parametrize("sort", [1, 2])
+def test_regrouped_continuations_render_the_same_frame(gpu, cwp, sort):
+    """Regrouping the continuation rays before each bounce only changes the order in which paths are traced: the same
+    rays are cast and the image agrees up to the order of float atomics."""
+    mesh, bvh = cwp.scene("boxes12k", variant=8, bins=32)
+    p = cwp.frame_params(mesh, 96, 64)
+    r0 = cwp.Renderer(); r0.init(p, bvh, variant=8, batch=4, bounces=4); s0 = r0.render(8)
+    r1 = cwp.Renderer(); r1.init(p, bvh, variant=8, batch=4, bounces=4, sort=sort); s1 = r1.render(8)
+    assert s0.rays == s1.rays and s0.shadow_rays == s1.shadow_rays
+    assert np.allclose(r0.read_accum(), r1.read_accum(), rtol=1e-5, atol=1e-6)
+
+
 def test_progressive_accumulation(gpu, cwp):
     """render(8) == render(4, s_base 0) + render(4, s_base 4, clear=False): the sample range is the resume point."""
     mesh, bvh = cwp.scene("boxes12k", variant=2, bins=32)
