@@ -8,6 +8,9 @@ Workloads (synthetic box-field scenes standing in for the reference's unreleased
   trace16m  117,002 triangles, 2^24 incoherent rays traced closest-hit and any-hit
   precision1m  12,290 triangles, 2^20 incoherent rays, precision form (f16 conservative slabs + watertight FP32
             triangles) closest + any, checked against the FP64 oracle (lost hits, ties, max relative t error)
+  serving   32 resident two-level scenes (animated instances, OpenPBR materials), a Poisson stream of requests
+            (256^2..1080p, 1..256 spp, depth 8) served with continuous batching and, on the same stream, by the plain
+            form (one request at a time); request throughput, p50 / p95 / p99 latency, Grays/s of both
   batched64  64 two-level scenes (TLAS over 1-4,096 instances of 1-8 box-field BLAS of 1k-500k triangles each, all
             BLAS built on the GPU by one H-PLOC launch), 4M rays per scene in one scene-tagged queue, closest + any
             in one persistent launch each, launch shape chosen by the autotuner
@@ -38,6 +41,7 @@ WORKLOADS = {
     "frame256": dict(scene="boxes12k", w=256, h=256, spp=16, batch=16, bounces=4),
     "trace16m": dict(scene="boxes117k", rays=1 << 24),
     "precision1m": dict(scene="boxes12k", rays=1 << 20, precision=True),
+    "serving": dict(serving=True, scenes=32, requests=64, rate=100.0, max_paths=16 << 20, max_requests=64, seed=7),
     "batched64": dict(batched=True, scenes=64, rays_per_scene=4 << 20, tris=(1000, 500000), instances=(1, 4096), blas=(1, 8), seed=5),
 }
 STATE_BYTES = 40          # path state per queued ray: (o, id) + (d, T.r) + (T.g, T.b); shadow entries the same size
@@ -334,6 +338,62 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
         out["cpu_baseline"] = cpu_batched_sample(b, tun.width, n_s, len(mesh_of), oh, dh, sh_, seconds=args.ref_seconds)
 
 
+def serve_stream(cwp, s, stream):
+    """Feeds (arrival_s, request) pairs at their arrival times and steps the server until all are done: per request
+    (latency ms, rays, shadow rays); throughput over the span from the first arrival to the last completion."""
+    t0 = s.clock_ms(); todo = list(stream); ids = {}; done = {}
+    while len(done) < len(stream):
+        if s.clock_ms() - t0 > 900e3:
+            raise RuntimeError(f"serving stream did not finish in 900 s ({len(done)} of {len(stream)} done)")
+        now = (s.clock_ms() - t0) / 1e3
+        while todo and todo[0][0] <= now:
+            arr, r = todo.pop(0); ids[s.submit(r)] = arr
+        a, p = s.step()
+        for i in s.poll():
+            _, st = s.result(i)
+            done[i] = (st.done_ms - st.submit_ms, st.rays, st.shadow_rays, st.done_ms - t0)
+        if a == 0 and p == 0 and todo and len(done) < len(stream):
+            time.sleep(max(0.0, min(0.002, todo[0][0] - (s.clock_ms() - t0) / 1e3)))
+    lat = sorted(v[0] for v in done.values())
+    span = max(v[3] for v in done.values()) / 1e3 - stream[0][0]
+    rays = sum(v[1] + v[2] for v in done.values())
+    q = lambda f: lat[min(len(lat) - 1, int(f * len(lat)))]
+    return {"requests": len(lat), "throughput_req_s": len(lat) / span, "grays_s": rays / span / 1e9, "p50_ms": q(0.50), "p95_ms": q(0.95), "p99_ms": q(0.99),
+            "span_s": span, "rays": rays}
+
+
+def bench_serving(args, wl, cwp, torch, out):
+    import numpy as np
+    t0 = time.perf_counter()
+    meshes, descs, first, mats, base, boxes = cwp.serving_scenes(n_scenes=wl["scenes"], seed=wl["seed"])
+    b = cwp.Batch(meshes, device=torch.cuda.current_device())
+    gen_s = time.perf_counter() - t0
+    n_req = args.rays if args.rays else wl["requests"]
+    stream = cwp.serving_requests(n_req, wl["rate"], boxes, seed=wl["seed"] + 1)
+    res = {}
+    for mode, maxr in (("continuous", wl["max_requests"]), ("plain", 1)):
+        s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=maxr)
+        s.set_scenes(descs, first)
+        clk = Clocks(str(torch.cuda.current_device()))
+        res[mode] = serve_stream(cwp, s, stream)
+        res[mode]["clocks"] = clk.stop()
+        del s
+    c, p = res["continuous"], res["plain"]
+    info = b.info()
+    out.update(metric="serving request throughput (continuous batching), Poisson stream", value=c["throughput_req_s"], unit="req/s",
+               ms_per_step=1e3 / c["throughput_req_s"], higher_is_better=True, dtype="f32",
+               config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "requests": n_req,
+                       "arrival_rate_req_s": wl["rate"], "resolutions": "256^2, 512^2, 1280x720, 1920x1080", "spp": "1, 4, 16, 64, 256", "depth": 8,
+                       "materials": "OpenPBR subset: roughness U[0.05,1], metallic Bernoulli(0.3), 10% glass IOR 1.5", "max_paths": wl["max_paths"],
+                       "max_requests": wl["max_requests"], "continuous": {k: v for k, v in c.items() if k != "clocks"},
+                       "plain": {k: v for k, v in p.items() if k != "clocks"}, "throughput_vs_plain": c["throughput_req_s"] / p["throughput_req_s"],
+                       "p99_vs_plain": c["p99_ms"] / p["p99_ms"], "scene_generation_s": gen_s, "blas_build_ms": info.blas_build_ms},
+               clocks=c["clocks"],
+               e2e={"value": c["throughput_req_s"], "unit": "req/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
+                    "note": "requests enter through the C ABI with host descriptors; every image is copied back to host memory (cwp_server_result) inside the served span"},
+               gpu_launches=None)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,7 +438,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     cwp = importlib.import_module("cuda-wavefront-pathtracer_b200")
     variant = args.variant
-    if not wl.get("batched"):
+    if not wl.get("batched") and not wl.get("serving"):
         mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=args.bins)
 
     def barrier():
@@ -404,7 +464,9 @@ def main():
     out = {"metric": "", "value": 0.0, "unit": "Grays/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 0.0,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
     import torch.distributed as tdist
-    if wl.get("batched"):
+    if wl.get("serving"):
+        bench_serving(args, wl, cwp, torch, out)
+    elif wl.get("batched"):
         bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_peak, peak_kind, out)
     elif "rays" not in wl:
         # ------------------------------------------------------------------ frames
@@ -552,7 +614,7 @@ def main():
                              "peak_kind": peak_kind, "traffic": None,
                              "algorithmic": "closest: 32 B ray in + 16 B hit out; any: 32 B in + 4 B out"})
         acc.close()
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline and not wl.get("batched"):
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and not wl.get("batched") and not wl.get("serving"):
         if "rays" not in wl:
             out["cpu_baseline"] = cpu_frame_sample(cwp, wl, mesh, bvh, variant)
         else:

@@ -7,6 +7,7 @@ There is no CPU fallback: every compute call goes through the CUDA library, and 
 libcwpb200.so has not been built.
 """
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -99,6 +100,26 @@ class BatchInfo(C.Structure):
                 ("blas_build_ms", C.c_double), ("tlas_build_ms", C.c_double), ("blas_hploc_launches", C.c_int32), ("pad", C.c_int32)]
 
 
+class Material(C.Structure):
+    _fields_ = [("base_color", C.c_float * 3), ("metallic", C.c_float), ("specular_color", C.c_float * 3), ("roughness", C.c_float),
+                ("emission", C.c_float * 3), ("ior", C.c_float), ("specular_weight", C.c_float), ("transmission", C.c_float), ("pad0", C.c_float), ("pad1", C.c_float)]
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("max_paths", C.c_int64), ("max_requests", C.c_int32), ("gd_energy", C.c_int32), ("hbm_reserve", C.c_int64), ("device", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
+
+
+class Request(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("frame", C.c_int32), ("cam", Camera), ("spp", C.c_int32), ("max_depth", C.c_int32), ("seed", C.c_uint32),
+                ("sun_to", C.c_float * 3), ("sun_e", C.c_float * 3), ("sky", C.c_float * 3), ("sun_cos", C.c_float), ("eps", C.c_float)]
+
+
+class RequestStats(C.Structure):
+    _fields_ = [("submit_ms", C.c_double), ("admit_ms", C.c_double), ("done_ms", C.c_double), ("rays", C.c_double), ("shadow_rays", C.c_double),
+                ("w", C.c_int32), ("h", C.c_int32), ("spp", C.c_int32), ("pad", C.c_int32)]
+
+
 # every exported symbol of the C ABI with its ctypes signature (restype, argtypes)
 SIGNATURES = {
     "cwp_last_error": (C.c_char_p, []),
@@ -149,6 +170,16 @@ SIGNATURES = {
     "cwp_batch_blas_root": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "cwp_batch_download_tlas": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64), C.c_void_p, C.c_void_p]),
     "cwp_batch_status": (C.c_int, [C.c_void_p]),
+    "cwp_server_create": (C.c_int, [C.c_void_p, C.POINTER(Material), C.c_int32, C.POINTER(C.c_int32), C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
+    "cwp_server_destroy": (None, [C.c_void_p]),
+    "cwp_server_set_scenes": (C.c_int, [C.c_void_p, C.POINTER(InstanceDesc), C.c_int64, C.POINTER(C.c_int32), C.c_int32]),
+    "cwp_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_int64)]),
+    "cwp_server_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "cwp_server_poll": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_int32)]),
+    "cwp_server_result": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.POINTER(RequestStats)]),
+    "cwp_server_clock_ms": (C.c_double, [C.c_void_p]),
+    "cwp_bsdf_eval_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 4 + [C.c_int32] + [C.c_void_p] * 3 + [C.c_int64]),
+    "cwp_bsdf_sample_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 3 + [C.c_int32] + [C.c_void_p] * 6 + [C.c_int64]),
     "cwp_camera_look_at": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_camera_from_c2w": (C.c_int, [C.POINTER(C.c_float), C.c_float, C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_params_defaults": (C.c_int, [C.POINTER(Params)]),
@@ -494,6 +525,91 @@ class Batch:
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value and _lib is not None:
             _lib.cwp_batch_destroy(self._h); self._h = C.c_void_p()
+
+
+def materials_array(m):
+    """(Material * n) from a float32 [n, 16] array in the cwp_material layout"""
+    m = np.ascontiguousarray(m, np.float32).reshape(-1, 16)
+    arr = (Material * len(m))()
+    C.memmove(arr, m.ctypes.data, m.nbytes)
+    return arr
+
+
+def bsdf_eval_batch(mats, mat, wo, wi, eta, gd, ux):
+    """Device BSDF values for (material index, wo, wi) triples in local frames: (f [n, 3], pdf [n])."""
+    M = materials_array(mats); n = len(mat)
+    a = [np.ascontiguousarray(x, t) for x, t in ((mat, np.int32), (wo, np.float32), (wi, np.float32), (eta, np.float32), (ux, np.float32))]
+    f = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32)
+    _check(lib().cwp_bsdf_eval_batch(M, len(M), a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, gd, a[4].ctypes.data,
+                                     f.ctypes.data, pdf.ctypes.data, n))
+    return f, pdf
+
+
+def bsdf_sample_batch(mats, mat, wo, eta, gd, ux, uvw):
+    """Device BSDF samples: (wi [n, 3], weight [n, 3], pdf [n], ok [n])."""
+    M = materials_array(mats); n = len(mat)
+    a = [np.ascontiguousarray(x, t) for x, t in ((mat, np.int32), (wo, np.float32), (eta, np.float32), (ux, np.float32), (uvw, np.float32))]
+    wi = np.zeros((n, 3), np.float32); w = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32); ok = np.zeros(n, np.int32)
+    _check(lib().cwp_bsdf_sample_batch(M, len(M), a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, gd, a[3].ctypes.data, a[4].ctypes.data,
+                                       wi.ctypes.data, w.ctypes.data, pdf.ctypes.data, ok.ctypes.data, n))
+    return wi, w, pdf, ok
+
+
+def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun_e=None, sky=None, sun_angle_rad=None, eps=1e-3):
+    """A serving request; lighting defaults to the benchmark's sun and sky."""
+    from . import workloads as W
+    sun_to = W.SUN_TO if sun_to is None else sun_to; sun_e = (W.SUN_E,) * 3 if sun_e is None else sun_e
+    sky = W.SKY if sky is None else sky; sun_angle_rad = W.SUN_ANGLE_RAD if sun_angle_rad is None else sun_angle_rad
+    r = Request()
+    r.scene, r.frame, r.cam, r.spp, r.max_depth, r.seed = scene, frame, cam, spp, max_depth, seed
+    s = np.array(sun_to, np.float64); s /= np.linalg.norm(s)
+    r.sun_to[:] = tuple(float(x) for x in s); r.sun_e[:] = tuple(sun_e); r.sky[:] = tuple(sky)
+    r.sun_cos = float(np.float32(math.cos(sun_angle_rad / 2.0))); r.eps = eps
+    return r
+
+
+class Server:
+    """Serving form: requests over the resident scenes of a Batch, continuous batching (max_requests > 1) or the plain
+    form (max_requests = 1)."""
+
+    def __init__(self, batch, materials, mesh_mat_base, max_paths=8 << 20, max_requests=64, gd_energy=1, hbm_reserve=1 << 30, device=0):
+        self._batch = batch
+        M = materials_array(materials); base = np.ascontiguousarray(mesh_mat_base, np.int32)
+        o = ServerOptions(max_paths, max_requests, gd_energy, hbm_reserve, device)
+        h = C.c_void_p()
+        _check(lib().cwp_server_create(batch._h, M, len(M), _iptr(base), C.byref(o), C.byref(h)))
+        self._h = h
+
+    def set_scenes(self, descs, scene_first):
+        first = np.ascontiguousarray(scene_first, np.int32)
+        _check(lib().cwp_server_set_scenes(self._h, descs, len(descs), _iptr(first), len(first) - 1))
+
+    def submit(self, req):
+        i = C.c_int64(); _check(lib().cwp_server_submit(self._h, C.byref(req), C.byref(i))); return i.value
+
+    def step(self):
+        a, p = C.c_int32(), C.c_int32()
+        _check(lib().cwp_server_step(self._h, C.byref(a), C.byref(p)))
+        return a.value, p.value
+
+    def poll(self, cap=1024):
+        ids = (C.c_int64 * cap)(); n = C.c_int32()
+        _check(lib().cwp_server_poll(self._h, ids, cap, C.byref(n)))
+        return list(ids[:n.value])
+
+    def result(self, rid, w=None, h=None):
+        """(accum [w h, 4] radiance sums or None when w is None, RequestStats); releases the request"""
+        st = RequestStats()
+        acc = np.zeros((w * h, 4), np.float32) if w else None
+        _check(lib().cwp_server_result(self._h, rid, acc.ctypes.data if acc is not None else None, C.byref(st)))
+        return acc, st
+
+    def clock_ms(self):
+        return lib().cwp_server_clock_ms(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.cwp_server_destroy(self._h); self._h = C.c_void_p()
 
 
 from . import imageio  # noqa: E402,F401

@@ -2,6 +2,7 @@
 // and one persistent two-level traversal launch over a ray queue whose rays carry their scene id. The launch shape
 // (block size, BLAS width, fetch granularity, stack placement) is a runtime tuning that cwp_batch_autotune measures.
 #include "cwp_b200.h"
+#include "batch_internal.h"
 #include "hploc.h"
 #include "runtime.h"
 #include "trav.cuh"
@@ -468,3 +469,15 @@ extern "C" int cwp_batch_download_tlas(const cwp_batch* b, float* nodes, int64_t
     if (inst && b->nInst) CWPB_CUDA(cudaMemcpy(inst, b->inst, (size_t)b->nInst * sizeof(cwp_instance), cudaMemcpyDeviceToHost));
     return CWP_OK;
 }
+
+namespace cwpb {
+int batch_trace_dev(cwp_batch* b, bool any, const float4* o, const float4* d, const int* sc, float4* hits, int* inst, int64_t n, cudaStream_t st) {
+    CWPB_CHECK(b->nScenes > 0, CWP_ERR_STATE, "no scenes");
+    if (n <= 0) return CWP_OK;
+    return launch(b, b->tuning, any, (const float*)o, (const float*)d, sc, (float*)hits, inst, n, st);
+}
+const float4* batch_tris(const cwp_batch* b) { return b->lay[lay_index(b->tuning.width)].tris; }
+const cwp_instance* batch_instances(const cwp_batch* b) { return b->inst; }
+int batch_mesh_count(const cwp_batch* b) { return b->nMesh; }
+int batch_device(const cwp_batch* b) { return b->device; }
+}  // namespace cwpb

@@ -1,0 +1,13 @@
+// batch_internal.h - what the serving loop uses of a cwp_batch: the scene-tagged trace on a caller's stream with the
+// batch's tuning, and the device arrays that shading reads (triangle records of the traced layout, instances).
+#pragma once
+#include "cwp_b200.h"
+#include <cuda_runtime.h>
+
+namespace cwpb {
+int batch_trace_dev(cwp_batch* b, bool any, const float4* o, const float4* d, const int* sc, float4* hits, int* inst, int64_t n, cudaStream_t st);
+const float4* batch_tris(const cwp_batch* b);          // triangle records (v0, id), (e1, material), (e2, 0) of the tuned width
+const cwp_instance* batch_instances(const cwp_batch* b);
+int batch_mesh_count(const cwp_batch* b);
+int batch_device(const cwp_batch* b);
+}  // namespace cwpb

@@ -1,0 +1,513 @@
+// serve.cu - the serving form: a request loop with continuous batching over the resident scenes of a cwp_batch.
+//
+// Requests wait in a FIFO queue and are admitted into one of max_requests slots when a slot is free and the device has
+// room for the request's image (cudaMemGetInfo, less hbm_reserve). Every step:
+//   1. admission, and when it admitted anything, one TLAS rebuild for all slots (slot k's scene animated to its frame);
+//   2. new camera paths for the admitted requests, up to the path capacity, shared evenly between the requests that
+//      still have samples to issue (so small requests are not stuck behind large ones);
+//   3. one scene-tagged closest-hit launch over every queued ray, whatever request it belongs to;
+//   4. shading (OpenPBR-subset BSDFs, sun next-event estimation, constant sky): continuations into the next queue,
+//      sun shadow rays into the shadow queue, per-slot counts of traced, shadow and finished paths;
+//   5. one any-hit launch over the shadow queue and the accumulation of the unoccluded contributions;
+//   6. completion: a request whose paths were all issued and have all finished is done.
+// A request's image depends only on its own inputs: every random number is keyed by (pixel, sample, depth, dimension,
+// request seed), and shading reads only its own slot's parameters. max_requests = 1 gives the plain form (one request
+// on the GPU at a time, the same kernels).
+#include "batch_internal.h"
+#include "bsdf.cuh"
+#include "cwp_b200.h"
+#include "runtime.h"
+#include "trav.cuh"
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <vector>
+
+namespace cwpb {
+
+struct SlotParams {
+    cwp_camera cam;
+    float3 sunTo, sunE, sky; float sunCos, eps;
+    unsigned seed; int maxDepth, N; float4* accum;
+};
+
+// queue entry k: o = (origin, tmin), d = (direction, tmax), scene id = slot, T = (throughput, pdf of the last BSDF
+// sample or 0), info = (slot, pixel, sample, depth)
+struct RayQueue { float4* o; float4* d; int* sc; float4* T; int4* info; };
+// shadow entry: o, d, scene id = slot, c = (contribution, pixel bits), slot
+struct ShadowQueue { float4* o; float4* d; int* sc; float4* c; };
+// per-slot counters: [0] closest rays shaded, [1] shadow rays, [2] paths finished
+static constexpr int kSlotCounters = 4;
+
+__device__ __forceinline__ unsigned lanes_lt() { unsigned m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
+__device__ __forceinline__ float rnd_s(unsigned seed, unsigned pix, unsigned smp, unsigned depth, unsigned dim) { return sample01(pix, smp, depth, dim, seed); }
+
+// paths j of a request: pixel (8 x 4 tiles when the image allows, else row-major) = j mod N, sample = j / N
+__device__ __forceinline__ int serve_pixel(int j, int w, int h) {
+    if ((w & 7) | (h & 3)) return j;
+    const int t = j >> 5, r = j & 31, tilesX = w >> 3;
+    return ((t / tilesX) * 4 + (r >> 3)) * w + (t % tilesX) * 8 + (r & 7);
+}
+
+// chunk c: slot, first path index, count, queue position of its first path (ascending)
+__global__ void k_serve_raygen(const int4* __restrict__ chunks, int nChunks, int total, const SlotParams* __restrict__ slots, RayQueue q, int base) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int lo = 0, hi = nChunks - 1;
+    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (__ldg(&chunks[mid].w) <= t) lo = mid; else hi = mid - 1; }
+    const int4 c = chunks[lo];
+    const int slot = c.x, j = c.y + (t - c.w);
+    const SlotParams& S = slots[slot];
+    const cwp_camera& C = S.cam;
+    const int pix = serve_pixel(j % S.N, C.w, C.h); const unsigned smp = (unsigned)(j / S.N);
+    const int x = pix % C.w, y = pix / C.w;
+    const float jx = rnd_s(S.seed, pix, smp, 0, 0) - 0.5f, jy = rnd_s(S.seed, pix, smp, 0, 1) - 0.5f;   // box filter
+    const float dx = (x + 0.5f + jx - C.px) / C.fx, dy = -(y + 0.5f + jy - C.py) / C.fy;
+    const float3 ax = f3(C.ax[0], C.ax[1], C.ax[2]), ay = f3(C.ay[0], C.ay[1], C.ay[2]), az = f3(C.az[0], C.az[1], C.az[2]);
+    const float3 d = normalize(ax * dx + ay * dy - az);
+    const int k = base + t;
+    q.o[k] = make_float4(C.pos[0], C.pos[1], C.pos[2], 0.f); q.d[k] = make_float4(d.x, d.y, d.z, 1e30f); q.sc[k] = slot;
+    q.T[k] = make_float4(1.f, 1.f, 1.f, 0.f); q.info[k] = make_int4(slot, pix, (int)smp, 0);
+}
+
+struct ShadeArgs {
+    int n; RayQueue in, out; ShadowQueue sq;
+    const float4* hits; const int* hinst; const cwp_instance* inst; const float4* tris;
+    const cwp_material* mats; int nMats; const int* meshMat; const SlotParams* slots; int gdEnergy;
+    int* cnt;          // [0] next queue length, [1] shadow queue length
+    int* slotCnt;      // kSlotCounters per slot
+};
+
+// per-slot counts of this warp's lanes: lanes are grouped by slot, and each group's lowest lane adds the group's counts
+__device__ __forceinline__ void slot_counts(int* slotCnt, int slot, bool valid, bool traced, bool shadow, bool ended) {
+    const unsigned peers = __match_any_sync(0xffffffffu, valid ? slot : -1);
+    const unsigned hasT = __ballot_sync(0xffffffffu, traced) & peers, hasS = __ballot_sync(0xffffffffu, shadow) & peers, hasE = __ballot_sync(0xffffffffu, ended) & peers;
+    if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+        if (hasT) atomicAdd(&slotCnt[kSlotCounters * slot + 0], __popc(hasT));
+        if (hasS) atomicAdd(&slotCnt[kSlotCounters * slot + 1], __popc(hasS));
+        if (hasE) atomicAdd(&slotCnt[kSlotCounters * slot + 2], __popc(hasE));
+    }
+}
+
+__device__ __forceinline__ int warp_slot(int* counter, bool want) {
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (!m) return -1;
+    const int leader = __ffs(m) - 1, lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return want ? base + __popc(m & lanes_lt()) : -1;
+}
+
+__device__ __forceinline__ void add_rgb(float4* accum, int pix, float3 c) { atomicAdd(accum + pix, make_float4(c.x, c.y, c.z, 0.f)); }
+
+// shading of one closest hit or miss (render/wavefront.cu:223-356 restricted to the sun and a constant sky)
+__global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < a.n; base += stride) {
+        const int k = base + (threadIdx.x & 31);
+        const bool valid = k < a.n;
+        int slot = 0, pix = 0, depth = 0; unsigned smp = 0;
+        bool ended = false, wantShadow = false, wantCont = false;
+        float3 T = f3(0.f, 0.f, 0.f), so = T, sd = T, contrib = T, co = T, cd = T; float cpdf = 0.f;
+        if (valid) {
+            const int4 info = a.in.info[k];
+            slot = info.x; pix = info.y; smp = (unsigned)info.z; depth = info.w;
+            const float4 T4 = a.in.T[k]; T = f3(T4.x, T4.y, T4.z);
+            const SlotParams& S = a.slots[slot];
+            const float4 O = a.in.o[k], D = a.in.d[k], H = a.hits[k];
+            const float3 d = f3(D.x, D.y, D.z);
+            const int tri = __float_as_int(H.w);
+            if (tri < 0) {   // miss: constant sky, BSDF-sampled only
+                add_rgb(S.accum, pix, T * S.sky);
+                ended = true;
+            } else {
+                const cwp_instance& I = a.inst[a.hinst[k]];
+                const float4 e1 = __ldg(a.tris + 3 * (size_t)tri + 1), e2 = __ldg(a.tris + 3 * (size_t)tri + 2);
+                const float3 no = cross(f3(e1.x, e1.y, e1.z), f3(e2.x, e2.y, e2.z));
+                // object -> world normal: inverse transpose, orientation by the sign of det(fwd)
+                const float3 nw = f3(I.inv[0] * no.x + I.inv[4] * no.y + I.inv[8] * no.z, I.inv[1] * no.x + I.inv[5] * no.y + I.inv[9] * no.z,
+                                     I.inv[2] * no.x + I.inv[6] * no.y + I.inv[10] * no.z);
+                const float3 ng0 = normalize(nw) * I.det_sign;
+                const int mid = min(max(__ldg(a.meshMat + I.mesh) + __float_as_int(e1.w), 0), a.nMats - 1);
+                const cwp_material M = a.mats[mid];
+                const float3 p = f3(O.x, O.y, O.z) + d * H.x;
+                const float3 em = mat_v3(M.emission);
+                if (em.x > 0.f || em.y > 0.f || em.z > 0.f) add_rgb(S.accum, pix, T * em);   // no emitters are light-sampled
+                if (depth > S.maxDepth) ended = true;
+                else {
+                    const bool front = dot(ng0, d) < 0.f;
+                    const float3 ng = front ? ng0 : -ng0;
+                    float3 ns = ng;
+                    const float3 wo = -d;
+                    if (dot(ns, wo) <= 1e-6f) ns = ng;
+                    float3 tx, ty; frame_of(ns, tx, ty);
+                    const float3 woL = f3(dot(wo, tx), dot(wo, ty), dot(wo, ns));
+                    const float eta = front ? M.ior : 1.f / M.ior;
+                    const float3 up = p + ng * S.eps, dn = p - ng * S.eps;
+                    const unsigned dr = (unsigned)depth + 1u;
+                    const float ux1 = rnd_s(S.seed, pix, smp, dr, 7), ux2 = sample01(pix, smp, dr, 7, S.seed ^ 0x68E31DA4u);
+                    if (has_non_delta(M)) {   // sun next-event estimation (the only sampled light: weight 1)
+                        const float3 l = cone_dir(S.sunTo, S.sunCos, rnd_s(S.seed, pix, smp, dr, 2), rnd_s(S.seed, pix, smp, dr, 3));
+                        const float3 lL = f3(dot(l, tx), dot(l, ty), dot(l, ns));
+                        const float gl = dot(ng, l);
+                        if (lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
+                            const BsdfValue e = bsdf_eval(M, woL, lL, eta, a.gdEnergy, ux1, ux2);
+                            contrib = T * e.f * S.sunE * fabsf(lL.z);
+                            if (contrib.x > 0.f || contrib.y > 0.f || contrib.z > 0.f) { wantShadow = true; so = gl > 0.f ? up : dn; sd = l; }
+                        }
+                    }
+                    float3 wiL, wgt; float pdf;
+                    if (bsdf_sample(M, woL, eta, a.gdEnergy, ux1, ux2, rnd_s(S.seed, pix, smp, dr, 4), rnd_s(S.seed, pix, smp, dr, 0), rnd_s(S.seed, pix, smp, dr, 1), wiL, wgt, pdf)) {
+                        const float3 wi = normalize(tx * wiL.x + ty * wiL.y + ns * wiL.z);
+                        const float gi = dot(ng, wi);
+                        if (gi != 0.f && (gi > 0.f) == (wiL.z > 0.f)) {
+                            T = T * wgt;
+                            if (maxc(T) > 0.f) { wantCont = true; co = gi > 0.f ? up : dn; cd = wi; cpdf = pdf; }
+                        }
+                    }
+                    if (!wantCont) ended = true;
+                }
+            }
+        }
+        slot_counts(a.slotCnt, slot, valid, valid, wantShadow, ended);
+        const int sp = warp_slot(a.cnt + 1, wantShadow);
+        if (sp >= 0) {
+            a.sq.o[sp] = make_float4(so.x, so.y, so.z, 0.f); a.sq.d[sp] = make_float4(sd.x, sd.y, sd.z, 1e30f); a.sq.sc[sp] = slot;
+            a.sq.c[sp] = make_float4(contrib.x, contrib.y, contrib.z, __int_as_float(pix));
+        }
+        const int cp = warp_slot(a.cnt, wantCont);
+        if (cp >= 0) {
+            a.out.o[cp] = make_float4(co.x, co.y, co.z, 0.f); a.out.d[cp] = make_float4(cd.x, cd.y, cd.z, 1e30f); a.out.sc[cp] = slot;
+            a.out.T[cp] = make_float4(T.x, T.y, T.z, cpdf); a.out.info[cp] = make_int4(slot, pix, (int)smp, depth + 1);
+        }
+    }
+}
+
+__global__ void k_serve_shadow_accum(int n, ShadowQueue sq, const int* __restrict__ occ, const SlotParams* __restrict__ slots) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n || occ[k] >= 0) return;
+    const float4 c = sq.c[k];
+    add_rgb(slots[sq.sc[k]].accum, __float_as_int(c.w), f3(c.x, c.y, c.z));
+}
+
+// ---------------- BSDF test kernels ----------------
+__global__ void k_bsdf_eval(const cwp_material* mats, const int* mat, const float3* wo, const float3* wi, const float* eta, int gd, const float2* ux,
+                            float4* f, float* pdf, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const BsdfValue e = bsdf_eval(mats[mat[i]], wo[i], wi[i], eta[i], gd, ux[i].x, ux[i].y);
+    f[i] = make_float4(e.f.x, e.f.y, e.f.z, 0.f); pdf[i] = e.pdf;
+}
+__global__ void k_bsdf_sample(const cwp_material* mats, const int* mat, const float3* wo, const float* eta, int gd, const float2* ux, const float3* uvw,
+                              float3* wi, float3* w, float* pdf, int* ok, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 a = f3(0.f, 0.f, 0.f), b = a; float p = 0.f;
+    ok[i] = bsdf_sample(mats[mat[i]], wo[i], eta[i], gd, ux[i].x, ux[i].y, uvw[i].x, uvw[i].y, uvw[i].z, a, b, p) ? 1 : 0;
+    wi[i] = a; w[i] = b; pdf[i] = p;
+}
+
+}  // namespace cwpb
+
+using namespace cwpb;
+
+struct ServeRequest {
+    cwp_request r; int64_t id; int slot = -1;
+    double submitMs = 0, admitMs = 0, doneMs = 0;
+    int64_t total = 0, issued = 0, finished = 0; double rays = 0, shadow = 0;
+    float4* accum = nullptr; bool done = false;
+};
+
+struct cwp_server {
+    cwp_batch* batch = nullptr; int device = 0;
+    cwp_server_options O{};
+    cwp_material* mats = nullptr; int nMats = 0; int* meshMat = nullptr;
+    // scenes: instance descriptors per scene (host)
+    std::vector<cwp_instance_desc> desc; std::vector<int> sceneFirst;
+    // per slot: request id or -1, its instances (host) for the TLAS rebuild
+    std::vector<int64_t> slotReq; std::vector<std::vector<cwp_instance>> slotInst;
+    SlotParams* dSlots = nullptr; int* slotCnt = nullptr; std::vector<int> hSlotCnt;
+    RayQueue q[2]{}; ShadowQueue sq{}; float4* hits = nullptr; int* hinst = nullptr; int* occ = nullptr; int* cnt = nullptr; int4* dChunks = nullptr;
+    int* hcnt = nullptr;   // pinned: [0..1] counts, then slot counters
+    int cur = 0; int64_t nCur = 0;
+    std::deque<int64_t> pending; std::map<int64_t, ServeRequest> reqs; std::vector<int64_t> completed;
+    int64_t nextId = 1;
+    cudaStream_t st = nullptr;
+    std::chrono::steady_clock::time_point t0;
+    std::vector<void*> allocs;
+};
+
+static double now_ms(const cwp_server* s) { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s->t0).count(); }
+
+extern "C" double cwp_server_clock_ms(const cwp_server* s) { return s ? now_ms(s) : 0.0; }
+
+extern "C" void cwp_server_destroy(cwp_server* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->st) cudaStreamSynchronize(s->st);
+    for (auto& kv : s->reqs) if (kv.second.accum) cudaFree(kv.second.accum);
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->hcnt) cudaFreeHost(s->hcnt);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+}
+
+static int server_create(cwp_batch* b, const cwp_material* mats, int n, const int* meshBase, const cwp_server_options* o, cwp_server* s) {
+    s->batch = b; s->device = batch_device(b);
+    s->O.max_paths = o && o->max_paths > 0 ? o->max_paths : (8ll << 20);
+    s->O.max_requests = o && o->max_requests > 0 ? o->max_requests : 64;
+    s->O.gd_energy = o ? o->gd_energy : 1;
+    s->O.hbm_reserve = o && o->hbm_reserve > 0 ? o->hbm_reserve : (1ll << 30);
+    CWPB_CHECK(s->O.max_paths < (1ll << 30), CWP_ERR_INVALID, "max_paths %lld above 2^30", (long long)s->O.max_paths);
+    CWPB_CHECK(s->O.max_requests <= 1024, CWP_ERR_INVALID, "max_requests %d above 1024", s->O.max_requests);
+    CWPB_CHECK(mats && n >= 1 && meshBase, CWP_ERR_INVALID, "no materials");
+    const int nMesh = batch_mesh_count(b);
+    for (int m = 0; m < nMesh; m++) CWPB_CHECK(meshBase[m] >= 0 && meshBase[m] < n, CWP_ERR_INVALID, "mesh %d material base %d out of range", m, meshBase[m]);
+    for (int i = 0; i < n; i++) CWPB_CHECK(mats[i].ior > 0.f && mats[i].roughness >= 0.f && mats[i].metallic >= 0.f && mats[i].metallic <= 1.f &&
+                                           mats[i].transmission >= 0.f && mats[i].transmission <= 1.f, CWP_ERR_INVALID, "material %d out of range", i);
+    CWPB_CUDA(cudaSetDevice(s->device));
+    CWPB_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+    auto alloc = [&](void** p, size_t bytes) -> int { CWPB_CUDA(cudaMalloc(p, bytes)); s->allocs.push_back(*p); return CWP_OK; };
+    const size_t P = (size_t)s->O.max_paths, R = (size_t)s->O.max_requests;
+    int rc = alloc((void**)&s->mats, (size_t)n * sizeof(cwp_material));
+    if (!rc) rc = alloc((void**)&s->meshMat, (size_t)nMesh * sizeof(int));
+    for (int k = 0; k < 2 && !rc; k++) {
+        rc = alloc((void**)&s->q[k].o, P * 16); if (!rc) rc = alloc((void**)&s->q[k].d, P * 16); if (!rc) rc = alloc((void**)&s->q[k].sc, P * 4);
+        if (!rc) rc = alloc((void**)&s->q[k].T, P * 16); if (!rc) rc = alloc((void**)&s->q[k].info, P * 16);
+    }
+    if (!rc) rc = alloc((void**)&s->sq.o, P * 16); if (!rc) rc = alloc((void**)&s->sq.d, P * 16); if (!rc) rc = alloc((void**)&s->sq.sc, P * 4);
+    if (!rc) rc = alloc((void**)&s->sq.c, P * 16);
+    if (!rc) rc = alloc((void**)&s->hits, P * 16); if (!rc) rc = alloc((void**)&s->hinst, P * 4); if (!rc) rc = alloc((void**)&s->occ, P * 4);
+    if (!rc) rc = alloc((void**)&s->cnt, 4 * sizeof(int));
+    if (!rc) rc = alloc((void**)&s->dSlots, R * sizeof(SlotParams));
+    if (!rc) rc = alloc((void**)&s->slotCnt, R * kSlotCounters * sizeof(int));
+    if (!rc) rc = alloc((void**)&s->dChunks, (R + 1) * sizeof(int4));
+    if (rc) return rc;
+    CWPB_CUDA(cudaMallocHost(&s->hcnt, (4 + R * kSlotCounters) * sizeof(int)));
+    CWPB_CUDA(cudaMemcpy(s->mats, mats, (size_t)n * sizeof(cwp_material), cudaMemcpyHostToDevice));
+    CWPB_CUDA(cudaMemcpy(s->meshMat, meshBase, (size_t)nMesh * sizeof(int), cudaMemcpyHostToDevice));
+    CWPB_CUDA(cudaMemset(s->slotCnt, 0, R * kSlotCounters * sizeof(int)));
+    s->nMats = n;
+    s->slotReq.assign(R, -1); s->slotInst.assign(R, {}); s->hSlotCnt.assign(R * kSlotCounters, 0);
+    s->t0 = std::chrono::steady_clock::now();
+    return CWP_OK;
+}
+
+extern "C" int cwp_server_create(cwp_batch* b, const cwp_material* mats, int32_t n, const int32_t* meshBase, const cwp_server_options* o, cwp_server** out) {
+    CWPB_CHECK(b && out, CWP_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    cwp_server* s = new cwp_server();
+    if (int rc = server_create(b, mats, n, meshBase, o, s)) { cwp_server_destroy(s); return rc; }
+    *out = s;
+    return CWP_OK;
+}
+
+extern "C" int cwp_server_set_scenes(cwp_server* s, const cwp_instance_desc* desc, int64_t n, const int32_t* first, int32_t nScenes) {
+    CWPB_CHECK(s && first && nScenes >= 1 && (n == 0 || desc), CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(first[0] == 0 && first[nScenes] == n, CWP_ERR_INVALID, "scene offsets do not cover the %lld descriptors", (long long)n);
+    for (int k = 0; k < nScenes; k++) CWPB_CHECK(first[k + 1] >= first[k], CWP_ERR_INVALID, "scene offsets decrease at %d", k);
+    const int nMesh = batch_mesh_count(s->batch);
+    for (int64_t i = 0; i < n; i++) CWPB_CHECK(desc[i].mesh >= 0 && desc[i].mesh < nMesh, CWP_ERR_INVALID, "descriptor %lld: mesh %d out of range", (long long)i, desc[i].mesh);
+    CWPB_CHECK(s->reqs.empty(), CWP_ERR_STATE, "scenes change only while no request is queued or running");
+    s->desc.assign(desc, desc + n); s->sceneFirst.assign(first, first + nScenes + 1);
+    return CWP_OK;
+}
+
+extern "C" int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* id) {
+    CWPB_CHECK(s && r && id, CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(!s->sceneFirst.empty(), CWP_ERR_STATE, "no scenes (cwp_server_set_scenes)");
+    CWPB_CHECK(r->scene >= 0 && r->scene + 1 < (int)s->sceneFirst.size(), CWP_ERR_INVALID, "scene %d out of range", r->scene);
+    CWPB_CHECK(r->cam.w > 0 && r->cam.h > 0 && r->spp > 0 && r->max_depth >= 0 && r->max_depth <= 64, CWP_ERR_INVALID, "bad request size");
+    const int64_t total = (int64_t)r->cam.w * r->cam.h * r->spp;
+    CWPB_CHECK(total < (1ll << 31), CWP_ERR_INVALID, "%lld paths in one request (limit 2^31)", (long long)total);
+    ServeRequest q; q.r = *r; q.id = s->nextId++; q.submitMs = now_ms(s); q.total = total;
+    s->reqs[q.id] = q; s->pending.push_back(q.id);
+    *id = q.id;
+    return CWP_OK;
+}
+
+static int rebuild_tlas(cwp_server* s) {
+    const int R = s->O.max_requests;
+    std::vector<cwp_instance> all; std::vector<int> first(R + 1, 0);
+    for (int k = 0; k < R; k++) {
+        if (s->slotReq[k] >= 0) all.insert(all.end(), s->slotInst[k].begin(), s->slotInst[k].end());
+        first[k + 1] = (int)all.size();
+    }
+    return cwp_batch_set_scenes(s->batch, all.data(), (int64_t)all.size(), first.data(), R);
+}
+
+static int admit(cwp_server* s, bool& changed) {
+    changed = false;
+    while (!s->pending.empty()) {
+        int slot = -1;
+        for (int k = 0; k < s->O.max_requests; k++) if (s->slotReq[k] < 0) { slot = k; break; }
+        if (slot < 0) break;
+        ServeRequest& q = s->reqs[s->pending.front()];
+        const size_t bytes = (size_t)q.r.cam.w * q.r.cam.h * sizeof(float4);
+        size_t freeB = 0, totalB = 0;
+        CWPB_CUDA(cudaMemGetInfo(&freeB, &totalB));
+        if (freeB < bytes + (size_t)s->O.hbm_reserve) break;   // admission by free device memory
+        CWPB_CUDA(cudaMalloc(&q.accum, bytes));
+        CWPB_CUDA(cudaMemsetAsync(q.accum, 0, bytes, s->st));
+        SlotParams P{};
+        P.cam = q.r.cam; P.sunTo = f3(q.r.sun_to[0], q.r.sun_to[1], q.r.sun_to[2]); P.sunE = f3(q.r.sun_e[0], q.r.sun_e[1], q.r.sun_e[2]);
+        P.sky = f3(q.r.sky[0], q.r.sky[1], q.r.sky[2]); P.sunCos = q.r.sun_cos; P.eps = q.r.eps; P.seed = q.r.seed; P.maxDepth = q.r.max_depth;
+        P.N = q.r.cam.w * q.r.cam.h; P.accum = q.accum;
+        CWPB_CUDA(cudaMemcpyAsync(s->dSlots + slot, &P, sizeof(P), cudaMemcpyHostToDevice, s->st));
+        CWPB_CUDA(cudaMemsetAsync(s->slotCnt + kSlotCounters * slot, 0, kSlotCounters * sizeof(int), s->st));
+        // the scene's instances at the request's frame
+        std::vector<cwp_instance>& v = s->slotInst[slot]; v.clear();
+        for (int i = s->sceneFirst[q.r.scene]; i < s->sceneFirst[q.r.scene + 1]; i++) {
+            float m[12]; cwp_instance rec;
+            if (int rc = cwp_xform_animate(&s->desc[i], q.r.frame, m)) return rc;
+            if (int rc = cwp_instance_from_xform(m, s->desc[i].mesh, &rec)) return rc;
+            v.push_back(rec);
+        }
+        q.slot = slot; q.admitMs = now_ms(s);
+        s->slotReq[slot] = q.id; s->hSlotCnt[kSlotCounters * slot + 2] = 0;
+        s->pending.pop_front();
+        changed = true;
+    }
+    return CWP_OK;
+}
+
+extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPending) {
+    CWPB_CHECK(s, CWP_ERR_INVALID, "server is NULL");
+    CWPB_CUDA(cudaSetDevice(s->device));
+    bool changed = false;
+    if (int rc = admit(s, changed)) return rc;
+    if (changed) { CWPB_CUDA(cudaStreamSynchronize(s->st)); if (int rc = rebuild_tlas(s)) return rc; }
+    // new camera paths: free capacity shared evenly by the slots with samples left to issue, oldest first
+    const int R = s->O.max_requests;
+    std::vector<int> needy;
+    for (int k = 0; k < R; k++) if (s->slotReq[k] >= 0) { const ServeRequest& q = s->reqs[s->slotReq[k]]; if (q.issued < q.total) needy.push_back(k); }
+    std::sort(needy.begin(), needy.end(), [&](int a, int b) { return s->reqs[s->slotReq[a]].admitMs < s->reqs[s->slotReq[b]].admitMs; });
+    int64_t freeCap = s->O.max_paths - s->nCur;
+    std::vector<int4> chunks; int64_t added = 0;
+    for (size_t i = 0; i < needy.size() && freeCap > 0; i++) {
+        ServeRequest& q = s->reqs[s->slotReq[needy[i]]];
+        const int64_t share = freeCap / (int64_t)(needy.size() - i);   // what is left split over the requests not yet served
+        const int64_t take = std::min(q.total - q.issued, std::max<int64_t>(share, 1));
+        if (take <= 0) continue;
+        chunks.push_back(make_int4(needy[i], (int)q.issued, (int)take, (int)added));
+        q.issued += take; added += take; freeCap -= take;
+    }
+    RayQueue& in = s->q[s->cur]; RayQueue& out = s->q[s->cur ^ 1];
+    if (added > 0) {
+        CWPB_CUDA(cudaMemcpyAsync(s->dChunks, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice, s->st));
+        k_serve_raygen<<<(unsigned)((added + 255) / 256), 256, 0, s->st>>>(s->dChunks, (int)chunks.size(), (int)added, s->dSlots, in, (int)s->nCur);
+        CWPB_CUDA(cudaGetLastError());
+    }
+    const int64_t n = s->nCur + added;
+    int64_t nNext = 0, nShadow = 0;
+    if (n > 0) {
+        if (int rc = batch_trace_dev(s->batch, false, in.o, in.d, in.sc, s->hits, s->hinst, n, s->st)) return rc;
+        CWPB_CUDA(cudaMemsetAsync(s->cnt, 0, 4 * sizeof(int), s->st));
+        ShadeArgs a{};
+        a.n = (int)n; a.in = in; a.out = out; a.sq = s->sq; a.hits = s->hits; a.hinst = s->hinst; a.inst = batch_instances(s->batch); a.tris = batch_tris(s->batch);
+        a.mats = s->mats; a.nMats = s->nMats; a.meshMat = s->meshMat; a.slots = s->dSlots; a.gdEnergy = s->O.gd_energy; a.cnt = s->cnt; a.slotCnt = s->slotCnt;
+        const unsigned g = (unsigned)std::min<int64_t>((n + 127) / 128, 148 * 16);
+        k_serve_shade<<<g, 128, 0, s->st>>>(a);
+        CWPB_CUDA(cudaGetLastError());
+        CWPB_CUDA(cudaMemcpyAsync(s->hcnt, s->cnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+        CWPB_CUDA(cudaStreamSynchronize(s->st));
+        nNext = s->hcnt[0]; nShadow = s->hcnt[1];
+        if (nShadow > 0) {
+            if (int rc = batch_trace_dev(s->batch, true, s->sq.o, s->sq.d, s->sq.sc, nullptr, s->occ, nShadow, s->st)) return rc;
+            k_serve_shadow_accum<<<(unsigned)((nShadow + 255) / 256), 256, 0, s->st>>>((int)nShadow, s->sq, s->occ, s->dSlots);
+            CWPB_CUDA(cudaGetLastError());
+        }
+    }
+    CWPB_CUDA(cudaMemcpyAsync(s->hcnt + 4, s->slotCnt, (size_t)R * kSlotCounters * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CWPB_CUDA(cudaStreamSynchronize(s->st));
+    if (int rc = cwp_batch_status(s->batch)) return rc;
+    s->cur ^= 1; s->nCur = nNext;
+    // completion
+    const double t = now_ms(s);
+    for (int k = 0; k < R; k++) {
+        if (s->slotReq[k] < 0) continue;
+        ServeRequest& q = s->reqs[s->slotReq[k]];
+        const int* c = s->hcnt + 4 + kSlotCounters * k;
+        q.rays = c[0]; q.shadow = c[1]; q.finished = c[2];
+        if (q.issued == q.total && q.finished == q.total) {
+            q.done = true; q.doneMs = t; s->completed.push_back(q.id); s->slotReq[k] = -1; q.slot = -1;
+        }
+    }
+    if (nActive) { int a = 0; for (int k = 0; k < R; k++) a += s->slotReq[k] >= 0; *nActive = a; }
+    if (nPending) *nPending = (int)s->pending.size();
+    return CWP_OK;
+}
+
+extern "C" int cwp_server_poll(cwp_server* s, int64_t* ids, int32_t cap, int32_t* n) {
+    CWPB_CHECK(s && n && (cap == 0 || ids), CWP_ERR_INVALID, "NULL argument");
+    const int k = (int)std::min<size_t>(s->completed.size(), (size_t)std::max(cap, 0));
+    for (int i = 0; i < k; i++) ids[i] = s->completed[i];
+    s->completed.erase(s->completed.begin(), s->completed.begin() + k);
+    *n = k;
+    return CWP_OK;
+}
+
+extern "C" int cwp_server_result(cwp_server* s, int64_t id, float* accum, cwp_request_stats* st) {
+    CWPB_CHECK(s, CWP_ERR_INVALID, "server is NULL");
+    auto it = s->reqs.find(id);
+    CWPB_CHECK(it != s->reqs.end(), CWP_ERR_INVALID, "unknown request %lld", (long long)id);
+    ServeRequest& q = it->second;
+    CWPB_CHECK(q.done, CWP_ERR_STATE, "request %lld is not complete", (long long)id);
+    CWPB_CUDA(cudaSetDevice(s->device));
+    if (accum) CWPB_CUDA(cudaMemcpy(accum, q.accum, (size_t)q.r.cam.w * q.r.cam.h * sizeof(float4), cudaMemcpyDeviceToHost));
+    if (st) {
+        st->submit_ms = q.submitMs; st->admit_ms = q.admitMs; st->done_ms = q.doneMs; st->rays = q.rays; st->shadow_rays = q.shadow;
+        st->w = q.r.cam.w; st->h = q.r.cam.h; st->spp = q.r.spp; st->pad = 0;
+    }
+    CWPB_CUDA(cudaFree(q.accum));
+    s->reqs.erase(it);
+    return CWP_OK;
+}
+
+extern "C" int cwp_bsdf_eval_batch(const cwp_material* mats, int32_t nm, const int32_t* mat, const float* wo, const float* wi, const float* eta, int32_t gd,
+                                   const float* ux, float* f, float* pdf, int64_t n) {
+    CWPB_CHECK(mats && nm > 0 && mat && wo && wi && eta && ux && f && pdf && n >= 0, CWP_ERR_INVALID, "NULL argument");
+    for (int64_t i = 0; i < n; i++) CWPB_CHECK(mat[i] >= 0 && mat[i] < nm, CWP_ERR_INVALID, "material index %d out of range", mat[i]);
+    if (n == 0) return CWP_OK;
+    cwp_material* dm; int* dmat; float3 *dwo, *dwi; float* deta; float2* dux; float4* df; float* dpdf;
+    CWPB_CUDA(cudaMalloc(&dm, nm * sizeof(cwp_material))); CWPB_CUDA(cudaMalloc(&dmat, n * 4)); CWPB_CUDA(cudaMalloc(&dwo, n * 12)); CWPB_CUDA(cudaMalloc(&dwi, n * 12));
+    CWPB_CUDA(cudaMalloc(&deta, n * 4)); CWPB_CUDA(cudaMalloc(&dux, n * 8)); CWPB_CUDA(cudaMalloc(&df, n * 16)); CWPB_CUDA(cudaMalloc(&dpdf, n * 4));
+    cudaMemcpy(dm, mats, nm * sizeof(cwp_material), cudaMemcpyHostToDevice); cudaMemcpy(dmat, mat, n * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dwo, wo, n * 12, cudaMemcpyHostToDevice); cudaMemcpy(dwi, wi, n * 12, cudaMemcpyHostToDevice); cudaMemcpy(deta, eta, n * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dux, ux, n * 8, cudaMemcpyHostToDevice);
+    k_bsdf_eval<<<(unsigned)((n + 127) / 128), 128>>>(dm, dmat, dwo, dwi, deta, gd, dux, df, dpdf, n);
+    cudaError_t e = cudaGetLastError();
+    std::vector<float4> hf(n);
+    if (e == cudaSuccess) e = cudaMemcpy(hf.data(), df, n * 16, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(pdf, dpdf, n * 4, cudaMemcpyDeviceToHost);
+    for (int64_t i = 0; i < n && e == cudaSuccess; i++) { f[3 * i] = hf[i].x; f[3 * i + 1] = hf[i].y; f[3 * i + 2] = hf[i].z; }
+    cudaFree(dm); cudaFree(dmat); cudaFree(dwo); cudaFree(dwi); cudaFree(deta); cudaFree(dux); cudaFree(df); cudaFree(dpdf);
+    CWPB_CUDA(e);
+    return CWP_OK;
+}
+
+extern "C" int cwp_bsdf_sample_batch(const cwp_material* mats, int32_t nm, const int32_t* mat, const float* wo, const float* eta, int32_t gd, const float* ux,
+                                     const float* uvw, float* wi, float* weight, float* pdf, int32_t* ok, int64_t n) {
+    CWPB_CHECK(mats && nm > 0 && mat && wo && eta && ux && uvw && wi && weight && pdf && ok && n >= 0, CWP_ERR_INVALID, "NULL argument");
+    for (int64_t i = 0; i < n; i++) CWPB_CHECK(mat[i] >= 0 && mat[i] < nm, CWP_ERR_INVALID, "material index %d out of range", mat[i]);
+    if (n == 0) return CWP_OK;
+    cwp_material* dm; int *dmat, *dok; float3 *dwo, *duvw, *dwi, *dw; float *deta, *dpdf; float2* dux;
+    CWPB_CUDA(cudaMalloc(&dm, nm * sizeof(cwp_material))); CWPB_CUDA(cudaMalloc(&dmat, n * 4)); CWPB_CUDA(cudaMalloc(&dwo, n * 12)); CWPB_CUDA(cudaMalloc(&deta, n * 4));
+    CWPB_CUDA(cudaMalloc(&dux, n * 8)); CWPB_CUDA(cudaMalloc(&duvw, n * 12)); CWPB_CUDA(cudaMalloc(&dwi, n * 12)); CWPB_CUDA(cudaMalloc(&dw, n * 12));
+    CWPB_CUDA(cudaMalloc(&dpdf, n * 4)); CWPB_CUDA(cudaMalloc(&dok, n * 4));
+    cudaMemcpy(dm, mats, nm * sizeof(cwp_material), cudaMemcpyHostToDevice); cudaMemcpy(dmat, mat, n * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dwo, wo, n * 12, cudaMemcpyHostToDevice); cudaMemcpy(deta, eta, n * 4, cudaMemcpyHostToDevice); cudaMemcpy(dux, ux, n * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(duvw, uvw, n * 12, cudaMemcpyHostToDevice);
+    k_bsdf_sample<<<(unsigned)((n + 127) / 128), 128>>>(dm, dmat, dwo, deta, gd, dux, duvw, dwi, dw, dpdf, dok, n);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(wi, dwi, n * 12, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(weight, dw, n * 12, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(pdf, dpdf, n * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(ok, dok, n * 4, cudaMemcpyDeviceToHost);
+    cudaFree(dm); cudaFree(dmat); cudaFree(dwo); cudaFree(deta); cudaFree(dux); cudaFree(duvw); cudaFree(dwi); cudaFree(dw); cudaFree(dpdf); cudaFree(dok);
+    CWPB_CUDA(e);
+    return CWP_OK;
+}

@@ -28,7 +28,7 @@ SEED = 1000
 EPS_SCALE = 1e-4
 
 __all__ = ["SCENES", "scene", "frame_params", "scene_extent", "camera_rays", "incoherent_rays", "reference_inputs",
-           "batch_scenes", "batch_rays", "HFOV", "SEED", "SUN_TO", "SUN_E", "SUN_ANGLE_RAD", "SKY", "ALBEDO"]
+           "batch_scenes", "batch_rays", "serving_scenes", "serving_requests", "RESOLUTIONS", "SPPS", "HFOV", "SEED", "SUN_TO", "SUN_E", "SUN_ANGLE_RAD", "SKY", "ALBEDO"]
 
 
 def scene(name_or_boxes, variant=8, bins=32, leaf=4, collapse=0, threads=0):
@@ -182,3 +182,68 @@ def batch_rays(xforms, scene_first, rays_per_scene, seed=9, extent=40.0):
         v = rng.normal(size=(rays_per_scene, 3)); v /= np.linalg.norm(v, axis=1, keepdims=True)
         d[sl, :3] = v; d[sl, 3] = 1e30
     return o, d, sc
+
+
+RESOLUTIONS = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
+SPPS = [1, 4, 16, 64, 256]
+
+
+def serving_scenes(n_scenes=32, seed=7, tris=(1000, 500000), instances=(1, 4096), blas_per_scene=(1, 8), mats_per_mesh=8):
+    """Resident scenes of the serving form: the batched form's generator (box-field BLAS of log-uniform size, a
+    log-uniform number of instances per scene) with animated instances (per-frame translation and rotation) and
+    OpenPBR materials per mesh: roughness uniform in [0.05, 1], metallic ~ Bernoulli(0.3), 10% glass at IOR 1.5.
+    Returns (mesh arrays [(verts, faces, face_mat, None)], descs (InstanceDesc array), scene_first, materials [n, 16],
+    mesh_mat_base, scene_boxes [n_scenes, 2, 3])."""
+    from . import InstanceDesc, Mesh
+    rng = np.random.default_rng(seed)
+    meshes, descs, first, mats, base, boxes = [], [], [0], [], [], []
+    for s in range(n_scenes):
+        nb = int(rng.integers(blas_per_scene[0], blas_per_scene[1] + 1))
+        ids = []
+        for _ in range(nb):
+            nt = _log_uniform_int(rng, *tris)
+            m = Mesh.box_field(max(1, (nt - 2) // 12), int(rng.integers(1 << 30)))
+            v, f, fm, _ = m.arrays()
+            fm = np.zeros(len(f), np.int32); fm[2:] = (np.arange(len(f) - 2) // 12) % (mats_per_mesh - 1) + 1   # ground 0, boxes 1..
+            ids.append(len(meshes)); meshes.append((v, f, fm, None)); base.append(len(mats))
+            for k in range(mats_per_mesh):
+                mt = np.zeros(16, np.float32)
+                mt[0:3] = rng.uniform(0.2, 0.9, 3); mt[4:7] = 1.0; mt[7] = rng.uniform(0.05, 1.0); mt[11] = 1.5; mt[12] = 1.0
+                if rng.random() < 0.1: mt[13] = 1.0                # glass
+                elif rng.random() < 0.3: mt[3] = 1.0               # metal
+                mats.append(mt)
+        ni = _log_uniform_int(rng, *instances)
+        half = 20.0 * max(1.0, ni ** (1.0 / 3.0))
+        for _ in range(ni):
+            d = InstanceDesc()
+            d.mesh = ids[int(rng.integers(len(ids)))]
+            d.translate[:] = tuple(rng.uniform(-half, half, 3)); d.translate_per_frame[:] = tuple(rng.normal(0, 0.2, 3))
+            ax = rng.normal(size=3); ax /= np.linalg.norm(ax); d.axis[:] = tuple(ax)
+            d.angle_deg = float(rng.uniform(0, 360)); d.angle_deg_per_frame = float(rng.uniform(-2, 2))
+            d.scale[:] = (1.0, 1.0, 1.0); d.scale_per_frame[:] = (0.0, 0.0, 0.0)
+            descs.append(d)
+        first.append(len(descs))
+        boxes.append([[-half - 30] * 3, [half + 30] * 3])
+    arr = (InstanceDesc * len(descs))(*descs)
+    return meshes, arr, np.array(first, np.int32), np.array(mats, np.float32), np.array(base, np.int32), np.array(boxes, np.float32)
+
+
+def serving_requests(n, rate, scene_boxes, seed=11, resolutions=None, spps=None, max_depth=8, frames=30):
+    """n requests of a Poisson stream at `rate` per second: arrival time, scene (uniform), animation frame (uniform in
+    [0, frames)), resolution and spp uniform over the given sets, camera looking at the scene centre from a random
+    direction above the horizon at the scene's extent. Returns a list of (arrival_s, Request)."""
+    from . import camera_look_at, make_request
+    rng = np.random.default_rng(seed)
+    resolutions = resolutions or RESOLUTIONS; spps = spps or SPPS
+    t, out = 0.0, []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        sc = int(rng.integers(len(scene_boxes))); lo, hi = scene_boxes[sc]
+        c = (lo + hi) * 0.5; ext = float(np.max(hi - lo))
+        th = rng.uniform(0, 2 * math.pi); el = rng.uniform(0.3, 1.2)
+        pos = c + 0.7 * ext * np.array([math.cos(th) * math.cos(el), math.sin(th) * math.cos(el), math.sin(el)])
+        w, h = resolutions[int(rng.integers(len(resolutions)))]
+        cam = camera_look_at(tuple(pos), tuple(c), (0, 0, 1), HFOV, w, h)
+        out.append((t, make_request(sc, cam, int(spps[int(rng.integers(len(spps)))]), frame=int(rng.integers(frames)), max_depth=max_depth,
+                                    seed=int(rng.integers(1 << 30)), eps=1e-4 * ext)))
+    return out

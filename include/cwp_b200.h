@@ -292,6 +292,71 @@ int cwp_batch_download_tlas(const cwp_batch* b, float* nodes, int64_t* n_node_fl
 int cwp_batch_status(cwp_batch* b);   /* synchronises; CWP_ERR_TRAVERSAL if a ray hit a stack bound or the visit budget */
 
 /* ------------------------------------------------------------------------------------------------------------------
+ * Serving form: a request loop over the resident scenes of a cwp_batch with continuous batching. Requests (scene,
+ * animation frame, camera / resolution, spp, depth, lighting, seed) are admitted while request slots and free device
+ * memory allow; every step advances all admitted requests' paths by one bounce in the same launches (new camera
+ * paths join at every step), so requests that arrive while others run share the GPU. Each request's image depends only
+ * on its own inputs: the sample streams are keyed by (pixel, sample, depth, dimension, seed).
+ * Replaces the full integrator for OpenPBR-subset materials with sun next-event estimation and a constant sky
+ * (render/wavefront.cu:223-356 shadeFull, render/bsdf.h, scene/material.h); the request loop itself is new.
+ * ------------------------------------------------------------------------------------------------------------------ */
+typedef struct cwp_material {        /* Material (scene/material.h:12-17), 64 B */
+    float base_color[3]; float metallic;
+    float specular_color[3]; float roughness;
+    float emission[3]; float ior;    /* emission radiance (colour x strength) */
+    float specular_weight; float transmission; float pad0, pad1;
+} cwp_material;
+
+typedef struct cwp_server cwp_server;
+typedef struct cwp_server_options {
+    int64_t max_paths;     /* paths in flight over all requests (default 8 Mi) */
+    int32_t max_requests;  /* requests admitted at once (default 64; 1 for the plain form) */
+    int32_t gd_energy;     /* glossy-diffuse energy compensation (default 1, as the reference's --gd_energy) */
+    int64_t hbm_reserve;   /* device bytes that admission leaves free (default 1 GiB) */
+    int32_t device;
+    int32_t reserved[5];
+} cwp_server_options;
+
+typedef struct cwp_request {
+    int32_t scene;         /* scene of the batch: its instances are animated to `frame` (cwp_server_set_scenes) */
+    int32_t frame;
+    cwp_camera cam;        /* pinhole; resolution cam.w x cam.h */
+    int32_t spp, max_depth;
+    uint32_t seed;
+    float sun_to[3], sun_e[3], sky[3];
+    float sun_cos, eps;    /* cos of the sun's half angle; ray offset */
+} cwp_request;
+
+typedef struct cwp_request_stats {
+    double submit_ms, admit_ms, done_ms;    /* on the server's clock (ms since creation) */
+    double rays, shadow_rays;
+    int32_t w, h, spp, pad;
+} cwp_request_stats;
+
+/* Materials: table of n_mats; mesh m's triangles use materials mesh_mat_base[m] + (triangle material id). */
+int cwp_server_create(cwp_batch* b, const cwp_material* mats, int32_t n_mats, const int32_t* mesh_mat_base, const cwp_server_options* o, cwp_server** out);
+void cwp_server_destroy(cwp_server* s);
+/* Scenes: scene k owns instance descriptors [scene_first[k], scene_first[k + 1]) (cwp_xform_animate at the request's
+ * frame gives their transforms); replaces the batch's scenes while the server lives. */
+int cwp_server_set_scenes(cwp_server* s, const cwp_instance_desc* desc, int64_t n, const int32_t* scene_first, int32_t n_scenes);
+int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* id);
+/* One step: admission, new camera paths, one bounce of every admitted request (closest hit + shading, sun shadow rays),
+ * completion. *n_active / *n_pending: admitted / waiting requests after the step. Synchronous. */
+int cwp_server_step(cwp_server* s, int32_t* n_active, int32_t* n_pending);
+/* Completed request ids since the last call (up to cap). */
+int cwp_server_poll(cwp_server* s, int64_t* ids, int32_t cap, int32_t* n);
+/* The image of a completed request (w * h float4 radiance sums over its spp, may be NULL) and its statistics; the
+ * request's device memory is released. */
+int cwp_server_result(cwp_server* s, int64_t id, float* accum, cwp_request_stats* st);
+double cwp_server_clock_ms(const cwp_server* s);
+/* Device-side BSDF of a material table for n (material, wo, wi) triples in local frames (wo.z > 0): f (float4) and
+ * pdf; and n samples (u, u1, u2 in uvw) -> wi, weight, pdf. For tests of the device arithmetic. */
+int cwp_bsdf_eval_batch(const cwp_material* mats, int32_t n_mats, const int32_t* mat, const float* wo, const float* wi, const float* eta,
+                        int32_t gd_energy, const float* ux, float* f, float* pdf, int64_t n);
+int cwp_bsdf_sample_batch(const cwp_material* mats, int32_t n_mats, const int32_t* mat, const float* wo, const float* eta, int32_t gd_energy,
+                          const float* ux, const float* uvw, float* wi, float* weight, float* pdf, int32_t* ok, int64_t n);
+
+/* ------------------------------------------------------------------------------------------------------------------
  * Camera and parameter helpers. Replace lookAtC2W / focalFromHfov / makeCamera (scene/camera.cpp:7-23) and the
  * Params filling of setupScene (app/scene_setup.cpp:175-185, Lighting defaults scene/lighting.h:7-13).
  * ------------------------------------------------------------------------------------------------------------------ */

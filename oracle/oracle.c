@@ -813,49 +813,301 @@ static int trav_blas(int width, const V4* nodes, const V4* tv, V3 o, V3 d, float
     if (width == 4) return trav4r(nodes, tv, o, d, tmin, any, 0, t, h, u, v, NULL, root);
     return trav8r(nodes, tv, o, d, tmin, any, 0, t, h, u, v, NULL, root);
 }
+/* one ray through one two-level scene (root = its TLAS root, < 0 for an empty scene); returns -1 on a stack bound */
+static int o_inst1(int width, int any, const float* blas, const float* tris, const V4* T, int root, const float* inst, V3 o, V3 d, float tmin,
+                   float* pt, int* ph, float* pu, float* pv, int* phi) {
+    float t = *pt, u = 0.f, v = 0.f; int h = -1, hi = -1, done = 0, bad = 0;
+    if (root >= 0) {
+        const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z), ox = -o.x * idx, oy = -o.y * idy, oz = -o.z * idz;
+        int stack[64], sp = 0, next = root;
+        while (!done) {
+            const V4 n0 = T[4 * next], n1 = T[4 * next + 1], nz = T[4 * next + 2], mt = T[4 * next + 3];
+            const int c0 = fi(mt.x), c1 = fi(mt.y), k0 = fi(mt.z), k1 = fi(mt.w);
+            const float a0 = fmaf(n0.x, idx, ox), a1 = fmaf(n0.y, idx, ox), a2 = fmaf(n0.z, idy, oy), a3 = fmaf(n0.w, idy, oy), a4 = fmaf(nz.x, idz, oz), a5 = fmaf(nz.y, idz, oz);
+            const float b0 = fmaf(n1.x, idx, ox), b1 = fmaf(n1.y, idx, ox), b2 = fmaf(n1.z, idy, oy), b3 = fmaf(n1.w, idy, oy), b4 = fmaf(nz.z, idz, oz), b5 = fmaf(nz.w, idz, oz);
+            const float t0n = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
+            const float t0f = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), t));
+            const float t1n = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
+            const float t1f = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), t));
+            const int h0 = c0 >= 0 && t0n <= t0f, h1 = c1 >= 0 && t1n <= t1f;
+            int e0 = k0 > 0 ? ~c0 : c0, e1 = k1 > 0 ? ~c1 : c1, go;
+            if (h0 && h1) { if (t1n < t0n) { int q = e0; e0 = e1; e1 = q; } if (sp == 64) { bad = 1; break; } stack[sp++] = e1; go = e0; }
+            else if (h0 || h1) go = h0 ? e0 : e1;
+            else { if (sp == 0) break; go = stack[--sp]; }
+            while (go < 0) {   /* an instance: its BLAS in object space, then the next TLAS entry */
+                const float* I = inst + 28 * (size_t)(~go);
+                const V3 lo = v3(I[0] * o.x + I[1] * o.y + I[2] * o.z + I[3], I[4] * o.x + I[5] * o.y + I[6] * o.z + I[7], I[8] * o.x + I[9] * o.y + I[10] * o.z + I[11]);
+                const V3 ld = v3(I[0] * d.x + I[1] * d.y + I[2] * d.z, I[4] * d.x + I[5] * d.y + I[6] * d.z, I[8] * d.x + I[9] * d.y + I[10] * d.z);
+                int iroot; memcpy(&iroot, &I[24], 4);
+                float bt = t, bu = 0.f, bv = 0.f; int bh = -1;
+                if (trav_blas(width, (const V4*)blas, (const V4*)tris, lo, ld, tmin, any, &bt, &bh, &bu, &bv, iroot) < 0) { bad = 1; done = 1; break; }
+                if (bh >= 0 && bt < t) { t = bt; h = bh; u = bu; v = bv; hi = ~go; }
+                if (any && h >= 0) { done = 1; break; }
+                if (sp == 0) { done = 1; break; }
+                go = stack[--sp];
+            }
+            if (!done) next = go;
+        }
+    }
+    *pt = t; *ph = h; *pu = u; *pv = v; *phi = hi;
+    return bad ? -1 : 0;
+}
 long orc_trace_inst(int width, int any, const float* blas, const float* tris, const float* tlas, const int* scene_root, int n_scenes, const float* inst,
                     const float* ro, const float* rd, const int* scene_of, long n, float* hits, int* hit_inst) {
     long bad = 0;
-    const V4* T = (const V4*)tlas;
     for (long i = 0; i < n; i++) {
         const V3 o = v3(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]), d = v3(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]);
-        const float tmin = ro[4 * i + 3];
-        float t = rd[4 * i + 3], u = 0.f, v = 0.f; int h = -1, hi = -1, done = 0;
+        float t = rd[4 * i + 3], u, v; int h, hi;
         const int sc = scene_of[i], root = sc >= 0 && sc < n_scenes ? scene_root[sc] : -1;
-        if (root >= 0) {
-            const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z), ox = -o.x * idx, oy = -o.y * idy, oz = -o.z * idz;
-            int stack[64], sp = 0, next = root;
-            while (!done) {
-                const V4 n0 = T[4 * next], n1 = T[4 * next + 1], nz = T[4 * next + 2], mt = T[4 * next + 3];
-                const int c0 = fi(mt.x), c1 = fi(mt.y), k0 = fi(mt.z), k1 = fi(mt.w);
-                const float a0 = fmaf(n0.x, idx, ox), a1 = fmaf(n0.y, idx, ox), a2 = fmaf(n0.z, idy, oy), a3 = fmaf(n0.w, idy, oy), a4 = fmaf(nz.x, idz, oz), a5 = fmaf(nz.y, idz, oz);
-                const float b0 = fmaf(n1.x, idx, ox), b1 = fmaf(n1.y, idx, ox), b2 = fmaf(n1.z, idy, oy), b3 = fmaf(n1.w, idy, oy), b4 = fmaf(nz.z, idz, oz), b5 = fmaf(nz.w, idz, oz);
-                const float t0n = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
-                const float t0f = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), t));
-                const float t1n = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
-                const float t1f = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), t));
-                const int h0 = c0 >= 0 && t0n <= t0f, h1 = c1 >= 0 && t1n <= t1f;
-                int e0 = k0 > 0 ? ~c0 : c0, e1 = k1 > 0 ? ~c1 : c1, go;
-                if (h0 && h1) { if (t1n < t0n) { int q = e0; e0 = e1; e1 = q; } if (sp == 64) { bad++; break; } stack[sp++] = e1; go = e0; }
-                else if (h0 || h1) go = h0 ? e0 : e1;
-                else { if (sp == 0) break; go = stack[--sp]; }
-                while (go < 0) {   /* an instance: its BLAS in object space, then the next TLAS entry */
-                    const float* I = inst + 28 * (size_t)(~go);
-                    const V3 lo = v3(I[0] * o.x + I[1] * o.y + I[2] * o.z + I[3], I[4] * o.x + I[5] * o.y + I[6] * o.z + I[7], I[8] * o.x + I[9] * o.y + I[10] * o.z + I[11]);
-                    const V3 ld = v3(I[0] * d.x + I[1] * d.y + I[2] * d.z, I[4] * d.x + I[5] * d.y + I[6] * d.z, I[8] * d.x + I[9] * d.y + I[10] * d.z);
-                    int iroot; memcpy(&iroot, &I[24], 4);
-                    float bt = t, bu = 0.f, bv = 0.f; int bh = -1;
-                    if (trav_blas(width, (const V4*)blas, (const V4*)tris, lo, ld, tmin, any, &bt, &bh, &bu, &bv, iroot) < 0) { bad++; done = 1; break; }
-                    if (bh >= 0 && bt < t) { t = bt; h = bh; u = bu; v = bv; hi = ~go; }
-                    if (any && h >= 0) { done = 1; break; }
-                    if (sp == 0) { done = 1; break; }
-                    go = stack[--sp];
-                }
-                if (!done) next = go;
-            }
-        }
+        if (o_inst1(width, any, blas, tris, (const V4*)tlas, root, inst, o, d, ro[4 * i + 3], &t, &h, &u, &v, &hi) < 0) bad++;
         if (hits) { hits[4 * i] = t; hits[4 * i + 1] = u; hits[4 * i + 2] = v; hits[4 * i + 3] = iff(h); }
         hit_inst[i] = hi;
+    }
+    return bad;
+}
+
+/* ------------------------------------------------------------------ OpenPBR-subset BSDF (render/bsdf.h:17-220)
+ * Local frame: z = shading normal, wo.z > 0. Material = 16 floats in the cwp_material / Material layout
+ * (scene/material.h:12-17): base[3], metallic, spec[3], roughness, emission[3], ior, spec_weight, transmission, pad[2].
+ * Written from the same papers as render/bsdf.h (GGX / height-correlated Smith, Dupuy-Benyoub visible normals,
+ * exact dielectric Fresnel, F82-tinted Schlick). */
+typedef struct { float base[3], metallic, spec[3], roughness, emission[3], ior, ws, transmission, pad0, pad1; } OMat;
+#define O_PI 3.14159265f
+#define O_DELTA 1e-3f
+static float o_lum(V3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+static float o_d(float cm, float a2) { if (cm <= 0.f) return 0.f; float c2 = cm * cm, k = c2 * (a2 - 1.f) + 1.f; return a2 / (O_PI * k * k); }
+static float o_lambda(float cw, float a2) { float c2 = cw * cw; if (c2 < 1e-12f) return 1e12f; return 0.5f * (sqrtf(1.f + a2 * (1.f - c2) / c2) - 1.f); }
+static float o_g1(float c, float a2) { return 1.f / (1.f + o_lambda(c, a2)); }
+static float o_g2(float co, float ci, float a2) { return 1.f / (1.f + o_lambda(co, a2) + o_lambda(ci, a2)); }
+static float o_vpdf(V3 wo, V3 m, float a2) { float om = dot3(wo, m); if (om <= 0.f || m.z <= 0.f) return 0.f; return o_g1(wo.z, a2) * om * o_d(m.z, a2) / wo.z; }
+static V3 o_vsample(V3 wo, float a, float u1, float u2) {
+    V3 v = normz(v3(a * wo.x, a * wo.y, wo.z)); float ph = 6.2831853f * u1, z = (1.f - u2) * (1.f + v.z) - v.z;
+    float s = sqrtf(fminf(fmaxf(1.f - z * z, 0.f), 1.f));
+    V3 h = v3(s * cosf(ph) + v.x, s * sinf(ph) + v.y, z + v.z);
+    return normz(v3(a * h.x, a * h.y, fmaxf(h.z, 0.f)));
+}
+static float o_fd(float ci, float eta) {
+    float s2 = (1.f - ci * ci) / (eta * eta); if (s2 >= 1.f) return 1.f;
+    float ct = sqrtf(1.f - s2), rs = (ci - eta * ct) / (ci + eta * ct), rp = (eta * ci - ct) / (eta * ci + ct);
+    return 0.5f * (rs * rs + rp * rp);
+}
+static V3 o_f82(V3 F0, V3 tint, float mu) {
+    mu = fminf(fmaxf(mu, 0.f), 1.f);
+    float q = 1.f - mu, q2 = q * q, q5 = q2 * q2 * q, q6 = q5 * q, mb = 1.f / 7.f, qb = 6.f / 7.f, qb2 = qb * qb, qb5 = qb2 * qb2 * qb, qb6 = qb5 * qb;
+    float c[3] = { F0.x, F0.y, F0.z }, t[3] = { tint.x, tint.y, tint.z }, o[3];
+    for (int i = 0; i < 3; i++) {
+        float s = c[i] + (1.f - c[i]) * q5, sb = c[i] + (1.f - c[i]) * qb5, b = sb * (1.f - t[i]) * (1.f / (mb * qb6));
+        float F = s - b * (mu * q6); o[i] = fminf(fmaxf(F, 0.f), 1.f);
+    }
+    return v3(o[0], o[1], o[2]);
+}
+static V3 o_cos_dir(float u0, float u1) {   /* cosine hemisphere about +z (core/sampling.h:19-22) */
+    V3 n = v3(0.f, 0.f, 1.f), t, b; onb(n, &t, &b);
+    float r = sqrtf(u0), ph = 6.2831853f * u1;
+    return normz(add(add(muls(t, r * cosf(ph)), muls(b, r * sinf(ph))), muls(n, sqrtf(fmaxf(0.f, 1.f - u0)))));
+}
+typedef struct { V3 f; float pdf; } OEval;
+/* glossy-diffuse (bsdf.h:84-124) */
+typedef struct { V3 base; float ws, eta, a, a2, Fo, pSpec, kd; int delta; } OGd;
+static OGd o_gd(const OMat* m, V3 wo, int energy, float ux1, float ux2) {
+    OGd g; g.base = v3(m->base[0], m->base[1], m->base[2]); g.ws = m->ws; g.eta = m->ior; g.a = m->roughness * m->roughness; g.a2 = g.a * g.a; g.delta = g.a < O_DELTA;
+    g.Fo = g.ws > 0.f ? g.ws * o_fd(wo.z, g.eta) : 0.f;
+    float pd = (1.f - g.Fo) * o_lum(g.base); g.pSpec = g.Fo + pd > 0.f ? g.Fo / (g.Fo + pd) : 0.f;
+    g.kd = 1.f - g.Fo;
+    if (energy && g.ws > 0.f && !g.delta) {
+        V3 mm = o_vsample(wo, g.a, ux1, ux2); float om = dot3(wo, mm); V3 wr = sub(muls(mm, 2.f * om), wo);
+        float X = (om > 0.f && wr.z > 0.f) ? g.ws * o_fd(om, g.eta) * o_g2(wo.z, wr.z, g.a2) / o_g1(wo.z, g.a2) : 0.f;
+        g.kd = 1.f - X;
+    }
+    g.kd = fmaxf(g.kd, 0.f);
+    return g;
+}
+static OEval o_gd_eval(const OGd* g, V3 wo, V3 wi) {
+    OEval r = { v3(0.f, 0.f, 0.f), 0.f };
+    if (wi.z <= 0.f) return r;
+    r.f = muls(g->base, g->kd * 0.31830989f); r.pdf = (1.f - g->pSpec) * wi.z * 0.31830989f;
+    if (!g->delta && g->Fo > 0.f) {
+        V3 m = normz(add(wo, wi)); float om = dot3(wo, m);
+        if (om > 0.f) {
+            float s = g->ws * o_fd(om, g->eta) * o_d(m.z, g->a2) * o_g2(wo.z, wi.z, g->a2) / (4.f * wo.z * wi.z);
+            r.f = add(r.f, v3(s, s, s)); r.pdf += g->pSpec * o_vpdf(wo, m, g->a2) / (4.f * om);
+        }
+    }
+    return r;
+}
+static int o_gd_sample(const OGd* g, V3 wo, float u, float u1, float u2, V3* wi, V3* w, float* pdf) {
+    if (u < g->pSpec) {
+        if (g->delta) { *wi = v3(-wo.x, -wo.y, wo.z); float s = g->Fo / g->pSpec; *w = v3(s, s, s); *pdf = 0.f; return 1; }
+        V3 m = o_vsample(wo, g->a, u1, u2); *wi = sub(muls(m, 2.f * dot3(wo, m)), wo);
+        if (wi->z <= 0.f) return 0;
+    } else { *wi = o_cos_dir(u1, u2); if (wi->z <= 0.f) return 0; }
+    OEval e = o_gd_eval(g, wo, *wi); if (e.pdf <= 0.f) return 0;
+    *w = muls(e.f, wi->z / e.pdf); *pdf = e.pdf; return 1;
+}
+/* conductor (bsdf.h:127-148) */
+static OEval o_cond_eval(const OMat* m, V3 wo, V3 wi) {
+    OEval r = { v3(0.f, 0.f, 0.f), 0.f }; float a = m->roughness * m->roughness, a2 = a * a;
+    if (a < O_DELTA || wi.z <= 0.f) return r;
+    V3 h = normz(add(wo, wi)); float om = dot3(wo, h); if (om <= 0.f) return r;
+    r.f = muls(o_f82(v3(m->base[0], m->base[1], m->base[2]), v3(m->spec[0], m->spec[1], m->spec[2]), om), m->ws * o_d(h.z, a2) * o_g2(wo.z, wi.z, a2) / (4.f * wo.z * wi.z));
+    r.pdf = o_vpdf(wo, h, a2) / (4.f * om);
+    return r;
+}
+static int o_cond_sample(const OMat* m, V3 wo, float u1, float u2, V3* wi, V3* w, float* pdf) {
+    float a = m->roughness * m->roughness, a2 = a * a; V3 F0 = v3(m->base[0], m->base[1], m->base[2]), tint = v3(m->spec[0], m->spec[1], m->spec[2]);
+    if (a < O_DELTA) { *wi = v3(-wo.x, -wo.y, wo.z); *w = muls(o_f82(F0, tint, wo.z), m->ws); *pdf = 0.f; return 1; }
+    V3 h = o_vsample(wo, a, u1, u2); float om = dot3(wo, h); *wi = sub(muls(h, 2.f * om), wo);
+    if (wi->z <= 0.f || om <= 0.f) return 0;
+    *w = muls(o_f82(F0, tint, om), m->ws * o_g2(wo.z, wi->z, a2) / o_g1(wo.z, a2));
+    *pdf = o_vpdf(wo, h, a2) / (4.f * om); return 1;
+}
+/* rough dielectric (bsdf.h:151-192) */
+static OEval o_diel_eval(const OMat* m, float eta, V3 wo, V3 wi) {
+    OEval r = { v3(0.f, 0.f, 0.f), 0.f }; float a = m->roughness * m->roughness, a2 = a * a;
+    if (a < O_DELTA) return r;
+    if (wi.z > 0.f) {
+        V3 h = normz(add(wo, wi)); float om = dot3(wo, h); if (om <= 0.f) return r;
+        float F = o_fd(om, eta), s = F * o_d(h.z, a2) * o_g2(wo.z, wi.z, a2) / (4.f * wo.z * wi.z);
+        r.f = v3(s, s, s); r.pdf = F * o_vpdf(wo, h, a2) / (4.f * om);
+    } else if (wi.z < 0.f) {
+        V3 h = normz(add(wo, muls(wi, eta))); if (h.z < 0.f) h = neg(h);
+        float om = dot3(wo, h), im = dot3(wi, h); if (om <= 0.f || im >= 0.f) return r;
+        float F = o_fd(om, eta); if (F >= 1.f) return r;
+        float den = om + eta * im, j = eta * eta * (-im) / (den * den);
+        float s = (1.f - F) * o_d(h.z, a2) * o_g2(wo.z, -wi.z, a2) * om * j / (wo.z * -wi.z);
+        r.f = muls(v3(m->base[0], m->base[1], m->base[2]), s); r.pdf = (1.f - F) * o_vpdf(wo, h, a2) * j;
+    }
+    return r;
+}
+static int o_diel_sample(const OMat* m, float eta, V3 wo, float u, float u1, float u2, V3* wi, V3* w, float* pdf) {
+    float a = m->roughness * m->roughness; int delta = a < O_DELTA;
+    V3 h = delta ? v3(0.f, 0.f, 1.f) : o_vsample(wo, a, u1, u2);
+    float om = dot3(wo, h); if (om <= 0.f) return 0;
+    float F = o_fd(om, eta);
+    if (u < F) { *wi = sub(muls(h, 2.f * om), wo); if (wi->z <= 0.f) return 0; if (delta) { *w = v3(1.f, 1.f, 1.f); *pdf = 0.f; return 1; } }
+    else {
+        float ct = sqrtf(fmaxf(1.f - (1.f - om * om) / (eta * eta), 0.f));
+        *wi = add(muls(wo, -1.f / eta), muls(h, om / eta - ct)); if (wi->z >= 0.f) return 0;
+        *wi = normz(*wi);
+        if (delta) { *w = v3(m->base[0], m->base[1], m->base[2]); *pdf = 0.f; return 1; }
+    }
+    OEval e = o_diel_eval(m, eta, wo, *wi); if (e.pdf <= 0.f) return 0;
+    *w = muls(e.f, fabsf(wi->z) / e.pdf); *pdf = e.pdf; return 1;
+}
+static void o_weights(const OMat* m, float* wM, float* wT, float* wD) { *wM = m->metallic; *wT = (1.f - m->metallic) * m->transmission; *wD = (1.f - m->metallic) * (1.f - m->transmission); }
+static int o_non_delta(const OMat* m) {
+    float wM, wT, wD; o_weights(m, &wM, &wT, &wD); int rough = m->roughness * m->roughness >= O_DELTA;
+    return (wD > 0.f && (o_lum(v3(m->base[0], m->base[1], m->base[2])) > 0.f || rough)) || ((wM > 0.f || wT > 0.f) && rough);
+}
+static OEval o_bsdf_eval(const OMat* m, V3 wo, V3 wi, float eta, int gd, float ux1, float ux2) {
+    float wM, wT, wD; o_weights(m, &wM, &wT, &wD); OEval r = { v3(0.f, 0.f, 0.f), 0.f };
+    if (wM > 0.f) { OEval e = o_cond_eval(m, wo, wi); r.f = add(r.f, muls(e.f, wM)); r.pdf += wM * e.pdf; }
+    if (wT > 0.f) { OEval e = o_diel_eval(m, eta, wo, wi); r.f = add(r.f, muls(e.f, wT)); r.pdf += wT * e.pdf; }
+    if (wD > 0.f) { OGd g = o_gd(m, wo, gd, ux1, ux2); OEval e = o_gd_eval(&g, wo, wi); r.f = add(r.f, muls(e.f, wD)); r.pdf += wD * e.pdf; }
+    return r;
+}
+static int o_bsdf_sample(const OMat* m, V3 wo, float eta, int gd, float ux1, float ux2, float u, float u1, float u2, V3* wi, V3* w, float* pdf) {
+    float wM, wT, wD; o_weights(m, &wM, &wT, &wD); int ok;
+    if (u < wM) ok = o_cond_sample(m, wo, u1, u2, wi, w, pdf);
+    else if (u < wM + wT) ok = o_diel_sample(m, eta, wo, fminf((u - wM) / wT, 0.99999994f), u1, u2, wi, w, pdf);
+    else { OGd g = o_gd(m, wo, gd, ux1, ux2); ok = o_gd_sample(&g, wo, fminf(wD > 0.f ? (u - wM - wT) / wD : 0.f, 0.99999994f), u1, u2, wi, w, pdf); }
+    if (!ok) return 0;
+    if (*pdf <= 0.f) return 1;
+    if (wM == 1.f || wT == 1.f || wD == 1.f) return 1;
+    OEval e = o_bsdf_eval(m, wo, *wi, eta, gd, ux1, ux2); if (e.pdf <= 0.f) return 0;
+    *w = muls(e.f, fabsf(wi->z) / e.pdf); *pdf = e.pdf; return 1;
+}
+void orc_bsdf_eval(const float* mats, const int* mat, const float* wo, const float* wi, const float* eta, int gd, const float* ux, float* f, float* pdf, long n) {
+    for (long i = 0; i < n; i++) {
+        OEval e = o_bsdf_eval((const OMat*)(mats + 16 * (size_t)mat[i]), a3(wo + 3 * i), a3(wi + 3 * i), eta[i], gd, ux[2 * i], ux[2 * i + 1]);
+        f[3 * i] = e.f.x; f[3 * i + 1] = e.f.y; f[3 * i + 2] = e.f.z; pdf[i] = e.pdf;
+    }
+}
+void orc_bsdf_sample(const float* mats, const int* mat, const float* wo, const float* eta, int gd, const float* ux, const float* uvw, float* wi, float* w, float* pdf, int* ok, long n) {
+    for (long i = 0; i < n; i++) {
+        V3 a = v3(0.f, 0.f, 0.f), b = a; float p = 0.f;
+        ok[i] = o_bsdf_sample((const OMat*)(mats + 16 * (size_t)mat[i]), a3(wo + 3 * i), eta[i], gd, ux[2 * i], ux[2 * i + 1], uvw[3 * i], uvw[3 * i + 1], uvw[3 * i + 2], &a, &b, &p);
+        wi[3 * i] = a.x; wi[3 * i + 1] = a.y; wi[3 * i + 2] = a.z; w[3 * i] = b.x; w[3 * i + 1] = b.y; w[3 * i + 2] = b.z; pdf[i] = p;
+    }
+}
+
+/* ------------------------------------------------------------------ serving form: one request on the host
+ * Not a reference function as a whole: restates the CUDA serving loop's per-path arithmetic (camera ray with a box
+ * filter, render/wavefront.cu:42-58; shading = shadeFull restricted to the sun and a constant sky,
+ * render/wavefront.cu:223-356) over the two-level scene above and the BSDF restatement. Paths [j0, j1) of the request
+ * in the CUDA path order (pixel = tile order of j mod N, sample j / N); accum = w * h float4 sums, counts[0] closest
+ * rays, counts[1] shadow rays. */
+typedef struct { float pos[3], ax[3], ay[3], az[3], fx, fy, px, py; int w, h; float lens_r, focus_d; } OCam;
+typedef struct { int scene, frame; OCam cam; int spp, max_depth; unsigned seed; float sun_to[3], sun_e[3], sky[3], sun_cos, eps; } OReq;
+static int o_tile_pixel(int j, int w, int h) {
+    if ((w & 7) | (h & 3)) return j;
+    const int t = j >> 5, r = j & 31, tilesX = w >> 3;
+    return ((t / tilesX) * 4 + (r >> 3)) * w + (t % tilesX) * 8 + (r & 7);
+}
+long orc_render_request(const void* reqp, int width, const float* blas, const float* tris, const float* tlas, int root, const float* inst,
+                        const float* mats, int n_mats, const int* mesh_mat, int gd, long j0, long j1, float* accum, long long* counts) {
+    const OReq* R = (const OReq*)reqp; const OCam* C = &R->cam;
+    const int N = C->w * C->h; long bad = 0;
+    const V3 sunTo = v3(R->sun_to[0], R->sun_to[1], R->sun_to[2]), sunE = v3(R->sun_e[0], R->sun_e[1], R->sun_e[2]), sky = v3(R->sky[0], R->sky[1], R->sky[2]);
+    for (long j = j0; j < j1; j++) {
+        const int pix = o_tile_pixel((int)(j % N), C->w, C->h); const unsigned smp = (unsigned)(j / N), seed = R->seed;
+        const int x = pix % C->w, y = pix / C->w;
+        const float jx = orc_rng(pix, smp, 0, 0, seed) - 0.5f, jy = orc_rng(pix, smp, 0, 1, seed) - 0.5f;
+        const float dx = (x + 0.5f + jx - C->px) / C->fx, dy = -(y + 0.5f + jy - C->py) / C->fy;
+        V3 o = v3(C->pos[0], C->pos[1], C->pos[2]);
+        V3 d = normz(sub(add(muls(v3(C->ax[0], C->ax[1], C->ax[2]), dx), muls(v3(C->ay[0], C->ay[1], C->ay[2]), dy)), v3(C->az[0], C->az[1], C->az[2])));
+        V3 T = v3(1.f, 1.f, 1.f);
+        float* A = accum + 4 * (size_t)pix;
+        for (int depth = 0;; depth++) {
+            float t = 1e30f, u, v; int tri, hi;
+            if (o_inst1(width, 0, blas, tris, (const V4*)tlas, root, inst, o, d, 0.f, &t, &tri, &u, &v, &hi) < 0) bad++;
+            counts[0]++;
+            if (tri < 0) { A[0] += T.x * sky.x; A[1] += T.y * sky.y; A[2] += T.z * sky.z; break; }
+            const float* I = inst + 28 * (size_t)hi;
+            const V4* TR = (const V4*)tris;
+            const V3 e1 = xyz4(TR[3 * tri + 1]), e2 = xyz4(TR[3 * tri + 2]), no = cross3(e1, e2);
+            const V3 nw = v3(I[0] * no.x + I[4] * no.y + I[8] * no.z, I[1] * no.x + I[5] * no.y + I[9] * no.z, I[2] * no.x + I[6] * no.y + I[10] * no.z);
+            int imesh; memcpy(&imesh, &I[25], 4);
+            const V3 ng0 = muls(normz(nw), I[26]);
+            int mid = mesh_mat[imesh] + fi(TR[3 * tri + 1].w); mid = mid < 0 ? 0 : mid >= n_mats ? n_mats - 1 : mid;
+            const OMat* M = (const OMat*)(mats + 16 * (size_t)mid);
+            const V3 p = add(o, muls(d, t));
+            if (M->emission[0] > 0.f || M->emission[1] > 0.f || M->emission[2] > 0.f) { A[0] += T.x * M->emission[0]; A[1] += T.y * M->emission[1]; A[2] += T.z * M->emission[2]; }
+            if (depth > R->max_depth) break;
+            const int front = dot3(ng0, d) < 0.f;
+            const V3 ng = front ? ng0 : neg(ng0);
+            V3 ns = ng; const V3 wo = neg(d);
+            if (dot3(ns, wo) <= 1e-6f) ns = ng;
+            V3 tx, ty; onb(ns, &tx, &ty);
+            const V3 woL = v3(dot3(wo, tx), dot3(wo, ty), dot3(wo, ns));
+            const float eta = front ? M->ior : 1.f / M->ior;
+            const V3 up = add(p, muls(ng, R->eps)), dn = sub(p, muls(ng, R->eps));
+            const unsigned dr = (unsigned)depth + 1u;
+            const float ux1 = orc_rng(pix, smp, dr, 7, seed), ux2 = orc_rng(pix, smp, dr, 7, seed ^ 0x68E31DA4u);
+            if (o_non_delta(M)) {
+                const V3 l = cone_dir(sunTo, R->sun_cos, orc_rng(pix, smp, dr, 2, seed), orc_rng(pix, smp, dr, 3, seed));
+                const V3 lL = v3(dot3(l, tx), dot3(l, ty), dot3(l, ns));
+                const float gl = dot3(ng, l);
+                if (lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
+                    const OEval e = o_bsdf_eval(M, woL, lL, eta, gd, ux1, ux2);
+                    const V3 c = muls(mulv(mulv(T, e.f), sunE), fabsf(lL.z));
+                    if (c.x > 0.f || c.y > 0.f || c.z > 0.f) {
+                        float st = 1e30f, su, sv; int sh, shi;
+                        if (o_inst1(width, 1, blas, tris, (const V4*)tlas, root, inst, gl > 0.f ? up : dn, l, 0.f, &st, &sh, &su, &sv, &shi) < 0) bad++;
+                        counts[1]++;
+                        if (sh < 0) { A[0] += c.x; A[1] += c.y; A[2] += c.z; }
+                    }
+                }
+            }
+            V3 wiL, wgt; float pdf;
+            if (!o_bsdf_sample(M, woL, eta, gd, ux1, ux2, orc_rng(pix, smp, dr, 4, seed), orc_rng(pix, smp, dr, 0, seed), orc_rng(pix, smp, dr, 1, seed), &wiL, &wgt, &pdf)) break;
+            const V3 wi = normz(add(add(muls(tx, wiL.x), muls(ty, wiL.y)), muls(ns, wiL.z)));
+            const float gi = dot3(ng, wi);
+            if (gi == 0.f || (gi > 0.f) != (wiL.z > 0.f)) break;
+            T = mulv(T, wgt);
+            if (!(fmaxf(T.x, fmaxf(T.y, T.z)) > 0.f)) break;
+            o = gi > 0.f ? up : dn; d = wi;
+        }
     }
     return bad;
 }

@@ -5,6 +5,7 @@
 //   traversal ........... accel/traverse.cuh trav<V, ANY, TRI> compiled as host C++ through ref_shim.h
 //   instance transforms . scene/instances.cpp invertXform / instanceXform (with io/json.cpp, which it links)
 //   two-level traversal . accel/traverse_inst.cuh travInst<V, ANY, TRI> compiled as host C++ through ref_shim.h
+//   materials ........... render/bsdf.h bsdfEval / bsdfSample (host + device code, compiled for the host)
 // The harness (threads, argument marshalling) is ours; the arithmetic is the reference's.
 #include "ref_shim.h"
 #include "accel/bvh_builder.h"
@@ -15,6 +16,7 @@
 #include "accel/traverse_inst.cuh"
 #include "core/rng.h"
 #include "scene/instances.h"
+#include "render/bsdf.h"
 #include "core/sampling.h"
 #include <algorithm>
 #include <chrono>
@@ -210,3 +212,21 @@ extern "C" double ref_trace_inst(int variant, int any, int tri, const float* bla
     for (auto& t : ts) t.join();
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
+
+// render/bsdf.h:196-220 for n (material, wo, wi) triples; mats: Material records (scene/material.h:12-17, 64 B)
+extern "C" void ref_bsdf_eval(const void* mats, const int* mat, const float* wo, const float* wi, const float* eta, int gd, const float* ux, float* f, float* pdf, long n) {
+    const Material* M = (const Material*)mats;
+    for (long i = 0; i < n; i++) {
+        BsdfEval e = bsdfEval(M[mat[i]], make_float3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), make_float3(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), eta[i], gd, ux[2 * i], ux[2 * i + 1]);
+        f[3 * i] = e.f.x; f[3 * i + 1] = e.f.y; f[3 * i + 2] = e.f.z; pdf[i] = e.pdf;
+    }
+}
+extern "C" void ref_bsdf_sample(const void* mats, const int* mat, const float* wo, const float* eta, int gd, const float* ux, const float* uvw, float* wi, float* w, float* pdf, int* ok, long n) {
+    const Material* M = (const Material*)mats;
+    for (long i = 0; i < n; i++) {
+        float3 a = make_float3(0.f, 0.f, 0.f), b = a; float p = 0.f;
+        ok[i] = bsdfSample(M[mat[i]], make_float3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), eta[i], gd, ux[2 * i], ux[2 * i + 1], uvw[3 * i], uvw[3 * i + 1], uvw[3 * i + 2], a, b, p) ? 1 : 0;
+        wi[3 * i] = a.x; wi[3 * i + 1] = a.y; wi[3 * i + 2] = a.z; w[3 * i] = b.x; w[3 * i + 1] = b.y; w[3 * i + 2] = b.z; pdf[i] = p;
+    }
+}
+extern "C" int ref_material_size(void) { return (int)sizeof(Material); }

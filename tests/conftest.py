@@ -51,6 +51,12 @@ def _load_oracle():
     L.orc_trace_prec.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_trace_inst.restype = C.c_long
     L.orc_trace_inst.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_long, C.c_void_p, C.c_void_p]
+    L.orc_bsdf_eval.restype = None
+    L.orc_bsdf_eval.argtypes = [C.c_void_p] * 5 + [C.c_int] + [C.c_void_p] * 3 + [C.c_long]
+    L.orc_bsdf_sample.restype = None
+    L.orc_bsdf_sample.argtypes = [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 6 + [C.c_long]
+    L.orc_render_request.restype = C.c_long
+    L.orc_render_request.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
     L.orc_half_round.restype = C.c_double
     L.orc_half_round.argtypes = [C.c_double, C.c_int]
     L.orc_rng.restype = C.c_float
@@ -124,6 +130,31 @@ class Oracle:
                                     hits.ctypes.data, hi.ctypes.data)
         assert bad == 0
         return hits, hi
+
+    def bsdf_eval(self, mats, mat, wo, wi, eta, gd, ux):
+        n = len(mat); f = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32)
+        a = [np.ascontiguousarray(x) for x in (mats, mat, wo, wi, eta, ux)]
+        self.L.orc_bsdf_eval(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, a[4].ctypes.data, gd, a[5].ctypes.data, f.ctypes.data, pdf.ctypes.data, n)
+        return f, pdf
+
+    def bsdf_sample(self, mats, mat, wo, eta, gd, ux, uvw):
+        n = len(mat); wi = np.zeros((n, 3), np.float32); w = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32); ok = np.zeros(n, np.int32)
+        a = [np.ascontiguousarray(x) for x in (mats, mat, wo, eta, ux, uvw)]
+        self.L.orc_bsdf_sample(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, gd, a[4].ctypes.data, a[5].ctypes.data,
+                               wi.ctypes.data, w.ctypes.data, pdf.ctypes.data, ok.ctypes.data, n)
+        return wi, w, pdf, ok
+
+    def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None):
+        """A serving request on the host: (accum [w h, 4], counts [2])."""
+        n = req.cam.w * req.cam.h * req.spp
+        j0, j1 = (0, n) if paths is None else paths
+        acc = np.zeros((req.cam.w * req.cam.h, 4), np.float32); cnt = np.zeros(2, np.int64)
+        a = [np.ascontiguousarray(x) for x in (blas, tris, tlas)]
+        ins = np.ascontiguousarray(inst, np.float32); ms = np.ascontiguousarray(mats, np.float32); mm = np.ascontiguousarray(mesh_mat, np.int32)
+        bad = self.L.orc_render_request(C.addressof(req), width, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, int(root), ins.ctypes.data,
+                                        ms.ctypes.data, len(ms), mm.ctypes.data, gd, j0, j1, acc.ctypes.data, cnt.ctypes.data)
+        assert bad == 0
+        return acc, cnt
 
     def render(self, params, variant, tri, bvh, bounces, spp, s_base=0, pix0=0, pix1=None):
         w, h = params.cam.w, params.cam.h

@@ -14,6 +14,13 @@ and tests/golden/instances.npz:
   outputs  the reference's invertXform inverses and determinant signs and its instanceXform matrices; the reference
            traversal's closest hits and any-hit occluders over its BVH4 nodes of boxes64 (Woop and Moller-Trumbore)
 
+and tests/golden/bsdf.npz:
+
+  inputs   96 seeded materials (Lambertian, glossy-diffuse, rough and mirror conductors, rough and smooth glass, blends)
+           and 2,048 (material, wo, wi, eta, glossy-diffuse random pair, sample triple) cases
+  outputs  the reference's bsdfEval f and pdf and bsdfSample wi / weight / pdf / success (render/bsdf.h), with the
+           glossy-diffuse energy compensation off and on
+
 The fixtures pin the oracle and the library where the reference sources are absent. Run from the repository root:
     python tests/golden/make_golden.py
 """
@@ -52,6 +59,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "boxes64.npz"), **out)
     print("wrote", os.path.join(HERE, "boxes64.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
     instances(ref, out)
+    bsdf(ref)
 
 
 def instances(ref, box):
@@ -97,3 +105,49 @@ def instances(ref, box):
 
 if __name__ == "__main__":
     main()
+
+
+def materials(rng, n):
+    """n materials as float32 [n, 16] in the cwp_material layout, spanning every base and blend"""
+    m = np.zeros((n, 16), np.float32)
+    for i in range(n):
+        kind = i % 8
+        base = rng.uniform(0.05, 0.95, 3); spec = rng.uniform(0.5, 1.0, 3)
+        rough = rng.choice([0.0, 0.02, rng.uniform(0.05, 1.0)], p=[0.1, 0.1, 0.8])
+        metallic, trans, ws = 0.0, 0.0, 1.0
+        if kind == 0: ws, rough = 0.0, 1.0                       # Lambertian
+        elif kind == 1: metallic = 1.0                           # conductor
+        elif kind == 2: trans = 1.0                              # glass
+        elif kind == 3: metallic = rng.uniform(0.2, 0.8)         # blend conductor / glossy-diffuse
+        elif kind == 4: trans = rng.uniform(0.2, 0.8)            # blend glass / glossy-diffuse
+        elif kind == 5: metallic, trans = 0.3, 0.5               # three bases
+        m[i, 0:3] = base; m[i, 3] = metallic; m[i, 4:7] = spec; m[i, 7] = rough; m[i, 11] = 1.5; m[i, 12] = ws; m[i, 13] = trans
+    return m
+
+
+def bsdf(ref):
+    import ctypes as C
+    L = ref.L
+    L.ref_bsdf_eval.restype = None; L.ref_bsdf_sample.restype = None
+    rng = np.random.default_rng(33)
+    mats = materials(rng, 96)
+    n = 2048
+    mat = rng.integers(0, len(mats), n).astype(np.int32)
+    def hemi(k, up=True):
+        v = rng.normal(size=(k, 3)); v /= np.linalg.norm(v, axis=1, keepdims=True)
+        if up: v[:, 2] = np.abs(v[:, 2]) + 1e-3
+        return (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
+    wo = hemi(n); wi = hemi(n, up=False)
+    wi[: n // 4] = (wo[: n // 4] * np.array([-1, -1, 1], np.float32))   # mirror directions
+    eta = np.where(rng.random(n) < 0.5, 1.5, 1 / 1.5).astype(np.float32)
+    ux = rng.random((n, 2)).astype(np.float32); uvw = rng.random((n, 3)).astype(np.float32)
+    out = dict(mats=mats, mat=mat, wo=wo, wi=wi, eta=eta, ux=ux, uvw=uvw)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    for gd in (0, 1):
+        f = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32)
+        L.ref_bsdf_eval(p(mats), p(mat), p(wo), p(wi), p(eta), C.c_int(gd), p(ux), p(f), p(pdf), C.c_long(n))
+        sw = np.zeros((n, 3), np.float32); sWt = np.zeros((n, 3), np.float32); spdf = np.zeros(n, np.float32); ok = np.zeros(n, np.int32)
+        L.ref_bsdf_sample(p(mats), p(mat), p(wo), p(eta), C.c_int(gd), p(ux), p(uvw), p(sw), p(sWt), p(spdf), p(ok), C.c_long(n))
+        out.update({f"f{gd}": f, f"pdf{gd}": pdf, f"s_wi{gd}": sw, f"s_w{gd}": sWt, f"s_pdf{gd}": spdf, f"s_ok{gd}": ok})
+    np.savez_compressed(os.path.join(HERE, "bsdf.npz"), **out)
+    print("wrote", os.path.join(HERE, "bsdf.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")

@@ -1,0 +1,103 @@
+"""Serving form on the GPU: device BSDFs against the reference's own render/bsdf.h (fixture), a request's image
+against the oracle's host restatement of the serving integrator, the same request alone and inside a mix of
+concurrent requests, continuous batching against the plain form, and admission by free device memory."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def close(a, b, rel, abs_):
+    return np.abs(a - b) <= abs_ + rel * np.maximum(np.abs(a), np.abs(b))
+
+
+def test_device_bsdf_matches_reference(gpu, cwp):
+    g = golden("bsdf.npz")
+    for gd in (0, 1):
+        f, pdf = cwp.bsdf_eval_batch(g["mats"], g["mat"], g["wo"], g["wi"], g["eta"], gd, g["ux"])
+        assert close(f, g[f"f{gd}"], 1e-4, 1e-6).mean() >= 0.999 and close(pdf, g[f"pdf{gd}"], 1e-4, 1e-6).mean() >= 0.999
+        wi, w, p, ok = cwp.bsdf_sample_batch(g["mats"], g["mat"], g["wo"], g["eta"], gd, g["ux"], g["uvw"])
+        same = ok == g[f"s_ok{gd}"]
+        assert same.mean() >= 0.998
+        k = same & (ok == 1)
+        assert close(wi[k], g[f"s_wi{gd}"][k], 1e-3, 1e-4).mean() >= 0.998 and close(w[k], g[f"s_w{gd}"][k], 1e-3, 1e-4).mean() >= 0.998
+
+
+@pytest.fixture(scope="module")
+def serving(gpu, cwp):
+    meshes, descs, first, mats, base, boxes = cwp.serving_scenes(n_scenes=3, seed=2, tris=(200, 8000), instances=(1, 24), blas_per_scene=(1, 3))
+    b = cwp.Batch(meshes)
+    return b, descs, first, mats, base, boxes
+
+
+def server(cwp, serving, **kw):
+    b, descs, first, mats, base, boxes = serving
+    s = cwp.Server(b, mats, base, **kw)
+    s.set_scenes(descs, first)
+    return s
+
+
+def run_all(s, reqs):
+    ids = [s.submit(r) for r in reqs]
+    done = {}
+    for _ in range(100000):
+        a, p = s.step()
+        for i in s.poll():
+            done[i] = True
+        if len(done) == len(ids):
+            break
+    assert len(done) == len(ids)
+    out = []
+    for i, r in zip(ids, reqs):
+        acc, st = s.result(i, r.cam.w, r.cam.h)
+        out.append((acc, st))
+    return out
+
+
+def requests(cwp, boxes, n, seed, res=((32, 32), (48, 32), (64, 64)), spps=(1, 2, 4)):
+    return [r for _, r in cwp.serving_requests(n, 100.0, boxes, seed=seed, resolutions=list(res), spps=list(spps))]
+
+
+def test_request_matches_oracle(gpu, cwp, oracle, serving):
+    b, descs, first, mats, base, boxes = serving
+    s = server(cwp, serving, max_paths=1 << 16, max_requests=4)
+    req = requests(cwp, boxes, 1, seed=3, res=((64, 48),), spps=(4,))[0]
+    (acc, st), = run_all(s, [req])
+    nodes, tris = b.download(b.tuning().width)
+    tlas, roots, inst = b.download_tlas(4, _n_inst(b, 4))   # the server's slots are the batch's scenes; slot 0 held the request
+    ref, cnt = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, mats, base)
+    a = acc[:, :3] / req.spp; r = ref[:, :3] / req.spp
+    assert cwp.imageio.psnr(a, r) >= 50.0
+    assert abs(st.rays - cnt[0]) <= 2e-3 * cnt[0] and abs(st.shadow_rays - cnt[1]) <= 2e-3 * max(cnt[1], 1)
+    assert st.done_ms >= st.admit_ms >= st.submit_ms
+
+
+def _n_inst(b, n_scenes):
+    """instances currently in the batch's TLAS set"""
+    return int(b.info().n_instances)
+
+
+def test_alone_equals_in_the_mix(gpu, cwp, serving):
+    """Every request's image is the same whether it runs alone (plain form, one request at a time) or among others
+    admitted concurrently: only the order of float atomics differs."""
+    b, descs, first, mats, base, boxes = serving
+    reqs = requests(cwp, boxes, 8, seed=5)
+    mix = run_all(server(cwp, serving, max_paths=1 << 15, max_requests=8), reqs)
+    alone = run_all(server(cwp, serving, max_paths=1 << 15, max_requests=1), reqs)
+    for (am, sm), (aa, sa) in zip(mix, alone):
+        assert sm.rays == sa.rays and sm.shadow_rays == sa.shadow_rays
+        assert np.allclose(am, aa, rtol=1e-4, atol=1e-5)
+    # in the mix, requests overlapped: some request was admitted before an earlier one finished
+    adm = sorted((s.admit_ms, s.done_ms) for _, s in mix)
+    assert any(adm[i + 1][0] < adm[i][1] for i in range(len(adm) - 1))
+
+
+def test_admission_waits_for_memory(gpu, cwp, serving):
+    s = server(cwp, serving, max_paths=1 << 12, max_requests=4, hbm_reserve=1 << 50)   # more than any device has
+    req = requests(cwp, serving[5], 1, seed=9)[0]
+    s.submit(req)
+    for _ in range(3):
+        a, p = s.step()
+        assert a == 0 and p == 1
