@@ -377,6 +377,7 @@ def bench_serving(args, wl, cwp, torch, out):
         clk = Clocks(str(torch.cuda.current_device()))
         res[mode] = serve_stream(cwp, s, stream)
         res[mode]["clocks"] = clk.stop()
+        res[mode]["breakdown"] = s.info()
         del s
     c, p = res["continuous"], res["plain"]
     info = b.info()
@@ -412,6 +413,7 @@ def main():
     ap.add_argument("--scenes", type=int, default=0, help="override the scene count of batched64 (profiling cases)")
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
+    ap.add_argument("--spatial", type=float, default=0.0, help="host BVH: spatial-split overlap threshold (0 = binned SAH only, 1e-5 = SBVH)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
@@ -439,7 +441,7 @@ def main():
     cwp = importlib.import_module("cuda-wavefront-pathtracer_b200")
     variant = args.variant
     if not wl.get("batched") and not wl.get("serving"):
-        mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=args.bins)
+        mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=args.bins, spatial=args.spatial)
 
     def barrier():
         if ws > 1:
@@ -512,6 +514,7 @@ def main():
         out.update(metric="closest+shadow rays per second, diffuse frame", value=value, ms_per_step=max_ms / args.steps,
                    config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles, box field seed 1)", "resolution": f"{w}x{h}",
                            "spp": spp, "batch": K, "depth": B, "layout": LAYOUT_NAMES[variant], "sah_bins": args.bins, "tri": "woop",
+                           "bvh": (f"sbvh (spatial splits at overlap > {args.spatial:g} of the root area, {len(bvh.order) / mesh.n_tris:.2f} references per triangle)" if args.spatial > 0 else "binned SAH"),
                            "graph": args.graph, "traversal": ["auto", "refill", "batch"][args.traversal], "sort": ["off", "octant", "octant+cell"][args.sort], "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
                            "rays_per_frame": (rays + shadow) / args.steps, "closest_per_frame": rays / args.steps, "shadow_per_frame": shadow / args.steps,
                            "rays_per_sample": (rays + shadow) / args.steps / (w * h * spp), "trace_shade_ms": float(tms.sum() / args.steps),
@@ -605,7 +608,8 @@ def main():
         out.update(metric="closest+any rays per second, incoherent ray batch", value=value, ms_per_step=max_ms / args.steps,
                    config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles)", "rays": n,
                            "layout": LAYOUT_NAMES[variant] + (" precision form (f16 conservative slabs, watertight fp32 triangles)" if wl.get("precision") else ""), **check,
-                           "sah_bins": args.bins, "tri": "woop", "traversal": ["auto", "refill", "batch"][args.traversal], "l2": f"ray batch {n * 32 / 1e9:.2f} GB > L2 (126 MB)",
+                           "sah_bins": args.bins, "tri": "woop", "traversal": ["auto", "refill", "batch"][args.traversal],
+                           "bvh": (f"sbvh ({len(bvh.order) / mesh.n_tris:.2f} references per triangle)" if args.spatial > 0 else "binned SAH"), "l2": f"ray batch {n * 32 / 1e9:.2f} GB > L2 (126 MB)",
                            "closest_ms": c_ms / args.steps, "any_ms": a_ms / args.steps},
                    clocks=clocks,
                    e2e={"value": 2 * n * args.steps * ws / e_s / 1e9, "unit": "Grays/s", "h2d_bytes_per_step": 2 * 2 * n * 16, "d2h_bytes_per_step": n * 16 + n * 4},

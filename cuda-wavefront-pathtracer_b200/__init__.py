@@ -33,7 +33,7 @@ class MeshView(C.Structure):
 
 
 class BuildOptions(C.Structure):
-    _fields_ = [("variant", C.c_int32), ("bins", C.c_int32), ("leaf", C.c_int32), ("collapse", C.c_int32), ("threads", C.c_int32)]
+    _fields_ = [("variant", C.c_int32), ("bins", C.c_int32), ("leaf", C.c_int32), ("collapse", C.c_int32), ("threads", C.c_int32), ("spatial", C.c_float)]
 
 
 class BvhData(C.Structure):
@@ -120,6 +120,12 @@ class RequestStats(C.Structure):
                 ("w", C.c_int32), ("h", C.c_int32), ("spp", C.c_int32), ("pad", C.c_int32)]
 
 
+class ServerInfo(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("rays", C.c_int64), ("shadow_rays", C.c_int64), ("admissions", C.c_int64), ("tlas_rebuilds", C.c_int64),
+                ("closest_ms", C.c_double), ("shade_ms", C.c_double), ("shadow_ms", C.c_double), ("raygen_ms", C.c_double), ("tlas_ms", C.c_double),
+                ("step_ms", C.c_double)]
+
+
 # every exported symbol of the C ABI with its ctypes signature (restype, argtypes)
 SIGNATURES = {
     "cwp_last_error": (C.c_char_p, []),
@@ -178,6 +184,7 @@ SIGNATURES = {
     "cwp_server_poll": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_int32)]),
     "cwp_server_result": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.POINTER(RequestStats)]),
     "cwp_server_clock_ms": (C.c_double, [C.c_void_p]),
+    "cwp_server_info_of": (C.c_int, [C.c_void_p, C.POINTER(ServerInfo)]),
     "cwp_bsdf_eval_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 4 + [C.c_int32] + [C.c_void_p] * 3 + [C.c_int64]),
     "cwp_bsdf_sample_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 3 + [C.c_int32] + [C.c_void_p] * 6 + [C.c_int64]),
     "cwp_camera_look_at": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
@@ -276,8 +283,8 @@ class Mesh:
 class Bvh:
     """Host BVH build result: GPU node array, leaf order, packed triangles and Woop rows (numpy copies)."""
 
-    def __init__(self, mesh, variant=LAYOUT_BVH2, bins=16, leaf=4, collapse=0, threads=0):
-        o = BuildOptions(variant, bins, leaf, collapse, threads)
+    def __init__(self, mesh, variant=LAYOUT_BVH2, bins=16, leaf=4, collapse=0, threads=0, spatial=0.0):
+        o = BuildOptions(variant, bins, leaf, collapse, threads, spatial)
         h = C.c_void_p()
         _check(lib().cwp_bvh_build(mesh._h, C.byref(o), C.byref(h)))
         try:
@@ -606,6 +613,10 @@ class Server:
 
     def clock_ms(self):
         return lib().cwp_server_clock_ms(self._h)
+
+    def info(self):
+        i = ServerInfo(); _check(lib().cwp_server_info_of(self._h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in ServerInfo._fields_}
 
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value and _lib is not None:

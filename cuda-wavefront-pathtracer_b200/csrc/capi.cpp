@@ -94,7 +94,9 @@ extern "C" int cwp_bvh_build(const cwp_mesh* h, const cwp_build_options* o, cwp_
     // the greedy 8-wide layout caps leaves at 4 (3 bits of count in the meta byte)
     so.leafMax = cw ? 1 : (o->variant == 8 && o->leaf > 4) ? 4 : o->leaf;
     CWPB_CHECK(o->variant == 8 || so.leafMax <= 64, CWP_ERR_INVALID, "leaf too large");
-    BinaryBvh B; build_sah(m, so, B);
+    CWPB_CHECK(o->spatial >= 0.f && o->spatial < 1.f, CWP_ERR_INVALID, "spatial %g out of [0, 1)", o->spatial);
+    BinaryBvh B;
+    if (o->spatial > 0.f) build_sbvh(m, so, o->spatial, 0.3f, B); else build_sah(m, so, B);
     cwp_bvh* r = new cwp_bvh();
     r->maxDepth = B.maxDepth;
     if (o->variant == 2) { r->sah = sah_cost(B, 1, 1); layout_bvh2(B, r->nodes); r->order = B.prim; r->stride = 4; }

@@ -139,6 +139,182 @@ void build_sah(const Mesh& m, const SahOptions& o, BinaryBvh& out) {
     out.nodes.swap(P.nodes); out.prim.swap(R.idx); out.maxDepth = P.maxDepth; out.leafMax = o.leafMax;
 }
 
+// ======================= spatial splits =======================
+// Binned SAH with spatial splits (Stich, Friedrich & Dietrich, "Spatial Splits in Bounding Volume Hierarchies",
+// HPG 2009): a node whose best object split leaves children overlapping by more than alpha of the root's area also
+// tries splitting space at bin planes, clipping the triangles that straddle a plane into both children; the cheaper
+// split by the SAH wins. Leaves then reference triangles (a triangle may appear in several leaves); a spatial split
+// may duplicate at most `budget` x the node's references (a local rule, so the tree does not depend on the order in
+// which subtrees are built).
+namespace {
+struct SRef { int tri; Box3 box; };
+struct SbvhRun {
+    const Mesh& m; const SahOptions& o; float alphaArea = 0.f, budget = 0.f;
+    struct Part { std::vector<BNode> nodes; std::vector<int> prim; int maxDepth = 0; };
+    SbvhRun(const Mesh& mm, const SahOptions& oo) : m(mm), o(oo) {}
+    static float comp(float3 v, int a) { return a == 0 ? v.x : a == 1 ? v.y : v.z; }
+    static void setc(float3& v, int a, float x) { if (a == 0) v.x = x; else if (a == 1) v.y = x; else v.z = x; }
+    static bool empty(const Box3& b) { return !(b.lo.x <= b.hi.x && b.lo.y <= b.hi.y && b.lo.z <= b.hi.z); }
+
+    // box of the part of triangle t with lo <= p[axis] <= hi, within `within`
+    Box3 chop(int t, int axis, float lo, float hi, const Box3& within) const {
+        const float3 v[3] = { m.vert(m.f[3 * t]), m.vert(m.f[3 * t + 1]), m.vert(m.f[3 * t + 2]) };
+        Box3 r;
+        for (int i = 0; i < 3; i++) {
+            const float3 a = v[i], c = v[(i + 1) % 3];
+            const float pa = comp(a, axis), pc = comp(c, axis);
+            if (pa >= lo && pa <= hi) r.grow(a);
+            for (int q = 0; q < 2; q++) {
+                const float plane = q ? hi : lo;
+                if ((pa < plane && pc > plane) || (pa > plane && pc < plane)) {
+                    const float s = (plane - pa) / (pc - pa);
+                    float3 x = f3(a.x + (c.x - a.x) * s, a.y + (c.y - a.y) * s, a.z + (c.z - a.z) * s); setc(x, axis, plane);
+                    r.grow(x);
+                }
+            }
+        }
+        r.lo = vmax(r.lo, within.lo); r.hi = vmin(r.hi, within.hi);
+        return r;
+    }
+
+    int node(std::vector<SRef>& refs, int depth, Part& P, int spawn) {
+        const int id = (int)P.nodes.size(); P.nodes.emplace_back();
+        P.maxDepth = std::max(P.maxDepth, depth);
+        Box3 box, cb;
+        for (const SRef& r : refs) { box.grow(r.box); cb.grow((r.box.lo + r.box.hi) * 0.5f); }
+        P.nodes[id].box = box;
+        const int n = (int)refs.size();
+        if (n <= o.leafMax || depth >= o.depthCap) {
+            P.nodes[id].first = (int)P.prim.size(); P.nodes[id].count = n;
+            for (const SRef& r : refs) P.prim.push_back(r.tri);
+            return id;
+        }
+        const int NB = o.bins;
+        // object split over the reference centroids
+        float objCost = FLT_MAX; int objAxis = -1, objBin = -1; Box3 objL, objR;
+        {
+            const float3 ext = cb.extent();
+            std::vector<Box3> bb(NB); std::vector<int> bc(NB); std::vector<Box3> rB(NB); std::vector<int> rC(NB);
+            for (int axis = 0; axis < 3; axis++) {
+                const float lo = comp(cb.lo, axis), ex = comp(ext, axis);
+                if (ex <= 1e-12f) continue;
+                const float scale = NB / ex;
+                std::fill(bb.begin(), bb.end(), Box3()); std::fill(bc.begin(), bc.end(), 0);
+                for (const SRef& r : refs) { int k = (int)((comp((r.box.lo + r.box.hi) * 0.5f, axis) - lo) * scale); k = k < 0 ? 0 : k > NB - 1 ? NB - 1 : k; bb[k].grow(r.box); bc[k]++; }
+                Box3 acc; int cnt = 0;
+                for (int k = NB - 1; k > 0; k--) { acc.grow(bb[k]); cnt += bc[k]; rB[k] = acc; rC[k] = cnt; }
+                Box3 la; int lc = 0;
+                for (int k = 0; k < NB - 1; k++) {
+                    la.grow(bb[k]); lc += bc[k];
+                    if (lc == 0 || rC[k + 1] == 0) continue;
+                    const float c = la.area() * lc + rB[k + 1].area() * rC[k + 1];
+                    if (c < objCost) { objCost = c; objAxis = axis; objBin = k; objL = la; objR = rB[k + 1]; }
+                }
+            }
+        }
+        // spatial split, when the object split's children overlap enough and the reference budget allows
+        float spCost = FLT_MAX; int spAxis = -1; float spPos = 0.f;
+        if (objAxis >= 0) {
+            Box3 ov; ov.lo = vmax(objL.lo, objR.lo); ov.hi = vmin(objL.hi, objR.hi);
+            if (!empty(ov) && ov.area() > alphaArea) {
+                std::vector<Box3> bb(NB); std::vector<int> enter(NB), leave(NB); std::vector<Box3> rB(NB); std::vector<int> rC(NB);
+                for (int axis = 0; axis < 3; axis++) {
+                    const float lo = comp(box.lo, axis), ex = comp(box.extent(), axis);
+                    if (ex <= 1e-12f) continue;
+                    const float w = ex / NB;
+                    std::fill(bb.begin(), bb.end(), Box3()); std::fill(enter.begin(), enter.end(), 0); std::fill(leave.begin(), leave.end(), 0);
+                    for (const SRef& r : refs) {
+                        int b0 = (int)((comp(r.box.lo, axis) - lo) / w), b1 = (int)((comp(r.box.hi, axis) - lo) / w);
+                        b0 = std::min(std::max(b0, 0), NB - 1); b1 = std::min(std::max(b1, b0), NB - 1);
+                        if (b0 == b1) bb[b0].grow(r.box);
+                        else for (int k = b0; k <= b1; k++) {
+                            const Box3 c = chop(r.tri, axis, k == b0 ? -FLT_MAX : lo + k * w, k == b1 ? FLT_MAX : lo + (k + 1) * w, r.box);
+                            if (!empty(c)) bb[k].grow(c);
+                        }
+                        enter[b0]++; leave[b1]++;
+                    }
+                    Box3 acc; int cnt = 0;
+                    for (int k = NB - 1; k > 0; k--) { acc.grow(bb[k]); cnt += leave[k]; rB[k] = acc; rC[k] = cnt; }
+                    Box3 la; int lc = 0;
+                    for (int k = 0; k < NB - 1; k++) {
+                        la.grow(bb[k]); lc += enter[k];
+                        if (lc == 0 || rC[k + 1] == 0 || lc + rC[k + 1] > n + budget * n) continue;
+                        const float c = la.area() * lc + rB[k + 1].area() * rC[k + 1];
+                        if (c < spCost) { spCost = c; spAxis = axis; spPos = lo + (k + 1) * w; }
+                    }
+                }
+            }
+        }
+        std::vector<SRef> L, R;
+        if (spAxis >= 0 && spCost < objCost) {
+            for (const SRef& r : refs) {
+                if (comp(r.box.hi, spAxis) <= spPos) L.push_back(r);
+                else if (comp(r.box.lo, spAxis) >= spPos) R.push_back(r);
+                else {
+                    const Box3 a = chop(r.tri, spAxis, -FLT_MAX, spPos, r.box), b = chop(r.tri, spAxis, spPos, FLT_MAX, r.box);
+                    const bool ea = empty(a), eb = empty(b);
+                    if (!ea) L.push_back({ r.tri, a });
+                    if (!eb) R.push_back({ r.tri, b });
+                    if (ea && eb) L.push_back(r);
+                }
+            }
+            if (L.empty() || R.empty()) { L.clear(); R.clear(); spAxis = -1; }
+        }
+        if (L.empty() && R.empty()) {
+            if (objAxis < 0) {   // coincident centroids: halves of the current order
+                L.assign(refs.begin(), refs.begin() + n / 2); R.assign(refs.begin() + n / 2, refs.end());
+            } else {
+                const float lo = comp(cb.lo, objAxis), scale = NB / comp(cb.extent(), objAxis);
+                for (const SRef& r : refs) {
+                    int k = (int)((comp((r.box.lo + r.box.hi) * 0.5f, objAxis) - lo) * scale); k = k < 0 ? 0 : k > NB - 1 ? NB - 1 : k;
+                    (k <= objBin ? L : R).push_back(r);
+                }
+                if (L.empty() || R.empty()) { L.assign(refs.begin(), refs.begin() + n / 2); R.assign(refs.begin() + n / 2, refs.end()); }
+            }
+        }
+        std::vector<SRef>().swap(refs);
+        if (spawn > 0 && n >= (1 << 12)) {
+            Part PL, PR;
+            auto right = std::async(std::launch::async, [&] { node(R, depth + 1, PR, spawn - 1); });
+            node(L, depth + 1, PL, spawn - 1);
+            right.get();
+            const int lb = splice(P, PL), rb = splice(P, PR);
+            P.nodes[id].left = lb; P.nodes[id].right = rb;
+        } else {
+            const int l = node(L, depth + 1, P, 0);
+            const int r = node(R, depth + 1, P, 0);
+            P.nodes[id].left = l; P.nodes[id].right = r;
+        }
+        return id;
+    }
+    static int splice(Part& P, const Part& S) {
+        const int base = (int)P.nodes.size(), pbase = (int)P.prim.size();
+        for (BNode b : S.nodes) { if (b.leaf()) b.first += pbase; else if (b.left >= 0) { b.left += base; b.right += base; } P.nodes.push_back(b); }
+        P.prim.insert(P.prim.end(), S.prim.begin(), S.prim.end());
+        P.maxDepth = std::max(P.maxDepth, S.maxDepth);
+        return base;
+    }
+};
+}  // namespace
+
+void build_sbvh(const Mesh& m, const SahOptions& o, float alpha, float budget, BinaryBvh& out) {
+    SbvhRun R(m, o);
+    const size_t n = m.nt();
+    std::vector<SRef> refs(n);
+    Box3 root;
+    for (size_t i = 0; i < n; i++) {
+        Box3 b; b.grow(m.vert(m.f[3 * i])); b.grow(m.vert(m.f[3 * i + 1])); b.grow(m.vert(m.f[3 * i + 2]));
+        refs[i] = { (int)i, b }; root.grow(b);
+    }
+    R.alphaArea = alpha * root.area(); R.budget = budget;
+    const int threads = o.threads > 0 ? o.threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    int spawn = 0; while ((1 << spawn) < threads * 4 && spawn < 12) spawn++;
+    if (threads <= 1) spawn = 0;
+    SbvhRun::Part P;
+    R.node(refs, 0, P, spawn);
+    out.nodes.swap(P.nodes); out.prim.swap(P.prim); out.maxDepth = P.maxDepth; out.leafMax = o.leafMax;
+}
+
 double sah_cost(const BinaryBvh& B, double cNode, double cPrim) {
     double s = 0, a0 = B.nodes[0].box.area();
     if (!(a0 > 0)) return 0;

@@ -47,6 +47,11 @@ struct SahOptions {
 // pre-order at the end, so the output is identical for any thread count and, at 16 bins, to the reference builder.
 void build_sah(const Mesh& m, const SahOptions& o, BinaryBvh& out);
 
+// Binned SAH with spatial splits (SBVH): prim then holds triangle references, a triangle possibly in several leaves.
+// alpha: relative overlap area above which a node tries spatial splits (1e-5 typical); budget: cap on the extra
+// references as a fraction of the triangle count. Parallel subtrees; the result does not depend on the thread count.
+void build_sbvh(const Mesh& m, const SahOptions& o, float alpha, float budget, BinaryBvh& out);
+
 // SAH cost normalised by the root area: internal nodes cost cNode, leaves cPrim per triangle (bvh_tools.cpp:40-44).
 double sah_cost(const BinaryBvh& B, double cNode, double cPrim);
 

@@ -238,6 +238,8 @@ struct cwp_server {
     cudaStream_t st = nullptr;
     std::chrono::steady_clock::time_point t0;
     std::vector<void*> allocs;
+    cudaEvent_t ev[6] = {};   // raygen start, closest start, shade start, shadow start, shadow end, (spare)
+    cwp_server_info info{};
 };
 
 static double now_ms(const cwp_server* s) { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s->t0).count(); }
@@ -251,6 +253,7 @@ extern "C" void cwp_server_destroy(cwp_server* s) {
     for (auto& kv : s->reqs) if (kv.second.accum) cudaFree(kv.second.accum);
     for (void* p : s->allocs) cudaFree(p);
     if (s->hcnt) cudaFreeHost(s->hcnt);
+    for (cudaEvent_t e : s->ev) if (e) cudaEventDestroy(e);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;
 }
@@ -270,6 +273,7 @@ static int server_create(cwp_batch* b, const cwp_material* mats, int n, const in
                                            mats[i].transmission >= 0.f && mats[i].transmission <= 1.f, CWP_ERR_INVALID, "material %d out of range", i);
     CWPB_CUDA(cudaSetDevice(s->device));
     CWPB_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : s->ev) CWPB_CUDA(cudaEventCreate(&e));
     auto alloc = [&](void** p, size_t bytes) -> int { CWPB_CUDA(cudaMalloc(p, bytes)); s->allocs.push_back(*p); return CWP_OK; };
     const size_t P = (size_t)s->O.max_paths, R = (size_t)s->O.max_requests;
     int rc = alloc((void**)&s->mats, (size_t)n * sizeof(cwp_material));
@@ -366,7 +370,7 @@ static int admit(cwp_server* s, bool& changed) {
             if (int rc = cwp_instance_from_xform(m, s->desc[i].mesh, &rec)) return rc;
             v.push_back(rec);
         }
-        q.slot = slot; q.admitMs = now_ms(s);
+        q.slot = slot; q.admitMs = now_ms(s); s->info.admissions++;
         s->slotReq[slot] = q.id; s->hSlotCnt[kSlotCounters * slot + 2] = 0;
         s->pending.pop_front();
         changed = true;
@@ -377,9 +381,15 @@ static int admit(cwp_server* s, bool& changed) {
 extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPending) {
     CWPB_CHECK(s, CWP_ERR_INVALID, "server is NULL");
     CWPB_CUDA(cudaSetDevice(s->device));
+    const double stepStart = now_ms(s);
     bool changed = false;
     if (int rc = admit(s, changed)) return rc;
-    if (changed) { CWPB_CUDA(cudaStreamSynchronize(s->st)); if (int rc = rebuild_tlas(s)) return rc; }
+    if (changed) {
+        CWPB_CUDA(cudaStreamSynchronize(s->st));
+        const double t = now_ms(s);
+        if (int rc = rebuild_tlas(s)) return rc;
+        s->info.tlas_ms += now_ms(s) - t; s->info.tlas_rebuilds++;
+    }
     // new camera paths: free capacity shared evenly by the slots with samples left to issue, oldest first
     const int R = s->O.max_requests;
     std::vector<int> needy;
@@ -396,6 +406,7 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         q.issued += take; added += take; freeCap -= take;
     }
     RayQueue& in = s->q[s->cur]; RayQueue& out = s->q[s->cur ^ 1];
+    CWPB_CUDA(cudaEventRecord(s->ev[0], s->st));
     if (added > 0) {
         CWPB_CUDA(cudaMemcpyAsync(s->dChunks, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice, s->st));
         k_serve_raygen<<<(unsigned)((added + 255) / 256), 256, 0, s->st>>>(s->dChunks, (int)chunks.size(), (int)added, s->dSlots, in, (int)s->nCur);
@@ -403,8 +414,12 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
     }
     const int64_t n = s->nCur + added;
     int64_t nNext = 0, nShadow = 0;
+    CWPB_CUDA(cudaEventRecord(s->ev[1], s->st));
+    CWPB_CUDA(cudaEventRecord(s->ev[2], s->st));
+    CWPB_CUDA(cudaEventRecord(s->ev[3], s->st));
     if (n > 0) {
         if (int rc = batch_trace_dev(s->batch, false, in.o, in.d, in.sc, s->hits, s->hinst, n, s->st)) return rc;
+        CWPB_CUDA(cudaEventRecord(s->ev[2], s->st));
         CWPB_CUDA(cudaMemsetAsync(s->cnt, 0, 4 * sizeof(int), s->st));
         ShadeArgs a{};
         a.n = (int)n; a.in = in; a.out = out; a.sq = s->sq; a.hits = s->hits; a.hinst = s->hinst; a.inst = batch_instances(s->batch); a.tris = batch_tris(s->batch);
@@ -412,6 +427,7 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         const unsigned g = (unsigned)std::min<int64_t>((n + 127) / 128, 148 * 16);
         k_serve_shade<<<g, 128, 0, s->st>>>(a);
         CWPB_CUDA(cudaGetLastError());
+        CWPB_CUDA(cudaEventRecord(s->ev[3], s->st));
         CWPB_CUDA(cudaMemcpyAsync(s->hcnt, s->cnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
         CWPB_CUDA(cudaStreamSynchronize(s->st));
         nNext = s->hcnt[0]; nShadow = s->hcnt[1];
@@ -421,9 +437,17 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
             CWPB_CUDA(cudaGetLastError());
         }
     }
+    CWPB_CUDA(cudaEventRecord(s->ev[4], s->st));
     CWPB_CUDA(cudaMemcpyAsync(s->hcnt + 4, s->slotCnt, (size_t)R * kSlotCounters * sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CWPB_CUDA(cudaStreamSynchronize(s->st));
-    if (int rc = cwp_batch_status(s->batch)) return rc;
+    {
+        float a = 0, b = 0, c = 0, d = 0;
+        CWPB_CUDA(cudaEventElapsedTime(&a, s->ev[0], s->ev[1])); CWPB_CUDA(cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
+        CWPB_CUDA(cudaEventElapsedTime(&c, s->ev[2], s->ev[3])); CWPB_CUDA(cudaEventElapsedTime(&d, s->ev[3], s->ev[4]));
+        s->info.raygen_ms += a; s->info.closest_ms += b; s->info.shade_ms += c; s->info.shadow_ms += d;
+        s->info.steps++; s->info.rays += n; s->info.shadow_rays += nShadow;
+    }
+    if ((s->info.steps & 63) == 0 || nNext == 0) { if (int rc = cwp_batch_status(s->batch)) return rc; }   // traversal bounds: checked every 64 steps and when the queue drains
     s->cur ^= 1; s->nCur = nNext;
     // completion
     const double t = now_ms(s);
@@ -436,6 +460,7 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
             q.done = true; q.doneMs = t; s->completed.push_back(q.id); s->slotReq[k] = -1; q.slot = -1;
         }
     }
+    s->info.step_ms += now_ms(s) - stepStart;
     if (nActive) { int a = 0; for (int k = 0; k < R; k++) a += s->slotReq[k] >= 0; *nActive = a; }
     if (nPending) *nPending = (int)s->pending.size();
     return CWP_OK;
@@ -509,5 +534,11 @@ extern "C" int cwp_bsdf_sample_batch(const cwp_material* mats, int32_t nm, const
     if (e == cudaSuccess) e = cudaMemcpy(ok, dok, n * 4, cudaMemcpyDeviceToHost);
     cudaFree(dm); cudaFree(dmat); cudaFree(dwo); cudaFree(deta); cudaFree(dux); cudaFree(duvw); cudaFree(dwi); cudaFree(dw); cudaFree(dpdf); cudaFree(dok);
     CWPB_CUDA(e);
+    return CWP_OK;
+}
+
+extern "C" int cwp_server_info_of(const cwp_server* s, cwp_server_info* out) {
+    CWPB_CHECK(s && out, CWP_ERR_INVALID, "NULL argument");
+    *out = s->info;
     return CWP_OK;
 }

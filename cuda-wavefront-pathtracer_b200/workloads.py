@@ -31,12 +31,12 @@ __all__ = ["SCENES", "scene", "frame_params", "scene_extent", "camera_rays", "in
            "batch_scenes", "batch_rays", "serving_scenes", "serving_requests", "RESOLUTIONS", "SPPS", "HFOV", "SEED", "SUN_TO", "SUN_E", "SUN_ANGLE_RAD", "SKY", "ALBEDO"]
 
 
-def scene(name_or_boxes, variant=8, bins=32, leaf=4, collapse=0, threads=0):
+def scene(name_or_boxes, variant=8, bins=32, leaf=4, collapse=0, threads=0, spatial=0.0):
     """(mesh, bvh) of a box-field scene; bvh.albedo is set to the benchmark albedo."""
     from . import Bvh, Mesh
     n = SCENES.get(name_or_boxes, name_or_boxes)
     mesh = Mesh.box_field(int(n), SCENE_SEED)
-    bvh = Bvh(mesh, variant=variant, bins=bins, leaf=leaf, collapse=collapse, threads=threads)
+    bvh = Bvh(mesh, variant=variant, bins=bins, leaf=leaf, collapse=collapse, threads=threads, spatial=spatial)
     bvh.albedo = np.full((1, 3), ALBEDO, np.float32)
     return mesh, bvh
 

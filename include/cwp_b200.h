@@ -66,6 +66,9 @@ typedef struct cwp_build_options {
     int32_t leaf;       /* max triangles per leaf (reference --leaf, default 4; CWBVH SAH collapse builds from leaf 1) */
     int32_t collapse;   /* CWBVH: 0 SAH dynamic programme, 1 greedy */
     int32_t threads;    /* host threads, 0 = all */
+    float spatial;      /* > 0: spatial splits (SBVH) where the object split's children overlap by more than this
+                           fraction of the root's area (1e-5 typical); a spatial split may add at most 30% references
+                           to a node. 0: the reference's binned SAH (byte-identical buffers at 16 bins) */
 } cwp_build_options;
 
 typedef struct cwp_bvh cwp_bvh;
@@ -349,6 +352,11 @@ int cwp_server_poll(cwp_server* s, int64_t* ids, int32_t cap, int32_t* n);
  * request's device memory is released. */
 int cwp_server_result(cwp_server* s, int64_t id, float* accum, cwp_request_stats* st);
 double cwp_server_clock_ms(const cwp_server* s);
+typedef struct cwp_server_info {
+    int64_t steps, rays, shadow_rays, admissions, tlas_rebuilds;
+    double closest_ms, shade_ms, shadow_ms, raygen_ms, tlas_ms, step_ms;   /* device time per phase (CUDA events), wall time of the steps */
+} cwp_server_info;
+int cwp_server_info_of(const cwp_server* s, cwp_server_info* out);
 /* Device-side BSDF of a material table for n (material, wo, wi) triples in local frames (wo.z > 0): f (float4) and
  * pdf; and n samples (u, u1, u2 in uvw) -> wi, weight, pdf. For tests of the device arithmetic. */
 int cwp_bsdf_eval_batch(const cwp_material* mats, int32_t n_mats, const int32_t* mat, const float* wo, const float* wi, const float* eta,

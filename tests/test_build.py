@@ -105,3 +105,30 @@ def test_invalid_inputs(cwp):
         with pytest.raises(cwp.CwpError) as e:
             cwp.Bvh(mesh, **kw)
         assert e.value.code == cwp.ERR_INVALID
+
+
+@pytest.mark.parametrize("variant", [2, 4, 8])
+def test_spatial_splits_same_hits_fewer_visits(cwp, oracle, variant):
+    """SBVH (spatial splits): every triangle is referenced, the tree does not depend on the thread count, and the
+    oracle traversal finds the same closest triangle (original id) at the same distance as over the binned-SAH tree,
+    visiting fewer nodes."""
+    mesh = cwp.Mesh.box_field(600, 1)
+    leaf = 1 if variant == 8 else 4
+    b0 = cwp.Bvh(mesh, variant=variant, bins=32, leaf=leaf)
+    b1 = cwp.Bvh(mesh, variant=variant, bins=32, leaf=leaf, spatial=1e-5)
+    b1s = cwp.Bvh(mesh, variant=variant, bins=32, leaf=leaf, spatial=1e-5, threads=1)
+    assert np.array_equal(b1.nodes.view(np.uint32), b1s.nodes.view(np.uint32)) and np.array_equal(b1.order, b1s.order)
+    assert set(b1.order.tolist()) == set(range(mesh.n_tris)) and len(b1.order) > mesh.n_tris
+    p = cwp.frame_params(mesh, 128, 128)
+    o, d = cwp.incoherent_rays(4000, p, b0.tris, lambda o, d: oracle.trace(variant, 1, False, b0.nodes, b0.woop, o, d), seed=2)
+    h0, s0 = oracle.trace(variant, 1, False, b0.nodes, b0.woop, o, d, stats=True)
+    h1, s1 = oracle.trace(variant, 1, False, b1.nodes, b1.woop, o, d, stats=True)
+    i0, i1 = h0[:, 3].view(np.int32), h1[:, 3].view(np.int32)
+    id0 = np.where(i0 >= 0, b0.tris[3 * np.maximum(i0, 0), 3].view(np.int32), -1)
+    id1 = np.where(i1 >= 0, b1.tris[3 * np.maximum(i1, 0), 3].view(np.int32), -1)
+    same = id0 == id1
+    tie = ~same & (i0 >= 0) & (i1 >= 0) & (np.abs(h0[:, 0] - h1[:, 0]) <= 1e-6 * np.abs(h0[:, 0]))
+    assert np.all(same | tie) and np.array_equal(h0[same, 0], h1[same, 0])
+    assert s1[0] < s0[0]
+    occ0 = oracle.trace(variant, 1, True, b0.nodes, b0.woop, o, d); occ1 = oracle.trace(variant, 1, True, b1.nodes, b1.woop, o, d)
+    assert np.array_equal(occ0 >= 0, occ1 >= 0)
