@@ -413,7 +413,7 @@ def main():
     ap.add_argument("--scenes", type=int, default=0, help="override the scene count of batched64 (profiling cases)")
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
-    ap.add_argument("--spatial", type=float, default=0.0, help="host BVH: spatial-split overlap threshold (0 = binned SAH only, 1e-5 = SBVH)")
+    ap.add_argument("--spatial", type=float, default=1e-5, help="host BVH: spatial-split overlap threshold (1e-5 = SBVH, the default; 0 = the reference's binned SAH only)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
