@@ -41,7 +41,8 @@ WORKLOADS = {
     "frame256": dict(scene="boxes12k", w=256, h=256, spp=16, batch=16, bounces=4),
     "trace16m": dict(scene="boxes117k", rays=1 << 24),
     "precision1m": dict(scene="boxes12k", rays=1 << 20, precision=True),
-    "serving": dict(serving=True, scenes=32, requests=64, rate=100.0, max_paths=16 << 20, max_requests=64, seed=7),
+    "serving": dict(serving=True, scenes=32, requests=48, rate=100.0, small_requests=400, small_rate=400.0, max_paths=16 << 20, max_requests=64, seed=7,
+                    builder=1),
     "batched64": dict(batched=True, scenes=64, rays_per_scene=4 << 20, tris=(1000, 500000), instances=(1, 4096), blas=(1, 8), seed=5),
 }
 STATE_BYTES = 40          # path state per queued ray: (o, id) + (d, T.r) + (T.g, T.b); shadow entries the same size
@@ -267,7 +268,7 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
     t0 = time.perf_counter()
     meshes, xf, mesh_of, first = batched_setup(cwp, wl)
     gen_s = time.perf_counter() - t0
-    b = cwp.Batch(meshes, device=torch.cuda.current_device())
+    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=args.builder)
     inst = cwp.instances(xf, mesh_of)
     b.set_scenes(inst, first)
     info = b.info()
@@ -323,7 +324,8 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
                config={"workload": args.workload, "scenes": n_s, "blas": info.n_blas, "tris": int(info.n_tris), "instances": int(info.n_instances),
                        "rays": n, "rays_per_scene": per, "hit_rate": hit_rate,
                        "tuning": {"block": tun.block, "width": tun.width, "fetch": tun.fetch, "smem_stack": tun.smem_stack, "sample_ms": tun.ms},
-                       "autotune_s": tune_s, "blas_build_ms": info.blas_build_ms, "blas_hploc_launches": info.blas_hploc_launches,
+                       "autotune_s": tune_s, "blas_builder": ["gpu h-ploc (one launch)", "host binned SAH"][args.builder], "blas_build_ms": info.blas_build_ms,
+                       "blas_hploc_launches": info.blas_hploc_launches if args.builder == 0 else 0,
                        "tlas_build_ms": info.tlas_build_ms, "node_bytes": {"bvh2": int(info.node_bytes[0]), "bvh4": int(info.node_bytes[1]), "cwbvh": int(info.node_bytes[2])},
                        "scene_generation_s": gen_s, "l2": f"ray queue {n * 36 / 1e9:.1f} GB > L2 (126 MB)",
                        "closest_ms": c_ms / args.steps, "any_ms": a_ms / args.steps, "tri": "moller-trumbore"},
@@ -363,35 +365,45 @@ def serve_stream(cwp, s, stream):
 
 
 def bench_serving(args, wl, cwp, torch, out):
+    """Two request streams, each served by continuous batching and by the plain form (one request at a time, the same
+    kernels): `mix` draws config 5's distribution (256^2..1080p, 1..256 spp), where single large requests already
+    fill the GPU; `small` draws 256^2 / 512^2 at 1 / 4 spp, where one request alone leaves the GPU mostly idle."""
     import numpy as np
     t0 = time.perf_counter()
     meshes, descs, first, mats, base, boxes = cwp.serving_scenes(n_scenes=wl["scenes"], seed=wl["seed"])
-    b = cwp.Batch(meshes, device=torch.cuda.current_device())
+    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=wl["builder"])
     gen_s = time.perf_counter() - t0
     n_req = args.rays if args.rays else wl["requests"]
-    stream = cwp.serving_requests(n_req, wl["rate"], boxes, seed=wl["seed"] + 1)
+    streams = {"mix": cwp.serving_requests(n_req, wl["rate"], boxes, seed=wl["seed"] + 1),
+               "small": cwp.serving_requests(wl["small_requests"], wl["small_rate"], boxes, seed=wl["seed"] + 2, resolutions=[(256, 256), (512, 512)], spps=[1, 4])}
     res = {}
-    for mode, maxr in (("continuous", wl["max_requests"]), ("plain", 1)):
-        s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=maxr)
-        s.set_scenes(descs, first)
-        clk = Clocks(str(torch.cuda.current_device()))
-        res[mode] = serve_stream(cwp, s, stream)
-        res[mode]["clocks"] = clk.stop()
-        res[mode]["breakdown"] = s.info()
-        del s
-    c, p = res["continuous"], res["plain"]
+    for name, stream in streams.items():
+        for mode, maxr in (("continuous", wl["max_requests"]), ("plain", 1)):
+            s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=maxr)
+            s.set_scenes(descs, first)
+            clk = Clocks(str(torch.cuda.current_device()))
+            r = serve_stream(cwp, s, stream)
+            r["clocks"] = clk.stop(); r["breakdown"] = s.info()
+            res[(name, mode)] = r
+            del s
     info = b.info()
-    out.update(metric="serving request throughput (continuous batching), Poisson stream", value=c["throughput_req_s"], unit="req/s",
+    c, p = res[("mix", "continuous")], res[("mix", "plain")]
+    cs, ps = res[("small", "continuous")], res[("small", "plain")]
+    strip = lambda r: {k: v for k, v in r.items() if k != "clocks"}
+    out.update(metric="serving request throughput (continuous batching), Poisson stream of config-5 requests", value=c["throughput_req_s"], unit="req/s",
                ms_per_step=1e3 / c["throughput_req_s"], higher_is_better=True, dtype="f32",
-               config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "requests": n_req,
-                       "arrival_rate_req_s": wl["rate"], "resolutions": "256^2, 512^2, 1280x720, 1920x1080", "spp": "1, 4, 16, 64, 256", "depth": 8,
-                       "materials": "OpenPBR subset: roughness U[0.05,1], metallic Bernoulli(0.3), 10% glass IOR 1.5", "max_paths": wl["max_paths"],
-                       "max_requests": wl["max_requests"], "continuous": {k: v for k, v in c.items() if k != "clocks"},
-                       "plain": {k: v for k, v in p.items() if k != "clocks"}, "throughput_vs_plain": c["throughput_req_s"] / p["throughput_req_s"],
-                       "p99_vs_plain": c["p99_ms"] / p["p99_ms"], "scene_generation_s": gen_s, "blas_build_ms": info.blas_build_ms},
+               config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "blas_builder": ["gpu h-ploc", "host binned SAH"][wl["builder"]],
+                       "blas_build_ms": info.blas_build_ms, "scene_generation_s": gen_s, "depth": 8, "max_paths": wl["max_paths"], "max_requests": wl["max_requests"],
+                       "materials": "OpenPBR subset: roughness U[0.05,1], metallic Bernoulli(0.3), 10% glass IOR 1.5",
+                       "mix": {"requests": n_req, "arrival_rate_req_s": wl["rate"], "resolutions": "256^2, 512^2, 1280x720, 1920x1080", "spp": "1, 4, 16, 64, 256",
+                               "continuous": strip(c), "plain": strip(p), "throughput_vs_plain": c["throughput_req_s"] / p["throughput_req_s"],
+                               "p99_vs_plain": c["p99_ms"] / p["p99_ms"], "p50_vs_plain": c["p50_ms"] / p["p50_ms"]},
+                       "small": {"requests": wl["small_requests"], "arrival_rate_req_s": wl["small_rate"], "resolutions": "256^2, 512^2", "spp": "1, 4",
+                                 "continuous": strip(cs), "plain": strip(ps), "throughput_vs_plain": cs["throughput_req_s"] / ps["throughput_req_s"],
+                                 "p99_vs_plain": cs["p99_ms"] / ps["p99_ms"], "p50_vs_plain": cs["p50_ms"] / ps["p50_ms"]}},
                clocks=c["clocks"],
                e2e={"value": c["throughput_req_s"], "unit": "req/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
-                    "note": "requests enter through the C ABI with host descriptors; every image is copied back to host memory (cwp_server_result) inside the served span"},
+                    "note": "requests enter through the C ABI with host descriptors; images stay on the device until cwp_server_result"},
                gpu_launches=None)
 
 
@@ -411,6 +423,7 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="override the frame's samples per pixel (profiling cases)")
     ap.add_argument("--rays", type=int, default=0, help="override the batch size of trace16m / rays per scene of batched64 (profiling cases)")
     ap.add_argument("--scenes", type=int, default=0, help="override the scene count of batched64 (profiling cases)")
+    ap.add_argument("--builder", type=int, default=0, help="batched64: 0 every BLAS on the GPU (H-PLOC, one launch), 1 on the host cores (binned SAH)")
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     ap.add_argument("--spatial", type=float, default=1e-5, help="host BVH: spatial-split overlap threshold (1e-5 = SBVH, the default; 0 = the reference's binned SAH only)")
@@ -619,10 +632,12 @@ def main():
                              "algorithmic": "closest: 32 B ray in + 16 B hit out; any: 32 B in + 4 B out"})
         acc.close()
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and not wl.get("batched") and not wl.get("serving"):
+        # the reference's own host build (binned SAH, 16 bins: byte-identical to its BVHBuilder) under its own code
+        _, rbvh = cwp.scene(wl["scene"], variant=variant, bins=16)
         if "rays" not in wl:
-            out["cpu_baseline"] = cpu_frame_sample(cwp, wl, mesh, bvh, variant)
+            out["cpu_baseline"] = cpu_frame_sample(cwp, wl, mesh, rbvh, variant)
         else:
-            out["cpu_baseline"] = cpu_trace_sample(cwp, bvh, variant, o, d)
+            out["cpu_baseline"] = cpu_trace_sample(cwp, rbvh, variant, o, d)
     if ws > 1:
         tdist.barrier()
         tdist.destroy_process_group()

@@ -88,7 +88,7 @@ class InstanceDesc(C.Structure):
 
 
 class BatchOptions(C.Structure):
-    _fields_ = [("device", C.c_int32), ("leaf", C.c_int32), ("widths", C.c_int32), ("reserved", C.c_int32 * 5)]
+    _fields_ = [("device", C.c_int32), ("leaf", C.c_int32), ("widths", C.c_int32), ("builder", C.c_int32), ("spatial", C.c_float), ("reserved", C.c_int32 * 3)]
 
 
 class BatchTuning(C.Structure):
@@ -476,7 +476,7 @@ class Batch:
     """Batched form: many meshes built on the GPU at once (segmented H-PLOC, BVH2 / BVH4 / CWBVH encodings), many
     two-level scenes, one persistent launch over a scene-tagged ray queue, and the launch-shape autotuner."""
 
-    def __init__(self, meshes, device=0, leaf=4, widths=0):
+    def __init__(self, meshes, device=0, leaf=4, widths=0, builder=0, spatial=0.0):
         arrs, views = [], (MeshView * len(meshes))()
         for i, m in enumerate(meshes):
             v, f, fm, _ = m.arrays() if isinstance(m, Mesh) else m
@@ -484,7 +484,7 @@ class Batch:
             fm = np.ascontiguousarray(fm if fm is not None else np.zeros(len(f)), np.int32)
             arrs += [v, f, fm]
             views[i].verts, views[i].n_verts, views[i].faces, views[i].n_tris, views[i].face_mat = _fptr(v), len(v), _iptr(f), len(f), _iptr(fm)
-        o = BatchOptions(device, leaf, widths)
+        o = BatchOptions(device, leaf, widths, builder, spatial)
         h = C.c_void_p()
         _check(lib().cwp_batch_create(views, len(meshes), C.byref(o), C.byref(h)))
         self._h = h

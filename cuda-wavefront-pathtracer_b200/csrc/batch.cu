@@ -3,13 +3,17 @@
 // (block size, BLAS width, fetch granularity, stack placement) is a runtime tuning that cwp_batch_autotune measures.
 #include "cwp_b200.h"
 #include "batch_internal.h"
+#include "host_bvh.h"
 #include "hploc.h"
 #include "runtime.h"
 #include "trav.cuh"
 #include "wide_emit.h"
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -23,9 +27,10 @@ static constexpr int kBatchMaxBlock = 512;
 struct BatchArgs {
     const float4* nodes; const float4* tris;        // BLAS layout of the chosen width (absolute indices, MT records)
     const float4* tlas; const int* sceneRoot; const float4* inst;   // TLAS BVH2 nodes, root per scene, instances (7 float4)
+    const int* meshRoot;                                              // BLAS root of each mesh in the traced layout
     int nScenes;
     const float4* ro; const float4* rd; const int* sceneOf;
-    float4* hits; int* hitInst; long long n;
+    float4* hits; int* hitInst; long long n; const int* nDev;   // nDev: ray count on the device (overrides n), or null
     unsigned long long* cursor; int fetch; int* err;
 };
 
@@ -47,10 +52,10 @@ struct TwoLevel {
         return troot < 0;   // an empty scene: nothing to traverse
     }
     // enter instance k: ray into object space, BLAS traversal from the instance's root
-    __device__ __forceinline__ void enter(const float4* __restrict__ instances, int k) {
+    __device__ __forceinline__ void enter(const float4* __restrict__ instances, const int* __restrict__ meshRoot, int k) {
         const float4* I = instances + 7 * (size_t)k;
         const float4 r0 = ld4(I), r1 = ld4(I + 1), r2 = ld4(I + 2);
-        const int root = __float_as_int(ld4(I + 6).x);
+        const int root = __ldg(meshRoot + __float_as_int(ld4(I + 6).y));
         const float3 lo_ = f3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w, r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w, r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
         const float3 ld_ = f3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z, r2.x * d.x + r2.y * d.y + r2.z * d.z);
         blas.begin(lo_, ld_, tmin, hitT, root);
@@ -65,7 +70,7 @@ struct TwoLevel {
             if (ANY && hitTri >= 0) return true;
             if (tsp == 0) return true;
             next = tstack[--tsp];
-            if (next < 0) { enter(a.inst, ~next); return false; }
+            if (next < 0) { enter(a.inst, a.meshRoot, ~next); return false; }
             return false;
         }
         if (--budget < 0) { err |= kTravBudget; return true; }
@@ -87,7 +92,7 @@ struct TwoLevel {
             tstack[tsp++] = e1; go = e0;
         } else if (h0 || h1) go = h0 ? e0 : e1;
         else { if (tsp == 0) return true; go = tstack[--tsp]; }
-        if (go < 0) enter(a.inst, ~go); else next = go;
+        if (go < 0) enter(a.inst, a.meshRoot, ~go); else next = go;
         return false;
     }
 };
@@ -105,6 +110,7 @@ __global__ void __launch_bounds__(kBatchMaxBlock, 2) k_batch_trace(const BatchAr
     int e = 0;
     TwoLevel<V, ANY> ray;
     int tstack[kTlasStack];
+    const long long nRays = a.nDev ? (long long)*a.nDev : a.n;
     LocalStack lstack;
     SharedStack<Entry> sstack{ reinterpret_cast<Entry*>(smem) + threadIdx.x, (int)blockDim.x };
     long long k = -1; bool fin = false, drained = false;
@@ -124,14 +130,14 @@ __global__ void __launch_bounds__(kBatchMaxBlock, 2) k_batch_trace(const BatchAr
                 if (lane == leader) base = (long long)atomicAdd(a.cursor, (unsigned long long)__popc(nm));
                 base = __shfl_sync(0xffffffffu, base, leader);
                 const long long kk = base + __popc(nm & lane_mask_lt());
-                if (need && kk < a.n) {
+                if (need && kk < nRays) {
                     k = kk;
                     const float4 O = __ldcs(a.ro + k), D = __ldcs(a.rd + k);
                     const int sc = __ldcs(a.sceneOf + k);
                     const int root = sc >= 0 && sc < a.nScenes ? __ldg(a.sceneRoot + sc) : -1;
                     fin = ray.begin(xyz(O), xyz(D), O.w, D.w, root);
                 }
-                drained = __any_sync(0xffffffffu, need && kk >= a.n);
+                drained = __any_sync(0xffffffffu, need && kk >= nRays);
             }
         }
         if (!__any_sync(0xffffffffu, k >= 0)) break;
@@ -166,6 +172,8 @@ struct cwp_batch {
     float4* triV = nullptr;              // input triangles, 3 float4 each
     float4 *primLo = nullptr, *primHi = nullptr, *meshBox = nullptr;
     int* meshFirstDev = nullptr;
+    int* meshRoot[3] = { nullptr, nullptr, nullptr }; std::vector<int> meshRootHost[3];   // per layout width
+    int builder = 0;
     SegBuilder blasB, tlasB;
     WideLayout lay[3];                   // width 2, 4, 8
     // scenes
@@ -179,6 +187,7 @@ struct cwp_batch {
     int* err = nullptr; unsigned long long* cursor = nullptr;
     cudaStream_t st = nullptr; cudaEvent_t e0 = nullptr, e1 = nullptr;
     double blasMs = 0, tlasMs = 0; int nSm = 0;
+    int64_t refs[3] = { 0, 0, 0 };   // triangle records per layout (host build with spatial splits: more than nTris)
 };
 
 static int lay_index(int w) { return w == 2 ? 0 : w == 4 ? 1 : w == 8 ? 2 : -1; }
@@ -191,6 +200,7 @@ static void batch_free(cwp_batch* b) {
     cudaFree(b->triV); cudaFree(b->primLo); cudaFree(b->primHi); cudaFree(b->meshBox); cudaFree(b->meshFirstDev);
     cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas); cudaFree(b->sceneRoot); cudaFree(b->segFirstTlas);
     cudaFree(b->err); cudaFree(b->cursor);
+    for (int i = 0; i < 3; i++) cudaFree(b->meshRoot[i]);
     if (b->st) cudaStreamDestroy(b->st);
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
@@ -198,6 +208,78 @@ static void batch_free(cwp_batch* b) {
 }
 
 extern "C" void cwp_batch_destroy(cwp_batch* b) { batch_free(b); }
+
+// append a BVH4 array with indices relative to its own nodes and triangles
+static int append_bvh4(std::vector<float4>& all, const std::vector<float4>& blas, int triBase) {
+    const int base = (int)(all.size() / 8);
+    for (size_t i = 0; i < blas.size(); i += 8) {
+        float4 c = blas[i + 6]; const float4 k = blas[i + 7];
+        int* cc = reinterpret_cast<int*>(&c); const int* kk = reinterpret_cast<const int*>(&k);
+        for (int j = 0; j < 4; j++) { if (kk[j] > 0) cc[j] += triBase; else if (cc[j] >= 0) cc[j] += base; }
+        for (int j = 0; j < 6; j++) all.push_back(blas[i + j]);
+        all.push_back(c); all.push_back(k);
+    }
+    return base;
+}
+
+// Every BLAS built on the host cores (meshes in parallel, one thread each): binned SAH with 32 bins, spatial splits
+// when spatial > 0, BVH2 / BVH4 layouts from leaf-`leaf` trees and the SAH-collapsed CWBVH from a leaf-1 tree,
+// concatenated with absolute indices; per-layout mesh roots; Moller-Trumbore records in each layout's leaf order.
+static int host_build(cwp_batch* b, const cwp_mesh_view* meshes, int n, float spatial) {
+    CWPB_CHECK(spatial >= 0.f && spatial < 1.f, CWP_ERR_INVALID, "spatial %g out of [0, 1)", spatial);
+    struct Out { std::vector<float4> nodes[3], tris[3]; Box3 box; };
+    std::vector<Out> out(n);
+    auto build_one = [&](int m) {
+        const cwp_mesh_view& v = meshes[m];
+        Mesh M; M.v.assign(v.verts, v.verts + 3 * v.n_verts); M.f.assign(v.faces, v.faces + 3 * v.n_tris);
+        if (v.face_mat) M.fm.assign(v.face_mat, v.face_mat + v.n_tris); else M.fm.assign(v.n_tris, 0);
+        for (size_t i = 0; i < M.nv(); i++) out[m].box.grow(M.vert((int)i));
+        SahOptions so; so.bins = 32; so.threads = 1;
+        std::vector<float4> nrm;
+        if (b->widths & ((1 << 2) | (1 << 4))) {
+            so.leafMax = b->leaf; BinaryBvh B;
+            if (spatial > 0.f) build_sbvh(M, so, spatial, 0.3f, B); else build_sah(M, so, B);
+            if (b->widths & (1 << 2)) { BinaryBvh B2 = B; layout_bvh2(B2, out[m].nodes[0]); pack_tris(M, B2.prim, out[m].tris[0], nrm); }
+            if (b->widths & (1 << 4)) { BinaryBvh B4 = B; layout_bvh4(B4, out[m].nodes[1]); pack_tris(M, B4.prim, out[m].tris[1], nrm); }
+        }
+        if (b->widths & (1 << 8)) {
+            so.leafMax = 1; BinaryBvh B;
+            if (spatial > 0.f) build_sbvh(M, so, spatial, 0.3f, B); else build_sah(M, so, B);
+            WideBvh W; collapse_cwbvh(B, W);
+            out[m].nodes[2].swap(W.nodes); pack_tris(M, W.order, out[m].tris[2], nrm);
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    const int threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<int> next{ 0 };
+    std::vector<std::thread> ts;
+    for (int t = 0; t < std::min(threads, n); t++) ts.emplace_back([&] { for (int m; (m = next++) < n;) build_one(m); });
+    for (auto& t : ts) t.join();
+    std::vector<float4> box(2 * (size_t)n);
+    for (int m = 0; m < n; m++) { box[2 * m] = make_float4(out[m].box.lo.x, out[m].box.lo.y, out[m].box.lo.z, 0.f); box[2 * m + 1] = make_float4(out[m].box.hi.x, out[m].box.hi.y, out[m].box.hi.z, 0.f); }
+    CWPB_CUDA(cudaMemcpy(b->meshBox, box.data(), box.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    for (int w : { 2, 4, 8 }) {
+        if (!(b->widths & (1 << w))) continue;
+        const int li = lay_index(w);
+        std::vector<float4> nodes, tris; b->meshRootHost[li].resize(n);
+        for (int m = 0; m < n; m++) {
+            const int triBase = (int)(tris.size() / 3);
+            b->meshRootHost[li][m] = w == 2 ? append_bvh2(nodes, out[m].nodes[li], triBase) : w == 4 ? append_bvh4(nodes, out[m].nodes[li], triBase)
+                                                                                          : append_bvh8(nodes, out[m].nodes[li], triBase);
+            tris.insert(tris.end(), out[m].tris[li].begin(), out[m].tris[li].end());
+            std::vector<float4>().swap(out[m].nodes[li]); std::vector<float4>().swap(out[m].tris[li]);
+        }
+        WideLayout& L = b->lay[li];
+        L.width = w; L.nNodes = (int64_t)nodes.size() / L.stride(); L.capNodes = L.nNodes;
+        CWPB_CUDA(cudaMalloc(&L.nodes, nodes.size() * sizeof(float4)));
+        CWPB_CUDA(cudaMalloc(&L.tris, tris.size() * sizeof(float4)));
+        CWPB_CUDA(cudaMemcpy(L.nodes, nodes.data(), nodes.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        CWPB_CUDA(cudaMemcpy(L.tris, tris.data(), tris.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        b->refs[li] = (int64_t)tris.size() / 3;
+    }
+    b->blasMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return CWP_OK;
+}
 
 static int batch_create(const cwp_mesh_view* meshes, int32_t n, const cwp_batch_options* opt, cwp_batch* b) {
     b->device = opt ? opt->device : 0;
@@ -244,22 +326,39 @@ static int batch_create(const cwp_mesh_view* meshes, int32_t n, const cwp_batch_
     CWPB_CUDA(cudaMemcpyAsync(b->triV, soup.data(), soup.size() * sizeof(float4), cudaMemcpyHostToDevice, b->st));
     CWPB_CUDA(cudaMemcpyAsync(b->meshFirstDev, b->meshFirst.data(), (size_t)(n + 1) * sizeof(int), cudaMemcpyHostToDevice, b->st));
     b->blasB.device = b->device; b->tlasB.device = b->device;
-    if (int rc = b->blasB.reserve(b->nTris, n)) return rc;
-    CWPB_CUDA(cudaStreamSynchronize(b->st));
-    // the timed build: boxes, keys, sort, one H-PLOC launch, root boxes, layouts
-    CWPB_CUDA(cudaEventRecord(b->e0, b->st));
-    triangle_boxes(b->triV, b->nTris, b->primLo, b->primHi, b->st);
-    if (int rc = b->blasB.build(b->primLo, b->primHi, b->nTris, b->meshFirst.data(), n, b->st)) return rc;
-    root_boxes(b->blasB, b->meshFirstDev, n, b->meshBox, b->st);
-    for (int w : { 2, 4, 8 }) {
-        if (!(b->widths & (1 << w))) continue;
-        if (int rc = emit_wide(b->blasB, b->meshFirst.data(), n, b->triV, w, w == 8 ? std::min(b->leaf, 3) : b->leaf, b->lay[lay_index(w)], b->st)) return rc;
+    b->builder = opt ? opt->builder : 0;
+    CWPB_CHECK(b->builder == 0 || b->builder == 1, CWP_ERR_INVALID, "builder %d is not 0 (GPU) or 1 (host)", b->builder);
+    if (b->builder == 1) {
+        if (int rc = host_build(b, meshes, n, opt ? opt->spatial : 0.f)) return rc;
+    } else {
+        if (int rc = b->blasB.reserve(b->nTris, n)) return rc;
+        CWPB_CUDA(cudaStreamSynchronize(b->st));
+        // the timed build: boxes, keys, sort, one H-PLOC launch, root boxes, layouts
+        CWPB_CUDA(cudaEventRecord(b->e0, b->st));
+        triangle_boxes(b->triV, b->nTris, b->primLo, b->primHi, b->st);
+        if (int rc = b->blasB.build(b->primLo, b->primHi, b->nTris, b->meshFirst.data(), n, b->st)) return rc;
+        root_boxes(b->blasB, b->meshFirstDev, n, b->meshBox, b->st);
+        for (int w : { 2, 4, 8 }) {
+            if (!(b->widths & (1 << w))) continue;
+            if (int rc = emit_wide(b->blasB, b->meshFirst.data(), n, b->triV, w, w == 8 ? std::min(b->leaf, 3) : b->leaf, b->lay[lay_index(w)], b->st)) return rc;
+            b->meshRootHost[lay_index(w)].resize(n);
+            for (int m = 0; m < n; m++) b->meshRootHost[lay_index(w)][m] = m;   // mesh m's root is node m
+        }
+        CWPB_CUDA(cudaEventRecord(b->e1, b->st));
+        CWPB_CUDA(cudaEventSynchronize(b->e1));
+        float ms = 0; CWPB_CUDA(cudaEventElapsedTime(&ms, b->e0, b->e1)); b->blasMs = ms;
+        CWPB_CUDA(cudaGetLastError());
     }
-    CWPB_CUDA(cudaEventRecord(b->e1, b->st));
-    CWPB_CUDA(cudaEventSynchronize(b->e1));
-    float ms = 0; CWPB_CUDA(cudaEventElapsedTime(&ms, b->e0, b->e1)); b->blasMs = ms;
-    CWPB_CUDA(cudaGetLastError());
-    for (auto& l : b->lay) if (l.nodes) if (int rc = check_wide(l, b->nTris, b->err, b->st)) return rc;
+    for (int i = 0; i < 3; i++) {
+        if (b->meshRootHost[i].empty()) continue;
+        CWPB_CUDA(cudaMalloc(&b->meshRoot[i], (size_t)n * sizeof(int)));
+        CWPB_CUDA(cudaMemcpy(b->meshRoot[i], b->meshRootHost[i].data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    for (int i = 0; i < 3; i++) {
+        if (!b->lay[i].nodes) continue;
+        if (!b->refs[i]) b->refs[i] = b->nTris;
+        if (int rc = check_wide(b->lay[i], b->refs[i], b->err, b->st)) return rc;
+    }
     b->tuning.block = 128; b->tuning.width = (b->widths & (1 << 8)) ? 8 : (b->widths & (1 << 4)) ? 4 : 2; b->tuning.fetch = 12; b->tuning.smem_stack = 0; b->tuning.ms = 0;
     return CWP_OK;
 }
@@ -285,7 +384,7 @@ extern "C" int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int6
     for (int64_t i = 0; i < n; i++) {
         CWPB_CHECK(h[i].mesh >= 0 && h[i].mesh < b->nMesh, CWP_ERR_INVALID, "instance %lld: mesh %d out of range", (long long)i, h[i].mesh);
         for (int k = 0; k < 12; k++) CWPB_CHECK(std::isfinite(h[i].inv[k]) && std::isfinite(h[i].fwd[k]), CWP_ERR_INVALID, "instance %lld: non-finite transform", (long long)i);
-        h[i].root = h[i].mesh;   // mesh m's BLAS root is node m in every layout
+        h[i].root = h[i].mesh;   // informative only: the traversal looks the BLAS root up per layout (meshRoot)
     }
     // segments: the non-empty scenes (their instance ranges are contiguous and cover the array)
     std::vector<int> seg; seg.push_back(0);
@@ -332,13 +431,15 @@ extern "C" int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int6
     return CWP_OK;
 }
 
-static int launch(cwp_batch* b, const cwp_batch_tuning& t, bool any, const float* o, const float* d, const int* sc, float* hits, int* hinst, int64_t n, cudaStream_t st) {
+static int launch(cwp_batch* b, const cwp_batch_tuning& t, bool any, const float* o, const float* d, const int* sc, float* hits, int* hinst, int64_t n, cudaStream_t st,
+                  const int* nDev = nullptr) {
     const WideLayout& L = b->lay[lay_index(t.width)];
     CWPB_CHECK(L.nodes, CWP_ERR_STATE, "layout width %d was not emitted (cwp_batch_options.widths)", t.width);
     BatchArgs a;
     a.nodes = L.nodes; a.tris = L.tris; a.tlas = b->tlas; a.sceneRoot = b->sceneRoot; a.inst = reinterpret_cast<const float4*>(b->inst);
+    a.meshRoot = b->meshRoot[lay_index(t.width)];
     a.nScenes = b->nScenes; a.ro = (const float4*)o; a.rd = (const float4*)d; a.sceneOf = sc; a.hits = (float4*)hits; a.hitInst = hinst;
-    a.n = n; a.cursor = b->cursor; a.fetch = t.fetch; a.err = b->err;
+    a.n = n; a.nDev = nDev; a.cursor = b->cursor; a.fetch = t.fetch; a.err = b->err;
     BatchKernel k = pick_kernel(t.width, any, t.smem_stack != 0);
     const size_t sm = t.smem_stack ? smem_bytes(t.width, t.block) : 0;
     if (sm > 48 * 1024) CWPB_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -445,9 +546,10 @@ extern "C" int cwp_batch_download(const cwp_batch* b, int32_t width, float* node
     CWPB_CHECK(L.nodes, CWP_ERR_STATE, "layout width %d was not emitted", width);
     CWPB_CUDA(cudaSetDevice(b->device));
     if (nNodeF4) *nNodeF4 = L.nNodes * L.stride();
-    if (nTriF4) *nTriF4 = 3 * b->nTris;
+    const int64_t nr = b->refs[lay_index(width)] ? b->refs[lay_index(width)] : b->nTris;
+    if (nTriF4) *nTriF4 = 3 * nr;
     if (nodes) CWPB_CUDA(cudaMemcpy(nodes, L.nodes, (size_t)L.nNodes * L.stride() * sizeof(float4), cudaMemcpyDeviceToHost));
-    if (tris) CWPB_CUDA(cudaMemcpy(tris, L.tris, (size_t)3 * b->nTris * sizeof(float4), cudaMemcpyDeviceToHost));
+    if (tris) CWPB_CUDA(cudaMemcpy(tris, L.tris, (size_t)3 * nr * sizeof(float4), cudaMemcpyDeviceToHost));
     return CWP_OK;
 }
 
@@ -455,7 +557,7 @@ extern "C" int cwp_batch_blas_root(const cwp_batch* b, int32_t width, int32_t me
     CWPB_CHECK(b && root, CWP_ERR_INVALID, "NULL argument");
     CWPB_CHECK(lay_index(width) >= 0 && b->lay[lay_index(width)].nodes, CWP_ERR_STATE, "layout width %d was not emitted", width);
     CWPB_CHECK(mesh >= 0 && mesh < b->nMesh, CWP_ERR_INVALID, "mesh %d out of range", mesh);
-    *root = mesh;
+    *root = b->meshRootHost[lay_index(width)][mesh];
     return CWP_OK;
 }
 
@@ -466,15 +568,19 @@ extern "C" int cwp_batch_download_tlas(const cwp_batch* b, float* nodes, int64_t
     if (nNodeF4) *nNodeF4 = 4 * b->nInst;
     if (nodes && b->nInst) CWPB_CUDA(cudaMemcpy(nodes, b->tlas, (size_t)4 * b->nInst * sizeof(float4), cudaMemcpyDeviceToHost));
     if (roots) CWPB_CUDA(cudaMemcpy(roots, b->sceneRoot, (size_t)b->nScenes * sizeof(int), cudaMemcpyDeviceToHost));
-    if (inst && b->nInst) CWPB_CUDA(cudaMemcpy(inst, b->inst, (size_t)b->nInst * sizeof(cwp_instance), cudaMemcpyDeviceToHost));
+    if (inst && b->nInst) {
+        CWPB_CUDA(cudaMemcpy(inst, b->inst, (size_t)b->nInst * sizeof(cwp_instance), cudaMemcpyDeviceToHost));
+        const std::vector<int>& R = b->meshRootHost[lay_index(b->tuning.width)];
+        for (int64_t i = 0; i < b->nInst; i++) inst[i].root = R[inst[i].mesh];   // roots of the layout the tuning traces
+    }
     return CWP_OK;
 }
 
 namespace cwpb {
-int batch_trace_dev(cwp_batch* b, bool any, const float4* o, const float4* d, const int* sc, float4* hits, int* inst, int64_t n, cudaStream_t st) {
+int batch_trace_dev(cwp_batch* b, bool any, const float4* o, const float4* d, const int* sc, float4* hits, int* inst, int64_t n, cudaStream_t st, const int* nDev) {
     CWPB_CHECK(b->nScenes > 0, CWP_ERR_STATE, "no scenes");
-    if (n <= 0) return CWP_OK;
-    return launch(b, b->tuning, any, (const float*)o, (const float*)d, sc, (float*)hits, inst, n, st);
+    if (n <= 0 && !nDev) return CWP_OK;
+    return launch(b, b->tuning, any, (const float*)o, (const float*)d, sc, (float*)hits, inst, n, st, nDev);
 }
 const float4* batch_tris(const cwp_batch* b) { return b->lay[lay_index(b->tuning.width)].tris; }
 const cwp_instance* batch_instances(const cwp_batch* b) { return b->inst; }

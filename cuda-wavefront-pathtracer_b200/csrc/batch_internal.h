@@ -5,7 +5,10 @@
 #include <cuda_runtime.h>
 
 namespace cwpb {
-int batch_trace_dev(cwp_batch* b, bool any, const float4* o, const float4* d, const int* sc, float4* hits, int* inst, int64_t n, cudaStream_t st);
+// nDev: the ray count read on the device at launch (n is then ignored), so a count produced by an earlier kernel needs no
+// host round trip
+int batch_trace_dev(cwp_batch* b, bool any, const float4* o, const float4* d, const int* sc, float4* hits, int* inst, int64_t n, cudaStream_t st,
+                    const int* nDev = nullptr);
 const float4* batch_tris(const cwp_batch* b);          // triangle records (v0, id), (e1, material), (e2, 0) of the tuned width
 const cwp_instance* batch_instances(const cwp_batch* b);
 int batch_mesh_count(const cwp_batch* b);

@@ -186,11 +186,14 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
     }
 }
 
-__global__ void k_serve_shadow_accum(int n, ShadowQueue sq, const int* __restrict__ occ, const SlotParams* __restrict__ slots) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n || occ[k] >= 0) return;
-    const float4 c = sq.c[k];
-    add_rgb(slots[sq.sc[k]].accum, __float_as_int(c.w), f3(c.x, c.y, c.z));
+// unoccluded shadow rays add their contributions; the count is read on the device (grid-stride)
+__global__ void k_serve_shadow_accum(const int* nDev, ShadowQueue sq, const int* __restrict__ occ, const SlotParams* __restrict__ slots) {
+    const int n = *nDev;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        if (occ[k] >= 0) continue;
+        const float4 c = sq.c[k];
+        add_rgb(slots[sq.sc[k]].accum, __float_as_int(c.w), f3(c.x, c.y, c.z));
+    }
 }
 
 // ---------------- BSDF test kernels ----------------
@@ -428,18 +431,16 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         k_serve_shade<<<g, 128, 0, s->st>>>(a);
         CWPB_CUDA(cudaGetLastError());
         CWPB_CUDA(cudaEventRecord(s->ev[3], s->st));
-        CWPB_CUDA(cudaMemcpyAsync(s->hcnt, s->cnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
-        CWPB_CUDA(cudaStreamSynchronize(s->st));
-        nNext = s->hcnt[0]; nShadow = s->hcnt[1];
-        if (nShadow > 0) {
-            if (int rc = batch_trace_dev(s->batch, true, s->sq.o, s->sq.d, s->sq.sc, nullptr, s->occ, nShadow, s->st)) return rc;
-            k_serve_shadow_accum<<<(unsigned)((nShadow + 255) / 256), 256, 0, s->st>>>((int)nShadow, s->sq, s->occ, s->dSlots);
-            CWPB_CUDA(cudaGetLastError());
-        }
+        // shadow rays: count on the device, no host round trip before the any-hit launch
+        if (int rc = batch_trace_dev(s->batch, true, s->sq.o, s->sq.d, s->sq.sc, nullptr, s->occ, 0, s->st, s->cnt + 1)) return rc;
+        k_serve_shadow_accum<<<148 * 8, 256, 0, s->st>>>(s->cnt + 1, s->sq, s->occ, s->dSlots);
+        CWPB_CUDA(cudaGetLastError());
     }
     CWPB_CUDA(cudaEventRecord(s->ev[4], s->st));
+    if (n > 0) CWPB_CUDA(cudaMemcpyAsync(s->hcnt, s->cnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CWPB_CUDA(cudaMemcpyAsync(s->hcnt + 4, s->slotCnt, (size_t)R * kSlotCounters * sizeof(int), cudaMemcpyDeviceToHost, s->st));
-    CWPB_CUDA(cudaStreamSynchronize(s->st));
+    CWPB_CUDA(cudaStreamSynchronize(s->st));   // the step's one host round trip: queue lengths and per-request counts
+    if (n > 0) { nNext = s->hcnt[0]; nShadow = s->hcnt[1]; }
     {
         float a = 0, b = 0, c = 0, d = 0;
         CWPB_CUDA(cudaEventElapsedTime(&a, s->ev[0], s->ev[1])); CWPB_CUDA(cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));

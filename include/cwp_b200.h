@@ -211,7 +211,7 @@ int cwp_render_noalloc(const cwp_params* p, const cwp_device_scene* s, const cwp
 typedef struct cwp_instance {
     float inv[12];      /* world -> object, 3 rows of (m0 m1 m2 t) */
     float fwd[12];      /* object -> world */
-    int32_t root;       /* root node of the instance's BLAS; filled in by cwp_batch_set_scenes */
+    int32_t root;       /* root node of the instance's BLAS in the traced layout (cwp_batch_download_tlas fills it in) */
     int32_t mesh;       /* BLAS index */
     float det_sign;     /* sign of det(fwd) */
     int32_t pad;
@@ -244,7 +244,10 @@ typedef struct cwp_batch_options {
     int32_t device;
     int32_t leaf;           /* max triangles per BVH2 / BVH4 leaf (default 4 when 0); CWBVH leaves hold at most 3 */
     int32_t widths;         /* bit mask of the layouts to emit: 1 << 2 (BVH2), 1 << 4 (BVH4), 1 << 8 (CWBVH); 0 = all */
-    int32_t reserved[5];
+    int32_t builder;        /* 0: every BLAS on the GPU in one H-PLOC launch; 1: on the host cores (binned SAH, 32 bins,
+                               SAH-collapsed CWBVH, spatial splits when `spatial` > 0), for resident scenes */
+    float spatial;          /* builder 1: spatial-split overlap threshold (cwp_build_options.spatial) */
+    int32_t reserved[3];
 } cwp_batch_options;
 
 typedef struct cwp_batch_tuning {
@@ -289,7 +292,8 @@ int cwp_batch_info_of(const cwp_batch* b, cwp_batch_info* out);
 /* Host copies for checking: the node array of one layout (width 2, 4 or 8) and the triangle records. Pass NULL
  * buffers to query the sizes (in float4). */
 int cwp_batch_download(const cwp_batch* b, int32_t width, float* nodes, int64_t* n_node_float4, float* tris, int64_t* n_tri_float4);
-/* root node of mesh m's BLAS in layout width; and the TLAS (BVH2 nodes, root per scene, instances with roots) */
+/* root node of mesh m's BLAS in layout width (instances name their mesh; the traversal looks its root up for the
+ * traced width); and the TLAS (BVH2 nodes, root per scene, instances with `root` set for the current tuning's width) */
 int cwp_batch_blas_root(const cwp_batch* b, int32_t width, int32_t mesh, int32_t* root);
 int cwp_batch_download_tlas(const cwp_batch* b, float* nodes, int64_t* n_node_float4, int32_t* roots, cwp_instance* inst);
 int cwp_batch_status(cwp_batch* b);   /* synchronises; CWP_ERR_TRAVERSAL if a ray hit a stack bound or the visit budget */
