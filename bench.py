@@ -283,7 +283,11 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
     so, sd, ss = o[samp].contiguous(), d[samp].contiguous(), sc[samp].contiguous()
     sh = torch.empty((len(samp), 4), dtype=torch.float32, device="cuda"); si = torch.empty(len(samp), dtype=torch.int32, device="cuda")
     t1 = time.perf_counter()
-    tun = b.autotune(so.data_ptr(), sd.data_ptr(), ss.data_ptr(), sh.data_ptr(), si.data_ptr(), len(samp))
+    if args.tuning:
+        blk, wd, fe, sm = (int(x) for x in args.tuning.split(","))
+        b.set_tuning(blk, wd, fe, sm); tun = b.tuning()
+    else:
+        tun = b.autotune(so.data_ptr(), sd.data_ptr(), ss.data_ptr(), sh.data_ptr(), si.data_ptr(), len(samp))
     tune_s = time.perf_counter() - t1
     del so, sd, ss, sh, si
 
@@ -423,10 +427,11 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="override the frame's samples per pixel (profiling cases)")
     ap.add_argument("--rays", type=int, default=0, help="override the batch size of trace16m / rays per scene of batched64 (profiling cases)")
     ap.add_argument("--scenes", type=int, default=0, help="override the scene count of batched64 (profiling cases)")
+    ap.add_argument("--tuning", default="", help="batched64: fixed launch shape block,width,fetch,smem instead of the autotuner (profiling cases)")
     ap.add_argument("--builder", type=int, default=0, help="batched64: 0 every BLAS on the GPU (H-PLOC, one launch), 1 on the host cores (binned SAH)")
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
-    ap.add_argument("--spatial", type=float, default=1e-5, help="host BVH: spatial-split overlap threshold (1e-5 = SBVH, the default; 0 = the reference's binned SAH only)")
+    ap.add_argument("--spatial", type=float, default=1e-3, help="host BVH: spatial-split overlap threshold (1e-3 = SBVH, the default; 0 = the reference binned SAH only)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])

@@ -253,7 +253,8 @@ extern "C" void cwp_server_destroy(cwp_server* s) {
     if (!s) return;
     cudaSetDevice(s->device);
     if (s->st) cudaStreamSynchronize(s->st);
-    for (auto& kv : s->reqs) if (kv.second.accum) cudaFree(kv.second.accum);
+    for (auto& kv : s->reqs) if (kv.second.accum) cudaFreeAsync(kv.second.accum, s->st);
+    if (s->st) cudaStreamSynchronize(s->st);
     for (void* p : s->allocs) cudaFree(p);
     if (s->hcnt) cudaFreeHost(s->hcnt);
     for (cudaEvent_t e : s->ev) if (e) cudaEventDestroy(e);
@@ -357,7 +358,7 @@ static int admit(cwp_server* s, bool& changed) {
         size_t freeB = 0, totalB = 0;
         CWPB_CUDA(cudaMemGetInfo(&freeB, &totalB));
         if (freeB < bytes + (size_t)s->O.hbm_reserve) break;   // admission by free device memory
-        CWPB_CUDA(cudaMalloc(&q.accum, bytes));
+        CWPB_CUDA(cudaMallocAsync((void**)&q.accum, bytes, s->st));   // stream-ordered: no device-wide synchronisation
         CWPB_CUDA(cudaMemsetAsync(q.accum, 0, bytes, s->st));
         SlotParams P{};
         P.cam = q.r.cam; P.sunTo = f3(q.r.sun_to[0], q.r.sun_to[1], q.r.sun_to[2]); P.sunE = f3(q.r.sun_e[0], q.r.sun_e[1], q.r.sun_e[2]);
@@ -483,12 +484,15 @@ extern "C" int cwp_server_result(cwp_server* s, int64_t id, float* accum, cwp_re
     ServeRequest& q = it->second;
     CWPB_CHECK(q.done, CWP_ERR_STATE, "request %lld is not complete", (long long)id);
     CWPB_CUDA(cudaSetDevice(s->device));
-    if (accum) CWPB_CUDA(cudaMemcpy(accum, q.accum, (size_t)q.r.cam.w * q.r.cam.h * sizeof(float4), cudaMemcpyDeviceToHost));
+    if (accum) {
+        CWPB_CUDA(cudaMemcpyAsync(accum, q.accum, (size_t)q.r.cam.w * q.r.cam.h * sizeof(float4), cudaMemcpyDeviceToHost, s->st));
+        CWPB_CUDA(cudaStreamSynchronize(s->st));
+    }
     if (st) {
         st->submit_ms = q.submitMs; st->admit_ms = q.admitMs; st->done_ms = q.doneMs; st->rays = q.rays; st->shadow_rays = q.shadow;
         st->w = q.r.cam.w; st->h = q.r.cam.h; st->spp = q.r.spp; st->pad = 0;
     }
-    CWPB_CUDA(cudaFree(q.accum));
+    CWPB_CUDA(cudaFreeAsync(q.accum, s->st));
     s->reqs.erase(it);
     return CWP_OK;
 }
