@@ -187,6 +187,7 @@ SIGNATURES = {
     "cwp_server_info_of": (C.c_int, [C.c_void_p, C.POINTER(ServerInfo)]),
     "cwp_bsdf_eval_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 4 + [C.c_int32] + [C.c_void_p] * 3 + [C.c_int64]),
     "cwp_bsdf_sample_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 3 + [C.c_int32] + [C.c_void_p] * 6 + [C.c_int64]),
+    "cwp_display": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_float, C.c_int32, C.c_void_p]),
     "cwp_camera_look_at": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_camera_from_c2w": (C.c_int, [C.POINTER(C.c_float), C.c_float, C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_params_defaults": (C.c_int, [C.POINTER(Params)]),
@@ -532,6 +533,11 @@ class Batch:
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value and _lib is not None:
             _lib.cwp_batch_destroy(self._h); self._h = C.c_void_p()
+
+
+def display(d_accum, d_rgba, n, spp, exposure_ev=0.0, mode=0, stream=None):
+    """Device tone mapping of an accumulation buffer into RGBA8 (mode 0: the PNG transform)."""
+    _check(lib().cwp_display(d_accum, d_rgba, n, spp, exposure_ev, mode, stream))
 
 
 def materials_array(m):

@@ -369,6 +369,13 @@ int cwp_bsdf_sample_batch(const cwp_material* mats, int32_t n_mats, const int32_
                           const float* ux, const float* uvw, float* wi, float* weight, float* pdf, int32_t* ok, int64_t n);
 
 /* ------------------------------------------------------------------------------------------------------------------
+ * Headless display transform. Replaces launchDisplay (app/display.cu, display.h:9) without the viewer's graphics
+ * interop: d_accum (w * h float4 radiance sums over spp samples) -> d_rgba (w * h RGBA8). Mode 0 = the PNG transform
+ * (io/image.cpp tonemapSRGB8: divide by spp, clip, sRGB OETF); 1 = Reinhard; 2 = ACES fit; exposure in EV.
+ * ------------------------------------------------------------------------------------------------------------------ */
+int cwp_display(const float* d_accum, uint8_t* d_rgba, int64_t n, int32_t spp, float exposure_ev, int32_t mode, void* stream);
+
+/* ------------------------------------------------------------------------------------------------------------------
  * Camera and parameter helpers. Replace lookAtC2W / focalFromHfov / makeCamera (scene/camera.cpp:7-23) and the
  * Params filling of setupScene (app/scene_setup.cpp:175-185, Lighting defaults scene/lighting.h:7-13).
  * ------------------------------------------------------------------------------------------------------------------ */

@@ -813,6 +813,10 @@ static int trav_blas(int width, const V4* nodes, const V4* tv, V3 o, V3 d, float
     if (width == 4) return trav4r(nodes, tv, o, d, tmin, any, 0, t, h, u, v, NULL, root);
     return trav8r(nodes, tv, o, d, tmin, any, 0, t, h, u, v, NULL, root);
 }
+/* visit counters of the two-level traversal: TLAS nodes, instance entries, BLAS nodes, triangle tests (enabled by
+ * orc_inst_stats; for cost studies) */
+static long long g_inst_stats[4]; static int g_inst_stats_on;
+void orc_inst_stats(int on, long long* out) { if (out) memcpy(out, g_inst_stats, sizeof g_inst_stats); memset(g_inst_stats, 0, sizeof g_inst_stats); g_inst_stats_on = on; }
 /* one ray through one two-level scene (root = its TLAS root, < 0 for an empty scene); returns -1 on a stack bound */
 static int o_inst1(int width, int any, const float* blas, const float* tris, const V4* T, int root, const float* inst, V3 o, V3 d, float tmin,
                    float* pt, int* ph, float* pu, float* pv, int* phi) {
@@ -821,6 +825,7 @@ static int o_inst1(int width, int any, const float* blas, const float* tris, con
         const float idx = safe_rcp(d.x), idy = safe_rcp(d.y), idz = safe_rcp(d.z), ox = -o.x * idx, oy = -o.y * idy, oz = -o.z * idz;
         int stack[64], sp = 0, next = root;
         while (!done) {
+            if (g_inst_stats_on) g_inst_stats[0]++;
             const V4 n0 = T[4 * next], n1 = T[4 * next + 1], nz = T[4 * next + 2], mt = T[4 * next + 3];
             const int c0 = fi(mt.x), c1 = fi(mt.y), k0 = fi(mt.z), k1 = fi(mt.w);
             const float a0 = fmaf(n0.x, idx, ox), a1 = fmaf(n0.y, idx, ox), a2 = fmaf(n0.z, idy, oy), a3 = fmaf(n0.w, idy, oy), a4 = fmaf(nz.x, idz, oz), a5 = fmaf(nz.y, idz, oz);
@@ -840,7 +845,12 @@ static int o_inst1(int width, int any, const float* blas, const float* tris, con
                 const V3 ld = v3(I[0] * d.x + I[1] * d.y + I[2] * d.z, I[4] * d.x + I[5] * d.y + I[6] * d.z, I[8] * d.x + I[9] * d.y + I[10] * d.z);
                 int iroot; memcpy(&iroot, &I[24], 4);
                 float bt = t, bu = 0.f, bv = 0.f; int bh = -1;
-                if (trav_blas(width, (const V4*)blas, (const V4*)tris, lo, ld, tmin, any, &bt, &bh, &bu, &bv, iroot) < 0) { bad = 1; done = 1; break; }
+                Stats bs = { 0, 0 };
+                if (g_inst_stats_on) g_inst_stats[1]++;
+                if ((width == 2 ? trav2r((const V4*)blas, (const V4*)tris, lo, ld, tmin, any, 0, &bt, &bh, &bu, &bv, g_inst_stats_on ? &bs : NULL, iroot)
+                     : width == 4 ? trav4r((const V4*)blas, (const V4*)tris, lo, ld, tmin, any, 0, &bt, &bh, &bu, &bv, g_inst_stats_on ? &bs : NULL, iroot)
+                     : trav8r((const V4*)blas, (const V4*)tris, lo, ld, tmin, any, 0, &bt, &bh, &bu, &bv, g_inst_stats_on ? &bs : NULL, iroot)) < 0) { bad = 1; done = 1; break; }
+                g_inst_stats[2] += bs.nodes; g_inst_stats[3] += bs.tris;
                 if (bh >= 0 && bt < t) { t = bt; h = bh; u = bu; v = bv; hi = ~go; }
                 if (any && h >= 0) { done = 1; break; }
                 if (sp == 0) { done = 1; break; }

@@ -190,3 +190,31 @@ def test_host_built_blas_match_oracle(gpu, cwp, oracle, spatial):
         same = (ka == kb) & (hi == gi)
         tie = ~same & (hi >= 0) & (gi >= 0) & (np.abs(h[:, 0].astype(np.float64) - g[:, 0]) <= 1e-6 * np.abs(g[:, 0].astype(np.float64)))
         assert np.all(same | tie) and tie.mean() < 0.02
+
+
+def test_degenerate_segments(gpu, cwp, oracle):
+    """One-triangle and two-triangle meshes (a segment whose root is a leaf), scenes with 0, 1 and 2 instances (an
+    empty TLAS, the one-instance wrapper node), a zero-length trace: every width returns the oracle's hits."""
+    tri1 = (np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32), np.array([[0, 1, 2]], np.int32), np.zeros(1, np.int32), None)
+    quad = (np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], np.float32), np.array([[0, 1, 2], [0, 2, 3]], np.int32), np.zeros(2, np.int32), None)
+    box = cwp.Mesh.box_field(3, 4)
+    b = cwp.Batch([tri1, quad, box])
+    I = np.eye(3, 4, dtype=np.float32).reshape(12)
+    shift = I.copy(); shift[3] = 2.0
+    xf = np.stack([I, I, shift, I]).astype(np.float32); mesh_of = np.array([0, 1, 0, 2], np.int32)
+    first = np.array([0, 0, 1, 3, 4], np.int32)   # scene 0 empty, 1: one instance, 2: two, 3: one box field
+    b.set_scenes(cwp.instances(xf, mesh_of), first)
+    rng = np.random.default_rng(1)
+    n = 4000
+    o = np.zeros((n, 4), np.float32); o[:, :3] = rng.uniform(-3, 4, (n, 3)); o[:, 2] = 5.0
+    d = np.zeros((n, 4), np.float32); v = rng.normal(size=(n, 3)); v[:, 2] = -np.abs(v[:, 2]) - 1.0; d[:, :3] = v / np.linalg.norm(v, axis=1, keepdims=True); d[:, 3] = 1e30
+    sc = rng.integers(0, 4, n).astype(np.int32)
+    for width in (2, 4, 8):
+        b.set_tuning(64, width, 1, 1)
+        h, hi = trace(gpu, b, o, d, sc)
+        nodes, tris = b.download(width)
+        tlas, roots, ins = b.download_tlas(4, 4)
+        ho, hio = oracle.trace_inst(width, False, nodes, tris, tlas, roots, ins, o, d, sc)
+        assert np.array_equal(h.view(np.uint32), ho.view(np.uint32)) and np.array_equal(hi, hio)
+        assert np.all(hi[sc == 0] == -1) and (hi[sc == 1] >= 0).any() and (hi[sc == 2] >= 0).any()
+    b.trace(0, 0, 0, 0, 0, 0)   # n = 0: nothing to do, no error

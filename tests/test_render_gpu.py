@@ -114,3 +114,21 @@ def test_psnr_vs_reference_pt(gpu, cwp, tmp_path):
     _, _, st, acc = render(cwp, mesh, bvh, w, h, spp, 256, 2)
     ours = cwp.imageio.accum_to_image(acc, w, h, spp)
     assert cwp.imageio.psnr(ours, ref_img) >= 50.0
+
+
+def test_display_transform_matches_png_transform(gpu, cwp):
+    """cwp_display mode 0 on a rendered accumulation buffer gives the PNG writer's 8-bit sRGB values (host transform
+    of sum / spp); the tone-mapped modes stay in range and preserve order."""
+    mesh, bvh = cwp.scene("boxes12k", variant=8, bins=32)
+    r, p, st, acc = render(cwp, mesh, bvh, 64, 48, 4, 4, 8)
+    d_acc = gpu.from_numpy(acc).cuda(); out = gpu.empty((64 * 48, 4), dtype=gpu.uint8, device="cuda")
+    cwp.display(d_acc.data_ptr(), out.data_ptr(), 64 * 48, 4, 0.0, 0); gpu.cuda.synchronize()
+    got = out.cpu().numpy()
+    want = cwp.imageio.tonemap_srgb8(acc[:, :3] / np.float32(4))
+    diff = np.abs(got[:, :3].astype(int) - want.astype(int))
+    assert diff.max() <= 1 and (diff == 0).mean() >= 0.999 and np.all(got[:, 3] == 255)   # powf may differ by an ulp at a rounding edge
+    for mode in (1, 2):
+        cwp.display(d_acc.data_ptr(), out.data_ptr(), 64 * 48, 4, 1.0, mode); gpu.cuda.synchronize()
+        m = out.cpu().numpy()[:, 0].astype(int); lin = acc[:, 0]
+        o = np.argsort(lin)
+        assert np.all(np.diff(m[o]) >= -1)
