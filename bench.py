@@ -146,6 +146,36 @@ def cpu_frame_sample(cwp, wl, mesh, bvh, variant, seconds=12.0):
                 sample=f"{npix} pixels x {wl['spp']} spp of the {wl['w']}x{wl['h']} frame ({rays} closest+shadow rays in {spent:.2f} s)")
 
 
+NODE_BYTES = {2: 64, 4: 128, 8: 80}
+TRI_BYTES = 48   # Woop rows, an upper bound (the test reads row 2 first and rows 0/1 only past the t check)
+
+
+def onchip_bytes_frame(cwp, wl, mesh, bvh, variant, npix=1024):
+    """Algorithmic on-chip bytes per ray of the frame (node visits x node size + triangle tests x 48 B), counted by
+    the oracle's traversal of the same tree over a band of pixels (part of the CPU-baseline leg)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from conftest import Oracle
+    p = cwp.frame_params(mesh, wl["w"], wl["h"], bounces=wl["bounces"])
+    N = wl["w"] * wl["h"]; pix0 = N // 2 - npix // 2
+    rc, st = Oracle().render_work(p, variant, 1, bvh, wl["bounces"], min(wl["spp"], 16), pix0, pix0 + npix)
+    nb = NODE_BYTES[variant]
+    return dict(closest=(st[0] * nb + st[1] * TRI_BYTES) / max(rc[0], 1), shadow=(st[2] * nb + st[3] * TRI_BYTES) / max(rc[1], 1),
+                nodes_per_closest=st[0] / max(rc[0], 1), tris_per_closest=st[1] / max(rc[0], 1),
+                nodes_per_shadow=st[2] / max(rc[1], 1), tris_per_shadow=st[3] / max(rc[1], 1),
+                sample=f"oracle traversal of {npix} pixels x {min(wl['spp'], 16)} spp ({int(rc[0])} closest, {int(rc[1])} shadow rays) on the same tree")
+
+
+def onchip_bytes_trace(cwp, bvh, variant, o, d, n=1 << 15):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from conftest import Oracle
+    orc = Oracle(); nb = NODE_BYTES[variant]
+    _, sc = orc.trace(variant, 1, False, bvh.nodes, bvh.woop, o[:n], d[:n], stats=True)
+    _, sa = orc.trace(variant, 1, True, bvh.nodes, bvh.woop, o[:n], d[:n], stats=True)
+    return dict(closest=(sc[0] * nb + sc[1] * TRI_BYTES) / n, shadow=(sa[0] * nb + sa[1] * TRI_BYTES) / n,
+                nodes_per_closest=sc[0] / n, tris_per_closest=sc[1] / n, nodes_per_shadow=sa[0] / n, tris_per_shadow=sa[1] / n,
+                sample=f"oracle traversal of {n} of the batch's rays on the same tree")
+
+
 def cpu_trace_sample(cwp, bvh, variant, o, d, seconds=12.0):
     import numpy as np
     L = reference_lib(); threads = os.cpu_count() or 1
@@ -383,7 +413,7 @@ def bench_serving(args, wl, cwp, torch, out):
     res = {}
     for name, stream in streams.items():
         for mode, maxr in (("continuous", wl["max_requests"]), ("plain", 1)):
-            s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=maxr)
+            s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=maxr, regroup=bool(args.regroup))
             s.set_scenes(descs, first)
             clk = Clocks(str(torch.cuda.current_device()))
             r = serve_stream(cwp, s, stream)
@@ -398,6 +428,7 @@ def bench_serving(args, wl, cwp, torch, out):
                ms_per_step=1e3 / c["throughput_req_s"], higher_is_better=True, dtype="f32",
                config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "blas_builder": ["gpu h-ploc", "host binned SAH"][wl["builder"]],
                        "blas_build_ms": info.blas_build_ms, "scene_generation_s": gen_s, "depth": 8, "max_paths": wl["max_paths"], "max_requests": wl["max_requests"],
+                       "regroup": bool(args.regroup),
                        "materials": "OpenPBR subset: roughness U[0.05,1], metallic Bernoulli(0.3), 10% glass IOR 1.5",
                        "mix": {"requests": n_req, "arrival_rate_req_s": wl["rate"], "resolutions": "256^2, 512^2, 1280x720, 1920x1080", "spp": "1, 4, 16, 64, 256",
                                "continuous": strip(c), "plain": strip(p), "throughput_vs_plain": c["throughput_req_s"] / p["throughput_req_s"],
@@ -432,6 +463,7 @@ def main():
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     ap.add_argument("--spatial", type=float, default=1e-3, help="host BVH: spatial-split overlap threshold (1e-3 = SBVH, the default; 0 = the reference binned SAH only)")
+    ap.add_argument("--regroup", type=int, default=1, help="serving: sort each step's continuations by request (1) or not (0)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
@@ -544,6 +576,7 @@ def main():
                    roofline={"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                              "peak_kind": peak_kind, "traffic": None,
                              "algorithmic": f"{STATE_BYTES} B of path state per queued ray read and per continuation/shadow ray written"})
+        onchip = dict(kind="frame", closest=float(c_tot.sum()), shadow=float(s_tot.sum()), closest_ms=float(tms.sum()), shadow_ms=float(sms.sum()))
         r.close()
     else:
         # ------------------------------------------------------------------ ray batches
@@ -623,6 +656,7 @@ def main():
                      "max_t_error": c["max_t_error"], "t_error_unit": "max(t, scene extent)",
                      "plain_grays_s": plain, "vs_plain": value / plain if plain else None}
         achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
+        onchip = dict(kind="batch", closest=float(n * args.steps), shadow=float(n * args.steps), closest_ms=c_ms, shadow_ms=a_ms)
         out.update(metric="closest+any rays per second, incoherent ray batch", value=value, ms_per_step=max_ms / args.steps,
                    config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles)", "rays": n,
                            "layout": LAYOUT_NAMES[variant] + (" precision form (f16 conservative slabs, watertight fp32 triangles)" if wl.get("precision") else ""), **check,
@@ -643,6 +677,22 @@ def main():
             out["cpu_baseline"] = cpu_frame_sample(cwp, wl, mesh, rbvh, variant)
         else:
             out["cpu_baseline"] = cpu_trace_sample(cwp, rbvh, variant, o, d)
+        # on-chip roofline: oracle-counted node + triangle bytes per ray on the GPU's own tree, over the kernels' event
+        # times, against the measured L2 read bandwidth (the scene is L2-resident, so this is the traversal's bound)
+        if not wl.get("precision"):
+            ob = onchip_bytes_frame(cwp, wl, mesh, bvh, variant) if "rays" not in wl else onchip_bytes_trace(cwp, bvh, variant, o, d)
+            l2 = cwp.measure_l2_read(device=local)
+            cb, sb = onchip["closest"] * ob["closest"], onchip["shadow"] * ob["shadow"]
+            kern = ("k_trace_shade", "k_shadow") if onchip["kind"] == "frame" else ("k_trace_closest", "k_trace_any")
+            big = 0 if onchip["closest_ms"] >= onchip["shadow_ms"] else 1
+            ach = [cb / (onchip["closest_ms"] * 1e-3) / 1e9, sb / (onchip["shadow_ms"] * 1e-3) / 1e9]
+            out["roofline_onchip"] = {"bound": "l2", "kernel": kern[big], "achieved": ach[big], "peak": l2, "unit": "GB/s", "frac": ach[big] / l2,
+                                      "other_kernel": {"kernel": kern[1 - big], "achieved": ach[1 - big], "frac": ach[1 - big] / l2},
+                                      "peak_kind": "measured: cwp_measure_l2_read, 32 MiB read 50 times per launch with 16-byte L2-cached loads",
+                                      "bytes_per_closest_ray": ob["closest"], "bytes_per_shadow_ray": ob["shadow"],
+                                      "nodes_per_closest_ray": ob["nodes_per_closest"], "tris_per_closest_ray": ob["tris_per_closest"],
+                                      "nodes_per_shadow_ray": ob["nodes_per_shadow"], "tris_per_shadow_ray": ob["tris_per_shadow"],
+                                      "algorithmic": f"node visits x {NODE_BYTES[variant]} B + triangle tests x {TRI_BYTES} B per ray ({ob['sample']})"}
     if ws > 1:
         tdist.barrier()
         tdist.destroy_process_group()

@@ -107,7 +107,7 @@ class Material(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("max_paths", C.c_int64), ("max_requests", C.c_int32), ("gd_energy", C.c_int32), ("hbm_reserve", C.c_int64), ("device", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("regroup", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class Request(C.Structure):
@@ -123,7 +123,7 @@ class RequestStats(C.Structure):
 class ServerInfo(C.Structure):
     _fields_ = [("steps", C.c_int64), ("rays", C.c_int64), ("shadow_rays", C.c_int64), ("admissions", C.c_int64), ("tlas_rebuilds", C.c_int64),
                 ("closest_ms", C.c_double), ("shade_ms", C.c_double), ("shadow_ms", C.c_double), ("raygen_ms", C.c_double), ("tlas_ms", C.c_double),
-                ("step_ms", C.c_double)]
+                ("step_ms", C.c_double), ("admit_ms", C.c_double), ("tlas_device_ms", C.c_double)]
 
 
 # every exported symbol of the C ABI with its ctypes signature (restype, argtypes)
@@ -166,6 +166,8 @@ SIGNATURES = {
     "cwp_instance_from_xform": (C.c_int, [C.POINTER(C.c_float), C.c_int32, C.POINTER(Instance)]),
     "cwp_batch_create": (C.c_int, [C.POINTER(MeshView), C.c_int32, C.POINTER(BatchOptions), C.POINTER(C.c_void_p)]),
     "cwp_batch_destroy": (None, [C.c_void_p]),
+    "cwp_batch_reserve_scenes": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "cwp_batch_update_scenes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "cwp_batch_set_scenes": (C.c_int, [C.c_void_p, C.POINTER(Instance), C.c_int64, C.POINTER(C.c_int32), C.c_int32]),
     "cwp_batch_trace": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "cwp_batch_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(BatchTuning)]),
@@ -188,6 +190,7 @@ SIGNATURES = {
     "cwp_bsdf_eval_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 4 + [C.c_int32] + [C.c_void_p] * 3 + [C.c_int64]),
     "cwp_bsdf_sample_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 3 + [C.c_int32] + [C.c_void_p] * 6 + [C.c_int64]),
     "cwp_display": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_float, C.c_int32, C.c_void_p]),
+    "cwp_measure_l2_read": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "cwp_camera_look_at": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_camera_from_c2w": (C.c_int, [C.POINTER(C.c_float), C.c_float, C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "cwp_params_defaults": (C.c_int, [C.POINTER(Params)]),
@@ -494,6 +497,16 @@ class Batch:
         first = np.ascontiguousarray(scene_first, np.int32)
         _check(lib().cwp_batch_set_scenes(self._h, inst, len(inst), _iptr(first), len(first) - 1))
 
+    def reserve_scenes(self, n_scenes, cap):
+        """n_scenes empty scenes with room for cap instances each (the incremental form)"""
+        _check(lib().cwp_batch_reserve_scenes(self._h, n_scenes, cap))
+
+    def update_scenes(self, scenes, inst, counts):
+        """replace the instances of the listed scenes (inst: their instances in order, counts per scene) and rebuild only
+        their TLAS"""
+        sc = np.ascontiguousarray(scenes, np.int32); ct = np.ascontiguousarray(counts, np.int32)
+        _check(lib().cwp_batch_update_scenes(self._h, _iptr(sc), len(sc), inst if inst is not None and len(inst) else None, _iptr(ct)))
+
     def trace(self, d_o, d_d, d_scene, d_hits, d_inst, n, any_hit=False, stream=None):
         _check(lib().cwp_batch_trace(self._h, 1 if any_hit else 0, d_o, d_d, d_scene, d_hits, d_inst, n, stream))
 
@@ -538,6 +551,11 @@ class Batch:
 def display(d_accum, d_rgba, n, spp, exposure_ev=0.0, mode=0, stream=None):
     """Device tone mapping of an accumulation buffer into RGBA8 (mode 0: the PNG transform)."""
     _check(lib().cwp_display(d_accum, d_rgba, n, spp, exposure_ev, mode, stream))
+
+
+def measure_l2_read(nbytes=32 << 20, reps=50, device=0):
+    """On-chip (L2) read bandwidth of the device in GB/s: the denominator of the traversal kernels' roofline."""
+    g = C.c_double(); _check(lib().cwp_measure_l2_read(nbytes, reps, device, C.byref(g))); return g.value
 
 
 def materials_array(m):
@@ -585,10 +603,11 @@ class Server:
     """Serving form: requests over the resident scenes of a Batch, continuous batching (max_requests > 1) or the plain
     form (max_requests = 1)."""
 
-    def __init__(self, batch, materials, mesh_mat_base, max_paths=8 << 20, max_requests=64, gd_energy=1, hbm_reserve=1 << 30, device=0):
+    def __init__(self, batch, materials, mesh_mat_base, max_paths=8 << 20, max_requests=64, gd_energy=1, hbm_reserve=1 << 30, device=0,
+                 regroup=True):
         self._batch = batch
         M = materials_array(materials); base = np.ascontiguousarray(mesh_mat_base, np.int32)
-        o = ServerOptions(max_paths, max_requests, gd_energy, hbm_reserve, device)
+        o = ServerOptions(max_paths, max_requests, gd_energy, hbm_reserve, device, 1 if regroup else -1)
         h = C.c_void_p()
         _check(lib().cwp_server_create(batch._h, M, len(M), _iptr(base), C.byref(o), C.byref(h)))
         self._h = h

@@ -182,6 +182,10 @@ struct cwp_batch {
     cwp_instance* inst = nullptr; int64_t capInst = 0;
     float4 *instLo = nullptr, *instHi = nullptr, *tlas = nullptr;
     int *sceneRoot = nullptr, *segFirstTlas = nullptr; int capScenes = 0;
+    // incremental form: fixed regions of `fixedCap` instances per scene, updates built over a compact copy
+    int fixedCap = 0;
+    cwp_instance* uInst = nullptr; float4 *uLo = nullptr, *uHi = nullptr; int64_t capU = 0;
+    int* dstFirstTlas = nullptr; int capDst = 0;
     // launch
     cwp_batch_tuning tuning{};
     int* err = nullptr; unsigned long long* cursor = nullptr;
@@ -199,6 +203,7 @@ static void batch_free(cwp_batch* b) {
     b->blasB.release(); b->tlasB.release();
     cudaFree(b->triV); cudaFree(b->primLo); cudaFree(b->primHi); cudaFree(b->meshBox); cudaFree(b->meshFirstDev);
     cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas); cudaFree(b->sceneRoot); cudaFree(b->segFirstTlas);
+    cudaFree(b->uInst); cudaFree(b->uLo); cudaFree(b->uHi); cudaFree(b->dstFirstTlas);
     cudaFree(b->err); cudaFree(b->cursor);
     for (int i = 0; i < 3; i++) cudaFree(b->meshRoot[i]);
     if (b->st) cudaStreamDestroy(b->st);
@@ -373,6 +378,14 @@ extern "C" int cwp_batch_create(const cwp_mesh_view* meshes, int32_t n, const cw
     return CWP_OK;
 }
 
+static int check_instances(const cwp_batch* b, const cwp_instance* h, int64_t n, int64_t at) {
+    for (int64_t i = 0; i < n; i++) {
+        CWPB_CHECK(h[i].mesh >= 0 && h[i].mesh < b->nMesh, CWP_ERR_INVALID, "instance %lld: mesh %d out of range", (long long)(at + i), h[i].mesh);
+        for (int k = 0; k < 12; k++) CWPB_CHECK(std::isfinite(h[i].inv[k]) && std::isfinite(h[i].fwd[k]), CWP_ERR_INVALID, "instance %lld: non-finite transform", (long long)(at + i));
+    }
+    return CWP_OK;
+}
+
 extern "C" int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int64_t n, const int32_t* first, int32_t nScenes) {
     CWPB_CHECK(b, CWP_ERR_INVALID, "batch is NULL");
     CWPB_CHECK(first && nScenes >= 1, CWP_ERR_INVALID, "no scenes");
@@ -380,12 +393,7 @@ extern "C" int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int6
     CWPB_CHECK(n >= 0 && n < (1ll << 30), CWP_ERR_INVALID, "%lld instances", (long long)n);
     CWPB_CHECK(n == 0 || inst, CWP_ERR_INVALID, "instances are NULL");
     for (int s = 0; s < nScenes; s++) CWPB_CHECK(first[s + 1] >= first[s], CWP_ERR_INVALID, "scene offsets decrease at scene %d", s);
-    std::vector<cwp_instance> h(inst, inst + n);
-    for (int64_t i = 0; i < n; i++) {
-        CWPB_CHECK(h[i].mesh >= 0 && h[i].mesh < b->nMesh, CWP_ERR_INVALID, "instance %lld: mesh %d out of range", (long long)i, h[i].mesh);
-        for (int k = 0; k < 12; k++) CWPB_CHECK(std::isfinite(h[i].inv[k]) && std::isfinite(h[i].fwd[k]), CWP_ERR_INVALID, "instance %lld: non-finite transform", (long long)i);
-        h[i].root = h[i].mesh;   // informative only: the traversal looks the BLAS root up per layout (meshRoot)
-    }
+    if (int rc = check_instances(b, inst, n, 0)) return rc;
     // segments: the non-empty scenes (their instance ranges are contiguous and cover the array)
     std::vector<int> seg; seg.push_back(0);
     std::vector<int> rootHost(nScenes, -1);
@@ -413,7 +421,7 @@ extern "C" int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int6
         b->capScenes = nScenes + 1;
     }
     CWPB_CUDA(cudaEventRecord(b->e0, b->st));
-    if (n > 0) CWPB_CUDA(cudaMemcpyAsync(b->inst, h.data(), (size_t)n * sizeof(cwp_instance), cudaMemcpyHostToDevice, b->st));
+    if (n > 0) CWPB_CUDA(cudaMemcpyAsync(b->inst, inst, (size_t)n * sizeof(cwp_instance), cudaMemcpyHostToDevice, b->st));
     CWPB_CUDA(cudaMemcpyAsync(b->sceneRoot, rootHost.data(), (size_t)nScenes * sizeof(int), cudaMemcpyHostToDevice, b->st));
     CWPB_CUDA(cudaMemcpyAsync(b->segFirstTlas, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice, b->st));
     if (n > 0) {
@@ -427,7 +435,103 @@ extern "C" int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int6
     CWPB_CUDA(cudaGetLastError());
     b->nScenes = 0;   // not traceable until the new TLAS passes its check
     if (int rc = check_tlas(b->tlas, (int)n, b->segFirstTlas, nSeg, b->err, b->st)) return rc;
-    b->nScenes = nScenes; b->nInst = n; b->sceneFirst.assign(first, first + nScenes + 1);
+    b->nScenes = nScenes; b->nInst = n; b->sceneFirst.assign(first, first + nScenes + 1); b->fixedCap = 0;
+    return CWP_OK;
+}
+
+extern "C" int cwp_batch_reserve_scenes(cwp_batch* b, int32_t nScenes, int32_t cap) {
+    CWPB_CHECK(b, CWP_ERR_INVALID, "batch is NULL");
+    CWPB_CHECK(nScenes >= 1 && cap >= 1 && (int64_t)nScenes * cap < (1ll << 30), CWP_ERR_INVALID, "%d scenes of %d instances", nScenes, cap);
+    CWPB_CHECK(nScenes <= (1 << kSegBits), CWP_ERR_INVALID, "%d scenes (limit %d)", nScenes, 1 << kSegBits);
+    CWPB_CUDA(cudaSetDevice(b->device));
+    const int64_t n = (int64_t)nScenes * cap;
+    b->nScenes = 0;   // not traceable while the arrays change
+    if (n > b->capInst) {
+        cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas);
+        b->inst = nullptr; b->instLo = b->instHi = b->tlas = nullptr; b->capInst = 0;
+        CWPB_CUDA(cudaMalloc(&b->inst, (size_t)n * sizeof(cwp_instance)));
+        CWPB_CUDA(cudaMalloc(&b->instLo, (size_t)n * sizeof(float4))); CWPB_CUDA(cudaMalloc(&b->instHi, (size_t)n * sizeof(float4)));
+        CWPB_CUDA(cudaMalloc(&b->tlas, (size_t)4 * n * sizeof(float4)));
+        b->capInst = n;
+    }
+    if (n > b->capU) {
+        cudaFree(b->uInst); cudaFree(b->uLo); cudaFree(b->uHi); b->uInst = nullptr; b->uLo = b->uHi = nullptr; b->capU = 0;
+        CWPB_CUDA(cudaMalloc(&b->uInst, (size_t)n * sizeof(cwp_instance)));
+        CWPB_CUDA(cudaMalloc(&b->uLo, (size_t)n * sizeof(float4))); CWPB_CUDA(cudaMalloc(&b->uHi, (size_t)n * sizeof(float4)));
+        b->capU = n;
+    }
+    if (nScenes + 1 > b->capScenes) {
+        cudaFree(b->sceneRoot); cudaFree(b->segFirstTlas); b->sceneRoot = b->segFirstTlas = nullptr;
+        CWPB_CUDA(cudaMalloc(&b->sceneRoot, (size_t)(nScenes + 1) * sizeof(int)));
+        CWPB_CUDA(cudaMalloc(&b->segFirstTlas, (size_t)(nScenes + 1) * sizeof(int)));
+        b->capScenes = nScenes + 1;
+    }
+    if (nScenes > b->capDst) {
+        cudaFree(b->dstFirstTlas); b->dstFirstTlas = nullptr;
+        CWPB_CUDA(cudaMalloc(&b->dstFirstTlas, (size_t)nScenes * sizeof(int)));
+        b->capDst = nScenes;
+    }
+    // every scene empty: root -1 (its rays miss); zeroed instances and nodes keep the downloads well-formed
+    CWPB_CUDA(cudaMemsetAsync(b->sceneRoot, 0xff, (size_t)nScenes * sizeof(int), b->st));
+    CWPB_CUDA(cudaMemsetAsync(b->inst, 0, (size_t)n * sizeof(cwp_instance), b->st));
+    CWPB_CUDA(cudaMemsetAsync(b->tlas, 0, (size_t)4 * n * sizeof(float4), b->st));
+    CWPB_CUDA(cudaStreamSynchronize(b->st));
+    b->fixedCap = cap; b->nInst = n; b->nScenes = nScenes;
+    b->sceneFirst.resize(nScenes + 1);
+    for (int s = 0; s <= nScenes; s++) b->sceneFirst[s] = s * cap;
+    return CWP_OK;
+}
+
+extern "C" int cwp_batch_update_scenes(cwp_batch* b, const int32_t* scenes, int32_t nUpd, const cwp_instance* inst, const int32_t* counts) {
+    CWPB_CHECK(b, CWP_ERR_INVALID, "batch is NULL");
+    CWPB_CHECK(b->fixedCap > 0 && b->nScenes > 0, CWP_ERR_STATE, "no reserved scenes (cwp_batch_reserve_scenes)");
+    CWPB_CHECK(nUpd >= 0 && (nUpd == 0 || (scenes && counts)), CWP_ERR_INVALID, "NULL scene list");
+    if (nUpd == 0) return CWP_OK;
+    const int cap = b->fixedCap;
+    std::vector<char> seen(b->nScenes, 0);
+    int64_t total = 0;
+    for (int i = 0; i < nUpd; i++) {
+        CWPB_CHECK(scenes[i] >= 0 && scenes[i] < b->nScenes, CWP_ERR_INVALID, "scene %d out of range", scenes[i]);
+        CWPB_CHECK(!seen[scenes[i]], CWP_ERR_INVALID, "scene %d listed twice", scenes[i]);
+        CWPB_CHECK(counts[i] >= 0 && counts[i] <= cap, CWP_ERR_INVALID, "scene %d: %d instances (room for %d)", scenes[i], counts[i], cap);
+        seen[scenes[i]] = 1; total += counts[i];
+    }
+    CWPB_CHECK(total == 0 || inst, CWP_ERR_INVALID, "instances are NULL");
+    if (int rc = check_instances(b, inst, total, 0)) return rc;
+    CWPB_CUDA(cudaSetDevice(b->device));
+    // segments over the compact copy (non-empty scenes), their regions, and the roots they will get
+    std::vector<int> seg{ 0 }, dst, rootOf(nUpd, -1);
+    for (int i = 0; i < nUpd; i++) {
+        if (counts[i] == 0) continue;
+        const int r0 = scenes[i] * cap, m = counts[i];
+        dst.push_back(r0); seg.push_back(seg.back() + m);
+        rootOf[i] = m == 1 ? r0 : r0 + m - 2;
+    }
+    const int nSeg = (int)dst.size();
+    CWPB_CUDA(cudaEventRecord(b->e0, b->st));
+    const int minus1 = -1;
+    for (int i = 0; i < nUpd; i++)   // the updated scenes are untraceable until their TLAS passes its check
+        CWPB_CUDA(cudaMemcpyAsync(b->sceneRoot + scenes[i], &minus1, sizeof(int), cudaMemcpyHostToDevice, b->st));
+    if (total > 0) {
+        CWPB_CUDA(cudaMemcpyAsync(b->uInst, inst, (size_t)total * sizeof(cwp_instance), cudaMemcpyHostToDevice, b->st));
+        for (int k = 0, at = 0; k < nSeg; k++) {   // the scene's region holds its instances (the traversal reads them there)
+            const int m = seg[k + 1] - seg[k];
+            CWPB_CUDA(cudaMemcpyAsync(b->inst + dst[k], b->uInst + at, (size_t)m * sizeof(cwp_instance), cudaMemcpyDeviceToDevice, b->st));
+            at += m;
+        }
+        CWPB_CUDA(cudaMemcpyAsync(b->dstFirstTlas, dst.data(), (size_t)nSeg * sizeof(int), cudaMemcpyHostToDevice, b->st));
+        CWPB_CUDA(cudaMemcpyAsync(b->segFirstTlas, seg.data(), (size_t)(nSeg + 1) * sizeof(int), cudaMemcpyHostToDevice, b->st));
+        instance_boxes(b->uInst, (int)total, b->meshBox, b->uLo, b->uHi, b->st);
+        if (int rc = b->tlasB.build(b->uLo, b->uHi, total, seg.data(), nSeg, b->st)) return rc;
+        emit_tlas(b->tlasB, (int)total, b->segFirstTlas, nSeg, b->tlas, b->st, b->dstFirstTlas);
+        CWPB_CUDA(cudaGetLastError());
+        if (int rc = check_tlas(b->tlas, (int)total, b->segFirstTlas, nSeg, b->err, b->st, b->dstFirstTlas)) return rc;
+    }
+    for (int i = 0; i < nUpd; i++)
+        if (rootOf[i] >= 0) CWPB_CUDA(cudaMemcpyAsync(b->sceneRoot + scenes[i], &rootOf[i], sizeof(int), cudaMemcpyHostToDevice, b->st));
+    CWPB_CUDA(cudaEventRecord(b->e1, b->st));
+    CWPB_CUDA(cudaEventSynchronize(b->e1));
+    float ms = 0; CWPB_CUDA(cudaEventElapsedTime(&ms, b->e0, b->e1)); b->tlasMs = ms;
     return CWP_OK;
 }
 

@@ -2,7 +2,8 @@
 //
 // Requests wait in a FIFO queue and are admitted into one of max_requests slots when a slot is free and the device has
 // room for the request's image (cudaMemGetInfo, less hbm_reserve). Every step:
-//   1. admission, and when it admitted anything, one TLAS rebuild for all slots (slot k's scene animated to its frame);
+//   1. admission, and when it admitted anything, one TLAS update of the admitted slots (slot k's scene animated to its
+//      frame; every slot owns a fixed TLAS region, so the other slots' TLAS stay untouched);
 //   2. new camera paths for the admitted requests, up to the path capacity, shared evenly between the requests that
 //      still have samples to issue (so small requests are not stuck behind large ones);
 //   3. one scene-tagged closest-hit launch over every queued ray, whatever request it belongs to;
@@ -196,6 +197,40 @@ __global__ void k_serve_shadow_accum(const int* nDev, ShadowQueue sq, const int*
     }
 }
 
+// ---------------- regrouping the queue by request ----------------
+// The continuations of a step come out interleaved across requests; a counting sort by slot (histogram, scan,
+// scatter of the 68-byte entries, counts read on the device) makes the rays a warp fetches belong to one scene, so the
+// traversal of a step touches one scene's TLAS and BLAS at a time instead of all of them at once.
+__global__ void __launch_bounds__(256) k_slot_hist(const int* __restrict__ nDev, const int4* __restrict__ info, int* hist, int nSlots) {
+    extern __shared__ int h[];
+    for (int i = threadIdx.x; i < nSlots; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const int n = *nDev;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) atomicAdd_block(&h[__ldg(&info[k].x)], 1);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nSlots; i += blockDim.x) if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+__global__ void __launch_bounds__(1024) k_slot_scan(int* hist, int* cursor, int nSlots) {   // one block, nSlots <= 1024
+    __shared__ int v[1024];
+    const int i = threadIdx.x, x = i < nSlots ? hist[i] : 0;
+    v[i] = x; __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) { const int y = i >= off ? v[i - off] : 0; __syncthreads(); v[i] += y; __syncthreads(); }
+    if (i < nSlots) cursor[i] = v[i] - x;
+}
+__global__ void __launch_bounds__(256) k_slot_scatter(const int* __restrict__ nDev, RayQueue src, RayQueue dst, int* cursor) {
+    const int n = *nDev, lane = threadIdx.x & 31;
+    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < n; base += gridDim.x * blockDim.x) {
+        const int k = base + lane; const bool ok = k < n;
+        const int4 info = ok ? src.info[k] : make_int4(-1, 0, 0, 0);
+        const unsigned peers = __match_any_sync(0xffffffffu, info.x);
+        const int leader = __ffs(peers) - 1;
+        int pos = 0;
+        if (ok && lane == leader) pos = atomicAdd(&cursor[info.x], __popc(peers));
+        pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(peers & lanes_lt());
+        if (ok) { dst.o[pos] = src.o[k]; dst.d[pos] = src.d[k]; dst.sc[pos] = src.sc[k]; dst.T[pos] = src.T[k]; dst.info[pos] = info; }
+    }
+}
+
 // ---------------- BSDF test kernels ----------------
 __global__ void k_bsdf_eval(const cwp_material* mats, const int* mat, const float3* wo, const float3* wi, const float* eta, int gd, const float2* ux,
                             float4* f, float* pdf, int64_t n) {
@@ -231,9 +266,9 @@ struct cwp_server {
     // scenes: instance descriptors per scene (host)
     std::vector<cwp_instance_desc> desc; std::vector<int> sceneFirst;
     // per slot: request id or -1, its instances (host) for the TLAS rebuild
-    std::vector<int64_t> slotReq; std::vector<std::vector<cwp_instance>> slotInst;
+    std::vector<int64_t> slotReq; std::vector<std::vector<cwp_instance>> slotInst; std::vector<int> admitted;   // slots admitted since the last TLAS update
     SlotParams* dSlots = nullptr; int* slotCnt = nullptr; std::vector<int> hSlotCnt;
-    RayQueue q[2]{}; ShadowQueue sq{}; float4* hits = nullptr; int* hinst = nullptr; int* occ = nullptr; int* cnt = nullptr; int4* dChunks = nullptr;
+    RayQueue q[2]{}; RayQueue qs{}; int* slotBins = nullptr; ShadowQueue sq{}; float4* hits = nullptr; int* hinst = nullptr; int* occ = nullptr; int* cnt = nullptr; int4* dChunks = nullptr;
     int* hcnt = nullptr;   // pinned: [0..1] counts, then slot counters
     int cur = 0; int64_t nCur = 0;
     std::deque<int64_t> pending; std::map<int64_t, ServeRequest> reqs; std::vector<int64_t> completed;
@@ -268,6 +303,7 @@ static int server_create(cwp_batch* b, const cwp_material* mats, int n, const in
     s->O.max_requests = o && o->max_requests > 0 ? o->max_requests : 64;
     s->O.gd_energy = o ? o->gd_energy : 1;
     s->O.hbm_reserve = o && o->hbm_reserve > 0 ? o->hbm_reserve : (1ll << 30);
+    s->O.regroup = o && o->regroup < 0 ? -1 : 1;
     CWPB_CHECK(s->O.max_paths < (1ll << 30), CWP_ERR_INVALID, "max_paths %lld above 2^30", (long long)s->O.max_paths);
     CWPB_CHECK(s->O.max_requests <= 1024, CWP_ERR_INVALID, "max_requests %d above 1024", s->O.max_requests);
     CWPB_CHECK(mats && n >= 1 && meshBase, CWP_ERR_INVALID, "no materials");
@@ -286,6 +322,9 @@ static int server_create(cwp_batch* b, const cwp_material* mats, int n, const in
         rc = alloc((void**)&s->q[k].o, P * 16); if (!rc) rc = alloc((void**)&s->q[k].d, P * 16); if (!rc) rc = alloc((void**)&s->q[k].sc, P * 4);
         if (!rc) rc = alloc((void**)&s->q[k].T, P * 16); if (!rc) rc = alloc((void**)&s->q[k].info, P * 16);
     }
+    if (!rc) { rc = alloc((void**)&s->qs.o, P * 16); if (!rc) rc = alloc((void**)&s->qs.d, P * 16); if (!rc) rc = alloc((void**)&s->qs.sc, P * 4);
+               if (!rc) rc = alloc((void**)&s->qs.T, P * 16); if (!rc) rc = alloc((void**)&s->qs.info, P * 16); }
+    if (!rc) rc = alloc((void**)&s->slotBins, 2 * R * sizeof(int));
     if (!rc) rc = alloc((void**)&s->sq.o, P * 16); if (!rc) rc = alloc((void**)&s->sq.d, P * 16); if (!rc) rc = alloc((void**)&s->sq.sc, P * 4);
     if (!rc) rc = alloc((void**)&s->sq.c, P * 16);
     if (!rc) rc = alloc((void**)&s->hits, P * 16); if (!rc) rc = alloc((void**)&s->hinst, P * 4); if (!rc) rc = alloc((void**)&s->occ, P * 4);
@@ -320,6 +359,10 @@ extern "C" int cwp_server_set_scenes(cwp_server* s, const cwp_instance_desc* des
     const int nMesh = batch_mesh_count(s->batch);
     for (int64_t i = 0; i < n; i++) CWPB_CHECK(desc[i].mesh >= 0 && desc[i].mesh < nMesh, CWP_ERR_INVALID, "descriptor %lld: mesh %d out of range", (long long)i, desc[i].mesh);
     CWPB_CHECK(s->reqs.empty(), CWP_ERR_STATE, "scenes change only while no request is queued or running");
+    int cap = 1;
+    for (int k = 0; k < nScenes; k++) cap = std::max(cap, first[k + 1] - first[k]);
+    // one TLAS region per slot, sized for the largest scene: admissions rebuild only the admitted slots' TLAS
+    if (int rc = cwp_batch_reserve_scenes(s->batch, s->O.max_requests, cap)) return rc;
     s->desc.assign(desc, desc + n); s->sceneFirst.assign(first, first + nScenes + 1);
     return CWP_OK;
 }
@@ -337,14 +380,13 @@ extern "C" int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* i
     return CWP_OK;
 }
 
+// TLAS of the slots admitted since the last update (their previous requests' rays are no longer in flight)
 static int rebuild_tlas(cwp_server* s) {
-    const int R = s->O.max_requests;
-    std::vector<cwp_instance> all; std::vector<int> first(R + 1, 0);
-    for (int k = 0; k < R; k++) {
-        if (s->slotReq[k] >= 0) all.insert(all.end(), s->slotInst[k].begin(), s->slotInst[k].end());
-        first[k + 1] = (int)all.size();
-    }
-    return cwp_batch_set_scenes(s->batch, all.data(), (int64_t)all.size(), first.data(), R);
+    std::vector<cwp_instance> all; std::vector<int> counts;
+    for (int k : s->admitted) { all.insert(all.end(), s->slotInst[k].begin(), s->slotInst[k].end()); counts.push_back((int)s->slotInst[k].size()); }
+    const int rc = cwp_batch_update_scenes(s->batch, s->admitted.data(), (int)s->admitted.size(), all.data(), counts.data());
+    s->admitted.clear();
+    return rc;
 }
 
 static int admit(cwp_server* s, bool& changed) {
@@ -374,7 +416,7 @@ static int admit(cwp_server* s, bool& changed) {
             if (int rc = cwp_instance_from_xform(m, s->desc[i].mesh, &rec)) return rc;
             v.push_back(rec);
         }
-        q.slot = slot; q.admitMs = now_ms(s); s->info.admissions++;
+        q.slot = slot; q.admitMs = now_ms(s); s->info.admissions++; s->admitted.push_back(slot);
         s->slotReq[slot] = q.id; s->hSlotCnt[kSlotCounters * slot + 2] = 0;
         s->pending.pop_front();
         changed = true;
@@ -388,11 +430,13 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
     const double stepStart = now_ms(s);
     bool changed = false;
     if (int rc = admit(s, changed)) return rc;
+    s->info.admit_ms += now_ms(s) - stepStart;
     if (changed) {
         CWPB_CUDA(cudaStreamSynchronize(s->st));
         const double t = now_ms(s);
         if (int rc = rebuild_tlas(s)) return rc;
         s->info.tlas_ms += now_ms(s) - t; s->info.tlas_rebuilds++;
+        cwp_batch_info bi{}; if (cwp_batch_info_of(s->batch, &bi) == CWP_OK) s->info.tlas_device_ms += bi.tlas_build_ms;
     }
     // new camera paths: free capacity shared evenly by the slots with samples left to issue, oldest first
     const int R = s->O.max_requests;
@@ -432,6 +476,14 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         k_serve_shade<<<g, 128, 0, s->st>>>(a);
         CWPB_CUDA(cudaGetLastError());
         CWPB_CUDA(cudaEventRecord(s->ev[3], s->st));
+        if (R > 1 && s->O.regroup >= 0) {   // regroup the next step's rays by request (continuous batching interleaves them)
+            CWPB_CUDA(cudaMemsetAsync(s->slotBins, 0, 2 * R * sizeof(int), s->st));
+            k_slot_hist<<<148 * 4, 256, R * sizeof(int), s->st>>>(s->cnt, out.info, s->slotBins, R);
+            k_slot_scan<<<1, 1024, 0, s->st>>>(s->slotBins, s->slotBins + R, R);
+            k_slot_scatter<<<148 * 8, 256, 0, s->st>>>(s->cnt, out, s->qs, s->slotBins + R);
+            CWPB_CUDA(cudaGetLastError());
+            std::swap(s->q[s->cur ^ 1], s->qs);   // the regrouped copy is the next step's input
+        }
         // shadow rays: count on the device, no host round trip before the any-hit launch
         if (int rc = batch_trace_dev(s->batch, true, s->sq.o, s->sq.d, s->sq.sc, nullptr, s->occ, 0, s->st, s->cnt + 1)) return rc;
         k_serve_shadow_accum<<<148 * 8, 256, 0, s->st>>>(s->cnt + 1, s->sq, s->occ, s->dSlots);

@@ -262,22 +262,24 @@ int emit_wide(const SegBuilder& B, const int* segFirstHost, int nSeg, const floa
 }
 
 // ---------------- TLAS ----------------
-__global__ void k_tlas(const float4* __restrict__ bn, int nInst, const int* __restrict__ segFirst, int nSeg, float4* tlas) {
+// dstFirst (may be NULL = segFirst): where segment s's nodes and instances live in the TLAS / instance arrays, when the
+// build ran over a compact copy of some scenes' instances (incremental updates of fixed per-scene regions)
+__global__ void k_tlas(const float4* __restrict__ bn, int nInst, const int* __restrict__ segFirst, int nSeg, float4* tlas, const int* __restrict__ dstFirst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nInst) return;
     int lo = 0, hi = nSeg - 1;
     while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (segFirst[mid] <= i) lo = mid; else hi = mid - 1; }
-    const int s = lo, f = segFirst[s], m = segFirst[s + 1] - f, base = 2 * f - s, j = i - f;
+    const int s = lo, f = segFirst[s], m = segFirst[s + 1] - f, base = 2 * f - s, j = i - f, d0 = dstFirst ? dstFirst[s] : f;
     int ch[2]; int outNode;
-    if (m == 1) { if (j != 0) return; ch[0] = base; ch[1] = -1; outNode = f; }
-    else { if (j >= m - 1) return; const int b = base + m + j; ch[0] = node_left(bn, b); ch[1] = node_right(bn, b); outNode = f + j; }
+    if (m == 1) { if (j != 0) return; ch[0] = base; ch[1] = -1; outNode = d0; }
+    else { if (j >= m - 1) return; const int b = base + m + j; ch[0] = node_left(bn, b); ch[1] = node_right(bn, b); outNode = d0 + j; }
     for (int q = 0; q < 2; q++) if (ch[q] >= base + 2 * m - 1 || (ch[q] < base && !(q == 1 && ch[q] == -1))) ch[q] = -1;   // outside the scene's region
     float3 l[2], h[2]; int c[2], k[2];
     for (int q = 0; q < 2; q++) {
         if (ch[q] < 0) { l[q] = h[q] = f3(kEmpty, kEmpty, kEmpty); c[q] = -1; k[q] = 0; continue; }
         l[q] = node_lo(bn, ch[q]); h[q] = node_hi(bn, ch[q]);
-        if (ch[q] < base + m) { c[q] = node_left(bn, ch[q]); k[q] = 1; }   // a leaf: the instance
-        else { c[q] = f + (ch[q] - base - m); k[q] = 0; }
+        if (ch[q] < base + m) { c[q] = d0 + (node_left(bn, ch[q]) - f); k[q] = 1; }   // a leaf: the instance
+        else { c[q] = d0 + (ch[q] - base - m); k[q] = 0; }
     }
     float4* o = tlas + 4 * (size_t)outNode;
     o[0] = make_float4(l[0].x, h[0].x, l[0].y, h[0].y);
@@ -285,8 +287,8 @@ __global__ void k_tlas(const float4* __restrict__ bn, int nInst, const int* __re
     o[2] = make_float4(l[0].z, h[0].z, l[1].z, h[1].z);
     o[3] = make_float4(__int_as_float(c[0]), __int_as_float(c[1]), __int_as_float(k[0]), __int_as_float(k[1]));
 }
-void emit_tlas(const SegBuilder& B, int nInst, const int* segFirstDev, int nSeg, float4* tlas, cudaStream_t st) {
-    if (nInst > 0) k_tlas<<<(nInst + 127) / 128, 128, 0, st>>>(B.nodes, nInst, segFirstDev, nSeg, tlas);
+void emit_tlas(const SegBuilder& B, int nInst, const int* segFirstDev, int nSeg, float4* tlas, cudaStream_t st, const int* dstFirstDev) {
+    if (nInst > 0) k_tlas<<<(nInst + 127) / 128, 128, 0, st>>>(B.nodes, nInst, segFirstDev, nSeg, tlas, dstFirstDev);
 }
 
 __global__ void k_inst_boxes(const cwp_instance* __restrict__ inst, int n, const float4* __restrict__ meshBox, float4* lo, float4* hi) {
@@ -347,20 +349,21 @@ __global__ void k_check_wide(int W, const float4* __restrict__ nodes, int64_t nN
     }
     if (!ok) atomicOr(bad, 1);
 }
-__global__ void k_check_tlas(const float4* __restrict__ tlas, int nInst, const int* __restrict__ segFirst, int nSeg, int* bad) {
+__global__ void k_check_tlas(const float4* __restrict__ tlas, int nInst, const int* __restrict__ segFirst, int nSeg, int* bad, const int* __restrict__ dstFirst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nInst) return;
     int lo = 0, hi = nSeg - 1;
     while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (segFirst[mid] <= i) lo = mid; else hi = mid - 1; }
-    const int f = segFirst[lo], m = segFirst[lo + 1] - f, j = i - f;
+    const int m = segFirst[lo + 1] - segFirst[lo], j = i - segFirst[lo], f = dstFirst ? dstFirst[lo] : segFirst[lo];
     if (j >= (m == 1 ? 1 : m - 1)) return;   // unused slot of the scene's region
-    const float4 mt = tlas[4 * (size_t)i + 3];
+    const int node = f + j;
+    const float4 mt = tlas[4 * (size_t)node + 3];
     const int c[2] = { __float_as_int(mt.x), __float_as_int(mt.y) }, k[2] = { __float_as_int(mt.z), __float_as_int(mt.w) };
     bool ok = true;
     for (int q = 0; q < 2; q++) {
         if (c[q] == -1) continue;
         if (k[q] > 0) ok &= k[q] == 1 && c[q] >= f && c[q] < f + m;           // an instance of this scene
-        else ok &= k[q] == 0 && c[q] >= f && c[q] < i;                        // an inner node of this scene, built before its parent
+        else ok &= k[q] == 0 && c[q] >= f && c[q] < node;                     // an inner node of this scene, built before its parent
     }
     if (!ok) atomicOr(bad, 1);
 }
@@ -373,9 +376,9 @@ int check_wide(const WideLayout& w, int64_t nTris, int* dBad, cudaStream_t st) {
     CWPB_CHECK(h == 0, CWP_ERR_INVALID, "width-%d layout has an out-of-range child or triangle reference", w.width);
     return CWP_OK;
 }
-int check_tlas(const float4* tlas, int nInst, const int* segFirstDev, int nSeg, int* dBad, cudaStream_t st) {
+int check_tlas(const float4* tlas, int nInst, const int* segFirstDev, int nSeg, int* dBad, cudaStream_t st, const int* dstFirstDev) {
     CWPB_CUDA(cudaMemsetAsync(dBad, 0, sizeof(int), st));
-    if (nInst > 0) k_check_tlas<<<(nInst + 127) / 128, 128, 0, st>>>(tlas, nInst, segFirstDev, nSeg, dBad);
+    if (nInst > 0) k_check_tlas<<<(nInst + 127) / 128, 128, 0, st>>>(tlas, nInst, segFirstDev, nSeg, dBad, dstFirstDev);
     int h = 0;
     CWPB_CUDA(cudaMemcpyAsync(&h, dBad, sizeof(int), cudaMemcpyDeviceToHost, st));
     CWPB_CUDA(cudaStreamSynchronize(st));

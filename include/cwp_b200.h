@@ -277,6 +277,14 @@ void cwp_batch_destroy(cwp_batch* b);
  * scene's TLAS (BVH2 over instance world boxes) on the device in one H-PLOC launch; call again each frame when the
  * transforms move. Synchronous. */
 int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int64_t n_inst, const int32_t* scene_first, int32_t n_scenes);
+/* Incremental form for scenes that change one at a time (a serving loop's slots): cwp_batch_reserve_scenes lays out
+ * n_scenes empty scenes with room for `cap` instances each (scene s owns instances [s * cap, s * cap + cap)); then
+ * cwp_batch_update_scenes replaces the instances of the n listed scenes (distinct) with counts[i] <= cap instances
+ * each, taken in order from inst, and rebuilds only their TLAS, in one H-PLOC launch; the other scenes' TLAS stay as
+ * they are and traceable. An empty scene's rays miss. Rays of the updated scenes must not be in flight. Synchronous.
+ * cwp_batch_set_scenes returns the batch to the packed form. */
+int cwp_batch_reserve_scenes(cwp_batch* b, int32_t n_scenes, int32_t cap);
+int cwp_batch_update_scenes(cwp_batch* b, const int32_t* scenes, int32_t n, const cwp_instance* inst, const int32_t* counts);
 /* One persistent launch over a queue of rays tagged with scene ids (d_scene, int32 per ray). any_hit: d_hits may be
  * NULL and d_inst receives the occluding instance or -1. */
 int cwp_batch_trace(cwp_batch* b, int32_t any_hit, const float* d_o, const float* d_d, const int32_t* d_scene, float* d_hits,
@@ -321,7 +329,8 @@ typedef struct cwp_server_options {
     int32_t gd_energy;     /* glossy-diffuse energy compensation (default 1, as the reference's --gd_energy) */
     int64_t hbm_reserve;   /* device bytes that admission leaves free (default 1 GiB) */
     int32_t device;
-    int32_t reserved[5];
+    int32_t regroup;       /* sort each step's continuations by request before tracing: 1 on, -1 off, 0 default (on) */
+    int32_t reserved[4];
 } cwp_server_options;
 
 typedef struct cwp_request {
@@ -359,6 +368,8 @@ double cwp_server_clock_ms(const cwp_server* s);
 typedef struct cwp_server_info {
     int64_t steps, rays, shadow_rays, admissions, tlas_rebuilds;
     double closest_ms, shade_ms, shadow_ms, raygen_ms, tlas_ms, step_ms;   /* device time per phase (CUDA events), wall time of the steps */
+    double admit_ms;         /* host time of admissions (instance animation, image allocation) */
+    double tlas_device_ms;   /* device time of the TLAS updates inside tlas_ms (which is their wall time) */
 } cwp_server_info;
 int cwp_server_info_of(const cwp_server* s, cwp_server_info* out);
 /* Device-side BSDF of a material table for n (material, wo, wi) triples in local frames (wo.z > 0): f (float4) and
@@ -374,6 +385,13 @@ int cwp_bsdf_sample_batch(const cwp_material* mats, int32_t n_mats, const int32_
  * (io/image.cpp tonemapSRGB8: divide by spp, clip, sRGB OETF); 1 = Reinhard; 2 = ACES fit; exposure in EV.
  * ------------------------------------------------------------------------------------------------------------------ */
 int cwp_display(const float* d_accum, uint8_t* d_rgba, int64_t n, int32_t spp, float exposure_ev, int32_t mode, void* stream);
+
+/* ------------------------------------------------------------------------------------------------------------------
+ * On-chip read bandwidth of a device, for the traversal kernels' roofline (not in the reference, whose node and
+ * triangle reads are served from L2): `bytes` (1..96 MiB, L2-resident) read `reps` times per launch with 16-byte
+ * L2-cached loads from every SM; *gbs = the best of five timed launches after a warm-up, in GB/s.
+ * ------------------------------------------------------------------------------------------------------------------ */
+int cwp_measure_l2_read(int64_t bytes, int32_t reps, int32_t device, double* gbs);
 
 /* ------------------------------------------------------------------------------------------------------------------
  * Camera and parameter helpers. Replace lookAtC2W / focalFromHfov / makeCamera (scene/camera.cpp:7-23) and the

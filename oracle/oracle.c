@@ -540,6 +540,11 @@ typedef struct {
 
 static V3 a3(const float* a) { return v3(a[0], a[1], a[2]); }
 
+/* Traversal work of orc_render, for the on-chip roofline: [0] node visits and [1] triangle tests of closest-hit rays,
+ * [2] and [3] of shadow rays. orc_render_stats(1, NULL) zeroes and enables the counters; (0, out) reads and disables. */
+static long long g_render_stats[4]; static int g_render_stats_on;
+void orc_render_stats(int on, long long* out) { if (out) memcpy(out, g_render_stats, sizeof g_render_stats); memset(g_render_stats, 0, sizeof g_render_stats); g_render_stats_on = on; }
+
 /* Renders samples [s_base, s_base + spp) of pixels [pix0, pix1) with `bounces` as the frame's depth limit
  * (depths 0 .. bounces + 1 are traced) and adds radiance sums to accum (float4 per pixel). Each path is traced
  * to completion before the next; the per-vertex decisions and sample dimensions are those of the wavefront loop.
@@ -558,9 +563,10 @@ void orc_render(const OrcParams* P, int variant, int tri, const float* nodes, co
             float tmin = P->near_clip;
             for (int depth = 0; depth < depths; depth++) {
                 nc++;
-                float t = 1e30f, u = 0.f, vv = 0.f; int h = -1;
-                if (variant == 2) trav2((const V4*)nodes, (const V4*)tv, o, d, tmin, 0, tri, &t, &h, &u, &vv, NULL);
-                else trav8((const V4*)nodes, (const V4*)tv, o, d, tmin, 0, tri, &t, &h, &u, &vv, NULL);
+                float t = 1e30f, u = 0.f, vv = 0.f; int h = -1; Stats cs = {0, 0};
+                if (variant == 2) trav2((const V4*)nodes, (const V4*)tv, o, d, tmin, 0, tri, &t, &h, &u, &vv, g_render_stats_on ? &cs : NULL);
+                else trav8((const V4*)nodes, (const V4*)tv, o, d, tmin, 0, tri, &t, &h, &u, &vv, g_render_stats_on ? &cs : NULL);
+                g_render_stats[0] += cs.nodes; g_render_stats[1] += cs.tris;
                 if (h < 0) { V3 c = mulv(T, a3(P->sky)); accum[4 * pix] += c.x; accum[4 * pix + 1] += c.y; accum[4 * pix + 2] += c.z; break; }
                 if (depth > P->max_b) break;
                 V3 p = add(o, muls(d, t));
@@ -576,9 +582,10 @@ void orc_render(const OrcParams* P, int variant, int tri, const float* nodes, co
                 if (cl > 0.f && dot3(ng, l) > 0.f) {
                     V3 contrib = muls(mulv(mulv(T, alb), a3(P->sun_e)), cl * 0.31830989f);
                     ns++;
-                    float st = 1e30f, su, sv; int sh = -1, occ;
-                    if (variant == 2) occ = trav2((const V4*)nodes, (const V4*)tv, po, l, 0.f, 1, tri, &st, &sh, &su, &sv, NULL);
-                    else occ = trav8((const V4*)nodes, (const V4*)tv, po, l, 0.f, 1, tri, &st, &sh, &su, &sv, NULL);
+                    float st = 1e30f, su, sv; int sh = -1, occ; Stats ss = {0, 0};
+                    if (variant == 2) occ = trav2((const V4*)nodes, (const V4*)tv, po, l, 0.f, 1, tri, &st, &sh, &su, &sv, g_render_stats_on ? &ss : NULL);
+                    else occ = trav8((const V4*)nodes, (const V4*)tv, po, l, 0.f, 1, tri, &st, &sh, &su, &sv, g_render_stats_on ? &ss : NULL);
+                    g_render_stats[2] += ss.nodes; g_render_stats[3] += ss.tris;
                     if (occ == 0) { accum[4 * pix] += contrib.x; accum[4 * pix + 1] += contrib.y; accum[4 * pix + 2] += contrib.z; }
                 }
                 V3 nd = cos_hemi(nsh, orc_rng(pix, smp, dr, 0, P->seed), orc_rng(pix, smp, dr, 1, P->seed));

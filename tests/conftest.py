@@ -55,6 +55,8 @@ def _load_oracle():
     L.orc_bsdf_eval.argtypes = [C.c_void_p] * 5 + [C.c_int] + [C.c_void_p] * 3 + [C.c_long]
     L.orc_bsdf_sample.restype = None
     L.orc_bsdf_sample.argtypes = [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 6 + [C.c_long]
+    L.orc_render_stats.restype = None
+    L.orc_render_stats.argtypes = [C.c_int, C.c_void_p]
     L.orc_render_request.restype = C.c_long
     L.orc_render_request.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
     L.orc_half_round.restype = C.c_double
@@ -164,6 +166,14 @@ class Oracle:
         self.L.orc_render(C.addressof(params), variant, tri, bvh.nodes.ctypes.data, tv.ctypes.data, bvh.tris.ctypes.data, alb.ctypes.data,
                           bounces, spp, s_base, pix0, w * h if pix1 is None else pix1, acc.ctypes.data, rc.ctypes.data)
         return acc, rc
+
+    def render_work(self, params, variant, tri, bvh, bounces, spp, pix0, pix1):
+        """Traversal work of orc_render over pixels [pix0, pix1): (ray counts [closest, shadow], [closest node visits,
+        closest triangle tests, shadow node visits, shadow triangle tests])."""
+        self.L.orc_render_stats(1, None)
+        _, rc = self.render(params, variant, tri, bvh, bounces, spp, 0, pix0, pix1)
+        st = np.zeros(4, np.int64); self.L.orc_render_stats(0, st.ctypes.data)
+        return rc, st
 
 
 @pytest.fixture(scope="session")

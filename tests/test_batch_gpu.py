@@ -218,3 +218,45 @@ def test_degenerate_segments(gpu, cwp, oracle):
         assert np.array_equal(h.view(np.uint32), ho.view(np.uint32)) and np.array_equal(hi, hio)
         assert np.all(hi[sc == 0] == -1) and (hi[sc == 1] >= 0).any() and (hi[sc == 2] >= 0).any()
     b.trace(0, 0, 0, 0, 0, 0)   # n = 0: nothing to do, no error
+
+
+def test_incremental_scene_updates_match_packed(gpu, cwp):
+    """Fixed per-scene regions updated a few scenes at a time trace exactly like the packed form built over the same
+    instances (hits bit for bit, instance indices moved into the scene's region); scenes left out of an update keep
+    their TLAS; an emptied scene's rays miss."""
+    meshes, xf, mesh_of, first = cwp.batch_scenes(n_scenes=3, seed=7, tris=(200, 5000), instances=(1, 40), blas_per_scene=(1, 3))
+    first = np.asarray(first, np.int32)
+    inst = cwp.instances(xf, mesh_of)
+    b = cwp.Batch(meshes)
+    b.set_scenes(inst, first)
+    o, d, sc = cwp.batch_rays(xf, first, 2000, seed=8)
+    sc[::50] = 3   # a scene that is empty (incremental) or absent (packed): misses either way
+    packed, pinst = trace(gpu, b, o, d, sc)
+    assert (pinst >= 0).any()
+
+    def part(scenes):
+        lst = [inst[i] for s in scenes for i in range(first[s], first[s + 1])]
+        return (cwp.Instance * len(lst))(*lst), [int(first[s + 1] - first[s]) for s in scenes]
+
+    def region(pi, cap):
+        s = np.searchsorted(first, np.maximum(pi, 0), side="right") - 1
+        return np.where(pi >= 0, s * cap + (pi - first[s]), -1)
+
+    cap = int(np.diff(first).max()) + 3
+    b.reserve_scenes(4, cap)
+    h0, _ = trace(gpu, b, o, d, sc)
+    assert np.all(h0[:, 3].view(np.int32) == -1)   # every scene empty
+    arr, cnt = part([2, 0]); b.update_scenes([2, 0], arr, cnt)
+    arr, cnt = part([1]); b.update_scenes([1], arr, cnt)   # scenes 0 and 2 untouched
+    h1, i1 = trace(gpu, b, o, d, sc)
+    assert np.array_equal(h1.view(np.uint32), packed.view(np.uint32)) and np.array_equal(i1, region(pinst, cap))
+    assert b.info().n_instances == 4 * cap
+    b.update_scenes([0], None, [0])   # scene 0 emptied
+    h2, i2 = trace(gpu, b, o, d, sc)
+    assert np.all(h2[sc == 0, 3].view(np.int32) == -1)
+    keep = sc != 0
+    assert np.array_equal(h2[keep].view(np.uint32), packed[keep].view(np.uint32))
+    with pytest.raises(Exception):
+        b.update_scenes([1, 1], None, [0, 0])   # listed twice
+    with pytest.raises(Exception):
+        arr, cnt = part([1]); b.update_scenes([4], arr, cnt)   # out of range

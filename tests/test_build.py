@@ -132,3 +132,20 @@ def test_spatial_splits_same_hits_fewer_visits(cwp, oracle, variant):
     assert s1[0] < s0[0]
     occ0 = oracle.trace(variant, 1, True, b0.nodes, b0.woop, o, d); occ1 = oracle.trace(variant, 1, True, b1.nodes, b1.woop, o, d)
     assert np.array_equal(occ0 >= 0, occ1 >= 0)
+
+
+def test_frame_work_counters(cwp, oracle):
+    """The oracle's frame counters (the on-chip roofline's algorithmic bytes) count the same rays as the frame and do
+    not change its image; the spatial-split tree needs fewer node visits per closest ray for the same frame."""
+    mesh = cwp.Mesh.box_field(300, 1)
+    p = cwp.frame_params(mesh, 32, 32, bounces=2)
+    b0 = cwp.Bvh(mesh, variant=8, bins=32, leaf=1)
+    b1 = cwp.Bvh(mesh, variant=8, bins=32, leaf=1, spatial=1e-3)
+    acc, rc = oracle.render(p, 8, 1, b0, 2, 4, 0, 0, 1024)
+    rc0, st0 = oracle.render_work(p, 8, 1, b0, 2, 4, 0, 1024)
+    assert np.array_equal(rc, rc0) and rc0[0] > 0 and rc0[1] > 0
+    assert np.all(st0 > 0) and st0[0] >= rc0[0] and st0[2] >= rc0[1]   # at least the root per ray
+    acc2, _ = oracle.render(p, 8, 1, b0, 2, 4, 0, 0, 1024)            # counters off again: same image
+    assert np.array_equal(acc, acc2)
+    rc1, st1 = oracle.render_work(p, 8, 1, b1, 2, 4, 0, 1024)
+    assert st1[0] / rc1[0] < st0[0] / rc0[0]

@@ -60,6 +60,13 @@ def test_version_and_error_string(cwp):
     assert rc == cwp.ERR_INVALID and b"out of range" in L.cwp_last_error()
 
 
+def test_l2_probe_arguments_checked_before_gpu(cwp):
+    L = cwp.lib(); g = C.c_double()
+    for nbytes, reps in ((100, 1), ((32 << 20) + 8, 1), (1 << 30, 1), (32 << 20, 0)):
+        assert L.cwp_measure_l2_read(nbytes, reps, 0, C.byref(g)) == cwp.ERR_INVALID
+    assert L.cwp_measure_l2_read(32 << 20, 1, 0, None) == cwp.ERR_INVALID
+
+
 def _scene_buffers(nodes, stride, tris):
     s = cwp_mod().SceneBuffers()
     s.nodes, s.n_node_float4, s.node_stride = nodes.ctypes.data, len(nodes), stride

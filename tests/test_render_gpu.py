@@ -132,3 +132,10 @@ def test_display_transform_matches_png_transform(gpu, cwp):
         m = out.cpu().numpy()[:, 0].astype(int); lin = acc[:, 0]
         o = np.argsort(lin)
         assert np.all(np.diff(m[o]) >= -1)
+
+
+def test_l2_probe(gpu, cwp):
+    """The on-chip bandwidth probe (the traversal roofline's denominator) reports more than HBM can deliver and less
+    than an implausible figure."""
+    g = cwp.measure_l2_read()
+    assert 3000.0 < g < 200000.0
