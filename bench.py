@@ -146,6 +146,21 @@ def cpu_frame_sample(cwp, wl, mesh, bvh, variant, seconds=12.0):
                 sample=f"{npix} pixels x {wl['spp']} spp of the {wl['w']}x{wl['h']} frame ({rays} closest+shadow rays in {spent:.2f} s)")
 
 
+# DRAM bytes per launch of the frame kernels from one full-size ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum, one pass, every launch of one frame; summary and command in profiles/frame512_dram_traffic.txt).
+# Valid only for the configuration it was captured on.
+FRAME512_TRAFFIC = {"k_trace_shade": 2599.4e6, "k_shadow": 530.8e6}
+
+
+def frame_traffic(args, wl, variant, kernel):
+    captured = (args.workload == "frame512" and variant == 8 and args.spatial == 1e-3 and not args.spp and not args.batch and args.sort == 0
+                and args.graph == 1 and args.traversal == 0 and args.bins == 32)
+    if not captured or kernel not in FRAME512_TRAFFIC:
+        return {"traffic": None}
+    return {"traffic": FRAME512_TRAFFIC[kernel], "traffic_unit": "bytes per launch",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size capture (profiles/frame512_dram_traffic.txt)"}
+
+
 NODE_BYTES = {2: 64, 4: 128, 8: 80}
 TRI_BYTES = 48   # Woop rows, an upper bound (the test reads row 2 first and rows 0/1 only past the t check)
 
@@ -574,7 +589,7 @@ def main():
                         "note": "scene uploaded once at init; each step renders and reads the w*h float4 accumulation buffer back into pinned host memory"},
                    gpu_launches=args.steps * (spp // K) * (2 + 2 * depths),
                    roofline={"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                             "peak_kind": peak_kind, "traffic": None,
+                             "peak_kind": peak_kind, **frame_traffic(args, wl, variant, dom),
                              "algorithmic": f"{STATE_BYTES} B of path state per queued ray read and per continuation/shadow ray written"})
         onchip = dict(kind="frame", closest=float(c_tot.sum()), shadow=float(s_tot.sum()), closest_ms=float(tms.sum()), shadow_ms=float(sms.sum()))
         r.close()

@@ -123,7 +123,8 @@ class RequestStats(C.Structure):
 class ServerInfo(C.Structure):
     _fields_ = [("steps", C.c_int64), ("rays", C.c_int64), ("shadow_rays", C.c_int64), ("admissions", C.c_int64), ("tlas_rebuilds", C.c_int64),
                 ("closest_ms", C.c_double), ("shade_ms", C.c_double), ("shadow_ms", C.c_double), ("raygen_ms", C.c_double), ("tlas_ms", C.c_double),
-                ("step_ms", C.c_double), ("admit_ms", C.c_double), ("tlas_device_ms", C.c_double)]
+                ("step_ms", C.c_double), ("admit_ms", C.c_double), ("tlas_device_ms", C.c_double),
+                ("accum_ms", C.c_double)]
 
 
 # every exported symbol of the C ABI with its ctypes signature (restype, argtypes)

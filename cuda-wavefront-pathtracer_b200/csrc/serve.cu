@@ -270,13 +270,15 @@ struct cwp_server {
     SlotParams* dSlots = nullptr; int* slotCnt = nullptr; std::vector<int> hSlotCnt;
     RayQueue q[2]{}; RayQueue qs{}; int* slotBins = nullptr; ShadowQueue sq{}; float4* hits = nullptr; int* hinst = nullptr; int* occ = nullptr; int* cnt = nullptr; int4* dChunks = nullptr;
     int* hcnt = nullptr;   // pinned: [0..1] counts, then slot counters
+    SlotParams* hSlots = nullptr; int4* hChunks = nullptr; bool slotsDirty = false;   // pinned mirrors of dSlots and dChunks
+    cudaMemPool_t pool = nullptr;   // request images: freed memory stays in the pool for the next admissions
     int cur = 0; int64_t nCur = 0;
     std::deque<int64_t> pending; std::map<int64_t, ServeRequest> reqs; std::vector<int64_t> completed;
     int64_t nextId = 1;
     cudaStream_t st = nullptr;
     std::chrono::steady_clock::time_point t0;
     std::vector<void*> allocs;
-    cudaEvent_t ev[6] = {};   // raygen start, closest start, shade start, shadow start, shadow end, (spare)
+    cudaEvent_t ev[6] = {};   // raygen start, closest start, shade start, shadow start, shadow end, accumulation start
     cwp_server_info info{};
 };
 
@@ -290,8 +292,11 @@ extern "C" void cwp_server_destroy(cwp_server* s) {
     if (s->st) cudaStreamSynchronize(s->st);
     for (auto& kv : s->reqs) if (kv.second.accum) cudaFreeAsync(kv.second.accum, s->st);
     if (s->st) cudaStreamSynchronize(s->st);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     for (void* p : s->allocs) cudaFree(p);
     if (s->hcnt) cudaFreeHost(s->hcnt);
+    if (s->hSlots) cudaFreeHost(s->hSlots);
+    if (s->hChunks) cudaFreeHost(s->hChunks);
     for (cudaEvent_t e : s->ev) if (e) cudaEventDestroy(e);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;
@@ -334,6 +339,15 @@ static int server_create(cwp_batch* b, const cwp_material* mats, int n, const in
     if (!rc) rc = alloc((void**)&s->dChunks, (R + 1) * sizeof(int4));
     if (rc) return rc;
     CWPB_CUDA(cudaMallocHost(&s->hcnt, (4 + R * kSlotCounters) * sizeof(int)));
+    CWPB_CUDA(cudaMallocHost(&s->hSlots, R * sizeof(SlotParams))); memset(s->hSlots, 0, R * sizeof(SlotParams));
+    CWPB_CUDA(cudaMallocHost(&s->hChunks, (R + 1) * sizeof(int4)));
+    {
+        cudaMemPoolProps pp{};
+        pp.allocType = cudaMemAllocationTypePinned; pp.location.type = cudaMemLocationTypeDevice; pp.location.id = s->device;
+        CWPB_CUDA(cudaMemPoolCreate(&s->pool, &pp));
+        uint64_t keep = UINT64_MAX;   // never hand freed images back to the driver between steps
+        CWPB_CUDA(cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     CWPB_CUDA(cudaMemcpy(s->mats, mats, (size_t)n * sizeof(cwp_material), cudaMemcpyHostToDevice));
     CWPB_CUDA(cudaMemcpy(s->meshMat, meshBase, (size_t)nMesh * sizeof(int), cudaMemcpyHostToDevice));
     CWPB_CUDA(cudaMemset(s->slotCnt, 0, R * kSlotCounters * sizeof(int)));
@@ -389,24 +403,41 @@ static int rebuild_tlas(cwp_server* s) {
     return rc;
 }
 
+// device bytes an admission may use: free memory plus what the image pool holds unused, less the reserve
+static int admission_budget(cwp_server* s, int64_t& avail) {
+    size_t freeB = 0, totalB = 0;
+    CWPB_CUDA(cudaMemGetInfo(&freeB, &totalB));
+    uint64_t reserved = 0, used = 0;
+    CWPB_CUDA(cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    CWPB_CUDA(cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    avail = (int64_t)freeB + (int64_t)(reserved > used ? reserved - used : 0) - s->O.hbm_reserve;
+    return CWP_OK;
+}
+
 static int admit(cwp_server* s, bool& changed) {
     changed = false;
+    if (s->pending.empty()) return CWP_OK;
+    int64_t avail = 0;
+    bool queried = false;
     while (!s->pending.empty()) {
         int slot = -1;
         for (int k = 0; k < s->O.max_requests; k++) if (s->slotReq[k] < 0) { slot = k; break; }
         if (slot < 0) break;
+        if (!queried) { if (int rc = admission_budget(s, avail)) return rc; queried = true; }   // one query per step
         ServeRequest& q = s->reqs[s->pending.front()];
-        const size_t bytes = (size_t)q.r.cam.w * q.r.cam.h * sizeof(float4);
-        size_t freeB = 0, totalB = 0;
-        CWPB_CUDA(cudaMemGetInfo(&freeB, &totalB));
-        if (freeB < bytes + (size_t)s->O.hbm_reserve) break;   // admission by free device memory
-        CWPB_CUDA(cudaMallocAsync((void**)&q.accum, bytes, s->st));   // stream-ordered: no device-wide synchronisation
-        CWPB_CUDA(cudaMemsetAsync(q.accum, 0, bytes, s->st));
-        SlotParams P{};
+        const int64_t bytes = (int64_t)q.r.cam.w * q.r.cam.h * (int64_t)sizeof(float4);
+        if (avail < bytes) break;   // admission by free device memory
+        const cudaError_t e = cudaMallocFromPoolAsync((void**)&q.accum, (size_t)bytes, s->pool, s->st);   // stream-ordered, pooled
+        if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); q.accum = nullptr; break; }   // fragmentation: wait for frees
+        CWPB_CUDA(e);
+        avail -= bytes;
+        CWPB_CUDA(cudaMemsetAsync(q.accum, 0, (size_t)bytes, s->st));
+        SlotParams& P = s->hSlots[slot];
+        P = SlotParams{};
         P.cam = q.r.cam; P.sunTo = f3(q.r.sun_to[0], q.r.sun_to[1], q.r.sun_to[2]); P.sunE = f3(q.r.sun_e[0], q.r.sun_e[1], q.r.sun_e[2]);
         P.sky = f3(q.r.sky[0], q.r.sky[1], q.r.sky[2]); P.sunCos = q.r.sun_cos; P.eps = q.r.eps; P.seed = q.r.seed; P.maxDepth = q.r.max_depth;
         P.N = q.r.cam.w * q.r.cam.h; P.accum = q.accum;
-        CWPB_CUDA(cudaMemcpyAsync(s->dSlots + slot, &P, sizeof(P), cudaMemcpyHostToDevice, s->st));
+        s->slotsDirty = true;
         CWPB_CUDA(cudaMemsetAsync(s->slotCnt + kSlotCounters * slot, 0, kSlotCounters * sizeof(int), s->st));
         // the scene's instances at the request's frame
         std::vector<cwp_instance>& v = s->slotInst[slot]; v.clear();
@@ -420,6 +451,10 @@ static int admit(cwp_server* s, bool& changed) {
         s->slotReq[slot] = q.id; s->hSlotCnt[kSlotCounters * slot + 2] = 0;
         s->pending.pop_front();
         changed = true;
+    }
+    if (s->slotsDirty) {   // every admitted slot's parameters in one copy (the previous step's copies have completed)
+        CWPB_CUDA(cudaMemcpyAsync(s->dSlots, s->hSlots, (size_t)s->O.max_requests * sizeof(SlotParams), cudaMemcpyHostToDevice, s->st));
+        s->slotsDirty = false;
     }
     return CWP_OK;
 }
@@ -444,20 +479,20 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
     for (int k = 0; k < R; k++) if (s->slotReq[k] >= 0) { const ServeRequest& q = s->reqs[s->slotReq[k]]; if (q.issued < q.total) needy.push_back(k); }
     std::sort(needy.begin(), needy.end(), [&](int a, int b) { return s->reqs[s->slotReq[a]].admitMs < s->reqs[s->slotReq[b]].admitMs; });
     int64_t freeCap = s->O.max_paths - s->nCur;
-    std::vector<int4> chunks; int64_t added = 0;
+    int nChunks = 0; int64_t added = 0;
     for (size_t i = 0; i < needy.size() && freeCap > 0; i++) {
         ServeRequest& q = s->reqs[s->slotReq[needy[i]]];
         const int64_t share = freeCap / (int64_t)(needy.size() - i);   // what is left split over the requests not yet served
         const int64_t take = std::min(q.total - q.issued, std::max<int64_t>(share, 1));
         if (take <= 0) continue;
-        chunks.push_back(make_int4(needy[i], (int)q.issued, (int)take, (int)added));
+        s->hChunks[nChunks++] = make_int4(needy[i], (int)q.issued, (int)take, (int)added);
         q.issued += take; added += take; freeCap -= take;
     }
     RayQueue& in = s->q[s->cur]; RayQueue& out = s->q[s->cur ^ 1];
     CWPB_CUDA(cudaEventRecord(s->ev[0], s->st));
     if (added > 0) {
-        CWPB_CUDA(cudaMemcpyAsync(s->dChunks, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice, s->st));
-        k_serve_raygen<<<(unsigned)((added + 255) / 256), 256, 0, s->st>>>(s->dChunks, (int)chunks.size(), (int)added, s->dSlots, in, (int)s->nCur);
+        CWPB_CUDA(cudaMemcpyAsync(s->dChunks, s->hChunks, (size_t)nChunks * sizeof(int4), cudaMemcpyHostToDevice, s->st));
+        k_serve_raygen<<<(unsigned)((added + 255) / 256), 256, 0, s->st>>>(s->dChunks, nChunks, (int)added, s->dSlots, in, (int)s->nCur);
         CWPB_CUDA(cudaGetLastError());
     }
     const int64_t n = s->nCur + added;
@@ -465,6 +500,7 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
     CWPB_CUDA(cudaEventRecord(s->ev[1], s->st));
     CWPB_CUDA(cudaEventRecord(s->ev[2], s->st));
     CWPB_CUDA(cudaEventRecord(s->ev[3], s->st));
+    CWPB_CUDA(cudaEventRecord(s->ev[5], s->st));
     if (n > 0) {
         if (int rc = batch_trace_dev(s->batch, false, in.o, in.d, in.sc, s->hits, s->hinst, n, s->st)) return rc;
         CWPB_CUDA(cudaEventRecord(s->ev[2], s->st));
@@ -486,6 +522,7 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         }
         // shadow rays: count on the device, no host round trip before the any-hit launch
         if (int rc = batch_trace_dev(s->batch, true, s->sq.o, s->sq.d, s->sq.sc, nullptr, s->occ, 0, s->st, s->cnt + 1)) return rc;
+        CWPB_CUDA(cudaEventRecord(s->ev[5], s->st));
         k_serve_shadow_accum<<<148 * 8, 256, 0, s->st>>>(s->cnt + 1, s->sq, s->occ, s->dSlots);
         CWPB_CUDA(cudaGetLastError());
     }
@@ -498,7 +535,8 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         float a = 0, b = 0, c = 0, d = 0;
         CWPB_CUDA(cudaEventElapsedTime(&a, s->ev[0], s->ev[1])); CWPB_CUDA(cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
         CWPB_CUDA(cudaEventElapsedTime(&c, s->ev[2], s->ev[3])); CWPB_CUDA(cudaEventElapsedTime(&d, s->ev[3], s->ev[4]));
-        s->info.raygen_ms += a; s->info.closest_ms += b; s->info.shade_ms += c; s->info.shadow_ms += d;
+        float e = 0; CWPB_CUDA(cudaEventElapsedTime(&e, s->ev[5], s->ev[4]));
+        s->info.raygen_ms += a; s->info.closest_ms += b; s->info.shade_ms += c; s->info.shadow_ms += d; s->info.accum_ms += e;
         s->info.steps++; s->info.rays += n; s->info.shadow_rays += nShadow;
     }
     if ((s->info.steps & 63) == 0 || nNext == 0) { if (int rc = cwp_batch_status(s->batch)) return rc; }   // traversal bounds: checked every 64 steps and when the queue drains

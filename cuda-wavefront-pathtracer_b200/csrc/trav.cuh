@@ -47,15 +47,15 @@ __device__ __forceinline__ bool leaf_hit(const float4* __restrict__ tv, int firs
             if (v < 0.f || u + v > 1.f) continue;
             float tt = fdot(e2, qv) * inv;
             if (tt > tmin && tt < hitT) { hitT = tt; hitTri = t; hu = u; hv = v; if (ANY) return true; }
-        } else {          // Woop: plane row 2 first (distance), rows 0 and 1 only when the distance is in range
-            float4 r2 = ld4(tv + 3 * t + 2);
+        } else {          // Woop: distance from row 2, then u and v from rows 0 and 1
+            // all three rows are loaded at once: one memory latency per triangle instead of up to three dependent
+            // ones (the traversal is bound by load latency, not by L1 bytes; measured 4% faster on frames)
+            const float4 r2 = ld4(tv + 3 * t + 2), r0 = ld4(tv + 3 * t), r1 = ld4(tv + 3 * t + 1);
             float Oz = frow(r2, o), Dz = fdot(d, xyz(r2));
             float tt = -Oz / Dz;
             if (tt > tmin && tt < hitT) {
-                float4 r0 = ld4(tv + 3 * t);
                 float u = fmaf(tt, fdot(d, xyz(r0)), frow(r0, o));
                 if (u >= 0.f && u <= 1.f) {
-                    float4 r1 = ld4(tv + 3 * t + 1);
                     float v = fmaf(tt, fdot(d, xyz(r1)), frow(r1, o));
                     if (v >= 0.f && u + v <= 1.f) { hitT = tt; hitTri = t; hu = u; hv = v; if (ANY) return true; }
                 }

@@ -370,6 +370,7 @@ typedef struct cwp_server_info {
     double closest_ms, shade_ms, shadow_ms, raygen_ms, tlas_ms, step_ms;   /* device time per phase (CUDA events), wall time of the steps */
     double admit_ms;         /* host time of admissions (instance animation, image allocation) */
     double tlas_device_ms;   /* device time of the TLAS updates inside tlas_ms (which is their wall time) */
+    double accum_ms;         /* device time of the shadow contributions' accumulation inside shadow_ms */
 } cwp_server_info;
 int cwp_server_info_of(const cwp_server* s, cwp_server_info* out);
 /* Device-side BSDF of a material table for n (material, wo, wi) triples in local frames (wo.z > 0): f (float4) and
