@@ -30,6 +30,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -59,18 +60,46 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons while the timed region runs."""
+    """SM clock and clock-event reasons while the timed region runs: NVML read every 10 ms from a thread (read-only
+    queries), or nvidia-smi at 200 ms where NVML is unavailable."""
     Q = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    BITS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, dev_id):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.samples, self.p, self.t, self.mx = [], None, None, None
+        self.done = threading.Event()
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200", "-i", dev_id],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByUUID(dev_id) if dev_id.startswith("GPU-") else N.nvmlDeviceGetHandleByIndex(int(dev_id))
+            reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or N.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.mx = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+
+            def run():
+                while not self.done.is_set():
+                    try:
+                        self.samples.append((float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)), int(reasons(h))))
+                    except Exception:
+                        pass
+                    self.done.wait(0.01)
+            self.t = threading.Thread(target=run, daemon=True)
+            self.t.start()
         except Exception:
-            self.p = None
+            self.t = None
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            try:
+                self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200", "-i", dev_id],
+                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            except Exception:
+                self.p = None
 
     def stop(self):
+        if self.t is not None:
+            self.done.set(); self.t.join(timeout=5)
+            sm = [c for c, _ in self.samples]
+            reasons = sorted({n for _, r in self.samples for bit, n in self.BITS.items() if r & bit})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.mx, "reasons": reasons, "samples": len(sm),
+                    "source": "nvml, 10 ms"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate(); self.p.wait(timeout=10); self.f.flush(); self.f.seek(0)
@@ -88,7 +117,8 @@ class Clocks:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         os.unlink(self.f.name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvidia-smi, 200 ms"}
 
 
 def dist_setup(args):
@@ -426,8 +456,9 @@ def bench_serving(args, wl, cwp, torch, out):
     streams = {"mix": cwp.serving_requests(n_req, wl["rate"], boxes, seed=wl["seed"] + 1),
                "small": cwp.serving_requests(wl["small_requests"], wl["small_rate"], boxes, seed=wl["seed"] + 2, resolutions=[(256, 256), (512, 512)], spps=[1, 4])}
     res = {}
+    maxr_c = args.max_requests or wl["max_requests"]
     for name, stream in streams.items():
-        for mode, maxr in (("continuous", wl["max_requests"]), ("plain", 1)):
+        for mode, maxr in (("continuous", maxr_c), ("plain", 1)):
             s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=maxr, regroup=bool(args.regroup))
             s.set_scenes(descs, first)
             clk = Clocks(str(torch.cuda.current_device()))
@@ -442,7 +473,7 @@ def bench_serving(args, wl, cwp, torch, out):
     out.update(metric="serving request throughput (continuous batching), Poisson stream of config-5 requests", value=c["throughput_req_s"], unit="req/s",
                ms_per_step=1e3 / c["throughput_req_s"], higher_is_better=True, dtype="f32",
                config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "blas_builder": ["gpu h-ploc", "host binned SAH"][wl["builder"]],
-                       "blas_build_ms": info.blas_build_ms, "scene_generation_s": gen_s, "depth": 8, "max_paths": wl["max_paths"], "max_requests": wl["max_requests"],
+                       "blas_build_ms": info.blas_build_ms, "scene_generation_s": gen_s, "depth": 8, "max_paths": wl["max_paths"], "max_requests": maxr_c,
                        "regroup": bool(args.regroup),
                        "materials": "OpenPBR subset: roughness U[0.05,1], metallic Bernoulli(0.3), 10% glass IOR 1.5",
                        "mix": {"requests": n_req, "arrival_rate_req_s": wl["rate"], "resolutions": "256^2, 512^2, 1280x720, 1920x1080", "spp": "1, 4, 16, 64, 256",
@@ -478,6 +509,7 @@ def main():
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     ap.add_argument("--spatial", type=float, default=1e-3, help="host BVH: spatial-split overlap threshold (1e-3 = SBVH, the default; 0 = the reference binned SAH only)")
+    ap.add_argument("--max-requests", type=int, default=0, help="serving: requests admitted at once by the continuous form (default: the workload's)")
     ap.add_argument("--regroup", type=int, default=1, help="serving: sort each step's continuations by request (1) or not (0)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     args = ap.parse_args()

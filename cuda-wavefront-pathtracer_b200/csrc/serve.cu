@@ -272,6 +272,7 @@ struct cwp_server {
     int* hcnt = nullptr;   // pinned: [0..1] counts, then slot counters
     SlotParams* hSlots = nullptr; int4* hChunks = nullptr; bool slotsDirty = false;   // pinned mirrors of dSlots and dChunks
     cudaMemPool_t pool = nullptr;   // request images: freed memory stays in the pool for the next admissions
+    double freeAt = -1e30; int64_t freeB = 0; uint64_t freeReserved = 0;   // last device free-memory query and the pool size then
     int cur = 0; int64_t nCur = 0;
     std::deque<int64_t> pending; std::map<int64_t, ServeRequest> reqs; std::vector<int64_t> completed;
     int64_t nextId = 1;
@@ -403,14 +404,20 @@ static int rebuild_tlas(cwp_server* s) {
     return rc;
 }
 
-// device bytes an admission may use: free memory plus what the image pool holds unused, less the reserve
+// device bytes an admission may use: free memory plus what the image pool holds unused, less the reserve. The
+// device query (milliseconds) runs at most every 50 ms; in between, the pool's own growth is taken off its answer.
 static int admission_budget(cwp_server* s, int64_t& avail) {
-    size_t freeB = 0, totalB = 0;
-    CWPB_CUDA(cudaMemGetInfo(&freeB, &totalB));
     uint64_t reserved = 0, used = 0;
     CWPB_CUDA(cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
     CWPB_CUDA(cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrUsedMemCurrent, &used));
-    avail = (int64_t)freeB + (int64_t)(reserved > used ? reserved - used : 0) - s->O.hbm_reserve;
+    const double t = now_ms(s);
+    if (t - s->freeAt > 50.0) {
+        size_t freeB = 0, totalB = 0;
+        CWPB_CUDA(cudaMemGetInfo(&freeB, &totalB));
+        s->freeB = (int64_t)freeB; s->freeReserved = reserved; s->freeAt = t;
+    }
+    const int64_t freeNow = s->freeB - ((int64_t)reserved - (int64_t)s->freeReserved);
+    avail = freeNow + (int64_t)(reserved > used ? reserved - used : 0) - s->O.hbm_reserve;
     return CWP_OK;
 }
 
