@@ -178,24 +178,6 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade(const __gr
 #ifndef CWPB_REFILL
 #define CWPB_REFILL 12   // a warp refetches rays once this many of its lanes are idle
 #endif
-#ifndef CWPB_SMEM_STACK
-#define CWPB_SMEM_STACK 0   // CWBVH stack entries per thread kept in shared memory by the refill kernels (0: all local)
-#endif
-
-// the refill kernels' traversal stack: local, or its first CWPB_SMEM_STACK entries in shared memory (CWBVH only)
-template <int V, bool ANY, int TRI, bool HYB = (V == 8 && CWPB_SMEM_STACK > 0)>
-struct RfStack { typename TravState<V, ANY, TRI>::Stack s; __device__ __forceinline__ RfStack(void*) {} __device__ __forceinline__ auto& get() { return s; } };
-template <int V, bool ANY, int TRI>
-struct RfStack<V, ANY, TRI, true> {
-    HybridStack<uint2, CWPB_SMEM_STACK, kStack8> s;
-    __device__ __forceinline__ RfStack(void* sh) { s.base = reinterpret_cast<uint2*>(sh) + threadIdx.x; s.stride = 128; }
-    __device__ __forceinline__ auto& get() { return s; }
-};
-#if CWPB_SMEM_STACK > 0
-#define CWPB_RF_SMEM __shared__ uint2 rfShared[CWPB_SMEM_STACK * 128];
-#else
-#define CWPB_RF_SMEM char* rfShared = nullptr;
-#endif
 
 // Persistent traversal with dynamic refill (Aila & Laine 2009): every lane holds one ray's traversal state and
 // advances it one node visit per step; once CWPB_REFILL lanes have finished, the warp shades those paths together,
@@ -207,8 +189,7 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade_rf(const _
     const int n = PRIMARY ? a.nk : c[0];
     const int lane = threadIdx.x & 31;
     int err = 0;
-    CWPB_RF_SMEM
-    TravState<V, false, TRI> ray; RfStack<V, false, TRI> stk(rfShared); auto& stack = stk.get();
+    TravState<V, false, TRI> ray; typename TravState<V, false, TRI>::Stack stack;
     int k = -1; bool fin = false, drained = false;
     for (;;) {
         if (__any_sync(0xffffffffu, fin)) {
@@ -244,8 +225,7 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow_rf(const __grid
     const int n = c[1];
     const int lane = threadIdx.x & 31;
     int err = 0;
-    CWPB_RF_SMEM
-    TravState<V, true, TRI> ray; RfStack<V, true, TRI> stk(rfShared); auto& stack = stk.get();
+    TravState<V, true, TRI> ray; typename TravState<V, true, TRI>::Stack stack;
     int k = -1; bool fin = false, drained = false;
     for (;;) {
         if (fin) {

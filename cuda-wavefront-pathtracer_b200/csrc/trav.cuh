@@ -184,14 +184,6 @@ struct SharedStack {
     __device__ __forceinline__ T& operator[](int i) const { return base[(size_t)i * stride]; }
 };
 
-// stack whose first S entries live in shared memory (entry-major, as SharedStack) and the rest in the thread's local
-// array: the shallow entries that most pops read stay on chip whatever L1 holds, at S x 8 bytes per thread of shared
-// memory instead of the full depth
-template <class T, int S, int N>
-struct HybridStack {
-    T* base; int stride; T deep[N - S];
-    __device__ __forceinline__ T& operator[](int i) { return i < S ? base[(size_t)i * stride] : deep[i - S]; }
-};
 
 // ---------------- CWBVH ----------------
 __device__ __forceinline__ unsigned byte_of(unsigned w, int s) { return (w >> (8 * (s & 3))) & 255u; }
