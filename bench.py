@@ -184,7 +184,7 @@ FRAME512_TRAFFIC = {"k_trace_shade": 2599.4e6, "k_shadow": 530.8e6}
 
 def frame_traffic(args, wl, variant, kernel):
     captured = (args.workload == "frame512" and variant == 8 and args.spatial == 1e-3 and not args.spp and not args.batch and args.sort == 0
-                and args.graph == 1 and args.traversal == 0 and args.bins == 32)
+                and args.graph == 1 and args.traversal == 0 and args.bins == 32 and args.l2_window < 0)
     if not captured or kernel not in FRAME512_TRAFFIC:
         return {"traffic": None}
     return {"traffic": FRAME512_TRAFFIC[kernel], "traffic_unit": "bytes per launch",
@@ -510,6 +510,7 @@ def main():
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     ap.add_argument("--spatial", type=float, default=1e-3, help="host BVH: spatial-split overlap threshold (1e-3 = SBVH, the default; 0 = the reference binned SAH only)")
     ap.add_argument("--max-requests", type=int, default=0, help="serving: requests admitted at once by the continuous form (default: the workload's)")
+    ap.add_argument("--l2-window", type=int, default=0, help="frames: 0 default (on), -1 off: the scene marked persisting in L2")
     ap.add_argument("--regroup", type=int, default=1, help="serving: sort each step's continuations by request (1) or not (0)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     args = ap.parse_args()
@@ -572,7 +573,8 @@ def main():
         w, h, spp, K, B = wl["w"], wl["h"], wl["spp"], wl["batch"], wl["bounces"]
         p = cwp.frame_params(mesh, w, h, bounces=B)
         r = cwp.Renderer()
-        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1, traversal=args.traversal, sort=args.sort)
+        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1, traversal=args.traversal, sort=args.sort,
+               l2_window=args.l2_window)
         for _ in range(args.warmup):
             r.render(spp)
         depths = B + 2
@@ -612,7 +614,8 @@ def main():
                    config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles, box field seed 1)", "resolution": f"{w}x{h}",
                            "spp": spp, "batch": K, "depth": B, "layout": LAYOUT_NAMES[variant], "sah_bins": args.bins, "tri": "woop",
                            "bvh": (f"sbvh (spatial splits at overlap > {args.spatial:g} of the root area, {len(bvh.order) / mesh.n_tris:.2f} references per triangle)" if args.spatial > 0 else "binned SAH"),
-                           "graph": args.graph, "traversal": ["auto", "refill", "batch"][args.traversal], "sort": ["off", "octant", "octant+cell"][args.sort], "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
+                           "graph": args.graph, "traversal": ["auto", "refill", "batch"][args.traversal], "sort": ["off", "octant", "octant+cell"][args.sort],
+                           "l2_window": "off" if args.l2_window < 0 else "scene nodes + triangles persisting", "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
                            "rays_per_frame": (rays + shadow) / args.steps, "closest_per_frame": rays / args.steps, "shadow_per_frame": shadow / args.steps,
                            "rays_per_sample": (rays + shadow) / args.steps / (w * h * spp), "trace_shade_ms": float(tms.sum() / args.steps),
                            "shadow_ms": float(sms.sum() / args.steps)},

@@ -15,6 +15,7 @@ struct DeviceScene {
     bool precise = false;                            // ray batches use the precision form (FP16 slabs + watertight)
     float3* albedo = nullptr; int nAlbedo = 0;
     size_t bytes = 0;
+    void* arena = nullptr; size_t hotBytes = 0;     // one allocation; its first hotBytes hold nodes, leaf rows, triangles, corners
     const float4* leafData() const { return precise ? verts : tri == 1 ? woop : tris; }
 };
 

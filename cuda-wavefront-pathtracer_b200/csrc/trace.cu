@@ -47,8 +47,7 @@ int validate_nodes(const float* nodes, int64_t nF4, int stride, int64_t nTris, i
 }
 
 void free_scene(DeviceScene& s) {
-    if (s.nodes || s.tris || s.woop || s.nrm || s.albedo || s.verts) cudaSetDevice(s.device);
-    cudaFree(s.nodes); cudaFree(s.tris); cudaFree(s.woop); cudaFree(s.nrm); cudaFree(s.albedo); cudaFree(s.verts);
+    if (s.arena) { cudaSetDevice(s.device); cudaFree(s.arena); }
     s = DeviceScene();
 }
 
@@ -63,21 +62,29 @@ int upload_scene(const cwp_scene_buffers* s, int tri, int device, DeviceScene& o
     out.device = device; out.variant = variant; out.tri = tri;
     out.nNodes = s->n_node_float4 / s->node_stride; out.nTris = s->n_tris;
     CWPB_CUDA(cudaSetDevice(device));
-    auto up = [&](void** dst, const void* src, size_t bytes) -> cudaError_t {
-        cudaError_t e = cudaMalloc(dst, bytes); if (e != cudaSuccess) return e;
-        out.bytes += bytes; return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
-    };
-    cudaError_t e = up((void**)&out.nodes, s->nodes, (size_t)s->n_node_float4 * 16);
-    if (e == cudaSuccess) e = up((void**)&out.tris, s->tris, (size_t)s->n_tris * 48);
-    if (e == cudaSuccess && s->woop) e = up((void**)&out.woop, s->woop, (size_t)s->n_tris * 48);
-    if (e == cudaSuccess && s->nrm) e = up((void**)&out.nrm, s->nrm, (size_t)s->n_tris * 48);
-    if (e == cudaSuccess && s->verts) e = up((void**)&out.verts, s->verts, (size_t)s->n_tris * 48);
+    std::vector<float3> alb;
+    for (int i = 0; i < s->n_albedo; i++) alb.push_back(make_float3(s->albedo[3 * i], s->albedo[3 * i + 1], s->albedo[3 * i + 2]));
+    if (alb.empty()) alb.push_back(make_float3(0.8f, 0.8f, 0.8f));
+    out.nAlbedo = (int)alb.size();
+    // one allocation, the traversal's data first (nodes, leaf rows, triangles, exact corners), so that a single L2
+    // access-policy window can cover what every ray reads
+    struct Part { void** dst; const void* src; size_t bytes; };
+    const size_t tb = (size_t)s->n_tris * 48;
+    const Part parts[] = { { (void**)&out.nodes, s->nodes, (size_t)s->n_node_float4 * 16 }, { (void**)&out.woop, s->woop, s->woop ? tb : 0 },
+                           { (void**)&out.tris, s->tris, tb }, { (void**)&out.verts, s->verts, s->verts ? tb : 0 },
+                           { (void**)&out.nrm, s->nrm, s->nrm ? tb : 0 }, { (void**)&out.albedo, alb.data(), alb.size() * sizeof(float3) } };
+    size_t total = 0, hot = 0;
+    for (int i = 0; i < 6; i++) { total += (parts[i].bytes + 255) & ~(size_t)255; if (i == 3) hot = total; }
+    cudaError_t e = cudaMalloc(&out.arena, total);
     if (e == cudaSuccess) {
-        std::vector<float3> alb;
-        for (int i = 0; i < s->n_albedo; i++) alb.push_back(make_float3(s->albedo[3 * i], s->albedo[3 * i + 1], s->albedo[3 * i + 2]));
-        if (alb.empty()) alb.push_back(make_float3(0.8f, 0.8f, 0.8f));
-        out.nAlbedo = (int)alb.size();
-        e = up((void**)&out.albedo, alb.data(), alb.size() * sizeof(float3));
+        out.bytes = total; out.hotBytes = hot;
+        size_t off = 0;
+        for (int i = 0; i < 6 && e == cudaSuccess; i++) {
+            if (!parts[i].bytes) { *parts[i].dst = nullptr; continue; }
+            *parts[i].dst = static_cast<char*>(out.arena) + off;
+            e = cudaMemcpy(*parts[i].dst, parts[i].src, parts[i].bytes, cudaMemcpyHostToDevice);
+            off += (parts[i].bytes + 255) & ~(size_t)255;
+        }
     }
     if (e != cudaSuccess) { free_scene(out); return set_error(e == cudaErrorMemoryAllocation ? CWP_ERR_NOMEM : CWP_ERR_CUDA, "scene upload: %s", cudaGetErrorString(e)); }
     // every material id referenced by a triangle must have an albedo entry
