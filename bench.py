@@ -184,7 +184,7 @@ FRAME512_TRAFFIC = {"k_trace_shade": 2599.4e6, "k_shadow": 530.8e6}
 
 def frame_traffic(args, wl, variant, kernel):
     captured = (args.workload == "frame512" and variant == 8 and args.spatial == 1e-3 and not args.spp and not args.batch and args.sort == 0
-                and args.graph == 1 and args.traversal == 0 and args.bins == 32 and args.l2_window < 0)
+                and args.graph == 1 and args.traversal == 0 and args.bins == 32)
     if not captured or kernel not in FRAME512_TRAFFIC:
         return {"traffic": None}
     return {"traffic": FRAME512_TRAFFIC[kernel], "traffic_unit": "bytes per launch",
@@ -339,7 +339,6 @@ def cpu_batched_sample(b, tuning_width, n_scenes, n_inst, o, d, sc, seconds=12.0
 
 def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_peak, peak_kind, out):
     import numpy as np
-    import torch.distributed as tdist
     t0 = time.perf_counter()
     meshes, xf, mesh_of, first = batched_setup(cwp, wl)
     gen_s = time.perf_counter() - t0
@@ -385,7 +384,7 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
     clocks = clk.stop()
     b.status()
     c_ms = sum(e[0].elapsed_time(e[1]) for e in ev); a_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
-    max_ms = reduce(c_ms + a_ms, tdist.ReduceOp.MAX if ws > 1 else None)
+    max_ms = reduce(c_ms + a_ms, "max")
     value = 2 * n * args.steps * ws / (max_ms * 1e-3) / 1e9
     hit_rate = float((hi >= 0).float().mean().item())
     # e2e: pinned host queue in, hits + instances out, every step, through the C ABI
@@ -396,7 +395,7 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
         o.copy_(ho, non_blocking=True); d.copy_(hd, non_blocking=True); sc.copy_(hs, non_blocking=True)
         step()
         hh.copy_(hits, non_blocking=True); hhi.copy_(hi, non_blocking=True); hoi.copy_(oi, non_blocking=True)
-    barrier(); e_s = reduce(time.perf_counter() - t2, tdist.ReduceOp.MAX if ws > 1 else None)
+    barrier(); e_s = reduce(time.perf_counter() - t2, "max")
     dom_ms, dom_b, dom = (c_ms, 56.0, "k_batch_trace (closest)") if c_ms >= a_ms else (a_ms, 40.0, "k_batch_trace (any)")
     achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
     out.update(metric="closest+any rays per second, batched two-level scenes", value=value, ms_per_step=max_ms / args.steps,
@@ -443,7 +442,7 @@ def serve_stream(cwp, s, stream):
             "span_s": span, "rays": rays}
 
 
-def bench_serving(args, wl, cwp, torch, out):
+def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda x, op: x):
     """Two request streams, each served by continuous batching and by the plain form (one request at a time, the same
     kernels): `mix` draws config 5's distribution (256^2..1080p, 1..256 spp), where single large requests already
     fill the GPU; `small` draws 256^2 / 512^2 at 1 / 4 spp, where one request alone leaves the GPU mostly idle."""
@@ -461,17 +460,21 @@ def bench_serving(args, wl, cwp, torch, out):
         for mode, maxr in (("continuous", maxr_c), ("plain", 1)):
             s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=maxr, regroup=bool(args.regroup))
             s.set_scenes(descs, first)
+            barrier()
             clk = Clocks(str(torch.cuda.current_device()))
             r = serve_stream(cwp, s, stream)
             r["clocks"] = clk.stop(); r["breakdown"] = s.info()
+            # replicas: every rank serves its own copy of the stream; the job's throughput is all requests over the
+            # slowest rank's span
+            r["job_throughput_req_s"] = reduce(r["requests"], "sum") / reduce(r["span_s"], "max")
             res[(name, mode)] = r
             del s
     info = b.info()
     c, p = res[("mix", "continuous")], res[("mix", "plain")]
     cs, ps = res[("small", "continuous")], res[("small", "plain")]
     strip = lambda r: {k: v for k, v in r.items() if k != "clocks"}
-    out.update(metric="serving request throughput (continuous batching), Poisson stream of config-5 requests", value=c["throughput_req_s"], unit="req/s",
-               ms_per_step=1e3 / c["throughput_req_s"], higher_is_better=True, dtype="f32",
+    out.update(metric="serving request throughput (continuous batching), Poisson stream of config-5 requests", value=c["job_throughput_req_s"], unit="req/s",
+               ms_per_step=1e3 / c["job_throughput_req_s"], higher_is_better=True, dtype="f32",
                config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "blas_builder": ["gpu h-ploc", "host binned SAH"][wl["builder"]],
                        "blas_build_ms": info.blas_build_ms, "scene_generation_s": gen_s, "depth": 8, "max_paths": wl["max_paths"], "max_requests": maxr_c,
                        "regroup": bool(args.regroup),
@@ -483,7 +486,7 @@ def bench_serving(args, wl, cwp, torch, out):
                                  "continuous": strip(cs), "plain": strip(ps), "throughput_vs_plain": cs["throughput_req_s"] / ps["throughput_req_s"],
                                  "p99_vs_plain": cs["p99_ms"] / ps["p99_ms"], "p50_vs_plain": cs["p50_ms"] / ps["p50_ms"]}},
                clocks=c["clocks"],
-               e2e={"value": c["throughput_req_s"], "unit": "req/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
+               e2e={"value": c["job_throughput_req_s"], "unit": "req/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
                     "note": "requests enter through the C ABI with host descriptors; images stay on the device until cwp_server_result"},
                gpu_launches=None)
 
@@ -510,7 +513,6 @@ def main():
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     ap.add_argument("--spatial", type=float, default=1e-3, help="host BVH: spatial-split overlap threshold (1e-3 = SBVH, the default; 0 = the reference binned SAH only)")
     ap.add_argument("--max-requests", type=int, default=0, help="serving: requests admitted at once by the continuous form (default: the workload's)")
-    ap.add_argument("--l2-window", type=int, default=0, help="frames: 0 default (on), -1 off: the scene marked persisting in L2")
     ap.add_argument("--regroup", type=int, default=1, help="serving: sort each step's continuations by request (1) or not (0)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     args = ap.parse_args()
@@ -532,28 +534,18 @@ def main():
     import numpy as np
     import torch
     torch.cuda.set_device(local)
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    rep = importlib.import_module("cuda-wavefront-pathtracer_b200.replicas").Replicas()   # NCCL between the GPUs when ws > 1
     cwp = importlib.import_module("cuda-wavefront-pathtracer_b200")
     variant = args.variant
     if not wl.get("batched") and not wl.get("serving"):
         mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=args.bins, spatial=args.spatial)
 
     def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
+        rep.barrier()
         torch.cuda.synchronize()
 
     def reduce(x, op):
-        if ws == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=op)
-        return float(t.item())
+        return rep.max(x) if op == "max" else rep.sum(x)
 
     props = torch.cuda.get_device_properties(local)
     try:
@@ -563,9 +555,8 @@ def main():
     hbm_peak, peak_kind = peaks()
     out = {"metric": "", "value": 0.0, "unit": "Grays/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 0.0,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
-    import torch.distributed as tdist
     if wl.get("serving"):
-        bench_serving(args, wl, cwp, torch, out)
+        bench_serving(args, wl, cwp, torch, out, barrier, reduce)
     elif wl.get("batched"):
         bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_peak, peak_kind, out)
     elif "rays" not in wl:
@@ -573,8 +564,7 @@ def main():
         w, h, spp, K, B = wl["w"], wl["h"], wl["spp"], wl["batch"], wl["bounces"]
         p = cwp.frame_params(mesh, w, h, bounces=B)
         r = cwp.Renderer()
-        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1, traversal=args.traversal, sort=args.sort,
-               l2_window=args.l2_window)
+        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1, traversal=args.traversal, sort=args.sort)
         for _ in range(args.warmup):
             r.render(spp)
         depths = B + 2
@@ -591,8 +581,8 @@ def main():
         torch.cuda.nvtx.range_pop()
         barrier()
         clocks = clk.stop()
-        max_ms = reduce(ms, tdist.ReduceOp.MAX if ws > 1 else None)
-        all_rays = reduce(rays + shadow, tdist.ReduceOp.SUM if ws > 1 else None)
+        max_ms = reduce(ms, "max")
+        all_rays = reduce(rays + shadow, "sum")
         value = all_rays / (max_ms * 1e-3) / 1e9
         # end to end through the C ABI with host buffers: frame + read of the accumulation buffer into pinned memory
         host = torch.empty((w * h, 4), dtype=torch.float32, pin_memory=True)
@@ -602,8 +592,8 @@ def main():
             cwp._check(cwp.lib().cwp_renderer_read_accum(r._h, host.data_ptr()))
             e_rays += st.rays + st.shadow_rays
         barrier(); e_s = time.perf_counter() - t0
-        e_s = reduce(e_s, tdist.ReduceOp.MAX if ws > 1 else None)
-        e_rays = reduce(e_rays, tdist.ReduceOp.SUM if ws > 1 else None)
+        e_s = reduce(e_s, "max")
+        e_rays = reduce(e_rays, "sum")
         # roofline of the dominant kernel (HBM: algorithmic path-state bytes per launch / its event-timed duration)
         tr_bytes = sum(STATE_BYTES * ((c_tot[d] if d > 0 else 0) + (c_tot[d + 1] if d + 1 < depths else 0) + s_tot[d]) for d in range(depths))
         sh_bytes = sum(STATE_BYTES * s_tot[d] for d in range(depths))
@@ -615,7 +605,7 @@ def main():
                            "spp": spp, "batch": K, "depth": B, "layout": LAYOUT_NAMES[variant], "sah_bins": args.bins, "tri": "woop",
                            "bvh": (f"sbvh (spatial splits at overlap > {args.spatial:g} of the root area, {len(bvh.order) / mesh.n_tris:.2f} references per triangle)" if args.spatial > 0 else "binned SAH"),
                            "graph": args.graph, "traversal": ["auto", "refill", "batch"][args.traversal], "sort": ["off", "octant", "octant+cell"][args.sort],
-                           "l2_window": "off" if args.l2_window < 0 else "scene nodes + triangles persisting", "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
+                           "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
                            "rays_per_frame": (rays + shadow) / args.steps, "closest_per_frame": rays / args.steps, "shadow_per_frame": shadow / args.steps,
                            "rays_per_sample": (rays + shadow) / args.steps / (w * h * spp), "trace_shade_ms": float(tms.sum() / args.steps),
                            "shadow_ms": float(sms.sum() / args.steps)},
@@ -676,7 +666,7 @@ def main():
         acc.status()
         c_ms = sum(ev[3 * i].elapsed_time(ev[3 * i + 1]) for i in range(args.steps))
         a_ms = sum(ev[3 * i + 1].elapsed_time(ev[3 * i + 2]) for i in range(args.steps))
-        max_ms = reduce(c_ms + a_ms, tdist.ReduceOp.MAX if ws > 1 else None)
+        max_ms = reduce(c_ms + a_ms, "max")
         value = 2 * n * args.steps * ws / (max_ms * 1e-3) / 1e9
         # e2e: pinned host rays in, hits / occluders out, every step
         ho = torch.from_numpy(o).pin_memory(); hd = torch.from_numpy(d).pin_memory()
@@ -686,7 +676,7 @@ def main():
         for _ in range(args.steps):
             cwp._check(cwp.lib().cwp_trace_closest_host(acc._h, ho.data_ptr(), hd.data_ptr(), hh.data_ptr(), n, None))
             cwp._check(cwp.lib().cwp_trace_any_host(acc._h, ho.data_ptr(), hd.data_ptr(), hoc.data_ptr(), n, None))
-        barrier(); e_s = reduce(time.perf_counter() - t0, tdist.ReduceOp.MAX if ws > 1 else None)
+        barrier(); e_s = reduce(time.perf_counter() - t0, "max")
         dom_ms, dom_b, dom = (c_ms, 48.0, "k_trace_closest") if c_ms >= a_ms else (a_ms, 36.0, "k_trace_any")
         check = {}
         if wl.get("precision"):
@@ -743,9 +733,7 @@ def main():
                                       "nodes_per_closest_ray": ob["nodes_per_closest"], "tris_per_closest_ray": ob["tris_per_closest"],
                                       "nodes_per_shadow_ray": ob["nodes_per_shadow"], "tris_per_shadow_ray": ob["tris_per_shadow"],
                                       "algorithmic": f"node visits x {NODE_BYTES[variant]} B + triangle tests x {TRI_BYTES} B per ray ({ob['sample']})"}
-    if ws > 1:
-        tdist.barrier()
-        tdist.destroy_process_group()
+    rep.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
 

@@ -63,7 +63,7 @@ class Params(C.Structure):
 class RenderOptions(C.Structure):
     _fields_ = [("variant", C.c_int32), ("tri", C.c_int32), ("batch", C.c_int32), ("bounces", C.c_int32), ("graph", C.c_int32),
                 ("block", C.c_int32), ("device", C.c_int32), ("profile", C.c_int32), ("traversal", C.c_int32),
-                ("sort", C.c_int32), ("l2_window", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("sort", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class DeviceScene(C.Structure):
@@ -401,10 +401,10 @@ class Renderer:
         _check(lib().cwp_renderer_create(C.byref(h)))
         self._h = h
 
-    def init(self, params, bvh, variant, tri=TRI_WOOP, batch=16, bounces=4, graph=1, device=0, profile=0, traversal=0, sort=0, l2_window=0):
+    def init(self, params, bvh, variant, tri=TRI_WOOP, batch=16, bounces=4, graph=1, device=0, profile=0, traversal=0, sort=0):
         self._params, self._bvh = params, bvh
         o = RenderOptions(); o.variant, o.tri, o.batch, o.bounces, o.graph, o.device, o.profile = variant, tri, batch, bounces, graph, device, profile
-        o.traversal, o.sort, o.l2_window = traversal, sort, l2_window
+        o.traversal, o.sort = traversal, sort
         self.depths = bounces + 2
         s = bvh.scene_buffers()
         _check(lib().cwp_renderer_init(self._h, C.byref(params), C.byref(s), C.byref(o)))

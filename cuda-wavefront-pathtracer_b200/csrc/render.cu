@@ -355,7 +355,6 @@ struct cwp_renderer {
     int gridTrace = 0, gridTrace0 = 0, gridShadow = 0, nSM = 0; bool refill = false, refillShadow = false;
     std::vector<void*> allocs;
     double vramMB = 0; std::string gpuName;
-    cudaAccessPolicyWindow window{}; bool hasWindow = false;   // the scene's L2 persisting window
 };
 
 namespace {
@@ -444,12 +443,6 @@ int enqueue_passes(cwp_renderer* r, int spp, int sBase) {
 
 void release(cwp_renderer* r) {
     if (r->st) cudaStreamSynchronize(r->st);
-    if (r->hasWindow) {   // drop the window and demote the scene's persisting lines to normal ones
-        cudaStreamAttrValue v{}; v.accessPolicyWindow.num_bytes = 0;
-        cudaStreamSetAttribute(r->st, cudaStreamAttributeAccessPolicyWindow, &v);
-        cudaCtxResetPersistingL2Cache();
-        r->hasWindow = false;
-    }
     for (cudaEvent_t e : r->ev) cudaEventDestroy(e);
     r->ev.clear(); r->evPasses = 0;
     if (r->gexec) cudaGraphExecDestroy(r->gexec);
@@ -461,45 +454,6 @@ void release(cwp_renderer* r) {
     r->hcnt = nullptr;
     free_scene(r->scene);
     r->ready = false;
-}
-
-// The scene in L2: every ray re-reads nodes and leaf rows while path state streams through once per depth (several GB
-// a frame), so without a hint the stream evicts scene lines that the next rays need. An access-policy window over the
-// scene arena's traversal part marks its lines persisting, within a set-aside of L2 that this call raises for the
-// calling process's context (the device's own configuration is not touched).
-int set_scene_window(cwp_renderer* r) {
-    int maxPersist = 0, maxWindow = 0;
-    CWPB_CUDA(cudaDeviceGetAttribute(&maxPersist, cudaDevAttrMaxPersistingL2CacheSize, r->O.device));
-    CWPB_CUDA(cudaDeviceGetAttribute(&maxWindow, cudaDevAttrMaxAccessPolicyWindowSize, r->O.device));
-    if (maxPersist <= 0 || maxWindow <= 0 || !r->scene.arena || !r->scene.hotBytes) return CWP_OK;
-    const size_t win = std::min(r->scene.hotBytes, (size_t)maxWindow), want = std::min(win, (size_t)maxPersist);
-    size_t cur = 0;
-    CWPB_CUDA(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
-    if (cur < want) CWPB_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
-    cudaStreamAttrValue v{};
-    v.accessPolicyWindow.base_ptr = r->scene.arena; v.accessPolicyWindow.num_bytes = win;
-    v.accessPolicyWindow.hitRatio = std::min(1.f, (float)want / (float)win);
-    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting; v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-    CWPB_CUDA(cudaStreamSetAttribute(r->st, cudaStreamAttributeAccessPolicyWindow, &v));
-    r->window = v.accessPolicyWindow; r->hasWindow = true;
-    return CWP_OK;
-}
-
-// kernel nodes of a captured frame carry the window too
-int apply_window(cwp_renderer* r, cudaGraph_t g) {
-    if (!r->hasWindow) return CWP_OK;
-    size_t n = 0;
-    CWPB_CUDA(cudaGraphGetNodes(g, nullptr, &n));
-    std::vector<cudaGraphNode_t> nodes(n);
-    CWPB_CUDA(cudaGraphGetNodes(g, nodes.data(), &n));
-    for (cudaGraphNode_t nd : nodes) {
-        cudaGraphNodeType t;
-        CWPB_CUDA(cudaGraphNodeGetType(nd, &t));
-        if (t != cudaGraphNodeTypeKernel) continue;
-        cudaKernelNodeAttrValue v{}; v.accessPolicyWindow = r->window;
-        CWPB_CUDA(cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributeAccessPolicyWindow, &v));
-    }
-    return CWP_OK;
 }
 
 }  // namespace
@@ -596,8 +550,6 @@ extern "C" int cwp_renderer_init(cwp_renderer* r, const cwp_params* p, const cwp
     (void)b1;
     if (rc) return rc;
     r->gridTrace0 = bt0 * r->nSM; r->gridTrace = bt * r->nSM; r->gridShadow = bs * r->nSM;
-    CWPB_CHECK(o->l2_window >= -1 && o->l2_window <= 1, CWP_ERR_INVALID, "l2_window %d is not -1, 0 or 1", o->l2_window);
-    if (o->l2_window >= 0) if (int rc2 = set_scene_window(r)) return rc2;
     r->ready = true;
     return CWP_OK;
 }
@@ -626,7 +578,6 @@ extern "C" int cwp_renderer_render(cwp_renderer* r, int32_t spp, cwp_frame_stats
             cudaError_t e = cudaStreamEndCapture(r->st, &g);
             if (rc) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
             CWPB_CUDA(e);
-            if (int rc2 = apply_window(r, g)) { cudaGraphDestroy(g); return rc2; }
             e = cudaGraphInstantiate(&r->gexec, g, 0);
             cudaGraphDestroy(g);
             CWPB_CUDA(e);

@@ -159,9 +159,7 @@ typedef struct cwp_render_options {
     int32_t profile;      /* 1: CUDA event pair around every kernel launch (also inside the graph), see cwp_renderer_depth_stats */
     int32_t traversal;    /* 0 auto (refill for CWBVH closest-hit), 1 persistent lanes with dynamic refill everywhere, 2 one 32-ray fetch per warp */
     int32_t sort;         /* continuation rays regrouped before each bounce: 0 off, 1 by direction octant, 2 by octant and a 4x4x4 origin cell */
-    int32_t l2_window;    /* 0 default (on), 1 on, -1 off: the scene's nodes and triangles marked persisting in L2 (an access-policy
-                             window on the renderer's stream and graph; the set-aside is a limit of the calling process's context) */
-    int32_t reserved[1];
+    int32_t reserved[2];
 } cwp_render_options;
 
 typedef struct cwp_frame_stats { double rays, shadow_rays, trace_ms, frame_ms; } cwp_frame_stats;
