@@ -442,6 +442,38 @@ def serve_stream(cwp, s, stream):
             "span_s": span, "rays": rays}
 
 
+def equal_p99(cont, plain):
+    """Throughput at equal p99 latency from two (arrival rate -> throughput, p99) sweeps: for each latency bound L
+    (every p99 either form reached), the highest throughput each form sustained with p99 <= L, and their ratio."""
+    bounds = sorted({pt["p99_ms"] for pt in cont + plain})
+    best = lambda pts, L: max([pt["throughput_req_s"] for pt in pts if pt["p99_ms"] <= L] or [0.0])
+    rows = []
+    for L in bounds:
+        c, p = best(cont, L), best(plain, L)
+        rows.append({"p99_bound_ms": L, "continuous_req_s": c, "plain_req_s": p, "ratio": c / p if p > 0 else None})
+    ratios = [r["ratio"] for r in rows if r["ratio"] is not None]
+    # the bound at which the plain form reaches its best throughput (its capacity within any bound it meets)
+    pmax = max(pt["throughput_req_s"] for pt in plain)
+    Lp = min(pt["p99_ms"] for pt in plain if pt["throughput_req_s"] >= pmax * 0.999)
+    at = next(r for r in rows if r["p99_bound_ms"] == Lp)
+    return {"rows": rows, "max_ratio": max(ratios) if ratios else None, "median_ratio": statistics.median(ratios) if ratios else None,
+            "at_plain_capacity": at}
+
+
+def slo_sweep(cwp, b, mats, base, descs, first, wl, maxr, args, boxes, name, rates, n_req, resolutions=None, spps=None):
+    """Each form fed Poisson streams of n_req requests at each arrival rate: (rate, throughput, p50, p99) points."""
+    pts = {"continuous": [], "plain": []}
+    for rate in rates:
+        stream = cwp.serving_requests(n_req, rate, boxes, seed=wl["seed"] + 100 + int(rate * 10), resolutions=resolutions, spps=spps)
+        for mode, m in (("continuous", maxr), ("plain", 1)):
+            s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=m, regroup=bool(args.regroup))
+            s.set_scenes(descs, first)
+            r = serve_stream(cwp, s, stream)
+            pts[mode].append({"rate_req_s": rate, "throughput_req_s": r["throughput_req_s"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"]})
+            del s
+    return {"stream": name, "requests_per_point": n_req, "points": pts, "equal_p99": equal_p99(pts["continuous"], pts["plain"])}
+
+
 def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda x, op: x):
     """Two request streams, each served by continuous batching and by the plain form (one request at a time, the same
     kernels): `mix` draws config 5's distribution (256^2..1080p, 1..256 spp), where single large requests already
@@ -469,6 +501,11 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
             r["job_throughput_req_s"] = reduce(r["requests"], "sum") / reduce(r["span_s"], "max")
             res[(name, mode)] = r
             del s
+    sweeps = {}
+    if args.slo_sweep:
+        sweeps["small"] = slo_sweep(cwp, b, mats, base, descs, first, wl, maxr_c, args, boxes, "small", [25.0, 50.0, 75.0, 100.0, 150.0], 200,
+                                    resolutions=[(256, 256), (512, 512)], spps=[1, 4])
+        sweeps["mix"] = slo_sweep(cwp, b, mats, base, descs, first, wl, maxr_c, args, boxes, "mix", [0.25, 0.5, 1.0], 16)
     info = b.info()
     c, p = res[("mix", "continuous")], res[("mix", "plain")]
     cs, ps = res[("small", "continuous")], res[("small", "plain")]
@@ -484,7 +521,8 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
                                "p99_vs_plain": c["p99_ms"] / p["p99_ms"], "p50_vs_plain": c["p50_ms"] / p["p50_ms"]},
                        "small": {"requests": wl["small_requests"], "arrival_rate_req_s": wl["small_rate"], "resolutions": "256^2, 512^2", "spp": "1, 4",
                                  "continuous": strip(cs), "plain": strip(ps), "throughput_vs_plain": cs["throughput_req_s"] / ps["throughput_req_s"],
-                                 "p99_vs_plain": cs["p99_ms"] / ps["p99_ms"], "p50_vs_plain": cs["p50_ms"] / ps["p50_ms"]}},
+                                 "p99_vs_plain": cs["p99_ms"] / ps["p99_ms"], "p50_vs_plain": cs["p50_ms"] / ps["p50_ms"]},
+                       "throughput_at_equal_p99": sweeps or None},
                clocks=c["clocks"],
                e2e={"value": c["job_throughput_req_s"], "unit": "req/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
                     "note": "requests enter through the C ABI with host descriptors; images stay on the device until cwp_server_result"},
@@ -513,6 +551,7 @@ def main():
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     ap.add_argument("--spatial", type=float, default=1e-3, help="host BVH: spatial-split overlap threshold (1e-3 = SBVH, the default; 0 = the reference binned SAH only)")
     ap.add_argument("--max-requests", type=int, default=0, help="serving: requests admitted at once by the continuous form (default: the workload's)")
+    ap.add_argument("--slo-sweep", type=int, default=1, help="serving: also sweep arrival rates for throughput at equal p99 (1) or not (0)")
     ap.add_argument("--regroup", type=int, default=1, help="serving: sort each step's continuations by request (1) or not (0)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     args = ap.parse_args()
