@@ -310,6 +310,8 @@ static int server_create(cwp_batch* b, const cwp_material* mats, int n, const in
     s->O.gd_energy = o ? o->gd_energy : 1;
     s->O.hbm_reserve = o && o->hbm_reserve > 0 ? o->hbm_reserve : (1ll << 30);
     s->O.regroup = o && o->regroup < 0 ? -1 : 1;
+    s->O.policy = o ? o->policy : 0;
+    CWPB_CHECK(s->O.policy == 0 || s->O.policy == 1, CWP_ERR_INVALID, "policy %d is not 0 or 1", s->O.policy);
     CWPB_CHECK(s->O.max_paths < (1ll << 30), CWP_ERR_INVALID, "max_paths %lld above 2^30", (long long)s->O.max_paths);
     CWPB_CHECK(s->O.max_requests <= 1024, CWP_ERR_INVALID, "max_requests %d above 1024", s->O.max_requests);
     CWPB_CHECK(mats && n >= 1 && meshBase, CWP_ERR_INVALID, "no materials");
@@ -489,7 +491,8 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
     int nChunks = 0; int64_t added = 0;
     for (size_t i = 0; i < needy.size() && freeCap > 0; i++) {
         ServeRequest& q = s->reqs[s->slotReq[needy[i]]];
-        const int64_t share = freeCap / (int64_t)(needy.size() - i);   // what is left split over the requests not yet served
+        // even share: what is left split over the requests not yet served; oldest first: all that is left
+        const int64_t share = s->O.policy == 1 ? freeCap : freeCap / (int64_t)(needy.size() - i);
         const int64_t take = std::min(q.total - q.issued, std::max<int64_t>(share, 1));
         if (take <= 0) continue;
         s->hChunks[nChunks++] = make_int4(needy[i], (int)q.issued, (int)take, (int)added);

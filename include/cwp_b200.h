@@ -330,7 +330,11 @@ typedef struct cwp_server_options {
     int64_t hbm_reserve;   /* device bytes that admission leaves free (default 1 GiB) */
     int32_t device;
     int32_t regroup;       /* sort each step's continuations by request before tracing: 1 on, -1 off, 0 default (on) */
-    int32_t reserved[4];
+    int32_t policy;        /* new camera paths each step: 0 even share of the free path capacity among the requests with
+                              samples left (oldest first, the default); 1 oldest first takes all it can use, the later
+                              ones fill what is left (a request's drain no longer idles the GPU, big requests keep the
+                              plain form's speed) */
+    int32_t reserved[3];
 } cwp_server_options;
 
 typedef struct cwp_request {
