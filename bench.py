@@ -245,9 +245,21 @@ def cpu_trace_sample(cwp, bvh, variant, o, d, seconds=12.0):
                 sample=f"{n} of the {len(o)} incoherent rays, closest-hit and any-hit ({2 * n} rays in {spent:.2f} s)")
 
 
+METRIC_FRAME = "closest+shadow rays per second, diffuse frame"
+METRIC_BATCH = "closest+any rays per second, incoherent ray batch"
+METRIC_BATCHED = "closest+any rays per second, batched two-level scenes"
+METRIC_SERVING = "serving request throughput (continuous batching), Poisson stream of config-5 requests"
+
+
 def run_reference(args, wl, rank):
-    """--impl reference: the reference's CPU implementation of the path on this host's cores (rank 0 only)."""
+    """--impl reference: the reference's CPU implementation of the path on this host's cores (rank 0 only), with the
+    product arm's metric, unit and workload."""
     if rank != 0:
+        return
+    if wl.get("batched") or wl.get("serving"):
+        why = ("the reference has no host path for many two-level scenes in one queue (its travInst on the host cores is the "
+               "batched64 line's cpu_baseline)" if wl.get("batched") else "the reference has no serving loop")
+        print(json.dumps({"impl": "reference", "metric": METRIC_BATCHED if wl.get("batched") else METRIC_SERVING, "unavailable": why}), flush=True)
         return
     cwp = importlib.import_module("cuda-wavefront-pathtracer_b200")
     variant = args.variant
@@ -273,10 +285,17 @@ def run_reference(args, wl, rank):
             vals.append(cb["value"])
     v = statistics.median(vals)
     cb["value"] = v
-    print(json.dumps({"impl": "reference", "metric": "closest+shadow rays per second" if "rays" not in wl else "closest+any rays per second",
+    if "rays" not in wl:
+        config = {"workload": args.workload, "scene": f"{wl['scene']} ({mesh.n_tris} triangles, box field seed 1)", "resolution": f"{wl['w']}x{wl['h']}",
+                  "spp": wl["spp"], "batch": wl["batch"], "depth": wl["bounces"], "layout": LAYOUT_NAMES[variant], "sah_bins": 16, "tri": "woop",
+                  "bvh": "binned SAH (the reference's BVHBuilder, 16 bins)"}
+    else:
+        config = {"workload": args.workload, "scene": f"{wl['scene']} ({mesh.n_tris} triangles)", "rays": wl["rays"], "layout": LAYOUT_NAMES[variant],
+                  "sah_bins": 16, "tri": "woop", "bvh": "binned SAH (the reference's BVHBuilder, 16 bins)"}
+    print(json.dumps({"impl": "reference", "metric": METRIC_FRAME if "rays" not in wl else METRIC_BATCH,
                       "value": v, "unit": "Grays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                       "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                      "config": {"workload": args.workload, **{k: wl[k] for k in wl}, "layout": LAYOUT_NAMES[variant], "tri": "woop"},
+                      "config": config,
                       "cpu_baseline": cb, "e2e": {"value": v, "unit": "Grays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
 
 
@@ -398,7 +417,7 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
     barrier(); e_s = reduce(time.perf_counter() - t2, "max")
     dom_ms, dom_b, dom = (c_ms, 56.0, "k_batch_trace (closest)") if c_ms >= a_ms else (a_ms, 40.0, "k_batch_trace (any)")
     achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
-    out.update(metric="closest+any rays per second, batched two-level scenes", value=value, ms_per_step=max_ms / args.steps,
+    out.update(metric=METRIC_BATCHED, value=value, ms_per_step=max_ms / args.steps,
                config={"workload": args.workload, "scenes": n_s, "blas": info.n_blas, "tris": int(info.n_tris), "instances": int(info.n_instances),
                        "rays": n, "rays_per_scene": per, "hit_rate": hit_rate,
                        "tuning": {"block": tun.block, "width": tun.width, "fetch": tun.fetch, "smem_stack": tun.smem_stack, "sample_ms": tun.ms},
@@ -510,7 +529,7 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
     c, p = res[("mix", "continuous")], res[("mix", "plain")]
     cs, ps = res[("small", "continuous")], res[("small", "plain")]
     strip = lambda r: {k: v for k, v in r.items() if k != "clocks"}
-    out.update(metric="serving request throughput (continuous batching), Poisson stream of config-5 requests", value=c["job_throughput_req_s"], unit="req/s",
+    out.update(metric=METRIC_SERVING, value=c["job_throughput_req_s"], unit="req/s",
                ms_per_step=1e3 / c["job_throughput_req_s"], higher_is_better=True, dtype="f32",
                config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "blas_builder": ["gpu h-ploc", "host binned SAH"][wl["builder"]],
                        "blas_build_ms": info.blas_build_ms, "scene_generation_s": gen_s, "depth": 8, "max_paths": wl["max_paths"], "max_requests": maxr_c,
@@ -640,7 +659,7 @@ def main():
         dom = "k_trace_shade" if tms.sum() >= sms.sum() else "k_shadow"
         b, t = (tr_bytes, tms.sum()) if dom == "k_trace_shade" else (sh_bytes, sms.sum())
         achieved = b / (t * 1e-3) / 1e9 if t > 0 else 0.0
-        out.update(metric="closest+shadow rays per second, diffuse frame", value=value, ms_per_step=max_ms / args.steps,
+        out.update(metric=METRIC_FRAME, value=value, ms_per_step=max_ms / args.steps,
                    config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles, box field seed 1)", "resolution": f"{w}x{h}",
                            "spp": spp, "batch": K, "depth": B, "layout": LAYOUT_NAMES[variant], "sah_bins": args.bins, "tri": "woop",
                            "bvh": (f"sbvh (spatial splits at overlap > {args.spatial:g} of the root area, {len(bvh.order) / mesh.n_tris:.2f} references per triangle)" if args.spatial > 0 else "binned SAH"),
@@ -737,7 +756,7 @@ def main():
                      "plain_grays_s": plain, "vs_plain": value / plain if plain else None}
         achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
         onchip = dict(kind="batch", closest=float(n * args.steps), shadow=float(n * args.steps), closest_ms=c_ms, shadow_ms=a_ms)
-        out.update(metric="closest+any rays per second, incoherent ray batch", value=value, ms_per_step=max_ms / args.steps,
+        out.update(metric=METRIC_BATCH, value=value, ms_per_step=max_ms / args.steps,
                    config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles)", "rays": n,
                            "layout": LAYOUT_NAMES[variant] + (" precision form (f16 conservative slabs, watertight fp32 triangles)" if wl.get("precision") else ""), **check,
                            "sah_bins": args.bins, "tri": "woop", "traversal": ["auto", "refill", "batch"][args.traversal],
