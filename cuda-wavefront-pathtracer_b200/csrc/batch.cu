@@ -23,7 +23,11 @@ namespace cwpb {
 
 static constexpr int kTlasStack = 64;
 
-static constexpr int kBatchMaxBlock = 512;
+#ifndef CWPB_BATCH_MAXB
+#define CWPB_BATCH_MAXB 512
+#define CWPB_BATCH_MINB 2
+#endif
+static constexpr int kBatchMaxBlock = CWPB_BATCH_MAXB;
 
 struct BatchArgs {
     const float4* nodes; const float4* tris;        // BLAS layout of the chosen width (absolute indices, MT records)
@@ -103,7 +107,7 @@ __device__ __forceinline__ unsigned lane_mask_lt() { unsigned m; asm("mov.u32 %0
 // Persistent launch: each lane advances its ray one node visit at a time; a warp refetches rays (one atomic on the
 // queue cursor) once a.fetch of its lanes are idle. SMEM: the BLAS stack in shared memory, entry-major.
 template <int V, bool ANY, bool SMEM>
-__global__ void __launch_bounds__(kBatchMaxBlock, 2) k_batch_trace(const BatchArgs a) {
+__global__ void __launch_bounds__(kBatchMaxBlock, CWPB_BATCH_MINB) k_batch_trace(const BatchArgs a) {
     typedef typename TravState<V, ANY, 0>::Stack LocalStack;
     typedef typename std::conditional<V == 8, uint2, int>::type Entry;
     extern __shared__ unsigned char smem[];
