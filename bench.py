@@ -328,7 +328,9 @@ def cpu_batched_sample(b, tuning_width, n_scenes, n_inst, o, d, sc, seconds=12.0
     a strided sample of the queue on the GPU-built buffers; the oracle restatement when the reference is absent."""
     import numpy as np
     nodes, tris = b.download(tuning_width)
+    b.set_tlas_width(2)   # the reference's travInst reads a BVH2 TLAS (both forms are built)
     tlas, roots, inst = b.download_tlas(n_scenes, n_inst)
+    b.set_tlas_width(4)
     L = reference_lib(); threads = os.cpu_count() or 1
     n = 1 << 12
     while True:
@@ -361,7 +363,7 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
     t0 = time.perf_counter()
     meshes, xf, mesh_of, first = batched_setup(cwp, wl)
     gen_s = time.perf_counter() - t0
-    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=args.builder)
+    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=args.builder, tlas_width=args.tlas_width)
     inst = cwp.instances(xf, mesh_of)
     b.set_scenes(inst, first)
     info = b.info()
@@ -500,7 +502,7 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
     import numpy as np
     t0 = time.perf_counter()
     meshes, descs, first, mats, base, boxes = cwp.serving_scenes(n_scenes=wl["scenes"], seed=wl["seed"])
-    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=wl["builder"])
+    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=wl["builder"], tlas_width=args.tlas_width)
     gen_s = time.perf_counter() - t0
     n_req = args.rays if args.rays else wl["requests"]
     streams = {"mix": cwp.serving_requests(n_req, wl["rate"], boxes, seed=wl["seed"] + 1),
@@ -570,6 +572,7 @@ def main():
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     ap.add_argument("--spatial", type=float, default=1e-3, help="host BVH: spatial-split overlap threshold (1e-3 = SBVH, the default; 0 = the reference binned SAH only)")
     ap.add_argument("--max-requests", type=int, default=0, help="serving: requests admitted at once by the continuous form (default: the workload's)")
+    ap.add_argument("--tlas-width", type=int, default=4, choices=[2, 4], help="batched / serving: TLAS node width the traversal reads")
     ap.add_argument("--policy", type=int, default=0, help="serving: new paths by even share (0) or oldest first with backfill (1)")
     ap.add_argument("--slo-sweep", type=int, default=1, help="serving: also sweep arrival rates for throughput at equal p99 (1) or not (0)")
     ap.add_argument("--regroup", type=int, default=1, help="serving: sort each step's continuations by request (1) or not (0)")

@@ -88,7 +88,8 @@ class InstanceDesc(C.Structure):
 
 
 class BatchOptions(C.Structure):
-    _fields_ = [("device", C.c_int32), ("leaf", C.c_int32), ("widths", C.c_int32), ("builder", C.c_int32), ("spatial", C.c_float), ("reserved", C.c_int32 * 3)]
+    _fields_ = [("device", C.c_int32), ("leaf", C.c_int32), ("widths", C.c_int32), ("builder", C.c_int32), ("spatial", C.c_float),
+                ("tlas_width", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class BatchTuning(C.Structure):
@@ -167,6 +168,7 @@ SIGNATURES = {
     "cwp_instance_from_xform": (C.c_int, [C.POINTER(C.c_float), C.c_int32, C.POINTER(Instance)]),
     "cwp_batch_create": (C.c_int, [C.POINTER(MeshView), C.c_int32, C.POINTER(BatchOptions), C.POINTER(C.c_void_p)]),
     "cwp_batch_destroy": (None, [C.c_void_p]),
+    "cwp_batch_set_tlas_width": (C.c_int, [C.c_void_p, C.c_int32]),
     "cwp_batch_reserve_scenes": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "cwp_batch_update_scenes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "cwp_batch_set_scenes": (C.c_int, [C.c_void_p, C.POINTER(Instance), C.c_int64, C.POINTER(C.c_int32), C.c_int32]),
@@ -481,7 +483,7 @@ class Batch:
     """Batched form: many meshes built on the GPU at once (segmented H-PLOC, BVH2 / BVH4 / CWBVH encodings), many
     two-level scenes, one persistent launch over a scene-tagged ray queue, and the launch-shape autotuner."""
 
-    def __init__(self, meshes, device=0, leaf=4, widths=0, builder=0, spatial=0.0):
+    def __init__(self, meshes, device=0, leaf=4, widths=0, builder=0, spatial=0.0, tlas_width=4):
         arrs, views = [], (MeshView * len(meshes))()
         for i, m in enumerate(meshes):
             v, f, fm, _ = m.arrays() if isinstance(m, Mesh) else m
@@ -489,10 +491,10 @@ class Batch:
             fm = np.ascontiguousarray(fm if fm is not None else np.zeros(len(f)), np.int32)
             arrs += [v, f, fm]
             views[i].verts, views[i].n_verts, views[i].faces, views[i].n_tris, views[i].face_mat = _fptr(v), len(v), _iptr(f), len(f), _iptr(fm)
-        o = BatchOptions(device, leaf, widths, builder, spatial)
+        o = BatchOptions(device, leaf, widths, builder, spatial, tlas_width)
         h = C.c_void_p()
         _check(lib().cwp_batch_create(views, len(meshes), C.byref(o), C.byref(h)))
-        self._h = h
+        self._h = h; self.tlas_width = tlas_width
 
     def set_scenes(self, inst, scene_first):
         first = np.ascontiguousarray(scene_first, np.int32)
@@ -537,10 +539,15 @@ class Batch:
         _check(lib().cwp_batch_download(self._h, width, nodes.ctypes.data, C.byref(nn), tris.ctypes.data, C.byref(nt)))
         return nodes, tris
 
+    def set_tlas_width(self, width):
+        """TLAS form the traversal reads (and download_tlas returns): 2 or 4"""
+        _check(lib().cwp_batch_set_tlas_width(self._h, width)); self.tlas_width = width
+
     def download_tlas(self, n_scenes, n_inst):
-        """(tlas nodes [4 n_inst, 4], scene roots [n_scenes], instances as float32 [n_inst, 28])"""
+        """(tlas nodes [4 n_inst, 4] for width 2 or [8 n_inst, 4] for width 4, scene roots [n_scenes], instances as
+        float32 [n_inst, 28])"""
         nn = C.c_int64()
-        nodes = np.zeros((4 * max(n_inst, 1), 4), np.float32); roots = np.zeros(n_scenes, np.int32); inst = np.zeros((max(n_inst, 1), 28), np.float32)
+        nodes = np.zeros((8 * max(n_inst, 1), 4), np.float32); roots = np.zeros(n_scenes, np.int32); inst = np.zeros((max(n_inst, 1), 28), np.float32)
         _check(lib().cwp_batch_download_tlas(self._h, nodes.ctypes.data, C.byref(nn), roots.ctypes.data, inst.ctypes.data))
         return nodes[:nn.value], roots, inst[:n_inst]
 

@@ -27,7 +27,8 @@ static constexpr int kBatchMaxBlock = 512;
 
 struct BatchArgs {
     const float4* nodes; const float4* tris;        // BLAS layout of the chosen width (absolute indices, MT records)
-    const float4* tlas; const int* sceneRoot; const float4* inst;   // TLAS BVH2 nodes, root per scene, instances (7 float4)
+    const float4* tlas; const int* sceneRoot; const float4* inst;   // TLAS nodes, root per scene, instances (7 float4)
+    int tlasW;                                                        // TLAS node width: 2 (4 float4 per node) or 4 (8 float4)
     const int* meshRoot;                                              // BLAS root of each mesh in the traced layout
     int nScenes;
     const float4* ro; const float4* rd; const int* sceneOf;
@@ -75,6 +76,38 @@ struct TwoLevel {
             return false;
         }
         if (--budget < 0) { err |= kTravBudget; return true; }
+        if (a.tlasW == 4) {   // four children, hit ones sorted by entry distance, nearest taken, others pushed far to near
+            const float INF = 3.4e38f;
+            const float4* nb = a.tlas + 8 * (size_t)next;
+            const float4 lx = ld4(nb), hx = ld4(nb + 1), ly = ld4(nb + 2), hy = ld4(nb + 3), lz = ld4(nb + 4), hz = ld4(nb + 5), cf = ld4(nb + 6), kf = ld4(nb + 7);
+            const float LX[4] = { lx.x, lx.y, lx.z, lx.w }, HX[4] = { hx.x, hx.y, hx.z, hx.w }, LY[4] = { ly.x, ly.y, ly.z, ly.w };
+            const float HY[4] = { hy.x, hy.y, hy.z, hy.w }, LZ[4] = { lz.x, lz.y, lz.z, lz.w }, HZ[4] = { hz.x, hz.y, hz.z, hz.w };
+            const int CC[4] = { __float_as_int(cf.x), __float_as_int(cf.y), __float_as_int(cf.z), __float_as_int(cf.w) };
+            const int KK[4] = { __float_as_int(kf.x), __float_as_int(kf.y), __float_as_int(kf.z), __float_as_int(kf.w) };
+            float ht[4]; int he[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float x0 = fmaf(LX[j], idx, ox), x1 = fmaf(HX[j], idx, ox), y0 = fmaf(LY[j], idy, oy), y1 = fmaf(HY[j], idy, oy), z0 = fmaf(LZ[j], idz, oz), z1 = fmaf(HZ[j], idz, oz);
+                const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+                const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), hitT));
+                ht[j] = CC[j] >= 0 && tn <= tf ? tn : INF;
+                he[j] = KK[j] > 0 ? ~CC[j] : CC[j];
+            }
+#define CWPB_CSWAP(p, q) { if (ht[q] < ht[p]) { const float tf_ = ht[p]; ht[p] = ht[q]; ht[q] = tf_; const int ti_ = he[p]; he[p] = he[q]; he[q] = ti_; } }
+            CWPB_CSWAP(0, 1) CWPB_CSWAP(2, 3) CWPB_CSWAP(0, 2) CWPB_CSWAP(1, 3) CWPB_CSWAP(1, 2)
+#undef CWPB_CSWAP
+            int go;
+            if (ht[0] == INF) { if (tsp == 0) return true; go = tstack[--tsp]; }
+            else {
+                if (tsp + 3 > kTlasStack) { err |= kTravOverflow; return true; }
+                if (ht[3] < INF) tstack[tsp++] = he[3];
+                if (ht[2] < INF) tstack[tsp++] = he[2];
+                if (ht[1] < INF) tstack[tsp++] = he[1];
+                go = he[0];
+            }
+            if (go < 0) enter(a.inst, a.meshRoot, ~go); else next = go;
+            return false;
+        }
         const float4* nb = a.tlas + 4 * (size_t)next;
         const float4 n0 = ld4(nb), n1 = ld4(nb + 1), nz = ld4(nb + 2), mt = ld4(nb + 3);
         const int c0 = __float_as_int(mt.x), c1 = __float_as_int(mt.y), k0 = __float_as_int(mt.z), k1 = __float_as_int(mt.w);
@@ -192,7 +225,8 @@ struct cwp_batch {
     int nScenes = 0; int64_t nInst = 0;
     std::vector<int> sceneFirst;         // nScenes + 1
     cwp_instance* inst = nullptr; int64_t capInst = 0;
-    float4 *instLo = nullptr, *instHi = nullptr, *tlas = nullptr;
+    float4 *instLo = nullptr, *instHi = nullptr, *tlas = nullptr, *tlas4 = nullptr;   // TLAS in BVH2 and width-4 form
+    int tlasWidth = 4;                   // the form the traversal reads
     int *sceneRoot = nullptr, *segFirstTlas = nullptr; int capScenes = 0;
     // incremental form: fixed regions of `fixedCap` instances per scene, updates built over a compact copy
     int fixedCap = 0;
@@ -214,7 +248,7 @@ static void batch_free(cwp_batch* b) {
     for (auto& l : b->lay) free_wide(l);
     b->blasB.release(); b->tlasB.release();
     cudaFree(b->triV); cudaFree(b->primLo); cudaFree(b->primHi); cudaFree(b->meshBox); cudaFree(b->meshFirstDev);
-    cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas); cudaFree(b->sceneRoot); cudaFree(b->segFirstTlas);
+    cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas); cudaFree(b->tlas4); cudaFree(b->sceneRoot); cudaFree(b->segFirstTlas);
     cudaFree(b->uInst); cudaFree(b->uLo); cudaFree(b->uHi); cudaFree(b->dstFirstTlas);
     cudaFree(b->err); cudaFree(b->cursor);
     for (int i = 0; i < 3; i++) cudaFree(b->meshRoot[i]);
@@ -345,6 +379,8 @@ static int batch_create(const cwp_mesh_view* meshes, int32_t n, const cwp_batch_
     b->blasB.device = b->device; b->tlasB.device = b->device;
     b->builder = opt ? opt->builder : 0;
     CWPB_CHECK(b->builder == 0 || b->builder == 1, CWP_ERR_INVALID, "builder %d is not 0 (GPU) or 1 (host)", b->builder);
+    b->tlasWidth = opt && opt->tlas_width ? opt->tlas_width : 4;
+    CWPB_CHECK(b->tlasWidth == 2 || b->tlasWidth == 4, CWP_ERR_INVALID, "TLAS width %d is not 2 or 4", b->tlasWidth);
     if (b->builder == 1) {
         if (int rc = host_build(b, meshes, n, opt ? opt->spatial : 0.f)) return rc;
     } else {
@@ -419,11 +455,12 @@ extern "C" int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int6
     CWPB_CHECK(nSeg <= (1 << kSegBits), CWP_ERR_INVALID, "%d non-empty scenes (limit %d)", nSeg, 1 << kSegBits);
     CWPB_CUDA(cudaSetDevice(b->device));
     if (n > b->capInst) {
-        cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas);
-        b->inst = nullptr; b->instLo = b->instHi = b->tlas = nullptr; b->capInst = 0;
+        cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas); cudaFree(b->tlas4);
+        b->inst = nullptr; b->instLo = b->instHi = b->tlas = b->tlas4 = nullptr; b->capInst = 0;
         CWPB_CUDA(cudaMalloc(&b->inst, (size_t)n * sizeof(cwp_instance)));
         CWPB_CUDA(cudaMalloc(&b->instLo, (size_t)n * sizeof(float4))); CWPB_CUDA(cudaMalloc(&b->instHi, (size_t)n * sizeof(float4)));
         CWPB_CUDA(cudaMalloc(&b->tlas, (size_t)4 * n * sizeof(float4)));
+        CWPB_CUDA(cudaMalloc(&b->tlas4, (size_t)8 * n * sizeof(float4)));
         b->capInst = n;
     }
     if (nScenes + 1 > b->capScenes) {
@@ -439,14 +476,14 @@ extern "C" int cwp_batch_set_scenes(cwp_batch* b, const cwp_instance* inst, int6
     if (n > 0) {
         instance_boxes(b->inst, (int)n, b->meshBox, b->instLo, b->instHi, b->st);
         if (int rc = b->tlasB.build(b->instLo, b->instHi, n, seg.data(), nSeg, b->st)) return rc;
-        emit_tlas(b->tlasB, (int)n, b->segFirstTlas, nSeg, b->tlas, b->st);
+        emit_tlas(b->tlasB, (int)n, b->segFirstTlas, nSeg, b->tlas, b->st, nullptr, b->tlas4);
     }
     CWPB_CUDA(cudaEventRecord(b->e1, b->st));
     CWPB_CUDA(cudaEventSynchronize(b->e1));
     float ms = 0; CWPB_CUDA(cudaEventElapsedTime(&ms, b->e0, b->e1)); b->tlasMs = ms;
     CWPB_CUDA(cudaGetLastError());
     b->nScenes = 0;   // not traceable until the new TLAS passes its check
-    if (int rc = check_tlas(b->tlas, (int)n, b->segFirstTlas, nSeg, b->err, b->st)) return rc;
+    if (int rc = check_tlas(b->tlas, (int)n, b->segFirstTlas, nSeg, b->err, b->st, nullptr, b->tlas4)) return rc;
     b->nScenes = nScenes; b->nInst = n; b->sceneFirst.assign(first, first + nScenes + 1); b->fixedCap = 0;
     return CWP_OK;
 }
@@ -459,11 +496,12 @@ extern "C" int cwp_batch_reserve_scenes(cwp_batch* b, int32_t nScenes, int32_t c
     const int64_t n = (int64_t)nScenes * cap;
     b->nScenes = 0;   // not traceable while the arrays change
     if (n > b->capInst) {
-        cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas);
-        b->inst = nullptr; b->instLo = b->instHi = b->tlas = nullptr; b->capInst = 0;
+        cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas); cudaFree(b->tlas4);
+        b->inst = nullptr; b->instLo = b->instHi = b->tlas = b->tlas4 = nullptr; b->capInst = 0;
         CWPB_CUDA(cudaMalloc(&b->inst, (size_t)n * sizeof(cwp_instance)));
         CWPB_CUDA(cudaMalloc(&b->instLo, (size_t)n * sizeof(float4))); CWPB_CUDA(cudaMalloc(&b->instHi, (size_t)n * sizeof(float4)));
         CWPB_CUDA(cudaMalloc(&b->tlas, (size_t)4 * n * sizeof(float4)));
+        CWPB_CUDA(cudaMalloc(&b->tlas4, (size_t)8 * n * sizeof(float4)));
         b->capInst = n;
     }
     if (n > b->capU) {
@@ -487,6 +525,7 @@ extern "C" int cwp_batch_reserve_scenes(cwp_batch* b, int32_t nScenes, int32_t c
     CWPB_CUDA(cudaMemsetAsync(b->sceneRoot, 0xff, (size_t)nScenes * sizeof(int), b->st));
     CWPB_CUDA(cudaMemsetAsync(b->inst, 0, (size_t)n * sizeof(cwp_instance), b->st));
     CWPB_CUDA(cudaMemsetAsync(b->tlas, 0, (size_t)4 * n * sizeof(float4), b->st));
+    CWPB_CUDA(cudaMemsetAsync(b->tlas4, 0, (size_t)8 * n * sizeof(float4), b->st));
     CWPB_CUDA(cudaStreamSynchronize(b->st));
     b->fixedCap = cap; b->nInst = n; b->nScenes = nScenes;
     b->sceneFirst.resize(nScenes + 1);
@@ -535,9 +574,9 @@ extern "C" int cwp_batch_update_scenes(cwp_batch* b, const int32_t* scenes, int3
         CWPB_CUDA(cudaMemcpyAsync(b->segFirstTlas, seg.data(), (size_t)(nSeg + 1) * sizeof(int), cudaMemcpyHostToDevice, b->st));
         instance_boxes(b->uInst, (int)total, b->meshBox, b->uLo, b->uHi, b->st);
         if (int rc = b->tlasB.build(b->uLo, b->uHi, total, seg.data(), nSeg, b->st)) return rc;
-        emit_tlas(b->tlasB, (int)total, b->segFirstTlas, nSeg, b->tlas, b->st, b->dstFirstTlas);
+        emit_tlas(b->tlasB, (int)total, b->segFirstTlas, nSeg, b->tlas, b->st, b->dstFirstTlas, b->tlas4);
         CWPB_CUDA(cudaGetLastError());
-        if (int rc = check_tlas(b->tlas, (int)total, b->segFirstTlas, nSeg, b->err, b->st, b->dstFirstTlas)) return rc;
+        if (int rc = check_tlas(b->tlas, (int)total, b->segFirstTlas, nSeg, b->err, b->st, b->dstFirstTlas, b->tlas4)) return rc;
     }
     for (int i = 0; i < nUpd; i++)
         if (rootOf[i] >= 0) CWPB_CUDA(cudaMemcpyAsync(b->sceneRoot + scenes[i], &rootOf[i], sizeof(int), cudaMemcpyHostToDevice, b->st));
@@ -552,7 +591,8 @@ static int launch(cwp_batch* b, const cwp_batch_tuning& t, bool any, const float
     const WideLayout& L = b->lay[lay_index(t.width)];
     CWPB_CHECK(L.nodes, CWP_ERR_STATE, "layout width %d was not emitted (cwp_batch_options.widths)", t.width);
     BatchArgs a;
-    a.nodes = L.nodes; a.tris = L.tris; a.tlas = b->tlas; a.sceneRoot = b->sceneRoot; a.inst = reinterpret_cast<const float4*>(b->inst);
+    a.nodes = L.nodes; a.tris = L.tris; a.tlas = b->tlasWidth == 4 ? b->tlas4 : b->tlas; a.tlasW = b->tlasWidth;
+    a.sceneRoot = b->sceneRoot; a.inst = reinterpret_cast<const float4*>(b->inst);
     a.meshRoot = b->meshRoot[lay_index(t.width)];
     a.nScenes = b->nScenes; a.ro = (const float4*)o; a.rd = (const float4*)d; a.sceneOf = sc; a.hits = (float4*)hits; a.hitInst = hinst;
     a.n = n; a.nDev = nDev; a.cursor = b->cursor; a.fetch = t.fetch; a.err = b->err;
@@ -635,6 +675,13 @@ extern "C" int cwp_batch_autotune(cwp_batch* b, const float* o, const float* d, 
     return cwp_batch_status(b);
 }
 
+extern "C" int cwp_batch_set_tlas_width(cwp_batch* b, int32_t width) {
+    CWPB_CHECK(b, CWP_ERR_INVALID, "batch is NULL");
+    CWPB_CHECK(width == 2 || width == 4, CWP_ERR_INVALID, "TLAS width %d is not 2 or 4", width);
+    b->tlasWidth = width;   // both forms are always built: the next traces read the chosen one
+    return CWP_OK;
+}
+
 extern "C" int cwp_batch_status(cwp_batch* b) {
     CWPB_CHECK(b, CWP_ERR_INVALID, "batch is NULL");
     CWPB_CUDA(cudaSetDevice(b->device));
@@ -681,8 +728,9 @@ extern "C" int cwp_batch_download_tlas(const cwp_batch* b, float* nodes, int64_t
     CWPB_CHECK(b, CWP_ERR_INVALID, "batch is NULL");
     CWPB_CHECK(b->nScenes > 0, CWP_ERR_STATE, "no scenes");
     CWPB_CUDA(cudaSetDevice(b->device));
-    if (nNodeF4) *nNodeF4 = 4 * b->nInst;
-    if (nodes && b->nInst) CWPB_CUDA(cudaMemcpy(nodes, b->tlas, (size_t)4 * b->nInst * sizeof(float4), cudaMemcpyDeviceToHost));
+    const int64_t stride = b->tlasWidth == 4 ? 8 : 4;   // the form the traversal reads
+    if (nNodeF4) *nNodeF4 = stride * b->nInst;
+    if (nodes && b->nInst) CWPB_CUDA(cudaMemcpy(nodes, b->tlasWidth == 4 ? b->tlas4 : b->tlas, (size_t)stride * b->nInst * sizeof(float4), cudaMemcpyDeviceToHost));
     if (roots) CWPB_CUDA(cudaMemcpy(roots, b->sceneRoot, (size_t)b->nScenes * sizeof(int), cudaMemcpyDeviceToHost));
     if (inst && b->nInst) {
         CWPB_CUDA(cudaMemcpy(inst, b->inst, (size_t)b->nInst * sizeof(cwp_instance), cudaMemcpyDeviceToHost));

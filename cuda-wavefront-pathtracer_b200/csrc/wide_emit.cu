@@ -262,33 +262,61 @@ int emit_wide(const SegBuilder& B, const int* segFirstHost, int nSeg, const floa
 }
 
 // ---------------- TLAS ----------------
-// dstFirst (may be NULL = segFirst): where segment s's nodes and instances live in the TLAS / instance arrays, when the
-// build ran over a compact copy of some scenes' instances (incremental updates of fixed per-scene regions)
-__global__ void k_tlas(const float4* __restrict__ bn, int nInst, const int* __restrict__ segFirst, int nSeg, float4* tlas, const int* __restrict__ dstFirst) {
+// One thread per binary inner node of a scene (or its single leaf): writes that node's TLAS entry in BVH2 form (two
+// children) and, when tlas4 is given, in width-4 form (its grandchildren: a child that is an instance stays one child,
+// an inner child contributes its two children). Every binary inner node gets an entry of each form, so both are
+// written in one pass with no numbering step; traversal of the width-4 form starts at the same root and only reaches
+// every other level. dstFirst (may be NULL = segFirst): where segment s's nodes and instances live in the TLAS /
+// instance arrays, when the build ran over a compact copy of some scenes' instances (incremental updates of fixed
+// per-scene regions).
+__global__ void k_tlas(const float4* __restrict__ bn, int nInst, const int* __restrict__ segFirst, int nSeg, float4* tlas, float4* tlas4,
+                       const int* __restrict__ dstFirst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nInst) return;
     int lo = 0, hi = nSeg - 1;
     while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (segFirst[mid] <= i) lo = mid; else hi = mid - 1; }
     const int s = lo, f = segFirst[s], m = segFirst[s + 1] - f, base = 2 * f - s, j = i - f, d0 = dstFirst ? dstFirst[s] : f;
+    const int end = base + 2 * m - 1;   // the scene's binary nodes: leaves [base, base + m), inner [base + m, end)
+    auto inside = [&](int c) { return c >= base && c < end; };
     int ch[2]; int outNode;
     if (m == 1) { if (j != 0) return; ch[0] = base; ch[1] = -1; outNode = d0; }
     else { if (j >= m - 1) return; const int b = base + m + j; ch[0] = node_left(bn, b); ch[1] = node_right(bn, b); outNode = d0 + j; }
-    for (int q = 0; q < 2; q++) if (ch[q] >= base + 2 * m - 1 || (ch[q] < base && !(q == 1 && ch[q] == -1))) ch[q] = -1;   // outside the scene's region
+    for (int q = 0; q < 2; q++) if (!inside(ch[q])) ch[q] = -1;   // outside the scene's region
+    // a child entry: box, reference (instance or output node), count (1 instance, 0 inner)
+    auto entry = [&](int c, float3& l, float3& h, int& ref, int& cnt) {
+        if (c < 0) { l = h = f3(kEmpty, kEmpty, kEmpty); ref = -1; cnt = 0; return; }
+        l = node_lo(bn, c); h = node_hi(bn, c);
+        if (c < base + m) { ref = d0 + (node_left(bn, c) - f); cnt = 1; }   // a leaf: the instance
+        else { ref = d0 + (c - base - m); cnt = 0; }
+    };
     float3 l[2], h[2]; int c[2], k[2];
-    for (int q = 0; q < 2; q++) {
-        if (ch[q] < 0) { l[q] = h[q] = f3(kEmpty, kEmpty, kEmpty); c[q] = -1; k[q] = 0; continue; }
-        l[q] = node_lo(bn, ch[q]); h[q] = node_hi(bn, ch[q]);
-        if (ch[q] < base + m) { c[q] = d0 + (node_left(bn, ch[q]) - f); k[q] = 1; }   // a leaf: the instance
-        else { c[q] = d0 + (ch[q] - base - m); k[q] = 0; }
+    for (int q = 0; q < 2; q++) entry(ch[q], l[q], h[q], c[q], k[q]);
+    if (tlas) {
+        float4* o = tlas + 4 * (size_t)outNode;
+        o[0] = make_float4(l[0].x, h[0].x, l[0].y, h[0].y);
+        o[1] = make_float4(l[1].x, h[1].x, l[1].y, h[1].y);
+        o[2] = make_float4(l[0].z, h[0].z, l[1].z, h[1].z);
+        o[3] = make_float4(__int_as_float(c[0]), __int_as_float(c[1]), __int_as_float(k[0]), __int_as_float(k[1]));
     }
-    float4* o = tlas + 4 * (size_t)outNode;
-    o[0] = make_float4(l[0].x, h[0].x, l[0].y, h[0].y);
-    o[1] = make_float4(l[1].x, h[1].x, l[1].y, h[1].y);
-    o[2] = make_float4(l[0].z, h[0].z, l[1].z, h[1].z);
-    o[3] = make_float4(__int_as_float(c[0]), __int_as_float(c[1]), __int_as_float(k[0]), __int_as_float(k[1]));
+    if (tlas4) {
+        int g[4] = { -1, -1, -1, -1 }, ng = 0;
+        for (int q = 0; q < 2; q++) {
+            if (ch[q] < 0) continue;
+            if (ch[q] < base + m) g[ng++] = ch[q];
+            else for (int r = 0; r < 2; r++) { const int x = r ? node_right(bn, ch[q]) : node_left(bn, ch[q]); if (inside(x)) g[ng++] = x; }
+        }
+        float3 gl[4], gh[4]; int gc[4], gk[4];
+        for (int q = 0; q < 4; q++) entry(g[q], gl[q], gh[q], gc[q], gk[q]);
+        float4* o = tlas4 + 8 * (size_t)outNode;
+        o[0] = make_float4(gl[0].x, gl[1].x, gl[2].x, gl[3].x); o[1] = make_float4(gh[0].x, gh[1].x, gh[2].x, gh[3].x);
+        o[2] = make_float4(gl[0].y, gl[1].y, gl[2].y, gl[3].y); o[3] = make_float4(gh[0].y, gh[1].y, gh[2].y, gh[3].y);
+        o[4] = make_float4(gl[0].z, gl[1].z, gl[2].z, gl[3].z); o[5] = make_float4(gh[0].z, gh[1].z, gh[2].z, gh[3].z);
+        o[6] = make_float4(__int_as_float(gc[0]), __int_as_float(gc[1]), __int_as_float(gc[2]), __int_as_float(gc[3]));
+        o[7] = make_float4(__int_as_float(gk[0]), __int_as_float(gk[1]), __int_as_float(gk[2]), __int_as_float(gk[3]));
+    }
 }
-void emit_tlas(const SegBuilder& B, int nInst, const int* segFirstDev, int nSeg, float4* tlas, cudaStream_t st, const int* dstFirstDev) {
-    if (nInst > 0) k_tlas<<<(nInst + 127) / 128, 128, 0, st>>>(B.nodes, nInst, segFirstDev, nSeg, tlas, dstFirstDev);
+void emit_tlas(const SegBuilder& B, int nInst, const int* segFirstDev, int nSeg, float4* tlas, cudaStream_t st, const int* dstFirstDev, float4* tlas4) {
+    if (nInst > 0) k_tlas<<<(nInst + 127) / 128, 128, 0, st>>>(B.nodes, nInst, segFirstDev, nSeg, tlas, tlas4, dstFirstDev);
 }
 
 __global__ void k_inst_boxes(const cwp_instance* __restrict__ inst, int n, const float4* __restrict__ meshBox, float4* lo, float4* hi) {
@@ -376,9 +404,31 @@ int check_wide(const WideLayout& w, int64_t nTris, int* dBad, cudaStream_t st) {
     CWPB_CHECK(h == 0, CWP_ERR_INVALID, "width-%d layout has an out-of-range child or triangle reference", w.width);
     return CWP_OK;
 }
-int check_tlas(const float4* tlas, int nInst, const int* segFirstDev, int nSeg, int* dBad, cudaStream_t st, const int* dstFirstDev) {
+// the width-4 entries: every instance reference inside the scene's instances, every inner reference an entry written
+// before its parent (grandchildren of the H-PLOC tree have lower indices), empty slots marked -1
+__global__ void k_check_tlas4(const float4* __restrict__ tlas4, int nInst, const int* __restrict__ segFirst, int nSeg, int* bad, const int* __restrict__ dstFirst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nInst) return;
+    int lo = 0, hi = nSeg - 1;
+    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (segFirst[mid] <= i) lo = mid; else hi = mid - 1; }
+    const int m = segFirst[lo + 1] - segFirst[lo], j = i - segFirst[lo], f = dstFirst ? dstFirst[lo] : segFirst[lo];
+    if (j >= (m == 1 ? 1 : m - 1)) return;
+    const int node = f + j;
+    const float4 cf = tlas4[8 * (size_t)node + 6], kf = tlas4[8 * (size_t)node + 7];
+    const int c[4] = { __float_as_int(cf.x), __float_as_int(cf.y), __float_as_int(cf.z), __float_as_int(cf.w) };
+    const int k[4] = { __float_as_int(kf.x), __float_as_int(kf.y), __float_as_int(kf.z), __float_as_int(kf.w) };
+    bool ok = true;
+    for (int q = 0; q < 4; q++) {
+        if (c[q] == -1) { ok &= k[q] == 0; continue; }
+        if (k[q] > 0) ok &= k[q] == 1 && c[q] >= f && c[q] < f + m;
+        else ok &= k[q] == 0 && c[q] >= f && c[q] < node;
+    }
+    if (!ok) atomicOr(bad, 1);
+}
+int check_tlas(const float4* tlas, int nInst, const int* segFirstDev, int nSeg, int* dBad, cudaStream_t st, const int* dstFirstDev, const float4* tlas4) {
     CWPB_CUDA(cudaMemsetAsync(dBad, 0, sizeof(int), st));
     if (nInst > 0) k_check_tlas<<<(nInst + 127) / 128, 128, 0, st>>>(tlas, nInst, segFirstDev, nSeg, dBad, dstFirstDev);
+    if (nInst > 0 && tlas4) k_check_tlas4<<<(nInst + 127) / 128, 128, 0, st>>>(tlas4, nInst, segFirstDev, nSeg, dBad, dstFirstDev);
     int h = 0;
     CWPB_CUDA(cudaMemcpyAsync(&h, dBad, sizeof(int), cudaMemcpyDeviceToHost, st));
     CWPB_CUDA(cudaStreamSynchronize(st));

@@ -22,10 +22,12 @@ int emit_wide(const SegBuilder& B, const int* segFirstHost, int nSeg, const floa
 void free_wide(WideLayout& w);
 
 // Per-scene TLAS from a segmented build over instance boxes: BVH2 nodes (leaves hold one instance, count 1) in the
-// region [first(s), first(s) + m) of scene s's instances; root(s) = first + m - 2 (first when m == 1). With
-// dstFirstDev, the build ran over a compact copy and segment s's nodes and instance references go to the region that
-// starts at dstFirstDev[s] instead of first(s).
-void emit_tlas(const SegBuilder& B, int nInst, const int* segFirstDev, int nSeg, float4* tlas, cudaStream_t st, const int* dstFirstDev = nullptr);
+// region [first(s), first(s) + m) of scene s's instances; root(s) = first + m - 2 (first when m == 1). With tlas4,
+// also the width-4 form (8 float4 per node, same indices and roots: each node's children are the BVH2 node's
+// grandchildren). With dstFirstDev, the build ran over a compact copy and segment s's nodes and instance references go
+// to the region that starts at dstFirstDev[s] instead of first(s).
+void emit_tlas(const SegBuilder& B, int nInst, const int* segFirstDev, int nSeg, float4* tlas, cudaStream_t st, const int* dstFirstDev = nullptr,
+               float4* tlas4 = nullptr);
 
 // World boxes of instances (the 8 corners of their mesh's root box through the object -> world rows).
 void instance_boxes(const cwp_instance* inst, int nInst, const float4* meshBox, float4* lo, float4* hi, cudaStream_t st);
@@ -37,6 +39,7 @@ void root_boxes(const SegBuilder& B, const int* segFirstDev, int nSeg, float4* m
 // Reference checks run after every build (CWP_ERR_INVALID if a child, triangle or instance index is out of range, or
 // an inner child does not come after its parent); dBad is one device int of scratch. Synchronise the stream.
 int check_wide(const WideLayout& w, int64_t nTris, int* dBad, cudaStream_t st);
-int check_tlas(const float4* tlas, int nInst, const int* segFirstDev, int nSeg, int* dBad, cudaStream_t st, const int* dstFirstDev = nullptr);
+int check_tlas(const float4* tlas, int nInst, const int* segFirstDev, int nSeg, int* dBad, cudaStream_t st, const int* dstFirstDev = nullptr,
+               const float4* tlas4 = nullptr);
 
 }  // namespace cwpb

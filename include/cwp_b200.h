@@ -247,7 +247,9 @@ typedef struct cwp_batch_options {
     int32_t builder;        /* 0: every BLAS on the GPU in one H-PLOC launch; 1: on the host cores (binned SAH, 32 bins,
                                SAH-collapsed CWBVH, spatial splits when `spatial` > 0), for resident scenes */
     float spatial;          /* builder 1: spatial-split overlap threshold (cwp_build_options.spatial) */
-    int32_t reserved[3];
+    int32_t tlas_width;     /* TLAS nodes the traversal reads: 4 (default when 0; each node holds the grandchildren of the
+                               BVH2 TLAS, about half the TLAS node visits) or 2 (the reference's BVH2 TLAS) */
+    int32_t reserved[2];
 } cwp_batch_options;
 
 typedef struct cwp_batch_tuning {
@@ -304,6 +306,10 @@ int cwp_batch_download(const cwp_batch* b, int32_t width, float* nodes, int64_t*
  * traced width); and the TLAS (BVH2 nodes, root per scene, instances with `root` set for the current tuning's width) */
 int cwp_batch_blas_root(const cwp_batch* b, int32_t width, int32_t mesh, int32_t* root);
 int cwp_batch_download_tlas(const cwp_batch* b, float* nodes, int64_t* n_node_float4, int32_t* roots, cwp_instance* inst);
+/* TLAS form the traversal reads from the next launch on (2 or 4; both are built by every scene update), and thereby
+ * the form cwp_batch_download_tlas returns (8 float4 per node for width 4: lo x, hi x, lo y, hi y, lo z, hi z of four
+ * children, references, counts; count 1 = an instance, reference -1 = an empty slot) */
+int cwp_batch_set_tlas_width(cwp_batch* b, int32_t width);
 int cwp_batch_status(cwp_batch* b);   /* synchronises; CWP_ERR_TRAVERSAL if a ray hit a stack bound or the visit budget */
 
 /* ------------------------------------------------------------------------------------------------------------------

@@ -824,8 +824,41 @@ static int trav_blas(int width, const V4* nodes, const V4* tv, V3 o, V3 d, float
  * orc_inst_stats; for cost studies) */
 static long long g_inst_stats[4]; static int g_inst_stats_on;
 void orc_inst_stats(int on, long long* out) { if (out) memcpy(out, g_inst_stats, sizeof g_inst_stats); memset(g_inst_stats, 0, sizeof g_inst_stats); g_inst_stats_on = on; }
-/* one ray through one two-level scene (root = its TLAS root, < 0 for an empty scene); returns -1 on a stack bound */
-static int o_inst1(int width, int any, const float* blas, const float* tris, const V4* T, int root, const float* inst, V3 o, V3 d, float tmin,
+/* One TLAS node of width 4 (8 float4: lo x, hi x, lo y, hi y, lo z, hi z of four children, child references,
+ * counts; count 1 = an instance, 0 = an inner node, reference -1 = empty): the hit children sorted by entry distance
+ * with the batched form's sorting network, the nearest returned and the others pushed far to near (instances as
+ * ~index). Returns 1 when it chose an entry (*go), 0 when nothing was hit, -1 on a stack bound. */
+static int o_tlas4_visit(const V4* T, int node, float idx, float idy, float idz, float ox, float oy, float oz, float tmin, float t,
+                         int* stack, int* sp, int* go) {
+    const float INF = 3.4e38f;
+    const V4* nb = T + 8 * (size_t)node;
+    const float LX[4] = { nb[0].x, nb[0].y, nb[0].z, nb[0].w }, HX[4] = { nb[1].x, nb[1].y, nb[1].z, nb[1].w };
+    const float LY[4] = { nb[2].x, nb[2].y, nb[2].z, nb[2].w }, HY[4] = { nb[3].x, nb[3].y, nb[3].z, nb[3].w };
+    const float LZ[4] = { nb[4].x, nb[4].y, nb[4].z, nb[4].w }, HZ[4] = { nb[5].x, nb[5].y, nb[5].z, nb[5].w };
+    const int CC[4] = { fi(nb[6].x), fi(nb[6].y), fi(nb[6].z), fi(nb[6].w) }, KK[4] = { fi(nb[7].x), fi(nb[7].y), fi(nb[7].z), fi(nb[7].w) };
+    float ht[4]; int he[4];
+    for (int j = 0; j < 4; j++) {
+        const float x0 = fmaf(LX[j], idx, ox), x1 = fmaf(HX[j], idx, ox), y0 = fmaf(LY[j], idy, oy), y1 = fmaf(HY[j], idy, oy), z0 = fmaf(LZ[j], idz, oz), z1 = fmaf(HZ[j], idz, oz);
+        const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+        const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), t));
+        ht[j] = CC[j] >= 0 && tn <= tf ? tn : INF;
+        he[j] = KK[j] > 0 ? ~CC[j] : CC[j];
+    }
+#define O_CSWAP(a, b) { if (ht[b] < ht[a]) { float q_ = ht[a]; ht[a] = ht[b]; ht[b] = q_; int r_ = he[a]; he[a] = he[b]; he[b] = r_; } }
+    O_CSWAP(0, 1) O_CSWAP(2, 3) O_CSWAP(0, 2) O_CSWAP(1, 3) O_CSWAP(1, 2)
+#undef O_CSWAP
+    if (ht[0] == INF) return 0;
+    if (*sp + 3 > 64) return -1;
+    if (ht[3] < INF) stack[(*sp)++] = he[3];
+    if (ht[2] < INF) stack[(*sp)++] = he[2];
+    if (ht[1] < INF) stack[(*sp)++] = he[1];
+    *go = he[0];
+    return 1;
+}
+
+/* one ray through one two-level scene (root = its TLAS root, < 0 for an empty scene); tlas_width 2 (BVH2 nodes) or
+ * 4 (o_tlas4_visit); returns -1 on a stack bound */
+static int o_inst1(int width, int tlas_width, int any, const float* blas, const float* tris, const V4* T, int root, const float* inst, V3 o, V3 d, float tmin,
                    float* pt, int* ph, float* pu, float* pv, int* phi) {
     float t = *pt, u = 0.f, v = 0.f; int h = -1, hi = -1, done = 0, bad = 0;
     if (root >= 0) {
@@ -833,6 +866,12 @@ static int o_inst1(int width, int any, const float* blas, const float* tris, con
         int stack[64], sp = 0, next = root;
         while (!done) {
             if (g_inst_stats_on) g_inst_stats[0]++;
+            int go;
+            if (tlas_width == 4) {
+                const int r = o_tlas4_visit(T, next, idx, idy, idz, ox, oy, oz, tmin, t, stack, &sp, &go);
+                if (r < 0) { bad = 1; break; }
+                if (r == 0) { if (sp == 0) break; go = stack[--sp]; }
+            } else {
             const V4 n0 = T[4 * next], n1 = T[4 * next + 1], nz = T[4 * next + 2], mt = T[4 * next + 3];
             const int c0 = fi(mt.x), c1 = fi(mt.y), k0 = fi(mt.z), k1 = fi(mt.w);
             const float a0 = fmaf(n0.x, idx, ox), a1 = fmaf(n0.y, idx, ox), a2 = fmaf(n0.z, idy, oy), a3 = fmaf(n0.w, idy, oy), a4 = fmaf(nz.x, idz, oz), a5 = fmaf(nz.y, idz, oz);
@@ -842,10 +881,11 @@ static int o_inst1(int width, int any, const float* blas, const float* tris, con
             const float t1n = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
             const float t1f = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), t));
             const int h0 = c0 >= 0 && t0n <= t0f, h1 = c1 >= 0 && t1n <= t1f;
-            int e0 = k0 > 0 ? ~c0 : c0, e1 = k1 > 0 ? ~c1 : c1, go;
+            int e0 = k0 > 0 ? ~c0 : c0, e1 = k1 > 0 ? ~c1 : c1;
             if (h0 && h1) { if (t1n < t0n) { int q = e0; e0 = e1; e1 = q; } if (sp == 64) { bad = 1; break; } stack[sp++] = e1; go = e0; }
             else if (h0 || h1) go = h0 ? e0 : e1;
             else { if (sp == 0) break; go = stack[--sp]; }
+            }
             while (go < 0) {   /* an instance: its BLAS in object space, then the next TLAS entry */
                 const float* I = inst + 28 * (size_t)(~go);
                 const V3 lo = v3(I[0] * o.x + I[1] * o.y + I[2] * o.z + I[3], I[4] * o.x + I[5] * o.y + I[6] * o.z + I[7], I[8] * o.x + I[9] * o.y + I[10] * o.z + I[11]);
@@ -869,14 +909,14 @@ static int o_inst1(int width, int any, const float* blas, const float* tris, con
     *pt = t; *ph = h; *pu = u; *pv = v; *phi = hi;
     return bad ? -1 : 0;
 }
-long orc_trace_inst(int width, int any, const float* blas, const float* tris, const float* tlas, const int* scene_root, int n_scenes, const float* inst,
+long orc_trace_inst(int width, int tlas_width, int any, const float* blas, const float* tris, const float* tlas, const int* scene_root, int n_scenes, const float* inst,
                     const float* ro, const float* rd, const int* scene_of, long n, float* hits, int* hit_inst) {
     long bad = 0;
     for (long i = 0; i < n; i++) {
         const V3 o = v3(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]), d = v3(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]);
         float t = rd[4 * i + 3], u, v; int h, hi;
         const int sc = scene_of[i], root = sc >= 0 && sc < n_scenes ? scene_root[sc] : -1;
-        if (o_inst1(width, any, blas, tris, (const V4*)tlas, root, inst, o, d, ro[4 * i + 3], &t, &h, &u, &v, &hi) < 0) bad++;
+        if (o_inst1(width, tlas_width, any, blas, tris, (const V4*)tlas, root, inst, o, d, ro[4 * i + 3], &t, &h, &u, &v, &hi) < 0) bad++;
         if (hits) { hits[4 * i] = t; hits[4 * i + 1] = u; hits[4 * i + 2] = v; hits[4 * i + 3] = iff(h); }
         hit_inst[i] = hi;
     }
@@ -1061,7 +1101,7 @@ static int o_tile_pixel(int j, int w, int h) {
     const int t = j >> 5, r = j & 31, tilesX = w >> 3;
     return ((t / tilesX) * 4 + (r >> 3)) * w + (t % tilesX) * 8 + (r & 7);
 }
-long orc_render_request(const void* reqp, int width, const float* blas, const float* tris, const float* tlas, int root, const float* inst,
+long orc_render_request(const void* reqp, int width, int tlas_width, const float* blas, const float* tris, const float* tlas, int root, const float* inst,
                         const float* mats, int n_mats, const int* mesh_mat, int gd, long j0, long j1, float* accum, long long* counts) {
     const OReq* R = (const OReq*)reqp; const OCam* C = &R->cam;
     const int N = C->w * C->h; long bad = 0;
@@ -1077,7 +1117,7 @@ long orc_render_request(const void* reqp, int width, const float* blas, const fl
         float* A = accum + 4 * (size_t)pix;
         for (int depth = 0;; depth++) {
             float t = 1e30f, u, v; int tri, hi;
-            if (o_inst1(width, 0, blas, tris, (const V4*)tlas, root, inst, o, d, 0.f, &t, &tri, &u, &v, &hi) < 0) bad++;
+            if (o_inst1(width, tlas_width, 0, blas, tris, (const V4*)tlas, root, inst, o, d, 0.f, &t, &tri, &u, &v, &hi) < 0) bad++;
             counts[0]++;
             if (tri < 0) { A[0] += T.x * sky.x; A[1] += T.y * sky.y; A[2] += T.z * sky.z; break; }
             const float* I = inst + 28 * (size_t)hi;
@@ -1110,7 +1150,7 @@ long orc_render_request(const void* reqp, int width, const float* blas, const fl
                     const V3 c = muls(mulv(mulv(T, e.f), sunE), fabsf(lL.z));
                     if (c.x > 0.f || c.y > 0.f || c.z > 0.f) {
                         float st = 1e30f, su, sv; int sh, shi;
-                        if (o_inst1(width, 1, blas, tris, (const V4*)tlas, root, inst, gl > 0.f ? up : dn, l, 0.f, &st, &sh, &su, &sv, &shi) < 0) bad++;
+                        if (o_inst1(width, tlas_width, 1, blas, tris, (const V4*)tlas, root, inst, gl > 0.f ? up : dn, l, 0.f, &st, &sh, &su, &sv, &shi) < 0) bad++;
                         counts[1]++;
                         if (sh < 0) { A[0] += c.x; A[1] += c.y; A[2] += c.z; }
                     }

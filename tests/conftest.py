@@ -50,7 +50,7 @@ def _load_oracle():
     L.orc_trace_prec.restype = C.c_long
     L.orc_trace_prec.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_trace_inst.restype = C.c_long
-    L.orc_trace_inst.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_long, C.c_void_p, C.c_void_p]
+    L.orc_trace_inst.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_long, C.c_void_p, C.c_void_p]
     L.orc_bsdf_eval.restype = None
     L.orc_bsdf_eval.argtypes = [C.c_void_p] * 5 + [C.c_int] + [C.c_void_p] * 3 + [C.c_long]
     L.orc_bsdf_sample.restype = None
@@ -58,7 +58,7 @@ def _load_oracle():
     L.orc_render_stats.restype = None
     L.orc_render_stats.argtypes = [C.c_int, C.c_void_p]
     L.orc_render_request.restype = C.c_long
-    L.orc_render_request.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
+    L.orc_render_request.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
     L.orc_half_round.restype = C.c_double
     L.orc_half_round.argtypes = [C.c_double, C.c_int]
     L.orc_rng.restype = C.c_float
@@ -121,13 +121,13 @@ class Oracle:
         res = occ if any_hit else hits
         return (res, st) if stats else res
 
-    def trace_inst(self, width, any_hit, blas, tris, tlas, scene_root, inst, o, d, scene_of):
-        """Two-level traversal of the batched form: (hits float4 [n, 4], hit instance [n])."""
+    def trace_inst(self, width, any_hit, blas, tris, tlas, scene_root, inst, o, d, scene_of, tlas_width=2):
+        """Two-level traversal of the batched form (TLAS nodes of width 2 or 4): (hits float4 [n, 4], hit instance [n])."""
         n = len(o)
         hits = np.zeros((n, 4), np.float32); hi = np.zeros(n, np.int32)
         a = [np.ascontiguousarray(x) for x in (blas, tris, tlas)]
         sr = np.ascontiguousarray(scene_root, np.int32); ins = np.ascontiguousarray(inst, np.float32); so = np.ascontiguousarray(scene_of, np.int32)
-        bad = self.L.orc_trace_inst(width, 1 if any_hit else 0, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, sr.ctypes.data, len(sr),
+        bad = self.L.orc_trace_inst(width, tlas_width, 1 if any_hit else 0, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, sr.ctypes.data, len(sr),
                                     ins.ctypes.data, np.ascontiguousarray(o).ctypes.data, np.ascontiguousarray(d).ctypes.data, so.ctypes.data, n,
                                     hits.ctypes.data, hi.ctypes.data)
         assert bad == 0
@@ -146,14 +146,14 @@ class Oracle:
                                wi.ctypes.data, w.ctypes.data, pdf.ctypes.data, ok.ctypes.data, n)
         return wi, w, pdf, ok
 
-    def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None):
+    def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None, tlas_width=2):
         """A serving request on the host: (accum [w h, 4], counts [2])."""
         n = req.cam.w * req.cam.h * req.spp
         j0, j1 = (0, n) if paths is None else paths
         acc = np.zeros((req.cam.w * req.cam.h, 4), np.float32); cnt = np.zeros(2, np.int64)
         a = [np.ascontiguousarray(x) for x in (blas, tris, tlas)]
         ins = np.ascontiguousarray(inst, np.float32); ms = np.ascontiguousarray(mats, np.float32); mm = np.ascontiguousarray(mesh_mat, np.int32)
-        bad = self.L.orc_render_request(C.addressof(req), width, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, int(root), ins.ctypes.data,
+        bad = self.L.orc_render_request(C.addressof(req), width, tlas_width, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, int(root), ins.ctypes.data,
                                         ms.ctypes.data, len(ms), mm.ctypes.data, gd, j0, j1, acc.ctypes.data, cnt.ctypes.data)
         assert bad == 0
         return acc, cnt

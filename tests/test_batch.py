@@ -102,3 +102,87 @@ def _brute_force(o, d, v):
         good = ok & (u >= 0) & (w >= 0) & (u + w <= 1) & (t > 0)
         best = np.where(good & (t < best), t, best)
     return best
+
+
+def _tlas2_from_boxes(cwp, lo, hi):
+    """host BVH2 over instance boxes (leaf = one instance; references are instance indices)"""
+    n = len(lo)
+    V = np.concatenate([np.stack([lo[i], hi[i], lo[i]]) for i in range(n)]).astype(np.float32)
+    tb = cwp.Bvh(cwp.Mesh.from_arrays(V, np.arange(3 * n, dtype=np.int32).reshape(n, 3)), variant=2, bins=32, leaf=1)
+    t = tb.nodes.copy(); tv = t.view(np.int32)
+    for r in range(3, len(t), 4):
+        for j in (0, 1):
+            if tv[r, 2 + j] > 0:
+                tv[r, j] = tb.order[tv[r, j]]
+    return t
+
+
+def tlas4_from_tlas2(t2):
+    """The width-4 TLAS of a BVH2 TLAS, node for node: node i's children are the grandchildren of BVH2 node i (a child
+    that is an instance stays one child). The GPU writes its width-4 TLAS by the same rule from the H-PLOC tree."""
+    E = np.float32(3.4e38)
+    n = len(t2) // 4
+    B = t2.reshape(n, 4, 4); iv = t2.view(np.int32).reshape(n, 4, 4)
+    child = lambda i, j: (iv[i, 3, j], iv[i, 3, 2 + j],
+                          (B[i, j, 0], B[i, j, 2], B[i, 2, 2 * j]), (B[i, j, 1], B[i, j, 3], B[i, 2, 2 * j + 1]))
+    out = np.zeros((n, 8, 4), np.float32); ov = out.view(np.int32)
+    for i in range(n):
+        kids = []
+        for j in (0, 1):
+            c, k, lo, hi = child(i, j)
+            if c < 0:
+                continue
+            if k > 0:
+                kids.append((c, 1, lo, hi))
+            else:
+                for jj in (0, 1):
+                    g, kg, glo, ghi = child(c, jj)
+                    if g >= 0:
+                        kids.append((g, 1 if kg > 0 else 0, glo, ghi))
+        for s in range(4):
+            if s < len(kids):
+                c, k, lo, hi = kids[s]
+                ov[i, 6, s], ov[i, 7, s] = c, k
+                for a in range(3):
+                    out[i, 2 * a, s], out[i, 2 * a + 1, s] = lo[a], hi[a]
+            else:
+                ov[i, 6, s], ov[i, 7, s] = -1, 0
+                for a in range(3):
+                    out[i, 2 * a, s], out[i, 2 * a + 1, s] = E, E
+    return out.reshape(8 * n, 4)
+
+
+def test_oracle_tlas4_matches_tlas2(cwp, oracle):
+    """The oracle's two-level traversal over a width-4 TLAS (grandchildren of a BVH2 TLAS) finds the same closest
+    hits and occlusion as over the BVH2 TLAS itself: 40 instances of a box field, rigid motions, random rays."""
+    g = golden("boxes64.npz")
+    mesh = cwp.Mesh.from_arrays(g["verts"], g["faces"], g["face_mat"])
+    bvh = cwp.Bvh(mesh, variant=8, bins=16, leaf=1)
+    rng = np.random.default_rng(5)
+    v = g["verts"].astype(np.float64); blo, bhi = v.min(0), v.max(0)
+    recs, lo, hi = [], [], []
+    for i in range(40):
+        m = cwp.xform_animate(0, 0, translate=tuple(rng.uniform(-60, 60, 3)), axis=tuple(rng.normal(size=3)), angle_deg=float(rng.uniform(0, 360)))
+        r = np.frombuffer(bytes(cwp.instances([m], [0])), np.float32).reshape(28).copy()
+        r[24] = np.array([0], np.int32).view(np.float32)[0]
+        recs.append(r)
+        A = m.reshape(3, 4).astype(np.float64)
+        cs = np.array([[x, y, z] for x in (blo[0], bhi[0]) for y in (blo[1], bhi[1]) for z in (blo[2], bhi[2])]) @ A[:, :3].T + A[:, 3]
+        lo.append(cs.min(0) - 1e-3); hi.append(cs.max(0) + 1e-3)
+    rec = np.array(recs, np.float32)
+    t2 = _tlas2_from_boxes(cwp, np.array(lo, np.float32), np.array(hi, np.float32))
+    t4 = tlas4_from_tlas2(t2)
+    o = np.zeros((3000, 4), np.float32); d = np.zeros((3000, 4), np.float32)
+    o[:, :3] = rng.uniform(-90, 90, (3000, 3)); dd = rng.normal(size=(3000, 3)); d[:, :3] = dd / np.linalg.norm(dd, axis=1, keepdims=True)
+    d[:, 3] = 1e30
+    sc = np.zeros(3000, np.int32); root = np.array([0], np.int32)
+    for any_hit in (False, True):
+        h2, i2 = oracle.trace_inst(8, any_hit, bvh.nodes, bvh.tris, t2, root, rec, o, d, sc, tlas_width=2)
+        h4, i4 = oracle.trace_inst(8, any_hit, bvh.nodes, bvh.tris, t4, root, rec, o, d, sc, tlas_width=4)
+        if any_hit:
+            assert np.array_equal(i2 >= 0, i4 >= 0)
+        else:
+            assert (i2 >= 0).mean() > 0.1
+            same = (i2 == i4) & (h2[:, 3].view(np.int32) == h4[:, 3].view(np.int32))
+            assert np.array_equal(h2[:, 0].view(np.uint32), h4[:, 0].view(np.uint32))   # closest t never depends on the order
+            assert same.mean() > 0.999

@@ -70,22 +70,25 @@ def test_binary_and_wide_boxes_contain_triangles(gpu, cwp, batch_case):
                     assert np.all(tlo[c:c + k] >= np.array(lo) - 1e-6) and np.all(thi[c:c + k] <= np.array(hi) + 1e-6)
 
 
+@pytest.mark.parametrize("tlas_width", [2, 4])
 @pytest.mark.parametrize("width", [2, 4, 8])
-def test_two_level_trace_matches_oracle(gpu, cwp, oracle, batch_case, width):
+def test_two_level_trace_matches_oracle(gpu, cwp, oracle, batch_case, width, tlas_width):
     meshes, xf, mesh_of, first, b, o, d, sc = batch_case
     b.set_tuning(block=128, width=width, fetch=8, smem_stack=0)
+    b.set_tlas_width(tlas_width)
     nodes, tris = b.download(width)
     tlas, roots, inst = b.download_tlas(len(first) - 1, len(mesh_of))
-    assert roots[2] == -1
+    assert roots[2] == -1 and len(tlas) == (8 if tlas_width == 4 else 4) * len(mesh_of)
     for any_hit in (False, True):
         h, hi = trace(gpu, b, o, d, sc, any_hit)
-        ho, hio = oracle.trace_inst(width, any_hit, nodes, tris, tlas, roots, inst, o, d, sc)
+        ho, hio = oracle.trace_inst(width, any_hit, nodes, tris, tlas, roots, inst, o, d, sc, tlas_width=tlas_width)
         if any_hit:
             assert np.array_equal(hi, hio) and np.array_equal(h[:, 3].view(np.int32), ho[:, 3].view(np.int32))
         else:
             assert np.array_equal(h.view(np.uint32), ho.view(np.uint32)) and np.array_equal(hi, hio)
     assert np.all(hi[sc == 99] == -1) and np.all(hi[sc == 2] == -1)
     assert (hi >= 0).mean() > 0.05   # the batch does hit geometry
+    b.set_tlas_width(4)
 
 
 @pytest.mark.parametrize("width", [2, 4, 8])
@@ -98,8 +101,10 @@ def test_two_level_trace_matches_reference_travinst(gpu, cwp, ref, batch_case, w
     meshes, xf, mesh_of, first, b, o, d, sc = batch_case
     b.set_tuning(block=128, width=width, fetch=8, smem_stack=0)
     nodes, tris = b.download(width)
+    h, hi = trace(gpu, b, o, d, sc)                           # the default width-4 TLAS
+    b.set_tlas_width(2)                                       # the reference's travInst reads a BVH2 TLAS
     tlas, roots, inst = b.download_tlas(len(first) - 1, len(mesh_of))
-    h, hi = trace(gpu, b, o, d, sc)
+    b.set_tlas_width(4)
     hr, hir = ref.trace_inst(width, False, nodes, tris, tlas, roots, inst, o, d, sc)
     tri, trr = h[:, 3].view(np.int32), hr[:, 3].view(np.int32)
     same = (tri == trr) & (hi == hir)
@@ -138,7 +143,7 @@ def test_tlas_rebuild_per_frame(gpu, cwp, oracle, batch_case):
     h, hi = trace(gpu, b, o, d, sc)
     nodes, tris = b.download(8)
     tlas, roots, inst = b.download_tlas(len(first) - 1, len(mesh_of))
-    ho, hio = oracle.trace_inst(8, False, nodes, tris, tlas, roots, inst, o, d, sc)
+    ho, hio = oracle.trace_inst(8, False, nodes, tris, tlas, roots, inst, o, d, sc, tlas_width=b.tlas_width)
     assert np.array_equal(h.view(np.uint32), ho.view(np.uint32)) and np.array_equal(hi, hio)
     assert b.info().tlas_build_ms > 0
     b.set_scenes(cwp.instances(xf, mesh_of), first)
@@ -180,7 +185,7 @@ def test_host_built_blas_match_oracle(gpu, cwp, oracle, spatial):
         h, hi = trace(gpu, hb, o, d, sc)
         nodes, tris = hb.download(width)
         tlas, roots, ins = hb.download_tlas(len(first) - 1, len(mesh_of))
-        ho, hio = oracle.trace_inst(width, False, nodes, tris, tlas, roots, ins, o, d, sc)
+        ho, hio = oracle.trace_inst(width, False, nodes, tris, tlas, roots, ins, o, d, sc, tlas_width=hb.tlas_width)
         assert np.array_equal(h.view(np.uint32), ho.view(np.uint32)) and np.array_equal(hi, hio)
         gb.set_tuning(128, width, 8, 0)
         g, gi = trace(gpu, gb, o, d, sc)
@@ -209,12 +214,13 @@ def test_degenerate_segments(gpu, cwp, oracle):
     o = np.zeros((n, 4), np.float32); o[:, :3] = rng.uniform(-3, 4, (n, 3)); o[:, 2] = 5.0
     d = np.zeros((n, 4), np.float32); v = rng.normal(size=(n, 3)); v[:, 2] = -np.abs(v[:, 2]) - 1.0; d[:, :3] = v / np.linalg.norm(v, axis=1, keepdims=True); d[:, 3] = 1e30
     sc = rng.integers(0, 4, n).astype(np.int32)
-    for width in (2, 4, 8):
+    for width, tw in ((2, 4), (4, 2), (8, 4), (8, 2)):
         b.set_tuning(64, width, 1, 1)
+        b.set_tlas_width(tw)
         h, hi = trace(gpu, b, o, d, sc)
         nodes, tris = b.download(width)
         tlas, roots, ins = b.download_tlas(4, 4)
-        ho, hio = oracle.trace_inst(width, False, nodes, tris, tlas, roots, ins, o, d, sc)
+        ho, hio = oracle.trace_inst(width, False, nodes, tris, tlas, roots, ins, o, d, sc, tlas_width=tw)
         assert np.array_equal(h.view(np.uint32), ho.view(np.uint32)) and np.array_equal(hi, hio)
         assert np.all(hi[sc == 0] == -1) and (hi[sc == 1] >= 0).any() and (hi[sc == 2] >= 0).any()
     b.trace(0, 0, 0, 0, 0, 0)   # n = 0: nothing to do, no error

@@ -67,7 +67,7 @@ def test_request_matches_oracle(gpu, cwp, oracle, serving):
     (acc, st), = run_all(s, [req])
     nodes, tris = b.download(b.tuning().width)
     tlas, roots, inst = b.download_tlas(4, _n_inst(b, 4))   # the server's slots are the batch's scenes; slot 0 held the request
-    ref, cnt = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, mats, base)
+    ref, cnt = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, mats, base, tlas_width=b.tlas_width)
     a = acc[:, :3] / req.spp; r = ref[:, :3] / req.spp
     assert cwp.imageio.psnr(a, r) >= 50.0
     assert abs(st.rays - cnt[0]) <= 2e-3 * cnt[0] and abs(st.shadow_rays - cnt[1]) <= 2e-3 * max(cnt[1], 1)
