@@ -423,6 +423,7 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
                config={"workload": args.workload, "scenes": n_s, "blas": info.n_blas, "tris": int(info.n_tris), "instances": int(info.n_instances),
                        "rays": n, "rays_per_scene": per, "hit_rate": hit_rate,
                        "tuning": {"block": tun.block, "width": tun.width, "fetch": tun.fetch, "smem_stack": tun.smem_stack, "sample_ms": tun.ms},
+                       "tlas_width": args.tlas_width,
                        "autotune_s": tune_s, "blas_builder": ["gpu h-ploc (one launch)", "host binned SAH"][args.builder], "blas_build_ms": info.blas_build_ms,
                        "blas_hploc_launches": info.blas_hploc_launches if args.builder == 0 else 0,
                        "tlas_build_ms": info.tlas_build_ms, "node_bytes": {"bvh2": int(info.node_bytes[0]), "bvh4": int(info.node_bytes[1]), "cwbvh": int(info.node_bytes[2])},
@@ -535,7 +536,7 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
                ms_per_step=1e3 / c["job_throughput_req_s"], higher_is_better=True, dtype="f32",
                config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "blas_builder": ["gpu h-ploc", "host binned SAH"][wl["builder"]],
                        "blas_build_ms": info.blas_build_ms, "scene_generation_s": gen_s, "depth": 8, "max_paths": wl["max_paths"], "max_requests": maxr_c,
-                       "regroup": bool(args.regroup), "policy": ["even share", "oldest first with backfill"][args.policy],
+                       "tlas_width": args.tlas_width, "regroup": bool(args.regroup), "policy": ["even share", "oldest first with backfill"][args.policy],
                        "materials": "OpenPBR subset: roughness U[0.05,1], metallic Bernoulli(0.3), 10% glass IOR 1.5",
                        "mix": {"requests": n_req, "arrival_rate_req_s": wl["rate"], "resolutions": "256^2, 512^2, 1280x720, 1920x1080", "spp": "1, 4, 16, 64, 256",
                                "continuous": strip(c), "plain": strip(p), "throughput_vs_plain": c["throughput_req_s"] / p["throughput_req_s"],
