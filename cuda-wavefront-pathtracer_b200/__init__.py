@@ -113,7 +113,12 @@ class ServerOptions(C.Structure):
 
 class Request(C.Structure):
     _fields_ = [("scene", C.c_int32), ("frame", C.c_int32), ("cam", Camera), ("spp", C.c_int32), ("max_depth", C.c_int32), ("seed", C.c_uint32),
-                ("sun_to", C.c_float * 3), ("sun_e", C.c_float * 3), ("sky", C.c_float * 3), ("sun_cos", C.c_float), ("eps", C.c_float)]
+                ("sun_to", C.c_float * 3), ("sun_e", C.c_float * 3), ("sky", C.c_float * 3), ("sun_cos", C.c_float), ("eps", C.c_float),
+                ("env", C.c_int32), ("env_rot_deg", C.c_float)]
+
+
+class EnvMap(C.Structure):
+    _fields_ = [("rgb", C.c_void_p), ("w", C.c_int32), ("h", C.c_int32), ("strength", C.c_float), ("pad", C.c_int32)]
 
 
 class RequestStats(C.Structure):
@@ -169,6 +174,9 @@ SIGNATURES = {
     "cwp_batch_create": (C.c_int, [C.POINTER(MeshView), C.c_int32, C.POINTER(BatchOptions), C.POINTER(C.c_void_p)]),
     "cwp_batch_destroy": (None, [C.c_void_p]),
     "cwp_batch_set_tlas_width": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cwp_server_set_envmaps": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "cwp_hdr_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
+    "cwp_envmap_build": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cwp_batch_reserve_scenes": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "cwp_batch_update_scenes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "cwp_batch_set_scenes": (C.c_int, [C.c_void_p, C.POINTER(Instance), C.c_int64, C.POINTER(C.c_int32), C.c_int32]),
@@ -594,8 +602,26 @@ def bsdf_sample_batch(mats, mat, wo, eta, gd, ux, uvw):
     return wi, w, pdf, ok
 
 
-def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun_e=None, sky=None, sun_angle_rad=None, eps=1e-3):
-    """A serving request; lighting defaults to the benchmark's sun and sky."""
+def hdr_load(path):
+    """Radiance .hdr file -> float32 [h, w, 3] linear radiance, row 0 = top"""
+    w, h = C.c_int32(), C.c_int32()
+    _check(lib().cwp_hdr_load(str(path).encode(), C.byref(w), C.byref(h), None))
+    rgb = np.zeros((h.value, w.value, 3), np.float32)
+    _check(lib().cwp_hdr_load(str(path).encode(), C.byref(w), C.byref(h), rgb.ctypes.data))
+    return rgb
+
+
+def envmap_build(rgb, strength=1.0):
+    """Importance-sampling tables of an equirectangular map: (texels [h, w, 4], marg [h + 1], cond [h, w + 1])"""
+    rgb = np.ascontiguousarray(rgb, np.float32); h, w = rgb.shape[:2]
+    tex = np.zeros((h, w, 4), np.float32); marg = np.zeros(h + 1, np.float32); cond = np.zeros((h, w + 1), np.float32)
+    _check(lib().cwp_envmap_build(rgb.ctypes.data, w, h, strength, tex.ctypes.data, marg.ctypes.data, cond.ctypes.data))
+    return tex, marg, cond
+
+
+def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun_e=None, sky=None, sun_angle_rad=None, eps=1e-3, env=-1, env_rot_deg=0.0):
+    """A serving request; lighting defaults to the benchmark's sun and sky (env = -1) or names one of the server's
+    environment maps."""
     from . import workloads as W
     sun_to = W.SUN_TO if sun_to is None else sun_to; sun_e = (W.SUN_E,) * 3 if sun_e is None else sun_e
     sky = W.SKY if sky is None else sky; sun_angle_rad = W.SUN_ANGLE_RAD if sun_angle_rad is None else sun_angle_rad
@@ -604,6 +630,7 @@ def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun
     s = np.array(sun_to, np.float64); s /= np.linalg.norm(s)
     r.sun_to[:] = tuple(float(x) for x in s); r.sun_e[:] = tuple(sun_e); r.sky[:] = tuple(sky)
     r.sun_cos = float(np.float32(math.cos(sun_angle_rad / 2.0))); r.eps = eps
+    r.env, r.env_rot_deg = env, env_rot_deg
     return r
 
 
@@ -619,6 +646,14 @@ class Server:
         h = C.c_void_p()
         _check(lib().cwp_server_create(batch._h, M, len(M), _iptr(base), C.byref(o), C.byref(h)))
         self._h = h
+
+    def set_envmaps(self, maps):
+        """maps: list of (rgb float32 [h, w, 3], strength); requests name them by index (Request.env)"""
+        keep = [np.ascontiguousarray(rgb, np.float32) for rgb, _ in maps]
+        arr = (EnvMap * max(len(maps), 1))()
+        for i, (rgb, (_, strength)) in enumerate(zip(keep, maps)):
+            arr[i].rgb, arr[i].w, arr[i].h, arr[i].strength = rgb.ctypes.data, rgb.shape[1], rgb.shape[0], strength
+        _check(lib().cwp_server_set_envmaps(self._h, arr, len(maps)))
 
     def set_scenes(self, descs, scene_first):
         first = np.ascontiguousarray(scene_first, np.int32)

@@ -20,6 +20,7 @@
 #include "runtime.h"
 #include "trav.cuh"
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <cstring>
 #include <deque>
@@ -32,7 +33,37 @@ struct SlotParams {
     cwp_camera cam;
     float3 sunTo, sunE, sky; float sunCos, eps;
     unsigned seed; int maxDepth, N; float4* accum;
+    // the request's environment map (envTex null: the constant sky): texels, CDF over rows, CDF within each row
+    const float4* envTex; const float* envMarg; const float* envCond; int envW, envH; float envRot;
 };
+
+// ---------------- environment map (scene/environment.h orientation; render/wavefront.cu:177-197, 319-331) ----------
+// equirectangular, row 0 = +z, the centre column facing +x, u growing toward -y; rotated by envRot about +z
+__device__ __forceinline__ void env_uv(const SlotParams& S, float3 d, float& u, float& v) {
+    u = 0.5f - (atan2f(d.y, d.x) - S.envRot) * (1.f / CWPB_TWO_PI); u -= floorf(u);
+    v = acosf(fminf(fmaxf(d.z, -1.f), 1.f)) * CWPB_INV_PI;
+}
+__device__ __forceinline__ float3 env_dir(const SlotParams& S, float u, float v) {
+    const float ph = (0.5f - u) * CWPB_TWO_PI + S.envRot, th = v * CWPB_PI, st = sinf(th);
+    return f3(st * cosf(ph), st * sinf(ph), cosf(th));
+}
+__device__ __forceinline__ void env_texel(const SlotParams& S, float3 d, int& x, int& y, float& v) {
+    float u; env_uv(S, d, u, v);
+    x = min((int)(u * S.envW), S.envW - 1); y = min((int)(v * S.envH), S.envH - 1);
+}
+// solid-angle density of sampling texel (x, y) at polar coordinate v: its probability over its solid angle
+__device__ __forceinline__ float env_pdf_texel(const SlotParams& S, int x, int y, float v) {
+    const float* cr = S.envCond + (size_t)y * (S.envW + 1);
+    const float puv = (S.envMarg[y + 1] - S.envMarg[y]) * (cr[x + 1] - cr[x]) * S.envW * S.envH;
+    const float st = sinf(v * CWPB_PI);
+    return st > 0.f ? puv / (2.f * CWPB_PI * CWPB_PI * st) : 0.f;
+}
+// largest i in [0, n) with cdf[i] <= u (cdf: n + 1 entries from 0 to 1)
+__device__ __forceinline__ int cdf_find(const float* cdf, int n, float u) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (cdf[mid] <= u) lo = mid; else hi = mid; }
+    return lo;
+}
 
 // queue entry k: o = (origin, tmin), d = (direction, tmax), scene id = slot, T = (throughput, pdf of the last BSDF
 // sample or 0), info = (slot, pixel, sample, depth)
@@ -121,8 +152,14 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
             const float4 O = a.in.o[k], D = a.in.d[k], H = a.hits[k];
             const float3 d = f3(D.x, D.y, D.z);
             const int tri = __float_as_int(H.w);
-            if (tri < 0) {   // miss: constant sky, BSDF-sampled only
-                add_rgb(S.accum, pix, T * S.sky);
+            if (tri < 0) {   // miss: the environment, weighted against its light sampling, or the constant sky
+                float3 L = S.sky;
+                if (S.envTex) {
+                    int x, y; float v; env_texel(S, d, x, y, v);
+                    L = f3(S.envTex[(size_t)y * S.envW + x].x, S.envTex[(size_t)y * S.envW + x].y, S.envTex[(size_t)y * S.envW + x].z);
+                    if (T4.w > 0.f) L = L * mis_power(T4.w, 0.5f * env_pdf_texel(S, x, y, v));   // T.w: the last BSDF sample's pdf
+                }
+                add_rgb(S.accum, pix, T * L);
                 ended = true;
             } else {
                 const cwp_instance& I = a.inst[a.hinst[k]];
@@ -150,13 +187,35 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                     const float3 up = p + ng * S.eps, dn = p - ng * S.eps;
                     const unsigned dr = (unsigned)depth + 1u;
                     const float ux1 = rnd_s(S.seed, pix, smp, dr, 7), ux2 = sample01(pix, smp, dr, 7, S.seed ^ 0x68E31DA4u);
-                    if (has_non_delta(M)) {   // sun next-event estimation (the only sampled light: weight 1)
-                        const float3 l = cone_dir(S.sunTo, S.sunCos, rnd_s(S.seed, pix, smp, dr, 2), rnd_s(S.seed, pix, smp, dr, 3));
+                    if (has_non_delta(M)) {
+                        // one light sample: the sun alone (weight 1), or with an environment map the sun or the map with
+                        // probability 1/2 each, the map's sample weighted against BSDF sampling by the power heuristic
+                        const float u2 = rnd_s(S.seed, pix, smp, dr, 2), u3 = rnd_s(S.seed, pix, smp, dr, 3);
+                        float3 l = f3(0.f, 0.f, 1.f), Le = S.sunE; float pl = 1.f; bool ok = true, isSun = true;
+                        if (S.envTex) {
+                            const float us = rnd_s(S.seed, pix, smp, dr, 5);
+                            pl = 0.5f;
+                            if (us >= 0.5f) {
+                                isSun = false; ok = false;
+                                const float ue = fminf((us - 0.5f) / 0.5f, 0.99999994f);
+                                const int y = cdf_find(S.envMarg, S.envH, ue);
+                                const float* cr = S.envCond + (size_t)y * (S.envW + 1);
+                                const int x = cdf_find(cr, S.envW, u2);
+                                const float v = (y + u3) / S.envH, w0 = cr[x + 1] - cr[x];
+                                float u = (x + 0.5f) / S.envW;
+                                if (w0 > 0.f) u = (x + fminf((u2 - cr[x]) / w0, 0.99999994f)) / S.envW;   // the rest of u2 within the texel
+                                l = env_dir(S, u, v);
+                                const float pe = env_pdf_texel(S, x, y, v);
+                                if (pe > 0.f) { pl = 0.5f * pe; const float4 t4 = S.envTex[(size_t)y * S.envW + x]; Le = f3(t4.x, t4.y, t4.z); ok = true; }
+                            }
+                        }
+                        if (isSun) l = cone_dir(S.sunTo, S.sunCos, u2, u3);
                         const float3 lL = f3(dot(l, tx), dot(l, ty), dot(l, ns));
                         const float gl = dot(ng, l);
-                        if (lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
+                        if (ok && lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
                             const BsdfValue e = bsdf_eval(M, woL, lL, eta, a.gdEnergy, ux1, ux2);
-                            contrib = T * e.f * S.sunE * fabsf(lL.z);
+                            const float w = isSun ? 1.f : mis_power(pl, e.pdf);
+                            contrib = T * e.f * Le * (fabsf(lL.z) * w / pl);
                             if (contrib.x > 0.f || contrib.y > 0.f || contrib.z > 0.f) { wantShadow = true; so = gl > 0.f ? up : dn; sd = l; }
                         }
                     }
@@ -267,6 +326,8 @@ struct cwp_server {
     std::vector<cwp_instance_desc> desc; std::vector<int> sceneFirst;
     // per slot: request id or -1, its instances (host) for the TLAS rebuild
     std::vector<int64_t> slotReq; std::vector<std::vector<cwp_instance>> slotInst; std::vector<int> admitted;   // slots admitted since the last TLAS update
+    struct EnvMap { float4* tex = nullptr; float* marg = nullptr; float* cond = nullptr; int w = 0, h = 0; };
+    std::vector<EnvMap> envs;   // environment maps the requests may name
     SlotParams* dSlots = nullptr; int* slotCnt = nullptr; std::vector<int> hSlotCnt;
     RayQueue q[2]{}; RayQueue qs{}; int* slotBins = nullptr; ShadowQueue sq{}; float4* hits = nullptr; int* hinst = nullptr; int* occ = nullptr; int* cnt = nullptr; int4* dChunks = nullptr;
     int* hcnt = nullptr;   // pinned: [0..1] counts, then slot counters
@@ -294,6 +355,7 @@ extern "C" void cwp_server_destroy(cwp_server* s) {
     for (auto& kv : s->reqs) if (kv.second.accum) cudaFreeAsync(kv.second.accum, s->st);
     if (s->st) cudaStreamSynchronize(s->st);
     if (s->pool) cudaMemPoolDestroy(s->pool);
+    for (auto& e : s->envs) { cudaFree(e.tex); cudaFree(e.marg); cudaFree(e.cond); }
     for (void* p : s->allocs) cudaFree(p);
     if (s->hcnt) cudaFreeHost(s->hcnt);
     if (s->hSlots) cudaFreeHost(s->hSlots);
@@ -384,10 +446,39 @@ extern "C" int cwp_server_set_scenes(cwp_server* s, const cwp_instance_desc* des
     return CWP_OK;
 }
 
+extern "C" int cwp_server_set_envmaps(cwp_server* s, const cwp_envmap* maps, int32_t n) {
+    CWPB_CHECK(s && n >= 0 && (n == 0 || maps), CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(s->reqs.empty(), CWP_ERR_STATE, "environment maps change only while no request is queued or running");
+    CWPB_CUDA(cudaSetDevice(s->device));
+    std::vector<cwp_server::EnvMap> built;
+    auto drop = [&]() { for (auto& e : built) { cudaFree(e.tex); cudaFree(e.marg); cudaFree(e.cond); } };
+    for (int i = 0; i < n; i++) {
+        const cwp_envmap& m = maps[i];
+        CWPB_CHECK(m.rgb && m.w > 0 && m.h > 0 && (int64_t)m.w * m.h < (1ll << 28), CWP_ERR_INVALID, "environment map %d: %dx%d", i, m.w, m.h);
+        const size_t nt = (size_t)m.w * m.h;
+        std::vector<float> tex(4 * nt), marg((size_t)m.h + 1), cond((size_t)m.h * (m.w + 1));
+        if (int rc = cwp_envmap_build(m.rgb, m.w, m.h, m.strength, tex.data(), marg.data(), cond.data())) { drop(); return rc; }
+        cwp_server::EnvMap E; E.w = m.w; E.h = m.h;
+        cudaError_t e = cudaMalloc(&E.tex, nt * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMalloc(&E.marg, marg.size() * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&E.cond, cond.size() * sizeof(float));
+        if (e == cudaSuccess) e = cudaMemcpy(E.tex, tex.data(), nt * sizeof(float4), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(E.marg, marg.data(), marg.size() * sizeof(float), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(E.cond, cond.data(), cond.size() * sizeof(float), cudaMemcpyHostToDevice);
+        built.push_back(E);
+        if (e != cudaSuccess) { drop(); return set_error(e == cudaErrorMemoryAllocation ? CWP_ERR_NOMEM : CWP_ERR_CUDA, "environment map %d: %s", i, cudaGetErrorString(e)); }
+    }
+    for (auto& e : s->envs) { cudaFree(e.tex); cudaFree(e.marg); cudaFree(e.cond); }
+    s->envs = built;
+    return CWP_OK;
+}
+
 extern "C" int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* id) {
     CWPB_CHECK(s && r && id, CWP_ERR_INVALID, "NULL argument");
     CWPB_CHECK(!s->sceneFirst.empty(), CWP_ERR_STATE, "no scenes (cwp_server_set_scenes)");
     CWPB_CHECK(r->scene >= 0 && r->scene + 1 < (int)s->sceneFirst.size(), CWP_ERR_INVALID, "scene %d out of range", r->scene);
+    CWPB_CHECK(r->env >= -1 && r->env < (int)s->envs.size(), CWP_ERR_INVALID, "environment map %d out of range (%d maps)", r->env, (int)s->envs.size());
+    CWPB_CHECK(std::isfinite(r->env_rot_deg), CWP_ERR_INVALID, "environment rotation is not finite");
     CWPB_CHECK(r->cam.w > 0 && r->cam.h > 0 && r->spp > 0 && r->max_depth >= 0 && r->max_depth <= 64, CWP_ERR_INVALID, "bad request size");
     const int64_t total = (int64_t)r->cam.w * r->cam.h * r->spp;
     CWPB_CHECK(total < (1ll << 31), CWP_ERR_INVALID, "%lld paths in one request (limit 2^31)", (long long)total);
@@ -446,6 +537,10 @@ static int admit(cwp_server* s, bool& changed) {
         P.cam = q.r.cam; P.sunTo = f3(q.r.sun_to[0], q.r.sun_to[1], q.r.sun_to[2]); P.sunE = f3(q.r.sun_e[0], q.r.sun_e[1], q.r.sun_e[2]);
         P.sky = f3(q.r.sky[0], q.r.sky[1], q.r.sky[2]); P.sunCos = q.r.sun_cos; P.eps = q.r.eps; P.seed = q.r.seed; P.maxDepth = q.r.max_depth;
         P.N = q.r.cam.w * q.r.cam.h; P.accum = q.accum;
+        if (q.r.env >= 0) {
+            const cwp_server::EnvMap& E = s->envs[q.r.env];
+            P.envTex = E.tex; P.envMarg = E.marg; P.envCond = E.cond; P.envW = E.w; P.envH = E.h; P.envRot = q.r.env_rot_deg * 3.14159265f / 180.f;
+        }
         s->slotsDirty = true;
         CWPB_CUDA(cudaMemsetAsync(s->slotCnt + kSlotCounters * slot, 0, kSlotCounters * sizeof(int), s->st));
         // the scene's instances at the request's frame

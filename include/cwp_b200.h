@@ -351,6 +351,10 @@ typedef struct cwp_request {
     uint32_t seed;
     float sun_to[3], sun_e[3], sky[3];
     float sun_cos, eps;    /* cos of the sun's half angle; ray offset */
+    int32_t env;           /* environment map of the server (cwp_server_set_envmaps) lighting the request, or -1: the
+                              constant sky. With a map, a light sample picks the sun or the map with probability 1/2 each,
+                              the map by luminance x sin(theta), combined with BSDF sampling by the power heuristic */
+    float env_rot_deg;     /* rotation of the map about +z (the reference's --env_rot) */
 } cwp_request;
 
 typedef struct cwp_request_stats {
@@ -366,6 +370,12 @@ void cwp_server_destroy(cwp_server* s);
  * frame gives their transforms); replaces the batch's scenes while the server lives. */
 int cwp_server_set_scenes(cwp_server* s, const cwp_instance_desc* desc, int64_t n, const int32_t* scene_first, int32_t n_scenes);
 int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* id);
+/* Environment maps the requests may name (cwp_request.env): equirectangular, row 0 = +z, the centre column facing +x
+ * (the reference's orientation, scene/environment.h:1-4); rgb = w x h x 3 linear floats scaled by strength. Replaces
+ * the server's maps; only while no request is queued or running. Replaces buildEnvMap's use in setupScene
+ * (app/scene_setup.cpp:252) for the serving form. */
+typedef struct cwp_envmap { const float* rgb; int32_t w, h; float strength; int32_t pad; } cwp_envmap;
+int cwp_server_set_envmaps(cwp_server* s, const cwp_envmap* maps, int32_t n);
 /* One step: admission, new camera paths, one bounce of every admitted request (closest hit + shading, sun shadow rays),
  * completion. *n_active / *n_pending: admitted / waiting requests after the step. Synchronous. */
 int cwp_server_step(cwp_server* s, int32_t* n_active, int32_t* n_pending);
@@ -396,6 +406,16 @@ int cwp_bsdf_sample_batch(const cwp_material* mats, int32_t n_mats, const int32_
  * (io/image.cpp tonemapSRGB8: divide by spp, clip, sRGB OETF); 1 = Reinhard; 2 = ACES fit; exposure in EV.
  * ------------------------------------------------------------------------------------------------------------------ */
 int cwp_display(const float* d_accum, uint8_t* d_rgba, int64_t n, int32_t spp, float exposure_ev, int32_t mode, void* stream);
+
+/* ------------------------------------------------------------------------------------------------------------------
+ * Environment maps on the host. cwp_hdr_load replaces loadHDR (io/hdr_image.cpp:13-45): a Radiance RGBE file
+ * (new-style run-length or flat scanlines, '-Y H +X W') into w x h x 3 floats, row 0 = top; rgb = NULL queries the
+ * size. cwp_envmap_build replaces buildEnvMap's tables (scene/environment.cpp:7-38): texels = w x h float4 radiance x
+ * strength, marg = h + 1 floats (CDF over rows), cond = h rows of w + 1 floats (CDF within each row), texel weight
+ * luminance x sin(theta); the same float tables as the reference's for the same input.
+ * ------------------------------------------------------------------------------------------------------------------ */
+int cwp_hdr_load(const char* path, int32_t* w, int32_t* h, float* rgb);
+int cwp_envmap_build(const float* rgb, int32_t w, int32_t h, float strength, float* texels, float* marg, float* cond);
 
 /* ------------------------------------------------------------------------------------------------------------------
  * On-chip read bandwidth of a device, for the traversal kernels' roofline (not in the reference, whose node and

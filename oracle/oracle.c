@@ -1095,16 +1095,65 @@ void orc_bsdf_sample(const float* mats, const int* mat, const float* wo, const f
  * in the CUDA path order (pixel = tile order of j mod N, sample j / N); accum = w * h float4 sums, counts[0] closest
  * rays, counts[1] shadow rays. */
 typedef struct { float pos[3], ax[3], ay[3], az[3], fx, fy, px, py; int w, h; float lens_r, focus_d; } OCam;
-typedef struct { int scene, frame; OCam cam; int spp, max_depth; unsigned seed; float sun_to[3], sun_e[3], sky[3], sun_cos, eps; } OReq;
+typedef struct { int scene, frame; OCam cam; int spp, max_depth; unsigned seed; float sun_to[3], sun_e[3], sky[3], sun_cos, eps; int env; float env_rot_deg; } OReq;
+
+/* Environment map tables (scene/environment.cpp:7-38): texels = rgb x strength (float4), marg = CDF over rows (h + 1),
+ * cond = CDF within each row (h rows of w + 1); texel weight luminance x sin(theta), sums in double. */
+void orc_envmap_build(const float* rgb, int w, int h, float strength, float* texels, float* marg, float* cond) {
+    const double pi = 3.14159265358979323846;
+    double* row = (double*)malloc(sizeof(double) * (size_t)(w + 1));
+    double* rs = (double*)malloc(sizeof(double) * (size_t)h);
+    for (int y = 0; y < h; y++) {
+        const double st = sin(pi * (y + 0.5) / h);
+        row[0] = 0.0;
+        for (int x = 0; x < w; x++) {
+            const float* c = rgb + ((size_t)y * w + x) * 3;
+            float* t = texels + 4 * ((size_t)y * w + x);
+            t[0] = c[0] * strength; t[1] = c[1] * strength; t[2] = c[2] * strength; t[3] = 0.f;
+            const double lum = 0.2126 * t[0] + 0.7152 * t[1] + 0.0722 * t[2];
+            row[x + 1] = row[x] + (lum > 0 ? lum : 0.0) * st;
+        }
+        rs[y] = row[w];
+        for (int x = 0; x <= w; x++) cond[(size_t)y * (w + 1) + x] = rs[y] > 0 ? (float)(row[x] / rs[y]) : (float)x / w;
+        cond[(size_t)y * (w + 1) + w] = 1.f;
+    }
+    double acc = 0.0, tot = 0.0;
+    for (int y = 0; y < h; y++) tot += rs[y];
+    marg[0] = 0.f;
+    for (int y = 0; y < h; y++) { acc += rs[y]; marg[y + 1] = tot > 0 ? (float)(acc / tot) : (float)(y + 1) / h; }
+    marg[h] = 1.f;
+    free(row); free(rs);
+}
+
+/* environment lookups of the serving integrator (render/wavefront.cu:177-197): equirectangular, row 0 = +z, centre
+ * column +x, rotated by rot about +z */
+typedef struct { const float* tex; const float* marg; const float* cond; int w, h; float rot; } OEnv;
+static void o_env_texel(const OEnv* E, V3 d, int* x, int* y, float* v) {
+    float u = 0.5f - (atan2f(d.y, d.x) - E->rot) * (1.f / 6.2831853f); u -= floorf(u);
+    *v = acosf(fminf(fmaxf(d.z, -1.f), 1.f)) * 0.31830989f;
+    *x = (int)(u * E->w); if (*x > E->w - 1) *x = E->w - 1;
+    *y = (int)(*v * E->h); if (*y > E->h - 1) *y = E->h - 1;
+}
+static float o_env_pdf_texel(const OEnv* E, int x, int y, float v) {
+    const float* cr = E->cond + (size_t)y * (E->w + 1);
+    const float puv = (E->marg[y + 1] - E->marg[y]) * (cr[x + 1] - cr[x]) * E->w * E->h;
+    const float st = sinf(v * 3.14159265f);
+    return st > 0.f ? puv / (2.f * 3.14159265f * 3.14159265f * st) : 0.f;
+}
+static int o_cdf_find(const float* cdf, int n, float u) { int lo = 0, hi = n; while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (cdf[mid] <= u) lo = mid; else hi = mid; } return lo; }
+static float o_mis(float a, float b) { const float a2 = a * a; return a2 / (a2 + b * b); }
 static int o_tile_pixel(int j, int w, int h) {
     if ((w & 7) | (h & 3)) return j;
     const int t = j >> 5, r = j & 31, tilesX = w >> 3;
     return ((t / tilesX) * 4 + (r >> 3)) * w + (t % tilesX) * 8 + (r & 7);
 }
 long orc_render_request(const void* reqp, int width, int tlas_width, const float* blas, const float* tris, const float* tlas, int root, const float* inst,
-                        const float* mats, int n_mats, const int* mesh_mat, int gd, long j0, long j1, float* accum, long long* counts) {
+                        const float* mats, int n_mats, const int* mesh_mat, int gd, long j0, long j1, float* accum, long long* counts,
+                        const float* env_tex, const float* env_marg, const float* env_cond, int env_w, int env_h) {
     const OReq* R = (const OReq*)reqp; const OCam* C = &R->cam;
     const int N = C->w * C->h; long bad = 0;
+    const OEnv E = { env_tex, env_marg, env_cond, env_w, env_h, R->env_rot_deg * 3.14159265f / 180.f };
+    const int hasEnv = R->env >= 0 && env_tex != NULL;
     const V3 sunTo = v3(R->sun_to[0], R->sun_to[1], R->sun_to[2]), sunE = v3(R->sun_e[0], R->sun_e[1], R->sun_e[2]), sky = v3(R->sky[0], R->sky[1], R->sky[2]);
     for (long j = j0; j < j1; j++) {
         const int pix = o_tile_pixel((int)(j % N), C->w, C->h); const unsigned smp = (unsigned)(j / N), seed = R->seed;
@@ -1114,12 +1163,21 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
         V3 o = v3(C->pos[0], C->pos[1], C->pos[2]);
         V3 d = normz(sub(add(muls(v3(C->ax[0], C->ax[1], C->ax[2]), dx), muls(v3(C->ay[0], C->ay[1], C->ay[2]), dy)), v3(C->az[0], C->az[1], C->az[2])));
         V3 T = v3(1.f, 1.f, 1.f);
+        float lastPdf = 0.f;   /* pdf of the last BSDF sample (0: camera ray; <= 0: a delta lobe) */
         float* A = accum + 4 * (size_t)pix;
         for (int depth = 0;; depth++) {
             float t = 1e30f, u, v; int tri, hi;
             if (o_inst1(width, tlas_width, 0, blas, tris, (const V4*)tlas, root, inst, o, d, 0.f, &t, &tri, &u, &v, &hi) < 0) bad++;
             counts[0]++;
-            if (tri < 0) { A[0] += T.x * sky.x; A[1] += T.y * sky.y; A[2] += T.z * sky.z; break; }
+            if (tri < 0) {   /* miss: the environment weighted against its light sampling, or the constant sky */
+                V3 L = sky;
+                if (hasEnv) {
+                    int ex, ey; float ev; o_env_texel(&E, d, &ex, &ey, &ev);
+                    const float* tx4 = E.tex + 4 * ((size_t)ey * E.w + ex); L = v3(tx4[0], tx4[1], tx4[2]);
+                    if (lastPdf > 0.f) L = muls(L, o_mis(lastPdf, 0.5f * o_env_pdf_texel(&E, ex, ey, ev)));
+                }
+                A[0] += T.x * L.x; A[1] += T.y * L.y; A[2] += T.z * L.z; break;
+            }
             const float* I = inst + 28 * (size_t)hi;
             const V4* TR = (const V4*)tris;
             const V3 e1 = xyz4(TR[3 * tri + 1]), e2 = xyz4(TR[3 * tri + 2]), no = cross3(e1, e2);
@@ -1142,12 +1200,34 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
             const unsigned dr = (unsigned)depth + 1u;
             const float ux1 = orc_rng(pix, smp, dr, 7, seed), ux2 = orc_rng(pix, smp, dr, 7, seed ^ 0x68E31DA4u);
             if (o_non_delta(M)) {
-                const V3 l = cone_dir(sunTo, R->sun_cos, orc_rng(pix, smp, dr, 2, seed), orc_rng(pix, smp, dr, 3, seed));
+                /* one light sample (render/wavefront.cu:300-341 with the sun and the map as the lights) */
+                const float u2 = orc_rng(pix, smp, dr, 2, seed), u3 = orc_rng(pix, smp, dr, 3, seed);
+                V3 l = v3(0.f, 0.f, 1.f), Le = sunE; float pl = 1.f; int ok = 1, isSun = 1;
+                if (hasEnv) {
+                    const float us = orc_rng(pix, smp, dr, 5, seed);
+                    pl = 0.5f;
+                    if (us >= 0.5f) {
+                        isSun = 0; ok = 0;
+                        const float ue = fminf((us - 0.5f) / 0.5f, 0.99999994f);
+                        const int y = o_cdf_find(E.marg, E.h, ue);
+                        const float* cr = E.cond + (size_t)y * (E.w + 1);
+                        const int x = o_cdf_find(cr, E.w, u2);
+                        const float v = (y + u3) / E.h, w0 = cr[x + 1] - cr[x];
+                        float u = (x + 0.5f) / E.w;
+                        if (w0 > 0.f) u = (x + fminf((u2 - cr[x]) / w0, 0.99999994f)) / E.w;
+                        const float ph = (0.5f - u) * 6.2831853f + E.rot, th = v * 3.14159265f, st = sinf(th);
+                        l = v3(st * cosf(ph), st * sinf(ph), cosf(th));
+                        const float pe = o_env_pdf_texel(&E, x, y, v);
+                        if (pe > 0.f) { const float* t4 = E.tex + 4 * ((size_t)y * E.w + x); pl = 0.5f * pe; Le = v3(t4[0], t4[1], t4[2]); ok = 1; }
+                    }
+                }
+                if (isSun) l = cone_dir(sunTo, R->sun_cos, u2, u3);
                 const V3 lL = v3(dot3(l, tx), dot3(l, ty), dot3(l, ns));
                 const float gl = dot3(ng, l);
-                if (lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
+                if (ok && lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
                     const OEval e = o_bsdf_eval(M, woL, lL, eta, gd, ux1, ux2);
-                    const V3 c = muls(mulv(mulv(T, e.f), sunE), fabsf(lL.z));
+                    const float wgt_l = isSun ? 1.f : o_mis(pl, e.pdf);
+                    const V3 c = muls(mulv(mulv(T, e.f), Le), fabsf(lL.z) * wgt_l / pl);
                     if (c.x > 0.f || c.y > 0.f || c.z > 0.f) {
                         float st = 1e30f, su, sv; int sh, shi;
                         if (o_inst1(width, tlas_width, 1, blas, tris, (const V4*)tlas, root, inst, gl > 0.f ? up : dn, l, 0.f, &st, &sh, &su, &sv, &shi) < 0) bad++;
@@ -1163,7 +1243,7 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
             if (gi == 0.f || (gi > 0.f) != (wiL.z > 0.f)) break;
             T = mulv(T, wgt);
             if (!(fmaxf(T.x, fmaxf(T.y, T.z)) > 0.f)) break;
-            o = gi > 0.f ? up : dn; d = wi;
+            o = gi > 0.f ? up : dn; d = wi; lastPdf = pdf;
         }
     }
     return bad;

@@ -16,6 +16,8 @@
 #include "accel/traverse_inst.cuh"
 #include "core/rng.h"
 #include "scene/instances.h"
+#include "scene/environment.h"
+#include "io/hdr_image.h"
 #include "render/bsdf.h"
 #include "core/sampling.h"
 #include <algorithm>
@@ -230,3 +232,15 @@ extern "C" void ref_bsdf_sample(const void* mats, const int* mat, const float* w
     }
 }
 extern "C" int ref_material_size(void) { return (int)sizeof(Material); }
+
+// the reference's loadHDR + buildEnvMap on a Radiance file: sizes first (texels/marg/cond NULL), then the tables
+extern "C" int ref_env_build(const char* path, float strength, int* w, int* h, float* rgb, float* texels, float* marg, float* cond) {
+    EnvMapHost E;
+    if (!buildEnvMap(path, strength, E)) return -1;
+    *w = E.w; *h = E.h;
+    if (rgb) { int ww, hh; std::vector<float> v; if (!loadHDR(path, ww, hh, v)) return -1; memcpy(rgb, v.data(), v.size() * sizeof(float)); }
+    if (texels) for (size_t i = 0; i < E.texels.size(); i++) { texels[4 * i] = E.texels[i].x; texels[4 * i + 1] = E.texels[i].y; texels[4 * i + 2] = E.texels[i].z; texels[4 * i + 3] = E.texels[i].w; }
+    if (marg) memcpy(marg, E.marg.data(), E.marg.size() * sizeof(float));
+    if (cond) memcpy(cond, E.cond.data(), E.cond.size() * sizeof(float));
+    return 0;
+}

@@ -58,7 +58,10 @@ def _load_oracle():
     L.orc_render_stats.restype = None
     L.orc_render_stats.argtypes = [C.c_int, C.c_void_p]
     L.orc_render_request.restype = C.c_long
-    L.orc_render_request.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
+    L.orc_render_request.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
+                                     + [C.c_void_p] * 3 + [C.c_int, C.c_int])
+    L.orc_envmap_build.restype = None
+    L.orc_envmap_build.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_half_round.restype = C.c_double
     L.orc_half_round.argtypes = [C.c_double, C.c_int]
     L.orc_rng.restype = C.c_float
@@ -146,15 +149,24 @@ class Oracle:
                                wi.ctypes.data, w.ctypes.data, pdf.ctypes.data, ok.ctypes.data, n)
         return wi, w, pdf, ok
 
-    def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None, tlas_width=2):
-        """A serving request on the host: (accum [w h, 4], counts [2])."""
+    def envmap_build(self, rgb, strength=1.0):
+        rgb = np.ascontiguousarray(rgb, np.float32); h, w = rgb.shape[:2]
+        tex = np.zeros((h, w, 4), np.float32); marg = np.zeros(h + 1, np.float32); cond = np.zeros((h, w + 1), np.float32)
+        self.L.orc_envmap_build(rgb.ctypes.data, w, h, strength, tex.ctypes.data, marg.ctypes.data, cond.ctypes.data)
+        return tex, marg, cond
+
+    def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None, tlas_width=2, env=None):
+        """A serving request on the host: (accum [w h, 4], counts [2]). env: (texels, marg, cond) of the request's
+        environment map when Request.env >= 0, else None."""
         n = req.cam.w * req.cam.h * req.spp
         j0, j1 = (0, n) if paths is None else paths
         acc = np.zeros((req.cam.w * req.cam.h, 4), np.float32); cnt = np.zeros(2, np.int64)
         a = [np.ascontiguousarray(x) for x in (blas, tris, tlas)]
         ins = np.ascontiguousarray(inst, np.float32); ms = np.ascontiguousarray(mats, np.float32); mm = np.ascontiguousarray(mesh_mat, np.int32)
         bad = self.L.orc_render_request(C.addressof(req), width, tlas_width, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, int(root), ins.ctypes.data,
-                                        ms.ctypes.data, len(ms), mm.ctypes.data, gd, j0, j1, acc.ctypes.data, cnt.ctypes.data)
+                                        ms.ctypes.data, len(ms), mm.ctypes.data, gd, j0, j1, acc.ctypes.data, cnt.ctypes.data,
+                                        *((env[0].ctypes.data, env[1].ctypes.data, env[2].ctypes.data, env[0].shape[1], env[0].shape[0]) if env is not None
+                                          else (None, None, None, 0, 0)))
         assert bad == 0
         return acc, cnt
 

@@ -21,8 +21,16 @@ and tests/golden/bsdf.npz:
   outputs  the reference's bsdfEval f and pdf and bsdfSample wi / weight / pdf / success (render/bsdf.h), with the
            glossy-diffuse energy compensation off and on
 
+and tests/golden/env.npz:
+
+  inputs   two Radiance RGBE files written here (a 40x20 map with run-length scanlines: a sky gradient, a bright sun
+           disc, a dark band; a 6x4 map with flat scanlines), kept as bytes
+  outputs  the reference's loadHDR radiance and buildEnvMap tables (texels x strength 1.5, marginal and conditional
+           CDFs) for each file
+
 The fixtures pin the oracle and the library where the reference sources are absent. Run from the repository root:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          (every fixture)
+    python tests/golden/make_golden.py env      (env.npz only)
 """
 import importlib
 import os
@@ -60,6 +68,7 @@ def main():
     print("wrote", os.path.join(HERE, "boxes64.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
     instances(ref, out)
     bsdf(ref)
+    envmaps(ref)
 
 
 def instances(ref, box):
@@ -101,10 +110,6 @@ def instances(ref, box):
     out["bvh4_tris"], out["bvh4_woop"] = r["tris"], r["woop"]
     np.savez_compressed(os.path.join(HERE, "instances.npz"), **out)
     print("wrote", os.path.join(HERE, "instances.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
-
-
-if __name__ == "__main__":
-    main()
 
 
 def materials(rng, n):
@@ -151,3 +156,74 @@ def bsdf(ref):
         out.update({f"f{gd}": f, f"pdf{gd}": pdf, f"s_wi{gd}": sw, f"s_w{gd}": sWt, f"s_pdf{gd}": spdf, f"s_ok{gd}": ok})
     np.savez_compressed(os.path.join(HERE, "bsdf.npz"), **out)
     print("wrote", os.path.join(HERE, "bsdf.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
+
+
+def rgbe_bytes(rgb, rle):
+    """Radiance RGBE file content for float rgb [h, w, 3] (new-style run-length scanlines when rle, else flat)"""
+    h, w = rgb.shape[:2]
+    out = bytearray(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n" + f"-Y {h} +X {w}\n".encode())
+    px = np.zeros((h, w, 4), np.uint8)
+    for y in range(h):
+        for x in range(w):
+            m = float(rgb[y, x].max())
+            if m < 1e-32:
+                continue
+            mant, e = np.frexp(m)
+            sc = mant * 256.0 / m
+            px[y, x, :3] = np.clip((rgb[y, x] * sc).astype(np.int64), 0, 255); px[y, x, 3] = e + 128
+    for y in range(h):
+        if not rle:
+            out += px[y].tobytes(); continue
+        out += bytes([2, 2, w >> 8, w & 255])
+        for c in range(4):
+            v = px[y, :, c]; x = 0
+            while x < w:
+                r = 1
+                while x + r < w and r < 127 and v[x + r] == v[x]:
+                    r += 1
+                if r >= 3:
+                    out += bytes([128 + r, int(v[x])]); x += r; continue
+                s0 = x
+                while x < w and x - s0 < 128 and not (x + 2 < w and v[x] == v[x + 1] == v[x + 2]):
+                    x += 1
+                out += bytes([x - s0]) + v[s0:x].tobytes()
+    return bytes(out)
+
+
+def envmaps(ref):
+    import ctypes as C
+    import tempfile
+    L = ref.L
+    L.ref_env_build.restype = C.c_int
+    L.ref_env_build.argtypes = [C.c_char_p, C.c_float] + [C.c_void_p] * 6
+    h, w = 20, 40
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    big = np.stack([0.2 + 0.6 * (1 - yy / h), 0.3 + 0.5 * (1 - yy / h), 0.6 + 0.3 * (1 - yy / h)], -1)
+    big[((yy - 5) ** 2 + (xx - 28) ** 2) < 4] = (40.0, 36.0, 30.0)   # sun disc
+    big[14:16] = 0.0                                                  # dark band (zero-luminance rows)
+    big[:, 3:9] = (0.5, 0.5, 0.5)                                     # a flat block (runs)
+    small = np.random.default_rng(3).uniform(0, 4, (4, 6, 3)).astype(np.float32)
+    out = {}
+    for name, img, rle in (("big", big, True), ("small", small, False)):
+        data = rgbe_bytes(img, rle)
+        with tempfile.NamedTemporaryFile(suffix=".hdr", delete=False) as f:
+            f.write(data); path = f.name
+        ww, hh = C.c_int(), C.c_int()
+        assert L.ref_env_build(path.encode(), 1.5, C.byref(ww), C.byref(hh), None, None, None, None) == 0
+        W, H = ww.value, hh.value
+        rgb = np.zeros((H, W, 3), np.float32); tex = np.zeros((H, W, 4), np.float32)
+        marg = np.zeros(H + 1, np.float32); cond = np.zeros((H, W + 1), np.float32)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)
+        assert L.ref_env_build(path.encode(), 1.5, C.byref(ww), C.byref(hh), p(rgb), p(tex), p(marg), p(cond)) == 0
+        os.unlink(path)
+        out.update({f"{name}_hdr": np.frombuffer(data, np.uint8), f"{name}_rgb": rgb, f"{name}_tex": tex, f"{name}_marg": marg, f"{name}_cond": cond})
+    np.savez_compressed(os.path.join(HERE, "env.npz"), **out)
+    print("wrote", os.path.join(HERE, "env.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
+
+
+if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "env":
+        from conftest import REF_DIR, Ref
+        envmaps(Ref(os.path.join(REF_DIR, "libcwpref.so")))
+    else:
+        main()

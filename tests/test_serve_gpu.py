@@ -104,3 +104,43 @@ def test_admission_waits_for_memory(gpu, cwp, serving):
     for _ in range(3):
         a, p = s.step()
         assert a == 0 and p == 1
+
+
+def test_environment_request_matches_oracle(gpu, cwp, oracle, serving):
+    """A request lit by an environment map (importance-sampled by luminance x sin(theta), combined with BSDF sampling
+    by the power heuristic, rotated 30 degrees) and the sun: the image matches the oracle's restatement at >= 50 dB and
+    the ray counts agree; environment and sky requests in one mix give each request's image alone."""
+    from conftest import golden
+    b, descs, first, mats, base, boxes = serving
+    g = golden("env.npz")
+    env_rgb = g["big_rgb"]
+    s = server(cwp, serving, max_paths=1 << 16, max_requests=4)
+    s.set_envmaps([(env_rgb, 1.5)])
+    req = requests(cwp, boxes, 1, seed=13, res=((64, 48),), spps=(4,))[0]
+    req.env, req.env_rot_deg = 0, 30.0
+    (acc, st), = run_all(s, [req])
+    nodes, tris = b.download(b.tuning().width)
+    tlas, roots, inst = b.download_tlas(4, _n_inst(b, 4))
+    ref, cnt = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, mats, base, tlas_width=b.tlas_width,
+                                     env=cwp.envmap_build(env_rgb, 1.5))
+    a = acc[:, :3] / req.spp; r = ref[:, :3] / req.spp
+    assert cwp.imageio.psnr(a, r) >= 50.0
+    assert abs(st.rays - cnt[0]) <= 2e-3 * cnt[0] and abs(st.shadow_rays - cnt[1]) <= 2e-3 * max(cnt[1], 1)
+    # the environment adds light over the sky-lit request of the same path samples
+    sky_req = requests(cwp, boxes, 1, seed=13, res=((64, 48),), spps=(4,))[0]
+    (acc_sky, _), = run_all(s, [sky_req])
+    assert not np.allclose(acc, acc_sky)
+    # mixed with sky requests, and alone: the same images up to the order of float atomics
+    reqs = requests(cwp, boxes, 6, seed=17)
+    for i, rq in enumerate(reqs):
+        rq.env, rq.env_rot_deg = (0, 45.0 * i) if i % 2 == 0 else (-1, 0.0)
+    mix = run_all(s, reqs)
+    alone_s = server(cwp, serving, max_paths=1 << 15, max_requests=1)
+    alone_s.set_envmaps([(env_rgb, 1.5)])
+    alone = run_all(alone_s, reqs)
+    for (am, sm), (aa, sa) in zip(mix, alone):
+        assert sm.rays == sa.rays and sm.shadow_rays == sa.shadow_rays
+        assert np.allclose(am, aa, rtol=1e-4, atol=1e-5)
+    with pytest.raises(cwp.CwpError):
+        bad = requests(cwp, boxes, 1, seed=3)[0]; bad.env = 1   # only one map
+        s.submit(bad)
