@@ -117,6 +117,43 @@ class Request(C.Structure):
                 ("env", C.c_int32), ("env_rot_deg", C.c_float)]
 
 
+class Texture(C.Structure):
+    _fields_ = [("rgba", C.c_void_p), ("w", C.c_int32), ("h", C.c_int32), ("srgb", C.c_int32), ("pad", C.c_int32)]
+
+
+class MaterialTextures(C.Structure):
+    _fields_ = [("base_color", C.c_int32), ("emission", C.c_int32), ("normal", C.c_int32), ("metallic", C.c_int32), ("roughness", C.c_int32),
+                ("metallic_ch", C.c_int32), ("roughness_ch", C.c_int32), ("normal_scale", C.c_float)]
+
+
+def textures_array(images):
+    """(cwp_texture array, the uint8 arrays it points into) from a list of (rgba uint8 [h, w, 4], srgb)"""
+    keep = [np.ascontiguousarray(img, np.uint8) for img, _ in images]
+    arr = (Texture * max(len(images), 1))()
+    for i, (img, (_, srgb)) in enumerate(zip(keep, images)):
+        arr[i].rgba, arr[i].w, arr[i].h, arr[i].srgb = img.ctypes.data, img.shape[1], img.shape[0], 1 if srgb else 0
+    return arr, keep
+
+
+def material_textures(bindings):
+    """cwp_material_textures array from a list of dicts (keys base_color, emission, normal, metallic, roughness,
+    metallic_ch, roughness_ch, normal_scale; missing ids = -1)"""
+    arr = (MaterialTextures * max(len(bindings), 1))()
+    for i, b in enumerate(bindings):
+        for k in ("base_color", "emission", "normal", "metallic", "roughness"):
+            setattr(arr[i], k, b.get(k, -1))
+        arr[i].metallic_ch, arr[i].roughness_ch, arr[i].normal_scale = b.get("metallic_ch", 2), b.get("roughness_ch", 1), b.get("normal_scale", 1.0)
+    return arr
+
+
+def texture_sample_batch(images, ids, uv):
+    """device lookups (texture id, (u, v)) -> rgba float32 [n, 4] with the textures bound as the server binds them"""
+    arr, keep = textures_array(images)
+    ids = np.ascontiguousarray(ids, np.int32); uv = np.ascontiguousarray(uv, np.float32); out = np.zeros((len(ids), 4), np.float32)
+    _check(lib().cwp_texture_sample_batch(arr, len(images), _iptr(ids), uv.ctypes.data, out.ctypes.data, len(ids)))
+    return out
+
+
 class EnvMap(C.Structure):
     _fields_ = [("rgb", C.c_void_p), ("w", C.c_int32), ("h", C.c_int32), ("strength", C.c_float), ("pad", C.c_int32)]
 
@@ -175,6 +212,8 @@ SIGNATURES = {
     "cwp_batch_destroy": (None, [C.c_void_p]),
     "cwp_batch_set_tlas_width": (C.c_int, [C.c_void_p, C.c_int32]),
     "cwp_server_set_envmaps": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "cwp_server_set_textures": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "cwp_texture_sample_batch": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_void_p, C.c_void_p, C.c_int64]),
     "cwp_hdr_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
     "cwp_envmap_build": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cwp_batch_reserve_scenes": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
@@ -646,6 +685,15 @@ class Server:
         h = C.c_void_p()
         _check(lib().cwp_server_create(batch._h, M, len(M), _iptr(base), C.byref(o), C.byref(h)))
         self._h = h
+
+    def set_textures(self, images, bindings, uvs, tans=None):
+        """images: list of (rgba uint8 [h, w, 4], srgb); bindings: cwp_material_textures array (material_textures);
+        uvs: float32 [n_tris, 8] over all batch meshes in mesh order; tans: float32 [n_tris, 12] or None"""
+        arr, keep = textures_array(images)
+        uvs = np.ascontiguousarray(uvs, np.float32)
+        tans = np.ascontiguousarray(tans, np.float32) if tans is not None else None
+        _check(lib().cwp_server_set_textures(self._h, arr, len(images), bindings, len(bindings), uvs.ctypes.data,
+                                             tans.ctypes.data if tans is not None else None))
 
     def set_envmaps(self, maps):
         """maps: list of (rgb float32 [h, w, 3], strength); requests name them by index (Request.env)"""

@@ -749,5 +749,7 @@ int batch_trace_dev(cwp_batch* b, bool any, const float4* o, const float4* d, co
 const float4* batch_tris(const cwp_batch* b) { return b->lay[lay_index(b->tuning.width)].tris; }
 const cwp_instance* batch_instances(const cwp_batch* b) { return b->inst; }
 int batch_mesh_count(const cwp_batch* b) { return b->nMesh; }
+const int* batch_mesh_first(const cwp_batch* b) { return b->meshFirstDev; }
+int64_t batch_tri_count(const cwp_batch* b) { return b->nTris; }
 int batch_device(const cwp_batch* b) { return b->device; }
 }  // namespace cwpb

@@ -13,4 +13,6 @@ const float4* batch_tris(const cwp_batch* b);          // triangle records (v0, 
 const cwp_instance* batch_instances(const cwp_batch* b);
 int batch_mesh_count(const cwp_batch* b);
 int batch_device(const cwp_batch* b);
+const int* batch_mesh_first(const cwp_batch* b);       // device: nMesh + 1 offsets of each mesh's triangles in mesh order
+int64_t batch_tri_count(const cwp_batch* b);            // triangles of all meshes
 }  // namespace cwpb

@@ -108,6 +108,9 @@ struct ShadeArgs {
     int n; RayQueue in, out; ShadowQueue sq;
     const float4* hits; const int* hinst; const cwp_instance* inst; const float4* tris;
     const cwp_material* mats; int nMats; const int* meshMat; const SlotParams* slots; int gdEnergy;
+    // material textures (mtex null: none): texture objects, bindings per material, per-triangle uvs / tangents by
+    // mesh-local index from each mesh's first triangle
+    const cudaTextureObject_t* texObj; const cwp_material_textures* mtex; int nMtex; const float4* uvs; const float4* tans; const int* meshFirst;
     int* cnt;          // [0] next queue length, [1] shadow queue length
     int* slotCnt;      // kSlotCounters per slot
 };
@@ -136,6 +139,50 @@ __device__ __forceinline__ int warp_slot(int* counter, bool want) {
 __device__ __forceinline__ void add_rgb(float4* accum, int pix, float3 c) { atomicAdd(accum + pix, make_float4(c.x, c.y, c.z, 0.f)); }
 
 // shading of one closest hit or miss (render/wavefront.cu:223-356 restricted to the sun and a constant sky)
+// ---------------- material textures (render/wavefront.cu:198-204, 252-270) ----------------
+// (u, v) of a hit from the corner uvs: b1, b2 = barycentric weights of corners 1 and 2
+__device__ __forceinline__ float2 tri_uv(const float4* uvs, int64_t t, float b1, float b2) {
+    const float4 p = uvs[2 * t], q = uvs[2 * t + 1]; const float b0 = 1.f - b1 - b2;
+    return make_float2(p.x * b0 + p.z * b1 + q.x * b2, p.y * b0 + p.w * b1 + q.y * b2);
+}
+// images are stored top row first and uvs have v up
+__device__ __forceinline__ float4 tex_rgba(cudaTextureObject_t o, float2 uv) { return tex2D<float4>(o, uv.x, 1.f - uv.y); }
+__device__ __forceinline__ float tex_ch(float4 c, int ch) { return ch == 0 ? c.x : ch == 1 ? c.y : ch == 2 ? c.z : c.w; }
+__device__ __forceinline__ float3 xf_vec(const float* m, float3 v) {   // the linear part of 3x4 rows m
+    return f3(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z, m[8] * v.x + m[9] * v.y + m[10] * v.z);
+}
+
+// The material of a hit with its textures applied (glTF semantics: the images multiply the factors), and the shading
+// normal ns (in: the geometric normal ng0; out: perturbed by a normal image in the corner tangents' frame).
+__device__ __forceinline__ void apply_textures(const ShadeArgs& a, int mid, const cwp_instance& I, int tri, float hu, float hv, cwp_material& M, float3& ns) {
+    if (!a.mtex || mid >= a.nMtex) return;
+    const cwp_material_textures X = a.mtex[mid];
+    if (X.base_color < 0 && X.emission < 0 && X.normal < 0 && X.metallic < 0 && X.roughness < 0) return;
+    const int64_t t = (int64_t)__ldg(a.meshFirst + I.mesh) + __float_as_int(__ldg(a.tris + 3 * (size_t)tri).w);   // mesh-local triangle id
+    const float2 uv = tri_uv(a.uvs, t, hu, hv);
+    if (X.base_color >= 0) { const float4 c = tex_rgba(a.texObj[X.base_color], uv); M.base_color[0] *= c.x; M.base_color[1] *= c.y; M.base_color[2] *= c.z; }
+    if (X.emission >= 0) { const float4 c = tex_rgba(a.texObj[X.emission], uv); M.emission[0] *= c.x; M.emission[1] *= c.y; M.emission[2] *= c.z; }
+    if (X.metallic >= 0) M.metallic *= tex_ch(tex_rgba(a.texObj[X.metallic], uv), X.metallic_ch);
+    if (X.roughness >= 0) M.roughness *= tex_ch(tex_rgba(a.texObj[X.roughness], uv), X.roughness_ch);
+    if (X.normal >= 0 && a.tans) {   // tangent-space normal: n = T x + B y + N z, B = sign * (N x T)
+        const float w0 = 1.f - hu - hv;
+        const float4 t0 = a.tans[3 * t], t1 = a.tans[3 * t + 1], t2 = a.tans[3 * t + 2];
+        float3 tg = f3(t0.x, t0.y, t0.z) * w0 + f3(t1.x, t1.y, t1.z) * hu + f3(t2.x, t2.y, t2.z) * hv;
+        const float sg = ((t0.w * w0 + t1.w * hu + t2.w * hv) < 0.f ? -1.f : 1.f) * I.det_sign;
+        tg = xf_vec(I.fwd, tg);
+        tg = tg - ns * dot(ns, tg);
+        const float tl = length(tg);
+        if (tl > 0.f) {
+            tg = tg * (1.f / tl);
+            const float3 bt = cross(ns, tg) * sg;
+            const float4 c = tex_rgba(a.texObj[X.normal], uv);
+            const float3 nm = tg * ((2.f * c.x - 1.f) * X.normal_scale) + bt * ((2.f * c.y - 1.f) * X.normal_scale) + ns * (2.f * c.z - 1.f);
+            const float nl = length(nm);
+            if (nl > 0.f) ns = nm * (1.f / nl);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
     const int stride = gridDim.x * blockDim.x;
     for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < a.n; base += stride) {
@@ -170,7 +217,9 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                                      I.inv[2] * no.x + I.inv[6] * no.y + I.inv[10] * no.z);
                 const float3 ng0 = normalize(nw) * I.det_sign;
                 const int mid = min(max(__ldg(a.meshMat + I.mesh) + __float_as_int(e1.w), 0), a.nMats - 1);
-                const cwp_material M = a.mats[mid];
+                cwp_material M = a.mats[mid];
+                float3 nsw = ng0;   // shading normal before orientation
+                apply_textures(a, mid, I, tri, H.y, H.z, M, nsw);
                 const float3 p = f3(O.x, O.y, O.z) + d * H.x;
                 const float3 em = mat_v3(M.emission);
                 if (em.x > 0.f || em.y > 0.f || em.z > 0.f) add_rgb(S.accum, pix, T * em);   // no emitters are light-sampled
@@ -178,7 +227,7 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                 else {
                     const bool front = dot(ng0, d) < 0.f;
                     const float3 ng = front ? ng0 : -ng0;
-                    float3 ns = ng;
+                    float3 ns = front ? nsw : -nsw;
                     const float3 wo = -d;
                     if (dot(ns, wo) <= 1e-6f) ns = ng;
                     float3 tx, ty; frame_of(ns, tx, ty);
@@ -328,6 +377,9 @@ struct cwp_server {
     std::vector<int64_t> slotReq; std::vector<std::vector<cwp_instance>> slotInst; std::vector<int> admitted;   // slots admitted since the last TLAS update
     struct EnvMap { float4* tex = nullptr; float* marg = nullptr; float* cond = nullptr; int w = 0, h = 0; };
     std::vector<EnvMap> envs;   // environment maps the requests may name
+    // material textures: images (CUDA arrays + texture objects) and the device tables shading reads
+    std::vector<cudaArray_t> texArrays; std::vector<cudaTextureObject_t> texObjs;
+    cudaTextureObject_t* dTexObj = nullptr; cwp_material_textures* dMtex = nullptr; int nMtex = 0; float4* dUvs = nullptr; float4* dTans = nullptr;
     SlotParams* dSlots = nullptr; int* slotCnt = nullptr; std::vector<int> hSlotCnt;
     RayQueue q[2]{}; RayQueue qs{}; int* slotBins = nullptr; ShadowQueue sq{}; float4* hits = nullptr; int* hinst = nullptr; int* occ = nullptr; int* cnt = nullptr; int4* dChunks = nullptr;
     int* hcnt = nullptr;   // pinned: [0..1] counts, then slot counters
@@ -344,6 +396,40 @@ struct cwp_server {
     cwp_server_info info{};
 };
 
+// one CUDA array and texture object per image: bilinear filtering, wrap addressing, normalised coordinates, 8-bit
+// channels read as [0, 1] floats, colour images decoded from sRGB by the texture unit (render/wavefront.cu:535-546)
+static void free_textures(std::vector<cudaArray_t>& arrays, std::vector<cudaTextureObject_t>& objs) {
+    for (cudaTextureObject_t o : objs) cudaDestroyTextureObject(o);
+    for (cudaArray_t a : arrays) cudaFreeArray(a);
+    objs.clear(); arrays.clear();
+}
+static int make_textures(const cwp_texture* tex, int n, std::vector<cudaArray_t>& arrays, std::vector<cudaTextureObject_t>& objs) {
+    for (int i = 0; i < n; i++) {
+        const cwp_texture& T = tex[i];
+        CWPB_CHECK(T.rgba && T.w > 0 && T.h > 0 && T.w <= 32768 && T.h <= 32768 && (T.srgb == 0 || T.srgb == 1), CWP_ERR_INVALID,
+                   "texture %d: %dx%d, srgb %d", i, T.w, T.h, T.srgb);
+    }
+    for (int i = 0; i < n; i++) {
+        const cwp_texture& T = tex[i];
+        const cudaChannelFormatDesc cd = cudaCreateChannelDesc<uchar4>();
+        cudaArray_t arr = nullptr;
+        cudaError_t e = cudaMallocArray(&arr, &cd, T.w, T.h);
+        if (e == cudaSuccess) arrays.push_back(arr);
+        if (e == cudaSuccess) e = cudaMemcpy2DToArray(arr, 0, 0, T.rgba, (size_t)T.w * 4, (size_t)T.w * 4, T.h, cudaMemcpyHostToDevice);
+        cudaTextureObject_t o = 0;
+        if (e == cudaSuccess) {
+            cudaResourceDesc rd; memset(&rd, 0, sizeof rd); rd.resType = cudaResourceTypeArray; rd.res.array.array = arr;
+            cudaTextureDesc td; memset(&td, 0, sizeof td);
+            td.addressMode[0] = td.addressMode[1] = cudaAddressModeWrap; td.filterMode = cudaFilterModeLinear;
+            td.readMode = cudaReadModeNormalizedFloat; td.normalizedCoords = 1; td.sRGB = T.srgb;
+            e = cudaCreateTextureObject(&o, &rd, &td, nullptr);
+        }
+        if (e != cudaSuccess) { free_textures(arrays, objs); return set_error(e == cudaErrorMemoryAllocation ? CWP_ERR_NOMEM : CWP_ERR_CUDA, "texture %d: %s", i, cudaGetErrorString(e)); }
+        objs.push_back(o);
+    }
+    return CWP_OK;
+}
+
 static double now_ms(const cwp_server* s) { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s->t0).count(); }
 
 extern "C" double cwp_server_clock_ms(const cwp_server* s) { return s ? now_ms(s) : 0.0; }
@@ -356,6 +442,8 @@ extern "C" void cwp_server_destroy(cwp_server* s) {
     if (s->st) cudaStreamSynchronize(s->st);
     if (s->pool) cudaMemPoolDestroy(s->pool);
     for (auto& e : s->envs) { cudaFree(e.tex); cudaFree(e.marg); cudaFree(e.cond); }
+    free_textures(s->texArrays, s->texObjs);
+    cudaFree(s->dTexObj); cudaFree(s->dMtex); cudaFree(s->dUvs); cudaFree(s->dTans);
     for (void* p : s->allocs) cudaFree(p);
     if (s->hcnt) cudaFreeHost(s->hcnt);
     if (s->hSlots) cudaFreeHost(s->hSlots);
@@ -470,6 +558,65 @@ extern "C" int cwp_server_set_envmaps(cwp_server* s, const cwp_envmap* maps, int
     }
     for (auto& e : s->envs) { cudaFree(e.tex); cudaFree(e.marg); cudaFree(e.cond); }
     s->envs = built;
+    return CWP_OK;
+}
+
+extern "C" int cwp_server_set_textures(cwp_server* s, const cwp_texture* tex, int32_t nTex, const cwp_material_textures* mtex, int32_t nMtex,
+                                       const float* uvs, const float* tans) {
+    CWPB_CHECK(s && nTex >= 0 && nMtex >= 0 && (nTex == 0 || tex) && (nMtex == 0 || mtex), CWP_ERR_INVALID, "NULL argument");
+    CWPB_CHECK(s->reqs.empty(), CWP_ERR_STATE, "textures change only while no request is queued or running");
+    bool used = false;
+    for (int m = 0; m < nMtex; m++) {
+        const cwp_material_textures& X = mtex[m];
+        const int ids[5] = { X.base_color, X.emission, X.normal, X.metallic, X.roughness };
+        for (int id : ids) { CWPB_CHECK(id >= -1 && id < nTex, CWP_ERR_INVALID, "material %d: texture %d out of range (%d images)", m, id, nTex); used |= id >= 0; }
+        CWPB_CHECK(X.metallic_ch >= 0 && X.metallic_ch < 4 && X.roughness_ch >= 0 && X.roughness_ch < 4, CWP_ERR_INVALID, "material %d: channel out of range", m);
+        CWPB_CHECK(std::isfinite(X.normal_scale), CWP_ERR_INVALID, "material %d: normal scale is not finite", m);
+    }
+    CWPB_CHECK(!used || uvs, CWP_ERR_INVALID, "texture bindings without uvs");
+    CWPB_CUDA(cudaSetDevice(s->device));
+    std::vector<cudaArray_t> arrays; std::vector<cudaTextureObject_t> objs;
+    if (int rc = make_textures(tex, nTex, arrays, objs)) return rc;
+    const int64_t nt = batch_tri_count(s->batch);
+    cudaTextureObject_t* dObj = nullptr; cwp_material_textures* dM = nullptr; float4* dU = nullptr; float4* dT = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (nTex) { e = cudaMalloc(&dObj, nTex * sizeof(cudaTextureObject_t)); if (e == cudaSuccess) e = cudaMemcpy(dObj, objs.data(), nTex * sizeof(cudaTextureObject_t), cudaMemcpyHostToDevice); }
+    if (e == cudaSuccess && nMtex) { e = cudaMalloc(&dM, nMtex * sizeof(cwp_material_textures)); if (e == cudaSuccess) e = cudaMemcpy(dM, mtex, nMtex * sizeof(cwp_material_textures), cudaMemcpyHostToDevice); }
+    if (e == cudaSuccess && used) { e = cudaMalloc(&dU, (size_t)nt * 2 * sizeof(float4)); if (e == cudaSuccess) e = cudaMemcpy(dU, uvs, (size_t)nt * 2 * sizeof(float4), cudaMemcpyHostToDevice); }
+    if (e == cudaSuccess && used && tans) { e = cudaMalloc(&dT, (size_t)nt * 3 * sizeof(float4)); if (e == cudaSuccess) e = cudaMemcpy(dT, tans, (size_t)nt * 3 * sizeof(float4), cudaMemcpyHostToDevice); }
+    if (e != cudaSuccess) {
+        cudaFree(dObj); cudaFree(dM); cudaFree(dU); cudaFree(dT); free_textures(arrays, objs);
+        return set_error(e == cudaErrorMemoryAllocation ? CWP_ERR_NOMEM : CWP_ERR_CUDA, "textures: %s", cudaGetErrorString(e));
+    }
+    free_textures(s->texArrays, s->texObjs);
+    cudaFree(s->dTexObj); cudaFree(s->dMtex); cudaFree(s->dUvs); cudaFree(s->dTans);
+    s->texArrays = arrays; s->texObjs = objs; s->dTexObj = dObj; s->dMtex = dM; s->nMtex = used ? nMtex : 0; s->dUvs = dU; s->dTans = dT;
+    return CWP_OK;
+}
+
+__global__ void k_tex_sample(const cudaTextureObject_t* obj, const int* id, const float2* uv, float4* out, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = tex_rgba(obj[id[i]], uv[i]);
+}
+
+extern "C" int cwp_texture_sample_batch(const cwp_texture* tex, int32_t nTex, const int32_t* id, const float* uv, float* rgba, int64_t n) {
+    CWPB_CHECK(tex && nTex > 0 && id && uv && rgba && n >= 0, CWP_ERR_INVALID, "NULL argument");
+    for (int64_t i = 0; i < n; i++) CWPB_CHECK(id[i] >= 0 && id[i] < nTex, CWP_ERR_INVALID, "lookup %lld: texture %d out of range", (long long)i, id[i]);
+    if (n == 0) return CWP_OK;
+    std::vector<cudaArray_t> arrays; std::vector<cudaTextureObject_t> objs;
+    if (int rc = make_textures(tex, nTex, arrays, objs)) return rc;
+    cudaTextureObject_t* dObj = nullptr; int* dId = nullptr; float2* dUv = nullptr; float4* dOut = nullptr;
+    cudaError_t e = cudaMalloc(&dObj, nTex * sizeof(cudaTextureObject_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dId, n * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&dUv, n * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMalloc(&dOut, n * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMemcpy(dObj, objs.data(), nTex * sizeof(cudaTextureObject_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dId, id, n * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dUv, uv, n * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) { k_tex_sample<<<(unsigned)((n + 255) / 256), 256>>>(dObj, dId, dUv, dOut, n); e = cudaGetLastError(); }
+    if (e == cudaSuccess) e = cudaMemcpy(rgba, dOut, n * sizeof(float4), cudaMemcpyDeviceToHost);
+    cudaFree(dObj); cudaFree(dId); cudaFree(dUv); cudaFree(dOut); free_textures(arrays, objs);
+    if (e != cudaSuccess) return set_error(CWP_ERR_CUDA, "texture lookups: %s", cudaGetErrorString(e));
     return CWP_OK;
 }
 
@@ -613,6 +760,7 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         ShadeArgs a{};
         a.n = (int)n; a.in = in; a.out = out; a.sq = s->sq; a.hits = s->hits; a.hinst = s->hinst; a.inst = batch_instances(s->batch); a.tris = batch_tris(s->batch);
         a.mats = s->mats; a.nMats = s->nMats; a.meshMat = s->meshMat; a.slots = s->dSlots; a.gdEnergy = s->O.gd_energy; a.cnt = s->cnt; a.slotCnt = s->slotCnt;
+        a.texObj = s->dTexObj; a.mtex = s->nMtex ? s->dMtex : nullptr; a.nMtex = s->nMtex; a.uvs = s->dUvs; a.tans = s->dTans; a.meshFirst = batch_mesh_first(s->batch);
         const unsigned g = (unsigned)std::min<int64_t>((n + 127) / 128, 148 * 16);
         k_serve_shade<<<g, 128, 0, s->st>>>(a);
         CWPB_CUDA(cudaGetLastError());

@@ -28,7 +28,7 @@ SEED = 1000
 EPS_SCALE = 1e-4
 
 __all__ = ["SCENES", "scene", "frame_params", "scene_extent", "camera_rays", "incoherent_rays", "reference_inputs",
-           "batch_scenes", "batch_rays", "serving_scenes", "serving_requests", "RESOLUTIONS", "SPPS", "HFOV", "SEED", "SUN_TO", "SUN_E", "SUN_ANGLE_RAD", "SKY", "ALBEDO"]
+           "batch_scenes", "batch_rays", "serving_scenes", "serving_requests", "planar_uvs", "texture_images", "RESOLUTIONS", "SPPS", "HFOV", "SEED", "SUN_TO", "SUN_E", "SUN_ANGLE_RAD", "SKY", "ALBEDO"]
 
 
 def scene(name_or_boxes, variant=8, bins=32, leaf=4, collapse=0, threads=0, spatial=0.0):
@@ -247,3 +247,45 @@ def serving_requests(n, rate, scene_boxes, seed=11, resolutions=None, spps=None,
         out.append((t, make_request(sc, cam, int(spps[int(rng.integers(len(spps)))]), frame=int(rng.integers(frames)), max_depth=max_depth,
                                     seed=int(rng.integers(1 << 30)), eps=1e-4 * ext)))
     return out
+
+
+def planar_uvs(meshes, scale=0.35):
+    """Texture coordinates and tangents for box-field meshes: each triangle projected along its normal's dominant axis
+    (u, v from the other two axes, scaled), the tangent along the u axis with the handedness that makes
+    sign * (n x t) the v axis. Returns (uvs float32 [n, 8], tans float32 [n, 12]) over all meshes in mesh order."""
+    uvs, tans = [], []
+    for m in meshes:
+        v, f = (m.arrays() if hasattr(m, "arrays") else m)[:2]
+        p = v[f].astype(np.float64)
+        n = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+        a = np.argmax(np.abs(n), axis=1); b = (a + 1) % 3; c = (a + 2) % 3
+        idx = np.arange(len(f))
+        uv = np.stack([p[idx[:, None], np.arange(3)[None, :], b[:, None]], p[idx[:, None], np.arange(3)[None, :], c[:, None]]], -1) * scale
+        u = np.zeros((len(f), 8), np.float32)
+        u[:, 0:2], u[:, 2:4], u[:, 4:6] = uv[:, 0], uv[:, 1], uv[:, 2]
+        t = np.zeros((len(f), 3)); t[idx, b] = 1.0
+        e_c = np.zeros((len(f), 3)); e_c[idx, c] = 1.0
+        sg = np.where(np.einsum("ij,ij->i", np.cross(n, t), e_c) < 0, -1.0, 1.0)
+        tg = np.zeros((len(f), 12), np.float32)
+        for k in range(3):
+            tg[:, 4 * k:4 * k + 3] = t; tg[:, 4 * k + 3] = sg
+        uvs.append(u); tans.append(tg)
+    return np.concatenate(uvs), np.concatenate(tans)
+
+
+def texture_images(seed=1):
+    """Procedural images: an sRGB colour checker (48x32), a linear roughness (G) / metalness (B) map (20x20), a
+    tangent-space bump normal map (32x32), an sRGB emission spot map (16x16). List of (rgba uint8, srgb)."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:32, 0:48]
+    chk = ((yy // 4 + xx // 6) % 2).astype(np.float64)
+    col = np.stack([40 + 180 * chk, 200 - 120 * chk, 90 + 60 * rng.random((32, 48)), np.full((32, 48), 255)], -1)
+    rm = np.stack([np.zeros((20, 20)), 40 + 200 * rng.random((20, 20)), 255.0 * (rng.random((20, 20)) < 0.3), np.full((20, 20), 255)], -1)
+    y2, x2 = np.mgrid[0:32, 0:32] / 32.0
+    nx, ny = 0.5 * np.sin(2 * np.pi * 3 * x2), 0.5 * np.cos(2 * np.pi * 2 * y2); nz = np.sqrt(np.maximum(0.0, 1 - nx ** 2 - ny ** 2))
+    nrm = np.stack([(nx + 1) * 127.5, (ny + 1) * 127.5, (nz + 1) * 127.5, np.full((32, 32), 255)], -1)
+    y3, x3 = np.mgrid[0:16, 0:16]
+    em = np.where(((y3 - 8) ** 2 + (x3 - 8) ** 2) < 12, 255, 0)
+    emi = np.stack([em, em * 0.8, em * 0.5, np.full((16, 16), 255)], -1)
+    return [(np.clip(col, 0, 255).astype(np.uint8), True), (np.clip(rm, 0, 255).astype(np.uint8), False),
+            (np.clip(nrm, 0, 255).astype(np.uint8), False), (np.clip(emi, 0, 255).astype(np.uint8), True)]

@@ -376,6 +376,25 @@ int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* id);
  * (app/scene_setup.cpp:252) for the serving form. */
 typedef struct cwp_envmap { const float* rgb; int32_t w, h; float strength; int32_t pad; } cwp_envmap;
 int cwp_server_set_envmaps(cwp_server* s, const cwp_envmap* maps, int32_t n);
+/* Material textures (glTF metallic-roughness; scene/texture.h:10-24): images are 8-bit RGBA, top row first, looked up
+ * at (u, 1 - v) with bilinear filtering and wrap addressing, colour images (srgb = 1) decoded from sRGB. Material m's
+ * factors are multiplied by its bound images: base colour and emission by rgb, metallic and roughness by one channel;
+ * a normal image perturbs the shading normal in the tangent frame. mtex has n_mtex entries (material index, as in the
+ * server's table; materials beyond n_mtex are untextured). uvs: 2 float4 per triangle of every batch mesh in mesh
+ * order, by mesh-local triangle index ((u0, v0, u1, v1), (u2, v2, -, -)); tans: 3 float4 per triangle (corner tangent
+ * xyz, handedness sign w) or NULL (normal images then ignored). Replaces the texture set-up of the full integrator
+ * (render/wavefront.cu:535-547, packAttributes in app/scene_setup.cpp:255). Only while no request is queued or running. */
+typedef struct cwp_texture { const uint8_t* rgba; int32_t w, h; int32_t srgb, pad; } cwp_texture;
+typedef struct cwp_material_textures {
+    int32_t base_color, emission, normal, metallic, roughness;   /* texture ids or -1 */
+    int32_t metallic_ch, roughness_ch;                          /* channel of the metallic / roughness image (glTF: 2, 1) */
+    float normal_scale;
+} cwp_material_textures;
+int cwp_server_set_textures(cwp_server* s, const cwp_texture* tex, int32_t n_tex, const cwp_material_textures* mtex, int32_t n_mtex,
+                            const float* uvs, const float* tans);
+/* Texture lookups on the device, for tests of the filtering: n (texture, u, v) -> rgba, with the images of tex bound as
+ * cwp_server_set_textures binds them. */
+int cwp_texture_sample_batch(const cwp_texture* tex, int32_t n_tex, const int32_t* id, const float* uv, float* rgba, int64_t n);
 /* One step: admission, new camera paths, one bounce of every admitted request (closest hit + shading, sun shadow rays),
  * completion. *n_active / *n_pending: admitted / waiting requests after the step. Synchronous. */
 int cwp_server_step(cwp_server* s, int32_t* n_active, int32_t* n_pending);

@@ -1140,6 +1140,33 @@ static float o_env_pdf_texel(const OEnv* E, int x, int y, float v) {
     const float st = sinf(v * 3.14159265f);
     return st > 0.f ? puv / (2.f * 3.14159265f * 3.14159265f * st) : 0.f;
 }
+/* Material textures (render/wavefront.cu:198-204, 252-270; scene/texture.h). A lookup restates the texture unit's
+ * documented linear filtering of 8-bit RGBA images with normalised coordinates and wrap addressing: coordinate
+ * frac(u) * w - 0.5, the four texels around it weighted by the fractional parts kept to 8 bits, channels read as
+ * value / 255 and, for colour images, decoded from sRGB before the weighting. Images top row first, looked up at
+ * (u, 1 - v). OTex and OMTex have the layouts of cwp_texture and cwp_material_textures. */
+typedef struct { const unsigned char* rgba; int w, h, srgb, pad; } OTex;
+typedef struct { int base_color, emission, normal, metallic, roughness, metallic_ch, roughness_ch; float normal_scale; } OMTex;
+static float o_srgb(float c) { return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f); }
+static void o_tex(const OTex* T, float u, float v, float out[4]) {
+    const float x = (u - floorf(u)) * T->w - 0.5f, y = (v - floorf(v)) * T->h - 0.5f;
+    const float fx = floorf(x), fy = floorf(y);
+    const float a = rintf((x - fx) * 256.f) / 256.f, b = rintf((y - fy) * 256.f) / 256.f;
+    const int i0 = (int)fx, j0 = (int)fy;
+    for (int c = 0; c < 4; c++) out[c] = 0.f;
+    for (int k = 0; k < 4; k++) {
+        int i = i0 + (k & 1), j = j0 + (k >> 1);
+        i %= T->w; if (i < 0) i += T->w; j %= T->h; if (j < 0) j += T->h;
+        const float wgt = ((k & 1) ? a : 1.f - a) * ((k >> 1) ? b : 1.f - b);
+        const unsigned char* p = T->rgba + 4 * ((size_t)j * T->w + i);
+        for (int c = 0; c < 4; c++) { float x8 = p[c] / 255.f; if (T->srgb && c < 3) x8 = o_srgb(x8); out[c] += wgt * x8; }
+    }
+}
+void orc_texture_sample(const void* tex, const int* id, const float* uv, float* rgba, long n) {
+    const OTex* T = (const OTex*)tex;
+    for (long i = 0; i < n; i++) o_tex(&T[id[i]], uv[2 * i], 1.f - uv[2 * i + 1], rgba + 4 * i);
+}
+
 static int o_cdf_find(const float* cdf, int n, float u) { int lo = 0, hi = n; while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (cdf[mid] <= u) lo = mid; else hi = mid; } return lo; }
 static float o_mis(float a, float b) { const float a2 = a * a; return a2 / (a2 + b * b); }
 static int o_tile_pixel(int j, int w, int h) {
@@ -1149,7 +1176,9 @@ static int o_tile_pixel(int j, int w, int h) {
 }
 long orc_render_request(const void* reqp, int width, int tlas_width, const float* blas, const float* tris, const float* tlas, int root, const float* inst,
                         const float* mats, int n_mats, const int* mesh_mat, int gd, long j0, long j1, float* accum, long long* counts,
-                        const float* env_tex, const float* env_marg, const float* env_cond, int env_w, int env_h) {
+                        const float* env_tex, const float* env_marg, const float* env_cond, int env_w, int env_h,
+                        const void* tex, const void* mtex, int n_mtex, const float* uvs, const float* tans, const int* mesh_first) {
+    const OTex* TX = (const OTex*)tex; const OMTex* MX = (const OMTex*)mtex;
     const OReq* R = (const OReq*)reqp; const OCam* C = &R->cam;
     const int N = C->w * C->h; long bad = 0;
     const OEnv E = { env_tex, env_marg, env_cond, env_w, env_h, R->env_rot_deg * 3.14159265f / 180.f };
@@ -1185,13 +1214,42 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
             int imesh; memcpy(&imesh, &I[25], 4);
             const V3 ng0 = muls(normz(nw), I[26]);
             int mid = mesh_mat[imesh] + fi(TR[3 * tri + 1].w); mid = mid < 0 ? 0 : mid >= n_mats ? n_mats - 1 : mid;
-            const OMat* M = (const OMat*)(mats + 16 * (size_t)mid);
+            OMat Mc = *(const OMat*)(mats + 16 * (size_t)mid); const OMat* M = &Mc;
+            V3 nsw = ng0;
+            if (MX && mid < n_mtex && (MX[mid].base_color >= 0 || MX[mid].emission >= 0 || MX[mid].normal >= 0 || MX[mid].metallic >= 0 || MX[mid].roughness >= 0)) {
+                const OMTex X = MX[mid];
+                const long ti = (long)mesh_first[imesh] + fi(TR[3 * tri].w);
+                const float* q = uvs + 8 * (size_t)ti; const float b0 = 1.f - u - v;
+                const float tu = q[0] * b0 + q[2] * u + q[4] * v, tv = q[1] * b0 + q[3] * u + q[5] * v;
+                float c[4];
+                if (X.base_color >= 0) { o_tex(&TX[X.base_color], tu, 1.f - tv, c); Mc.base[0] *= c[0]; Mc.base[1] *= c[1]; Mc.base[2] *= c[2]; }
+                if (X.emission >= 0) { o_tex(&TX[X.emission], tu, 1.f - tv, c); Mc.emission[0] *= c[0]; Mc.emission[1] *= c[1]; Mc.emission[2] *= c[2]; }
+                if (X.metallic >= 0) { o_tex(&TX[X.metallic], tu, 1.f - tv, c); Mc.metallic *= c[X.metallic_ch]; }
+                if (X.roughness >= 0) { o_tex(&TX[X.roughness], tu, 1.f - tv, c); Mc.roughness *= c[X.roughness_ch]; }
+                if (X.normal >= 0 && tans) {   /* tangent-space normal: n = T x + B y + N z, B = sign (N x T) */
+                    const float* t0 = tans + 12 * (size_t)ti; const float w0 = 1.f - u - v;
+                    V3 tg = v3(t0[0] * w0 + t0[4] * u + t0[8] * v, t0[1] * w0 + t0[5] * u + t0[9] * v, t0[2] * w0 + t0[6] * u + t0[10] * v);
+                    const float sg = ((t0[3] * w0 + t0[7] * u + t0[11] * v) < 0.f ? -1.f : 1.f) * I[26];
+                    const float* F = I + 12;
+                    tg = v3(F[0] * tg.x + F[1] * tg.y + F[2] * tg.z, F[4] * tg.x + F[5] * tg.y + F[6] * tg.z, F[8] * tg.x + F[9] * tg.y + F[10] * tg.z);
+                    tg = sub(tg, muls(nsw, dot3(nsw, tg)));
+                    const float tl = sqrtf(dot3(tg, tg));
+                    if (tl > 0.f) {
+                        tg = muls(tg, 1.f / tl);
+                        const V3 bt = muls(cross3(nsw, tg), sg);
+                        o_tex(&TX[X.normal], tu, 1.f - tv, c);
+                        const V3 nm = add(add(muls(tg, (2.f * c[0] - 1.f) * X.normal_scale), muls(bt, (2.f * c[1] - 1.f) * X.normal_scale)), muls(nsw, 2.f * c[2] - 1.f));
+                        const float nl = sqrtf(dot3(nm, nm));
+                        if (nl > 0.f) nsw = muls(nm, 1.f / nl);
+                    }
+                }
+            }
             const V3 p = add(o, muls(d, t));
             if (M->emission[0] > 0.f || M->emission[1] > 0.f || M->emission[2] > 0.f) { A[0] += T.x * M->emission[0]; A[1] += T.y * M->emission[1]; A[2] += T.z * M->emission[2]; }
             if (depth > R->max_depth) break;
             const int front = dot3(ng0, d) < 0.f;
             const V3 ng = front ? ng0 : neg(ng0);
-            V3 ns = ng; const V3 wo = neg(d);
+            V3 ns = front ? nsw : neg(nsw); const V3 wo = neg(d);
             if (dot3(ns, wo) <= 1e-6f) ns = ng;
             V3 tx, ty; onb(ns, &tx, &ty);
             const V3 woL = v3(dot3(wo, tx), dot3(wo, ty), dot3(wo, ns));

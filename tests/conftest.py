@@ -59,7 +59,9 @@ def _load_oracle():
     L.orc_render_stats.argtypes = [C.c_int, C.c_void_p]
     L.orc_render_request.restype = C.c_long
     L.orc_render_request.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
-                                     + [C.c_void_p] * 3 + [C.c_int, C.c_int])
+                                     + [C.c_void_p] * 3 + [C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3)
+    L.orc_texture_sample.restype = None
+    L.orc_texture_sample.argtypes = [C.c_void_p] * 4 + [C.c_long]
     L.orc_envmap_build.restype = None
     L.orc_envmap_build.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_half_round.restype = C.c_double
@@ -155,9 +157,17 @@ class Oracle:
         self.L.orc_envmap_build(rgb.ctypes.data, w, h, strength, tex.ctypes.data, marg.ctypes.data, cond.ctypes.data)
         return tex, marg, cond
 
-    def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None, tlas_width=2, env=None):
+    def texture_sample(self, tex, ids, uv):
+        """lookups (texture id, (u, v)) -> rgba [n, 4] with the oracle's restatement of the texture unit; tex: a
+        cwp_texture array"""
+        ids = np.ascontiguousarray(ids, np.int32); uv = np.ascontiguousarray(uv, np.float32); out = np.zeros((len(ids), 4), np.float32)
+        self.L.orc_texture_sample(C.addressof(tex), ids.ctypes.data, uv.ctypes.data, out.ctypes.data, len(ids))
+        return out
+
+    def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None, tlas_width=2, env=None, textures=None):
         """A serving request on the host: (accum [w h, 4], counts [2]). env: (texels, marg, cond) of the request's
-        environment map when Request.env >= 0, else None."""
+        environment map when Request.env >= 0, else None. textures: (cwp_texture array, cwp_material_textures array,
+        uvs, tans or None, mesh_first) as given to the server, else None."""
         n = req.cam.w * req.cam.h * req.spp
         j0, j1 = (0, n) if paths is None else paths
         acc = np.zeros((req.cam.w * req.cam.h, 4), np.float32); cnt = np.zeros(2, np.int64)
@@ -166,7 +176,10 @@ class Oracle:
         bad = self.L.orc_render_request(C.addressof(req), width, tlas_width, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, int(root), ins.ctypes.data,
                                         ms.ctypes.data, len(ms), mm.ctypes.data, gd, j0, j1, acc.ctypes.data, cnt.ctypes.data,
                                         *((env[0].ctypes.data, env[1].ctypes.data, env[2].ctypes.data, env[0].shape[1], env[0].shape[0]) if env is not None
-                                          else (None, None, None, 0, 0)))
+                                          else (None, None, None, 0, 0)),
+                                        *((C.addressof(textures[0]), C.addressof(textures[1]), len(textures[1]), textures[2].ctypes.data,
+                                           textures[3].ctypes.data if textures[3] is not None else None, textures[4].ctypes.data) if textures is not None
+                                          else (None, None, 0, None, None, None)))
         assert bad == 0
         return acc, cnt
 

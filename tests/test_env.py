@@ -67,3 +67,27 @@ def test_bad_files_and_arguments(cwp, g, tmp_path):
     assert L.cwp_hdr_load(str(other).encode(), C.byref(w), C.byref(h), None) == cwp.ERR_IO
     with pytest.raises(cwp.CwpError):
         cwp.envmap_build(np.zeros((2, 2, 3), np.float32), -1.0)
+
+
+def test_oracle_texture_filtering(cwp, oracle):
+    """The oracle's texture lookup: a texel centre returns the texel (linear images exactly, sRGB decoded); halfway
+    between two texels, their mean; coordinates wrap"""
+    img = np.zeros((4, 6, 4), np.uint8)
+    img[..., 0] = np.arange(6)[None, :] * 40; img[..., 1] = np.arange(4)[:, None] * 60; img[..., 2] = 200; img[..., 3] = 255
+    tex, keep = cwp.textures_array([(img, False), (img, True)])
+    # centre of texel (x=2, y=1) at (u, v) with v up: u = 2.5/6, 1 - v = 1.5/4
+    uv = np.array([[2.5 / 6, 1 - 1.5 / 4], [3.0 / 6, 1 - 1.5 / 4], [2.5 / 6 + 1, 1 - 1.5 / 4 - 2]], np.float32)
+    lin = oracle.texture_sample(tex, [0, 0, 0], uv)
+    assert np.allclose(lin[0], img[1, 2] / 255.0, atol=1e-7)
+    assert np.allclose(lin[1], (img[1, 2] / 255.0 + img[1, 3] / 255.0) / 2, atol=1e-6)
+    assert np.allclose(lin[2], lin[0], atol=1e-7)                           # wrapped
+    srgb = oracle.texture_sample(tex, [1], uv[:1])[0]
+    c = img[1, 2, :3] / 255.0
+    assert np.allclose(srgb[:3], np.where(c <= 0.04045, c / 12.92, ((c + 0.055) / 1.055) ** 2.4), atol=1e-6) and abs(srgb[3] - 1.0) < 1e-7
+
+
+def test_planar_uvs(cwp):
+    m = cwp.Mesh.box_field(3, 2)
+    uvs, tans = cwp.planar_uvs([m])
+    assert uvs.shape == (m.n_tris, 8) and tans.shape == (m.n_tris, 12)
+    assert np.all(np.isfinite(uvs)) and np.allclose(np.linalg.norm(tans[:, :3], axis=1), 1.0) and set(np.unique(tans[:, 3])) <= {-1.0, 1.0}
