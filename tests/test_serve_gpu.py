@@ -148,8 +148,10 @@ def test_environment_request_matches_oracle(gpu, cwp, oracle, serving):
 
 def test_texture_lookups_match_oracle(gpu, cwp, oracle):
     """Hardware bilinear lookups (wrap, normalised coordinates, sRGB decode for colour images) against the oracle's
-    restatement of the documented filtering rule: within 1/255 per channel, odd image sizes, coordinates wrapping
-    over several periods."""
+    restatement of the documented filtering rule, over odd image sizes and coordinates wrapping over several periods.
+    The filter weights are kept to 8 fractional bits, and the hardware's rounding of them (and of its sRGB decode) is
+    not documented, so a lookup may differ by one weight step per axis times the texel difference (at most about
+    2/255); the mean difference stays far below that."""
     rng = np.random.default_rng(2)
     imgs = [(rng.integers(0, 256, (7, 13, 4)).astype(np.uint8), False), (rng.integers(0, 256, (5, 9, 4)).astype(np.uint8), True)]
     imgs += cwp.texture_images()
@@ -160,7 +162,7 @@ def test_texture_lookups_match_oracle(gpu, cwp, oracle):
     tex, keep = cwp.textures_array(imgs)
     ref = oracle.texture_sample(tex, ids, uv)
     err = np.abs(got - ref)
-    assert err.max() <= 1.0 / 255.0 and err.mean() < 2e-3
+    assert err.max() <= 2.5 / 255.0 and err.mean() < 1e-3
 
 
 def test_textured_request_matches_oracle(gpu, cwp, oracle, serving):
