@@ -181,8 +181,8 @@ def cpu_frame_sample(cwp, wl, mesh, bvh, variant, seconds=12.0):
 # DRAM bytes per launch of the frame kernels from one full-size ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum, one pass, every launch of one frame; summary and command in profiles/frame512_dram_traffic.txt).
 # Valid only for the configuration it was captured on.
-FRAME512_TRAFFIC = {"k_trace_shade": 2599.4e6, "k_shadow": 530.8e6}
-FRAME512_TRAFFIC_BINS = 32   # the build the capture ran on
+FRAME512_TRAFFIC = {"k_trace_shade": 2583.8e6, "k_shadow": 531.0e6}
+FRAME512_TRAFFIC_BINS = 128   # the build the capture ran on
 
 
 def frame_traffic(args, wl, variant, kernel):
