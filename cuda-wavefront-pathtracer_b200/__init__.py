@@ -114,7 +114,11 @@ class ServerOptions(C.Structure):
 class Request(C.Structure):
     _fields_ = [("scene", C.c_int32), ("frame", C.c_int32), ("cam", Camera), ("spp", C.c_int32), ("max_depth", C.c_int32), ("seed", C.c_uint32),
                 ("sun_to", C.c_float * 3), ("sun_e", C.c_float * 3), ("sky", C.c_float * 3), ("sun_cos", C.c_float), ("eps", C.c_float),
-                ("env", C.c_int32), ("env_rot_deg", C.c_float)]
+                ("env", C.c_int32), ("env_rot_deg", C.c_float),
+                ("light_mode", C.c_int32), ("rr", C.c_int32), ("rr_depth", C.c_int32), ("env_uniform", C.c_int32)]
+
+
+LIGHT_MIS, LIGHT_NEE, LIGHT_BSDF = 0, 1, 2
 
 
 class Texture(C.Structure):
@@ -216,6 +220,8 @@ SIGNATURES = {
     "cwp_texture_sample_batch": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_void_p, C.c_void_p, C.c_int64]),
     "cwp_hdr_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
     "cwp_envmap_build": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cwp_emissive_tables": (C.c_int, [C.POINTER(MeshView), C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]),
     "cwp_batch_reserve_scenes": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "cwp_batch_update_scenes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "cwp_batch_set_scenes": (C.c_int, [C.c_void_p, C.POINTER(Instance), C.c_int64, C.POINTER(C.c_int32), C.c_int32]),
@@ -517,6 +523,16 @@ def xform_animate(mesh, frame=0, translate=(0, 0, 0), axis=(0, 0, 1), angle_deg=
     return m
 
 
+def scene_xforms(descs, scene_first, scene, frame):
+    """3x4 maps and meshes of one scene's instances at a frame, as the server animates them: (xforms [n, 12], mesh [n])"""
+    i0, i1 = int(scene_first[scene]), int(scene_first[scene + 1])
+    xf = np.zeros((i1 - i0, 12), np.float32); im = np.zeros(i1 - i0, np.int32)
+    for k in range(i0, i1):
+        _check(lib().cwp_xform_animate(C.byref(descs[k]), frame, _fptr(xf[k - i0])))
+        im[k - i0] = descs[k].mesh
+    return xf, im
+
+
 def instances(xforms, meshes):
     """Array of cwp_instance records (numpy structured bytes, 112 B each) from 3x4 maps and mesh indices."""
     xforms = np.ascontiguousarray(xforms, np.float32).reshape(-1, 12)
@@ -658,9 +674,11 @@ def envmap_build(rgb, strength=1.0):
     return tex, marg, cond
 
 
-def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun_e=None, sky=None, sun_angle_rad=None, eps=1e-3, env=-1, env_rot_deg=0.0):
+def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun_e=None, sky=None, sun_angle_rad=None, eps=1e-3, env=-1, env_rot_deg=0.0,
+                 light_mode=LIGHT_MIS, rr=0, rr_depth=3, env_uniform=0):
     """A serving request; lighting defaults to the benchmark's sun and sky (env = -1) or names one of the server's
-    environment maps."""
+    environment maps; emissive materials of the scene are light-sampled too (light_mode, as the reference's
+    --light_sampling mis / nee / bsdf); rr / rr_depth: Russian roulette (--rr, --rr_depth)."""
     from . import workloads as W
     sun_to = W.SUN_TO if sun_to is None else sun_to; sun_e = (W.SUN_E,) * 3 if sun_e is None else sun_e
     sky = W.SKY if sky is None else sky; sun_angle_rad = W.SUN_ANGLE_RAD if sun_angle_rad is None else sun_angle_rad
@@ -670,7 +688,29 @@ def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun
     r.sun_to[:] = tuple(float(x) for x in s); r.sun_e[:] = tuple(sun_e); r.sky[:] = tuple(sky)
     r.sun_cos = float(np.float32(math.cos(sun_angle_rad / 2.0))); r.eps = eps
     r.env, r.env_rot_deg = env, env_rot_deg
+    r.light_mode, r.rr, r.rr_depth, r.env_uniform = light_mode, rr, rr_depth, env_uniform
     return r
+
+
+def emissive_tables(meshes, mesh_mat_base, materials, xforms, inst_mesh):
+    """Light tables of the emissive triangles of an instanced scene at one frame (what the server builds at admission):
+    (em_tris [n, 12] float32 = world (w0, global id bits), (w1 - w0, material bits), (w2 - w0, 0); em_cdf [n + 1];
+    mat_pdf [n_mats]). meshes: (verts, faces, face_mat, _) tuples or Mesh; xforms: [n_inst, 12] 3x4 rows."""
+    arrs, views = [], (MeshView * len(meshes))()
+    for i, m in enumerate(meshes):
+        v, f, fm, _ = m.arrays() if isinstance(m, Mesh) else m
+        v = np.ascontiguousarray(v, np.float32); f = np.ascontiguousarray(f, np.int32)
+        fm = np.ascontiguousarray(fm if fm is not None else np.zeros(len(f)), np.int32)
+        arrs += [v, f, fm]
+        views[i].verts, views[i].n_verts, views[i].faces, views[i].n_tris, views[i].face_mat = _fptr(v), len(v), _iptr(f), len(f), _iptr(fm)
+    M = materials_array(materials); base = np.ascontiguousarray(mesh_mat_base, np.int32)
+    xf = np.ascontiguousarray(xforms, np.float32).reshape(-1, 12); im = np.ascontiguousarray(inst_mesh, np.int32)
+    n = C.c_int64()
+    args = (views, len(meshes), base.ctypes.data, C.cast(M, C.c_void_p), len(M), xf.ctypes.data, im.ctypes.data, len(im))
+    _check(lib().cwp_emissive_tables(*args, None, None, None, C.byref(n)))
+    t = np.zeros((n.value, 12), np.float32); c = np.zeros(n.value + 1, np.float32); p = np.zeros(len(M), np.float32)
+    _check(lib().cwp_emissive_tables(*args, t.ctypes.data, c.ctypes.data, p.ctypes.data, C.byref(n)))
+    return t, (c if n.value else np.zeros(0, np.float32)), p
 
 
 class Server:

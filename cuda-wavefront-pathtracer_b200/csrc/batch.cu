@@ -751,5 +751,7 @@ const cwp_instance* batch_instances(const cwp_batch* b) { return b->inst; }
 int batch_mesh_count(const cwp_batch* b) { return b->nMesh; }
 const int* batch_mesh_first(const cwp_batch* b) { return b->meshFirstDev; }
 int64_t batch_tri_count(const cwp_batch* b) { return b->nTris; }
+const float4* batch_tri_soup(const cwp_batch* b) { return b->triV; }
+const int* batch_mesh_first_host(const cwp_batch* b) { return b->meshFirst.data(); }
 int batch_device(const cwp_batch* b) { return b->device; }
 }  // namespace cwpb

@@ -15,4 +15,6 @@ int batch_mesh_count(const cwp_batch* b);
 int batch_device(const cwp_batch* b);
 const int* batch_mesh_first(const cwp_batch* b);       // device: nMesh + 1 offsets of each mesh's triangles in mesh order
 int64_t batch_tri_count(const cwp_batch* b);            // triangles of all meshes
+const float4* batch_tri_soup(const cwp_batch* b);     // device: the input triangles, (v0, face id), (v1, face material), (v2, 0) in mesh order
+const int* batch_mesh_first_host(const cwp_batch* b);  // host: nMesh + 1 offsets
 }  // namespace cwpb

@@ -7,8 +7,9 @@
 //   2. new camera paths for the admitted requests, up to the path capacity, shared evenly between the requests that
 //      still have samples to issue (so small requests are not stuck behind large ones);
 //   3. one scene-tagged closest-hit launch over every queued ray, whatever request it belongs to;
-//   4. shading (OpenPBR-subset BSDFs, sun next-event estimation, constant sky): continuations into the next queue,
-//      sun shadow rays into the shadow queue, per-slot counts of traced, shadow and finished paths;
+//   4. shading (OpenPBR-subset BSDFs, one light sample per vertex over the sun, the emissive triangles and an
+//      environment map, MIS with BSDF sampling, Russian roulette): continuations into the next queue, shadow rays into
+//      the shadow queue, per-slot counts of traced, shadow and finished paths;
 //   5. one any-hit launch over the shadow queue and the accumulation of the unoccluded contributions;
 //   6. completion: a request whose paths were all issued and have all finished is done.
 // A request's image depends only on its own inputs: every random number is keyed by (pixel, sample, depth, dimension,
@@ -17,6 +18,7 @@
 #include "batch_internal.h"
 #include "bsdf.cuh"
 #include "cwp_b200.h"
+#include "lights.h"
 #include "runtime.h"
 #include "trav.cuh"
 #include <algorithm>
@@ -35,6 +37,10 @@ struct SlotParams {
     unsigned seed; int maxDepth, N; float4* accum;
     // the request's environment map (envTex null: the constant sky): texels, CDF over rows, CDF within each row
     const float4* envTex; const float* envMarg; const float* envCond; int envW, envH; float envRot;
+    // light sampling: light-type probabilities, mode (CWP_LIGHT_*), Russian roulette, uniform environment samples; the
+    // scene's emissive triangles at the request's frame (nEm = 0: none): 3 float4 each, power CDF, area density by material
+    float pSun, pTri, pEnv; int lightMode, rr, rrDepth, envUniform, nEm;
+    const float4* emTris; const float* emCdf; const float* matPdf;
 };
 
 // ---------------- environment map (scene/environment.h orientation; render/wavefront.cu:177-197, 319-331) ----------
@@ -57,6 +63,15 @@ __device__ __forceinline__ float env_pdf_texel(const SlotParams& S, int x, int y
     const float puv = (S.envMarg[y + 1] - S.envMarg[y]) * (cr[x + 1] - cr[x]) * S.envW * S.envH;
     const float st = sinf(v * CWPB_PI);
     return st > 0.f ? puv / (2.f * CWPB_PI * CWPB_PI * st) : 0.f;
+}
+__device__ __forceinline__ float3 env_radiance(const SlotParams& S, float3 d) {
+    int x, y; float v; env_texel(S, d, x, y, v);
+    const float4 t = S.envTex[(size_t)y * S.envW + x];
+    return f3(t.x, t.y, t.z);
+}
+__device__ __forceinline__ float3 uniform_sphere(float u0, float u1) {   // core/sampling.h:55-58
+    const float z = 1.f - 2.f * u0, r = sqrtf(fmaxf(0.f, 1.f - z * z)), ph = CWPB_TWO_PI * u1;
+    return f3(r * cosf(ph), r * sinf(ph), z);
 }
 // largest i in [0, n) with cdf[i] <= u (cdf: n + 1 entries from 0 to 1)
 __device__ __forceinline__ int cdf_find(const float* cdf, int n, float u) {
@@ -138,7 +153,6 @@ __device__ __forceinline__ int warp_slot(int* counter, bool want) {
 
 __device__ __forceinline__ void add_rgb(float4* accum, int pix, float3 c) { atomicAdd(accum + pix, make_float4(c.x, c.y, c.z, 0.f)); }
 
-// shading of one closest hit or miss (render/wavefront.cu:223-356 restricted to the sun and a constant sky)
 // ---------------- material textures (render/wavefront.cu:198-204, 252-270) ----------------
 // (u, v) of a hit from the corner uvs: b1, b2 = barycentric weights of corners 1 and 2
 __device__ __forceinline__ float2 tri_uv(const float4* uvs, int64_t t, float b1, float b2) {
@@ -190,7 +204,7 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
         const bool valid = k < a.n;
         int slot = 0, pix = 0, depth = 0; unsigned smp = 0;
         bool ended = false, wantShadow = false, wantCont = false;
-        float3 T = f3(0.f, 0.f, 0.f), so = T, sd = T, contrib = T, co = T, cd = T; float cpdf = 0.f;
+        float3 T = f3(0.f, 0.f, 0.f), so = T, sd = T, contrib = T, co = T, cd = T; float cpdf = 0.f, stmax = 1e30f;
         if (valid) {
             const int4 info = a.in.info[k];
             slot = info.x; pix = info.y; smp = (unsigned)info.z; depth = info.w;
@@ -203,8 +217,12 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                 float3 L = S.sky;
                 if (S.envTex) {
                     int x, y; float v; env_texel(S, d, x, y, v);
-                    L = f3(S.envTex[(size_t)y * S.envW + x].x, S.envTex[(size_t)y * S.envW + x].y, S.envTex[(size_t)y * S.envW + x].z);
-                    if (T4.w > 0.f) L = L * mis_power(T4.w, 0.5f * env_pdf_texel(S, x, y, v));   // T.w: the last BSDF sample's pdf
+                    const float4 t4 = S.envTex[(size_t)y * S.envW + x];
+                    L = f3(t4.x, t4.y, t4.z);
+                    if (T4.w > 0.f) {   // T.w: pdf of the last BSDF sample (0: camera ray or a delta lobe, counted fully)
+                        if (S.lightMode == CWP_LIGHT_NEE) L = f3(0.f, 0.f, 0.f);
+                        else if (S.lightMode == CWP_LIGHT_MIS) L = L * mis_power(T4.w, S.pEnv * (S.envUniform ? 0.25f * CWPB_INV_PI : env_pdf_texel(S, x, y, v)));
+                    }
                 }
                 add_rgb(S.accum, pix, T * L);
                 ended = true;
@@ -222,8 +240,24 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                 apply_textures(a, mid, I, tri, H.y, H.z, M, nsw);
                 const float3 p = f3(O.x, O.y, O.z) + d * H.x;
                 const float3 em = mat_v3(M.emission);
-                if (em.x > 0.f || em.y > 0.f || em.z > 0.f) add_rgb(S.accum, pix, T * em);   // no emitters are light-sampled
-                if (depth > S.maxDepth) ended = true;
+                if (em.x > 0.f || em.y > 0.f || em.z > 0.f) {   // two-sided emission, weighted against light sampling of this triangle
+                    float w = 1.f;
+                    if (T4.w > 0.f) {
+                        if (S.lightMode == CWP_LIGHT_NEE) w = 0.f;
+                        else if (S.lightMode == CWP_LIGHT_MIS) {
+                            const float cl = fabsf(dot(ng0, d)), pa = S.nEm > 0 ? __ldg(S.matPdf + mid) : 0.f;
+                            w = mis_power(T4.w, cl > 0.f ? S.pTri * pa * H.x * H.x / cl : 0.f);
+                        }
+                    }
+                    if (w > 0.f) add_rgb(S.accum, pix, T * em * w);
+                }
+                bool alive = depth <= S.maxDepth;
+                if (alive && S.rr && depth >= S.rrDepth) {   // Russian roulette: survive with max(T) in [0.05, 1]
+                    const float qs = fminf(fmaxf(maxc(T), 0.05f), 1.f);
+                    if (rnd_s(S.seed, pix, smp, (unsigned)depth + 1u, 6) >= qs) alive = false;
+                    else T = T * (1.f / qs);
+                }
+                if (!alive) ended = true;
                 else {
                     const bool front = dot(ng0, d) < 0.f;
                     const float3 ng = front ? ng0 : -ng0;
@@ -237,35 +271,58 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                     const unsigned dr = (unsigned)depth + 1u;
                     const float ux1 = rnd_s(S.seed, pix, smp, dr, 7), ux2 = sample01(pix, smp, dr, 7, S.seed ^ 0x68E31DA4u);
                     if (has_non_delta(M)) {
-                        // one light sample: the sun alone (weight 1), or with an environment map the sun or the map with
-                        // probability 1/2 each, the map's sample weighted against BSDF sampling by the power heuristic
-                        const float u2 = rnd_s(S.seed, pix, smp, dr, 2), u3 = rnd_s(S.seed, pix, smp, dr, 3);
-                        float3 l = f3(0.f, 0.f, 1.f), Le = S.sunE; float pl = 1.f; bool ok = true, isSun = true;
-                        if (S.envTex) {
-                            const float us = rnd_s(S.seed, pix, smp, dr, 5);
-                            pl = 0.5f;
-                            if (us >= 0.5f) {
-                                isSun = false; ok = false;
-                                const float ue = fminf((us - 0.5f) / 0.5f, 0.99999994f);
-                                const int y = cdf_find(S.envMarg, S.envH, ue);
-                                const float* cr = S.envCond + (size_t)y * (S.envW + 1);
-                                const int x = cdf_find(cr, S.envW, u2);
-                                const float v = (y + u3) / S.envH, w0 = cr[x + 1] - cr[x];
-                                float u = (x + 0.5f) / S.envW;
-                                if (w0 > 0.f) u = (x + fminf((u2 - cr[x]) / w0, 0.99999994f)) / S.envW;   // the rest of u2 within the texel
-                                l = env_dir(S, u, v);
-                                const float pe = env_pdf_texel(S, x, y, v);
-                                if (pe > 0.f) { pl = 0.5f * pe; const float4 t4 = S.envTex[(size_t)y * S.envW + x]; Le = f3(t4.x, t4.y, t4.z); ok = true; }
+                        // one light sample: the light type by its probability, a triangle by power (a uniform point on
+                        // it), an environment texel by luminance x sin(theta); weighted against BSDF sampling by the
+                        // power heuristic (the sun, a near-delta cone, and NEE mode: weight 1)
+                        const float us = rnd_s(S.seed, pix, smp, dr, 5), u2 = rnd_s(S.seed, pix, smp, dr, 2), u3 = rnd_s(S.seed, pix, smp, dr, 3);
+                        float3 l = f3(0.f, 0.f, 1.f), Le = f3(0.f, 0.f, 0.f); float pl = 0.f, tmax = 1e30f; bool isSun = false, ok = false;
+                        int side = 0;   // +1 / -1: the origin side fixed by a triangle sample
+                        if (us < S.pSun) { l = cone_dir(S.sunTo, S.sunCos, u2, u3); Le = S.sunE; pl = S.pSun; isSun = true; ok = true; }
+                        else if (us < S.pSun + S.pTri) {
+                            const int e = cdf_find(S.emCdf, S.nEm, fminf((us - S.pSun) / S.pTri, 0.99999994f));
+                            const float4 a0 = S.emTris[3 * e], a1 = S.emTris[3 * e + 1], a2 = S.emTris[3 * e + 2];
+                            const float su = sqrtf(u2);
+                            const float3 pL = f3(a0.x, a0.y, a0.z) + f3(a1.x, a1.y, a1.z) * (su * (1.f - u3)) + f3(a2.x, a2.y, a2.z) * (su * u3);
+                            const float3 nL = normalize(cross(f3(a1.x, a1.y, a1.z), f3(a2.x, a2.y, a2.z)));
+                            // connect from the shadow ray's own offset origin, so that tmax ends just short of the point
+                            side = dot(ng, pL - p) > 0.f ? 1 : -1;
+                            const float3 dv = pL - (side > 0 ? up : dn);
+                            const float dist2 = dot(dv, dv), dist = sqrtf(dist2);
+                            if (dist > 0.f) {
+                                l = dv * (1.f / dist);
+                                const float cl = fabsf(dot(nL, l));
+                                if (cl > 0.f) {
+                                    const int lm = __float_as_int(a1.w);
+                                    pl = S.pTri * __ldg(S.matPdf + lm) * dist2 / cl; Le = mat_v3(a.mats[lm].emission); tmax = dist * (1.f - 1e-3f); ok = true;
+                                    if (a.mtex && lm < a.nMtex && a.mtex[lm].emission >= 0) {
+                                        const float4 c = tex_rgba(a.texObj[a.mtex[lm].emission], tri_uv(a.uvs, __float_as_int(a0.w), su * (1.f - u3), su * u3));
+                                        Le = Le * f3(c.x, c.y, c.z);
+                                    }
+                                }
                             }
+                        } else if (S.pEnv > 0.f && S.envUniform) {
+                            l = uniform_sphere(u2, u3); pl = S.pEnv * (0.25f * CWPB_INV_PI); Le = env_radiance(S, l); ok = true;
+                        } else if (S.pEnv > 0.f) {
+                            const float ue = fminf((us - S.pSun - S.pTri) / S.pEnv, 0.99999994f);
+                            const int y = cdf_find(S.envMarg, S.envH, ue);
+                            const float* cr = S.envCond + (size_t)y * (S.envW + 1);
+                            const int x = cdf_find(cr, S.envW, u2);
+                            const float v = (y + u3) / S.envH, w0 = cr[x + 1] - cr[x];
+                            float u = (x + 0.5f) / S.envW;
+                            if (w0 > 0.f) u = (x + fminf((u2 - cr[x]) / w0, 0.99999994f)) / S.envW;   // the rest of u2 within the texel
+                            l = env_dir(S, u, v);
+                            const float pe = env_pdf_texel(S, x, y, v);
+                            if (pe > 0.f) { pl = S.pEnv * pe; const float4 t4 = S.envTex[(size_t)y * S.envW + x]; Le = f3(t4.x, t4.y, t4.z); ok = true; }
                         }
-                        if (isSun) l = cone_dir(S.sunTo, S.sunCos, u2, u3);
                         const float3 lL = f3(dot(l, tx), dot(l, ty), dot(l, ns));
                         const float gl = dot(ng, l);
                         if (ok && lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
                             const BsdfValue e = bsdf_eval(M, woL, lL, eta, a.gdEnergy, ux1, ux2);
-                            const float w = isSun ? 1.f : mis_power(pl, e.pdf);
+                            const float w = (isSun || S.lightMode == CWP_LIGHT_NEE) ? 1.f : mis_power(pl, e.pdf);
                             contrib = T * e.f * Le * (fabsf(lL.z) * w / pl);
-                            if (contrib.x > 0.f || contrib.y > 0.f || contrib.z > 0.f) { wantShadow = true; so = gl > 0.f ? up : dn; sd = l; }
+                            if (contrib.x > 0.f || contrib.y > 0.f || contrib.z > 0.f) {
+                                wantShadow = true; so = (side ? side > 0 : gl > 0.f) ? up : dn; sd = l; stmax = tmax;
+                            }
                         }
                     }
                     float3 wiL, wgt; float pdf;
@@ -284,7 +341,7 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
         slot_counts(a.slotCnt, slot, valid, valid, wantShadow, ended);
         const int sp = warp_slot(a.cnt + 1, wantShadow);
         if (sp >= 0) {
-            a.sq.o[sp] = make_float4(so.x, so.y, so.z, 0.f); a.sq.d[sp] = make_float4(sd.x, sd.y, sd.z, 1e30f); a.sq.sc[sp] = slot;
+            a.sq.o[sp] = make_float4(so.x, so.y, so.z, 0.f); a.sq.d[sp] = make_float4(sd.x, sd.y, sd.z, stmax); a.sq.sc[sp] = slot;
             a.sq.c[sp] = make_float4(contrib.x, contrib.y, contrib.z, __int_as_float(pix));
         }
         const int cp = warp_slot(a.cnt, wantCont);
@@ -365,12 +422,14 @@ struct ServeRequest {
     double submitMs = 0, admitMs = 0, doneMs = 0;
     int64_t total = 0, issued = 0, finished = 0; double rays = 0, shadow = 0;
     float4* accum = nullptr; bool done = false;
+    void* lights = nullptr;   // the request's emissive-triangle tables (pool memory), freed at completion
 };
 
 struct cwp_server {
     cwp_batch* batch = nullptr; int device = 0;
     cwp_server_options O{};
     cwp_material* mats = nullptr; int nMats = 0; int* meshMat = nullptr;
+    std::vector<cwp_material> hMats; EmissiveSet em;   // host materials; the meshes' emissive triangles (object space)
     // scenes: instance descriptors per scene (host)
     std::vector<cwp_instance_desc> desc; std::vector<int> sceneFirst;
     // per slot: request id or -1, its instances (host) for the TLAS rebuild
@@ -438,7 +497,10 @@ extern "C" void cwp_server_destroy(cwp_server* s) {
     if (!s) return;
     cudaSetDevice(s->device);
     if (s->st) cudaStreamSynchronize(s->st);
-    for (auto& kv : s->reqs) if (kv.second.accum) cudaFreeAsync(kv.second.accum, s->st);
+    for (auto& kv : s->reqs) {
+        if (kv.second.accum) cudaFreeAsync(kv.second.accum, s->st);
+        if (kv.second.lights) cudaFreeAsync(kv.second.lights, s->st);
+    }
     if (s->st) cudaStreamSynchronize(s->st);
     if (s->pool) cudaMemPoolDestroy(s->pool);
     for (auto& e : s->envs) { cudaFree(e.tex); cudaFree(e.marg); cudaFree(e.cond); }
@@ -504,7 +566,12 @@ static int server_create(cwp_batch* b, const cwp_material* mats, int n, const in
     CWPB_CUDA(cudaMemcpy(s->mats, mats, (size_t)n * sizeof(cwp_material), cudaMemcpyHostToDevice));
     CWPB_CUDA(cudaMemcpy(s->meshMat, meshBase, (size_t)nMesh * sizeof(int), cudaMemcpyHostToDevice));
     CWPB_CUDA(cudaMemset(s->slotCnt, 0, R * kSlotCounters * sizeof(int)));
-    s->nMats = n;
+    s->nMats = n; s->hMats.assign(mats, mats + n);
+    if (std::any_of(mats, mats + n, is_emissive)) {   // emissive triangles of every mesh, from the batch's input triangles
+        std::vector<float4> soup((size_t)3 * batch_tri_count(b));
+        CWPB_CUDA(cudaMemcpy(soup.data(), batch_tri_soup(b), soup.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+        emissive_set((const float*)soup.data(), batch_mesh_first_host(b), nMesh, meshBase, mats, n, s->em);
+    }
     s->slotReq.assign(R, -1); s->slotInst.assign(R, {}); s->hSlotCnt.assign(R * kSlotCounters, 0);
     s->t0 = std::chrono::steady_clock::now();
     return CWP_OK;
@@ -626,6 +693,8 @@ extern "C" int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* i
     CWPB_CHECK(r->scene >= 0 && r->scene + 1 < (int)s->sceneFirst.size(), CWP_ERR_INVALID, "scene %d out of range", r->scene);
     CWPB_CHECK(r->env >= -1 && r->env < (int)s->envs.size(), CWP_ERR_INVALID, "environment map %d out of range (%d maps)", r->env, (int)s->envs.size());
     CWPB_CHECK(std::isfinite(r->env_rot_deg), CWP_ERR_INVALID, "environment rotation is not finite");
+    CWPB_CHECK(r->light_mode >= CWP_LIGHT_MIS && r->light_mode <= CWP_LIGHT_BSDF && (r->rr == 0 || r->rr == 1) && r->rr_depth >= 0 && (r->env_uniform == 0 || r->env_uniform == 1),
+               CWP_ERR_INVALID, "light mode %d, rr %d, rr_depth %d, env_uniform %d", r->light_mode, r->rr, r->rr_depth, r->env_uniform);
     CWPB_CHECK(r->cam.w > 0 && r->cam.h > 0 && r->spp > 0 && r->max_depth >= 0 && r->max_depth <= 64, CWP_ERR_INVALID, "bad request size");
     const int64_t total = (int64_t)r->cam.w * r->cam.h * r->spp;
     CWPB_CHECK(total < (1ll << 31), CWP_ERR_INVALID, "%lld paths in one request (limit 2^31)", (long long)total);
@@ -688,16 +757,43 @@ static int admit(cwp_server* s, bool& changed) {
             const cwp_server::EnvMap& E = s->envs[q.r.env];
             P.envTex = E.tex; P.envMarg = E.marg; P.envCond = E.cond; P.envW = E.w; P.envH = E.h; P.envRot = q.r.env_rot_deg * 3.14159265f / 180.f;
         }
-        s->slotsDirty = true;
-        CWPB_CUDA(cudaMemsetAsync(s->slotCnt + kSlotCounters * slot, 0, kSlotCounters * sizeof(int), s->st));
-        // the scene's instances at the request's frame
+        // the scene's instances at the request's frame, and its emissive triangles there
         std::vector<cwp_instance>& v = s->slotInst[slot]; v.clear();
+        std::vector<float> xf; std::vector<int> im;
         for (int i = s->sceneFirst[q.r.scene]; i < s->sceneFirst[q.r.scene + 1]; i++) {
             float m[12]; cwp_instance rec;
             if (int rc = cwp_xform_animate(&s->desc[i], q.r.frame, m)) return rc;
             if (int rc = cwp_instance_from_xform(m, s->desc[i].mesh, &rec)) return rc;
-            v.push_back(rec);
+            v.push_back(rec); xf.insert(xf.end(), m, m + 12); im.push_back(s->desc[i].mesh);
         }
+        if (!s->em.empty() && q.r.light_mode != CWP_LIGHT_BSDF) {
+            std::vector<float> emT, emC, mlp;
+            frame_lights(s->em, xf.data(), im.data(), (int64_t)im.size(), s->hMats.data(), s->nMats, emT, emC, mlp);
+            if (!emT.empty()) {
+                const size_t bT = emT.size() * sizeof(float), bC = (emC.size() * sizeof(float) + 15) & ~(size_t)15, bM = mlp.size() * sizeof(float);
+                const cudaError_t e2 = (int64_t)(bT + bC + bM) <= avail ? cudaMallocFromPoolAsync(&q.lights, bT + bC + bM, s->pool, s->st) : cudaErrorMemoryAllocation;
+                if (e2 == cudaErrorMemoryAllocation) {   // no room for the tables: the request waits with its image freed
+                    cudaGetLastError(); q.lights = nullptr;
+                    CWPB_CUDA(cudaFreeAsync(q.accum, s->st)); q.accum = nullptr;
+                    break;
+                }
+                CWPB_CUDA(e2);
+                avail -= (int64_t)(bT + bC + bM);
+                char* base = (char*)q.lights;   // pageable sources: staged before the calls return
+                CWPB_CUDA(cudaMemcpyAsync(base, emT.data(), bT, cudaMemcpyHostToDevice, s->st));
+                CWPB_CUDA(cudaMemcpyAsync(base + bT, emC.data(), emC.size() * sizeof(float), cudaMemcpyHostToDevice, s->st));
+                CWPB_CUDA(cudaMemcpyAsync(base + bT + bC, mlp.data(), bM, cudaMemcpyHostToDevice, s->st));
+                P.emTris = (const float4*)base; P.emCdf = (const float*)(base + bT); P.matPdf = (const float*)(base + bT + bC); P.nEm = (int)(emT.size() / 12);
+            }
+        }
+        // light-type probabilities (render/wavefront.cu:531-533): equal over the enabled types
+        const float sunL = 0.2126f * P.sunE.x + 0.7152f * P.sunE.y + 0.0722f * P.sunE.z;
+        const bool sunOn = sunL > 0.f, triOn = P.nEm > 0 && q.r.light_mode != CWP_LIGHT_BSDF, envOn = q.r.env >= 0 && q.r.light_mode != CWP_LIGHT_BSDF;
+        const int nt = (int)sunOn + (int)triOn + (int)envOn;
+        P.pSun = sunOn ? 1.f / nt : 0.f; P.pTri = triOn ? 1.f / nt : 0.f; P.pEnv = envOn ? 1.f / nt : 0.f;
+        P.lightMode = q.r.light_mode; P.rr = q.r.rr; P.rrDepth = q.r.rr_depth; P.envUniform = q.r.env_uniform;
+        s->slotsDirty = true;
+        CWPB_CUDA(cudaMemsetAsync(s->slotCnt + kSlotCounters * slot, 0, kSlotCounters * sizeof(int), s->st));
         q.slot = slot; q.admitMs = now_ms(s); s->info.admissions++; s->admitted.push_back(slot);
         s->slotReq[slot] = q.id; s->hSlotCnt[kSlotCounters * slot + 2] = 0;
         s->pending.pop_front();
@@ -803,6 +899,7 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         q.rays = c[0]; q.shadow = c[1]; q.finished = c[2];
         if (q.issued == q.total && q.finished == q.total) {
             q.done = true; q.doneMs = t; s->completed.push_back(q.id); s->slotReq[k] = -1; q.slot = -1;
+            if (q.lights) { CWPB_CUDA(cudaFreeAsync(q.lights, s->st)); q.lights = nullptr; }
         }
     }
     s->info.step_ms += now_ms(s) - stepStart;

@@ -318,8 +318,10 @@ int cwp_batch_status(cwp_batch* b);   /* synchronises; CWP_ERR_TRAVERSAL if a ra
  * memory allow; every step advances all admitted requests' paths by one bounce in the same launches (new camera
  * paths join at every step), so requests that arrive while others run share the GPU. Each request's image depends only
  * on its own inputs: the sample streams are keyed by (pixel, sample, depth, dimension, seed).
- * Replaces the full integrator for OpenPBR-subset materials with sun next-event estimation and a constant sky
- * (render/wavefront.cu:223-356 shadeFull, render/bsdf.h, scene/material.h); the request loop itself is new.
+ * Replaces the full integrator for instanced scenes (render/wavefront.cu:223-356 shadeFull<INST>, render/bsdf.h,
+ * scene/material.h): OpenPBR-subset materials, next-event estimation with one light sample per vertex over the sun,
+ * the emissive triangles (by power) and an environment map (by luminance x sin(theta)), combined with BSDF sampling by
+ * the power heuristic, optional Russian roulette; the request loop itself is new.
  * ------------------------------------------------------------------------------------------------------------------ */
 typedef struct cwp_material {        /* Material (scene/material.h:12-17), 64 B */
     float base_color[3]; float metallic;
@@ -352,10 +354,19 @@ typedef struct cwp_request {
     float sun_to[3], sun_e[3], sky[3];
     float sun_cos, eps;    /* cos of the sun's half angle; ray offset */
     int32_t env;           /* environment map of the server (cwp_server_set_envmaps) lighting the request, or -1: the
-                              constant sky. With a map, a light sample picks the sun or the map with probability 1/2 each,
-                              the map by luminance x sin(theta), combined with BSDF sampling by the power heuristic */
+                              constant sky (not light-sampled) */
     float env_rot_deg;     /* rotation of the map about +z (the reference's --env_rot) */
+    /* Light sampling (RenderOptions, render/renderer.h:21-25). A light sample picks one of the enabled light types with
+     * equal probability (render/wavefront.cu:531-533): the sun when luminance(sun_e) > 0, the emissive triangles of
+     * the scene at the request's frame when it has any, the map when env >= 0; the latter two not in BSDF mode. */
+    int32_t light_mode;    /* CWP_LIGHT_MIS (0, default), CWP_LIGHT_NEE: emitters hit by BSDF samples count nothing,
+                              CWP_LIGHT_BSDF: only the sun is light-sampled */
+    int32_t rr, rr_depth;  /* Russian roulette from depth rr_depth on (survival max(T) clamped to [0.05, 1]); rr = 0 off */
+    int32_t env_uniform;   /* 1: environment light samples uniform on the sphere instead of by luminance */
 } cwp_request;
+#define CWP_LIGHT_MIS 0
+#define CWP_LIGHT_NEE 1
+#define CWP_LIGHT_BSDF 2
 
 typedef struct cwp_request_stats {
     double submit_ms, admit_ms, done_ms;    /* on the server's clock (ms since creation) */
@@ -435,6 +446,20 @@ int cwp_display(const float* d_accum, uint8_t* d_rgba, int64_t n, int32_t spp, f
  * ------------------------------------------------------------------------------------------------------------------ */
 int cwp_hdr_load(const char* path, int32_t* w, int32_t* h, float* rgb);
 int cwp_envmap_build(const float* rgb, int32_t w, int32_t h, float strength, float* texels, float* marg, float* cond);
+
+/* ------------------------------------------------------------------------------------------------------------------
+ * Emissive triangles of an instanced scene at one frame, as the serving form light-samples them. Replaces the light
+ * tables of SceneSetup::frameData (app/scene_setup.cpp:274-299): every instance in order, each emissive triangle of
+ * its mesh in mesh order (material = mesh_mat_base[mesh] + face material, emissive when an emission component is
+ * > 0), corners transformed by the instance's 3x4 rows (xforms, 12 floats per instance, as cwp_xform_animate gives),
+ * power = luminance(emission) x area in double. em_tris: 3 float4 per triangle ((w0, global triangle id), (w1 - w0,
+ * material), (w2 - w0, 0)); the global id (mesh's first triangle + face index) addresses the uvs of
+ * cwp_server_set_textures. em_cdf: n_em + 1 floats, the CDF of power; mat_pdf: n_mats floats, luminance(emission) /
+ * total power = the area density of sampling a point of that material. em_tris = NULL: *n_em only. A scene whose
+ * emissive triangles have no area has n_em = 0.
+ * ------------------------------------------------------------------------------------------------------------------ */
+int cwp_emissive_tables(const cwp_mesh_view* meshes, int32_t n_meshes, const int32_t* mesh_mat_base, const cwp_material* mats, int32_t n_mats,
+                        const float* xforms, const int32_t* inst_mesh, int64_t n_inst, float* em_tris, float* em_cdf, float* mat_pdf, int64_t* n_em);
 
 /* ------------------------------------------------------------------------------------------------------------------
  * On-chip read bandwidth of a device, for the traversal kernels' roofline (not in the reference, whose node and

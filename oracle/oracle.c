@@ -1090,12 +1090,66 @@ void orc_bsdf_sample(const float* mats, const int* mat, const float* wo, const f
 
 /* ------------------------------------------------------------------ serving form: one request on the host
  * Not a reference function as a whole: restates the CUDA serving loop's per-path arithmetic (camera ray with a box
- * filter, render/wavefront.cu:42-58; shading = shadeFull restricted to the sun and a constant sky,
- * render/wavefront.cu:223-356) over the two-level scene above and the BSDF restatement. Paths [j0, j1) of the request
+ * filter, render/wavefront.cu:42-58; shading = shadeFull<INST>, render/wavefront.cu:223-356: one light sample per
+ * vertex over the sun, the emissive triangles and an environment map with the power heuristic, light modes, Russian
+ * roulette) over the two-level scene above and the BSDF restatement. Paths [j0, j1) of the request
  * in the CUDA path order (pixel = tile order of j mod N, sample j / N); accum = w * h float4 sums, counts[0] closest
  * rays, counts[1] shadow rays. */
 typedef struct { float pos[3], ax[3], ay[3], az[3], fx, fy, px, py; int w, h; float lens_r, focus_d; } OCam;
-typedef struct { int scene, frame; OCam cam; int spp, max_depth; unsigned seed; float sun_to[3], sun_e[3], sky[3], sun_cos, eps; int env; float env_rot_deg; } OReq;
+typedef struct { int scene, frame; OCam cam; int spp, max_depth; unsigned seed; float sun_to[3], sun_e[3], sky[3], sun_cos, eps; int env; float env_rot_deg;
+                 int light_mode, rr, rr_depth, env_uniform; } OReq;
+enum { O_LIGHT_MIS = 0, O_LIGHT_NEE = 1, O_LIGHT_BSDF = 2 };   /* render/params.h:23 */
+
+/* Emissive-triangle light tables of one frame (SceneSetup::frameData, app/scene_setup.cpp:274-299). soup: 12 floats
+ * per triangle of every mesh in mesh order, (v0, face id), (v1, face material), (v2, 0); triangle material =
+ * mesh_mat[mesh] + face material clamped to the table; emissive when an emission component is > 0. Instances in
+ * order, each one's emissive triangles in mesh order: corners by the float 3x4 rows, area 0.5 |e1 x e2| in float,
+ * power luminance x area summed in double. em_tris: 12 floats per triangle, (w0, global id), (e1, material), (e2, 0);
+ * em_cdf n + 1 floats; mat_pdf n_mats floats = luminance / total power. Returns n (0 when the total power is 0);
+ * em_tris NULL: the count only. */
+long orc_emissive_tables(const float* soup, const int* mesh_first, int n_mesh, const int* mesh_mat, const float* mats, int n_mats,
+                         const float* xf, const int* inst_mesh, long n_inst, float* em_tris, float* em_cdf, float* mat_pdf) {
+    const OMat* M = (const OMat*)mats;
+    long n = 0; double tot = 0.0;
+    double* pw = NULL; long cap = 0;
+    for (long i = 0; i < n_inst; i++) {
+        const float* m = xf + 12 * i; const int mesh = inst_mesh[i];
+        for (int g = mesh_first[mesh]; g < mesh_first[mesh + 1]; g++) {
+            const float* r = soup + 12 * (size_t)g;
+            int mid = mesh_mat[mesh] + fi(r[7]); mid = mid < 0 ? 0 : mid >= n_mats ? n_mats - 1 : mid;
+            if (!(M[mid].emission[0] > 0.f || M[mid].emission[1] > 0.f || M[mid].emission[2] > 0.f)) continue;
+            float w[3][3];
+            for (int c = 0; c < 3; c++) for (int k = 0; k < 3; k++)
+                w[c][k] = m[4 * k] * r[4 * c] + m[4 * k + 1] * r[4 * c + 1] + m[4 * k + 2] * r[4 * c + 2] + m[4 * k + 3];
+            const V3 e1 = v3(w[1][0] - w[0][0], w[1][1] - w[0][1], w[1][2] - w[0][2]), e2 = v3(w[2][0] - w[0][0], w[2][1] - w[0][1], w[2][2] - w[0][2]);
+            const V3 cr = cross3(e1, e2);
+            const double area = 0.5 * sqrtf(dot3(cr, cr));
+            double pwr = o_lum(v3(M[mid].emission[0], M[mid].emission[1], M[mid].emission[2])) * area; pwr = pwr > 0 ? pwr : 0;
+            if (n == cap) { cap = cap ? 2 * cap : 256; pw = (double*)realloc(pw, sizeof(double) * (size_t)cap); }
+            pw[n] = pwr; tot += pwr;
+            if (em_tris) {
+                float* t = em_tris + 12 * (size_t)n;
+                t[0] = w[0][0]; t[1] = w[0][1]; t[2] = w[0][2]; memcpy(&t[3], &g, 4);
+                t[4] = e1.x; t[5] = e1.y; t[6] = e1.z; memcpy(&t[7], &mid, 4);
+                t[8] = e2.x; t[9] = e2.y; t[10] = e2.z; t[11] = 0.f;
+            }
+            n++;
+        }
+    }
+    if (!(tot > 0)) n = 0;
+    if (em_tris) {
+        for (int j = 0; j < n_mats; j++) mat_pdf[j] = 0.f;
+        if (n) {
+            double c = 0.0; em_cdf[0] = 0.f;
+            for (long e = 0; e < n; e++) { c += pw[e]; em_cdf[e + 1] = (float)(c / tot); }
+            em_cdf[n] = 1.f;
+            for (int j = 0; j < n_mats; j++)
+                if (M[j].emission[0] > 0.f || M[j].emission[1] > 0.f || M[j].emission[2] > 0.f) mat_pdf[j] = (float)(o_lum(v3(M[j].emission[0], M[j].emission[1], M[j].emission[2])) / tot);
+        }
+    }
+    free(pw);
+    return n;
+}
 
 /* Environment map tables (scene/environment.cpp:7-38): texels = rgb x strength (float4), marg = CDF over rows (h + 1),
  * cond = CDF within each row (h rows of w + 1); texel weight luminance x sin(theta), sums in double. */
@@ -1177,13 +1231,20 @@ static int o_tile_pixel(int j, int w, int h) {
 long orc_render_request(const void* reqp, int width, int tlas_width, const float* blas, const float* tris, const float* tlas, int root, const float* inst,
                         const float* mats, int n_mats, const int* mesh_mat, int gd, long j0, long j1, float* accum, long long* counts,
                         const float* env_tex, const float* env_marg, const float* env_cond, int env_w, int env_h,
-                        const void* tex, const void* mtex, int n_mtex, const float* uvs, const float* tans, const int* mesh_first) {
+                        const void* tex, const void* mtex, int n_mtex, const float* uvs, const float* tans, const int* mesh_first,
+                        const float* em_tris, const float* em_cdf, const float* mat_pdf, long n_em) {
     const OTex* TX = (const OTex*)tex; const OMTex* MX = (const OMTex*)mtex;
     const OReq* R = (const OReq*)reqp; const OCam* C = &R->cam;
     const int N = C->w * C->h; long bad = 0;
     const OEnv E = { env_tex, env_marg, env_cond, env_w, env_h, R->env_rot_deg * 3.14159265f / 180.f };
     const int hasEnv = R->env >= 0 && env_tex != NULL;
     const V3 sunTo = v3(R->sun_to[0], R->sun_to[1], R->sun_to[2]), sunE = v3(R->sun_e[0], R->sun_e[1], R->sun_e[2]), sky = v3(R->sky[0], R->sky[1], R->sky[2]);
+    const OMat* MT = (const OMat*)mats;
+    /* light-type probabilities (render/wavefront.cu:531-533): equal over the sun (luminance > 0), the emissive
+     * triangles and the map, the latter two not in BSDF mode */
+    const int sunOn = o_lum(sunE) > 0.f, triOn = n_em > 0 && R->light_mode != O_LIGHT_BSDF, envOn = hasEnv && R->light_mode != O_LIGHT_BSDF;
+    const int nt = sunOn + triOn + envOn;
+    const float pSun = sunOn ? 1.f / nt : 0.f, pTri = triOn ? 1.f / nt : 0.f, pEnv = envOn ? 1.f / nt : 0.f;
     for (long j = j0; j < j1; j++) {
         const int pix = o_tile_pixel((int)(j % N), C->w, C->h); const unsigned smp = (unsigned)(j / N), seed = R->seed;
         const int x = pix % C->w, y = pix / C->w;
@@ -1203,7 +1264,10 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
                 if (hasEnv) {
                     int ex, ey; float ev; o_env_texel(&E, d, &ex, &ey, &ev);
                     const float* tx4 = E.tex + 4 * ((size_t)ey * E.w + ex); L = v3(tx4[0], tx4[1], tx4[2]);
-                    if (lastPdf > 0.f) L = muls(L, o_mis(lastPdf, 0.5f * o_env_pdf_texel(&E, ex, ey, ev)));
+                    if (lastPdf > 0.f) {
+                        if (R->light_mode == O_LIGHT_NEE) L = v3(0.f, 0.f, 0.f);
+                        else if (R->light_mode == O_LIGHT_MIS) L = muls(L, o_mis(lastPdf, pEnv * (R->env_uniform ? 0.25f * 0.31830989f : o_env_pdf_texel(&E, ex, ey, ev))));
+                    }
                 }
                 A[0] += T.x * L.x; A[1] += T.y * L.y; A[2] += T.z * L.z; break;
             }
@@ -1245,8 +1309,23 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
                 }
             }
             const V3 p = add(o, muls(d, t));
-            if (M->emission[0] > 0.f || M->emission[1] > 0.f || M->emission[2] > 0.f) { A[0] += T.x * M->emission[0]; A[1] += T.y * M->emission[1]; A[2] += T.z * M->emission[2]; }
+            if (M->emission[0] > 0.f || M->emission[1] > 0.f || M->emission[2] > 0.f) {   /* MIS against light sampling of this triangle */
+                float w = 1.f;
+                if (lastPdf > 0.f) {
+                    if (R->light_mode == O_LIGHT_NEE) w = 0.f;
+                    else if (R->light_mode == O_LIGHT_MIS) {
+                        const float cl = fabsf(dot3(ng0, d)), pa = n_em > 0 ? mat_pdf[mid] : 0.f;
+                        w = o_mis(lastPdf, cl > 0.f ? pTri * pa * t * t / cl : 0.f);
+                    }
+                }
+                if (w > 0.f) { A[0] += T.x * M->emission[0] * w; A[1] += T.y * M->emission[1] * w; A[2] += T.z * M->emission[2] * w; }
+            }
             if (depth > R->max_depth) break;
+            if (R->rr && depth >= R->rr_depth) {   /* Russian roulette */
+                const float qs = fminf(fmaxf(fmaxf(T.x, fmaxf(T.y, T.z)), 0.05f), 1.f);
+                if (orc_rng(pix, smp, (unsigned)depth + 1u, 6, seed) >= qs) break;
+                T = muls(T, 1.f / qs);
+            }
             const int front = dot3(ng0, d) < 0.f;
             const V3 ng = front ? ng0 : neg(ng0);
             V3 ns = front ? nsw : neg(nsw); const V3 wo = neg(d);
@@ -1258,37 +1337,62 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
             const unsigned dr = (unsigned)depth + 1u;
             const float ux1 = orc_rng(pix, smp, dr, 7, seed), ux2 = orc_rng(pix, smp, dr, 7, seed ^ 0x68E31DA4u);
             if (o_non_delta(M)) {
-                /* one light sample (render/wavefront.cu:300-341 with the sun and the map as the lights) */
-                const float u2 = orc_rng(pix, smp, dr, 2, seed), u3 = orc_rng(pix, smp, dr, 3, seed);
-                V3 l = v3(0.f, 0.f, 1.f), Le = sunE; float pl = 1.f; int ok = 1, isSun = 1;
-                if (hasEnv) {
-                    const float us = orc_rng(pix, smp, dr, 5, seed);
-                    pl = 0.5f;
-                    if (us >= 0.5f) {
-                        isSun = 0; ok = 0;
-                        const float ue = fminf((us - 0.5f) / 0.5f, 0.99999994f);
-                        const int y = o_cdf_find(E.marg, E.h, ue);
-                        const float* cr = E.cond + (size_t)y * (E.w + 1);
-                        const int x = o_cdf_find(cr, E.w, u2);
-                        const float v = (y + u3) / E.h, w0 = cr[x + 1] - cr[x];
-                        float u = (x + 0.5f) / E.w;
-                        if (w0 > 0.f) u = (x + fminf((u2 - cr[x]) / w0, 0.99999994f)) / E.w;
-                        const float ph = (0.5f - u) * 6.2831853f + E.rot, th = v * 3.14159265f, st = sinf(th);
-                        l = v3(st * cosf(ph), st * sinf(ph), cosf(th));
-                        const float pe = o_env_pdf_texel(&E, x, y, v);
-                        if (pe > 0.f) { const float* t4 = E.tex + 4 * ((size_t)y * E.w + x); pl = 0.5f * pe; Le = v3(t4[0], t4[1], t4[2]); ok = 1; }
+                /* one light sample (render/wavefront.cu:295-344) */
+                const float us = orc_rng(pix, smp, dr, 5, seed), u2 = orc_rng(pix, smp, dr, 2, seed), u3 = orc_rng(pix, smp, dr, 3, seed);
+                V3 l = v3(0.f, 0.f, 1.f), Le = v3(0.f, 0.f, 0.f); float pl = 0.f, tmax = 1e30f; int ok = 0, isSun = 0, side = 0;
+                if (us < pSun) { l = cone_dir(sunTo, R->sun_cos, u2, u3); Le = sunE; pl = pSun; isSun = 1; ok = 1; }
+                else if (us < pSun + pTri) {
+                    const float ut = fminf((us - pSun) / pTri, 0.99999994f);
+                    const int e = o_cdf_find(em_cdf, (int)n_em, ut);
+                    const float* a = em_tris + 12 * (size_t)e;
+                    const float su = sqrtf(u2);
+                    const V3 a1 = v3(a[4], a[5], a[6]), a2 = v3(a[8], a[9], a[10]);
+                    const V3 pL = add(add(v3(a[0], a[1], a[2]), muls(a1, su * (1.f - u3))), muls(a2, su * u3));
+                    const V3 nL = normz(cross3(a1, a2));
+                    side = dot3(ng, sub(pL, p)) > 0.f ? 1 : -1;
+                    const V3 dv = sub(pL, side > 0 ? up : dn);
+                    const float dist2 = dot3(dv, dv), dist = sqrtf(dist2);
+                    if (dist > 0.f) {
+                        l = muls(dv, 1.f / dist);
+                        const float cl = fabsf(dot3(nL, l));
+                        if (cl > 0.f) {
+                            const int lm = fi(a[7]);
+                            pl = pTri * mat_pdf[lm] * dist2 / cl; Le = v3(MT[lm].emission[0], MT[lm].emission[1], MT[lm].emission[2]); tmax = dist * (1.f - 1e-3f); ok = 1;
+                            if (MX && lm < n_mtex && MX[lm].emission >= 0) {
+                                const float* q = uvs + 8 * (size_t)fi(a[3]); const float b1 = su * (1.f - u3), b2 = su * u3, b0 = 1.f - b1 - b2;
+                                float c[4]; o_tex(&TX[MX[lm].emission], q[0] * b0 + q[2] * b1 + q[4] * b2, 1.f - (q[1] * b0 + q[3] * b1 + q[5] * b2), c);
+                                Le = v3(Le.x * c[0], Le.y * c[1], Le.z * c[2]);
+                            }
+                        }
                     }
+                } else if (pEnv > 0.f && R->env_uniform) {
+                    const float z = 1.f - 2.f * u2, r = sqrtf(fmaxf(0.f, 1.f - z * z)), ph = 6.2831853f * u3;
+                    l = v3(r * cosf(ph), r * sinf(ph), z); pl = pEnv * (0.25f * 0.31830989f);
+                    int ex, ey; float ev; o_env_texel(&E, l, &ex, &ey, &ev);
+                    const float* t4 = E.tex + 4 * ((size_t)ey * E.w + ex); Le = v3(t4[0], t4[1], t4[2]); ok = 1;
+                } else if (pEnv > 0.f) {
+                    const float ue = fminf((us - pSun - pTri) / pEnv, 0.99999994f);
+                    const int y = o_cdf_find(E.marg, E.h, ue);
+                    const float* cr = E.cond + (size_t)y * (E.w + 1);
+                    const int x = o_cdf_find(cr, E.w, u2);
+                    const float v = (y + u3) / E.h, w0 = cr[x + 1] - cr[x];
+                    float u = (x + 0.5f) / E.w;
+                    if (w0 > 0.f) u = (x + fminf((u2 - cr[x]) / w0, 0.99999994f)) / E.w;
+                    const float ph = (0.5f - u) * 6.2831853f + E.rot, th = v * 3.14159265f, st = sinf(th);
+                    l = v3(st * cosf(ph), st * sinf(ph), cosf(th));
+                    const float pe = o_env_pdf_texel(&E, x, y, v);
+                    if (pe > 0.f) { const float* t4 = E.tex + 4 * ((size_t)y * E.w + x); pl = pEnv * pe; Le = v3(t4[0], t4[1], t4[2]); ok = 1; }
                 }
-                if (isSun) l = cone_dir(sunTo, R->sun_cos, u2, u3);
                 const V3 lL = v3(dot3(l, tx), dot3(l, ty), dot3(l, ns));
                 const float gl = dot3(ng, l);
                 if (ok && lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
                     const OEval e = o_bsdf_eval(M, woL, lL, eta, gd, ux1, ux2);
-                    const float wgt_l = isSun ? 1.f : o_mis(pl, e.pdf);
+                    const float wgt_l = (isSun || R->light_mode == O_LIGHT_NEE) ? 1.f : o_mis(pl, e.pdf);
                     const V3 c = muls(mulv(mulv(T, e.f), Le), fabsf(lL.z) * wgt_l / pl);
                     if (c.x > 0.f || c.y > 0.f || c.z > 0.f) {
-                        float st = 1e30f, su, sv; int sh, shi;
-                        if (o_inst1(width, tlas_width, 1, blas, tris, (const V4*)tlas, root, inst, gl > 0.f ? up : dn, l, 0.f, &st, &sh, &su, &sv, &shi) < 0) bad++;
+                        float st = tmax, su, sv; int sh, shi;
+                        const V3 so = (side ? side > 0 : gl > 0.f) ? up : dn;
+                        if (o_inst1(width, tlas_width, 1, blas, tris, (const V4*)tlas, root, inst, so, l, 0.f, &st, &sh, &su, &sv, &shi) < 0) bad++;
                         counts[1]++;
                         if (sh < 0) { A[0] += c.x; A[1] += c.y; A[2] += c.z; }
                     }

@@ -59,7 +59,9 @@ def _load_oracle():
     L.orc_render_stats.argtypes = [C.c_int, C.c_void_p]
     L.orc_render_request.restype = C.c_long
     L.orc_render_request.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
-                                     + [C.c_void_p] * 3 + [C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3)
+                                     + [C.c_void_p] * 3 + [C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3 + [C.c_void_p] * 3 + [C.c_long])
+    L.orc_emissive_tables.restype = C.c_long
+    L.orc_emissive_tables.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_long] + [C.c_void_p] * 3
     L.orc_texture_sample.restype = None
     L.orc_texture_sample.argtypes = [C.c_void_p] * 4 + [C.c_long]
     L.orc_envmap_build.restype = None
@@ -157,6 +159,27 @@ class Oracle:
         self.L.orc_envmap_build(rgb.ctypes.data, w, h, strength, tex.ctypes.data, marg.ctypes.data, cond.ctypes.data)
         return tex, marg, cond
 
+    def emissive_tables(self, meshes, mesh_mat, mats, xforms, inst_mesh):
+        """light tables of the emissive triangles of an instanced scene at one frame: (em_tris [n, 12], em_cdf [n + 1],
+        mat_pdf [n_mats]); meshes: (verts, faces, face_mat, _) tuples"""
+        soup, first = [], [0]
+        for v, f, fm, _ in meshes:
+            v = np.asarray(v, np.float32); f = np.asarray(f, np.int64)
+            r = np.zeros((len(f), 12), np.float32)
+            r[:, 0:3], r[:, 4:7], r[:, 8:11] = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+            r[:, 3] = np.arange(len(f), dtype=np.int32).view(np.float32)
+            r[:, 7] = (np.zeros(len(f), np.int32) if fm is None else np.asarray(fm, np.int32)).view(np.float32)
+            soup.append(r); first.append(first[-1] + len(f))
+        soup = np.ascontiguousarray(np.concatenate(soup)); first = np.array(first, np.int32)
+        mm = np.ascontiguousarray(mesh_mat, np.int32); ms = np.ascontiguousarray(mats, np.float32)
+        xf = np.ascontiguousarray(xforms, np.float32).reshape(-1, 12); im = np.ascontiguousarray(inst_mesh, np.int32)
+        args = (soup.ctypes.data, first.ctypes.data, len(first) - 1, mm.ctypes.data, ms.ctypes.data, len(ms), xf.ctypes.data, im.ctypes.data, len(im))
+        n = self.L.orc_emissive_tables(*args, None, None, None)
+        t = np.zeros((n, 12), np.float32); c = np.zeros(n + 1, np.float32); p = np.zeros(len(ms), np.float32)
+        n2 = self.L.orc_emissive_tables(*args, t.ctypes.data, c.ctypes.data, p.ctypes.data)
+        assert n2 == n
+        return t, (c if n else np.zeros(0, np.float32)), p
+
     def texture_sample(self, tex, ids, uv):
         """lookups (texture id, (u, v)) -> rgba [n, 4] with the oracle's restatement of the texture unit; tex: a
         cwp_texture array"""
@@ -164,10 +187,12 @@ class Oracle:
         self.L.orc_texture_sample(C.addressof(tex), ids.ctypes.data, uv.ctypes.data, out.ctypes.data, len(ids))
         return out
 
-    def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None, tlas_width=2, env=None, textures=None):
+    def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None, tlas_width=2, env=None, textures=None,
+                       lights=None):
         """A serving request on the host: (accum [w h, 4], counts [2]). env: (texels, marg, cond) of the request's
         environment map when Request.env >= 0, else None. textures: (cwp_texture array, cwp_material_textures array,
-        uvs, tans or None, mesh_first) as given to the server, else None."""
+        uvs, tans or None, mesh_first) as given to the server, else None. lights: (em_tris, em_cdf, mat_pdf) of the
+        request's scene at its frame (emissive_tables), else None."""
         n = req.cam.w * req.cam.h * req.spp
         j0, j1 = (0, n) if paths is None else paths
         acc = np.zeros((req.cam.w * req.cam.h, 4), np.float32); cnt = np.zeros(2, np.int64)
@@ -179,7 +204,9 @@ class Oracle:
                                           else (None, None, None, 0, 0)),
                                         *((C.addressof(textures[0]), C.addressof(textures[1]), len(textures[1]), textures[2].ctypes.data,
                                            textures[3].ctypes.data if textures[3] is not None else None, textures[4].ctypes.data) if textures is not None
-                                          else (None, None, 0, None, None, None)))
+                                          else (None, None, 0, None, None, None)),
+                                        *((lights[0].ctypes.data, lights[1].ctypes.data, lights[2].ctypes.data, len(lights[0])) if lights is not None and len(lights[0])
+                                          else (None, None, None, 0)))
         assert bad == 0
         return acc, cnt
 

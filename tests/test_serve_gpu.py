@@ -29,6 +29,7 @@ def test_device_bsdf_matches_reference(gpu, cwp):
 def serving(gpu, cwp):
     meshes, descs, first, mats, base, boxes = cwp.serving_scenes(n_scenes=3, seed=2, tris=(200, 8000), instances=(1, 24), blas_per_scene=(1, 3))
     b = cwp.Batch(meshes)
+    b.meshes = meshes   # the host meshes, for the oracle's emissive-triangle tables
     return b, descs, first, mats, base, boxes
 
 
@@ -143,6 +144,94 @@ def test_environment_request_matches_oracle(gpu, cwp, oracle, serving):
         assert np.allclose(am, aa, rtol=1e-4, atol=1e-5)
     with pytest.raises(cwp.CwpError):
         bad = requests(cwp, boxes, 1, seed=3)[0]; bad.env = 1   # only one map
+        s.submit(bad)
+
+
+def _emissive(mats, base, rgb=(4.0, 3.0, 2.0)):
+    """every mesh's material 1 (one box in seven) emits"""
+    m = mats.copy()
+    for b0 in base:
+        m[b0 + 1, 8:11] = rgb
+    return m
+
+
+@pytest.mark.parametrize("case", ["sun", "env", "nee", "bsdf", "rr", "env_uniform"])
+def test_emissive_request_matches_oracle(gpu, cwp, oracle, serving, case):
+    """Emissive boxes as area lights: a light sample picks the sun, a triangle by power (a uniform point on it, the
+    shadow ray ending just short of it) or an environment texel, each type with equal probability, and is weighted
+    against BSDF sampling by the power heuristic; emitters hit by BSDF samples are weighted the other way. The MIS, NEE
+    and BSDF modes, Russian roulette and uniform environment samples: the request's image matches the oracle's
+    restatement at >= 45 dB and the ray counts agree."""
+    b, descs, first, mats, base, boxes = serving
+    em = _emissive(mats, base)
+    s = cwp.Server(b, em, base, max_paths=1 << 16, max_requests=4)
+    s.set_scenes(descs, first)
+    g = golden("env.npz")
+    s.set_envmaps([(g["big_rgb"], 1.5)])
+    req = requests(cwp, boxes, 1, seed=29, res=((64, 48),), spps=(4,))[0]
+    if case != "sun":
+        req.env, req.env_rot_deg = 0, 30.0
+    req.light_mode = {"nee": cwp.LIGHT_NEE, "bsdf": cwp.LIGHT_BSDF}.get(case, cwp.LIGHT_MIS)
+    if case == "rr":
+        req.rr, req.rr_depth = 1, 1
+    req.env_uniform = 1 if case == "env_uniform" else 0
+    (acc, st), = run_all(s, [req])
+    nodes, tris = b.download(b.tuning().width)
+    tlas, roots, inst = b.download_tlas(4, _n_inst(b, 4))
+    lights = cwp.emissive_tables(b.meshes, base, em, *cwp.scene_xforms(descs, first, req.scene, req.frame))
+    assert len(lights[0]) > 0
+    ref, cnt = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, em, base, tlas_width=b.tlas_width,
+                                     env=cwp.envmap_build(g["big_rgb"], 1.5) if req.env >= 0 else None, lights=lights)
+    a = acc[:, :3] / req.spp; r = ref[:, :3] / req.spp
+    assert cwp.imageio.psnr(a, r) >= 45.0
+    assert abs(st.rays - cnt[0]) <= 2e-3 * cnt[0] and abs(st.shadow_rays - cnt[1]) <= 2e-3 * max(cnt[1], 1)
+
+
+def test_light_modes_agree_and_requests_keep_their_lights(gpu, cwp, serving):
+    """Lit by the emissive boxes alone (no sun, black sky): light sampling with MIS, light sampling alone (NEE), BSDF
+    sampling alone and MIS with Russian roulette converge to the same image. The reference's consistency check
+    (tests/mis_consistency.py:1-6) restated: 8 independent seeds per mode, the mean luminance of every region of a 4x4
+    grid per seed, per mode its mean and standard error over the seeds, every pair of modes z = |a - b| / sqrt(se_a^2 +
+    se_b^2) <= 3. MIS is less noisy than BSDF sampling. Requests of different scenes and frames in one mix give each
+    one's image alone (every slot reads its own request's light tables)."""
+    b, descs, first, mats, base, boxes = serving
+    em = _emissive(mats, base)
+    s = cwp.Server(b, em, base, max_paths=1 << 20, max_requests=8)
+    s.set_scenes(descs, first)
+    w, h, gx, gy = 64, 48, 4, 4
+    stats = {}
+    for name, mode, rr in (("mis", cwp.LIGHT_MIS, 0), ("nee", cwp.LIGHT_NEE, 0), ("bsdf", cwp.LIGHT_BSDF, 0), ("rr", cwp.LIGHT_MIS, 1)):
+        reqs = []
+        for seed in range(8):
+            r = requests(cwp, boxes, 1, seed=31, res=((w, h),), spps=(32,))[0]
+            r.sun_e[:] = (0.0, 0.0, 0.0); r.sky[:] = (0.0, 0.0, 0.0)
+            r.light_mode, r.rr, r.rr_depth, r.seed = mode, rr, 2, 1000 + seed
+            reqs.append(r)
+        vals = []
+        for acc, _ in run_all(s, reqs):
+            im = (acc[:, :3] / 32).reshape(h, w, 3).astype(np.float64)
+            L = 0.2126 * im[..., 0] + 0.7152 * im[..., 1] + 0.0722 * im[..., 2]
+            vals.append([L[j * h // gy:(j + 1) * h // gy, i * w // gx:(i + 1) * w // gx].mean() for j in range(gy) for i in range(gx)])
+        v = np.array(vals)
+        stats[name] = (v.mean(0), v.std(0, ddof=1) / np.sqrt(len(v)))
+    assert np.all(stats["mis"][0] > 0)
+    names = list(stats)
+    for i in range(len(names)):
+        for j in range(i + 1, len(names)):
+            (ma, sa), (mb, sb) = stats[names[i]], stats[names[j]]
+            z = np.abs(ma - mb) / np.sqrt(sa ** 2 + sb ** 2)
+            assert z.max() <= 3.0, (names[i], names[j], z.max())
+    assert np.median(stats["mis"][1] / stats["mis"][0]) < np.median(stats["bsdf"][1] / stats["bsdf"][0])
+    reqs = requests(cwp, boxes, 4, seed=37)
+    mix = run_all(s, reqs)
+    alone_s = cwp.Server(b, em, base, max_paths=1 << 15, max_requests=1)
+    alone_s.set_scenes(descs, first)
+    alone = run_all(alone_s, reqs)
+    for (am, sm), (aa, sa) in zip(mix, alone):
+        assert sm.rays == sa.rays and sm.shadow_rays == sa.shadow_rays
+        assert np.allclose(am, aa, rtol=1e-4, atol=1e-5)
+    with pytest.raises(cwp.CwpError):
+        bad = requests(cwp, boxes, 1, seed=3)[0]; bad.light_mode = 3
         s.submit(bad)
 
 
