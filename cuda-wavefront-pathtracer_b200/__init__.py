@@ -546,7 +546,8 @@ class Batch:
     """Batched form: many meshes built on the GPU at once (segmented H-PLOC, BVH2 / BVH4 / CWBVH encodings), many
     two-level scenes, one persistent launch over a scene-tagged ray queue, and the launch-shape autotuner."""
 
-    def __init__(self, meshes, device=0, leaf=4, widths=0, builder=0, spatial=0.0, tlas_width=4):
+    def __init__(self, meshes, device=0, leaf=4, widths=0, builder=0, spatial=0.0, tlas_width=4, normals=None):
+        """normals: per mesh, vertex normals [n_verts, 3] or None (the serving integrator's shading normals)"""
         arrs, views = [], (MeshView * len(meshes))()
         for i, m in enumerate(meshes):
             v, f, fm, _ = m.arrays() if isinstance(m, Mesh) else m
@@ -554,6 +555,9 @@ class Batch:
             fm = np.ascontiguousarray(fm if fm is not None else np.zeros(len(f)), np.int32)
             arrs += [v, f, fm]
             views[i].verts, views[i].n_verts, views[i].faces, views[i].n_tris, views[i].face_mat = _fptr(v), len(v), _iptr(f), len(f), _iptr(fm)
+            if normals is not None and normals[i] is not None:
+                nv = np.ascontiguousarray(normals[i], np.float32).reshape(len(v), 3); arrs.append(nv)
+                views[i].normals = _fptr(nv)
         o = BatchOptions(device, leaf, widths, builder, spatial, tlas_width)
         h = C.c_void_p()
         _check(lib().cwp_batch_create(views, len(meshes), C.byref(o), C.byref(h)))

@@ -215,6 +215,7 @@ struct cwp_batch {
     int nMesh = 0; int64_t nTris = 0;
     std::vector<int> meshFirst;          // nMesh + 1 triangle offsets
     float4* triV = nullptr;              // input triangles, 3 float4 each
+    float4* nrm = nullptr;               // corner normals, 3 float4 per triangle in mesh order (zero for meshes without), or null
     float4 *primLo = nullptr, *primHi = nullptr, *meshBox = nullptr;
     int* meshFirstDev = nullptr;
     int* meshRoot[3] = { nullptr, nullptr, nullptr }; std::vector<int> meshRootHost[3];   // per layout width
@@ -247,7 +248,7 @@ static void batch_free(cwp_batch* b) {
     cudaSetDevice(b->device);
     for (auto& l : b->lay) free_wide(l);
     b->blasB.release(); b->tlasB.release();
-    cudaFree(b->triV); cudaFree(b->primLo); cudaFree(b->primHi); cudaFree(b->meshBox); cudaFree(b->meshFirstDev);
+    cudaFree(b->triV); cudaFree(b->nrm); cudaFree(b->primLo); cudaFree(b->primHi); cudaFree(b->meshBox); cudaFree(b->meshFirstDev);
     cudaFree(b->inst); cudaFree(b->instLo); cudaFree(b->instHi); cudaFree(b->tlas); cudaFree(b->tlas4); cudaFree(b->sceneRoot); cudaFree(b->segFirstTlas);
     cudaFree(b->uInst); cudaFree(b->uLo); cudaFree(b->uHi); cudaFree(b->dstFirstTlas);
     cudaFree(b->err); cudaFree(b->cursor);
@@ -366,8 +367,25 @@ static int batch_create(const cwp_mesh_view* meshes, int32_t n, const cwp_batch_
             memcpy(&o[0].w, &id, 4); memcpy(&o[1].w, &mat, 4);
         }
     }
+    // corner normals of the meshes that have them (shading normals of the serving integrator)
+    std::vector<float4> nr;
+    for (int m = 0; m < n; m++) {
+        const cwp_mesh_view& v = meshes[m];
+        if (!v.normals) continue;
+        if (nr.empty()) nr.assign((size_t)3 * b->nTris, make_float4(0.f, 0.f, 0.f, 0.f));
+        for (int64_t t = 0; t < v.n_tris; t++)
+            for (int k = 0; k < 3; k++) {
+                const float* q = v.normals + 3 * (size_t)v.faces[3 * t + k];
+                CWPB_CHECK(std::isfinite(q[0]) && std::isfinite(q[1]) && std::isfinite(q[2]), CWP_ERR_INVALID, "mesh %d: non-finite normal", m);
+                nr[(size_t)3 * (b->meshFirst[m] + t) + k] = make_float4(q[0], q[1], q[2], 0.f);
+            }
+    }
     CWPB_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
     CWPB_CUDA(cudaEventCreate(&b->e0)); CWPB_CUDA(cudaEventCreate(&b->e1));
+    if (!nr.empty()) {
+        CWPB_CUDA(cudaMalloc(&b->nrm, nr.size() * sizeof(float4)));
+        CWPB_CUDA(cudaMemcpy(b->nrm, nr.data(), nr.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    }
     CWPB_CUDA(cudaMalloc(&b->err, sizeof(int))); CWPB_CUDA(cudaMemset(b->err, 0, sizeof(int)));
     CWPB_CUDA(cudaMalloc(&b->cursor, sizeof(unsigned long long)));
     CWPB_CUDA(cudaMalloc(&b->triV, soup.size() * sizeof(float4)));
@@ -752,6 +770,7 @@ int batch_mesh_count(const cwp_batch* b) { return b->nMesh; }
 const int* batch_mesh_first(const cwp_batch* b) { return b->meshFirstDev; }
 int64_t batch_tri_count(const cwp_batch* b) { return b->nTris; }
 const float4* batch_tri_soup(const cwp_batch* b) { return b->triV; }
+const float4* batch_normals(const cwp_batch* b) { return b->nrm; }
 const int* batch_mesh_first_host(const cwp_batch* b) { return b->meshFirst.data(); }
 int batch_device(const cwp_batch* b) { return b->device; }
 }  // namespace cwpb

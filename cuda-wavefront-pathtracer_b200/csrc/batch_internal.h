@@ -17,4 +17,5 @@ const int* batch_mesh_first(const cwp_batch* b);       // device: nMesh + 1 offs
 int64_t batch_tri_count(const cwp_batch* b);            // triangles of all meshes
 const float4* batch_tri_soup(const cwp_batch* b);     // device: the input triangles, (v0, face id), (v1, face material), (v2, 0) in mesh order
 const int* batch_mesh_first_host(const cwp_batch* b);  // host: nMesh + 1 offsets
+const float4* batch_normals(const cwp_batch* b);      // device: corner normals, 3 float4 per triangle in mesh order, or null
 }  // namespace cwpb

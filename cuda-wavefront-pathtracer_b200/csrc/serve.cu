@@ -126,6 +126,7 @@ struct ShadeArgs {
     // material textures (mtex null: none): texture objects, bindings per material, per-triangle uvs / tangents by
     // mesh-local index from each mesh's first triangle
     const cudaTextureObject_t* texObj; const cwp_material_textures* mtex; int nMtex; const float4* uvs; const float4* tans; const int* meshFirst;
+    const float4* nrm;   // corner normals by global triangle id (3 float4 each), or null: flat shading
     int* cnt;          // [0] next queue length, [1] shadow queue length
     int* slotCnt;      // kSlotCounters per slot
 };
@@ -237,6 +238,16 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                 const int mid = min(max(__ldg(a.meshMat + I.mesh) + __float_as_int(e1.w), 0), a.nMats - 1);
                 cwp_material M = a.mats[mid];
                 float3 nsw = ng0;   // shading normal before orientation
+                if (a.nrm) {   // interpolated corner normals by the inverse transpose, turned to the geometric normal's side
+                    const int64_t t = (int64_t)__ldg(a.meshFirst + I.mesh) + __float_as_int(__ldg(a.tris + 3 * (size_t)tri).w);
+                    const float4 n0 = __ldg(a.nrm + 3 * t), n1 = __ldg(a.nrm + 3 * t + 1), n2 = __ldg(a.nrm + 3 * t + 2);
+                    const float3 nn = f3(n0.x, n0.y, n0.z) * (1.f - H.y - H.z) + f3(n1.x, n1.y, n1.z) * H.y + f3(n2.x, n2.y, n2.z) * H.z;
+                    const float3 nt = f3(I.inv[0] * nn.x + I.inv[4] * nn.y + I.inv[8] * nn.z, I.inv[1] * nn.x + I.inv[5] * nn.y + I.inv[9] * nn.z,
+                                         I.inv[2] * nn.x + I.inv[6] * nn.y + I.inv[10] * nn.z);
+                    const float l = length(nt);
+                    if (l > 0.f) nsw = nt * (1.f / l);
+                    if (dot(nsw, ng0) < 0.f) nsw = -nsw;
+                }
                 apply_textures(a, mid, I, tri, H.y, H.z, M, nsw);
                 const float3 p = f3(O.x, O.y, O.z) + d * H.x;
                 const float3 em = mat_v3(M.emission);
@@ -857,6 +868,7 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         a.n = (int)n; a.in = in; a.out = out; a.sq = s->sq; a.hits = s->hits; a.hinst = s->hinst; a.inst = batch_instances(s->batch); a.tris = batch_tris(s->batch);
         a.mats = s->mats; a.nMats = s->nMats; a.meshMat = s->meshMat; a.slots = s->dSlots; a.gdEnergy = s->O.gd_energy; a.cnt = s->cnt; a.slotCnt = s->slotCnt;
         a.texObj = s->dTexObj; a.mtex = s->nMtex ? s->dMtex : nullptr; a.nMtex = s->nMtex; a.uvs = s->dUvs; a.tans = s->dTans; a.meshFirst = batch_mesh_first(s->batch);
+        a.nrm = batch_normals(s->batch);
         const unsigned g = (unsigned)std::min<int64_t>((n + 127) / 128, 148 * 16);
         k_serve_shade<<<g, 128, 0, s->st>>>(a);
         CWPB_CUDA(cudaGetLastError());

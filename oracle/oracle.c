@@ -1111,7 +1111,7 @@ long orc_emissive_tables(const float* soup, const int* mesh_first, int n_mesh, c
                          const float* xf, const int* inst_mesh, long n_inst, float* em_tris, float* em_cdf, float* mat_pdf) {
     const OMat* M = (const OMat*)mats;
     long n = 0; double tot = 0.0;
-    double* pw = NULL; long cap = 0;
+    double* pw = NULL; float* rec = NULL; long cap = 0;   /* records staged here: the caller's array holds only what is returned */
     for (long i = 0; i < n_inst; i++) {
         const float* m = xf + 12 * i; const int mesh = inst_mesh[i];
         for (int g = mesh_first[mesh]; g < mesh_first[mesh + 1]; g++) {
@@ -1125,10 +1125,10 @@ long orc_emissive_tables(const float* soup, const int* mesh_first, int n_mesh, c
             const V3 cr = cross3(e1, e2);
             const double area = 0.5 * sqrtf(dot3(cr, cr));
             double pwr = o_lum(v3(M[mid].emission[0], M[mid].emission[1], M[mid].emission[2])) * area; pwr = pwr > 0 ? pwr : 0;
-            if (n == cap) { cap = cap ? 2 * cap : 256; pw = (double*)realloc(pw, sizeof(double) * (size_t)cap); }
+            if (n == cap) { cap = cap ? 2 * cap : 256; pw = (double*)realloc(pw, sizeof(double) * (size_t)cap); rec = (float*)realloc(rec, sizeof(float) * 12 * (size_t)cap); }
             pw[n] = pwr; tot += pwr;
-            if (em_tris) {
-                float* t = em_tris + 12 * (size_t)n;
+            {
+                float* t = rec + 12 * (size_t)n;
                 t[0] = w[0][0]; t[1] = w[0][1]; t[2] = w[0][2]; memcpy(&t[3], &g, 4);
                 t[4] = e1.x; t[5] = e1.y; t[6] = e1.z; memcpy(&t[7], &mid, 4);
                 t[8] = e2.x; t[9] = e2.y; t[10] = e2.z; t[11] = 0.f;
@@ -1140,6 +1140,7 @@ long orc_emissive_tables(const float* soup, const int* mesh_first, int n_mesh, c
     if (em_tris) {
         for (int j = 0; j < n_mats; j++) mat_pdf[j] = 0.f;
         if (n) {
+            memcpy(em_tris, rec, sizeof(float) * 12 * (size_t)n);
             double c = 0.0; em_cdf[0] = 0.f;
             for (long e = 0; e < n; e++) { c += pw[e]; em_cdf[e + 1] = (float)(c / tot); }
             em_cdf[n] = 1.f;
@@ -1147,7 +1148,7 @@ long orc_emissive_tables(const float* soup, const int* mesh_first, int n_mesh, c
                 if (M[j].emission[0] > 0.f || M[j].emission[1] > 0.f || M[j].emission[2] > 0.f) mat_pdf[j] = (float)(o_lum(v3(M[j].emission[0], M[j].emission[1], M[j].emission[2])) / tot);
         }
     }
-    free(pw);
+    free(pw); free(rec);
     return n;
 }
 
@@ -1232,7 +1233,7 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
                         const float* mats, int n_mats, const int* mesh_mat, int gd, long j0, long j1, float* accum, long long* counts,
                         const float* env_tex, const float* env_marg, const float* env_cond, int env_w, int env_h,
                         const void* tex, const void* mtex, int n_mtex, const float* uvs, const float* tans, const int* mesh_first,
-                        const float* em_tris, const float* em_cdf, const float* mat_pdf, long n_em) {
+                        const float* em_tris, const float* em_cdf, const float* mat_pdf, long n_em, const float* nrm) {
     const OTex* TX = (const OTex*)tex; const OMTex* MX = (const OMTex*)mtex;
     const OReq* R = (const OReq*)reqp; const OCam* C = &R->cam;
     const int N = C->w * C->h; long bad = 0;
@@ -1280,6 +1281,15 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
             int mid = mesh_mat[imesh] + fi(TR[3 * tri + 1].w); mid = mid < 0 ? 0 : mid >= n_mats ? n_mats - 1 : mid;
             OMat Mc = *(const OMat*)(mats + 16 * (size_t)mid); const OMat* M = &Mc;
             V3 nsw = ng0;
+            if (nrm) {   /* corner normals (12 floats per triangle in mesh order) by the inverse transpose (wavefront.cu:245-249) */
+                const float* n0 = nrm + 12 * ((size_t)mesh_first[imesh] + fi(TR[3 * tri].w));
+                const float w0 = 1.f - u - v;
+                const V3 nn = add(add(muls(v3(n0[0], n0[1], n0[2]), w0), muls(v3(n0[4], n0[5], n0[6]), u)), muls(v3(n0[8], n0[9], n0[10]), v));
+                const V3 nt = v3(I[0] * nn.x + I[4] * nn.y + I[8] * nn.z, I[1] * nn.x + I[5] * nn.y + I[9] * nn.z, I[2] * nn.x + I[6] * nn.y + I[10] * nn.z);
+                const float l = sqrtf(dot3(nt, nt));
+                if (l > 0.f) nsw = muls(nt, 1.f / l);
+                if (dot3(nsw, ng0) < 0.f) nsw = neg(nsw);
+            }
             if (MX && mid < n_mtex && (MX[mid].base_color >= 0 || MX[mid].emission >= 0 || MX[mid].normal >= 0 || MX[mid].metallic >= 0 || MX[mid].roughness >= 0)) {
                 const OMTex X = MX[mid];
                 const long ti = (long)mesh_first[imesh] + fi(TR[3 * tri].w);

@@ -59,7 +59,7 @@ def _load_oracle():
     L.orc_render_stats.argtypes = [C.c_int, C.c_void_p]
     L.orc_render_request.restype = C.c_long
     L.orc_render_request.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
-                                     + [C.c_void_p] * 3 + [C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3 + [C.c_void_p] * 3 + [C.c_long])
+                                     + [C.c_void_p] * 3 + [C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3 + [C.c_void_p] * 3 + [C.c_long, C.c_void_p])
     L.orc_emissive_tables.restype = C.c_long
     L.orc_emissive_tables.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_long] + [C.c_void_p] * 3
     L.orc_texture_sample.restype = None
@@ -188,25 +188,29 @@ class Oracle:
         return out
 
     def render_request(self, req, width, blas, tris, tlas, root, inst, mats, mesh_mat, gd=1, paths=None, tlas_width=2, env=None, textures=None,
-                       lights=None):
+                       lights=None, normals=None):
         """A serving request on the host: (accum [w h, 4], counts [2]). env: (texels, marg, cond) of the request's
         environment map when Request.env >= 0, else None. textures: (cwp_texture array, cwp_material_textures array,
         uvs, tans or None, mesh_first) as given to the server, else None. lights: (em_tris, em_cdf, mat_pdf) of the
-        request's scene at its frame (emissive_tables), else None."""
+        request's scene at its frame (emissive_tables), else None. normals: (corner normals [n_tris, 12] in mesh
+        order, mesh_first) when the batch's meshes have normals, else None."""
         n = req.cam.w * req.cam.h * req.spp
         j0, j1 = (0, n) if paths is None else paths
         acc = np.zeros((req.cam.w * req.cam.h, 4), np.float32); cnt = np.zeros(2, np.int64)
         a = [np.ascontiguousarray(x) for x in (blas, tris, tlas)]
         ins = np.ascontiguousarray(inst, np.float32); ms = np.ascontiguousarray(mats, np.float32); mm = np.ascontiguousarray(mesh_mat, np.int32)
+        nr = np.ascontiguousarray(normals[0], np.float32) if normals is not None else None
+        mf = np.ascontiguousarray(normals[1], np.int32) if normals is not None else None
         bad = self.L.orc_render_request(C.addressof(req), width, tlas_width, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, int(root), ins.ctypes.data,
                                         ms.ctypes.data, len(ms), mm.ctypes.data, gd, j0, j1, acc.ctypes.data, cnt.ctypes.data,
                                         *((env[0].ctypes.data, env[1].ctypes.data, env[2].ctypes.data, env[0].shape[1], env[0].shape[0]) if env is not None
                                           else (None, None, None, 0, 0)),
                                         *((C.addressof(textures[0]), C.addressof(textures[1]), len(textures[1]), textures[2].ctypes.data,
                                            textures[3].ctypes.data if textures[3] is not None else None, textures[4].ctypes.data) if textures is not None
-                                          else (None, None, 0, None, None, None)),
+                                          else (None, None, 0, None, None, mf.ctypes.data if mf is not None else None)),
                                         *((lights[0].ctypes.data, lights[1].ctypes.data, lights[2].ctypes.data, len(lights[0])) if lights is not None and len(lights[0])
-                                          else (None, None, None, 0)))
+                                          else (None, None, None, 0)),
+                                        nr.ctypes.data if nr is not None else None)
         assert bad == 0
         return acc, cnt
 

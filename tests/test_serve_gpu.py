@@ -235,6 +235,60 @@ def test_light_modes_agree_and_requests_keep_their_lights(gpu, cwp, serving):
         s.submit(bad)
 
 
+def vertex_normals(meshes, seed=3):
+    """per-vertex normals for the box-field meshes: the direction from the mesh's centre, tilted at random (every
+    second mesh keeps flat shading: None)"""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k, (v, f, fm, _) in enumerate(meshes):
+        if k % 2:
+            out.append(None); continue
+        n = v - v.mean(0) + rng.normal(0, 0.3, v.shape)
+        out.append((n / np.linalg.norm(n, axis=1, keepdims=True)).astype(np.float32))
+    return out
+
+
+def mesh_order_normals(meshes, normals):
+    """corner normals [n_tris, 12] in mesh order (zero for meshes without) and each mesh's first triangle"""
+    rows, first = [], [0]
+    for (v, f, fm, _), n in zip(meshes, normals):
+        r = np.zeros((len(f), 12), np.float32)
+        if n is not None:
+            r[:, 0:3], r[:, 4:7], r[:, 8:11] = n[f[:, 0]], n[f[:, 1]], n[f[:, 2]]
+        rows.append(r); first.append(first[-1] + len(f))
+    return np.concatenate(rows), np.array(first, np.int32)
+
+
+def test_smooth_normals_request_matches_oracle(gpu, cwp, oracle):
+    """Meshes with vertex normals (every second one; the others flat): the shading normal interpolates the corner
+    normals, maps them by the instance's inverse transpose and turns them to the geometric normal's side; with
+    emissive boxes and an environment map the request's image matches the oracle at >= 45 dB."""
+    meshes, descs, first, mats, base, boxes = cwp.serving_scenes(n_scenes=2, seed=6, tris=(200, 3000), instances=(2, 12), blas_per_scene=(2, 3))
+    nrm = vertex_normals(meshes)
+    b = cwp.Batch(meshes, normals=nrm)
+    em = _emissive(mats, base)
+    s = cwp.Server(b, em, base, max_paths=1 << 16, max_requests=2)
+    s.set_scenes(descs, first)
+    g = golden("env.npz")
+    s.set_envmaps([(g["big_rgb"], 1.0)])
+    req = requests(cwp, boxes, 1, seed=43, res=((64, 48),), spps=(4,))[0]
+    req.env = 0
+    (acc, st), = run_all(s, [req])
+    nodes, tris = b.download(b.tuning().width)
+    tlas, roots, inst = b.download_tlas(2, _n_inst(b, 2))
+    lights = cwp.emissive_tables(meshes, base, em, *cwp.scene_xforms(descs, first, req.scene, req.frame))
+    ref, cnt = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, em, base, tlas_width=b.tlas_width,
+                                     env=cwp.envmap_build(g["big_rgb"], 1.0), lights=lights, normals=mesh_order_normals(meshes, nrm))
+    a = acc[:, :3] / req.spp; r = ref[:, :3] / req.spp
+    assert cwp.imageio.psnr(a, r) >= 45.0
+    assert abs(st.rays - cnt[0]) <= 2e-3 * cnt[0] and abs(st.shadow_rays - cnt[1]) <= 2e-3 * max(cnt[1], 1)
+    # the normals change the image against flat shading of the same paths
+    flat = cwp.Batch(meshes)
+    sf = cwp.Server(flat, em, base, max_paths=1 << 16, max_requests=2); sf.set_scenes(descs, first); sf.set_envmaps([(g["big_rgb"], 1.0)])
+    (acc_flat, _), = run_all(sf, [req])
+    assert not np.allclose(acc, acc_flat)
+
+
 def test_texture_lookups_match_oracle(gpu, cwp, oracle):
     """Hardware bilinear lookups (wrap, normalised coordinates, sRGB decode for colour images) against the oracle's
     restatement of the documented filtering rule, over odd image sizes and coordinates wrapping over several periods.
