@@ -115,7 +115,7 @@ class Request(C.Structure):
     _fields_ = [("scene", C.c_int32), ("frame", C.c_int32), ("cam", Camera), ("spp", C.c_int32), ("max_depth", C.c_int32), ("seed", C.c_uint32),
                 ("sun_to", C.c_float * 3), ("sun_e", C.c_float * 3), ("sky", C.c_float * 3), ("sun_cos", C.c_float), ("eps", C.c_float),
                 ("env", C.c_int32), ("env_rot_deg", C.c_float),
-                ("light_mode", C.c_int32), ("rr", C.c_int32), ("rr_depth", C.c_int32), ("env_uniform", C.c_int32)]
+                ("light_mode", C.c_int32), ("rr", C.c_int32), ("rr_depth", C.c_int32), ("env_uniform", C.c_int32), ("bump_shadow", C.c_int32)]
 
 
 LIGHT_MIS, LIGHT_NEE, LIGHT_BSDF = 0, 1, 2
@@ -243,8 +243,8 @@ SIGNATURES = {
     "cwp_server_result": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.POINTER(RequestStats)]),
     "cwp_server_clock_ms": (C.c_double, [C.c_void_p]),
     "cwp_server_info_of": (C.c_int, [C.c_void_p, C.POINTER(ServerInfo)]),
-    "cwp_bsdf_eval_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 4 + [C.c_int32] + [C.c_void_p] * 3 + [C.c_int64]),
-    "cwp_bsdf_sample_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 3 + [C.c_int32] + [C.c_void_p] * 6 + [C.c_int64]),
+    "cwp_bsdf_eval_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 4 + [C.c_int32] + [C.c_void_p] * 3 + [C.c_int64, C.c_void_p]),
+    "cwp_bsdf_sample_batch": (C.c_int, [C.POINTER(Material), C.c_int32] + [C.c_void_p] * 3 + [C.c_int32] + [C.c_void_p] * 6 + [C.c_int64, C.c_void_p]),
     "cwp_display": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_float, C.c_int32, C.c_void_p]),
     "cwp_measure_l2_read": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "cwp_camera_look_at": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32, C.POINTER(Camera)]),
@@ -641,23 +641,26 @@ def materials_array(m):
     return arr
 
 
-def bsdf_eval_batch(mats, mat, wo, wi, eta, gd, ux):
-    """Device BSDF values for (material index, wo, wi) triples in local frames: (f [n, 3], pdf [n])."""
+def bsdf_eval_batch(mats, mat, wo, wi, eta, gd, ux, nr=None):
+    """Device BSDF values for (material index, wo, wi) triples in local frames: (f [n, 3], pdf [n]); nr: unperturbed
+    normals [n, 3] for the bump-terminator term, or None"""
     M = materials_array(mats); n = len(mat)
     a = [np.ascontiguousarray(x, t) for x, t in ((mat, np.int32), (wo, np.float32), (wi, np.float32), (eta, np.float32), (ux, np.float32))]
+    nr = np.ascontiguousarray(nr, np.float32) if nr is not None else None
     f = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32)
     _check(lib().cwp_bsdf_eval_batch(M, len(M), a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, gd, a[4].ctypes.data,
-                                     f.ctypes.data, pdf.ctypes.data, n))
+                                     f.ctypes.data, pdf.ctypes.data, n, nr.ctypes.data if nr is not None else None))
     return f, pdf
 
 
-def bsdf_sample_batch(mats, mat, wo, eta, gd, ux, uvw):
+def bsdf_sample_batch(mats, mat, wo, eta, gd, ux, uvw, nr=None):
     """Device BSDF samples: (wi [n, 3], weight [n, 3], pdf [n], ok [n])."""
     M = materials_array(mats); n = len(mat)
     a = [np.ascontiguousarray(x, t) for x, t in ((mat, np.int32), (wo, np.float32), (eta, np.float32), (ux, np.float32), (uvw, np.float32))]
+    nr = np.ascontiguousarray(nr, np.float32) if nr is not None else None
     wi = np.zeros((n, 3), np.float32); w = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32); ok = np.zeros(n, np.int32)
     _check(lib().cwp_bsdf_sample_batch(M, len(M), a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, gd, a[3].ctypes.data, a[4].ctypes.data,
-                                       wi.ctypes.data, w.ctypes.data, pdf.ctypes.data, ok.ctypes.data, n))
+                                       wi.ctypes.data, w.ctypes.data, pdf.ctypes.data, ok.ctypes.data, n, nr.ctypes.data if nr is not None else None))
     return wi, w, pdf, ok
 
 
@@ -679,7 +682,7 @@ def envmap_build(rgb, strength=1.0):
 
 
 def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun_e=None, sky=None, sun_angle_rad=None, eps=1e-3, env=-1, env_rot_deg=0.0,
-                 light_mode=LIGHT_MIS, rr=0, rr_depth=3, env_uniform=0):
+                 light_mode=LIGHT_MIS, rr=0, rr_depth=3, env_uniform=0, bump_shadow=0):
     """A serving request; lighting defaults to the benchmark's sun and sky (env = -1) or names one of the server's
     environment maps; emissive materials of the scene are light-sampled too (light_mode, as the reference's
     --light_sampling mis / nee / bsdf); rr / rr_depth: Russian roulette (--rr, --rr_depth)."""
@@ -692,7 +695,7 @@ def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun
     r.sun_to[:] = tuple(float(x) for x in s); r.sun_e[:] = tuple(sun_e); r.sky[:] = tuple(sky)
     r.sun_cos = float(np.float32(math.cos(sun_angle_rad / 2.0))); r.eps = eps
     r.env, r.env_rot_deg = env, env_rot_deg
-    r.light_mode, r.rr, r.rr_depth, r.env_uniform = light_mode, rr, rr_depth, env_uniform
+    r.light_mode, r.rr, r.rr_depth, r.env_uniform, r.bump_shadow = light_mode, rr, rr_depth, env_uniform, bump_shadow
     return r
 
 

@@ -81,8 +81,19 @@ struct BsdfValue { float3 f; float pdf; };
 // ---- glossy-diffuse base: GGX dielectric specular (weight ws, ior) + Lambertian base colour weighted by kd ----
 // energy = 0: kd = 1 - ws F(wo.z). energy = 1: kd = 1 - X with X = ws F(wo.m) G2 / G1(wo) for one visible normal m
 // drawn from (ux1, ux2), an unbiased estimate of the specular lobe's directional albedo. Lobe choice uses F(wo.z).
+// bump-terminator shadowing of the diffuse lobe (Chiang, Li, Burley, "Taming the Shadow Terminator", SIGGRAPH 2019
+// talk): nr = the unperturbed normal in the frame of the mapped shading normal, g = (nr . wi) / (wi.z nr.z), G = g +
+// g^2 - g^3 on [0, 1), 1 above, 0 below; nr = +z gives G = 1 exactly (the term off)
+CWPB_HD float bump_shadowing(float3 nr, float3 wi) {
+    if (nr.z >= 1.f) return 1.f;
+    const float g = dot(nr, wi) / (wi.z * nr.z);
+    if (g >= 1.f) return 1.f;
+    if (g < 0.f) return 0.f;
+    return g + g * g - g * g * g;
+}
+
 struct GlossyDiffuseLobe {
-    float3 base; float ws, eta, a, a2, Fo, pSpec, kd; bool delta;
+    float3 base; float ws, eta, a, a2, Fo, pSpec, kd; bool delta; float3 nr = f3(0.f, 0.f, 1.f);
     CWPB_HD GlossyDiffuseLobe(const cwp_material& m, float3 wo, int energy, float ux1, float ux2) {
         base = mat_v3(m.base_color); ws = m.specular_weight; eta = m.ior; a = m.roughness * m.roughness; a2 = a * a; delta = a < kDeltaAlpha;
         Fo = ws > 0.f ? ws * fresnel_dielectric(wo.z, eta) : 0.f;
@@ -101,7 +112,7 @@ struct GlossyDiffuseLobe {
     CWPB_HD BsdfValue eval(float3 wo, float3 wi) const {
         BsdfValue r{ f3(0.f, 0.f, 0.f), 0.f };
         if (wi.z <= 0.f) return r;
-        r.f = base * (kd * CWPB_INV_PI); r.pdf = (1.f - pSpec) * wi.z * CWPB_INV_PI;
+        r.f = base * (kd * CWPB_INV_PI * bump_shadowing(nr, wi)); r.pdf = (1.f - pSpec) * wi.z * CWPB_INV_PI;
         if (!delta && Fo > 0.f) {
             const float3 m = normalize(wo + wi); const float om = dot(wo, m);
             if (om > 0.f) {
@@ -208,26 +219,27 @@ CWPB_HD bool has_non_delta(const cwp_material& m) {
     const bool rough = m.roughness * m.roughness >= kDeltaAlpha;
     return (wD > 0.f && (luminance(mat_v3(m.base_color)) > 0.f || rough)) || ((wM > 0.f || wT > 0.f) && rough);
 }
-CWPB_HD BsdfValue bsdf_eval(const cwp_material& m, float3 wo, float3 wi, float etaRel, int gdEnergy, float ux1, float ux2) {
+// nr: the unperturbed normal for the bump-terminator term, +z = off
+CWPB_HD BsdfValue bsdf_eval(const cwp_material& m, float3 wo, float3 wi, float etaRel, int gdEnergy, float ux1, float ux2, float3 nr = f3(0.f, 0.f, 1.f)) {
     float wM, wT, wD; base_weights(m, wM, wT, wD);
     BsdfValue r{ f3(0.f, 0.f, 0.f), 0.f };
     if (wM > 0.f) { const BsdfValue e = ConductorLobe(m).eval(wo, wi); r.f = r.f + e.f * wM; r.pdf += wM * e.pdf; }
     if (wT > 0.f) { const BsdfValue e = DielectricLobe(m, etaRel).eval(wo, wi); r.f = r.f + e.f * wT; r.pdf += wT * e.pdf; }
-    if (wD > 0.f) { const BsdfValue e = GlossyDiffuseLobe(m, wo, gdEnergy, ux1, ux2).eval(wo, wi); r.f = r.f + e.f * wD; r.pdf += wD * e.pdf; }
+    if (wD > 0.f) { GlossyDiffuseLobe g(m, wo, gdEnergy, ux1, ux2); g.nr = nr; const BsdfValue e = g.eval(wo, wi); r.f = r.f + e.f * wD; r.pdf += wD * e.pdf; }
     return r;
 }
 // one base chosen by u (one-sample MIS over the bases); weight of the whole material, pdf 0 for delta samples
 CWPB_HD bool bsdf_sample(const cwp_material& m, float3 wo, float etaRel, int gdEnergy, float ux1, float ux2, float u, float u1, float u2,
-                         float3& wi, float3& weight, float& pdf) {
+                         float3& wi, float3& weight, float& pdf, float3 nr = f3(0.f, 0.f, 1.f)) {
     float wM, wT, wD; base_weights(m, wM, wT, wD);
     bool ok;
     if (u < wM) ok = ConductorLobe(m).sample(wo, u1, u2, wi, weight, pdf);
     else if (u < wM + wT) ok = DielectricLobe(m, etaRel).sample(wo, fminf((u - wM) / wT, 0.99999994f), u1, u2, wi, weight, pdf);
-    else ok = GlossyDiffuseLobe(m, wo, gdEnergy, ux1, ux2).sample(wo, fminf(wD > 0.f ? (u - wM - wT) / wD : 0.f, 0.99999994f), u1, u2, wi, weight, pdf);
+    else { GlossyDiffuseLobe g(m, wo, gdEnergy, ux1, ux2); g.nr = nr; ok = g.sample(wo, fminf(wD > 0.f ? (u - wM - wT) / wD : 0.f, 0.99999994f), u1, u2, wi, weight, pdf); }
     if (!ok) return false;
     if (pdf <= 0.f) return true;                          // a delta sample: no other base has density there
     if (wM == 1.f || wT == 1.f || wD == 1.f) return true;  // one base: its own weight is already f |cos| / pdf
-    const BsdfValue e = bsdf_eval(m, wo, wi, etaRel, gdEnergy, ux1, ux2);
+    const BsdfValue e = bsdf_eval(m, wo, wi, etaRel, gdEnergy, ux1, ux2, nr);
     if (e.pdf <= 0.f) return false;
     weight = e.f * (fabsf(wi.z) / e.pdf); pdf = e.pdf;
     return true;

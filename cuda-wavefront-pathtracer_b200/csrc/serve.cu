@@ -39,7 +39,7 @@ struct SlotParams {
     const float4* envTex; const float* envMarg; const float* envCond; int envW, envH; float envRot;
     // light sampling: light-type probabilities, mode (CWP_LIGHT_*), Russian roulette, uniform environment samples; the
     // scene's emissive triangles at the request's frame (nEm = 0: none): 3 float4 each, power CDF, area density by material
-    float pSun, pTri, pEnv; int lightMode, rr, rrDepth, envUniform, nEm;
+    float pSun, pTri, pEnv; int lightMode, rr, rrDepth, envUniform, nEm, bumpShadow;
     const float4* emTris; const float* emCdf; const float* matPdf;
 };
 
@@ -169,10 +169,11 @@ __device__ __forceinline__ float3 xf_vec(const float* m, float3 v) {   // the li
 
 // The material of a hit with its textures applied (glTF semantics: the images multiply the factors), and the shading
 // normal ns (in: the geometric normal ng0; out: perturbed by a normal image in the corner tangents' frame).
-__device__ __forceinline__ void apply_textures(const ShadeArgs& a, int mid, const cwp_instance& I, int tri, float hu, float hv, cwp_material& M, float3& ns) {
-    if (!a.mtex || mid >= a.nMtex) return;
+// Returns whether a normal image perturbed ns.
+__device__ __forceinline__ bool apply_textures(const ShadeArgs& a, int mid, const cwp_instance& I, int tri, float hu, float hv, cwp_material& M, float3& ns) {
+    if (!a.mtex || mid >= a.nMtex) return false;
     const cwp_material_textures X = a.mtex[mid];
-    if (X.base_color < 0 && X.emission < 0 && X.normal < 0 && X.metallic < 0 && X.roughness < 0) return;
+    if (X.base_color < 0 && X.emission < 0 && X.normal < 0 && X.metallic < 0 && X.roughness < 0) return false;
     const int64_t t = (int64_t)__ldg(a.meshFirst + I.mesh) + __float_as_int(__ldg(a.tris + 3 * (size_t)tri).w);   // mesh-local triangle id
     const float2 uv = tri_uv(a.uvs, t, hu, hv);
     if (X.base_color >= 0) { const float4 c = tex_rgba(a.texObj[X.base_color], uv); M.base_color[0] *= c.x; M.base_color[1] *= c.y; M.base_color[2] *= c.z; }
@@ -193,9 +194,10 @@ __device__ __forceinline__ void apply_textures(const ShadeArgs& a, int mid, cons
             const float4 c = tex_rgba(a.texObj[X.normal], uv);
             const float3 nm = tg * ((2.f * c.x - 1.f) * X.normal_scale) + bt * ((2.f * c.y - 1.f) * X.normal_scale) + ns * (2.f * c.z - 1.f);
             const float nl = length(nm);
-            if (nl > 0.f) ns = nm * (1.f / nl);
+            if (nl > 0.f) { ns = nm * (1.f / nl); return true; }
         }
     }
+    return false;
 }
 
 __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
@@ -248,7 +250,8 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                     if (l > 0.f) nsw = nt * (1.f / l);
                     if (dot(nsw, ng0) < 0.f) nsw = -nsw;
                 }
-                apply_textures(a, mid, I, tri, H.y, H.z, M, nsw);
+                const float3 nsU = nsw;   // the normal before a normal image (the bump-terminator term)
+                const bool mapped = apply_textures(a, mid, I, tri, H.y, H.z, M, nsw);
                 const float3 p = f3(O.x, O.y, O.z) + d * H.x;
                 const float3 em = mat_v3(M.emission);
                 if (em.x > 0.f || em.y > 0.f || em.z > 0.f) {   // two-sided emission, weighted against light sampling of this triangle
@@ -277,6 +280,12 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                     if (dot(ns, wo) <= 1e-6f) ns = ng;
                     float3 tx, ty; frame_of(ns, tx, ty);
                     const float3 woL = f3(dot(wo, tx), dot(wo, ty), dot(wo, ns));
+                    float3 nrL = f3(0.f, 0.f, 1.f);   // the unperturbed normal in the shading frame: bump-terminator shadowing
+                    if (S.bumpShadow && mapped) {
+                        const float3 nu = front ? nsU : -nsU;
+                        nrL = f3(dot(nu, tx), dot(nu, ty), dot(nu, ns));
+                        if (!(nrL.z > 0.f)) nrL = f3(0.f, 0.f, 1.f);
+                    }
                     const float eta = front ? M.ior : 1.f / M.ior;
                     const float3 up = p + ng * S.eps, dn = p - ng * S.eps;
                     const unsigned dr = (unsigned)depth + 1u;
@@ -328,7 +337,7 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                         const float3 lL = f3(dot(l, tx), dot(l, ty), dot(l, ns));
                         const float gl = dot(ng, l);
                         if (ok && lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
-                            const BsdfValue e = bsdf_eval(M, woL, lL, eta, a.gdEnergy, ux1, ux2);
+                            const BsdfValue e = bsdf_eval(M, woL, lL, eta, a.gdEnergy, ux1, ux2, nrL);
                             const float w = (isSun || S.lightMode == CWP_LIGHT_NEE) ? 1.f : mis_power(pl, e.pdf);
                             contrib = T * e.f * Le * (fabsf(lL.z) * w / pl);
                             if (contrib.x > 0.f || contrib.y > 0.f || contrib.z > 0.f) {
@@ -337,7 +346,7 @@ __global__ void __launch_bounds__(128) k_serve_shade(const ShadeArgs a) {
                         }
                     }
                     float3 wiL, wgt; float pdf;
-                    if (bsdf_sample(M, woL, eta, a.gdEnergy, ux1, ux2, rnd_s(S.seed, pix, smp, dr, 4), rnd_s(S.seed, pix, smp, dr, 0), rnd_s(S.seed, pix, smp, dr, 1), wiL, wgt, pdf)) {
+                    if (bsdf_sample(M, woL, eta, a.gdEnergy, ux1, ux2, rnd_s(S.seed, pix, smp, dr, 4), rnd_s(S.seed, pix, smp, dr, 0), rnd_s(S.seed, pix, smp, dr, 1), wiL, wgt, pdf, nrL)) {
                         const float3 wi = normalize(tx * wiL.x + ty * wiL.y + ns * wiL.z);
                         const float gi = dot(ng, wi);
                         if (gi != 0.f && (gi > 0.f) == (wiL.z > 0.f)) {
@@ -409,18 +418,18 @@ __global__ void __launch_bounds__(256) k_slot_scatter(const int* __restrict__ nD
 
 // ---------------- BSDF test kernels ----------------
 __global__ void k_bsdf_eval(const cwp_material* mats, const int* mat, const float3* wo, const float3* wi, const float* eta, int gd, const float2* ux,
-                            float4* f, float* pdf, int64_t n) {
+                            const float3* nr, float4* f, float* pdf, int64_t n) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const BsdfValue e = bsdf_eval(mats[mat[i]], wo[i], wi[i], eta[i], gd, ux[i].x, ux[i].y);
+    const BsdfValue e = bsdf_eval(mats[mat[i]], wo[i], wi[i], eta[i], gd, ux[i].x, ux[i].y, nr ? nr[i] : f3(0.f, 0.f, 1.f));
     f[i] = make_float4(e.f.x, e.f.y, e.f.z, 0.f); pdf[i] = e.pdf;
 }
 __global__ void k_bsdf_sample(const cwp_material* mats, const int* mat, const float3* wo, const float* eta, int gd, const float2* ux, const float3* uvw,
-                              float3* wi, float3* w, float* pdf, int* ok, int64_t n) {
+                              const float3* nr, float3* wi, float3* w, float* pdf, int* ok, int64_t n) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float3 a = f3(0.f, 0.f, 0.f), b = a; float p = 0.f;
-    ok[i] = bsdf_sample(mats[mat[i]], wo[i], eta[i], gd, ux[i].x, ux[i].y, uvw[i].x, uvw[i].y, uvw[i].z, a, b, p) ? 1 : 0;
+    ok[i] = bsdf_sample(mats[mat[i]], wo[i], eta[i], gd, ux[i].x, ux[i].y, uvw[i].x, uvw[i].y, uvw[i].z, a, b, p, nr ? nr[i] : f3(0.f, 0.f, 1.f)) ? 1 : 0;
     wi[i] = a; w[i] = b; pdf[i] = p;
 }
 
@@ -704,8 +713,9 @@ extern "C" int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* i
     CWPB_CHECK(r->scene >= 0 && r->scene + 1 < (int)s->sceneFirst.size(), CWP_ERR_INVALID, "scene %d out of range", r->scene);
     CWPB_CHECK(r->env >= -1 && r->env < (int)s->envs.size(), CWP_ERR_INVALID, "environment map %d out of range (%d maps)", r->env, (int)s->envs.size());
     CWPB_CHECK(std::isfinite(r->env_rot_deg), CWP_ERR_INVALID, "environment rotation is not finite");
-    CWPB_CHECK(r->light_mode >= CWP_LIGHT_MIS && r->light_mode <= CWP_LIGHT_BSDF && (r->rr == 0 || r->rr == 1) && r->rr_depth >= 0 && (r->env_uniform == 0 || r->env_uniform == 1),
-               CWP_ERR_INVALID, "light mode %d, rr %d, rr_depth %d, env_uniform %d", r->light_mode, r->rr, r->rr_depth, r->env_uniform);
+    CWPB_CHECK(r->light_mode >= CWP_LIGHT_MIS && r->light_mode <= CWP_LIGHT_BSDF && (r->rr == 0 || r->rr == 1) && r->rr_depth >= 0 && (r->env_uniform == 0 || r->env_uniform == 1) &&
+               (r->bump_shadow == 0 || r->bump_shadow == 1),
+               CWP_ERR_INVALID, "light mode %d, rr %d, rr_depth %d, env_uniform %d, bump_shadow %d", r->light_mode, r->rr, r->rr_depth, r->env_uniform, r->bump_shadow);
     CWPB_CHECK(r->cam.w > 0 && r->cam.h > 0 && r->spp > 0 && r->max_depth >= 0 && r->max_depth <= 64, CWP_ERR_INVALID, "bad request size");
     const int64_t total = (int64_t)r->cam.w * r->cam.h * r->spp;
     CWPB_CHECK(total < (1ll << 31), CWP_ERR_INVALID, "%lld paths in one request (limit 2^31)", (long long)total);
@@ -802,7 +812,7 @@ static int admit(cwp_server* s, bool& changed) {
         const bool sunOn = sunL > 0.f, triOn = P.nEm > 0 && q.r.light_mode != CWP_LIGHT_BSDF, envOn = q.r.env >= 0 && q.r.light_mode != CWP_LIGHT_BSDF;
         const int nt = (int)sunOn + (int)triOn + (int)envOn;
         P.pSun = sunOn ? 1.f / nt : 0.f; P.pTri = triOn ? 1.f / nt : 0.f; P.pEnv = envOn ? 1.f / nt : 0.f;
-        P.lightMode = q.r.light_mode; P.rr = q.r.rr; P.rrDepth = q.r.rr_depth; P.envUniform = q.r.env_uniform;
+        P.lightMode = q.r.light_mode; P.rr = q.r.rr; P.rrDepth = q.r.rr_depth; P.envUniform = q.r.env_uniform; P.bumpShadow = q.r.bump_shadow;
         s->slotsDirty = true;
         CWPB_CUDA(cudaMemsetAsync(s->slotCnt + kSlotCounters * slot, 0, kSlotCounters * sizeof(int), s->st));
         q.slot = slot; q.admitMs = now_ms(s); s->info.admissions++; s->admitted.push_back(slot);
@@ -950,7 +960,7 @@ extern "C" int cwp_server_result(cwp_server* s, int64_t id, float* accum, cwp_re
 }
 
 extern "C" int cwp_bsdf_eval_batch(const cwp_material* mats, int32_t nm, const int32_t* mat, const float* wo, const float* wi, const float* eta, int32_t gd,
-                                   const float* ux, float* f, float* pdf, int64_t n) {
+                                   const float* ux, float* f, float* pdf, int64_t n, const float* nr) {
     CWPB_CHECK(mats && nm > 0 && mat && wo && wi && eta && ux && f && pdf && n >= 0, CWP_ERR_INVALID, "NULL argument");
     for (int64_t i = 0; i < n; i++) CWPB_CHECK(mat[i] >= 0 && mat[i] < nm, CWP_ERR_INVALID, "material index %d out of range", mat[i]);
     if (n == 0) return CWP_OK;
@@ -960,19 +970,21 @@ extern "C" int cwp_bsdf_eval_batch(const cwp_material* mats, int32_t nm, const i
     cudaMemcpy(dm, mats, nm * sizeof(cwp_material), cudaMemcpyHostToDevice); cudaMemcpy(dmat, mat, n * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(dwo, wo, n * 12, cudaMemcpyHostToDevice); cudaMemcpy(dwi, wi, n * 12, cudaMemcpyHostToDevice); cudaMemcpy(deta, eta, n * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(dux, ux, n * 8, cudaMemcpyHostToDevice);
-    k_bsdf_eval<<<(unsigned)((n + 127) / 128), 128>>>(dm, dmat, dwo, dwi, deta, gd, dux, df, dpdf, n);
+    float3* dnr = nullptr;
+    if (nr) { CWPB_CUDA(cudaMalloc(&dnr, n * 12)); cudaMemcpy(dnr, nr, n * 12, cudaMemcpyHostToDevice); }
+    k_bsdf_eval<<<(unsigned)((n + 127) / 128), 128>>>(dm, dmat, dwo, dwi, deta, gd, dux, dnr, df, dpdf, n);
     cudaError_t e = cudaGetLastError();
     std::vector<float4> hf(n);
     if (e == cudaSuccess) e = cudaMemcpy(hf.data(), df, n * 16, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(pdf, dpdf, n * 4, cudaMemcpyDeviceToHost);
     for (int64_t i = 0; i < n && e == cudaSuccess; i++) { f[3 * i] = hf[i].x; f[3 * i + 1] = hf[i].y; f[3 * i + 2] = hf[i].z; }
-    cudaFree(dm); cudaFree(dmat); cudaFree(dwo); cudaFree(dwi); cudaFree(deta); cudaFree(dux); cudaFree(df); cudaFree(dpdf);
+    cudaFree(dm); cudaFree(dmat); cudaFree(dwo); cudaFree(dwi); cudaFree(deta); cudaFree(dux); cudaFree(df); cudaFree(dpdf); cudaFree(dnr);
     CWPB_CUDA(e);
     return CWP_OK;
 }
 
 extern "C" int cwp_bsdf_sample_batch(const cwp_material* mats, int32_t nm, const int32_t* mat, const float* wo, const float* eta, int32_t gd, const float* ux,
-                                     const float* uvw, float* wi, float* weight, float* pdf, int32_t* ok, int64_t n) {
+                                     const float* uvw, float* wi, float* weight, float* pdf, int32_t* ok, int64_t n, const float* nr) {
     CWPB_CHECK(mats && nm > 0 && mat && wo && eta && ux && uvw && wi && weight && pdf && ok && n >= 0, CWP_ERR_INVALID, "NULL argument");
     for (int64_t i = 0; i < n; i++) CWPB_CHECK(mat[i] >= 0 && mat[i] < nm, CWP_ERR_INVALID, "material index %d out of range", mat[i]);
     if (n == 0) return CWP_OK;
@@ -983,13 +995,15 @@ extern "C" int cwp_bsdf_sample_batch(const cwp_material* mats, int32_t nm, const
     cudaMemcpy(dm, mats, nm * sizeof(cwp_material), cudaMemcpyHostToDevice); cudaMemcpy(dmat, mat, n * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(dwo, wo, n * 12, cudaMemcpyHostToDevice); cudaMemcpy(deta, eta, n * 4, cudaMemcpyHostToDevice); cudaMemcpy(dux, ux, n * 8, cudaMemcpyHostToDevice);
     cudaMemcpy(duvw, uvw, n * 12, cudaMemcpyHostToDevice);
-    k_bsdf_sample<<<(unsigned)((n + 127) / 128), 128>>>(dm, dmat, dwo, deta, gd, dux, duvw, dwi, dw, dpdf, dok, n);
+    float3* dnr = nullptr;
+    if (nr) { CWPB_CUDA(cudaMalloc(&dnr, n * 12)); cudaMemcpy(dnr, nr, n * 12, cudaMemcpyHostToDevice); }
+    k_bsdf_sample<<<(unsigned)((n + 127) / 128), 128>>>(dm, dmat, dwo, deta, gd, dux, duvw, dnr, dwi, dw, dpdf, dok, n);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpy(wi, dwi, n * 12, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(weight, dw, n * 12, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(pdf, dpdf, n * 4, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(ok, dok, n * 4, cudaMemcpyDeviceToHost);
-    cudaFree(dm); cudaFree(dmat); cudaFree(dwo); cudaFree(deta); cudaFree(dux); cudaFree(duvw); cudaFree(dwi); cudaFree(dw); cudaFree(dpdf); cudaFree(dok);
+    cudaFree(dm); cudaFree(dmat); cudaFree(dwo); cudaFree(deta); cudaFree(dux); cudaFree(duvw); cudaFree(dwi); cudaFree(dw); cudaFree(dpdf); cudaFree(dok); cudaFree(dnr);
     CWPB_CUDA(e);
     return CWP_OK;
 }

@@ -363,6 +363,8 @@ typedef struct cwp_request {
                               CWP_LIGHT_BSDF: only the sun is light-sampled */
     int32_t rr, rr_depth;  /* Russian roulette from depth rr_depth on (survival max(T) clamped to [0.05, 1]); rr = 0 off */
     int32_t env_uniform;   /* 1: environment light samples uniform on the sphere instead of by luminance */
+    int32_t bump_shadow;   /* 1: bump-terminator shadowing of the diffuse lobe where a normal image perturbed the normal
+                              (Chiang et al. 2019; the reference's --bump_shadow) */
 } cwp_request;
 #define CWP_LIGHT_MIS 0
 #define CWP_LIGHT_NEE 1
@@ -424,11 +426,12 @@ typedef struct cwp_server_info {
 } cwp_server_info;
 int cwp_server_info_of(const cwp_server* s, cwp_server_info* out);
 /* Device-side BSDF of a material table for n (material, wo, wi) triples in local frames (wo.z > 0): f (float4) and
- * pdf; and n samples (u, u1, u2 in uvw) -> wi, weight, pdf. For tests of the device arithmetic. */
+ * pdf; and n samples (u, u1, u2 in uvw) -> wi, weight, pdf. nr: an unperturbed normal per triple for the
+ * bump-terminator term (bsdfEval's nr, render/bsdf.h:196), or NULL (+z, off). For tests of the device arithmetic. */
 int cwp_bsdf_eval_batch(const cwp_material* mats, int32_t n_mats, const int32_t* mat, const float* wo, const float* wi, const float* eta,
-                        int32_t gd_energy, const float* ux, float* f, float* pdf, int64_t n);
+                        int32_t gd_energy, const float* ux, float* f, float* pdf, int64_t n, const float* nr);
 int cwp_bsdf_sample_batch(const cwp_material* mats, int32_t n_mats, const int32_t* mat, const float* wo, const float* eta, int32_t gd_energy,
-                          const float* ux, const float* uvw, float* wi, float* weight, float* pdf, int32_t* ok, int64_t n);
+                          const float* ux, const float* uvw, float* wi, float* weight, float* pdf, int32_t* ok, int64_t n, const float* nr);
 
 /* ------------------------------------------------------------------------------------------------------------------
  * Headless display transform. Replaces launchDisplay (app/display.cu, display.h:9) without the viewer's graphics

@@ -965,7 +965,17 @@ static V3 o_cos_dir(float u0, float u1) {   /* cosine hemisphere about +z (core/
 }
 typedef struct { V3 f; float pdf; } OEval;
 /* glossy-diffuse (bsdf.h:84-124) */
-typedef struct { V3 base; float ws, eta, a, a2, Fo, pSpec, kd; int delta; } OGd;
+typedef struct { V3 base; float ws, eta, a, a2, Fo, pSpec, kd; int delta; V3 nr; } OGd;
+/* bump-terminator shadowing of the diffuse lobe (Chiang, Li, Burley, SIGGRAPH 2019 talk; bsdf.h:67-75): nr = the
+ * unperturbed normal in the frame of the mapped shading normal, g = (nr . wi) / (wi.z nr.z), G = g + g^2 - g^3 on
+ * [0, 1), 1 above, 0 below; nr = +z: G = 1 */
+static float o_bump(V3 nr, V3 wi) {
+    if (nr.z >= 1.f) return 1.f;
+    const float g = dot3(nr, wi) / (wi.z * nr.z);
+    if (g >= 1.f) return 1.f;
+    if (g < 0.f) return 0.f;
+    return g + g * g - g * g * g;
+}
 static OGd o_gd(const OMat* m, V3 wo, int energy, float ux1, float ux2) {
     OGd g; g.base = v3(m->base[0], m->base[1], m->base[2]); g.ws = m->ws; g.eta = m->ior; g.a = m->roughness * m->roughness; g.a2 = g.a * g.a; g.delta = g.a < O_DELTA;
     g.Fo = g.ws > 0.f ? g.ws * o_fd(wo.z, g.eta) : 0.f;
@@ -976,13 +986,13 @@ static OGd o_gd(const OMat* m, V3 wo, int energy, float ux1, float ux2) {
         float X = (om > 0.f && wr.z > 0.f) ? g.ws * o_fd(om, g.eta) * o_g2(wo.z, wr.z, g.a2) / o_g1(wo.z, g.a2) : 0.f;
         g.kd = 1.f - X;
     }
-    g.kd = fmaxf(g.kd, 0.f);
+    g.kd = fmaxf(g.kd, 0.f); g.nr = v3(0.f, 0.f, 1.f);
     return g;
 }
 static OEval o_gd_eval(const OGd* g, V3 wo, V3 wi) {
     OEval r = { v3(0.f, 0.f, 0.f), 0.f };
     if (wi.z <= 0.f) return r;
-    r.f = muls(g->base, g->kd * 0.31830989f); r.pdf = (1.f - g->pSpec) * wi.z * 0.31830989f;
+    r.f = muls(g->base, g->kd * 0.31830989f * o_bump(g->nr, wi)); r.pdf = (1.f - g->pSpec) * wi.z * 0.31830989f;
     if (!g->delta && g->Fo > 0.f) {
         V3 m = normz(add(wo, wi)); float om = dot3(wo, m);
         if (om > 0.f) {
@@ -1056,34 +1066,39 @@ static int o_non_delta(const OMat* m) {
     float wM, wT, wD; o_weights(m, &wM, &wT, &wD); int rough = m->roughness * m->roughness >= O_DELTA;
     return (wD > 0.f && (o_lum(v3(m->base[0], m->base[1], m->base[2])) > 0.f || rough)) || ((wM > 0.f || wT > 0.f) && rough);
 }
-static OEval o_bsdf_eval(const OMat* m, V3 wo, V3 wi, float eta, int gd, float ux1, float ux2) {
+static OEval o_bsdf_eval(const OMat* m, V3 wo, V3 wi, float eta, int gd, float ux1, float ux2, V3 nr) {
     float wM, wT, wD; o_weights(m, &wM, &wT, &wD); OEval r = { v3(0.f, 0.f, 0.f), 0.f };
     if (wM > 0.f) { OEval e = o_cond_eval(m, wo, wi); r.f = add(r.f, muls(e.f, wM)); r.pdf += wM * e.pdf; }
     if (wT > 0.f) { OEval e = o_diel_eval(m, eta, wo, wi); r.f = add(r.f, muls(e.f, wT)); r.pdf += wT * e.pdf; }
-    if (wD > 0.f) { OGd g = o_gd(m, wo, gd, ux1, ux2); OEval e = o_gd_eval(&g, wo, wi); r.f = add(r.f, muls(e.f, wD)); r.pdf += wD * e.pdf; }
+    if (wD > 0.f) { OGd g = o_gd(m, wo, gd, ux1, ux2); g.nr = nr; OEval e = o_gd_eval(&g, wo, wi); r.f = add(r.f, muls(e.f, wD)); r.pdf += wD * e.pdf; }
     return r;
 }
-static int o_bsdf_sample(const OMat* m, V3 wo, float eta, int gd, float ux1, float ux2, float u, float u1, float u2, V3* wi, V3* w, float* pdf) {
+static int o_bsdf_sample(const OMat* m, V3 wo, float eta, int gd, float ux1, float ux2, float u, float u1, float u2, V3* wi, V3* w, float* pdf, V3 nr) {
     float wM, wT, wD; o_weights(m, &wM, &wT, &wD); int ok;
     if (u < wM) ok = o_cond_sample(m, wo, u1, u2, wi, w, pdf);
     else if (u < wM + wT) ok = o_diel_sample(m, eta, wo, fminf((u - wM) / wT, 0.99999994f), u1, u2, wi, w, pdf);
-    else { OGd g = o_gd(m, wo, gd, ux1, ux2); ok = o_gd_sample(&g, wo, fminf(wD > 0.f ? (u - wM - wT) / wD : 0.f, 0.99999994f), u1, u2, wi, w, pdf); }
+    else { OGd g = o_gd(m, wo, gd, ux1, ux2); g.nr = nr; ok = o_gd_sample(&g, wo, fminf(wD > 0.f ? (u - wM - wT) / wD : 0.f, 0.99999994f), u1, u2, wi, w, pdf); }
     if (!ok) return 0;
     if (*pdf <= 0.f) return 1;
     if (wM == 1.f || wT == 1.f || wD == 1.f) return 1;
-    OEval e = o_bsdf_eval(m, wo, *wi, eta, gd, ux1, ux2); if (e.pdf <= 0.f) return 0;
+    OEval e = o_bsdf_eval(m, wo, *wi, eta, gd, ux1, ux2, nr); if (e.pdf <= 0.f) return 0;
     *w = muls(e.f, fabsf(wi->z) / e.pdf); *pdf = e.pdf; return 1;
 }
-void orc_bsdf_eval(const float* mats, const int* mat, const float* wo, const float* wi, const float* eta, int gd, const float* ux, float* f, float* pdf, long n) {
+/* nr: an unperturbed normal per case (the bump-terminator term), or NULL: +z (off) */
+void orc_bsdf_eval(const float* mats, const int* mat, const float* wo, const float* wi, const float* eta, int gd, const float* ux, float* f, float* pdf, long n,
+                   const float* nr) {
     for (long i = 0; i < n; i++) {
-        OEval e = o_bsdf_eval((const OMat*)(mats + 16 * (size_t)mat[i]), a3(wo + 3 * i), a3(wi + 3 * i), eta[i], gd, ux[2 * i], ux[2 * i + 1]);
+        OEval e = o_bsdf_eval((const OMat*)(mats + 16 * (size_t)mat[i]), a3(wo + 3 * i), a3(wi + 3 * i), eta[i], gd, ux[2 * i], ux[2 * i + 1],
+                              nr ? a3(nr + 3 * i) : v3(0.f, 0.f, 1.f));
         f[3 * i] = e.f.x; f[3 * i + 1] = e.f.y; f[3 * i + 2] = e.f.z; pdf[i] = e.pdf;
     }
 }
-void orc_bsdf_sample(const float* mats, const int* mat, const float* wo, const float* eta, int gd, const float* ux, const float* uvw, float* wi, float* w, float* pdf, int* ok, long n) {
+void orc_bsdf_sample(const float* mats, const int* mat, const float* wo, const float* eta, int gd, const float* ux, const float* uvw, float* wi, float* w, float* pdf, int* ok, long n,
+                     const float* nr) {
     for (long i = 0; i < n; i++) {
         V3 a = v3(0.f, 0.f, 0.f), b = a; float p = 0.f;
-        ok[i] = o_bsdf_sample((const OMat*)(mats + 16 * (size_t)mat[i]), a3(wo + 3 * i), eta[i], gd, ux[2 * i], ux[2 * i + 1], uvw[3 * i], uvw[3 * i + 1], uvw[3 * i + 2], &a, &b, &p);
+        ok[i] = o_bsdf_sample((const OMat*)(mats + 16 * (size_t)mat[i]), a3(wo + 3 * i), eta[i], gd, ux[2 * i], ux[2 * i + 1], uvw[3 * i], uvw[3 * i + 1], uvw[3 * i + 2], &a, &b, &p,
+                              nr ? a3(nr + 3 * i) : v3(0.f, 0.f, 1.f));
         wi[3 * i] = a.x; wi[3 * i + 1] = a.y; wi[3 * i + 2] = a.z; w[3 * i] = b.x; w[3 * i + 1] = b.y; w[3 * i + 2] = b.z; pdf[i] = p;
     }
 }
@@ -1097,7 +1112,7 @@ void orc_bsdf_sample(const float* mats, const int* mat, const float* wo, const f
  * rays, counts[1] shadow rays. */
 typedef struct { float pos[3], ax[3], ay[3], az[3], fx, fy, px, py; int w, h; float lens_r, focus_d; } OCam;
 typedef struct { int scene, frame; OCam cam; int spp, max_depth; unsigned seed; float sun_to[3], sun_e[3], sky[3], sun_cos, eps; int env; float env_rot_deg;
-                 int light_mode, rr, rr_depth, env_uniform; } OReq;
+                 int light_mode, rr, rr_depth, env_uniform, bump_shadow; } OReq;
 enum { O_LIGHT_MIS = 0, O_LIGHT_NEE = 1, O_LIGHT_BSDF = 2 };   /* render/params.h:23 */
 
 /* Emissive-triangle light tables of one frame (SceneSetup::frameData, app/scene_setup.cpp:274-299). soup: 12 floats
@@ -1290,6 +1305,7 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
                 if (l > 0.f) nsw = muls(nt, 1.f / l);
                 if (dot3(nsw, ng0) < 0.f) nsw = neg(nsw);
             }
+            const V3 nsU0 = nsw; int mapped = 0;   /* the normal before a normal image, for the bump-terminator term */
             if (MX && mid < n_mtex && (MX[mid].base_color >= 0 || MX[mid].emission >= 0 || MX[mid].normal >= 0 || MX[mid].metallic >= 0 || MX[mid].roughness >= 0)) {
                 const OMTex X = MX[mid];
                 const long ti = (long)mesh_first[imesh] + fi(TR[3 * tri].w);
@@ -1314,7 +1330,7 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
                         o_tex(&TX[X.normal], tu, 1.f - tv, c);
                         const V3 nm = add(add(muls(tg, (2.f * c[0] - 1.f) * X.normal_scale), muls(bt, (2.f * c[1] - 1.f) * X.normal_scale)), muls(nsw, 2.f * c[2] - 1.f));
                         const float nl = sqrtf(dot3(nm, nm));
-                        if (nl > 0.f) nsw = muls(nm, 1.f / nl);
+                        if (nl > 0.f) { nsw = muls(nm, 1.f / nl); mapped = 1; }
                     }
                 }
             }
@@ -1342,6 +1358,12 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
             if (dot3(ns, wo) <= 1e-6f) ns = ng;
             V3 tx, ty; onb(ns, &tx, &ty);
             const V3 woL = v3(dot3(wo, tx), dot3(wo, ty), dot3(wo, ns));
+            V3 nrL = v3(0.f, 0.f, 1.f);
+            if (R->bump_shadow && mapped) {
+                const V3 nsU = front ? nsU0 : neg(nsU0);
+                nrL = v3(dot3(nsU, tx), dot3(nsU, ty), dot3(nsU, ns));
+                if (!(nrL.z > 0.f)) nrL = v3(0.f, 0.f, 1.f);
+            }
             const float eta = front ? M->ior : 1.f / M->ior;
             const V3 up = add(p, muls(ng, R->eps)), dn = sub(p, muls(ng, R->eps));
             const unsigned dr = (unsigned)depth + 1u;
@@ -1396,7 +1418,7 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
                 const V3 lL = v3(dot3(l, tx), dot3(l, ty), dot3(l, ns));
                 const float gl = dot3(ng, l);
                 if (ok && lL.z != 0.f && (gl > 0.f) == (lL.z > 0.f)) {
-                    const OEval e = o_bsdf_eval(M, woL, lL, eta, gd, ux1, ux2);
+                    const OEval e = o_bsdf_eval(M, woL, lL, eta, gd, ux1, ux2, nrL);
                     const float wgt_l = (isSun || R->light_mode == O_LIGHT_NEE) ? 1.f : o_mis(pl, e.pdf);
                     const V3 c = muls(mulv(mulv(T, e.f), Le), fabsf(lL.z) * wgt_l / pl);
                     if (c.x > 0.f || c.y > 0.f || c.z > 0.f) {
@@ -1409,7 +1431,7 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
                 }
             }
             V3 wiL, wgt; float pdf;
-            if (!o_bsdf_sample(M, woL, eta, gd, ux1, ux2, orc_rng(pix, smp, dr, 4, seed), orc_rng(pix, smp, dr, 0, seed), orc_rng(pix, smp, dr, 1, seed), &wiL, &wgt, &pdf)) break;
+            if (!o_bsdf_sample(M, woL, eta, gd, ux1, ux2, orc_rng(pix, smp, dr, 4, seed), orc_rng(pix, smp, dr, 0, seed), orc_rng(pix, smp, dr, 1, seed), &wiL, &wgt, &pdf, nrL)) break;
             const V3 wi = normz(add(add(muls(tx, wiL.x), muls(ty, wiL.y)), muls(ns, wiL.z)));
             const float gi = dot3(ng, wi);
             if (gi == 0.f || (gi > 0.f) != (wiL.z > 0.f)) break;

@@ -231,6 +231,26 @@ extern "C" void ref_bsdf_sample(const void* mats, const int* mat, const float* w
         wi[3 * i] = a.x; wi[3 * i + 1] = a.y; wi[3 * i + 2] = a.z; w[3 * i] = b.x; w[3 * i + 1] = b.y; w[3 * i + 2] = b.z; pdf[i] = p;
     }
 }
+// the same with an unperturbed normal nr per triple (the bump-terminator term of the diffuse lobe, render/bsdf.h:67-75)
+extern "C" void ref_bsdf_eval_nr(const void* mats, const int* mat, const float* wo, const float* wi, const float* eta, int gd, const float* ux, const float* nr,
+                                 float* f, float* pdf, long n) {
+    const Material* M = (const Material*)mats;
+    for (long i = 0; i < n; i++) {
+        BsdfEval e = bsdfEval(M[mat[i]], make_float3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), make_float3(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), eta[i], gd, ux[2 * i], ux[2 * i + 1],
+                              make_float3(nr[3 * i], nr[3 * i + 1], nr[3 * i + 2]));
+        f[3 * i] = e.f.x; f[3 * i + 1] = e.f.y; f[3 * i + 2] = e.f.z; pdf[i] = e.pdf;
+    }
+}
+extern "C" void ref_bsdf_sample_nr(const void* mats, const int* mat, const float* wo, const float* eta, int gd, const float* ux, const float* uvw, const float* nr,
+                                   float* wi, float* w, float* pdf, int* ok, long n) {
+    const Material* M = (const Material*)mats;
+    for (long i = 0; i < n; i++) {
+        float3 a = make_float3(0.f, 0.f, 0.f), b = a; float p = 0.f;
+        ok[i] = bsdfSample(M[mat[i]], make_float3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), eta[i], gd, ux[2 * i], ux[2 * i + 1], uvw[3 * i], uvw[3 * i + 1], uvw[3 * i + 2], a, b, p,
+                           make_float3(nr[3 * i], nr[3 * i + 1], nr[3 * i + 2])) ? 1 : 0;
+        wi[3 * i] = a.x; wi[3 * i + 1] = a.y; wi[3 * i + 2] = a.z; w[3 * i] = b.x; w[3 * i + 1] = b.y; w[3 * i + 2] = b.z; pdf[i] = p;
+    }
+}
 extern "C" int ref_material_size(void) { return (int)sizeof(Material); }
 
 // the reference's loadHDR + buildEnvMap on a Radiance file: sizes first (texels/marg/cond NULL), then the tables

@@ -52,9 +52,9 @@ def _load_oracle():
     L.orc_trace_inst.restype = C.c_long
     L.orc_trace_inst.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_long, C.c_void_p, C.c_void_p]
     L.orc_bsdf_eval.restype = None
-    L.orc_bsdf_eval.argtypes = [C.c_void_p] * 5 + [C.c_int] + [C.c_void_p] * 3 + [C.c_long]
+    L.orc_bsdf_eval.argtypes = [C.c_void_p] * 5 + [C.c_int] + [C.c_void_p] * 3 + [C.c_long, C.c_void_p]
     L.orc_bsdf_sample.restype = None
-    L.orc_bsdf_sample.argtypes = [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 6 + [C.c_long]
+    L.orc_bsdf_sample.argtypes = [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 6 + [C.c_long, C.c_void_p]
     L.orc_render_stats.restype = None
     L.orc_render_stats.argtypes = [C.c_int, C.c_void_p]
     L.orc_render_request.restype = C.c_long
@@ -140,17 +140,21 @@ class Oracle:
         assert bad == 0
         return hits, hi
 
-    def bsdf_eval(self, mats, mat, wo, wi, eta, gd, ux):
+    def bsdf_eval(self, mats, mat, wo, wi, eta, gd, ux, nr=None):
+        """nr: an unperturbed normal per case (the bump-terminator term) or None"""
         n = len(mat); f = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32)
         a = [np.ascontiguousarray(x) for x in (mats, mat, wo, wi, eta, ux)]
-        self.L.orc_bsdf_eval(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, a[4].ctypes.data, gd, a[5].ctypes.data, f.ctypes.data, pdf.ctypes.data, n)
+        nr = np.ascontiguousarray(nr, np.float32) if nr is not None else None
+        self.L.orc_bsdf_eval(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, a[4].ctypes.data, gd, a[5].ctypes.data, f.ctypes.data, pdf.ctypes.data, n,
+                             nr.ctypes.data if nr is not None else None)
         return f, pdf
 
-    def bsdf_sample(self, mats, mat, wo, eta, gd, ux, uvw):
+    def bsdf_sample(self, mats, mat, wo, eta, gd, ux, uvw, nr=None):
         n = len(mat); wi = np.zeros((n, 3), np.float32); w = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32); ok = np.zeros(n, np.int32)
         a = [np.ascontiguousarray(x) for x in (mats, mat, wo, eta, ux, uvw)]
+        nr = np.ascontiguousarray(nr, np.float32) if nr is not None else None
         self.L.orc_bsdf_sample(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, gd, a[4].ctypes.data, a[5].ctypes.data,
-                               wi.ctypes.data, w.ctypes.data, pdf.ctypes.data, ok.ctypes.data, n)
+                               wi.ctypes.data, w.ctypes.data, pdf.ctypes.data, ok.ctypes.data, n, nr.ctypes.data if nr is not None else None)
         return wi, w, pdf, ok
 
     def envmap_build(self, rgb, strength=1.0):

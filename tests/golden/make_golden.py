@@ -28,9 +28,15 @@ and tests/golden/env.npz:
   outputs  the reference's loadHDR radiance and buildEnvMap tables (texels x strength 1.5, marginal and conditional
            CDFs) for each file
 
+and tests/golden/bsdf_bump.npz:
+
+  inputs   the cases of bsdf.npz with an unperturbed normal per case (the bump-terminator term of the diffuse lobe)
+  outputs  the reference's bsdfEval and bsdfSample with it, energy compensation off and on
+
 The fixtures pin the oracle and the library where the reference sources are absent. Run from the repository root:
-    python tests/golden/make_golden.py          (every fixture)
-    python tests/golden/make_golden.py env      (env.npz only)
+    python tests/golden/make_golden.py              (every fixture)
+    python tests/golden/make_golden.py env          (env.npz only)
+    python tests/golden/make_golden.py bsdf_bump    (bsdf_bump.npz only, from bsdf.npz's inputs)
 """
 import importlib
 import os
@@ -68,6 +74,7 @@ def main():
     print("wrote", os.path.join(HERE, "boxes64.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
     instances(ref, out)
     bsdf(ref)
+    bsdf_bump(ref)
     envmaps(ref)
 
 
@@ -158,6 +165,33 @@ def bsdf(ref):
     print("wrote", os.path.join(HERE, "bsdf.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
 
 
+def bsdf_bump(ref):
+    """The bump-terminator term (render/bsdf.h:67-75): the inputs of bsdf.npz with an unperturbed normal nr per triple,
+    tilted from the shading normal by up to ~70 degrees (nr.z > 0, the only case the integrator passes), and nr = +z
+    exactly for the last quarter (the term is off there); the reference's bsdfEval / bsdfSample with it."""
+    import ctypes as C
+    L = ref.L
+    g = np.load(os.path.join(HERE, "bsdf.npz"))
+    mats, mat, wo, wi, eta, ux, uvw = (np.ascontiguousarray(g[k]) for k in ("mats", "mat", "wo", "wi", "eta", "ux", "uvw"))
+    n = len(mat)
+    rng = np.random.default_rng(35)
+    nr = rng.normal(size=(n, 3)); nr[:, 2] = np.abs(nr[:, 2]) + 0.35
+    nr /= np.linalg.norm(nr, axis=1, keepdims=True)
+    nr[3 * n // 4:] = (0.0, 0.0, 1.0)
+    nr = np.ascontiguousarray(nr, np.float32)
+    out = dict(nr=nr)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    L.ref_bsdf_eval_nr.restype = None; L.ref_bsdf_sample_nr.restype = None
+    for gd in (0, 1):
+        f = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32)
+        L.ref_bsdf_eval_nr(p(mats), p(mat), p(wo), p(wi), p(eta), C.c_int(gd), p(ux), p(nr), p(f), p(pdf), C.c_long(n))
+        sw = np.zeros((n, 3), np.float32); sWt = np.zeros((n, 3), np.float32); spdf = np.zeros(n, np.float32); ok = np.zeros(n, np.int32)
+        L.ref_bsdf_sample_nr(p(mats), p(mat), p(wo), p(eta), C.c_int(gd), p(ux), p(uvw), p(nr), p(sw), p(sWt), p(spdf), p(ok), C.c_long(n))
+        out.update({f"f{gd}": f, f"pdf{gd}": pdf, f"s_wi{gd}": sw, f"s_w{gd}": sWt, f"s_pdf{gd}": spdf, f"s_ok{gd}": ok})
+    np.savez_compressed(os.path.join(HERE, "bsdf_bump.npz"), **out)
+    print("wrote", os.path.join(HERE, "bsdf_bump.npz"), sum(a.nbytes for a in out.values()), "bytes uncompressed")
+
+
 def rgbe_bytes(rgb, rle):
     """Radiance RGBE file content for float rgb [h, w, 3] (new-style run-length scanlines when rle, else flat)"""
     h, w = rgb.shape[:2]
@@ -222,8 +256,8 @@ def envmaps(ref):
 
 
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "env":
+    if len(sys.argv) > 1 and sys.argv[1] in ("env", "bsdf_bump"):
         from conftest import REF_DIR, Ref
-        envmaps(Ref(os.path.join(REF_DIR, "libcwpref.so")))
+        (envmaps if sys.argv[1] == "env" else bsdf_bump)(Ref(os.path.join(REF_DIR, "libcwpref.so")))
     else:
         main()

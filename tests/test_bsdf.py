@@ -39,3 +39,21 @@ def test_bsdf_reciprocity_and_energy(oracle):
     lam = np.where(g["mat"] % 8 == 0)[0]
     wi, w, p, ok = oracle.bsdf_sample(g["mats"], g["mat"][lam], g["wo"][lam], g["eta"][lam], 0, g["ux"][lam], g["uvw"][lam])
     assert np.allclose(w[ok == 1], g["mats"][g["mat"][lam][ok == 1], 0:3], rtol=1e-5)
+
+
+def test_oracle_bump_terminator_matches_reference(oracle):
+    """The bump-terminator term of the diffuse lobe (render/bsdf.h:67-75) with an unperturbed normal per case
+    (fixture tests/golden/bsdf_bump.npz, the reference's bsdfEval / bsdfSample with nr): eval and sample agree as
+    without the term; cases with nr = +z give the plain values; the term only ever darkens the diffuse lobe."""
+    g, b = golden("bsdf.npz"), golden("bsdf_bump.npz")
+    n = len(b["nr"])
+    for gd in (0, 1):
+        f, pdf = oracle.bsdf_eval(g["mats"], g["mat"], g["wo"], g["wi"], g["eta"], gd, g["ux"], nr=b["nr"])
+        assert close(f, b[f"f{gd}"]) and close(pdf, b[f"pdf{gd}"]), gd
+        assert np.array_equal(b[f"f{gd}"][3 * n // 4:], g[f"f{gd}"][3 * n // 4:])
+        assert np.all(b[f"f{gd}"] <= g[f"f{gd}"] + 1e-7) and (b[f"f{gd}"] < g[f"f{gd}"]).mean() > 0.1
+        wi, w, pdf, ok = oracle.bsdf_sample(g["mats"], g["mat"], g["wo"], g["eta"], gd, g["ux"], g["uvw"], nr=b["nr"])
+        same = ok == b[f"s_ok{gd}"]
+        assert same.mean() >= 0.999, gd
+        k = same & (ok == 1)
+        assert close(wi[k], b[f"s_wi{gd}"][k], rel=1e-4, abs_=1e-5) and close(w[k], b[f"s_w{gd}"][k], rel=1e-4, abs_=1e-5)

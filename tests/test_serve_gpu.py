@@ -14,7 +14,13 @@ def close(a, b, rel, abs_):
 
 
 def test_device_bsdf_matches_reference(gpu, cwp):
-    g = golden("bsdf.npz")
+    g, bump = golden("bsdf.npz"), golden("bsdf_bump.npz")
+    for gd in (0, 1):   # the bump-terminator term (unperturbed normals per case)
+        f, pdf = cwp.bsdf_eval_batch(g["mats"], g["mat"], g["wo"], g["wi"], g["eta"], gd, g["ux"], nr=bump["nr"])
+        assert close(f, bump[f"f{gd}"], 1e-4, 1e-6).mean() >= 0.999 and close(pdf, bump[f"pdf{gd}"], 1e-4, 1e-6).mean() >= 0.999
+        wi, w, p, ok = cwp.bsdf_sample_batch(g["mats"], g["mat"], g["wo"], g["eta"], gd, g["ux"], g["uvw"], nr=bump["nr"])
+        k = (ok == bump[f"s_ok{gd}"]) & (ok == 1)
+        assert (ok == bump[f"s_ok{gd}"]).mean() >= 0.998 and close(w[k], bump[f"s_w{gd}"][k], 1e-3, 1e-4).mean() >= 0.998
     for gd in (0, 1):
         f, pdf = cwp.bsdf_eval_batch(g["mats"], g["mat"], g["wo"], g["wi"], g["eta"], gd, g["ux"])
         assert close(f, g[f"f{gd}"], 1e-4, 1e-6).mean() >= 0.999 and close(pdf, g[f"pdf{gd}"], 1e-4, 1e-6).mean() >= 0.999
@@ -309,9 +315,11 @@ def test_texture_lookups_match_oracle(gpu, cwp, oracle):
 
 
 def test_textured_request_matches_oracle(gpu, cwp, oracle, serving):
-    """Materials with base-colour, metallic/roughness, normal and emission images on box-field uvs: the request's image
-    matches the oracle's at >= 45 dB (the texture unit's filtering is restated, not bit-identical) with the same ray
-    counts within 0.5%, and differs from the untextured image."""
+    """Materials with base-colour, metallic/roughness, normal and emission images on box-field uvs (the emissive
+    material is light-sampled, its image scaling the sampled radiance): the request's image matches the oracle's at
+    >= 45 dB (the texture unit's filtering is restated, not bit-identical) with the same ray counts within 0.5%, and
+    differs from the untextured image. With bump-terminator shadowing on the normal-mapped materials it matches again
+    and differs from the image without."""
     b, descs, first, mats, base, boxes = serving
     meshes = cwp.serving_scenes(n_scenes=3, seed=2, tris=(200, 8000), instances=(1, 24), blas_per_scene=(1, 3))[0]   # the fixture's meshes
     uvs, tans = cwp.planar_uvs(meshes)
@@ -336,10 +344,19 @@ def test_textured_request_matches_oracle(gpu, cwp, oracle, serving):
     tlas, roots, inst = b.download_tlas(4, _n_inst(b, 4))
     tex, keep = cwp.textures_array(imgs)
     mesh_first = np.concatenate([[0], np.cumsum([len(f) for _, f, _, _ in meshes])]).astype(np.int32)
+    lights = cwp.emissive_tables(meshes, base, mats_e, *cwp.scene_xforms(descs, first, req.scene, req.frame))
     ref, cnt = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, mats_e, base, tlas_width=b.tlas_width,
-                                     textures=(tex, mt, uvs, tans, mesh_first))
+                                     textures=(tex, mt, uvs, tans, mesh_first), lights=lights)
     a = acc[:, :3] / req.spp; r = ref[:, :3] / req.spp
     assert cwp.imageio.psnr(a, r) >= 45.0
     assert abs(st.rays - cnt[0]) <= 5e-3 * cnt[0] and abs(st.shadow_rays - cnt[1]) <= 5e-3 * max(cnt[1], 1)
+    req.bump_shadow = 1
+    (acc_b, st_b), = run_all(s, [req])
+    assert not np.allclose(acc_b, acc)
+    tlas, roots, inst = b.download_tlas(4, _n_inst(b, 4))
+    ref_b, cnt_b = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, mats_e, base, tlas_width=b.tlas_width,
+                                         textures=(tex, mt, uvs, tans, mesh_first), lights=lights)
+    assert cwp.imageio.psnr(acc_b[:, :3] / req.spp, ref_b[:, :3] / req.spp) >= 45.0
+    assert abs(st_b.rays - cnt_b[0]) <= 5e-3 * cnt_b[0]
     with pytest.raises(cwp.CwpError):
         s.set_textures(imgs, cwp.material_textures([dict(base_color=9)]), uvs)   # texture id out of range
