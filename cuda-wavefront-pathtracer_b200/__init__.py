@@ -115,7 +115,8 @@ class Request(C.Structure):
     _fields_ = [("scene", C.c_int32), ("frame", C.c_int32), ("cam", Camera), ("spp", C.c_int32), ("max_depth", C.c_int32), ("seed", C.c_uint32),
                 ("sun_to", C.c_float * 3), ("sun_e", C.c_float * 3), ("sky", C.c_float * 3), ("sun_cos", C.c_float), ("eps", C.c_float),
                 ("env", C.c_int32), ("env_rot_deg", C.c_float),
-                ("light_mode", C.c_int32), ("rr", C.c_int32), ("rr_depth", C.c_int32), ("env_uniform", C.c_int32), ("bump_shadow", C.c_int32)]
+                ("light_mode", C.c_int32), ("rr", C.c_int32), ("rr_depth", C.c_int32), ("env_uniform", C.c_int32), ("bump_shadow", C.c_int32),
+                ("near_clip", C.c_float), ("filter_bh", C.c_int32)]
 
 
 LIGHT_MIS, LIGHT_NEE, LIGHT_BSDF = 0, 1, 2
@@ -682,7 +683,7 @@ def envmap_build(rgb, strength=1.0):
 
 
 def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun_e=None, sky=None, sun_angle_rad=None, eps=1e-3, env=-1, env_rot_deg=0.0,
-                 light_mode=LIGHT_MIS, rr=0, rr_depth=3, env_uniform=0, bump_shadow=0):
+                 light_mode=LIGHT_MIS, rr=0, rr_depth=3, env_uniform=0, bump_shadow=0, near_clip=0.0, filter_bh=0):
     """A serving request; lighting defaults to the benchmark's sun and sky (env = -1) or names one of the server's
     environment maps; emissive materials of the scene are light-sampled too (light_mode, as the reference's
     --light_sampling mis / nee / bsdf); rr / rr_depth: Russian roulette (--rr, --rr_depth)."""
@@ -696,6 +697,7 @@ def make_request(scene, cam, spp, frame=0, max_depth=8, seed=1, sun_to=None, sun
     r.sun_cos = float(np.float32(math.cos(sun_angle_rad / 2.0))); r.eps = eps
     r.env, r.env_rot_deg = env, env_rot_deg
     r.light_mode, r.rr, r.rr_depth, r.env_uniform, r.bump_shadow = light_mode, rr, rr_depth, env_uniform, bump_shadow
+    r.near_clip, r.filter_bh = near_clip, filter_bh
     return r
 
 

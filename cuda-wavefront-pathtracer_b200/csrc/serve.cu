@@ -40,6 +40,7 @@ struct SlotParams {
     // light sampling: light-type probabilities, mode (CWP_LIGHT_*), Russian roulette, uniform environment samples; the
     // scene's emissive triangles at the request's frame (nEm = 0: none): 3 float4 each, power CDF, area density by material
     float pSun, pTri, pEnv; int lightMode, rr, rrDepth, envUniform, nEm, bumpShadow;
+    float nearClip; int filterBh;
     const float4* emTris; const float* emCdf; const float* matPdf;
 };
 
@@ -98,8 +99,10 @@ __device__ __forceinline__ int serve_pixel(int j, int w, int h) {
     return ((t / tilesX) * 4 + (r >> 3)) * w + (t % tilesX) * 8 + (r & 7);
 }
 
-// chunk c: slot, first path index, count, queue position of its first path (ascending)
-__global__ void k_serve_raygen(const int4* __restrict__ chunks, int nChunks, int total, const SlotParams* __restrict__ slots, RayQueue q, int base) {
+// chunk c: slot, first path index, count, queue position of its first path (ascending). Camera rays as k_raygen
+// (render/wavefront.cu:42-58): box or Blackman-Harris pixel filter (ftab: its inverse CDF), thin lens, near clip.
+__global__ void k_serve_raygen(const int4* __restrict__ chunks, int nChunks, int total, const SlotParams* __restrict__ slots, RayQueue q, int base,
+                               const float* __restrict__ ftab) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total) return;
     int lo = 0, hi = nChunks - 1;
@@ -110,12 +113,21 @@ __global__ void k_serve_raygen(const int4* __restrict__ chunks, int nChunks, int
     const cwp_camera& C = S.cam;
     const int pix = serve_pixel(j % S.N, C.w, C.h); const unsigned smp = (unsigned)(j / S.N);
     const int x = pix % C.w, y = pix / C.w;
-    const float jx = rnd_s(S.seed, pix, smp, 0, 0) - 0.5f, jy = rnd_s(S.seed, pix, smp, 0, 1) - 0.5f;   // box filter
+    const float u0 = rnd_s(S.seed, pix, smp, 0, 0), u1 = rnd_s(S.seed, pix, smp, 0, 1);
+    float jx, jy;
+    if (S.filterBh) { jx = table_lookup(ftab, CWP_FILTER_TABLE, u0); jy = table_lookup(ftab, CWP_FILTER_TABLE, u1); }
+    else { jx = u0 - 0.5f; jy = u1 - 0.5f; }
     const float dx = (x + 0.5f + jx - C.px) / C.fx, dy = -(y + 0.5f + jy - C.py) / C.fy;
-    const float3 ax = f3(C.ax[0], C.ax[1], C.ax[2]), ay = f3(C.ay[0], C.ay[1], C.ay[2]), az = f3(C.az[0], C.az[1], C.az[2]);
-    const float3 d = normalize(ax * dx + ay * dy - az);
+    const float3 ax = f3(C.ax[0], C.ax[1], C.ax[2]), ay = f3(C.ay[0], C.ay[1], C.ay[2]), az = f3(C.az[0], C.az[1], C.az[2]), pos = f3(C.pos[0], C.pos[1], C.pos[2]);
+    float3 d = normalize(ax * dx + ay * dy - az), o = pos;
+    if (C.lens_r > 0.f) {   // thin lens: origin on the lens disk, aimed at the pinhole ray's point on the focal plane
+        float lx, ly; disk_map(rnd_s(S.seed, pix, smp, 0, 2), rnd_s(S.seed, pix, smp, 0, 3), lx, ly);
+        const float3 pf = pos + (ax * dx + ay * dy - az) * C.focus_d;
+        o = pos + ax * (lx * C.lens_r) + ay * (ly * C.lens_r);
+        d = normalize(pf - o);
+    }
     const int k = base + t;
-    q.o[k] = make_float4(C.pos[0], C.pos[1], C.pos[2], 0.f); q.d[k] = make_float4(d.x, d.y, d.z, 1e30f); q.sc[k] = slot;
+    q.o[k] = make_float4(o.x, o.y, o.z, S.nearClip); q.d[k] = make_float4(d.x, d.y, d.z, 1e30f); q.sc[k] = slot;
     q.T[k] = make_float4(1.f, 1.f, 1.f, 0.f); q.info[k] = make_int4(slot, pix, (int)smp, 0);
 }
 
@@ -460,6 +472,7 @@ struct cwp_server {
     std::vector<cudaArray_t> texArrays; std::vector<cudaTextureObject_t> texObjs;
     cudaTextureObject_t* dTexObj = nullptr; cwp_material_textures* dMtex = nullptr; int nMtex = 0; float4* dUvs = nullptr; float4* dTans = nullptr;
     SlotParams* dSlots = nullptr; int* slotCnt = nullptr; std::vector<int> hSlotCnt;
+    float* ftab = nullptr;   // Blackman-Harris pixel-filter inverse CDF (CWP_FILTER_TABLE + 1 floats)
     RayQueue q[2]{}; RayQueue qs{}; int* slotBins = nullptr; ShadowQueue sq{}; float4* hits = nullptr; int* hinst = nullptr; int* occ = nullptr; int* cnt = nullptr; int4* dChunks = nullptr;
     int* hcnt = nullptr;   // pinned: [0..1] counts, then slot counters
     SlotParams* hSlots = nullptr; int4* hChunks = nullptr; bool slotsDirty = false;   // pinned mirrors of dSlots and dChunks
@@ -572,7 +585,13 @@ static int server_create(cwp_batch* b, const cwp_material* mats, int n, const in
     if (!rc) rc = alloc((void**)&s->dSlots, R * sizeof(SlotParams));
     if (!rc) rc = alloc((void**)&s->slotCnt, R * kSlotCounters * sizeof(int));
     if (!rc) rc = alloc((void**)&s->dChunks, (R + 1) * sizeof(int4));
+    if (!rc) rc = alloc((void**)&s->ftab, (CWP_FILTER_TABLE + 1) * sizeof(float));
     if (rc) return rc;
+    {
+        cwp_params pd;
+        if (int r2 = cwp_params_defaults(&pd)) return r2;
+        CWPB_CUDA(cudaMemcpy(s->ftab, pd.ftab, (CWP_FILTER_TABLE + 1) * sizeof(float), cudaMemcpyHostToDevice));
+    }
     CWPB_CUDA(cudaMallocHost(&s->hcnt, (4 + R * kSlotCounters) * sizeof(int)));
     CWPB_CUDA(cudaMallocHost(&s->hSlots, R * sizeof(SlotParams))); memset(s->hSlots, 0, R * sizeof(SlotParams));
     CWPB_CUDA(cudaMallocHost(&s->hChunks, (R + 1) * sizeof(int4)));
@@ -714,8 +733,10 @@ extern "C" int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* i
     CWPB_CHECK(r->env >= -1 && r->env < (int)s->envs.size(), CWP_ERR_INVALID, "environment map %d out of range (%d maps)", r->env, (int)s->envs.size());
     CWPB_CHECK(std::isfinite(r->env_rot_deg), CWP_ERR_INVALID, "environment rotation is not finite");
     CWPB_CHECK(r->light_mode >= CWP_LIGHT_MIS && r->light_mode <= CWP_LIGHT_BSDF && (r->rr == 0 || r->rr == 1) && r->rr_depth >= 0 && (r->env_uniform == 0 || r->env_uniform == 1) &&
-               (r->bump_shadow == 0 || r->bump_shadow == 1),
-               CWP_ERR_INVALID, "light mode %d, rr %d, rr_depth %d, env_uniform %d, bump_shadow %d", r->light_mode, r->rr, r->rr_depth, r->env_uniform, r->bump_shadow);
+               (r->bump_shadow == 0 || r->bump_shadow == 1) && (r->filter_bh == 0 || r->filter_bh == 1) && std::isfinite(r->near_clip) && r->near_clip >= 0.f &&
+               std::isfinite(r->cam.lens_r) && r->cam.lens_r >= 0.f && (r->cam.lens_r == 0.f || (std::isfinite(r->cam.focus_d) && r->cam.focus_d > 0.f)),
+               CWP_ERR_INVALID, "light mode %d, rr %d, rr_depth %d, env_uniform %d, bump_shadow %d, filter_bh %d, near %g, lens %g / %g", r->light_mode, r->rr, r->rr_depth,
+               r->env_uniform, r->bump_shadow, r->filter_bh, r->near_clip, r->cam.lens_r, r->cam.focus_d);
     CWPB_CHECK(r->cam.w > 0 && r->cam.h > 0 && r->spp > 0 && r->max_depth >= 0 && r->max_depth <= 64, CWP_ERR_INVALID, "bad request size");
     const int64_t total = (int64_t)r->cam.w * r->cam.h * r->spp;
     CWPB_CHECK(total < (1ll << 31), CWP_ERR_INVALID, "%lld paths in one request (limit 2^31)", (long long)total);
@@ -813,6 +834,7 @@ static int admit(cwp_server* s, bool& changed) {
         const int nt = (int)sunOn + (int)triOn + (int)envOn;
         P.pSun = sunOn ? 1.f / nt : 0.f; P.pTri = triOn ? 1.f / nt : 0.f; P.pEnv = envOn ? 1.f / nt : 0.f;
         P.lightMode = q.r.light_mode; P.rr = q.r.rr; P.rrDepth = q.r.rr_depth; P.envUniform = q.r.env_uniform; P.bumpShadow = q.r.bump_shadow;
+        P.nearClip = q.r.near_clip; P.filterBh = q.r.filter_bh;
         s->slotsDirty = true;
         CWPB_CUDA(cudaMemsetAsync(s->slotCnt + kSlotCounters * slot, 0, kSlotCounters * sizeof(int), s->st));
         q.slot = slot; q.admitMs = now_ms(s); s->info.admissions++; s->admitted.push_back(slot);
@@ -861,7 +883,7 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
     CWPB_CUDA(cudaEventRecord(s->ev[0], s->st));
     if (added > 0) {
         CWPB_CUDA(cudaMemcpyAsync(s->dChunks, s->hChunks, (size_t)nChunks * sizeof(int4), cudaMemcpyHostToDevice, s->st));
-        k_serve_raygen<<<(unsigned)((added + 255) / 256), 256, 0, s->st>>>(s->dChunks, nChunks, (int)added, s->dSlots, in, (int)s->nCur);
+        k_serve_raygen<<<(unsigned)((added + 255) / 256), 256, 0, s->st>>>(s->dChunks, nChunks, (int)added, s->dSlots, in, (int)s->nCur, s->ftab);
         CWPB_CUDA(cudaGetLastError());
     }
     const int64_t n = s->nCur + added;

@@ -365,6 +365,10 @@ typedef struct cwp_request {
     int32_t env_uniform;   /* 1: environment light samples uniform on the sphere instead of by luminance */
     int32_t bump_shadow;   /* 1: bump-terminator shadowing of the diffuse lobe where a normal image perturbed the normal
                               (Chiang et al. 2019; the reference's --bump_shadow) */
+    /* Camera rays (k_raygen, render/wavefront.cu:42-58): a thin lens when cam.lens_r > 0 (focused at cam.focus_d),
+     * tmin = near_clip, pixel filter box or Blackman-Harris of radius 1.5 (the reference's --filter bh, its default) */
+    float near_clip;
+    int32_t filter_bh;
 } cwp_request;
 #define CWP_LIGHT_MIS 0
 #define CWP_LIGHT_NEE 1

@@ -1112,7 +1112,15 @@ void orc_bsdf_sample(const float* mats, const int* mat, const float* wo, const f
  * rays, counts[1] shadow rays. */
 typedef struct { float pos[3], ax[3], ay[3], az[3], fx, fy, px, py; int w, h; float lens_r, focus_d; } OCam;
 typedef struct { int scene, frame; OCam cam; int spp, max_depth; unsigned seed; float sun_to[3], sun_e[3], sky[3], sun_cos, eps; int env; float env_rot_deg;
-                 int light_mode, rr, rr_depth, env_uniform, bump_shadow; } OReq;
+                 int light_mode, rr, rr_depth, env_uniform, bump_shadow; float near_clip; int filter_bh; } OReq;
+/* concentric disk map (Shirley & Chiu 1997; core/sampling.h:46-52) */
+static void o_disk(float u0, float u1, float* x, float* y) {
+    const float a = 2.f * u0 - 1.f, b = 2.f * u1 - 1.f;
+    if (a == 0.f && b == 0.f) { *x = *y = 0.f; return; }
+    float r, ph;
+    if (fabsf(a) > fabsf(b)) { r = a; ph = 0.78539816f * (b / a); } else { r = b; ph = 1.57079633f - 0.78539816f * (a / b); }
+    *x = r * cosf(ph); *y = r * sinf(ph);
+}
 enum { O_LIGHT_MIS = 0, O_LIGHT_NEE = 1, O_LIGHT_BSDF = 2 };   /* render/params.h:23 */
 
 /* Emissive-triangle light tables of one frame (SceneSetup::frameData, app/scene_setup.cpp:274-299). soup: 12 floats
@@ -1248,7 +1256,7 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
                         const float* mats, int n_mats, const int* mesh_mat, int gd, long j0, long j1, float* accum, long long* counts,
                         const float* env_tex, const float* env_marg, const float* env_cond, int env_w, int env_h,
                         const void* tex, const void* mtex, int n_mtex, const float* uvs, const float* tans, const int* mesh_first,
-                        const float* em_tris, const float* em_cdf, const float* mat_pdf, long n_em, const float* nrm) {
+                        const float* em_tris, const float* em_cdf, const float* mat_pdf, long n_em, const float* nrm, const float* ftab) {
     const OTex* TX = (const OTex*)tex; const OMTex* MX = (const OMTex*)mtex;
     const OReq* R = (const OReq*)reqp; const OCam* C = &R->cam;
     const int N = C->w * C->h; long bad = 0;
@@ -1264,16 +1272,27 @@ long orc_render_request(const void* reqp, int width, int tlas_width, const float
     for (long j = j0; j < j1; j++) {
         const int pix = o_tile_pixel((int)(j % N), C->w, C->h); const unsigned smp = (unsigned)(j / N), seed = R->seed;
         const int x = pix % C->w, y = pix / C->w;
-        const float jx = orc_rng(pix, smp, 0, 0, seed) - 0.5f, jy = orc_rng(pix, smp, 0, 1, seed) - 0.5f;
+        /* camera ray (render/wavefront.cu:42-58): box or Blackman-Harris filter, thin lens, near clip */
+        const float u0 = orc_rng(pix, smp, 0, 0, seed), u1 = orc_rng(pix, smp, 0, 1, seed);
+        float jx, jy;
+        if (R->filter_bh) { jx = table_lookup(ftab, 64, u0); jy = table_lookup(ftab, 64, u1); } else { jx = u0 - 0.5f; jy = u1 - 0.5f; }
         const float dx = (x + 0.5f + jx - C->px) / C->fx, dy = -(y + 0.5f + jy - C->py) / C->fy;
-        V3 o = v3(C->pos[0], C->pos[1], C->pos[2]);
-        V3 d = normz(sub(add(muls(v3(C->ax[0], C->ax[1], C->ax[2]), dx), muls(v3(C->ay[0], C->ay[1], C->ay[2]), dy)), v3(C->az[0], C->az[1], C->az[2])));
+        const V3 cax = v3(C->ax[0], C->ax[1], C->ax[2]), cay = v3(C->ay[0], C->ay[1], C->ay[2]), caz = v3(C->az[0], C->az[1], C->az[2]);
+        const V3 pos = v3(C->pos[0], C->pos[1], C->pos[2]), pin = sub(add(muls(cax, dx), muls(cay, dy)), caz);
+        V3 o = pos, d = normz(pin);
+        if (C->lens_r > 0.f) {
+            float lx, ly; o_disk(orc_rng(pix, smp, 0, 2, seed), orc_rng(pix, smp, 0, 3, seed), &lx, &ly);
+            const V3 pf = add(pos, muls(pin, C->focus_d));
+            o = add(add(pos, muls(cax, lx * C->lens_r)), muls(cay, ly * C->lens_r));
+            d = normz(sub(pf, o));
+        }
+        float tmin0 = R->near_clip;
         V3 T = v3(1.f, 1.f, 1.f);
         float lastPdf = 0.f;   /* pdf of the last BSDF sample (0: camera ray; <= 0: a delta lobe) */
         float* A = accum + 4 * (size_t)pix;
         for (int depth = 0;; depth++) {
             float t = 1e30f, u, v; int tri, hi;
-            if (o_inst1(width, tlas_width, 0, blas, tris, (const V4*)tlas, root, inst, o, d, 0.f, &t, &tri, &u, &v, &hi) < 0) bad++;
+            if (o_inst1(width, tlas_width, 0, blas, tris, (const V4*)tlas, root, inst, o, d, depth == 0 ? tmin0 : 0.f, &t, &tri, &u, &v, &hi) < 0) bad++;
             counts[0]++;
             if (tri < 0) {   /* miss: the environment weighted against its light sampling, or the constant sky */
                 V3 L = sky;

@@ -252,6 +252,8 @@ extern "C" void ref_bsdf_sample_nr(const void* mats, const int* mat, const float
     }
 }
 extern "C" int ref_material_size(void) { return (int)sizeof(Material); }
+// the pixel-filter inverse CDF of setupScene (core/sampling.h:38-43, app/scene_setup.cpp:185): n + 1 entries
+extern "C" void ref_bh_table(float* tab, int n, double width) { buildBlackmanHarrisTable(tab, n, width); }
 
 // the reference's loadHDR + buildEnvMap on a Radiance file: sizes first (texels/marg/cond NULL), then the tables
 extern "C" int ref_env_build(const char* path, float strength, int* w, int* h, float* rgb, float* texels, float* marg, float* cond) {

@@ -59,7 +59,7 @@ def _load_oracle():
     L.orc_render_stats.argtypes = [C.c_int, C.c_void_p]
     L.orc_render_request.restype = C.c_long
     L.orc_render_request.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
-                                     + [C.c_void_p] * 3 + [C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3 + [C.c_void_p] * 3 + [C.c_long, C.c_void_p])
+                                     + [C.c_void_p] * 3 + [C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3 + [C.c_void_p] * 3 + [C.c_long, C.c_void_p, C.c_void_p])
     L.orc_emissive_tables.restype = C.c_long
     L.orc_emissive_tables.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_long] + [C.c_void_p] * 3
     L.orc_texture_sample.restype = None
@@ -78,6 +78,7 @@ class Oracle:
 
     def __init__(self):
         self.L = _load_oracle()
+        self._ftab = None   # the pixel-filter table of camera rays (the library's, pinned to the reference's)
 
     def build(self, verts, faces, bins=16, leaf=4, variant=2):
         nt = len(faces)
@@ -205,6 +206,9 @@ class Oracle:
         ins = np.ascontiguousarray(inst, np.float32); ms = np.ascontiguousarray(mats, np.float32); mm = np.ascontiguousarray(mesh_mat, np.int32)
         nr = np.ascontiguousarray(normals[0], np.float32) if normals is not None else None
         mf = np.ascontiguousarray(normals[1], np.int32) if normals is not None else None
+        if self._ftab is None:
+            import importlib
+            self._ftab = np.array(list(importlib.import_module("cuda-wavefront-pathtracer_b200").params_defaults().ftab), np.float32)
         bad = self.L.orc_render_request(C.addressof(req), width, tlas_width, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, int(root), ins.ctypes.data,
                                         ms.ctypes.data, len(ms), mm.ctypes.data, gd, j0, j1, acc.ctypes.data, cnt.ctypes.data,
                                         *((env[0].ctypes.data, env[1].ctypes.data, env[2].ctypes.data, env[0].shape[1], env[0].shape[0]) if env is not None
@@ -214,7 +218,7 @@ class Oracle:
                                           else (None, None, 0, None, None, mf.ctypes.data if mf is not None else None)),
                                         *((lights[0].ctypes.data, lights[1].ctypes.data, lights[2].ctypes.data, len(lights[0])) if lights is not None and len(lights[0])
                                           else (None, None, None, 0)),
-                                        nr.ctypes.data if nr is not None else None)
+                                        nr.ctypes.data if nr is not None else None, self._ftab.ctypes.data)
         assert bad == 0
         return acc, cnt
 

@@ -114,6 +114,16 @@ def test_camera_look_at_matches_reference_formula(cwp):
     assert abs(c.fx - 256 / np.tan(np.radians(22.5))) < 1e-3 and c.px == 256 and c.w == 512
 
 
+def test_filter_table_matches_reference(cwp, ref):
+    """the Blackman-Harris pixel-filter inverse CDF (camera rays with --filter bh, the reference's default) is the
+    reference's buildBlackmanHarrisTable output bit for bit"""
+    import ctypes as C
+    t = np.zeros(65, np.float32)
+    ref.L.ref_bh_table.restype = None; ref.L.ref_bh_table.argtypes = [C.c_void_p, C.c_int, C.c_double]
+    ref.L.ref_bh_table(t.ctypes.data, 64, 1.5)
+    assert np.array_equal(np.array(list(cwp.params_defaults().ftab), np.float32).view(np.uint32), t.view(np.uint32))
+
+
 def test_params_finish(cwp):
     p = cwp.params_defaults()
     assert p.seed == 1000 and p.max_b == 8

@@ -295,6 +295,31 @@ def test_smooth_normals_request_matches_oracle(gpu, cwp, oracle):
     assert not np.allclose(acc, acc_flat)
 
 
+def test_camera_options_match_oracle(gpu, cwp, oracle, serving):
+    """Camera rays as the reference's k_raygen: a thin lens focused on the scene centre, a near clip and the
+    Blackman-Harris pixel filter; the request's image matches the oracle's at >= 45 dB and differs from the pinhole
+    box-filtered image of the same samples."""
+    b, descs, first, mats, base, boxes = serving
+    s = server(cwp, serving, max_paths=1 << 16, max_requests=4)
+    req = requests(cwp, boxes, 1, seed=47, res=((64, 48),), spps=(4,))[0]
+    (pin, _), = run_all(s, [req])
+    c = (boxes[req.scene][0] + boxes[req.scene][1]) / 2
+    req.cam.lens_r = 0.02 * float(np.max(boxes[req.scene][1] - boxes[req.scene][0]))
+    req.cam.focus_d = float(np.linalg.norm(np.array(list(req.cam.pos)) - c))
+    req.near_clip = 0.05 * req.cam.focus_d
+    req.filter_bh = 1
+    (acc, st), = run_all(s, [req])
+    assert not np.allclose(acc, pin)
+    nodes, tris = b.download(b.tuning().width)
+    tlas, roots, inst = b.download_tlas(4, _n_inst(b, 4))
+    ref, cnt = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, mats, base, tlas_width=b.tlas_width)
+    assert cwp.imageio.psnr(acc[:, :3] / req.spp, ref[:, :3] / req.spp) >= 45.0
+    assert abs(st.rays - cnt[0]) <= 2e-3 * cnt[0] and abs(st.shadow_rays - cnt[1]) <= 2e-3 * max(cnt[1], 1)
+    with pytest.raises(cwp.CwpError):
+        bad = requests(cwp, boxes, 1, seed=3)[0]; bad.cam.lens_r = 0.1; bad.cam.focus_d = 0.0   # a lens needs a focus distance
+        s.submit(bad)
+
+
 def test_texture_lookups_match_oracle(gpu, cwp, oracle):
     """Hardware bilinear lookups (wrap, normalised coordinates, sRGB decode for colour images) against the oracle's
     restatement of the documented filtering rule, over odd image sizes and coordinates wrapping over several periods.

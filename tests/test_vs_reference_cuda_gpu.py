@@ -133,7 +133,8 @@ def test_serving_vs_reference_full_integrator(gpu, cwp, tmp_path, case):
     lights and seed. The sample streams are the same; the reference's fast-math build rounds differently, so paths
     decorrelate after a bounce and the agreement is Monte Carlo-limited. The bound: the two images differ less than
     two of this library's own renders with independent seeds do (PSNR in tone-mapped sRGB). Cases: sun and sky; with
-    an environment map; NEE-only light sampling with Russian roulette; vertex normals on every second mesh."""
+    an environment map; NEE-only light sampling with Russian roulette; vertex normals on every second mesh. The first
+    uses the Blackman-Harris pixel filter (the reference's default), the others the box filter."""
     import numpy as np
     from conftest import golden
     pt = os.path.join(REF_DIR, "pt")
@@ -165,9 +166,10 @@ def test_serving_vs_reference_full_integrator(gpu, cwp, tmp_path, case):
         json.dump({"sun_dir_to_light_world_zup": list(W.SUN_TO), "sun_irradiance_W_m2": W.SUN_E, "sun_angle_rad": W.SUN_ANGLE_RAD,
                    "sky_radiance_rgb_linear": list(W.SKY)}, fp)
     args = [pt, "--scene", scene, "--frame_start", str(req.frame), "--frames", "1", "--camera", str(tmp_path / "camera.json"),
-            "--lighting", str(tmp_path / "lighting.json"), "--filter", "box", "--hfov", str(W.HFOV), "--width", str(w), "--height", str(h),
+            "--lighting", str(tmp_path / "lighting.json"), "--filter", "bh" if case == "sun" else "box", "--hfov", str(W.HFOV), "--width", str(w), "--height", str(h),
             "--spp", str(spp), "--batch", "64", "--bounces", str(depth), "--seed", str(req.seed), "--variant", "bvh2", "--warm", "0",
             "--out", str(tmp_path / "ref")]
+    req.filter_bh = 1 if case == "sun" else 0   # the reference's default pixel filter in one case
     b = cwp.Batch(meshes, normals=nrm)
     s = cwp.Server(b, mats, base, max_paths=1 << 20, max_requests=2)
     s.set_scenes(descs, first)
