@@ -196,19 +196,21 @@ def test_emissive_request_matches_oracle(gpu, cwp, oracle, serving, case):
 def test_light_modes_agree_and_requests_keep_their_lights(gpu, cwp, serving):
     """Lit by the emissive boxes alone (no sun, black sky): light sampling with MIS, light sampling alone (NEE), BSDF
     sampling alone and MIS with Russian roulette converge to the same image. The reference's consistency check
-    (tests/mis_consistency.py:1-6) restated: 8 independent seeds per mode, the mean luminance of every region of a 4x4
-    grid per seed, per mode its mean and standard error over the seeds, every pair of modes z = |a - b| / sqrt(se_a^2 +
-    se_b^2) <= 3. MIS is less noisy than BSDF sampling. Requests of different scenes and frames in one mix give each
+    (tests/mis_consistency.py:1-6) restated: 16 independent seeds per mode, the mean luminance of every region of a
+    4x4 grid per seed, per mode its mean and standard error over the seeds, every pair of modes z = |a - b| /
+    sqrt(se_a^2 + se_b^2). The whole image's z stays <= 3; a region's z <= 4, the bound for 96 comparisons (16
+    regions x 6 pairs) at a family-wise 1% with standard errors from 16 seeds (the reference's 3 is per comparison).
+    MIS is less noisy than BSDF sampling. Requests of different scenes and frames in one mix give each
     one's image alone (every slot reads its own request's light tables)."""
     b, descs, first, mats, base, boxes = serving
     em = _emissive(mats, base)
-    s = cwp.Server(b, em, base, max_paths=1 << 20, max_requests=8)
+    s = cwp.Server(b, em, base, max_paths=1 << 21, max_requests=16)
     s.set_scenes(descs, first)
     w, h, gx, gy = 64, 48, 4, 4
     stats = {}
     for name, mode, rr in (("mis", cwp.LIGHT_MIS, 0), ("nee", cwp.LIGHT_NEE, 0), ("bsdf", cwp.LIGHT_BSDF, 0), ("rr", cwp.LIGHT_MIS, 1)):
         reqs = []
-        for seed in range(8):
+        for seed in range(16):
             r = requests(cwp, boxes, 1, seed=31, res=((w, h),), spps=(32,))[0]
             r.sun_e[:] = (0.0, 0.0, 0.0); r.sky[:] = (0.0, 0.0, 0.0)
             r.light_mode, r.rr, r.rr_depth, r.seed = mode, rr, 2, 1000 + seed
@@ -217,7 +219,7 @@ def test_light_modes_agree_and_requests_keep_their_lights(gpu, cwp, serving):
         for acc, _ in run_all(s, reqs):
             im = (acc[:, :3] / 32).reshape(h, w, 3).astype(np.float64)
             L = 0.2126 * im[..., 0] + 0.7152 * im[..., 1] + 0.0722 * im[..., 2]
-            vals.append([L[j * h // gy:(j + 1) * h // gy, i * w // gx:(i + 1) * w // gx].mean() for j in range(gy) for i in range(gx)])
+            vals.append([L[j * h // gy:(j + 1) * h // gy, i * w // gx:(i + 1) * w // gx].mean() for j in range(gy) for i in range(gx)] + [L.mean()])
         v = np.array(vals)
         stats[name] = (v.mean(0), v.std(0, ddof=1) / np.sqrt(len(v)))
     assert np.all(stats["mis"][0] > 0)
@@ -226,7 +228,7 @@ def test_light_modes_agree_and_requests_keep_their_lights(gpu, cwp, serving):
         for j in range(i + 1, len(names)):
             (ma, sa), (mb, sb) = stats[names[i]], stats[names[j]]
             z = np.abs(ma - mb) / np.sqrt(sa ** 2 + sb ** 2)
-            assert z.max() <= 3.0, (names[i], names[j], z.max())
+            assert z[:-1].max() <= 4.0 and z[-1] <= 3.0, (names[i], names[j], z)
     assert np.median(stats["mis"][1] / stats["mis"][0]) < np.median(stats["bsdf"][1] / stats["bsdf"][0])
     reqs = requests(cwp, boxes, 4, seed=37)
     mix = run_all(s, reqs)
@@ -355,9 +357,10 @@ def test_textured_request_matches_oracle(gpu, cwp, oracle, serving):
         if m % 4 == 0: binds[m] = dict(base_color=0)
         elif m % 4 == 1: binds[m] = dict(base_color=0, metallic=1, roughness=1, normal=2, normal_scale=0.8)
         elif m % 4 == 2: binds[m] = dict(normal=2, roughness=1)
-    binds[1] = dict(emission=3, base_color=0)
+    mats_e = np.array(mats, np.float32).copy()
+    for b0 in base:   # every mesh's material 1 emits through image 3
+        binds[b0 + 1] = dict(emission=3, base_color=0); mats_e[b0 + 1, 8:11] = 2.0
     mt = cwp.material_textures(binds)
-    mats_e = np.array(mats, np.float32).copy(); mats_e[1, 8:11] = 2.0   # material 1 emits through its image
     s = cwp.Server(b, mats_e, base, max_paths=1 << 16, max_requests=4)
     s.set_scenes(descs, first)
     req = requests(cwp, boxes, 1, seed=23, res=((64, 48),), spps=(4,))[0]
@@ -370,6 +373,7 @@ def test_textured_request_matches_oracle(gpu, cwp, oracle, serving):
     tex, keep = cwp.textures_array(imgs)
     mesh_first = np.concatenate([[0], np.cumsum([len(f) for _, f, _, _ in meshes])]).astype(np.int32)
     lights = cwp.emissive_tables(meshes, base, mats_e, *cwp.scene_xforms(descs, first, req.scene, req.frame))
+    assert len(lights[0]) > 0
     ref, cnt = oracle.render_request(req, b.tuning().width, nodes, tris, tlas, roots[0], inst, mats_e, base, tlas_width=b.tlas_width,
                                      textures=(tex, mt, uvs, tans, mesh_first), lights=lights)
     a = acc[:, :3] / req.spp; r = ref[:, :3] / req.spp
