@@ -123,7 +123,7 @@ LIGHT_MIS, LIGHT_NEE, LIGHT_BSDF = 0, 1, 2
 
 
 class Texture(C.Structure):
-    _fields_ = [("rgba", C.c_void_p), ("w", C.c_int32), ("h", C.c_int32), ("srgb", C.c_int32), ("pad", C.c_int32)]
+    _fields_ = [("rgba", C.c_void_p), ("w", C.c_int32), ("h", C.c_int32), ("srgb", C.c_int32), ("nearest", C.c_int32)]
 
 
 class MaterialTextures(C.Structure):
@@ -131,12 +131,14 @@ class MaterialTextures(C.Structure):
                 ("metallic_ch", C.c_int32), ("roughness_ch", C.c_int32), ("normal_scale", C.c_float)]
 
 
-def textures_array(images):
-    """(cwp_texture array, the uint8 arrays it points into) from a list of (rgba uint8 [h, w, 4], srgb)"""
-    keep = [np.ascontiguousarray(img, np.uint8) for img, _ in images]
+def textures_array(images, nearest=False):
+    """(cwp_texture array, the uint8 arrays it points into) from a list of (rgba uint8 [h, w, 4], srgb); nearest: the
+    nearest texel instead of bilinear filtering for every image (the reference's --tex_filter nearest)"""
+    keep = [np.ascontiguousarray(img[0], np.uint8) for img in images]
     arr = (Texture * max(len(images), 1))()
-    for i, (img, (_, srgb)) in enumerate(zip(keep, images)):
-        arr[i].rgba, arr[i].w, arr[i].h, arr[i].srgb = img.ctypes.data, img.shape[1], img.shape[0], 1 if srgb else 0
+    for i, (img, spec) in enumerate(zip(keep, images)):
+        arr[i].rgba, arr[i].w, arr[i].h, arr[i].srgb = img.ctypes.data, img.shape[1], img.shape[0], 1 if spec[1] else 0
+        arr[i].nearest = 1 if nearest else 0
     return arr, keep
 
 
@@ -151,9 +153,9 @@ def material_textures(bindings):
     return arr
 
 
-def texture_sample_batch(images, ids, uv):
+def texture_sample_batch(images, ids, uv, nearest=False):
     """device lookups (texture id, (u, v)) -> rgba float32 [n, 4] with the textures bound as the server binds them"""
-    arr, keep = textures_array(images)
+    arr, keep = textures_array(images, nearest)
     ids = np.ascontiguousarray(ids, np.int32); uv = np.ascontiguousarray(uv, np.float32); out = np.zeros((len(ids), 4), np.float32)
     _check(lib().cwp_texture_sample_batch(arr, len(images), _iptr(ids), uv.ctypes.data, out.ctypes.data, len(ids)))
     return out
@@ -735,10 +737,11 @@ class Server:
         _check(lib().cwp_server_create(batch._h, M, len(M), _iptr(base), C.byref(o), C.byref(h)))
         self._h = h
 
-    def set_textures(self, images, bindings, uvs, tans=None):
+    def set_textures(self, images, bindings, uvs, tans=None, nearest=False):
         """images: list of (rgba uint8 [h, w, 4], srgb); bindings: cwp_material_textures array (material_textures);
-        uvs: float32 [n_tris, 8] over all batch meshes in mesh order; tans: float32 [n_tris, 12] or None"""
-        arr, keep = textures_array(images)
+        uvs: float32 [n_tris, 8] over all batch meshes in mesh order; tans: float32 [n_tris, 12] or None; nearest: the
+        nearest texel instead of bilinear filtering"""
+        arr, keep = textures_array(images, nearest)
         uvs = np.ascontiguousarray(uvs, np.float32)
         tans = np.ascontiguousarray(tans, np.float32) if tans is not None else None
         _check(lib().cwp_server_set_textures(self._h, arr, len(images), bindings, len(bindings), uvs.ctypes.data,

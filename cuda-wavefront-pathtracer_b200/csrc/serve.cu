@@ -498,8 +498,8 @@ static void free_textures(std::vector<cudaArray_t>& arrays, std::vector<cudaText
 static int make_textures(const cwp_texture* tex, int n, std::vector<cudaArray_t>& arrays, std::vector<cudaTextureObject_t>& objs) {
     for (int i = 0; i < n; i++) {
         const cwp_texture& T = tex[i];
-        CWPB_CHECK(T.rgba && T.w > 0 && T.h > 0 && T.w <= 32768 && T.h <= 32768 && (T.srgb == 0 || T.srgb == 1), CWP_ERR_INVALID,
-                   "texture %d: %dx%d, srgb %d", i, T.w, T.h, T.srgb);
+        CWPB_CHECK(T.rgba && T.w > 0 && T.h > 0 && T.w <= 32768 && T.h <= 32768 && (T.srgb == 0 || T.srgb == 1) && (T.nearest == 0 || T.nearest == 1),
+                   CWP_ERR_INVALID, "texture %d: %dx%d, srgb %d, nearest %d", i, T.w, T.h, T.srgb, T.nearest);
     }
     for (int i = 0; i < n; i++) {
         const cwp_texture& T = tex[i];
@@ -512,7 +512,7 @@ static int make_textures(const cwp_texture* tex, int n, std::vector<cudaArray_t>
         if (e == cudaSuccess) {
             cudaResourceDesc rd; memset(&rd, 0, sizeof rd); rd.resType = cudaResourceTypeArray; rd.res.array.array = arr;
             cudaTextureDesc td; memset(&td, 0, sizeof td);
-            td.addressMode[0] = td.addressMode[1] = cudaAddressModeWrap; td.filterMode = cudaFilterModeLinear;
+            td.addressMode[0] = td.addressMode[1] = cudaAddressModeWrap; td.filterMode = T.nearest ? cudaFilterModePoint : cudaFilterModeLinear;
             td.readMode = cudaReadModeNormalizedFloat; td.normalizedCoords = 1; td.sRGB = T.srgb;
             e = cudaCreateTextureObject(&o, &rd, &td, nullptr);
         }

@@ -394,14 +394,15 @@ int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* id);
 typedef struct cwp_envmap { const float* rgb; int32_t w, h; float strength; int32_t pad; } cwp_envmap;
 int cwp_server_set_envmaps(cwp_server* s, const cwp_envmap* maps, int32_t n);
 /* Material textures (glTF metallic-roughness; scene/texture.h:10-24): images are 8-bit RGBA, top row first, looked up
- * at (u, 1 - v) with bilinear filtering and wrap addressing, colour images (srgb = 1) decoded from sRGB. Material m's
+ * at (u, 1 - v) with bilinear filtering (nearest = 1: the nearest texel, the reference's --tex_filter nearest, which it
+ * applies to every image) and wrap addressing, colour images (srgb = 1) decoded from sRGB. Material m's
  * factors are multiplied by its bound images: base colour and emission by rgb, metallic and roughness by one channel;
  * a normal image perturbs the shading normal in the tangent frame. mtex has n_mtex entries (material index, as in the
  * server's table; materials beyond n_mtex are untextured). uvs: 2 float4 per triangle of every batch mesh in mesh
  * order, by mesh-local triangle index ((u0, v0, u1, v1), (u2, v2, -, -)); tans: 3 float4 per triangle (corner tangent
  * xyz, handedness sign w) or NULL (normal images then ignored). Replaces the texture set-up of the full integrator
  * (render/wavefront.cu:535-547, packAttributes in app/scene_setup.cpp:255). Only while no request is queued or running. */
-typedef struct cwp_texture { const uint8_t* rgba; int32_t w, h; int32_t srgb, pad; } cwp_texture;
+typedef struct cwp_texture { const uint8_t* rgba; int32_t w, h; int32_t srgb, nearest; } cwp_texture;
 typedef struct cwp_material_textures {
     int32_t base_color, emission, normal, metallic, roughness;   /* texture ids or -1 */
     int32_t metallic_ch, roughness_ch;                          /* channel of the metallic / roughness image (glTF: 2, 1) */

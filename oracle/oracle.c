@@ -1223,10 +1223,17 @@ static float o_env_pdf_texel(const OEnv* E, int x, int y, float v) {
  * frac(u) * w - 0.5, the four texels around it weighted by the fractional parts kept to 8 bits, channels read as
  * value / 255 and, for colour images, decoded from sRGB before the weighting. Images top row first, looked up at
  * (u, 1 - v). OTex and OMTex have the layouts of cwp_texture and cwp_material_textures. */
-typedef struct { const unsigned char* rgba; int w, h, srgb, pad; } OTex;
+typedef struct { const unsigned char* rgba; int w, h, srgb, nearest; } OTex;
 typedef struct { int base_color, emission, normal, metallic, roughness, metallic_ch, roughness_ch; float normal_scale; } OMTex;
 static float o_srgb(float c) { return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f); }
 static void o_tex(const OTex* T, float u, float v, float out[4]) {
+    if (T->nearest) {   /* point sampling: the texel containing (frac(u) w, frac(v) h) */
+        int i = (int)floorf((u - floorf(u)) * T->w), j = (int)floorf((v - floorf(v)) * T->h);
+        i = i < T->w ? i : T->w - 1; j = j < T->h ? j : T->h - 1;
+        const unsigned char* p = T->rgba + 4 * ((size_t)j * T->w + i);
+        for (int c = 0; c < 4; c++) { float x8 = p[c] / 255.f; if (T->srgb && c < 3) x8 = o_srgb(x8); out[c] = x8; }
+        return;
+    }
     const float x = (u - floorf(u)) * T->w - 0.5f, y = (v - floorf(v)) * T->h - 0.5f;
     const float fx = floorf(x), fy = floorf(y);
     const float a = rintf((x - fx) * 256.f) / 256.f, b = rintf((y - fy) * 256.f) / 256.f;

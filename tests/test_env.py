@@ -81,6 +81,8 @@ def test_oracle_texture_filtering(cwp, oracle):
     assert np.allclose(lin[0], img[1, 2] / 255.0, atol=1e-7)
     assert np.allclose(lin[1], (img[1, 2] / 255.0 + img[1, 3] / 255.0) / 2, atol=1e-6)
     assert np.allclose(lin[2], lin[0], atol=1e-7)                           # wrapped
+    near, keep2 = cwp.textures_array([(img, False)], nearest=True)
+    assert np.allclose(oracle.texture_sample(near, [0], uv[1:2])[0], img[1, 3] / 255.0, atol=1e-7)   # halfway: the texel right of the edge
     srgb = oracle.texture_sample(tex, [1], uv[:1])[0]
     c = img[1, 2, :3] / 255.0
     assert np.allclose(srgb[:3], np.where(c <= 0.04045, c / 12.92, ((c + 0.055) / 1.055) ** 2.4), atol=1e-6) and abs(srgb[3] - 1.0) < 1e-7

@@ -339,6 +339,13 @@ def test_texture_lookups_match_oracle(gpu, cwp, oracle):
     ref = oracle.texture_sample(tex, ids, uv)
     err = np.abs(got - ref)
     assert err.max() <= 2.5 / 255.0 and err.mean() < 1e-3
+    # nearest-texel lookups (the reference's --tex_filter nearest): the same texel except where a coordinate lies
+    # within rounding of a texel edge
+    got = cwp.texture_sample_batch(imgs, ids, uv, nearest=True)
+    tex, keep = cwp.textures_array(imgs, nearest=True)
+    ref = oracle.texture_sample(tex, ids, uv)
+    same = np.all(np.abs(got - ref) <= 1e-6, axis=1)
+    assert same.mean() >= 0.999
 
 
 def test_textured_request_matches_oracle(gpu, cwp, oracle, serving):
