@@ -201,8 +201,16 @@ def test_light_modes_agree_and_requests_keep_their_lights(gpu, cwp, serving):
     sqrt(se_a^2 + se_b^2). The whole image's z stays <= 3; a region's z <= 4, the bound for 96 comparisons (16
     regions x 6 pairs) at a family-wise 1% with standard errors from 16 seeds (the reference's 3 is per comparison).
     MIS is less noisy than BSDF sampling. Requests of different scenes and frames in one mix give each
-    one's image alone (every slot reads its own request's light tables)."""
-    b, descs, first, mats, base, boxes = serving
+    one's image alone (every slot reads its own request's light tables).
+    The emissive boxes float 0.6 above the ground here. An emitter face coplanar with another surface (a box bottom
+    on the ground) leaks light into light sampling, in the reference's algorithm as in this one: a shadow ray starts
+    on the light point's side of the surface, below the ground for a point on the ground plane, and passes under the
+    walls. The estimators then disagree by design, so the check needs emitters clear of other surfaces."""
+    b0, descs, first, mats, base, boxes = serving
+    lifted = []
+    for v, f, fm, x in b0.meshes:
+        v = v.copy(); v[np.unique(f[fm == 1]), 2] += 0.6; lifted.append((v, f, fm, x))
+    b = cwp.Batch(lifted)
     em = _emissive(mats, base)
     s = cwp.Server(b, em, base, max_paths=1 << 21, max_requests=16)
     s.set_scenes(descs, first)
