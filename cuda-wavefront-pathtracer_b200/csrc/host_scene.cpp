@@ -161,6 +161,7 @@ void load_mtl(const std::string& path, Mesh& m, std::map<std::string, int>& ids)
         char nm[512]; float r, g, b;
         if (!strncmp(line, "newmtl", 6) && sscanf(line + 6, "%511s", nm) == 1) {
             cur = (int)(m.kd.size() / 3); ids[nm] = cur; m.kd.push_back(0.8f); m.kd.push_back(0.8f); m.kd.push_back(0.8f);
+            m.matName.resize((size_t)cur + 1); m.matName[cur] = nm;
         } else if (cur >= 0 && !strncmp(line, "Kd", 2) && sscanf(line + 2, "%f %f %f", &r, &g, &b) == 3) {
             m.kd[3 * cur] = r; m.kd[3 * cur + 1] = g; m.kd[3 * cur + 2] = b;
         }

@@ -13,6 +13,7 @@ struct Mesh {
     std::vector<float> v, n;
     std::vector<int> f, fm;
     std::vector<float> kd;
+    std::vector<std::string> matName;   // material names (OBJ newmtl order), empty for other formats
     size_t nv() const { return v.size() / 3; }
     size_t nt() const { return f.size() / 3; }
     bool hasN() const { return !n.empty() && n.size() == v.size(); }

@@ -200,3 +200,43 @@ def test_serving_vs_reference_full_integrator(gpu, cwp, tmp_path, case):
     db, floor = cwp.imageio.psnr(ours, ref), cwp.imageio.psnr(ours, other)
     print(json.dumps({"case": case, "psnr_vs_reference_db": db, "psnr_independent_seeds_db": floor}))
     assert db >= floor, (db, floor)
+
+
+def test_cli_scene_file_vs_reference(gpu, cwp, tmp_path):
+    """This library's command-line renderer and the reference's, on the same scene file, camera, lighting file and
+    environment map (emissive boxes, animated instances, frame 7, Blackman-Harris filter, both CLIs' defaults
+    otherwise): the images differ less than two of this CLI's renders with independent seeds do."""
+    import numpy as np
+    from conftest import golden
+    pt = os.path.join(REF_DIR, "pt")
+    ours = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "cuda-wavefront-pathtracer_b200", "pt")
+    if not os.path.exists(pt):
+        pytest.skip("oracle/_ref/pt not built")
+    meshes, descs, first, mats, base, boxes = cwp.serving_scenes(n_scenes=1, seed=9, tris=(500, 4000), instances=(6, 16), blas_per_scene=(2, 3))
+    mats = mats.copy()
+    for b0 in base:
+        mats[b0 + 1, 8:11] = (4.0, 3.0, 2.0)
+    scene = write_reference_scene(tmp_path, meshes, descs, first, mats, base, frames=30)
+    (_, req), = cwp.serving_requests(1, 100.0, boxes, seed=43, resolutions=[(96, 64)], spps=[256], max_depth=4, frames=30)
+    c = req.cam
+    c2w = [c.ax[0], c.ay[0], c.az[0], c.pos[0], c.ax[1], c.ay[1], c.az[1], c.pos[1], c.ax[2], c.ay[2], c.az[2], c.pos[2], 0, 0, 0, 1]
+    with open(tmp_path / "camera.json", "w") as fp:
+        fp.write('{"c2w_blender_zup": [' + ", ".join("%.9g" % x for x in c2w) + "]}\n")
+    g = golden("env.npz")
+    (tmp_path / "env.hdr").write_bytes(g["big_hdr"].tobytes())
+    W = cwp.workloads
+    with open(tmp_path / "lighting.json", "w") as fp:
+        json.dump({"sun_dir_to_light_world_zup": list(W.SUN_TO), "sun_irradiance_W_m2": W.SUN_E, "sun_angle_rad": W.SUN_ANGLE_RAD,
+                   "sky_radiance_rgb_linear": list(W.SKY), "env_map": str(tmp_path / "env.hdr"), "env_strength": 1.5, "env_rotation_deg": 30.0}, fp)
+    args = ["--scene", scene, "--frame_start", "7", "--frames", "1", "--camera", str(tmp_path / "camera.json"), "--lighting", str(tmp_path / "lighting.json"),
+            "--hfov", str(W.HFOV), "--width", "96", "--height", "64", "--spp", "256", "--batch", "64", "--bounces", "4", "--variant", "bvh2", "--warm", "0"]
+    subprocess.run([pt] + args + ["--seed", "11", "--out", str(tmp_path / "ref")], check=True, capture_output=True, text=True, timeout=600)
+    for seed, name in ((11, "ours"), (12, "other")):
+        r = subprocess.run([ours] + args + ["--seed", str(seed), "--out", str(tmp_path / name)], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+    line = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")][-1]
+    assert line["integrator"] == "full" and line["env"] == 1 and line["frame"] == 7 and line["rays_total"] > 0
+    ref, a, b = (cwp.imageio.read_pfm(str(tmp_path / f"{n}.pfm")) for n in ("ref", "ours", "other"))
+    db, floor = cwp.imageio.psnr(a, ref), cwp.imageio.psnr(a, b)
+    print(json.dumps({"cli_psnr_vs_reference_db": db, "cli_psnr_independent_seeds_db": floor}))
+    assert db >= floor, (db, floor)
