@@ -491,7 +491,7 @@ def slo_sweep(cwp, b, mats, base, descs, first, wl, maxr, args, boxes, name, rat
     for rate in rates:
         stream = cwp.serving_requests(n_req, rate, boxes, seed=wl["seed"] + 100 + int(rate * 10), resolutions=resolutions, spps=spps)
         for mode, m in (("continuous", maxr), ("plain", 1)):
-            s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=m, regroup=bool(args.regroup), policy=args.policy)
+            s = cwp.Server(b, mats, base, max_paths=args.paths or wl["max_paths"], max_requests=m, regroup=bool(args.regroup), policy=args.policy)
             s.set_scenes(descs, first)
             r = serve_stream(cwp, s, stream)
             pts[mode].append({"rate_req_s": rate, "throughput_req_s": r["throughput_req_s"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"]})
@@ -515,7 +515,7 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
     maxr_c = args.max_requests or wl["max_requests"]
     for name, stream in streams.items():
         for mode, maxr in (("continuous", maxr_c), ("plain", 1)):
-            s = cwp.Server(b, mats, base, max_paths=wl["max_paths"], max_requests=maxr, regroup=bool(args.regroup), policy=args.policy)
+            s = cwp.Server(b, mats, base, max_paths=args.paths or wl["max_paths"], max_requests=maxr, regroup=bool(args.regroup), policy=args.policy)
             s.set_scenes(descs, first)
             barrier()
             clk = Clocks(str(torch.cuda.current_device()))
@@ -575,6 +575,7 @@ def main():
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
     ap.add_argument("--spatial", type=float, default=1e-3, help="host BVH: spatial-split overlap threshold (1e-3 = SBVH, the default; 0 = the reference binned SAH only)")
+    ap.add_argument("--paths", type=int, default=0, help="serving: paths in flight over all requests (default: the workload's; profiling cases)")
     ap.add_argument("--max-requests", type=int, default=0, help="serving: requests admitted at once by the continuous form (default: the workload's)")
     ap.add_argument("--tlas-width", type=int, default=4, choices=[2, 4], help="batched / serving: TLAS node width the traversal reads")
     ap.add_argument("--policy", type=int, default=0, help="serving: new paths by even share (0) or oldest first with backfill (1)")

@@ -198,9 +198,12 @@ def test_light_modes_agree_and_requests_keep_their_lights(gpu, cwp, serving):
     sampling alone and MIS with Russian roulette converge to the same image. The reference's consistency check
     (tests/mis_consistency.py:1-6) restated: 16 independent seeds per mode, the mean luminance of every region of a
     4x4 grid per seed, per mode its mean and standard error over the seeds, every pair of modes z = |a - b| /
-    sqrt(se_a^2 + se_b^2). The whole image's z stays <= 3; a region's z <= 4, the bound for 96 comparisons (16
-    regions x 6 pairs) at a family-wise 1% with standard errors from 16 seeds (the reference's 3 is per comparison).
-    MIS is less noisy than BSDF sampling. Requests of different scenes and frames in one mix give each
+    sqrt(se_a^2 + se_b^2). The whole image's z stays <= 3 for every pair. Per region, z <= 4 (the bound for 48
+    comparisons at a family-wise 1% with standard errors from 16 seeds; the reference's 3 is per comparison) for the
+    pairs among MIS, BSDF sampling and MIS with roulette. NEE alone is left out of the regional test: its
+    contribution grows as 1 / distance^2 for shading points near an emitter, so its variance is unbounded and a
+    standard-error test does not apply (16 seeds of one region gave z = 5.6 against MIS, 64 seeds z = 0.35). MIS is
+    less noisy than BSDF sampling. Requests of different scenes and frames in one mix give each
     one's image alone (every slot reads its own request's light tables).
     The emissive boxes float 0.6 above the ground here. An emitter face coplanar with another surface (a box bottom
     on the ground) leaks light into light sampling, in the reference's algorithm as in this one: a shadow ray starts
@@ -236,7 +239,9 @@ def test_light_modes_agree_and_requests_keep_their_lights(gpu, cwp, serving):
         for j in range(i + 1, len(names)):
             (ma, sa), (mb, sb) = stats[names[i]], stats[names[j]]
             z = np.abs(ma - mb) / np.sqrt(sa ** 2 + sb ** 2)
-            assert z[:-1].max() <= 4.0 and z[-1] <= 3.0, (names[i], names[j], z)
+            assert z[-1] <= 3.0, (names[i], names[j], z)
+            if "nee" not in (names[i], names[j]):
+                assert z[:-1].max() <= 4.0, (names[i], names[j], z)
     assert np.median(stats["mis"][1] / stats["mis"][0]) < np.median(stats["bsdf"][1] / stats["bsdf"][0])
     reqs = requests(cwp, boxes, 4, seed=37)
     mix = run_all(s, reqs)
@@ -348,12 +353,13 @@ def test_texture_lookups_match_oracle(gpu, cwp, oracle):
     err = np.abs(got - ref)
     assert err.max() <= 2.5 / 255.0 and err.mean() < 1e-3
     # nearest-texel lookups (the reference's --tex_filter nearest): the same texel except where a coordinate lies
-    # within rounding of a texel edge
+    # within rounding of a texel edge; linear images exactly, colour images within the hardware's sRGB decode
     got = cwp.texture_sample_batch(imgs, ids, uv, nearest=True)
     tex, keep = cwp.textures_array(imgs, nearest=True)
     ref = oracle.texture_sample(tex, ids, uv)
-    same = np.all(np.abs(got - ref) <= 1e-6, axis=1)
-    assert same.mean() >= 0.999
+    srgb = np.array([bool(sp) for _, sp in imgs])[ids]
+    err = np.abs(got - ref).max(axis=1)
+    assert (err[~srgb] <= 1e-6).mean() >= 0.999 and (err[srgb] <= 2.5 / 255.0).mean() >= 0.999
 
 
 def test_textured_request_matches_oracle(gpu, cwp, oracle, serving):
