@@ -240,6 +240,7 @@ SIGNATURES = {
     "cwp_server_create": (C.c_int, [C.c_void_p, C.POINTER(Material), C.c_int32, C.POINTER(C.c_int32), C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
     "cwp_server_destroy": (None, [C.c_void_p]),
     "cwp_server_set_scenes": (C.c_int, [C.c_void_p, C.POINTER(InstanceDesc), C.c_int64, C.POINTER(C.c_int32), C.c_int32]),
+    "cwp_server_set_instance_xforms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "cwp_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_int64)]),
     "cwp_server_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "cwp_server_poll": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_int32)]),
@@ -758,6 +759,19 @@ class Server:
     def set_scenes(self, descs, scene_first):
         first = np.ascontiguousarray(scene_first, np.int32)
         _check(lib().cwp_server_set_scenes(self._h, descs, len(descs), _iptr(first), len(first) - 1))
+
+    def set_instance_xforms(self, per_desc):
+        """per descriptor: a [k, 12] array of 3x4 matrices by frame (the last held), or None for its animation
+        parameters; None clears them"""
+        if per_desc is None:
+            _check(lib().cwp_server_set_instance_xforms(self._h, None, None, None, 0)); return
+        first, count, rows = [], [], []
+        for x in per_desc:
+            x = np.zeros((0, 12), np.float32) if x is None else np.asarray(x, np.float32).reshape(-1, 12)
+            first.append(sum(len(r) for r in rows)); count.append(len(x)); rows.append(x)
+        xf = np.ascontiguousarray(np.concatenate(rows) if rows else np.zeros((0, 12), np.float32))
+        f = np.array(first, np.int32); c = np.array(count, np.int32)
+        _check(lib().cwp_server_set_instance_xforms(self._h, xf.ctypes.data if len(xf) else None, f.ctypes.data, c.ctypes.data, len(per_desc)))
 
     def submit(self, req):
         i = C.c_int64(); _check(lib().cwp_server_submit(self._h, C.byref(req), C.byref(i))); return i.value

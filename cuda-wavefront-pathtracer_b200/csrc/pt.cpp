@@ -7,9 +7,10 @@
 //   files, materials files with non-Lambertian or emissive entries, environment maps, Russian roulette, or
 //   --integrator full) through the library's serving form: instanced scene files with animated instances and per-mesh
 //   materials files, or one mesh as a single identity instance, one request per frame. Not provided: the sphere scene
-//   (--synthetic), the Assimp loader and image textures (no image decoder here), matrix-valued scene instances, the viewer.
+//   (--synthetic), the Assimp loader and the image textures it reads (a third-party library), the viewer.
 #include "cwp_b200.h"
 #include "host_scene.h"
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -163,6 +164,7 @@ std::vector<cwp_material> mesh_materials(const cwpb::Mesh& m, const std::vector<
 struct FullScene {
     std::vector<cwpb::Mesh> meshes; std::vector<std::vector<cwp_material>> mats;
     std::vector<cwp_instance_desc> inst; int frames = 1;
+    std::vector<std::vector<float>> xf;   // per instance: 3x4 matrices by frame ("transform" / "transforms"), or empty
 };
 
 // scene file (scene/instances.cpp:19-47): meshes with their materials files, parametric animated instances
@@ -189,7 +191,23 @@ bool load_scene(const std::string& path, const Args& A, FullScene& S) {
         S.mats.push_back(mesh_materials(mesh, fileMats)); S.meshes.push_back(std::move(mesh));
     }
     for (const Json& o : is->arr) {
-        if (o.at("transform") || o.at("transforms")) { fprintf(stderr, "scene file: matrix-valued instances (\"transform\" / \"transforms\") are not supported by this build\n"); return false; }
+        // a fixed matrix or one per frame (12 or 16 numbers each, the first 12 used; scene/instances.cpp:8-12, 36-40)
+        std::vector<float> xf;
+        if (o.at("transform")) {
+            std::vector<double> v = o.numbers("transform");
+            if (v.size() != 12 && v.size() != 16) { fprintf(stderr, "scene file: transform needs 12 or 16 numbers\n"); return false; }
+            for (int k = 0; k < 12; k++) xf.push_back((float)v[k]);
+        }
+        if (const Json* tf = o.at("transforms")) {
+            std::vector<float> per;
+            for (const Json& t : tf->arr) {
+                std::vector<double> v; for (const Json& x : t.arr) v.push_back(x.num);
+                if (v.size() != 12 && v.size() != 16) { fprintf(stderr, "scene file: transforms entries need 12 or 16 numbers\n"); return false; }
+                for (int k = 0; k < 12; k++) per.push_back((float)v[k]);
+            }
+            if (!per.empty()) xf = per;   // per-frame matrices take precedence over a fixed one
+        }
+        S.xf.push_back(xf);
         cwp_instance_desc d{}; d.mesh = (int)o.number("mesh", 0);
         if (d.mesh < 0 || d.mesh >= (int)S.meshes.size()) { fprintf(stderr, "scene file: instance mesh %d out of range\n", d.mesh); return false; }
         auto v3 = [&](const char* k, float* out, float def, bool scalar) {
@@ -276,8 +294,11 @@ int run_full(Args& A, const std::string& envFromLighting, float envStrengthL, fl
     }
     // the frame-0 world box of every instance's vertices gives the ray offset (scene_setup.cpp:107, 153-155)
     float lo[3] = { 1e30f, 1e30f, 1e30f }, hi[3] = { -1e30f, -1e30f, -1e30f };
-    for (auto& d : S.inst) {
-        float x[12]; if (cwp_xform_animate(&d, 0, x)) return fail("instance");
+    for (size_t i = 0; i < S.inst.size(); i++) {
+        const cwp_instance_desc& d = S.inst[i];
+        float x[12];
+        if (i < S.xf.size() && !S.xf[i].empty()) std::copy(S.xf[i].begin(), S.xf[i].begin() + 12, x);
+        else if (cwp_xform_animate(&d, 0, x)) return fail("instance");
         const cwpb::Mesh& m = S.meshes[d.mesh];
         for (size_t i = 0; i < m.v.size(); i += 3)
             for (int r = 0; r < 3; r++) {
@@ -305,6 +326,12 @@ int run_full(Args& A, const std::string& envFromLighting, float envStrengthL, fl
     if (cwp_server_create(B, mats.data(), (int32_t)mats.size(), base.data(), &so, &Srv)) return fail("server");
     const int32_t first[2] = { 0, (int32_t)S.inst.size() };
     if (cwp_server_set_scenes(Srv, S.inst.data(), (int64_t)S.inst.size(), first, 1)) return fail("scene");
+    bool anyXf = false; for (auto& x : S.xf) anyXf = anyXf || !x.empty();
+    if (anyXf) {
+        std::vector<float> all; std::vector<int32_t> fx, nx;
+        for (auto& x : S.xf) { fx.push_back((int32_t)(all.size() / 12)); nx.push_back((int32_t)(x.size() / 12)); all.insert(all.end(), x.begin(), x.end()); }
+        if (cwp_server_set_instance_xforms(Srv, all.data(), fx.data(), nx.data(), (int64_t)nx.size())) return fail("instance matrices");
+    }
     const std::string envPath = !A.env.empty() ? A.env : envFromLighting;
     const float envStrength = A.envStrength >= 0.f ? A.envStrength : envStrengthL, envRot = A.envRot > -1e29f ? A.envRot : envRotL;
     if (!envPath.empty()) {

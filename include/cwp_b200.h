@@ -386,6 +386,12 @@ void cwp_server_destroy(cwp_server* s);
 /* Scenes: scene k owns instance descriptors [scene_first[k], scene_first[k + 1]) (cwp_xform_animate at the request's
  * frame gives their transforms); replaces the batch's scenes while the server lives. */
 int cwp_server_set_scenes(cwp_server* s, const cwp_instance_desc* desc, int64_t n, const int32_t* scene_first, int32_t n_scenes);
+/* Instances placed by 3x4 matrices instead of animation parameters (scene files' "transform" and "transforms" keys;
+ * instanceXform, scene/instances.cpp:50-51): descriptor i of the scenes uses xforms[first_xf[i] .. first_xf[i] +
+ * n_xf[i]) (12 floats each, row-major object to world), frame f taking entry min(f, n_xf[i] - 1); n_xf[i] = 0 keeps
+ * its animation parameters. n = the descriptor count of cwp_server_set_scenes; NULL arrays clear the matrices. Only
+ * while no request is queued or running. */
+int cwp_server_set_instance_xforms(cwp_server* s, const float* xforms, const int32_t* first_xf, const int32_t* n_xf, int64_t n);
 int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* id);
 /* Environment maps the requests may name (cwp_request.env): equirectangular, row 0 = +z, the centre column facing +x
  * (the reference's orientation, scene/environment.h:1-4); rgb = w x h x 3 linear floats scaled by strength. Replaces

@@ -35,9 +35,12 @@ def test_scene_file_errors(tmp_path):
     ply.write_text("ply\nformat ascii 1.0\nelement vertex 3\nproperty float x\nproperty float y\nproperty float z\n"
                    "element face 1\nproperty list uchar int vertex_indices\nend_header\n0 0 0\n1 0 0\n0 1 0\n3 0 1 2\n")
     s = tmp_path / "s.json"
-    s.write_text(json.dumps({"meshes": [{"file": "q.ply"}], "instances": [{"mesh": 0, "transform": [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0]}]}))
+    s.write_text(json.dumps({"meshes": [{"file": "q.ply"}], "instances": [{"mesh": 0, "transform": [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1]}]}))
     rc, err = run("--scene", s)
-    assert rc == 1 and "matrix-valued instances" in err
+    assert rc == 1 and "transform needs 12 or 16 numbers" in err
+    s.write_text(json.dumps({"meshes": [{"file": "q.ply"}], "instances": [{"mesh": 0, "transforms": [[1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0], [1, 0]]}]}))
+    rc, err = run("--scene", s)
+    assert rc == 1 and "transforms entries need 12 or 16 numbers" in err
     s.write_text(json.dumps({"meshes": [{"file": "q.ply"}], "instances": [{"mesh": 3}]}))
     rc, err = run("--scene", s)
     assert rc == 1 and "instance mesh 3 out of range" in err

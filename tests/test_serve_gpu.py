@@ -335,6 +335,41 @@ def test_camera_options_match_oracle(gpu, cwp, oracle, serving):
         s.submit(bad)
 
 
+def test_instance_matrices_match_animation(gpu, cwp, serving):
+    """Instances placed by per-frame matrices (scene files' "transforms") render as the animation parameters
+    that produced the matrices; past the last matrix the last one holds; a fixed matrix ("transform") for every
+    frame; clearing the matrices restores the animation."""
+    b, descs, first, mats, base, boxes = serving
+    s = server(cwp, serving, max_paths=1 << 16, max_requests=2)
+    ref_s = server(cwp, serving, max_paths=1 << 16, max_requests=2)
+    n = len(descs)
+    per = [np.stack([cwp.scene_xforms(descs, [0, n], 0, f)[0][i] for f in range(12)]) for i in range(n)]
+    s.set_instance_xforms(per)
+    req = requests(cwp, boxes, 1, seed=51, res=((48, 32),), spps=(2,))[0]
+    req.frame = 5
+    (a, _), = run_all(s, [req])
+    (r, _), = run_all(ref_s, [req])
+    assert np.allclose(a, r, rtol=1e-4, atol=1e-5)   # up to the order of float atomics
+    req.frame = 20   # past the 12 matrices: frame 11's placement
+    (a, _), = run_all(s, [req])
+    req.frame = 11
+    (r, _), = run_all(ref_s, [req])
+    assert np.allclose(a, r, rtol=1e-4, atol=1e-5)   # up to the order of float atomics
+    s.set_instance_xforms([p[3:4] for p in per])   # one fixed matrix each: frame 3's placement at any frame
+    req.frame = 9
+    (a, _), = run_all(s, [req])
+    req.frame = 3
+    (r, _), = run_all(ref_s, [req])
+    assert np.allclose(a, r, rtol=1e-4, atol=1e-5)   # up to the order of float atomics
+    s.set_instance_xforms(None)
+    req.frame = 9
+    (a, _), = run_all(s, [req])
+    (r, _), = run_all(ref_s, [req])
+    assert np.allclose(a, r, rtol=1e-4, atol=1e-5)   # up to the order of float atomics
+    with pytest.raises(cwp.CwpError):
+        s.set_instance_xforms(per[:-1])   # one range per descriptor
+
+
 def test_texture_lookups_match_oracle(gpu, cwp, oracle):
     """Hardware bilinear lookups (wrap, normalised coordinates, sRGB decode for colour images) against the oracle's
     restatement of the documented filtering rule, over odd image sizes and coordinates wrapping over several periods.
