@@ -183,6 +183,8 @@ SIGNATURES = {
     "cwp_version": (C.c_int32, []),
     "cwp_mesh_box_field": (C.c_int, [C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]),
     "cwp_mesh_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "cwp_mesh_sphere_grid": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "cwp_sphere_grid_c2w": (None, [C.POINTER(C.c_float)]),
     "cwp_mesh_from_view": (C.c_int, [C.POINTER(MeshView), C.POINTER(C.c_void_p)]),
     "cwp_mesh_view_of": (C.c_int, [C.c_void_p, C.POINTER(MeshView)]),
     "cwp_mesh_write_ply": (C.c_int, [C.c_void_p, C.c_char_p]),
@@ -297,6 +299,13 @@ class Mesh:
     def box_field(cls, n_boxes, seed=1):
         h = C.c_void_p()
         _check(lib().cwp_mesh_box_field(n_boxes, seed, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def sphere_grid(cls, grid, nu=200, nv=100, ground=200):
+        """The reference's synthetic scene (scene/synthetic.cpp:6-48); the defaults are its CLI's (2.0 M tris at 7)."""
+        h = C.c_void_p()
+        _check(lib().cwp_mesh_sphere_grid(grid, nu, nv, ground, C.byref(h)))
         return cls(h.value)
 
     @classmethod
@@ -432,6 +441,13 @@ class Accel:
     def __del__(self):
         if _lib is not None:
             self.close()
+
+
+def sphere_grid_c2w():
+    """Row-major camera-to-world matrix of the synthetic scene's default view (scene/synthetic.cpp:50)."""
+    m = (C.c_float * 16)()
+    lib().cwp_sphere_grid_c2w(m)
+    return np.array(m[:], np.float32).reshape(4, 4)
 
 
 def camera_look_at(pos, target, up, hfov_deg, w, h):

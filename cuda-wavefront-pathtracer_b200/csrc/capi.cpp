@@ -33,6 +33,19 @@ extern "C" int cwp_mesh_box_field(int32_t n_boxes, uint64_t seed, cwp_mesh** out
     *out = h; return CWP_OK;
 }
 
+extern "C" int cwp_mesh_sphere_grid(int32_t grid, int32_t nu, int32_t nv, int32_t ground, cwp_mesh** out) {
+    CWPB_CHECK(out, CWP_ERR_INVALID, "out is NULL");
+    CWPB_CHECK(grid >= 0 && grid <= 64 && nu >= 3 && nu <= 4096 && nv >= 2 && nv <= 4096 && ground >= 1 && ground <= 8192,
+               CWP_ERR_INVALID, "sphere grid %d, %d x %d quads, ground %d out of range", grid, nu, nv, ground);
+    CWPB_CHECK((int64_t)grid * grid * nu * (nv + 1) + (int64_t)(ground + 1) * (ground + 1) < (1ll << 31), CWP_ERR_INVALID,
+               "sphere grid has more than 2^31 vertices");
+    cwp_mesh* h = new cwp_mesh();
+    sphere_grid(grid, nu, nv, ground, h->m);
+    *out = h; return CWP_OK;
+}
+
+extern "C" void cwp_sphere_grid_c2w(float c2w[16]) { if (c2w) sphere_grid_c2w(c2w); }
+
 extern "C" int cwp_mesh_load(const char* path, cwp_mesh** out) {
     CWPB_CHECK(path && out, CWP_ERR_INVALID, "NULL argument");
     cwp_mesh* h = new cwp_mesh(); std::string err;

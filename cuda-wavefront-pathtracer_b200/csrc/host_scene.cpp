@@ -48,6 +48,63 @@ void box_field(int nBoxes, uint64_t seed, float half, float edgeLo, float edgeHi
     m.kd = { 0.8f, 0.8f, 0.8f };
 }
 
+// Sphere grid (scene/synthetic.cpp:6-48): the geometry must be the reference's to the bit, so every expression below
+// keeps its operand order (float, left to right, no fused multiply-add on the host).
+void sphere_grid(int grid, int nu, int nv, int ground, Mesh& m) {
+    m = Mesh();
+    m.kd = { 0.5f, 0.5f, 0.5f,  0.8f, 0.3f, 0.2f,  0.2f, 0.6f, 0.3f,  0.25f, 0.35f, 0.8f,  0.8f, 0.8f, 0.8f };
+    const float half = 6.0f, pi = 3.14159265f;
+    auto vert = [&](float x, float y, float z) { m.v.push_back(x); m.v.push_back(y); m.v.push_back(z); };
+    auto tri = [&](int a, int b, int c, int mat) { m.f.push_back(a); m.f.push_back(b); m.f.push_back(c); m.fm.push_back(mat); };
+    // ground: (ground+1)^2 vertices over [-half, half]^2 with a low ripple in z, two triangles per cell
+    for (int row = 0; row <= ground; row++)
+        for (int col = 0; col <= ground; col++) {
+            const float x = -half + 2 * half * col / ground, y = -half + 2 * half * row / ground;
+            vert(x, y, 0.05f * sinf(1.3f * x) * cosf(1.7f * y));
+        }
+    const int stride = ground + 1;
+    for (int row = 0; row < ground; row++)
+        for (int col = 0; col < ground; col++) {
+            const int p00 = row * stride + col, p01 = p00 + 1, p10 = p00 + stride, p11 = p10 + 1;
+            tri(p00, p01, p11, 0); tri(p00, p11, p10, 0);
+        }
+    // spheres: nu longitudes x (nv + 1) latitude rings each (pole rings keep nu coincident vertices), radius bumped
+    // by a per-sphere phase, one of four colours in turn; the pole caps are single triangles per quad
+    const float pitch = 2 * half / (grid + 1), r0 = pitch * 0.33f;
+    for (int k = 0; k < grid * grid; k++) {
+        const int gx = k % grid, gy = k / grid;
+        const float cx = -half + pitch * (gx + 1), cy = -half + pitch * (gy + 1);
+        const float cz = r0 * (1.1f + 0.3f * ((k * 7) % 5) / 4.0f);
+        const float rad = r0 * (0.7f + 0.3f * ((k * 3) % 4) / 3.0f);
+        const int first = (int)m.nv();
+        for (int ring = 0; ring <= nv; ring++)
+            for (int seg = 0; seg < nu; seg++) {
+                const float th = pi * ring / nv, ph = 2 * pi * seg / nu;
+                const float s = rad * (1.0f + 0.12f * sinf(6 * th + k) * cosf(5 * ph + 0.5f * k));
+                const float dx = sinf(th) * cosf(ph), dy = sinf(th) * sinf(ph), dz = cosf(th);
+                vert(cx + dx * s, cy + dy * s, cz + dz * s);
+            }
+        const int mat = 1 + k % 4;
+        for (int ring = 0; ring < nv; ring++)
+            for (int seg = 0; seg < nu; seg++) {
+                const int next = (seg + 1) % nu;
+                const int a = first + ring * nu + seg, b = first + ring * nu + next;
+                const int c = a + nu, d = b + nu;
+                if (ring > 0) tri(a, c, b, mat);
+                if (ring < nv - 1) tri(b, c, d, mat);
+            }
+    }
+}
+
+void sphere_grid_c2w(float c2w[16]) {   // syntheticCamera (synthetic.cpp:50): from (0, -9.5, 6.5) at (0, 0, 0.4), z up
+    const float3 pos = f3(0.f, -9.5f, 6.5f), fwd = normalize(f3(0.f, 0.f, 0.4f) - pos);
+    const float3 right = normalize(cross(fwd, f3(0.f, 0.f, 1.f))), up = cross(right, fwd), back = -fwd;
+    const float3 axes[3] = { right, up, back };
+    for (int j = 0; j < 16; j++) c2w[j] = (j % 5 == 0) ? 1.f : 0.f;
+    for (int col = 0; col < 3; col++) { c2w[col] = axes[col].x; c2w[4 + col] = axes[col].y; c2w[8 + col] = axes[col].z; }
+    c2w[3] = pos.x; c2w[7] = pos.y; c2w[11] = pos.z;
+}
+
 // ---------------- PLY ----------------
 namespace {
 struct PlyProp { std::string name, type, countType, itemType; bool list = false; };

@@ -26,6 +26,12 @@ struct Mesh {
 // 2 half x 2 half two-triangle ground plane. Deterministic for a given seed (splitmix64 stream).
 void box_field(int nBoxes, uint64_t seed, float half, float edgeLo, float edgeHi, Mesh& out);
 
+// The reference's procedural scene (scene/synthetic.h:6-8): a ground of ground x ground quads over [-6, 6]^2 and a
+// grid x grid array of bumpy spheres of nu x nv quads, 2 (ground^2 + grid^2 nu (nv - 1)) triangles, five albedos
+// (ground, then four sphere colours). sphere_grid_c2w gives its default view (row-major camera-to-world).
+void sphere_grid(int grid, int nu, int nv, int ground, Mesh& out);
+void sphere_grid_c2w(float c2w[16]);
+
 bool load_ply(const std::string& path, Mesh& m, std::string* err);
 bool load_obj(const std::string& path, Mesh& m, std::string* err);
 bool load_mesh(const std::string& path, Mesh& m, std::string* err);   // by extension

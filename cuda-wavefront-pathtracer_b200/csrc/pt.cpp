@@ -6,8 +6,9 @@
 //   Moller-Trumbore triangles, CUDA-graph or host-loop frames; and the full integrator (setupScene's rule: scene
 //   files, materials files with non-Lambertian or emissive entries, environment maps, Russian roulette, or
 //   --integrator full) through the library's serving form: instanced scene files with animated instances and per-mesh
-//   materials files, or one mesh as a single identity instance, one request per frame. Not provided: the sphere scene
-//   (--synthetic), the Assimp loader and the image textures it reads (a third-party library), the viewer.
+//   materials files, or one mesh as a single identity instance, one request per frame. --synthetic N generates the
+//   reference's sphere-grid scene (N x N spheres, 200 x 100 quads each, 200 x 200 ground) with its default view. Not
+//   provided: the Assimp loader and the image textures it reads (a third-party library), the viewer.
 #include "cwp_b200.h"
 #include "host_scene.h"
 #include <algorithm>
@@ -29,7 +30,7 @@ struct Args {
     std::string scene, materials, env, lightSampling = "mis", texFilter = "linear", envSampling = "importance", loader = "auto";
     int frames = 0, frameStart = 0, flatten = 0, rr = 0, rrDepth = 3, gdEnergy = 1, bumpShadow = 0;
     float envStrength = -1.f, envRot = -1e30f;
-    int fuse = -1, leaf = 4, batch = 64, boxes = 0, frame = 0, w = 512, h = 512, spp = 256, bounces = 8, persistent = 0, filterBH = 1, smooth = 1;
+    int fuse = -1, leaf = 4, batch = 64, boxes = 0, synthetic = 0, frame = 0, w = 512, h = 512, spp = 256, bounces = 8, persistent = 0, filterBH = 1, smooth = 1;
     int warm = 8, yupToZup = -1, reps = 1, devloop = 0, sort = 0, graph = -1, bins = 16, threads = 0;
     float fx = 0, fy = 0, hfov = 0, epsScale = 1e-4f, nearClip = 0.f, sunAngleDeg = 0.526f, aperture = -1.f, focusDist = -1.f;
     unsigned seed = 1000;
@@ -62,7 +63,7 @@ bool parse(int argc, char** argv, Args& A) {
         else if (k == "--rr") A.rr = I(); else if (k == "--rr_depth") A.rrDepth = I(); else if (k == "--gd_energy") A.gdEnergy = I(); else if (k == "--bump_shadow") A.bumpShadow = I();
         else if (k == "--tex_filter") A.texFilter = S(); else if (k == "--textures") S(); else if (k == "--loader") A.loader = S(); else if (k == "--env_sampling") A.envSampling = S();
         else if (k == "--frames") A.frames = I(); else if (k == "--frame_start") A.frameStart = I(); else if (k == "--flatten") A.flatten = I();
-        else if (k == "--synthetic") { fprintf(stderr, "--synthetic: the sphere scene is not provided by this build\n"); return false; }
+        else if (k == "--synthetic") A.synthetic = I();
         else { fprintf(stderr, "unknown arg %s\n", argv[i]); return false; }
     }
     if (A.integrator != "auto" && A.integrator != "legacy" && A.integrator != "full") { fprintf(stderr, "--integrator must be auto, legacy or full\n"); return false; }
@@ -248,6 +249,7 @@ bool camera_c2w(Args& A, float c2w[16]) {
         if (A.focusDist < 0.f && C.at("focus_distance")) A.focusDist = (float)C.number("focus_distance", 0);
     }
     if (!A.c2w.empty()) { std::string s = A.c2w; for (char& ch : s) if (ch == ',') ch = ' '; const char* p = s.c_str(); char* e; for (int j = 0; j < 16; j++) { c2w[j] = (float)strtod(p, &e); p = e; } haveC2w = true; }
+    if (!haveC2w && A.synthetic > 0) { cwp_sphere_grid_c2w(c2w); haveC2w = true; }   // scene_setup.cpp:94
     if (!haveC2w && A.boxes > 0) {   // box field without a camera: the benchmark view
         const float pos[3] = { 0.f, -34.f, 22.f }, tgt[3] = { 0.f, 0.f, 0.f }, up[3] = { 0.f, 0.f, 1.f }; cwp_camera c;
         if (A.hfov == 0 && A.fx == 0) A.hfov = 45.f;
@@ -270,8 +272,9 @@ int run_full(Args& A, const std::string& envFromLighting, float envStrengthL, fl
     else {
         cwpb::Mesh mesh; std::string err;
         if (A.boxes > 0) cwpb::box_field(A.boxes, 1, 20.f, 0.2f, 3.f, mesh);   // as cwp_mesh_box_field
+        else if (A.synthetic > 0) cwpb::sphere_grid(A.synthetic, 200, 100, 200, mesh);   // scene_setup.cpp:93
         else if (!cwpb::load_mesh(A.mesh, mesh, &err)) { fprintf(stderr, "%s: %s\n", A.mesh.c_str(), err.c_str()); return 1; }
-        if (A.yupToZup == 1) {
+        if (A.yupToZup == 1 && A.synthetic <= 0) {   // files only: the generated scenes are z-up
             for (size_t i = 0; i < mesh.v.size(); i += 3) { float y = mesh.v[i + 1], z = mesh.v[i + 2]; mesh.v[i + 1] = -z; mesh.v[i + 2] = y; }
             for (size_t i = 0; i < mesh.n.size(); i += 3) { float y = mesh.n[i + 1], z = mesh.n[i + 2]; mesh.n[i + 1] = -z; mesh.n[i + 2] = y; }
         }
@@ -376,7 +379,7 @@ int run_full(Args& A, const std::string& envFromLighting, float envStrengthL, fl
             printf("{\"rep\":%d,\"integrator\":\"full\",\"scene\":\"%s\",\"tris\":%zu,\"instances\":%zu,\"frame\":%d,\"w\":%d,\"h\":%d,\"spp\":%d,\"bounces\":%d,"
                    "\"rays_closest\":%.0f,\"rays_shadow\":%.0f,\"rays_total\":%.0f,\"t_frame_ms\":%.2f,\"mrays_s_e2e\":%.1f,\"avg_path_len\":%.3f,\"light_sampling\":\"%s\","
                    "\"rr\":%d,\"env\":%d,\"filter\":\"%s\",\"seed\":%u,\"setup_s\":%.2f}\n",
-                   r, A.scene.empty() ? (A.boxes > 0 ? "boxes" : A.mesh.c_str()) : A.scene.c_str(), nTris, S.inst.size(), f, A.w, A.h, A.spp, A.bounces,
+                   r, A.scene.empty() ? (A.boxes > 0 ? "boxes" : A.synthetic > 0 ? "synthetic" : A.mesh.c_str()) : A.scene.c_str(), nTris, S.inst.size(), f, A.w, A.h, A.spp, A.bounces,
                    st.rays, st.shadow_rays, tot, ms, tot / (ms * 1e3), st.rays / ((double)N * A.spp), A.lightSampling.c_str(), R0.rr, R0.env >= 0,
                    A.filterBH ? "blackman-harris1.5" : "box", A.seed, setupS);
             fflush(stdout);
@@ -440,15 +443,16 @@ int main(int argc, char** argv) {
     // ---- scene ----
     cwp_mesh* mesh = nullptr;
     if (A.boxes > 0) { if (cwp_mesh_box_field(A.boxes, 1, &mesh)) return fail("box field"); }
+    else if (A.synthetic > 0) { if (cwp_mesh_sphere_grid(A.synthetic, 200, 100, 200, &mesh)) return fail("sphere grid"); }
     else if (!A.mesh.empty()) { if (cwp_mesh_load(A.mesh.c_str(), &mesh)) return fail("mesh"); }
-    else { fprintf(stderr, "no scene: give --mesh PATH or --boxes N\n"); return 1; }
+    else { fprintf(stderr, "no scene: give --mesh PATH, --boxes N or --synthetic N\n"); return 1; }
     cwp_mesh_view mv; cwp_mesh_view_of(mesh, &mv);
     std::vector<float> v(mv.verts, mv.verts + 3 * mv.n_verts), nrm, kd(mv.albedo, mv.albedo + 3 * mv.n_albedo);
     if (mv.normals) nrm.assign(mv.normals, mv.normals + 3 * mv.n_verts);
     std::vector<int> f(mv.faces, mv.faces + 3 * mv.n_tris), fm(mv.n_tris, 0);
     if (mv.face_mat) fm.assign(mv.face_mat, mv.face_mat + mv.n_tris);
     std::string ext = A.mesh.size() > 5 ? A.mesh.substr(A.mesh.size() - 5) : "";
-    if (A.yupToZup == 1) {   // y-up -> z-up: (x, y, z) -> (x, -z, y), scene_setup.cpp:65-67
+    if (A.yupToZup == 1 && A.synthetic <= 0) {   // y-up -> z-up: (x, y, z) -> (x, -z, y), scene_setup.cpp:65-67
         for (size_t i = 0; i < v.size(); i += 3) { float y = v[i + 1], z = v[i + 2]; v[i + 1] = -z; v[i + 2] = y; }
         for (size_t i = 0; i < nrm.size(); i += 3) { float y = nrm[i + 1], z = nrm[i + 2]; nrm[i + 1] = -z; nrm[i + 2] = y; }
     }
@@ -512,7 +516,7 @@ int main(int argc, char** argv) {
                "\"rays_total\":%.0f,\"t_trace_ms\":%.2f,\"t_frame_ms\":%.2f,\"mrays_s_trace\":%.1f,\"mrays_s_e2e\":%.1f,\"avg_path_len\":%.3f,\"vram_MB\":%.0f,\"pt_blocks\":%d,"
                "\"gpu\":\"%s\",\"filter\":\"%s\",\"smooth\":%d,\"seed\":%u,\"integrator\":\"legacy\",\"lens_r\":%.4f,\"focus_d\":%.4f,\"env_sampling\":\"importance\",\"textures\":0,"
                "\"builder\":\"sah\",\"collapse\":\"%s\",\"bvh_tree_ms\":%.2f,\"bvh_post_ms\":0.00,\"bvh_sah\":%.4f,\"graph\":%d,\"instances\":0,\"flatten\":0,\"frame\":%d,\"tlas_ms\":0.000,\"bins\":%d}\n",
-               r, V, A.tri.c_str(), A.persistent, A.devloop, A.sort, A.fuse < 0 ? 1 : A.fuse, reportLeaf, K, A.boxes > 0 ? "boxes" : A.mesh.c_str(), (long long)bd.n_tris,
+               r, V, A.tri.c_str(), A.persistent, A.devloop, A.sort, A.fuse < 0 ? 1 : A.fuse, reportLeaf, K, A.boxes > 0 ? "boxes" : A.synthetic > 0 ? "synthetic" : A.mesh.c_str(), (long long)bd.n_tris,
                (long long)(bd.n_node_float4 / bd.node_stride), (long long)(bd.n_node_float4 * 16), bd.max_depth, bvhS, A.w, A.h, A.spp, A.bounces, st.rays, st.shadow_rays,
                tot, st.trace_ms, st.frame_ms, tot / (st.trace_ms * 1e3), tot / (st.frame_ms * 1e3), st.rays / ((double)N * A.spp), info.vram_mb, info.pt_blocks, info.gpu_name,
                A.filterBH ? "blackman-harris1.5" : "box", P.has_n, A.seed, P.cam.lens_r, P.cam.focus_d, V == 8 ? A.collapse.c_str() : "-", bd.build_ms, bd.sah, A.graph, A.frame, A.bins);

@@ -49,6 +49,12 @@ typedef struct cwp_mesh_view {
 
 int cwp_mesh_box_field(int32_t n_boxes, uint64_t seed, cwp_mesh** out);
 int cwp_mesh_load(const char* path, cwp_mesh** out);
+/* The reference's procedural scene, makeSynthetic (scene/synthetic.h:6, synthetic.cpp:6-48), vertex for vertex: a
+ * ground of ground x ground quads and grid x grid bumpy spheres of nu x nv quads, five albedos. The reference's CLI
+ * uses nu = 200, nv = 100, ground = 200 (app/scene_setup.cpp:93): 2,000,000 triangles at grid = 7.
+ * cwp_sphere_grid_c2w replaces syntheticCamera (synthetic.h:8): its row-major camera-to-world matrix. */
+int cwp_mesh_sphere_grid(int32_t grid, int32_t nu, int32_t nv, int32_t ground, cwp_mesh** out);
+void cwp_sphere_grid_c2w(float c2w[16]);
 int cwp_mesh_from_view(const cwp_mesh_view* v, cwp_mesh** out);
 int cwp_mesh_view_of(const cwp_mesh* m, cwp_mesh_view* out);
 int cwp_mesh_write_ply(const cwp_mesh* m, const char* path);

@@ -17,6 +17,8 @@
 #include "core/rng.h"
 #include "scene/instances.h"
 #include "scene/environment.h"
+#include "scene/synthetic.h"
+#include "scene/camera.h"
 #include "io/hdr_image.h"
 #include "render/bsdf.h"
 #include "core/sampling.h"
@@ -265,4 +267,16 @@ extern "C" int ref_env_build(const char* path, float strength, int* w, int* h, f
     if (marg) memcpy(marg, E.marg.data(), E.marg.size() * sizeof(float));
     if (cond) memcpy(cond, E.cond.data(), E.cond.size() * sizeof(float));
     return 0;
+}
+
+// the reference's makeSynthetic + syntheticCamera: counts first (v/f/fm/kd NULL), then the arrays; c2w may be NULL
+extern "C" void ref_synthetic(int grid, int nu, int nv, int gs, long* nverts, long* ntris, float* v, int* f, int* fm, float* kd, float* c2w) {
+    Mesh M;
+    makeSynthetic(M, grid, nu, nv, gs);
+    *nverts = (long)M.v.size(); *ntris = (long)M.f.size();
+    if (v) for (size_t i = 0; i < M.v.size(); i++) { v[3 * i] = M.v[i].x; v[3 * i + 1] = M.v[i].y; v[3 * i + 2] = M.v[i].z; }
+    if (f) for (size_t i = 0; i < M.f.size(); i++) { f[3 * i] = M.f[i].x; f[3 * i + 1] = M.f[i].y; f[3 * i + 2] = M.f[i].z; }
+    if (fm) memcpy(fm, M.fm.data(), M.fm.size() * sizeof(int));
+    if (kd) for (size_t i = 0; i < M.kd.size(); i++) { kd[3 * i] = M.kd[i].x; kd[3 * i + 1] = M.kd[i].y; kd[3 * i + 2] = M.kd[i].z; }
+    if (c2w) syntheticCamera(c2w);
 }

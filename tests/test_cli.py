@@ -17,7 +17,6 @@ def run(*args):
 
 
 @pytest.mark.parametrize("args,msg", [
-    (["--synthetic", "1"], "sphere scene is not provided"),
     (["--scene", "s.json", "--materials", "m.json"], "per mesh in scene files"),
     (["--loader", "assimp"], "only the built-in PLY / OBJ loader"),
     (["--light_sampling", "all"], "--light_sampling must be"),
