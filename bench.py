@@ -139,21 +139,64 @@ def reference_lib():
     L.ref_render_cpu.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p, C.c_int]
     L.ref_trace.restype = C.c_double
     L.ref_trace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_int]
+    L.ref_build.restype = C.c_long
+    L.ref_build.argtypes = [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p,
+                            C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    if hasattr(L, "ref_frame_params"):
+        L.ref_params_size.restype = C.c_int
+        L.ref_frame_params.restype = None
+        L.ref_frame_params.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_uint,
+                                       C.c_float, C.c_float, C.c_void_p]
     if hasattr(L, "ref_trace_inst"):
         L.ref_trace_inst.restype = C.c_double
         L.ref_trace_inst.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_long, C.c_void_p, C.c_void_p, C.c_int]
     return L
 
 
-def cpu_frame_sample(cwp, wl, mesh, bvh, variant, seconds=12.0):
-    """The frame on the host cores: the reference's own host code (oracle/_ref) when built, else the oracle port.
-    Pixels are taken as a contiguous band from the middle of the image, grown until about `seconds` of work."""
+class RefScene:
+    """A workload's scene as the reference's own host code builds it, with no part of this library loaded: the box
+    field in plain Python (workloads.box_field_arrays, bit-identical to the library's generator), the reference's
+    BVHBuilder (16 SAH bins, one thread, accel/bvh_builder.cpp) with its CWBVH collapse or BVH2 layout and triangle
+    packing (ref_build, oracle/_ref/libcwpref.so), and the frame parameters from its camera code (ref_frame_params:
+    lookAtC2W / focalFromHfov / makeCamera and setupScene's sun, eps and filter arithmetic). Attributes: p (a Params
+    record), nodes, woop, tris, albedo, order, n_tris, build_ms."""
+
+    def __init__(self, L, wl, variant, w=512, h=512, bounces=4):
+        import ctypes as C
+        import numpy as np
+        wk = importlib.import_module("cuda-wavefront-pathtracer_b200.workloads")
+        pkg = sys.modules["cuda-wavefront-pathtracer_b200"]
+        v, f, fm = wk.box_field_arrays(wk.SCENES[wl["scene"]], wk.SCENE_SEED)
+        nt = len(f)
+        cap = 5 * 2 * nt + 64
+        nodes = np.zeros((cap, 4), np.float32); order = np.zeros(nt, np.int32)
+        tris = np.zeros((3 * nt, 4), np.float32); woop = np.zeros((3 * nt, 4), np.float32)
+        md, sah, ms = C.c_int(), C.c_double(), C.c_double()
+        n = L.ref_build(v.ctypes.data, len(v), f.ctypes.data, fm.ctypes.data, nt, variant, 4, 0, nodes.ctypes.data, cap, order.ctypes.data,
+                        tris.ctypes.data, woop.ctypes.data, C.byref(md), C.byref(sah), C.byref(ms))
+        assert n > 0, "ref_build failed"
+        self.nodes, self.order, self.tris, self.woop = nodes[:n].copy(), order, tris, woop
+        self.albedo = np.full((1, 3), wk.ALBEDO, np.float32)
+        self.n_tris, self.build_ms, self.sah = nt, ms.value, sah.value
+        p = pkg.Params()
+        assert L.ref_params_size() == C.sizeof(p), "cwp_params and the reference harness's RefParams differ in size"
+        f3 = C.c_float * 3
+        ext = float(np.max(v.max(0) - v.min(0)))
+        L.ref_frame_params(f3(*wk.CAM_POS), f3(*wk.CAM_TARGET), f3(*wk.CAM_UP), wk.HFOV, w, h, f3(*wk.SUN_TO), f3(*(wk.SUN_E,) * 3), f3(*wk.SKY),
+                           float(np.float32(wk.SUN_ANGLE_RAD * 180.0 / math.pi)), bounces, wk.SEED, wk.EPS_SCALE, ext, C.byref(p))
+        self.p = p
+
+
+def cpu_frame_sample(wl, rs, variant, seconds=12.0):
+    """The frame on the host cores: the reference's own host code (oracle/_ref) over the reference-built scene rs
+    (RefScene), else the oracle port. Pixels are taken as a contiguous band from the middle of the image, grown until
+    about `seconds` of work."""
     import ctypes as C
     import numpy as np
-    p = cwp.frame_params(mesh, wl["w"], wl["h"], bounces=wl["bounces"])
+    p = rs.p
     threads = os.cpu_count() or 1
     L = reference_lib()
-    alb = np.ascontiguousarray(bvh.albedo, np.float32)
+    alb = np.ascontiguousarray(rs.albedo, np.float32)
     N = wl["w"] * wl["h"]
     npix, spent, rays = 64, 0.0, 0
     while True:
@@ -161,21 +204,32 @@ def cpu_frame_sample(cwp, wl, mesh, bvh, variant, seconds=12.0):
         acc = np.zeros((N, 4), np.float32); cnt = np.zeros(2, np.int64)
         if L is not None:
             kind = "reference"
-            sec = L.ref_render_cpu(C.addressof(p), variant, 1, bvh.nodes.ctypes.data, bvh.woop.ctypes.data, bvh.tris.ctypes.data, alb.ctypes.data,
+            sec = L.ref_render_cpu(C.addressof(p), variant, 1, rs.nodes.ctypes.data, rs.woop.ctypes.data, rs.tris.ctypes.data, alb.ctypes.data,
                                    wl["bounces"], wl["spp"], 0, pix0, pix0 + npix, acc.ctypes.data, cnt.ctypes.data, threads)
         else:
             sys.path.insert(0, os.path.join(ROOT, "tests"))
             from conftest import Oracle
             kind, threads = "port", 1
             t0 = time.perf_counter()
-            acc, cnt = Oracle().render(p, variant, 1, bvh, wl["bounces"], wl["spp"], 0, pix0, pix0 + npix)
+            acc, cnt = Oracle().render(p, variant, 1, rs, wl["bounces"], wl["spp"], 0, pix0, pix0 + npix)
             sec = time.perf_counter() - t0
         rays = int(cnt.sum()); spent = sec
         if sec >= seconds / 4 or npix >= N:
             break
         npix = min(N, int(npix * max(2.0, min(16.0, seconds / 4 / max(sec, 1e-3)))))
     return dict(value=rays / spent / 1e9, unit="Grays/s", cores=threads, kind=kind,
-                sample=f"{npix} pixels x {wl['spp']} spp of the {wl['w']}x{wl['h']} frame ({rays} closest+shadow rays in {spent:.2f} s)")
+                sample=f"{npix} pixels x {wl['spp']} spp of the {wl['w']}x{wl['h']} frame ({rays} closest+shadow rays in {spent:.2f} s)",
+                host_build_ms=getattr(rs, "build_ms", None),
+                host_build=("the reference's BVHBuilder (16 SAH bins, one thread) and " + ("CWBVH collapse" if variant == 8 else f"BVH{variant} layout")
+                            + f" of the {rs.n_tris}-triangle scene") if getattr(rs, "build_ms", None) is not None else None)
+
+
+def port_scene(cwp, wl, variant, w=512, h=512, bounces=4):
+    """Where oracle/_ref is not built: the scene from the library's byte-identical 16-bin build, timed as a port."""
+    from types import SimpleNamespace
+    mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=16)
+    return SimpleNamespace(p=cwp.frame_params(mesh, w, h, bounces=bounces), nodes=bvh.nodes, woop=bvh.woop, tris=bvh.tris, albedo=bvh.albedo,
+                           order=bvh.order, n_tris=mesh.n_tris, build_ms=None, stride=bvh.stride)
 
 
 # DRAM bytes per launch of the frame kernels from one full-size ncu capture (dram__bytes_read.sum +
@@ -224,7 +278,9 @@ def onchip_bytes_trace(cwp, bvh, variant, o, d, n=1 << 15):
                 sample=f"oracle traversal of {n} of the batch's rays on the same tree")
 
 
-def cpu_trace_sample(cwp, bvh, variant, o, d, seconds=12.0):
+def cpu_trace_sample(bvh, variant, o, d, seconds=12.0):
+    """Closest-hit and any-hit traversal of a sample of the batch on the host cores with the reference's own trav<>
+    (oracle/_ref), else the oracle port. bvh: anything with nodes, woop (RefScene)."""
     import numpy as np
     L = reference_lib(); threads = os.cpu_count() or 1
     n, spent = 1 << 14, 0.0
@@ -245,7 +301,10 @@ def cpu_trace_sample(cwp, bvh, variant, o, d, seconds=12.0):
             break
         n = min(len(o), int(n * max(2.0, min(16.0, seconds / 4 / max(spent, 1e-3)))))
     return dict(value=2 * n / spent / 1e9, unit="Grays/s", cores=threads, kind=kind,
-                sample=f"{n} of the {len(o)} incoherent rays, closest-hit and any-hit ({2 * n} rays in {spent:.2f} s)")
+                sample=f"{n} of the {len(o)} incoherent rays, closest-hit and any-hit ({2 * n} rays in {spent:.2f} s)",
+                host_build_ms=getattr(bvh, "build_ms", None),
+                host_build=(f"the reference's BVHBuilder (16 SAH bins, one thread) and " + ("CWBVH collapse" if variant == 8 else f"BVH{variant} layout")
+                            + f" of the {bvh.n_tris}-triangle scene") if getattr(bvh, "build_ms", None) is not None else None)
 
 
 METRIC_FRAME = "closest+shadow rays per second, diffuse frame"
@@ -264,42 +323,95 @@ def run_reference(args, wl, rank):
                "batched64 line's cpu_baseline)" if wl.get("batched") else "the reference has no serving loop")
         print(json.dumps({"impl": "reference", "metric": METRIC_BATCHED if wl.get("batched") else METRIC_SERVING, "unavailable": why}), flush=True)
         return
-    cwp = importlib.import_module("cuda-wavefront-pathtracer_b200")
+    # nothing of this library is loaded on this arm: the scene, the BVH, the frame parameters and the rays come from
+    # the reference's own host code (oracle/_ref/libcwpref.so) and plain Python
     variant = args.variant
-    mesh, bvh = cwp.scene(wl["scene"], variant=variant, bins=16)
+    L = reference_lib()
+    if L is None or not hasattr(L, "ref_frame_params"):
+        print(json.dumps({"impl": "reference", "metric": METRIC_FRAME if "rays" not in wl else METRIC_BATCH,
+                          "unavailable": "oracle/_ref/libcwpref.so (the reference's host code compiled from its sources) is not built"}), flush=True)
+        return
+    importlib.import_module("cuda-wavefront-pathtracer_b200")   # ctypes records and workloads only; the CUDA library is not loaded
+    wk = importlib.import_module("cuda-wavefront-pathtracer_b200.workloads")
+    rs = RefScene(L, wl, variant, w=wl.get("w", 512), h=wl.get("h", 512), bounces=wl.get("bounces", 4))
     vals = []
     for i in range(args.warmup + args.steps):
         if "rays" in wl:
-            # rays from the oracle-free generator need a tracer: use the reference's own host traversal
-            L = reference_lib()
             import numpy as np
-            p = cwp.frame_params(mesh, 512, 512)
 
-            def tr(o, d):
+            def tr(o, d):   # the reference's host traversal finds the surface points of the incoherent batch
                 h = np.zeros((len(o), 4), np.float32)
-                L.ref_trace(variant, 0, 1, bvh.nodes.ctypes.data, bvh.woop.ctypes.data, o.ctypes.data, d.ctypes.data, len(o), h.ctypes.data, None, 0)
+                L.ref_trace(variant, 0, 1, rs.nodes.ctypes.data, rs.woop.ctypes.data, o.ctypes.data, d.ctypes.data, len(o), h.ctypes.data, None, 0)
                 return h
             if i == 0:
-                ro, rd = cwp.incoherent_rays(1 << 20, p, bvh.tris, tr, seed=41)
-            cb = cpu_trace_sample(cwp, bvh, variant, ro, rd, seconds=args.ref_seconds)
+                ro, rd = wk.incoherent_rays(1 << 20, rs.p, rs.tris, tr, seed=41)
+            cb = cpu_trace_sample(rs, variant, ro, rd, seconds=args.ref_seconds)
         else:
-            cb = cpu_frame_sample(cwp, wl, mesh, bvh, variant, seconds=args.ref_seconds)
+            cb = cpu_frame_sample(wl, rs, variant, seconds=args.ref_seconds)
         if i >= args.warmup:
             vals.append(cb["value"])
     v = statistics.median(vals)
     cb["value"] = v
     if "rays" not in wl:
-        config = {"workload": args.workload, "scene": f"{wl['scene']} ({mesh.n_tris} triangles, box field seed 1)", "resolution": f"{wl['w']}x{wl['h']}",
+        config = {"workload": args.workload, "scene": f"{wl['scene']} ({rs.n_tris} triangles, box field seed 1)", "resolution": f"{wl['w']}x{wl['h']}",
                   "spp": wl["spp"], "batch": wl["batch"], "depth": wl["bounces"], "layout": LAYOUT_NAMES[variant], "sah_bins": 16, "tri": "woop",
                   "bvh": "binned SAH (the reference's BVHBuilder, 16 bins)"}
     else:
-        config = {"workload": args.workload, "scene": f"{wl['scene']} ({mesh.n_tris} triangles)", "rays": wl["rays"], "layout": LAYOUT_NAMES[variant],
+        config = {"workload": args.workload, "scene": f"{wl['scene']} ({rs.n_tris} triangles)", "rays": wl["rays"], "layout": LAYOUT_NAMES[variant],
                   "sah_bins": 16, "tri": "woop", "bvh": "binned SAH (the reference's BVHBuilder, 16 bins)"}
+    assert sys.modules["cuda-wavefront-pathtracer_b200"]._lib is None, "the reference arm loaded this library"
     print(json.dumps({"impl": "reference", "metric": METRIC_FRAME if "rays" not in wl else METRIC_BATCH,
                       "value": v, "unit": "Grays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                       "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                       "config": config,
                       "cpu_baseline": cb, "e2e": {"value": v, "unit": "Grays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def reference_cuda_frame(cwp, wl, mesh, p, ours_ms, ours_img, device, reps=2):
+    """The same frame rendered by the reference's own CUDA build on this GPU (oracle/_ref/pt, compiled from its
+    sources for sm_100 with its own flags), outside the timed region, from the same scene written as PLY with the
+    camera and lighting files (its binned-SAH BVHBuilder at 16 bins builds its tree). Records its frame time on BVH2
+    and BVH8 (best of `reps` after its warm-up), this library's frame time on the same 16-bin trees and on the
+    benchmark's own tree (ours_ms, the bench's timed frames), the ratios, and the PSNR of every image against the
+    reference's BVH2 image."""
+    import tempfile as tf
+    pt = os.path.join(ROOT, "oracle", "_ref", "pt")
+    if not os.path.exists(pt):
+        return {"unavailable": "oracle/_ref/pt (the reference's CUDA build) is not built"}
+    w, h, spp, K, B = wl["w"], wl["h"], wl["spp"], wl["batch"], wl["bounces"]
+    rec = {"command": "oracle/_ref/pt --mesh scene.ply --camera camera.json --lighting lighting.json --albedo 0.7 0.7 0.7 --filter box "
+                      f"--hfov 45 --width {w} --height {h} --spp {spp} --bounces {B} --variant bvh2|bvh8 --tri woop --fuse 1 --batch {K} --leaf 4 --reps {reps}"}
+    ref_img = None
+    with tf.TemporaryDirectory() as tmp:
+        for rv in ("bvh2", "bvh8"):
+            a = cwp.reference_inputs(mesh, p, tmp, w, h, spp, K, variant=rv)
+            out = os.path.join(tmp, f"ref_{rv}")
+            res = subprocess.run([pt] + a + ["--out", out, "--reps", str(reps)], capture_output=True, text=True, timeout=900)   # one-GPU runs: its device 0 is ours
+            if res.returncode != 0:
+                return {"unavailable": f"oracle/_ref/pt exited {res.returncode}: {res.stderr.strip().splitlines()[-1:] }"}
+            lines = [json.loads(l) for l in res.stdout.splitlines() if l.startswith("{")]
+            best = min(lines, key=lambda l: l["t_frame_ms"])
+            img = cwp.imageio.read_pfm(out + ".pfm")
+            ref_img = img if ref_img is None else ref_img
+            rec[f"reference_{rv}"] = {"t_frame_ms": best["t_frame_ms"], "rays_total": best["rays_total"], "grays_s": best["rays_total"] / best["t_frame_ms"] / 1e6,
+                                      "psnr_vs_reference_bvh2_db": cwp.imageio.psnr(img, ref_img) if rv != "bvh2" else None}
+    for variant in (2, 8):
+        _, bvh = cwp.scene(wl["scene"], variant=variant, bins=16)
+        r = cwp.Renderer(); r.init(p, bvh, variant=variant, batch=K, bounces=B, device=device)
+        r.render(spp)   # graph capture
+        best = min((r.render(spp) for _ in range(reps)), key=lambda st: st.frame_ms)
+        img = cwp.imageio.accum_to_image(r.read_accum(), w, h, spp)
+        r.close()
+        rec[f"ours_same_tree_{LAYOUT_NAMES[variant]}"] = {"t_frame_ms": best.frame_ms, "grays_s": (best.rays + best.shadow_rays) / best.frame_ms / 1e6,
+                                                          "psnr_vs_reference_bvh2_db": cwp.imageio.psnr(img, ref_img)}
+    rec["ours_benchmark_tree"] = {"t_frame_ms": ours_ms, "psnr_vs_reference_bvh2_db": cwp.imageio.psnr(ours_img, ref_img)}
+    ref_best = min(rec["reference_bvh2"]["t_frame_ms"], rec["reference_bvh8"]["t_frame_ms"])
+    same_best = min(rec["ours_same_tree_bvh2"]["t_frame_ms"], rec["ours_same_tree_cwbvh"]["t_frame_ms"])
+    rec["speedup_same_tree"] = ref_best / same_best
+    rec["speedup_benchmark_tree"] = ref_best / ours_ms
+    rec["note"] = ("ratios are the reference's best frame time (BVH2 or BVH8) over ours: on the same 16-bin binned-SAH trees (kernels alone), "
+                   "and on the benchmark's own tree (kernels and tree); frame times are CUDA-event frame times of each build's own frame loop")
+    return rec
 
 
 def batched_setup(cwp, wl):
@@ -566,6 +678,7 @@ def main():
     ap.add_argument("--graph", type=int, default=1)
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-cuda", type=int, default=1, help="frames: also render the frame with the reference's CUDA build (oracle/_ref/pt), outside the timed region")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--spp", type=int, default=0, help="override the frame's samples per pixel (profiling cases)")
     ap.add_argument("--rays", type=int, default=0, help="override the batch size of trace16m / rays per scene of batched64 (profiling cases)")
@@ -670,7 +783,7 @@ def main():
         b, t = (tr_bytes, tms.sum()) if dom == "k_trace_shade" else (sh_bytes, sms.sum())
         achieved = b / (t * 1e-3) / 1e9 if t > 0 else 0.0
         out.update(metric=METRIC_FRAME, value=value, ms_per_step=max_ms / args.steps,
-                   config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles, box field seed 1)", "resolution": f"{w}x{h}",
+                   config={"workload": args.workload, "scene": f"{wl['scene']} ({mesh.n_tris} triangles, box field seed 1)", "references": len(bvh.order), "resolution": f"{w}x{h}",
                            "spp": spp, "batch": K, "depth": B, "layout": LAYOUT_NAMES[variant], "sah_bins": args.bins, "tri": "woop",
                            "bvh": (f"sbvh (spatial splits at overlap > {args.spatial:g} of the root area, {len(bvh.order) / mesh.n_tris:.2f} references per triangle)" if args.spatial > 0 else "binned SAH"),
                            "graph": args.graph, "traversal": ["auto", "refill", "batch"][args.traversal], "sort": ["off", "octant", "octant+cell"][args.sort],
@@ -686,7 +799,10 @@ def main():
                              "peak_kind": peak_kind, **frame_traffic(args, wl, variant, dom),
                              "algorithmic": f"{STATE_BYTES} B of path state per queued ray read and per continuation/shadow ray written"})
         onchip = dict(kind="frame", closest=float(c_tot.sum()), shadow=float(s_tot.sum()), closest_ms=float(tms.sum()), shadow_ms=float(sms.sum()))
+        ours_img = cwp.imageio.accum_to_image(r.read_accum(), w, h, spp)
         r.close()
+        if rank == 0 and ws == 1 and args.reference_cuda:
+            out["reference_cuda"] = reference_cuda_frame(cwp, wl, mesh, p, max_ms / args.steps, ours_img, local)
     else:
         # ------------------------------------------------------------------ ray batches
         n = wl["rays"]
@@ -767,7 +883,7 @@ def main():
         achieved = dom_b * n * args.steps / (dom_ms * 1e-3) / 1e9
         onchip = dict(kind="batch", closest=float(n * args.steps), shadow=float(n * args.steps), closest_ms=c_ms, shadow_ms=a_ms)
         out.update(metric=METRIC_BATCH, value=value, ms_per_step=max_ms / args.steps,
-                   config={"workload": args.workload, "scene": f"{wl['scene']} ({len(bvh.order)} triangles)", "rays": n,
+                   config={"workload": args.workload, "scene": f"{wl['scene']} ({mesh.n_tris} triangles)", "references": len(bvh.order), "rays": n,
                            "layout": LAYOUT_NAMES[variant] + (" precision form (f16 conservative slabs, watertight fp32 triangles)" if wl.get("precision") else ""), **check,
                            "sah_bins": args.bins, "tri": "woop", "traversal": ["auto", "refill", "batch"][args.traversal],
                            "bvh": (f"sbvh ({len(bvh.order) / mesh.n_tris:.2f} references per triangle)" if args.spatial > 0 else "binned SAH"), "l2": f"ray batch {n * 32 / 1e9:.2f} GB > L2 (126 MB)",
@@ -780,12 +896,14 @@ def main():
                              "algorithmic": "closest: 32 B ray in + 16 B hit out; any: 32 B in + 4 B out"})
         acc.close()
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and not wl.get("batched") and not wl.get("serving"):
-        # the reference's own host build (binned SAH, 16 bins: byte-identical to its BVHBuilder) under its own code
-        _, rbvh = cwp.scene(wl["scene"], variant=variant, bins=16)
+        # the reference's own host build (its BVHBuilder, 16 bins, timed) and its own traversal code on the host cores
+        L = reference_lib()
+        rs = (RefScene(L, wl, variant, w=wl.get("w", 512), h=wl.get("h", 512), bounces=wl.get("bounces", 4)) if L is not None and hasattr(L, "ref_frame_params")
+              else port_scene(cwp, wl, variant, w=wl.get("w", 512), h=wl.get("h", 512), bounces=wl.get("bounces", 4)))
         if "rays" not in wl:
-            out["cpu_baseline"] = cpu_frame_sample(cwp, wl, mesh, rbvh, variant)
+            out["cpu_baseline"] = cpu_frame_sample(wl, rs, variant)
         else:
-            out["cpu_baseline"] = cpu_trace_sample(cwp, rbvh, variant, o, d)
+            out["cpu_baseline"] = cpu_trace_sample(rs, variant, o, d)
         # on-chip roofline: oracle-counted node + triangle bytes per ray on the GPU's own tree, over the kernels' event
         # times, against the measured L2 read bandwidth (the scene is L2-resident, so this is the traversal's bound)
         if not wl.get("precision"):

@@ -71,6 +71,9 @@ bool parse(int argc, char** argv, Args& A) {
     if (A.loader != "auto" && A.loader != "builtin") { fprintf(stderr, "--loader %s: only the built-in PLY / OBJ loader is available\n", A.loader.c_str()); return false; }
     if (A.envSampling != "importance" && A.envSampling != "uniform") { fprintf(stderr, "--env_sampling must be importance or uniform\n"); return false; }
     if (A.texFilter != "linear" && A.texFilter != "nearest") { fprintf(stderr, "--tex_filter must be linear or nearest\n"); return false; }
+    // the reference builds the sphere grid and then still reads the scene file's box for the ray offset
+    // (scene_setup.cpp:92-154): an ill-defined mix, refused here
+    if (!A.scene.empty() && A.synthetic > 0) { fprintf(stderr, "--synthetic and --scene cannot be combined\n"); return false; }
     if (!A.scene.empty() && !A.materials.empty()) { fprintf(stderr, "--materials is per mesh in scene files (\"materials\" key)\n"); return false; }
     if (A.builder != "sah") { fprintf(stderr, "--builder %s: only the host binned-SAH builder is available\n", A.builder.c_str()); return false; }
     if (A.collapse != "sah" && A.collapse != "greedy") { fprintf(stderr, "--collapse must be sah or greedy\n"); return false; }
@@ -233,6 +236,9 @@ bool write_images(const std::string& name, int w, int h, const std::vector<float
 bool camera_c2w(Args& A, float c2w[16]) {
     bool haveC2w = false;
     for (int j = 0; j < 16; j++) c2w[j] = (j % 5 == 0) ? 1.f : 0.f;
+    // the sphere grid sets its view and a 50 deg field before any camera file is read (scene_setup.cpp:92-95), so a
+    // file's matrix replaces the view but its hfov_deg does not replace the 50 deg
+    if (A.synthetic > 0) { cwp_sphere_grid_c2w(c2w); haveC2w = true; if (A.hfov == 0 && A.fx == 0) A.hfov = 50.f; }
     if (!A.camera.empty()) {
         Json C; std::string err;
         if (!cwpb::parse_json(cwpb::read_text(A.camera), C, &err)) { fprintf(stderr, "camera file %s: %s\n", A.camera.c_str(), err.c_str()); return false; }
@@ -249,7 +255,6 @@ bool camera_c2w(Args& A, float c2w[16]) {
         if (A.focusDist < 0.f && C.at("focus_distance")) A.focusDist = (float)C.number("focus_distance", 0);
     }
     if (!A.c2w.empty()) { std::string s = A.c2w; for (char& ch : s) if (ch == ',') ch = ' '; const char* p = s.c_str(); char* e; for (int j = 0; j < 16; j++) { c2w[j] = (float)strtod(p, &e); p = e; } haveC2w = true; }
-    if (!haveC2w && A.synthetic > 0) { cwp_sphere_grid_c2w(c2w); haveC2w = true; }   // scene_setup.cpp:94
     if (!haveC2w && A.boxes > 0) {   // box field without a camera: the benchmark view
         const float pos[3] = { 0.f, -34.f, 22.f }, tgt[3] = { 0.f, 0.f, 0.f }, up[3] = { 0.f, 0.f, 1.f }; cwp_camera c;
         if (A.hfov == 0 && A.fx == 0) A.hfov = 45.f;
@@ -268,11 +273,12 @@ bool camera_c2w(Args& A, float c2w[16]) {
 int run_full(Args& A, const std::string& envFromLighting, float envStrengthL, float envRotL, const std::vector<float>& kdLighting) {
     FullScene S;
     const float gray[3] = { 0.8f, 0.8f, 0.8f };
+    // the sphere grid wins over every mesh source, as in the reference (scene_setup.cpp:92)
     if (!A.scene.empty()) { if (!load_scene(A.scene, A, S)) return 1; }
     else {
         cwpb::Mesh mesh; std::string err;
-        if (A.boxes > 0) cwpb::box_field(A.boxes, 1, 20.f, 0.2f, 3.f, mesh);   // as cwp_mesh_box_field
-        else if (A.synthetic > 0) cwpb::sphere_grid(A.synthetic, 200, 100, 200, mesh);   // scene_setup.cpp:93
+        if (A.synthetic > 0) cwpb::sphere_grid(A.synthetic, 200, 100, 200, mesh);   // scene_setup.cpp:93
+        else if (A.boxes > 0) cwpb::box_field(A.boxes, 1, 20.f, 0.2f, 3.f, mesh);   // as cwp_mesh_box_field
         else if (!cwpb::load_mesh(A.mesh, mesh, &err)) { fprintf(stderr, "%s: %s\n", A.mesh.c_str(), err.c_str()); return 1; }
         if (A.yupToZup == 1 && A.synthetic <= 0) {   // files only: the generated scenes are z-up
             for (size_t i = 0; i < mesh.v.size(); i += 3) { float y = mesh.v[i + 1], z = mesh.v[i + 2]; mesh.v[i + 1] = -z; mesh.v[i + 2] = y; }
@@ -442,8 +448,8 @@ int main(int argc, char** argv) {
     if (needFull) fprintf(stderr, "warn: --integrator legacy ignores specular/transmissive/emissive materials, the environment map and RR\n");
     // ---- scene ----
     cwp_mesh* mesh = nullptr;
-    if (A.boxes > 0) { if (cwp_mesh_box_field(A.boxes, 1, &mesh)) return fail("box field"); }
-    else if (A.synthetic > 0) { if (cwp_mesh_sphere_grid(A.synthetic, 200, 100, 200, &mesh)) return fail("sphere grid"); }
+    if (A.synthetic > 0) { if (cwp_mesh_sphere_grid(A.synthetic, 200, 100, 200, &mesh)) return fail("sphere grid"); }   // first, as scene_setup.cpp:92
+    else if (A.boxes > 0) { if (cwp_mesh_box_field(A.boxes, 1, &mesh)) return fail("box field"); }
     else if (!A.mesh.empty()) { if (cwp_mesh_load(A.mesh.c_str(), &mesh)) return fail("mesh"); }
     else { fprintf(stderr, "no scene: give --mesh PATH, --boxes N or --synthetic N\n"); return 1; }
     cwp_mesh_view mv; cwp_mesh_view_of(mesh, &mv);

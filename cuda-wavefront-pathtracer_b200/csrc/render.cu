@@ -16,6 +16,7 @@
 #include "trav.cuh"
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -708,11 +709,14 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 struct NoAllocDevice { unsigned char* base = nullptr; int gridTrace0 = 0, gridTrace = 0, gridShadow = 0; };
 
 // device address of the scratch on the current device, looked up once per device (host code cannot use the symbol
-// itself: on the host it names a stand-in, not device memory)
+// itself: on the host it names a stand-in, not device memory). The table is guarded by a mutex, so host threads that
+// make their first calls at the same time each see a complete entry.
 static int noalloc_setup(int dev, NoAllocDevice& out) {
+    static std::mutex mu;
     static NoAllocDevice table[64];
     static bool ready[64] = { false };
     CWPB_CHECK(dev >= 0 && dev < 64, CWP_ERR_INVALID, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
     if (!ready[dev]) {
         void* p = nullptr;
         CWPB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
@@ -725,6 +729,16 @@ static int noalloc_setup(int dev, NoAllocDevice& out) {
         table[dev] = d; ready[dev] = true;
     }
     out = table[dev];
+    return CWP_OK;
+}
+
+// a caller's buffer must be device (or managed) memory that the current device can address
+static int noalloc_check_ptr(const void* ptr, int dev, const char* what) {
+    if (!ptr) return CWP_OK;
+    cudaPointerAttributes at{};
+    CWPB_CUDA(cudaPointerGetAttributes(&at, ptr));
+    CWPB_CHECK(at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged, CWP_ERR_INVALID, "%s is not device memory", what);
+    CWPB_CHECK(at.type == cudaMemoryTypeManaged || at.device == dev, CWP_ERR_INVALID, "%s lives on device %d, not on the current device %d", what, at.device, dev);
     return CWP_OK;
 }
 
@@ -742,7 +756,15 @@ extern "C" int cwp_render_noalloc(const cwp_params* p, const cwp_device_scene* s
     CWPB_CHECK(o->bounces >= 0 && o->bounces <= kNoAllocMaxBounces, CWP_ERR_INVALID, "bounces %d outside [0, %d] of the no-allocation path", o->bounces, kNoAllocMaxBounces);
     CWPB_CHECK(p->max_b <= o->bounces, CWP_ERR_INVALID, "params max_b %d exceeds bounces %d", p->max_b, o->bounces);
     CWPB_CHECK(spp > 0 && spp % o->batch == 0 && s_base >= 0, CWP_ERR_INVALID, "spp %d must be a positive multiple of batch %d", spp, o->batch);
+    CWPB_CHECK(o->traversal == 0 || o->traversal == 2, CWP_ERR_INVALID, "traversal %d: the no-allocation path runs one 32-ray fetch per warp (0 or 2)", o->traversal);
+    CWPB_CHECK(o->sort == 0, CWP_ERR_INVALID, "sort %d: the no-allocation path has no regrouping buffers (sort must be 0)", o->sort);
     int dev = 0; CWPB_CUDA(cudaGetDevice(&dev));
+    CWPB_CHECK(o->device == dev, CWP_ERR_INVALID, "options.device %d is not the current device %d (make it current before the call)", o->device, dev);
+    {
+        const void* ptrs[6] = { s->nodes, s->tris, s->woop, s->nrm, s->albedo, d_accum };
+        const char* names[6] = { "scene nodes", "scene tris", "scene woop", "scene nrm", "scene albedo", "accumulation buffer" };
+        for (int k = 0; k < 6; k++) if (int rc = noalloc_check_ptr(ptrs[k], dev, names[k])) return rc;
+    }
     NoAllocDevice na; if (int rc = noalloc_setup(dev, na)) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     const size_t NK = (size_t)kNoAllocMaxPaths;

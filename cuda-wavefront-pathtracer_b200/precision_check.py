@@ -62,10 +62,11 @@ def wt32(o, d, verts, tri):
     return ~rej & (det != 0), t
 
 
-def edge_excess(o, d, verts, tri):
-    """For rays (o, d float4) and leaf-order triangles tri (exact corners verts, 3 float4 each): how far outside the
-    triangle the ray passes in FP64, in units of the precision form's FP32 edge bound 1e-6 (Sx Sy' + Sy Sx'); <= 1
-    means the conservative FP32 edge test may accept it, 0 means inside."""
+def edge_margin(o, d, verts, tri):
+    """For rays (o, d float4) and leaf-order triangles tri (exact corners verts, 3 float4 each): the signed distance
+    of the ray from the triangle's edges in FP64, in units of the precision form's FP32 edge bound
+    1e-6 (Sx Sy' + Sy Sx'): the largest of the three edge functions taken outward, so > 0 outside (by that much),
+    <= 0 inside (|value| = the margin to the nearest edge)."""
     o = o[:, :3].astype(np.float64); d32 = d[:, :3]; dd = d32.astype(np.float64)
     ad = np.abs(d32)
     kz = np.where(ad[:, 0] >= ad[:, 1], np.where(ad[:, 0] >= ad[:, 2], 0, 2), np.where(ad[:, 1] >= ad[:, 2], 1, 2))
@@ -85,4 +86,73 @@ def edge_excess(o, d, verts, tri):
     E = np.stack([Cx * By - Cy * Bx, Ax * Cy - Ay * Cx, Bx * Ay - By * Ax], 1)
     e = 1e-6 * np.stack([SCx * SBy + SCy * SBx, SAx * SCy + SAy * SCx, SBx * SAy + SBy * SAx], 1) + 1e-30
     sgn = np.where(E.sum(1) >= 0, 1.0, -1.0)[:, None]
-    return np.maximum(0.0, (-sgn * E / e).max(1))
+    return (-sgn * E / e).max(1)
+
+
+def edge_excess(o, d, verts, tri):
+    """How far outside the triangle the ray passes in FP64, in the units of edge_margin; <= 1 means the conservative
+    FP32 edge test may accept it, 0 means inside."""
+    return np.maximum(0.0, edge_margin(o, d, verts, tri))
+
+
+def fp64_hit(o, d, verts, tri):
+    """FP64 test of given (ray, leaf-order triangle) pairs on the exact corners: (t of the triangle's plane, signed
+    edge margin as edge_margin), nan / inf where tri < 0."""
+    t = np.full(len(o), np.nan)
+    m = np.full(len(o), np.inf)
+    k = np.where(tri >= 0)[0]
+    if not len(k):
+        return t, m
+    oo = o[k, :3].astype(np.float64); dd = d[k, :3].astype(np.float64); tt = tri[k]
+    v = [verts[3 * tt + j, :3].astype(np.float64) for j in range(3)]
+    n = np.cross(v[1] - v[0], v[2] - v[0])
+    den = (n * dd).sum(1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t[k] = np.where(den != 0, ((v[0] - oo) * n).sum(1) / den, np.nan)
+    m[k] = edge_margin(o[k], d[k], verts, tt)
+    return t, m
+
+
+def explain_differences(o, d, verts, ours, other, any_hit=False, rel=1e-6, graze=16.0):
+    """Rays on which this library and another traversal of the same tree disagree, classified in FP64 on the exact
+    corners. Closest hit: ours / other are float4 (t, u, v, leaf-order triangle bits) and a ray disagrees when the
+    triangles differ; any hit: int32 triangle or -1, and a ray disagrees when one side finds an occluder and the
+    other does not. Classes:
+      tie         (closest) both hits within rel * t of each other;
+      ours_exact  ours is the exact answer of the two: our triangle is hit in exact arithmetic (margin <= 0) and the
+                  other reports none, a farther one, or one that exact arithmetic misses (margin > 0);
+      graze       a triangle that one side reports and the other does not lies within `graze` edge-bound units of one
+                  of its edges, inside or out (FP32 rounding decides such rays);
+      unexplained anything else.
+    Returns (counts, rows), one row per disagreeing ray."""
+    if any_hit:
+        ia, ib = np.asarray(ours, np.int32), np.asarray(other, np.int32)
+        diff = np.where((ia >= 0) != (ib >= 0))[0]
+    else:
+        ia, ib = ours[:, 3].view(np.int32), other[:, 3].view(np.int32)
+        diff = np.where(ia != ib)[0]
+    counts = {"rays": int(len(o)), "differ": int(len(diff)), "tie": 0, "ours_exact": 0, "graze": 0, "unexplained": 0}
+    rows = []
+    if not len(diff):
+        return counts, rows
+    oo, dd = o[diff], d[diff]
+    ta, ma = fp64_hit(oo, dd, verts, ia[diff])
+    tb, mb = fp64_hit(oo, dd, verts, ib[diff])
+    for j, i in enumerate(diff):
+        a, b = int(ia[i]), int(ib[i])
+        if not any_hit and a >= 0 and b >= 0 and abs(ours[i, 0] - other[i, 0]) <= rel * max(abs(ours[i, 0]), abs(other[i, 0])):
+            c = "tie"
+        elif a >= 0 and ma[j] <= 0 and (b < 0 or mb[j] > 0 or ta[j] < tb[j]):
+            c = "ours_exact"
+        elif any_hit and a < 0 and mb[j] > graze:
+            c = "ours_exact"   # the other's occluder is missed by exact arithmetic
+        elif (a >= 0 and abs(ma[j]) <= graze) or (b >= 0 and abs(mb[j]) <= graze):
+            c = "graze"
+        else:
+            c = "unexplained"
+        counts[c] += 1
+        rows.append({"ray": int(i), "ours": a, "other": b, "t64_ours": float(ta[j]), "t64_other": float(tb[j]),
+                     "margin_ours": float(ma[j]), "margin_other": float(mb[j]), "class": c,
+                     **({} if any_hit else {"t_ours": float(ours[i, 0]), "t_other": float(other[i, 0]), "uv_ours": [float(ours[i, 1]), float(ours[i, 2])],
+                                            "uv_other": [float(other[i, 1]), float(other[i, 2])]})})
+    return counts, rows

@@ -27,8 +27,43 @@ ALBEDO = 0.7
 SEED = 1000
 EPS_SCALE = 1e-4
 
-__all__ = ["SCENES", "scene", "frame_params", "scene_extent", "camera_rays", "incoherent_rays", "reference_inputs",
+__all__ = ["SCENES", "scene", "box_field_arrays", "frame_params", "scene_extent", "camera_rays", "incoherent_rays", "reference_inputs",
            "batch_scenes", "batch_rays", "serving_scenes", "serving_requests", "planar_uvs", "texture_images", "RESOLUTIONS", "SPPS", "HFOV", "SEED", "SUN_TO", "SUN_E", "SUN_ANGLE_RAD", "SKY", "ALBEDO"]
+
+
+def box_field_arrays(n_boxes, seed=SCENE_SEED, half=20.0, edge_lo=0.2, edge_hi=3.0):
+    """The box field of Mesh.box_field (cwp_mesh_box_field) in plain Python, without the CUDA library: (verts float32
+    (nv, 3), faces int32 (nt, 3), face material int32 (nt,)). Same SplitMix64 stream, same double arithmetic through
+    the C library's exp / log / cos / sin, same float rounding, so the arrays are bit-identical to the library's (a
+    CPU test checks it). Used where the library must not be loaded: the reference arm of the benchmark."""
+    M64 = (1 << 64) - 1
+    state = [int(seed) & M64]
+
+    def unit():
+        state[0] = (state[0] + 0x9E3779B97F4A7C15) & M64
+        z = state[0]
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+        return ((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0)
+    half = float(np.float32(half))
+    l_lo, l_hi = math.log(float(np.float32(edge_lo))), math.log(float(np.float32(edge_hi)))
+    v = [(-half, 0.0, -half), (half, 0.0, -half), (half, 0.0, half), (-half, 0.0, half)]   # ground, y-up
+    f = [(0, 2, 1), (0, 3, 2)]
+    quads = ((0, 4, 6, 2), (1, 3, 7, 5), (0, 1, 5, 4), (2, 6, 7, 3), (0, 2, 3, 1), (4, 5, 7, 6))
+    for _ in range(int(n_boxes)):
+        cx = -half + 2.0 * half * unit(); cz = -half + 2.0 * half * unit()
+        ex = math.exp(l_lo + (l_hi - l_lo) * unit()); ey = math.exp(l_lo + (l_hi - l_lo) * unit()); ez = math.exp(l_lo + (l_hi - l_lo) * unit())
+        th = 2.0 * 3.14159265358979323846 * unit(); c, s = math.cos(th), math.sin(th)
+        base = len(v)
+        for k in range(8):
+            lx = (0.5 if k & 1 else -0.5) * ex; ly = ey if k & 2 else 0.0; lz = (0.5 if k & 4 else -0.5) * ez
+            v.append((cx + lx * c + lz * s, ly, cz - lx * s + lz * c))
+        for q in quads:
+            f.append((base + q[0], base + q[1], base + q[2])); f.append((base + q[0], base + q[2], base + q[3]))
+    vd = np.array(v, np.float64)
+    verts = np.stack([vd[:, 0], -vd[:, 2], vd[:, 1]], 1).astype(np.float32)   # y-up -> z-up, (x, y, z) -> (x, -z, y)
+    faces = np.array(f, np.int32)
+    return verts, faces, np.zeros(len(faces), np.int32)
 
 
 def scene(name_or_boxes, variant=8, bins=32, leaf=4, collapse=0, threads=0, spatial=0.0):

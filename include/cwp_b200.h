@@ -198,7 +198,11 @@ void cwp_renderer_destroy(cwp_renderer* r);
  * device address (do it before any stream capture on that device). All calls share the array: calls whose work
  * overlaps on the GPU (other streams, other host threads) race and must be serialised by the caller. Launches are
  * stream-ordered on `stream`; when h_rays is not NULL the call waits for the frame and stores the closest and shadow
- * ray totals there (and reports traversal errors).
+ * ray totals there (and reports traversal errors). The call runs on the current device: options.device must name
+ * it, and every scene pointer and d_accum must be device (or managed) memory of that device, else CWP_ERR_INVALID.
+ * Of the options, variant, tri, batch, bounces and device are used; the traversal is always one 32-ray fetch per
+ * warp (traversal must be 0 or 2), there is no regrouping (sort must be 0), and graph, block and profile are
+ * ignored: the passes are plain stream launches.
  * ------------------------------------------------------------------------------------------------------------------ */
 typedef struct cwp_device_scene {
     const float* nodes; const float* tris; const float* woop; const float* nrm;   /* device pointers; woop / nrm may be NULL */

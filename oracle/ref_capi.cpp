@@ -110,6 +110,31 @@ struct RefParams {
     float sun_to[3], sun_e[3], sky[3]; float sun_cos; int max_b; unsigned seed; float eps, near_clip; int has_n, filter_bh; float ftab[65];
 };
 
+// The frame parameters the reference's CLI sets up for a look-at camera with a horizontal field of view
+// (app/scene_setup.cpp:172-185): the camera from its own lookAtC2W / focalFromHfov / makeCamera (scene/camera.cpp),
+// the normalised sun direction, the sun cone's cosine, the ray offset eps_scale x extent and its Blackman-Harris
+// table. out: one RefParams (the cwp_params layout), ref_params_size() bytes.
+extern "C" int ref_params_size(void) { return (int)sizeof(RefParams); }
+extern "C" void ref_frame_params(const float* pos, const float* tgt, const float* up, float hfov_deg, int w, int h, const float* sun_to, const float* sun_e,
+                                 const float* sky, float sun_angle_deg, int max_b, unsigned seed, float eps_scale, float extent, void* out) {
+    float c2w[16];
+    lookAtC2W(make_float3(pos[0], pos[1], pos[2]), make_float3(tgt[0], tgt[1], tgt[2]), make_float3(up[0], up[1], up[2]), c2w);
+    const float fx = focalFromHfov(w, hfov_deg);
+    const Cam c = makeCamera(c2w, fx, fx, w, h);
+    RefParams& P = *(RefParams*)out;
+    memset(&P, 0, sizeof P);
+    const float3 v3[4] = { c.pos, c.ax, c.ay, c.az };
+    float* dst[4] = { P.pos, P.ax, P.ay, P.az };
+    for (int k = 0; k < 4; k++) { dst[k][0] = v3[k].x; dst[k][1] = v3[k].y; dst[k][2] = v3[k].z; }
+    P.fx = c.fx; P.fy = c.fy; P.px = c.px; P.py = c.py; P.w = c.w; P.h = c.h; P.lens_r = c.lensR; P.focus_d = c.focusD;
+    const float3 s = normalize(make_float3(sun_to[0], sun_to[1], sun_to[2]));
+    P.sun_to[0] = s.x; P.sun_to[1] = s.y; P.sun_to[2] = s.z;
+    for (int k = 0; k < 3; k++) { P.sun_e[k] = sun_e[k]; P.sky[k] = sky[k]; }
+    P.sun_cos = cosf(0.5f * sun_angle_deg * 3.14159265f / 180.f);
+    P.max_b = max_b; P.seed = seed; P.eps = eps_scale * extent; P.near_clip = 0.f; P.has_n = 0; P.filter_bh = 0;
+    buildBlackmanHarrisTable(P.ftab, 64, 1.5);
+}
+
 template <int V, int TRI>
 static void ref_paths(const RefParams& P, const float4* nodes, const float4* tv, const float4* tris, const float3* albedo, int bounces,
                       int spp, int sBase, long pix0, long pix1, float* accum, long long* nClosest, long long* nShadow) {

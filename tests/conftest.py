@@ -311,7 +311,7 @@ def gpu():
 
 from importlib import import_module as _im
 _pc = _im("cuda-wavefront-pathtracer_b200.precision_check")
-classify_vs_fp64, wt32, edge_excess = _pc.classify_vs_fp64, _pc.wt32, _pc.edge_excess
+classify_vs_fp64, wt32, edge_excess, explain_differences = _pc.classify_vs_fp64, _pc.wt32, _pc.edge_excess, _pc.explain_differences
 
 
 def golden(name):

@@ -91,3 +91,30 @@ def test_precision_restatement_corners_and_edges(cwp, oracle):
     assert c["lost"] == 0, c
     ex = c["extra_mask"]
     assert np.all(edge_excess(o[ex], d[ex], bvh.verts, h[ex, 3].view(np.int32)) <= 1.0)
+
+
+def test_explain_differences_classes():
+    """The FP64 classification of disagreeing rays (used against the reference's fast-math device traversal): one
+    unit triangle in the plane z = 0 and a second one behind it at z = -1, rays straight down."""
+    from conftest import explain_differences
+    verts = np.zeros((6, 4), np.float32)
+    verts[0, :3], verts[1, :3], verts[2, :3] = (0, 0, 0), (1, 0, 0), (0, 1, 0)
+    verts[3, :3], verts[4, :3], verts[5, :3] = (-5, -5, -1), (5, -5, -1), (0, 5, -1)
+    xy = np.array([[0.25, 0.25], [0.25, 0.25], [0.5, 0.5 + 1e-9], [0.25, 0.25], [0.25, 0.25]], np.float32)
+    o = np.zeros((len(xy), 4), np.float32); o[:, :2] = xy; o[:, 2] = 1
+    d = np.zeros((len(xy), 4), np.float32); d[:, 2] = -1; d[:, 3] = 1e30
+
+    def hits(tri, t):
+        h = np.zeros((len(tri), 4), np.float32); h[:, 0] = t; h[:, 3] = np.asarray(tri, np.int32).view(np.float32)
+        return h
+    ours = hits([0, 0, 1, 1, 0], [1, 1, 2, 2, 1])
+    other = hits([0, 1, 0, 0, -1], [1, 2, 1, 1, 1e30])
+    c, rows = explain_differences(o, d, verts, ours, other)
+    cls = [r["class"] for r in rows]
+    # ray 1: ours inside and closer; ray 2: the other's triangle within 1e-9 of the edge u + v = 1; ray 3: the other
+    # reports the closer triangle, well inside it, and ours the farther one; ray 4: the other misses a hit inside
+    assert cls == ["ours_exact", "graze", "unexplained", "ours_exact"] and c["differ"] == 4
+    occ_o, occ_x = np.array([0, -1, -1, 0, 0], np.int32), np.array([0, 0, 0, -1, 0], np.int32)
+    c, rows = explain_differences(o, d, verts, occ_o, occ_x, any_hit=True)
+    # ray 1: the other's occluder is inside (we missed it); ray 2: near the edge; ray 3: ours inside
+    assert [r["class"] for r in rows] == ["unexplained", "graze", "ours_exact"]

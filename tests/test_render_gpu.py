@@ -20,13 +20,14 @@ def render(cwp, mesh, bvh, w, h, spp, batch, variant, tri=1, graph=1, bounces=4,
     return r, p, st, r.read_accum()
 
 
-@pytest.mark.parametrize("variant", [2, 8])
-def test_frame_matches_oracle(gpu, cwp, oracle, variant):
-    """64x64, 4 spp, depth 4, boxes12k: per-pixel radiance sums agree with the oracle; the only differences come from
-    the order of float atomics and ulp-level differences of sin/cos between the GPU and the host's libm (which can
-    change a rare path), so the bound is on the image error, stated here: PSNR >= 60 dB in sRGB and >= 99% of the
-    pixels within 1e-4 relative."""
-    mesh, bvh = cwp.scene("boxes12k", variant=variant, bins=32)
+@pytest.mark.parametrize("name,variant,bins,spatial", [("boxes12k", 2, 32, 0.0), ("boxes12k", 8, 32, 0.0), ("boxes117k", 8, 128, 1e-3)])
+def test_frame_matches_oracle(gpu, cwp, oracle, name, variant, bins, spatial):
+    """64x64, 4 spp, depth 4: per-pixel radiance sums agree with the oracle; the only differences come from the order
+    of float atomics and ulp-level differences of sin/cos between the GPU and the host's libm (which can change a rare
+    path), so the bound is on the image error, stated here: PSNR >= 60 dB in sRGB and >= 99% of the pixels within 1e-4
+    relative. Trees: binned SAH on config 1's scene, and the benchmark's SBVH-built CWBVH (128 bins, spatial splits
+    at overlap > 1e-3) on config 2's."""
+    mesh, bvh = cwp.scene(name, variant=variant, bins=bins, spatial=spatial)
     r, p, st, acc = render(cwp, mesh, bvh, 64, 64, 4, 4, variant)
     ref_acc, counts = oracle.render(p, variant, 1, bvh, 4, 4)
     a = acc[:, :3] / 4; b = ref_acc[:, :3] / 4
