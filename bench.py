@@ -695,6 +695,7 @@ def main():
     ap.add_argument("--slo-sweep", type=int, default=1, help="serving: also sweep arrival rates for throughput at equal p99 (1) or not (0)")
     ap.add_argument("--regroup", type=int, default=1, help="serving: sort each step's continuations by request (1) or not (0)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
+    ap.add_argument("--stage-levels", type=int, default=0, help="frames (CWBVH): top tree levels staged in shared memory per block (0 library default, -1 none, 1..3)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.batch:
@@ -746,7 +747,8 @@ def main():
         w, h, spp, K, B = wl["w"], wl["h"], wl["spp"], wl["batch"], wl["bounces"]
         p = cwp.frame_params(mesh, w, h, bounces=B)
         r = cwp.Renderer()
-        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1, traversal=args.traversal, sort=args.sort)
+        r.init(p, bvh, variant=variant, tri=1, batch=K, bounces=B, graph=args.graph, device=local, profile=1, traversal=args.traversal, sort=args.sort,
+               stage_levels=args.stage_levels)
         for _ in range(args.warmup):
             r.render(spp)
         depths = B + 2
@@ -787,6 +789,7 @@ def main():
                            "spp": spp, "batch": K, "depth": B, "layout": LAYOUT_NAMES[variant], "sah_bins": args.bins, "tri": "woop",
                            "bvh": (f"sbvh (spatial splits at overlap > {args.spatial:g} of the root area, {len(bvh.order) / mesh.n_tris:.2f} references per triangle)" if args.spatial > 0 else "binned SAH"),
                            "graph": args.graph, "traversal": ["auto", "refill", "batch"][args.traversal], "sort": ["off", "octant", "octant+cell"][args.sort],
+                           "stage_levels": args.stage_levels,
                            "l2": f"path state {STATE_BYTES * 3 * w * h * K / 1e9:.1f} GB > L2 (126 MB); scene BVH resident",
                            "rays_per_frame": (rays + shadow) / args.steps, "closest_per_frame": rays / args.steps, "shadow_per_frame": shadow / args.steps,
                            "rays_per_sample": (rays + shadow) / args.steps / (w * h * spp), "trace_shade_ms": float(tms.sum() / args.steps),

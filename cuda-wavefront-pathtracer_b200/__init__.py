@@ -33,7 +33,8 @@ class MeshView(C.Structure):
 
 
 class BuildOptions(C.Structure):
-    _fields_ = [("variant", C.c_int32), ("bins", C.c_int32), ("leaf", C.c_int32), ("collapse", C.c_int32), ("threads", C.c_int32), ("spatial", C.c_float)]
+    _fields_ = [("variant", C.c_int32), ("bins", C.c_int32), ("leaf", C.c_int32), ("collapse", C.c_int32), ("threads", C.c_int32), ("spatial", C.c_float),
+                ("builder", C.c_int32), ("device", C.c_int32)]
 
 
 class BvhData(C.Structure):
@@ -63,7 +64,7 @@ class Params(C.Structure):
 class RenderOptions(C.Structure):
     _fields_ = [("variant", C.c_int32), ("tri", C.c_int32), ("batch", C.c_int32), ("bounces", C.c_int32), ("graph", C.c_int32),
                 ("block", C.c_int32), ("device", C.c_int32), ("profile", C.c_int32), ("traversal", C.c_int32),
-                ("sort", C.c_int32), ("reserved", C.c_int32 * 2)]
+                ("sort", C.c_int32), ("stage_levels", C.c_int32), ("reserved", C.c_int32)]
 
 
 class DeviceScene(C.Structure):
@@ -356,8 +357,10 @@ class Mesh:
 class Bvh:
     """Host BVH build result: GPU node array, leaf order, packed triangles and Woop rows (numpy copies)."""
 
-    def __init__(self, mesh, variant=LAYOUT_BVH2, bins=16, leaf=4, collapse=0, threads=0, spatial=0.0):
-        o = BuildOptions(variant, bins, leaf, collapse, threads, spatial)
+    def __init__(self, mesh, variant=LAYOUT_BVH2, bins=16, leaf=4, collapse=0, threads=0, spatial=0.0, builder=0, device=0):
+        """builder 0: host binned SAH (spatial splits when spatial > 0); 1: GPU H-PLOC with SAH leaf collapse (the
+        reference's --builder hploc; build_ms is then the GPU build time)."""
+        o = BuildOptions(variant, bins, leaf, collapse, threads, spatial, builder, device)
         h = C.c_void_p()
         _check(lib().cwp_bvh_build(mesh._h, C.byref(o), C.byref(h)))
         try:
@@ -476,10 +479,10 @@ class Renderer:
         _check(lib().cwp_renderer_create(C.byref(h)))
         self._h = h
 
-    def init(self, params, bvh, variant, tri=TRI_WOOP, batch=16, bounces=4, graph=1, device=0, profile=0, traversal=0, sort=0):
+    def init(self, params, bvh, variant, tri=TRI_WOOP, batch=16, bounces=4, graph=1, device=0, profile=0, traversal=0, sort=0, stage_levels=0):
         self._params, self._bvh = params, bvh
         o = RenderOptions(); o.variant, o.tri, o.batch, o.bounces, o.graph, o.device, o.profile = variant, tri, batch, bounces, graph, device, profile
-        o.traversal, o.sort = traversal, sort
+        o.traversal, o.sort, o.stage_levels = traversal, sort, stage_levels
         self.depths = bounces + 2
         s = bvh.scene_buffers()
         _check(lib().cwp_renderer_init(self._h, C.byref(params), C.byref(s), C.byref(o)))

@@ -1,250 +1,275 @@
-// bsdf.cuh - OpenPBR-subset materials (host + device) for the serving form's integrator.
+// bsdf.cuh - the serving integrator's materials, an OpenPBR subset (host + device code).
 //
-// cwp_material (64 B) blends three bases linearly: metallic -> rough conductor; (1 - metallic) transmission -> rough
-// dielectric (reflection + refraction); the rest -> glossy-diffuse (a GGX dielectric specular lobe over a Lambertian
-// base). Roughness r gives GGX alpha = r^2; alpha below kDeltaAlpha is a perfectly specular lobe. The semantics follow
-// the reference's render/bsdf.h and scene/material.h (same lobes, weights and sample weights, so images agree); the
-// formulas are those of the cited papers:
-//   GGX distribution, height-correlated Smith masking-shadowing ... Walter et al. 2007; Heitz, JCGT 2014
-//   visible-normal sampling with spherical caps .................. Dupuy & Benyoub, HPG 2023
-//   exact unpolarised dielectric Fresnel, rough refraction ....... Walter et al. 2007 (energy convention: no eta^2)
-//   conductor Fresnel: Schlick with the F82 tint term ............ Kutz et al. 2021, as specified by OpenPBR 1.0
-// Frame: z = shading normal, wo.z > 0 (towards the viewer). eval() returns f and the solid-angle pdf of the non-delta
-// lobes; sample() returns wi, weight = f |cos| / pdf and pdf (0 marks a delta sample).
+// A material (cwp_material, 64 B) is a fixed mix of three bases, weighted metal = metallic, glass =
+// (1 - metallic) transmission, gloss = (1 - metallic)(1 - transmission):
+//   metal  a rough conductor whose reflectance is the F82-tint Fresnel curve of (base colour, specular colour),
+//          scaled by the specular weight;
+//   glass  a rough dielectric interface that reflects and refracts (exact Fresnel), refraction tinted by the base colour;
+//   gloss  an opaque dielectric: a GGX specular layer (specular weight, IOR) over a Lambertian base colour.
+// All three share one GGX microfacet distribution with alpha = roughness^2; alpha below kSmoothAlpha is a smooth
+// surface (a Dirac lobe, sampled but never evaluated).
+//
+// What an image depends on - which lobes exist, their weights, how a sample picks a base and spends the random
+// numbers (u, u1, u2, and ux1, ux2 for the gloss base's albedo estimate), the delta conventions - is the reference's
+// (render/bsdf.h), so that both integrators render the same images. The formulas are written here from the papers:
+//   GGX normal distribution, the generalised half vector of refraction and its Jacobian, and the exact unpolarised
+//     Fresnel reflectance in its g-form: Walter, Marschner, Li, Torrance, EGSR 2007 (eqs. 13-17, 21-22, 33)
+//   height-correlated Smith masking-shadowing, G2 = 1 / (1 + Lambda(o) + Lambda(i)), and the distribution of visible
+//     normals D_wo(m) = G1(wo) max(0, wo.m) D(m) / wo.z: Heitz, JCGT 2014
+//   sampling the visible normals with spherical caps: Dupuy & Benyoub, HPG 2023
+//   the conductor's F82-tint Fresnel: Kutz, Hasan, Edmondson 2021, as specified by OpenPBR 1.0
+//   the bump-terminator shadowing of the diffuse base: Chiang, Li, Burley, SIGGRAPH 2019 talk
+//   the power heuristic: Veach 1997
+// Transmission keeps the energy convention: a lossless smooth interface passes a throughput of 1 - F both ways (no
+// eta^2 radiance scaling).
+// Conventions: local frame with z = the shading normal, wo.z > 0 (towards the viewer). bsdf_eval returns f and the
+// solid-angle pdf of the non-delta lobes; bsdf_sample returns wi, weight = f |cos| / pdf and pdf (0 = a delta sample).
 #pragma once
 #include "cwp_b200.h"
 #include "vecmath.h"
 
 namespace cwpb {
 
-static constexpr float kDeltaAlpha = 1e-3f;
 #define CWPB_PI 3.14159265f
+static constexpr float kSmoothAlpha = 1e-3f;
 
-CWPB_HD float luminance(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+CWPB_HD float luminance(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }   // Rec. 709 weights
 CWPB_HD float3 mat_v3(const float* a) { return f3(a[0], a[1], a[2]); }
-
-// ---- microfacet terms ----
-CWPB_HD float ggx_ndf(float cosM, float a2) {
-    if (cosM <= 0.f) return 0.f;
-    const float c2 = cosM * cosM, k = c2 * (a2 - 1.f) + 1.f;
-    return a2 / (CWPB_PI * k * k);
-}
-CWPB_HD float smith_lambda(float cosW, float a2) {
-    const float c2 = cosW * cosW;
-    if (c2 < 1e-12f) return 1e12f;
-    return 0.5f * (sqrtf(1.f + a2 * (1.f - c2) / c2) - 1.f);
-}
-CWPB_HD float smith_g1(float cosW, float a2) { return 1.f / (1.f + smith_lambda(cosW, a2)); }
-CWPB_HD float smith_g2(float cosO, float cosI, float a2) { return 1.f / (1.f + smith_lambda(cosO, a2) + smith_lambda(cosI, a2)); }
-// density of the normals visible from wo: G1(wo) max(0, wo.m) D(m) / wo.z
-CWPB_HD float vndf_pdf(float3 wo, float3 m, float a2) {
-    const float om = dot(wo, m);
-    if (om <= 0.f || m.z <= 0.f) return 0.f;
-    return smith_g1(wo.z, a2) * om * ggx_ndf(m.z, a2) / wo.z;
-}
-// a visible normal: the hemisphere configuration of wo stretched to alpha 1, a uniform point on the spherical cap
-// below it, shifted by the stretched view direction and unstretched
-CWPB_HD float3 vndf_sample(float3 wo, float a, float u1, float u2) {
-    const float3 v = normalize(f3(a * wo.x, a * wo.y, wo.z));
-    const float phi = CWPB_TWO_PI * u1;
-    const float z = (1.f - u2) * (1.f + v.z) - v.z;
-    const float s = sqrtf(fminf(fmaxf(1.f - z * z, 0.f), 1.f));
-    const float3 h = f3(s * cosf(phi) + v.x, s * sinf(phi) + v.y, z + v.z);
-    return normalize(f3(a * h.x, a * h.y, fmaxf(h.z, 0.f)));
-}
-
-// ---- Fresnel ----
-// unpolarised dielectric reflectance; cosI > 0 on the incident side, eta = n_transmitted / n_incident
-CWPB_HD float fresnel_dielectric(float cosI, float eta) {
-    const float sin2T = (1.f - cosI * cosI) / (eta * eta);
-    if (sin2T >= 1.f) return 1.f;   // total internal reflection
-    const float cosT = sqrtf(1.f - sin2T);
-    const float rs = (cosI - eta * cosT) / (cosI + eta * cosT), rp = (eta * cosI - cosT) / (eta * cosI + cosT);
-    return 0.5f * (rs * rs + rp * rp);
-}
-// Schlick's curve from F0 minus b mu (1 - mu)^6, with b chosen so that the curve equals tint x Schlick at
-// mu = 1/7 (the angle of the F82 measurement): F82 tint correction of OpenPBR's conductor
-CWPB_HD float3 fresnel_f82(float3 F0, float3 tint, float mu) {
-    mu = fminf(fmaxf(mu, 0.f), 1.f);
-    const float q = 1.f - mu, q2 = q * q, q5 = q2 * q2 * q, q6 = q5 * q;
-    const float mb = 1.f / 7.f, qb = 6.f / 7.f, qb2 = qb * qb, qb5 = qb2 * qb2 * qb, qb6 = qb5 * qb;
-    const float3 one = f3(1.f, 1.f, 1.f);
-    const float3 schlick = F0 + (one - F0) * q5;
-    const float3 schlickB = F0 + (one - F0) * qb5;
-    const float3 b = schlickB * (one - tint) * (1.f / (mb * qb6));
-    const float3 F = schlick - b * (mu * q6);
-    return f3(fminf(fmaxf(F.x, 0.f), 1.f), fminf(fmaxf(F.y, 0.f), 1.f), fminf(fmaxf(F.z, 0.f), 1.f));
-}
+CWPB_HD float sat(float x) { return fminf(fmaxf(x, 0.f), 1.f); }
+CWPB_HD float3 reflect_about(float3 w, float3 m, float wm) { return m * (2.f * wm) - w; }
 
 struct BsdfValue { float3 f; float pdf; };
 
-// ---- glossy-diffuse base: GGX dielectric specular (weight ws, ior) + Lambertian base colour weighted by kd ----
-// energy = 0: kd = 1 - ws F(wo.z). energy = 1: kd = 1 - X with X = ws F(wo.m) G2 / G1(wo) for one visible normal m
-// drawn from (ux1, ux2), an unbiased estimate of the specular lobe's directional albedo. Lobe choice uses F(wo.z).
-// bump-terminator shadowing of the diffuse lobe (Chiang, Li, Burley, "Taming the Shadow Terminator", SIGGRAPH 2019
-// talk): nr = the unperturbed normal in the frame of the mapped shading normal, g = (nr . wi) / (wi.z nr.z), G = g +
-// g^2 - g^3 on [0, 1), 1 above, 0 below; nr = +z gives G = 1 exactly (the term off)
-CWPB_HD float bump_shadowing(float3 nr, float3 wi) {
-    if (nr.z >= 1.f) return 1.f;
-    const float g = dot(nr, wi) / (wi.z * nr.z);
-    if (g >= 1.f) return 1.f;
-    if (g < 0.f) return 0.f;
-    return g + g * g - g * g * g;
-}
-
-struct GlossyDiffuseLobe {
-    float3 base; float ws, eta, a, a2, Fo, pSpec, kd; bool delta; float3 nr = f3(0.f, 0.f, 1.f);
-    CWPB_HD GlossyDiffuseLobe(const cwp_material& m, float3 wo, int energy, float ux1, float ux2) {
-        base = mat_v3(m.base_color); ws = m.specular_weight; eta = m.ior; a = m.roughness * m.roughness; a2 = a * a; delta = a < kDeltaAlpha;
-        Fo = ws > 0.f ? ws * fresnel_dielectric(wo.z, eta) : 0.f;
-        const float pd = (1.f - Fo) * luminance(base);
-        pSpec = Fo + pd > 0.f ? Fo / (Fo + pd) : 0.f;
-        kd = 1.f - Fo;
-        if (energy && ws > 0.f && !delta) {
-            const float3 mm = vndf_sample(wo, a, ux1, ux2);
-            const float om = dot(wo, mm);
-            const float3 wr = mm * (2.f * om) - wo;
-            const float X = (om > 0.f && wr.z > 0.f) ? ws * fresnel_dielectric(om, eta) * smith_g2(wo.z, wr.z, a2) / smith_g1(wo.z, a2) : 0.f;
-            kd = 1.f - X;
-        }
-        kd = fmaxf(kd, 0.f);
+// ---- the isotropic GGX microfacet model ----
+struct Ggx {
+    float alpha, a2;
+    bool smooth;
+    CWPB_HD explicit Ggx(float roughness) : alpha(roughness * roughness), a2(alpha * alpha), smooth(alpha < kSmoothAlpha) {}
+    // D(m) = a^2 / (pi ((a^2 - 1) cos^2 + 1)^2) for cos > 0
+    CWPB_HD float D(float cosM) const {
+        if (!(cosM > 0.f)) return 0.f;
+        const float t = (a2 - 1.f) * (cosM * cosM) + 1.f;
+        return a2 / (CWPB_PI * t * t);
     }
-    CWPB_HD BsdfValue eval(float3 wo, float3 wi) const {
-        BsdfValue r{ f3(0.f, 0.f, 0.f), 0.f };
-        if (wi.z <= 0.f) return r;
-        r.f = base * (kd * CWPB_INV_PI * bump_shadowing(nr, wi)); r.pdf = (1.f - pSpec) * wi.z * CWPB_INV_PI;
-        if (!delta && Fo > 0.f) {
-            const float3 m = normalize(wo + wi); const float om = dot(wo, m);
-            if (om > 0.f) {
-                const float spec = ws * fresnel_dielectric(om, eta) * ggx_ndf(m.z, a2) * smith_g2(wo.z, wi.z, a2) / (4.f * wo.z * wi.z);
-                r.f = r.f + f3(spec, spec, spec); r.pdf += pSpec * vndf_pdf(wo, m, a2) / (4.f * om);
-            }
-        }
-        return r;
+    // Smith's Lambda: (sqrt(1 + a^2 tan^2) - 1) / 2, unbounded at grazing
+    CWPB_HD float Lambda(float cosW) const {
+        const float c2 = cosW * cosW;
+        if (c2 < 1e-12f) return 1e12f;
+        const float tan2 = (1.f - c2) / c2;
+        return 0.5f * (sqrtf(1.f + a2 * tan2) - 1.f);
     }
-    CWPB_HD bool sample(float3 wo, float u, float u1, float u2, float3& wi, float3& w, float& pdf) const {
-        if (u < pSpec) {
-            if (delta) { wi = f3(-wo.x, -wo.y, wo.z); const float s = Fo / pSpec; w = f3(s, s, s); pdf = 0.f; return true; }
-            const float3 m = vndf_sample(wo, a, u1, u2); wi = m * (2.f * dot(wo, m)) - wo;
-            if (wi.z <= 0.f) return false;
-        } else {
-            wi = cosine_dir(f3(0.f, 0.f, 1.f), u1, u2);
-            if (wi.z <= 0.f) return false;
-        }
-        const BsdfValue e = eval(wo, wi);
-        if (e.pdf <= 0.f) return false;
-        w = e.f * (wi.z / e.pdf); pdf = e.pdf; return true;
+    CWPB_HD float G1(float cosW) const { return 1.f / (1.f + Lambda(cosW)); }
+    CWPB_HD float G2(float cosO, float cosI) const { return 1.f / (1.f + Lambda(cosO) + Lambda(cosI)); }
+    // density of the normals visible from wo
+    CWPB_HD float visible_pdf(float3 wo, float3 m) const {
+        const float wm = dot(wo, m);
+        if (wm <= 0.f || m.z <= 0.f) return 0.f;
+        return G1(wo.z) * wm * D(m.z) / wo.z;
+    }
+    // a visible normal: wo stretched to the alpha = 1 configuration, a uniform point on the spherical cap of the unit
+    // sphere below the stretched direction, offset by it, then unstretched (Dupuy & Benyoub)
+    CWPB_HD float3 sample_visible(float3 wo, float u1, float u2) const {
+        const float3 s = normalize(f3(alpha * wo.x, alpha * wo.y, wo.z));
+        const float z = (1.f - u2) * (1.f + s.z) - s.z;
+        const float r = sqrtf(sat(1.f - z * z)), phi = CWPB_TWO_PI * u1;
+        const float3 h = f3(r * cosf(phi) + s.x, r * sinf(phi) + s.y, z + s.z);
+        return normalize(f3(alpha * h.x, alpha * h.y, fmaxf(h.z, 0.f)));
     }
 };
 
-// ---- metallic base: rough conductor, F = ws F82(base colour, specular colour) ----
-struct ConductorLobe {
-    float3 F0, tint; float ws, a, a2; bool delta;
-    CWPB_HD explicit ConductorLobe(const cwp_material& m) { F0 = mat_v3(m.base_color); tint = mat_v3(m.specular_color); ws = m.specular_weight; a = m.roughness * m.roughness; a2 = a * a; delta = a < kDeltaAlpha; }
-    CWPB_HD BsdfValue eval(float3 wo, float3 wi) const {
+// ---- Fresnel reflectance ----
+// exact unpolarised reflectance of a dielectric interface at |cos| = c, eta = n(transmitted side) / n(incident side):
+// with g^2 = eta^2 - 1 + c^2 (negative: total internal reflection),
+// F = 1/2 ((g - c) / (g + c))^2 (1 + ((c (g + c) - 1) / (c (g - c) + 1))^2)
+CWPB_HD float fresnel_exact(float c, float eta) {
+    const float g2 = eta * eta - 1.f + c * c;
+    if (g2 <= 0.f) return 1.f;
+    const float g = sqrtf(g2);
+    const float p = (g - c) / (g + c), q = (c * (g + c) - 1.f) / (c * (g - c) + 1.f);
+    return 0.5f * p * p * (1.f + q * q);
+}
+// F82-tint conductor reflectance: Schlick's curve S(mu) = F0 + (1 - F0)(1 - mu)^5 lowered by b mu (1 - mu)^6, where
+// b makes the curve equal tint x S at mu = 1/7; clamped to [0, 1] per channel
+struct F82Curve {
+    float q5, lower;   // (1 - mu)^5 and mu (1 - mu)^6 / (mu_b (1 - mu_b)^6) at this mu
+    static constexpr float muB = 1.f / 7.f, qB = 1.f - muB, qB5 = qB * qB * qB * qB * qB;
+    CWPB_HD explicit F82Curve(float mu) {
+        mu = sat(mu);
+        const float q = 1.f - mu;
+        q5 = (q * q) * (q * q) * q;
+        lower = mu * q5 * q * (1.f / (muB * qB5 * qB));
+    }
+    CWPB_HD float channel(float f0, float tint) const {
+        const float schlick = f0 + (1.f - f0) * q5, schlickB = f0 + (1.f - f0) * qB5;
+        return sat(schlick - schlickB * (1.f - tint) * lower);
+    }
+};
+CWPB_HD float3 fresnel_conductor(float3 F0, float3 tint, float mu) {
+    const F82Curve c(mu);
+    return f3(c.channel(F0.x, tint.x), c.channel(F0.y, tint.y), c.channel(F0.z, tint.z));
+}
+
+// ---- bump-terminator shadowing of the diffuse base ----
+// nr = the unperturbed normal in the frame of the mapped shading normal; g = (nr . wi) / (wi.z nr.z) is the ratio
+// of the two cosines; the smooth step g (1 + g (1 - g)) on [0, 1), 1 above, 0 below. nr = +z switches it off.
+CWPB_HD float terminator_shadowing(float3 nr, float3 wi) {
+    if (nr.z >= 1.f) return 1.f;
+    const float g = dot(nr, wi) / (wi.z * nr.z);
+    return g >= 1.f ? 1.f : (g < 0.f ? 0.f : g * (1.f + g * (1.f - g)));
+}
+
+// ---- one shading vertex: the three bases of a material for one outgoing direction ----
+struct PbrVertex {
+    const cwp_material& m;
+    Ggx ggx;
+    float wMetal, wGlass, wGloss;   // base weights
+    float eta;                      // relative IOR of the glass base at this side
+    // gloss base: Fresnel at the normal (times the specular weight), probability of sampling its specular layer and
+    // the diffuse scale kd; nr for the terminator term
+    float glossF, glossPSpec, glossKd;
+    float3 nr;
+
+    CWPB_HD PbrVertex(const cwp_material& mat, float3 wo, float etaRel, int gdEnergy, float ux1, float ux2, float3 nrLocal)
+        : m(mat), ggx(mat.roughness), eta(etaRel), glossF(0.f), glossPSpec(0.f), glossKd(1.f), nr(nrLocal) {
+        wMetal = m.metallic;
+        wGlass = (1.f - m.metallic) * m.transmission;
+        wGloss = (1.f - m.metallic) * (1.f - m.transmission);
+        if (wGloss > 0.f) {
+            const float ws = m.specular_weight;
+            if (ws > 0.f) glossF = ws * fresnel_exact(wo.z, m.ior);
+            const float diffuse = (1.f - glossF) * luminance(mat_v3(m.base_color));
+            glossPSpec = glossF + diffuse > 0.f ? glossF / (glossF + diffuse) : 0.f;
+            float spec = glossF;   // the specular layer's albedo: F at the normal, or one visible-normal estimate of it
+            if (gdEnergy && ws > 0.f && !ggx.smooth) {
+                const float3 mm = ggx.sample_visible(wo, ux1, ux2);
+                const float wm = dot(wo, mm);
+                const float3 wr = reflect_about(wo, mm, wm);
+                spec = (wm > 0.f && wr.z > 0.f) ? ws * fresnel_exact(wm, m.ior) * ggx.G2(wo.z, wr.z) / ggx.G1(wo.z) : 0.f;
+            }
+            glossKd = fmaxf(1.f - spec, 0.f);
+        }
+    }
+
+    // every non-delta lobe at (wo, wi): the material's f and pdf; with base >= 0 also that base's own (unweighted)
+    // pdf in *ownPdf, from the same terms
+    CWPB_HD BsdfValue eval(float3 wo, float3 wi, int base = -1, float* ownPdf = nullptr) const {
         BsdfValue r{ f3(0.f, 0.f, 0.f), 0.f };
-        if (delta || wi.z <= 0.f) return r;
-        const float3 m = normalize(wo + wi); const float om = dot(wo, m);
-        if (om <= 0.f) return r;
-        r.f = fresnel_f82(F0, tint, om) * (ws * ggx_ndf(m.z, a2) * smith_g2(wo.z, wi.z, a2) / (4.f * wo.z * wi.z));
-        r.pdf = vndf_pdf(wo, m, a2) / (4.f * om);
+        float o = 0.f;
+        auto add = [&](int b, float weight, float3 f, float pdf) {
+            r.f = r.f + f * weight; r.pdf += weight * pdf;
+            if (b == base) o = pdf;
+        };
+        if (wi.z > 0.f) {
+            // reflection: the terms every reflecting lobe shares for the half vector of (wo, wi)
+            const float3 h = normalize(wo + wi);
+            const float wh = dot(wo, h);
+            const bool rough = !ggx.smooth && wh > 0.f;
+            float micro = 0.f, pdfH = 0.f;   // D G2 / (4 wo.z wi.z) and the reflection pdf of the visible normals
+            if (rough) { micro = ggx.D(h.z) * ggx.G2(wo.z, wi.z) / (4.f * wo.z * wi.z); pdfH = ggx.visible_pdf(wo, h) / (4.f * wh); }
+            if (wMetal > 0.f && rough) add(0, wMetal, fresnel_conductor(mat_v3(m.base_color), mat_v3(m.specular_color), wh) * (m.specular_weight * micro), pdfH);
+            if (wGlass > 0.f && rough) { const float F = fresnel_exact(wh, eta); add(1, wGlass, f3(F * micro, F * micro, F * micro), F * pdfH); }
+            if (wGloss > 0.f) {
+                float3 f = mat_v3(m.base_color) * (glossKd * CWPB_INV_PI * terminator_shadowing(nr, wi));
+                float pdf = (1.f - glossPSpec) * wi.z * CWPB_INV_PI;
+                if (rough && glossF > 0.f) {
+                    const float s = m.specular_weight * fresnel_exact(wh, m.ior) * micro;
+                    f = f + f3(s, s, s); pdf += glossPSpec * pdfH;
+                }
+                add(2, wGloss, f, pdf);
+            }
+        } else if (wi.z < 0.f && wGlass > 0.f && !ggx.smooth) {
+            // refraction through the glass base: generalised half vector h ~ wo + eta wi on the wo side
+            float3 h = normalize(wo + wi * eta);
+            if (h.z < 0.f) h = -h;
+            const float wh = dot(wo, h), ih = dot(wi, h);
+            const float F = wh > 0.f && ih < 0.f ? fresnel_exact(wh, eta) : 1.f;
+            if (F < 1.f) {
+                const float den = wh + eta * ih;
+                const float jacobian = eta * eta * -ih / (den * den);   // |dh / dwi|
+                add(1, wGlass, mat_v3(m.base_color) * ((1.f - F) * ggx.D(h.z) * ggx.G2(wo.z, -wi.z) * wh * jacobian / (wo.z * -wi.z)),
+                    (1.f - F) * ggx.visible_pdf(wo, h) * jacobian);
+            }
+        }
+        if (ownPdf) *ownPdf = o;
         return r;
     }
-    CWPB_HD bool sample(float3 wo, float u1, float u2, float3& wi, float3& w, float& pdf) const {
-        if (delta) { wi = f3(-wo.x, -wo.y, wo.z); w = fresnel_f82(F0, tint, wo.z) * ws; pdf = 0.f; return true; }
-        const float3 m = vndf_sample(wo, a, u1, u2); const float om = dot(wo, m);
-        wi = m * (2.f * om) - wo;
-        if (wi.z <= 0.f || om <= 0.f) return false;
-        w = fresnel_f82(F0, tint, om) * (ws * smith_g2(wo.z, wi.z, a2) / smith_g1(wo.z, a2));   // F G2 / G1(wo)
-        pdf = vndf_pdf(wo, m, a2) / (4.f * om);
+
+    // a direction from one base, chosen by u; the weight covers the whole material
+    CWPB_HD bool sample(float3 wo, float u, float u1, float u2, float3& wi, float3& w, float& pdf) const {
+        int base; float uu = 0.f;
+        if (u < wMetal) base = 0;
+        else if (u < wMetal + wGlass) { base = 1; uu = fminf((u - wMetal) / wGlass, 0.99999994f); }
+        else { base = 2; uu = fminf(wGloss > 0.f ? (u - wMetal - wGlass) / wGloss : 0.f, 0.99999994f); }
+        bool delta = false;
+        if (base == 0) {
+            if (ggx.smooth) {
+                wi = f3(-wo.x, -wo.y, wo.z);
+                w = fresnel_conductor(mat_v3(m.base_color), mat_v3(m.specular_color), wo.z) * m.specular_weight;
+                delta = true;
+            } else {
+                const float3 h = ggx.sample_visible(wo, u1, u2);
+                const float wh = dot(wo, h);
+                wi = reflect_about(wo, h, wh);
+                if (wi.z <= 0.f || wh <= 0.f) return false;
+                // f cos / pdf of the conductor alone: F ws G2 / G1(wo)
+                w = fresnel_conductor(mat_v3(m.base_color), mat_v3(m.specular_color), wh) * (m.specular_weight * ggx.G2(wo.z, wi.z) / ggx.G1(wo.z));
+                pdf = ggx.visible_pdf(wo, h) / (4.f * wh);
+            }
+        } else if (base == 1) {
+            const float3 h = ggx.smooth ? f3(0.f, 0.f, 1.f) : ggx.sample_visible(wo, u1, u2);
+            const float wh = dot(wo, h);
+            if (wh <= 0.f) return false;
+            if (uu < fresnel_exact(wh, eta)) {   // reflect
+                wi = reflect_about(wo, h, wh);
+                if (wi.z <= 0.f) return false;
+                if (ggx.smooth) { w = f3(1.f, 1.f, 1.f); delta = true; }
+            } else {                              // refract (Snell's law about h)
+                const float cosT = sqrtf(fmaxf(1.f - (1.f - wh * wh) / (eta * eta), 0.f));
+                wi = wo * (-1.f / eta) + h * (wh / eta - cosT);
+                if (wi.z >= 0.f) return false;
+                wi = normalize(wi);
+                if (ggx.smooth) { w = mat_v3(m.base_color); delta = true; }
+            }
+        } else {
+            if (uu < glossPSpec) {
+                if (ggx.smooth) { wi = f3(-wo.x, -wo.y, wo.z); const float s = glossF / glossPSpec; w = f3(s, s, s); delta = true; }
+                else {
+                    const float3 h = ggx.sample_visible(wo, u1, u2);
+                    wi = reflect_about(wo, h, dot(wo, h));
+                    if (wi.z <= 0.f) return false;
+                }
+            } else {
+                wi = cosine_dir(f3(0.f, 0.f, 1.f), u1, u2);
+                if (wi.z <= 0.f) return false;
+            }
+        }
+        if (delta) { pdf = 0.f; return true; }                       // no other base has density on a Dirac lobe
+        if (base == 0 && wMetal == 1.f) return true;                  // the metal alone: its closed-form weight
+        float ownPdf;
+        const BsdfValue e = eval(wo, wi, base, &ownPdf);
+        if (base != 0 && !(ownPdf > 0.f)) return false;               // the sampled base has no density there
+        // (with one base of weight 1 the material's f and pdf are that base's own, so one formula covers both)
+        if (e.pdf <= 0.f) return false;
+        w = e.f * (fabsf(wi.z) / e.pdf); pdf = e.pdf;
         return true;
     }
 };
 
-// ---- transmissive base: rough dielectric; eta = n(other side) / n(wo side); refraction tinted by the base colour ----
-struct DielectricLobe {
-    float3 tint; float eta, a, a2; bool delta;
-    CWPB_HD DielectricLobe(const cwp_material& m, float etaRel) { tint = mat_v3(m.base_color); eta = etaRel; a = m.roughness * m.roughness; a2 = a * a; delta = a < kDeltaAlpha; }
-    CWPB_HD BsdfValue eval(float3 wo, float3 wi) const {
-        BsdfValue r{ f3(0.f, 0.f, 0.f), 0.f };
-        if (delta) return r;
-        if (wi.z > 0.f) {
-            const float3 m = normalize(wo + wi); const float om = dot(wo, m);
-            if (om <= 0.f) return r;
-            const float F = fresnel_dielectric(om, eta);
-            const float s = F * ggx_ndf(m.z, a2) * smith_g2(wo.z, wi.z, a2) / (4.f * wo.z * wi.z);
-            r.f = f3(s, s, s); r.pdf = F * vndf_pdf(wo, m, a2) / (4.f * om);
-        } else if (wi.z < 0.f) {
-            float3 m = normalize(wo + wi * eta);   // generalised half vector of refraction
-            if (m.z < 0.f) m = -m;
-            const float om = dot(wo, m), im = dot(wi, m);
-            if (om <= 0.f || im >= 0.f) return r;
-            const float F = fresnel_dielectric(om, eta);
-            if (F >= 1.f) return r;
-            const float den = om + eta * im, jac = eta * eta * (-im) / (den * den);   // |dm / dwi|
-            const float s = (1.f - F) * ggx_ndf(m.z, a2) * smith_g2(wo.z, -wi.z, a2) * om * jac / (wo.z * -wi.z);
-            r.f = tint * s; r.pdf = (1.f - F) * vndf_pdf(wo, m, a2) * jac;
-        }
-        return r;
-    }
-    CWPB_HD bool sample(float3 wo, float u, float u1, float u2, float3& wi, float3& w, float& pdf) const {
-        const float3 m = delta ? f3(0.f, 0.f, 1.f) : vndf_sample(wo, a, u1, u2);
-        const float om = dot(wo, m);
-        if (om <= 0.f) return false;
-        const float F = fresnel_dielectric(om, eta);
-        if (u < F) {
-            wi = m * (2.f * om) - wo;
-            if (wi.z <= 0.f) return false;
-            if (delta) { w = f3(1.f, 1.f, 1.f); pdf = 0.f; return true; }
-        } else {
-            const float cosT = sqrtf(fmaxf(1.f - (1.f - om * om) / (eta * eta), 0.f));
-            wi = wo * (-1.f / eta) + m * (om / eta - cosT);
-            if (wi.z >= 0.f) return false;
-            wi = normalize(wi);
-            if (delta) { w = tint; pdf = 0.f; return true; }
-        }
-        const BsdfValue e = eval(wo, wi);
-        if (e.pdf <= 0.f) return false;
-        w = e.f * (fabsf(wi.z) / e.pdf); pdf = e.pdf; return true;
-    }
-};
-
-// ---- the blended material ----
-CWPB_HD void base_weights(const cwp_material& m, float& wM, float& wT, float& wD) {
-    wM = m.metallic; wT = (1.f - m.metallic) * m.transmission; wD = (1.f - m.metallic) * (1.f - m.transmission);
-}
-// some lobe has a density (light sampling can help)
+// some lobe of the material has a density, so light sampling can contribute
 CWPB_HD bool has_non_delta(const cwp_material& m) {
-    float wM, wT, wD; base_weights(m, wM, wT, wD);
-    const bool rough = m.roughness * m.roughness >= kDeltaAlpha;
-    return (wD > 0.f && (luminance(mat_v3(m.base_color)) > 0.f || rough)) || ((wM > 0.f || wT > 0.f) && rough);
+    const float wMetal = m.metallic, wGlass = (1.f - m.metallic) * m.transmission, wGloss = (1.f - m.metallic) * (1.f - m.transmission);
+    const bool rough = m.roughness * m.roughness >= kSmoothAlpha;
+    return (wGloss > 0.f && (rough || luminance(mat_v3(m.base_color)) > 0.f)) || (rough && (wMetal > 0.f || wGlass > 0.f));
 }
-// nr: the unperturbed normal for the bump-terminator term, +z = off
+// f and pdf of the material; nr is the unperturbed normal for the terminator term (+z: off)
 CWPB_HD BsdfValue bsdf_eval(const cwp_material& m, float3 wo, float3 wi, float etaRel, int gdEnergy, float ux1, float ux2, float3 nr = f3(0.f, 0.f, 1.f)) {
-    float wM, wT, wD; base_weights(m, wM, wT, wD);
-    BsdfValue r{ f3(0.f, 0.f, 0.f), 0.f };
-    if (wM > 0.f) { const BsdfValue e = ConductorLobe(m).eval(wo, wi); r.f = r.f + e.f * wM; r.pdf += wM * e.pdf; }
-    if (wT > 0.f) { const BsdfValue e = DielectricLobe(m, etaRel).eval(wo, wi); r.f = r.f + e.f * wT; r.pdf += wT * e.pdf; }
-    if (wD > 0.f) { GlossyDiffuseLobe g(m, wo, gdEnergy, ux1, ux2); g.nr = nr; const BsdfValue e = g.eval(wo, wi); r.f = r.f + e.f * wD; r.pdf += wD * e.pdf; }
-    return r;
+    return PbrVertex(m, wo, etaRel, gdEnergy, ux1, ux2, nr).eval(wo, wi);
 }
-// one base chosen by u (one-sample MIS over the bases); weight of the whole material, pdf 0 for delta samples
 CWPB_HD bool bsdf_sample(const cwp_material& m, float3 wo, float etaRel, int gdEnergy, float ux1, float ux2, float u, float u1, float u2,
                          float3& wi, float3& weight, float& pdf, float3 nr = f3(0.f, 0.f, 1.f)) {
-    float wM, wT, wD; base_weights(m, wM, wT, wD);
-    bool ok;
-    if (u < wM) ok = ConductorLobe(m).sample(wo, u1, u2, wi, weight, pdf);
-    else if (u < wM + wT) ok = DielectricLobe(m, etaRel).sample(wo, fminf((u - wM) / wT, 0.99999994f), u1, u2, wi, weight, pdf);
-    else { GlossyDiffuseLobe g(m, wo, gdEnergy, ux1, ux2); g.nr = nr; ok = g.sample(wo, fminf(wD > 0.f ? (u - wM - wT) / wD : 0.f, 0.99999994f), u1, u2, wi, weight, pdf); }
-    if (!ok) return false;
-    if (pdf <= 0.f) return true;                          // a delta sample: no other base has density there
-    if (wM == 1.f || wT == 1.f || wD == 1.f) return true;  // one base: its own weight is already f |cos| / pdf
-    const BsdfValue e = bsdf_eval(m, wo, wi, etaRel, gdEnergy, ux1, ux2, nr);
-    if (e.pdf <= 0.f) return false;
-    weight = e.f * (fabsf(wi.z) / e.pdf); pdf = e.pdf;
-    return true;
+    return PbrVertex(m, wo, etaRel, gdEnergy, ux1, ux2, nr).sample(wo, u, u1, u2, wi, weight, pdf);
 }
-// power heuristic (Veach 1997), beta = 2
+// power heuristic with exponent 2
 CWPB_HD float mis_power(float a, float b) { const float a2 = a * a; return a2 / (a2 + b * b); }
 
 }  // namespace cwpb

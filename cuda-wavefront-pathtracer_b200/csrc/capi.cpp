@@ -1,5 +1,6 @@
 // capi.cpp - C entry points: errors, meshes, host BVH builds, camera and parameter helpers.
 #include "host_bvh.h"
+#include "hploc.h"
 #include "runtime.h"
 #include <chrono>
 #include <cmath>
@@ -108,8 +109,16 @@ extern "C" int cwp_bvh_build(const cwp_mesh* h, const cwp_build_options* o, cwp_
     so.leafMax = cw ? 1 : (o->variant == 8 && o->leaf > 4) ? 4 : o->leaf;
     CWPB_CHECK(o->variant == 8 || so.leafMax <= 64, CWP_ERR_INVALID, "leaf too large");
     CWPB_CHECK(o->spatial >= 0.f && o->spatial < 1.f, CWP_ERR_INVALID, "spatial %g out of [0, 1)", o->spatial);
+    CWPB_CHECK(o->builder == 0 || o->builder == 1, CWP_ERR_INVALID, "builder %d is not 0 (host SAH) or 1 (GPU H-PLOC)", o->builder);
+    CWPB_CHECK(o->builder == 0 || o->spatial == 0.f, CWP_ERR_INVALID, "spatial splits need the host builder");
     BinaryBvh B;
-    if (o->spatial > 0.f) build_sbvh(m, so, o->spatial, 0.3f, B); else build_sah(m, so, B);
+    double gpuMs = -1.0;
+    if (o->builder == 1) {
+        std::vector<float4> hn;
+        if (int rc = hploc_build_mesh(m.v.data(), m.f.data(), (int64_t)m.nt(), o->device, hn, gpuMs)) return rc;
+        tree_from_hploc(hn, (int64_t)m.nt(), so.leafMax, B);
+    } else if (o->spatial > 0.f) build_sbvh(m, so, o->spatial, 0.3f, B);
+    else build_sah(m, so, B);
     cwp_bvh* r = new cwp_bvh();
     r->maxDepth = B.maxDepth;
     if (o->variant == 2) { r->sah = sah_cost(B, 1, 1); layout_bvh2(B, r->nodes); r->order = B.prim; r->stride = 4; }
@@ -123,7 +132,7 @@ extern "C" int cwp_bvh_build(const cwp_mesh* h, const cwp_build_options* o, cwp_
     pack_tris(m, r->order, r->tris, r->nrm);
     pack_woop(m, r->order, r->woop);
     pack_verts(m, r->order, r->verts);
-    r->ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    r->ms = gpuMs >= 0.0 ? gpuMs : std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (o->variant != 8 && B.maxDepth > 63) { delete r; return set_error(CWP_ERR_INVALID, "BVH depth %d exceeds the traversal stack (64)", B.maxDepth); }
     *out = r; return CWP_OK;
 }

@@ -315,6 +315,51 @@ void build_sbvh(const Mesh& m, const SahOptions& o, float alpha, float budget, B
     out.nodes.swap(P.nodes); out.prim.swap(P.prim); out.maxDepth = P.maxDepth; out.leafMax = o.leafMax;
 }
 
+// Binary tree of a one-mesh H-PLOC build (2n - 1 nodes of 2 float4: (lo, left), (hi, right); leaves [0, n) hold one
+// primitive in `left`; children have smaller ids than their parent; root 2n - 2) with its leaves collapsed where that
+// lowers the SAH cost: a subtree of at most leafMax triangles becomes one leaf when A x count <= A + cost(left) +
+// cost(right), leaf cost = area x triangles, inner cost = area + the children's (the dynamic programme of the
+// reference's treeFromHploc, accel/bvh_tools.cpp:12-38). The result is numbered in pre-order, left subtree first.
+void tree_from_hploc(const std::vector<float4>& hn, int64_t n, int leafMax, BinaryBvh& out) {
+    const int64_t tot = 2 * n - 1;
+    std::vector<int> L((size_t)tot), R((size_t)tot), cnt((size_t)tot);
+    std::vector<double> cost((size_t)tot); std::vector<char> asLeaf((size_t)tot); std::vector<Box3> box((size_t)tot);
+    for (int64_t h = 0; h < tot; h++) {   // ids increase from children to parents: one pass visits children first
+        box[h].lo = xyz(hn[2 * h]); box[h].hi = xyz(hn[2 * h + 1]);
+        L[h] = bits_i(hn[2 * h].w); R[h] = bits_i(hn[2 * h + 1].w);
+        const double A = box[h].area();
+        if (h < n) { cnt[h] = 1; cost[h] = A; asLeaf[h] = 1; continue; }
+        cnt[h] = cnt[L[h]] + cnt[R[h]];
+        const double inner = A + cost[L[h]] + cost[R[h]], leaf = cnt[h] <= leafMax ? A * cnt[h] : 1e300;
+        asLeaf[h] = leaf <= inner;
+        cost[h] = leaf <= inner ? leaf : inner;
+    }
+    out = BinaryBvh(); out.leafMax = leafMax;
+    out.nodes.reserve((size_t)tot); out.prim.reserve((size_t)n);
+    struct Item { int64_t h; int parent; bool right; int depth; };
+    std::vector<Item> todo{ { tot - 1, -1, false, 0 } };
+    std::vector<int64_t> gather;
+    while (!todo.empty()) {
+        const Item it = todo.back(); todo.pop_back();
+        const int id = (int)out.nodes.size();
+        out.nodes.push_back(BNode()); out.nodes[id].box = box[it.h];
+        if (it.parent >= 0) (it.right ? out.nodes[it.parent].right : out.nodes[it.parent].left) = id;
+        out.maxDepth = std::max(out.maxDepth, it.depth);
+        if (asLeaf[it.h]) {   // the subtree's primitives, left to right
+            out.nodes[id].first = (int)out.prim.size();
+            gather.assign(1, it.h);
+            while (!gather.empty()) {
+                const int64_t g = gather.back(); gather.pop_back();
+                if (g < n) out.prim.push_back(L[g]); else { gather.push_back(R[g]); gather.push_back(L[g]); }
+            }
+            out.nodes[id].count = (int)out.prim.size() - out.nodes[id].first;
+        } else {
+            todo.push_back({ R[it.h], id, true, it.depth + 1 });
+            todo.push_back({ L[it.h], id, false, it.depth + 1 });
+        }
+    }
+}
+
 double sah_cost(const BinaryBvh& B, double cNode, double cPrim) {
     double s = 0, a0 = B.nodes[0].box.area();
     if (!(a0 > 0)) return 0;

@@ -52,6 +52,10 @@ void build_sah(const Mesh& m, const SahOptions& o, BinaryBvh& out);
 // references as a fraction of the triangle count. Parallel subtrees; the result does not depend on the thread count.
 void build_sbvh(const Mesh& m, const SahOptions& o, float alpha, float budget, BinaryBvh& out);
 
+// Binary BVH from a one-mesh GPU H-PLOC build (hploc.h: hploc_build_mesh) with SAH-optimal leaf collapse to at
+// most leafMax triangles per leaf; numbered in pre-order like build_sah's trees.
+void tree_from_hploc(const std::vector<float4>& hn, int64_t n, int leafMax, BinaryBvh& out);
+
 // SAH cost normalised by the root area: internal nodes cost cNode, leaves cPrim per triangle (bvh_tools.cpp:40-44).
 double sah_cost(const BinaryBvh& B, double cNode, double cPrim);
 

@@ -2,6 +2,7 @@
 #include "hploc.h"
 #include "vecmath.h"
 #include <cub/device/device_radix_sort.cuh>
+#include <vector>
 
 namespace cwpb {
 
@@ -254,6 +255,40 @@ int SegBuilder::build(const float4* lo, const float4* hi, int64_t n64, const int
     k_seg_hploc<<<(n + kClimbBlock - 1) / kClimbBlock, kClimbBlock, 0, st>>>(nodes, count, keysSorted, clusters, bounds, segFirst, counters, n);
     CWPB_CUDA(cudaGetLastError());
     return CWP_OK;
+}
+
+// ---------------- one mesh, for the host layouts ----------------
+int hploc_build_mesh(const float* v, const int* f, int64_t nt, int device, std::vector<float4>& nodesOut, double& gpuMs) {
+    CWPB_CHECK(nt > 0 && nt < (1ll << 30), CWP_ERR_INVALID, "%lld triangles", (long long)nt);
+    CWPB_CUDA(cudaSetDevice(device));
+    std::vector<float4> lo((size_t)nt), hi((size_t)nt);
+    for (int64_t t = 0; t < nt; t++) {
+        float3 a = f3(3e38f, 3e38f, 3e38f), b = f3(-3e38f, -3e38f, -3e38f);
+        for (int k = 0; k < 3; k++) { const float* p = v + 3 * (int64_t)f[3 * t + k]; const float3 q = f3(p[0], p[1], p[2]); a = vmin(a, q); b = vmax(b, q); }
+        lo[(size_t)t] = make_float4(a.x, a.y, a.z, 0.f); hi[(size_t)t] = make_float4(b.x, b.y, b.z, 0.f);
+    }
+    float4 *dLo = nullptr, *dHi = nullptr; cudaStream_t st = nullptr; cudaEvent_t e0 = nullptr, e1 = nullptr;
+    SegBuilder B; B.device = device;
+    const int seg[2] = { 0, (int)nt };
+    int rc = CWP_OK;
+    auto ck = [&](cudaError_t e) { if (e != cudaSuccess && rc == CWP_OK) rc = set_error(CWP_ERR_CUDA, "H-PLOC build: %s", cudaGetErrorString(e)); return rc == CWP_OK; };
+    if (ck(cudaMalloc(&dLo, (size_t)nt * 16)) && ck(cudaMalloc(&dHi, (size_t)nt * 16)) && ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) &&
+        ck(cudaEventCreate(&e0)) && ck(cudaEventCreate(&e1)) &&
+        ck(cudaMemcpyAsync(dLo, lo.data(), (size_t)nt * 16, cudaMemcpyHostToDevice, st)) && ck(cudaMemcpyAsync(dHi, hi.data(), (size_t)nt * 16, cudaMemcpyHostToDevice, st))) {
+        // a first build loads the kernels and allocates; the second is timed
+        rc = B.build(dLo, dHi, nt, seg, 1, st);
+        if (rc == CWP_OK && ck(cudaEventRecord(e0, st))) rc = B.build(dLo, dHi, nt, seg, 1, st);
+        if (rc == CWP_OK && ck(cudaEventRecord(e1, st)) && ck(cudaEventSynchronize(e1))) {
+            float ms = 0.f; ck(cudaEventElapsedTime(&ms, e0, e1)); gpuMs = ms;
+            nodesOut.resize((size_t)2 * (2 * nt - 1));
+            ck(cudaMemcpy(nodesOut.data(), B.nodes, nodesOut.size() * 16, cudaMemcpyDeviceToHost));
+        }
+    }
+    B.release(); cudaFree(dLo); cudaFree(dHi);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+    return rc;
 }
 
 }  // namespace cwpb

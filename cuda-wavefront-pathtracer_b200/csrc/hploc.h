@@ -18,6 +18,7 @@
 #pragma once
 #include "runtime.h"
 #include <cstdint>
+#include <vector>
 
 namespace cwpb {
 
@@ -44,5 +45,10 @@ struct SegBuilder {
     void release();
     static int64_t regionBase(int64_t first, int s) { return 2 * first - s; }
 };
+
+// One mesh (v: 3 floats per vertex, f: 3 ints per triangle) built on `device` with one segment: the triangle boxes
+// are made on the host, a warm-up build runs, then a CUDA-event-timed build (gpuMs: bounds, keys, sort, H-PLOC);
+// nodesOut receives its 2 nt - 1 binary nodes (2 float4 each, leaves [0, nt) in sorted order, root last).
+int hploc_build_mesh(const float* v, const int* f, int64_t nt, int device, std::vector<float4>& nodesOut, double& gpuMs);
 
 }  // namespace cwpb

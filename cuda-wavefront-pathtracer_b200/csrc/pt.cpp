@@ -75,7 +75,7 @@ bool parse(int argc, char** argv, Args& A) {
     // (scene_setup.cpp:92-154): an ill-defined mix, refused here
     if (!A.scene.empty() && A.synthetic > 0) { fprintf(stderr, "--synthetic and --scene cannot be combined\n"); return false; }
     if (!A.scene.empty() && !A.materials.empty()) { fprintf(stderr, "--materials is per mesh in scene files (\"materials\" key)\n"); return false; }
-    if (A.builder != "sah") { fprintf(stderr, "--builder %s: only the host binned-SAH builder is available\n", A.builder.c_str()); return false; }
+    if (A.builder != "sah" && A.builder != "hploc") { fprintf(stderr, "--builder must be sah or hploc\n"); return false; }
     if (A.collapse != "sah" && A.collapse != "greedy") { fprintf(stderr, "--collapse must be sah or greedy\n"); return false; }
     if (A.variant != "bvh2" && A.variant != "bvh4" && A.variant != "bvh8") { fprintf(stderr, "--variant must be bvh2, bvh4 or bvh8\n"); return false; }
     return true;
@@ -328,7 +328,8 @@ int run_full(Args& A, const std::string& envFromLighting, float envStrengthL, fl
     cwp_params_finish(&P, A.sunAngleDeg, A.epsScale, extent);
     // device scene, server, environment map
     auto tb = std::chrono::steady_clock::now();
-    cwp_batch_options bo{}; cwp_batch* B = nullptr;
+    // BLAS on the host (binned SAH, the reference's default --builder sah) or on the GPU (--builder hploc)
+    cwp_batch_options bo{}; bo.builder = A.builder == "hploc" ? 0 : 1; cwp_batch* B = nullptr;
     if (cwp_batch_create(views.data(), (int32_t)views.size(), &bo, &B)) return fail("scene upload / BLAS build");
     cwp_server_options so{}; so.max_requests = 1; so.max_paths = std::min<int64_t>((int64_t)A.w * A.h * A.spp, 8ll << 20); so.gd_energy = A.gdEnergy;
     cwp_server* Srv = nullptr;
@@ -490,14 +491,18 @@ int main(int argc, char** argv) {
     // ---- BVH ----
     const int V = A.variant == "bvh4" ? 4 : A.variant == "bvh8" ? 8 : 2, TRI = A.tri == "woop" ? 1 : 0;
     const bool cw = V == 8 && A.collapse == "sah";
-    cwp_build_options bo{ V, A.bins, A.leaf, cw ? 0 : 1, A.threads };
+    // --builder hploc: the binary tree from the GPU's H-PLOC, leaves collapsed to the SAH optimum on the host, then the
+    // same layouts (scene_setup.cpp:76-83)
+    const int hp = A.builder == "hploc" ? 1 : 0;
+    cwp_build_options bo{ V, A.bins, A.leaf, cw ? 0 : 1, A.threads, 0.f, hp, 0 };
     cwp_bvh* bvh = nullptr;
     auto tb = std::chrono::steady_clock::now();
     if (cwp_bvh_build(mesh, &bo, &bvh)) return fail("BVH");
     double bvhS = std::chrono::duration<double>(std::chrono::steady_clock::now() - tb).count();
     cwp_bvh_data bd; cwp_bvh_data_of(bvh, &bd);
     const int reportLeaf = cw ? 3 : (V == 8 && A.leaf > 4) ? 4 : A.leaf;
-    fprintf(stderr, "BVH%d (sah, %d bins%s): %lld nodes (%.1f MB), depth %d, SAH %.3f, build %.2fs, tri=%s\n", V, A.bins, V == 8 ? (cw ? ", SAH collapse" : ", greedy collapse") : "",
+    const double treeMs = hp ? bd.build_ms : bvhS * 1e3, postMs = hp ? std::max(0.0, bvhS * 1e3 - bd.build_ms) : 0.0;
+    fprintf(stderr, "BVH%d (%s, %d bins%s): %lld nodes (%.1f MB), depth %d, SAH %.3f, build %.2fs, tri=%s\n", V, hp ? "gpu h-ploc" : "sah", A.bins, V == 8 ? (cw ? ", SAH collapse" : ", greedy collapse") : "",
             (long long)(bd.n_node_float4 / bd.node_stride), bd.n_node_float4 * 16 / 1e6, bd.max_depth, bd.sah, bvhS, A.tri.c_str());
     // ---- render ----
     const int K = A.batch < 1 ? 1 : A.batch;
@@ -521,11 +526,11 @@ int main(int argc, char** argv) {
                "\"bvh_nodes\":%lld,\"bvh_bytes\":%lld,\"bvh_depth\":%d,\"bvh_build_s\":%.2f,\"w\":%d,\"h\":%d,\"spp\":%d,\"bounces\":%d,\"rays_closest\":%.0f,\"rays_shadow\":%.0f,"
                "\"rays_total\":%.0f,\"t_trace_ms\":%.2f,\"t_frame_ms\":%.2f,\"mrays_s_trace\":%.1f,\"mrays_s_e2e\":%.1f,\"avg_path_len\":%.3f,\"vram_MB\":%.0f,\"pt_blocks\":%d,"
                "\"gpu\":\"%s\",\"filter\":\"%s\",\"smooth\":%d,\"seed\":%u,\"integrator\":\"legacy\",\"lens_r\":%.4f,\"focus_d\":%.4f,\"env_sampling\":\"importance\",\"textures\":0,"
-               "\"builder\":\"sah\",\"collapse\":\"%s\",\"bvh_tree_ms\":%.2f,\"bvh_post_ms\":0.00,\"bvh_sah\":%.4f,\"graph\":%d,\"instances\":0,\"flatten\":0,\"frame\":%d,\"tlas_ms\":0.000,\"bins\":%d}\n",
+               "\"builder\":\"%s\",\"collapse\":\"%s\",\"bvh_tree_ms\":%.2f,\"bvh_post_ms\":%.2f,\"bvh_sah\":%.4f,\"graph\":%d,\"instances\":0,\"flatten\":0,\"frame\":%d,\"tlas_ms\":0.000,\"bins\":%d}\n",
                r, V, A.tri.c_str(), A.persistent, A.devloop, A.sort, A.fuse < 0 ? 1 : A.fuse, reportLeaf, K, A.boxes > 0 ? "boxes" : A.synthetic > 0 ? "synthetic" : A.mesh.c_str(), (long long)bd.n_tris,
                (long long)(bd.n_node_float4 / bd.node_stride), (long long)(bd.n_node_float4 * 16), bd.max_depth, bvhS, A.w, A.h, A.spp, A.bounces, st.rays, st.shadow_rays,
                tot, st.trace_ms, st.frame_ms, tot / (st.trace_ms * 1e3), tot / (st.frame_ms * 1e3), st.rays / ((double)N * A.spp), info.vram_mb, info.pt_blocks, info.gpu_name,
-               A.filterBH ? "blackman-harris1.5" : "box", P.has_n, A.seed, P.cam.lens_r, P.cam.focus_d, V == 8 ? A.collapse.c_str() : "-", bd.build_ms, bd.sah, A.graph, A.frame, A.bins);
+               A.filterBH ? "blackman-harris1.5" : "box", P.has_n, A.seed, P.cam.lens_r, P.cam.focus_d, A.builder.c_str(), V == 8 ? A.collapse.c_str() : "-", treeMs, postMs, bd.sah, A.graph, A.frame, A.bins);
         fflush(stdout);
     }
     std::vector<float> acc((size_t)N * 4), lin((size_t)N * 3);

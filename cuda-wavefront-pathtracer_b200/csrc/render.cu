@@ -36,7 +36,21 @@ struct KArgs {
     const float4* nodes; const float4* tv; const float4* tris; const float4* nrm; const float3* albedo;
     Queues q; float4* accum; int* cnt; int* err;
     int nk, N, sBase, depth;
+    int staged;   // CWBVH nodes each block copies into shared memory (the first `staged`, i.e. the top levels)
 };
+
+// The node source of a traversal kernel: with STAGE, the block first copies the first a.staged nodes (the top levels
+// of the breadth-first numbered CWBVH, which every ray visits) into its shared memory, and the traversal reads those
+// from there and the rest from global memory.
+template <bool STAGE>
+__device__ __forceinline__ auto node_source(const KArgs& a) {
+    if constexpr (STAGE) {
+        extern __shared__ float4 sNodes[];
+        for (int i = threadIdx.x; i < 5 * a.staged; i += blockDim.x) sNodes[i] = __ldg(a.nodes + i);
+        __syncthreads();
+        return StagedNodes{ a.nodes, sNodes, a.staged };
+    } else return a.nodes;
+}
 
 __device__ __forceinline__ float rnd(const cwp_params& P, unsigned pix, unsigned smp, unsigned depth, unsigned dim) { return sample01(pix, smp, depth, dim, P.seed); }
 __device__ __forceinline__ float3 v3(const float* a) { return f3(a[0], a[1], a[2]); }
@@ -84,6 +98,9 @@ __device__ __forceinline__ void camera_ray(const cwp_params& P, int i, int N, in
         d = normalize(pf - o);
     }
 }
+
+static constexpr int kMaxStagedNodes = 512;    // 40 KB of shared memory per block at most
+static constexpr int kDefaultStageLevels = -1;  // stage_levels = 0 means this
 
 #ifndef CWPB_TRACE_MINB
 #define CWPB_TRACE_MINB 8   // resident 128-thread blocks per SM the traversal kernels are compiled for
@@ -154,8 +171,9 @@ __device__ __forceinline__ void path_ray(const KArgs& a, const cwp_params& P, in
 }
 
 // one warp fetch of 32 queue entries at a time, each ray traversed to completion, then the 32 shaded together
-template <int V, int TRI, bool PRIMARY>
+template <int V, int TRI, bool PRIMARY, bool STAGE = false>
 __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade(const __grid_constant__ KArgs a, const __grid_constant__ cwp_params P) {
+    const auto nodes = node_source<STAGE>(a);
     int* const c = a.cnt + 4 * a.depth;
     const int n = PRIMARY ? a.nk : c[0];
     const int lane = threadIdx.x & 31;
@@ -170,7 +188,7 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade(const __gr
         float3 o = f3(0.f, 0.f, 0.f), d = f3(0.f, 0.f, 1.f); float tmin = 0.f;
         if (valid) path_ray<PRIMARY>(a, P, k, o, d, tmin);
         float t = 1e30f, hu = 0.f, hv = 0.f; int tri = -1;
-        if (valid) trace_ray<V, false, TRI>(a.nodes, a.tv, o, d, tmin, t, tri, hu, hv, 0, err);
+        if (valid) trace_ray<V, false, TRI>(nodes, a.tv, o, d, tmin, t, tri, hu, hv, 0, err);
         shade_path<PRIMARY>(a, P, valid, k, o, d, t, tri, hu, hv);
     }
     if (err) atomicOr(a.err, err);
@@ -184,8 +202,9 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade(const __gr
 // advances it one node visit per step; once CWPB_REFILL lanes have finished, the warp shades those paths together,
 // hands their lanes new queue entries with one atomic, and resumes. Lanes stay busy instead of waiting for the slowest
 // ray of a 32-ray batch.
-template <int V, int TRI, bool PRIMARY>
+template <int V, int TRI, bool PRIMARY, bool STAGE = false>
 __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade_rf(const __grid_constant__ KArgs a, const __grid_constant__ cwp_params P) {
+    const auto nodes = node_source<STAGE>(a);
     int* const c = a.cnt + 4 * a.depth;
     const int n = PRIMARY ? a.nk : c[0];
     const int lane = threadIdx.x & 31;
@@ -212,7 +231,7 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade_rf(const _
         }
         if (!__any_sync(0xffffffffu, k >= 0)) break;
         for (;;) {
-            if (k >= 0 && !fin) fin = ray.step(a.nodes, a.tv, stack, err);
+            if (k >= 0 && !fin) fin = ray.step(nodes, a.tv, stack, err);
             const unsigned busy = __ballot_sync(0xffffffffu, k >= 0 && !fin);
             if (!busy || (!drained && 32 - __popc(busy) >= CWPB_REFILL)) break;
         }
@@ -220,8 +239,9 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade_rf(const _
     if (err) atomicOr(a.err, err);
 }
 
-template <int V, int TRI>
+template <int V, int TRI, bool STAGE = false>
 __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow_rf(const __grid_constant__ KArgs a) {
+    const auto nodes = node_source<STAGE>(a);
     int* const c = a.cnt + 4 * a.depth;
     const int n = c[1];
     const int lane = threadIdx.x & 31;
@@ -248,7 +268,7 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow_rf(const __grid
         }
         if (!__any_sync(0xffffffffu, k >= 0)) break;
         for (;;) {
-            if (k >= 0 && !fin) fin = ray.step(a.nodes, a.tv, stack, err);
+            if (k >= 0 && !fin) fin = ray.step(nodes, a.tv, stack, err);
             const unsigned busy = __ballot_sync(0xffffffffu, k >= 0 && !fin);
             if (!busy || (!drained && 32 - __popc(busy) >= CWPB_REFILL)) break;
         }
@@ -256,8 +276,9 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow_rf(const __grid
     if (err) atomicOr(a.err, err);
 }
 
-template <int V, int TRI>
+template <int V, int TRI, bool STAGE = false>
 __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow(const __grid_constant__ KArgs a) {
+    const auto nodes = node_source<STAGE>(a);
     int* const c = a.cnt + 4 * a.depth;
     const int n = c[1];
     const int lane = threadIdx.x & 31;
@@ -271,7 +292,7 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow(const __grid_co
         if (k < n) {
             const float4 h0 = __ldcs(a.q.h0 + k), h1 = __ldcs(a.q.h1 + k); const float2 h2 = __ldcs(a.q.h2 + k);
             float t = 1e30f, u, v; int tri = -1;
-            if (!trace_ray<V, true, TRI>(a.nodes, a.tv, xyz(h0), xyz(h1), 0.f, t, tri, u, v, 0, err))
+            if (!trace_ray<V, true, TRI>(nodes, a.tv, xyz(h0), xyz(h1), 0.f, t, tri, u, v, 0, err))
                 accum_add(a.accum, __float_as_int(h0.w), f3(h1.w, h2.x, h2.y));
         }
     }
@@ -354,42 +375,44 @@ struct cwp_renderer {
     cudaStream_t st = nullptr; cudaEvent_t f0 = nullptr, f1 = nullptr;
     cudaGraphExec_t gexec = nullptr; int gSpp = -1, gBase = 0;
     int gridTrace = 0, gridTrace0 = 0, gridShadow = 0, nSM = 0; bool refill = false, refillShadow = false;
+    int staged = 0;   // CWBVH nodes staged in each traversal block's shared memory (0 = none)
     std::vector<void*> allocs;
     double vramMB = 0; std::string gpuName;
 };
 
 namespace {
 
-template <int V, int TRI> int occupancy_of(int& bt0, int& bt, int& bs, bool refill = false) {
+template <int V, int TRI, bool STAGE = false> int occupancy_of(int& bt0, int& bt, int& bs, bool refill = false, size_t smem = 0) {
     if constexpr (V != 4) {
         if (refill) {
-            CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt0, k_trace_shade_rf<V, TRI, true>, 128, 0));
-            CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace_shade_rf<V, TRI, false>, 128, 0));
-            CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shadow_rf<V, TRI>, 128, 0));
+            CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt0, k_trace_shade_rf<V, TRI, true, STAGE>, 128, smem));
+            CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace_shade_rf<V, TRI, false, STAGE>, 128, smem));
+            CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shadow_rf<V, TRI, STAGE>, 128, smem));
             return CWP_OK;
         }
     }
-    CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt0, k_trace_shade<V, TRI, true>, 128, 0));
-    CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace_shade<V, TRI, false>, 128, 0));
-    CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shadow<V, TRI>, 128, 0));
+    CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt0, k_trace_shade<V, TRI, true, STAGE>, 128, smem));
+    CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace_shade<V, TRI, false, STAGE>, 128, smem));
+    CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shadow<V, TRI, STAGE>, 128, smem));
     return CWP_OK;
 }
 
 // ev: 4 events (trace start/end, shadow start/end) or nullptr
-template <int V, int TRI> void launch_depth(cwp_renderer* r, KArgs a, int gt0, int gt, int gs, cudaEvent_t* ev) {
+template <int V, int TRI, bool STAGE = false> void launch_depth(cwp_renderer* r, KArgs a, int gt0, int gt, int gs, cudaEvent_t* ev) {
     // external records: inside a stream capture they become event-record nodes of the graph
     bool rf = false, rfShadow = false;
+    const size_t sm = STAGE ? (size_t)80 * a.staged : 0;
     if constexpr (V != 4) { rf = r->refill; rfShadow = r->refillShadow; }
     if (ev) cudaEventRecordWithFlags(ev[0], r->st, cudaEventRecordExternal);
     if constexpr (V != 4) {
         if (rf) {
-            if (a.depth == 0) k_trace_shade_rf<V, TRI, true><<<gt0, 128, 0, r->st>>>(a, r->P);
-            else k_trace_shade_rf<V, TRI, false><<<gt, 128, 0, r->st>>>(a, r->P);
+            if (a.depth == 0) k_trace_shade_rf<V, TRI, true, STAGE><<<gt0, 128, sm, r->st>>>(a, r->P);
+            else k_trace_shade_rf<V, TRI, false, STAGE><<<gt, 128, sm, r->st>>>(a, r->P);
         }
     }
     if (!rf) {
-        if (a.depth == 0) k_trace_shade<V, TRI, true><<<gt0, 128, 0, r->st>>>(a, r->P);
-        else k_trace_shade<V, TRI, false><<<gt, 128, 0, r->st>>>(a, r->P);
+        if (a.depth == 0) k_trace_shade<V, TRI, true, STAGE><<<gt0, 128, sm, r->st>>>(a, r->P);
+        else k_trace_shade<V, TRI, false, STAGE><<<gt, 128, sm, r->st>>>(a, r->P);
     }
     if (r->O.sort && a.depth + 1 < r->depths) {   // regroup the continuations that the next bounce traces
         const int wr = (a.depth & 1) ^ 1;
@@ -400,15 +423,15 @@ template <int V, int TRI> void launch_depth(cwp_renderer* r, KArgs a, int gt0, i
         k_sort_scatter<<<r->nSM * 8, 256, 0, r->st>>>(sa);
     }
     if (ev) { cudaEventRecordWithFlags(ev[1], r->st, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], r->st, cudaEventRecordExternal); }
-    if constexpr (V != 4) { if (rfShadow) k_shadow_rf<V, TRI><<<gs, 128, 0, r->st>>>(a); }
-    if (!rfShadow) k_shadow<V, TRI><<<gs, 128, 0, r->st>>>(a);
+    if constexpr (V != 4) { if (rfShadow) k_shadow_rf<V, TRI, STAGE><<<gs, 128, sm, r->st>>>(a); }
+    if (!rfShadow) k_shadow<V, TRI, STAGE><<<gs, 128, sm, r->st>>>(a);
     if (ev) cudaEventRecordWithFlags(ev[3], r->st, cudaEventRecordExternal);
 }
 
 KArgs base_args(cwp_renderer* r) {
     KArgs a{};
     a.nodes = r->scene.nodes; a.tv = r->scene.leafData(); a.tris = r->scene.tris; a.nrm = r->scene.nrm; a.albedo = r->scene.albedo;
-    a.q = r->q; a.accum = r->accum; a.cnt = r->cnt; a.err = r->err; a.nk = (int)r->nk; a.N = r->N;
+    a.q = r->q; a.accum = r->accum; a.cnt = r->cnt; a.err = r->err; a.nk = (int)r->nk; a.N = r->N; a.staged = r->staged;
     return a;
 }
 
@@ -418,6 +441,7 @@ void dispatch_depth(cwp_renderer* r, KArgs a, int gt0, int gt, int gs, int pass)
     cudaEvent_t* ev = r->O.profile ? &r->ev[((size_t)pass * r->depths + a.depth) * 4] : nullptr;
     if (V == 2) { if (T) launch_depth<2, 1>(r, a, gt0, gt, gs, ev); else launch_depth<2, 0>(r, a, gt0, gt, gs, ev); }
     else if (V == 4) { if (T) launch_depth<4, 1>(r, a, gt0, gt, gs, ev); else launch_depth<4, 0>(r, a, gt0, gt, gs, ev); }
+    else if (r->staged) { if (T) launch_depth<8, 1, true>(r, a, gt0, gt, gs, ev); else launch_depth<8, 0, true>(r, a, gt0, gt, gs, ev); }
     else { if (T) launch_depth<8, 1>(r, a, gt0, gt, gs, ev); else launch_depth<8, 0>(r, a, gt0, gt, gs, ev); }
 }
 
@@ -539,14 +563,25 @@ extern "C" int cwp_renderer_init(cwp_renderer* r, const cwp_params* p, const cwp
     // (coherent rays towards the sun) and BVH2 (bound by dependent node-fetch latency) run faster per 32-ray batch
     r->refill = o->traversal == 1 || (o->traversal == 0 && V == 8);
     r->refillShadow = o->traversal == 1;
+    // CWBVH top levels staged in shared memory: stage_levels 0 = the default, < 0 none, 1..3 levels 0..L (at most
+    // kMaxStagedNodes nodes)
+    CWPB_CHECK(o->stage_levels <= 3, CWP_ERR_INVALID, "stage_levels %d is above 3", o->stage_levels);
+    r->staged = 0;
+    if (V == 8) {
+        const int L = o->stage_levels == 0 ? kDefaultStageLevels : o->stage_levels;
+        if (L > 0) r->staged = std::min(r->scene.levelEnd[L], kMaxStagedNodes);
+    }
+    const size_t sm = (size_t)80 * r->staged;
     int b0 = 0, b1 = 0;
     if (V == 2) rc = T ? occupancy_of<2, 1>(bt0, bt, b0, r->refill) : occupancy_of<2, 0>(bt0, bt, b0, r->refill);
     else if (V == 4) rc = T ? occupancy_of<4, 1>(bt0, bt, b0) : occupancy_of<4, 0>(bt0, bt, b0);
+    else if (r->staged) rc = T ? occupancy_of<8, 1, true>(bt0, bt, b0, r->refill, sm) : occupancy_of<8, 0, true>(bt0, bt, b0, r->refill, sm);
     else rc = T ? occupancy_of<8, 1>(bt0, bt, b0, r->refill) : occupancy_of<8, 0>(bt0, bt, b0, r->refill);
     if (rc) return rc;
     int d0 = 0, d1 = 0;   // shadow grid from the shadow kernel actually used
     if (V == 2) rc = T ? occupancy_of<2, 1>(d0, d1, bs, r->refillShadow) : occupancy_of<2, 0>(d0, d1, bs, r->refillShadow);
     else if (V == 4) rc = T ? occupancy_of<4, 1>(d0, d1, bs) : occupancy_of<4, 0>(d0, d1, bs);
+    else if (r->staged) rc = T ? occupancy_of<8, 1, true>(d0, d1, bs, r->refillShadow, sm) : occupancy_of<8, 0, true>(d0, d1, bs, r->refillShadow, sm);
     else rc = T ? occupancy_of<8, 1>(d0, d1, bs, r->refillShadow) : occupancy_of<8, 0>(d0, d1, bs, r->refillShadow);
     (void)b1;
     if (rc) return rc;

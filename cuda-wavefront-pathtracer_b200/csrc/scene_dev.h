@@ -2,6 +2,7 @@
 #pragma once
 #include "runtime.h"
 #include <cstdint>
+#include <vector>
 
 namespace cwpb {
 
@@ -16,6 +17,9 @@ struct DeviceScene {
     float3* albedo = nullptr; int nAlbedo = 0;
     size_t bytes = 0;
     void* arena = nullptr; size_t hotBytes = 0;     // one allocation; its first hotBytes hold nodes, leaf rows, triangles, corners
+    // CWBVH: the device copy is numbered breadth first (same tree, same child order), so the nodes of levels 0..L are
+    // the first levelEnd[L] nodes - the ones the frame kernels can stage in shared memory
+    int levelEnd[4] = { 0, 0, 0, 0 };
     const float4* leafData() const { return precise ? verts : tri == 1 ? woop : tris; }
 };
 
@@ -24,5 +28,9 @@ struct DeviceScene {
 int upload_scene(const cwp_scene_buffers* s, int tri, int device, DeviceScene& out);
 void free_scene(DeviceScene& s);
 int validate_nodes(const float* nodes, int64_t nF4, int stride, int64_t nTris, int* variantOut);
+// Breadth-first renumbering of a validated CWBVH (5 float4 per node, root 0): every node keeps its children, in slot
+// order and contiguous; only the node indices (and each node's child base) change. levelEnd[L] = number of nodes in
+// levels 0..L. False when the nodes do not form one tree rooted at node 0.
+bool cwbvh_breadth_first(const float* in, int64_t nNodes, std::vector<float>& out, int levelEnd[4]);
 
 }  // namespace cwpb

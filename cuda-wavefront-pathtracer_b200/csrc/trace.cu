@@ -46,6 +46,30 @@ int validate_nodes(const float* nodes, int64_t nF4, int stride, int64_t nTris, i
     return CWP_OK;
 }
 
+bool cwbvh_breadth_first(const float* in, int64_t nNodes, std::vector<float>& out, int levelEnd[4]) {
+    out.assign((size_t)nNodes * 20, 0.f);
+    std::vector<int32_t> order; order.reserve((size_t)nNodes);   // old index of each new index
+    std::vector<int> level; level.reserve((size_t)nNodes);
+    std::vector<char> seen((size_t)nNodes, 0);
+    order.push_back(0); level.push_back(0); seen[0] = 1;
+    for (size_t q = 0; q < order.size(); q++) {
+        const int32_t* w = reinterpret_cast<const int32_t*>(in) + (int64_t)order[q] * 20;
+        const int nInt = __builtin_popcount((uint32_t)w[3] >> 24);
+        const int32_t newBase = (int32_t)order.size();
+        for (int c = 0; c < nInt; c++) {
+            const int32_t old = w[4] + c;   // in range: validate_nodes checked every child group
+            if (seen[old]) return false;    // a node with two parents: not a tree
+            seen[old] = 1; order.push_back(old); level.push_back(level[q] + 1);
+        }
+        int32_t* o = reinterpret_cast<int32_t*>(out.data()) + (int64_t)q * 20;
+        memcpy(o, w, 80);
+        if (nInt) o[4] = newBase;
+    }
+    if ((int64_t)order.size() != nNodes) return false;   // unreachable nodes
+    for (int L = 0; L < 4; L++) { int64_t k = 0; while (k < (int64_t)level.size() && level[k] <= L) k++; levelEnd[L] = (int)k; }
+    return true;
+}
+
 void free_scene(DeviceScene& s) {
     if (s.arena) { cudaSetDevice(s.device); cudaFree(s.arena); }
     s = DeviceScene();
@@ -70,7 +94,14 @@ int upload_scene(const cwp_scene_buffers* s, int tri, int device, DeviceScene& o
     // access-policy window can cover what every ray reads
     struct Part { void** dst; const void* src; size_t bytes; };
     const size_t tb = (size_t)s->n_tris * 48;
-    const Part parts[] = { { (void**)&out.nodes, s->nodes, (size_t)s->n_node_float4 * 16 }, { (void**)&out.woop, s->woop, s->woop ? tb : 0 },
+    std::vector<float> bfs;
+    const float* nodeSrc = s->nodes;
+    if (variant == 8) {
+        CWPB_CHECK(cwbvh_breadth_first(s->nodes, out.nNodes, bfs, out.levelEnd), CWP_ERR_INVALID,
+                   "CWBVH of %lld nodes is not a tree rooted at node 0 (a node unreachable or with two parents)", (long long)out.nNodes);
+        nodeSrc = bfs.data();
+    }
+    const Part parts[] = { { (void**)&out.nodes, nodeSrc, (size_t)s->n_node_float4 * 16 }, { (void**)&out.woop, s->woop, s->woop ? tb : 0 },
                            { (void**)&out.tris, s->tris, tb }, { (void**)&out.verts, s->verts, s->verts ? tb : 0 },
                            { (void**)&out.nrm, s->nrm, s->nrm ? tb : 0 }, { (void**)&out.albedo, alb.data(), alb.size() * sizeof(float3) } };
     size_t total = 0, hot = 0;

@@ -26,6 +26,25 @@ static constexpr int kVisitBudget = 1 << 22;
 
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 
+// Where a traversal reads its nodes. A plain node pointer reads global memory through the read-only path;
+// StagedNodes reads the first k nodes from a block's copy in shared memory and the rest from global memory. With a
+// breadth-first node numbering the first k nodes are the tree's top levels, which every ray visits.
+struct StagedNodes { const float4* __restrict__ g; const float4* s; int k; };
+template <int W>
+__device__ __forceinline__ void fetch_node(const float4* __restrict__ g, int node, float4 (&f)[W]) {
+    const float4* p = g + (size_t)W * node;
+#pragma unroll
+    for (int i = 0; i < W; i++) f[i] = __ldg(p + i);
+}
+template <int W>
+__device__ __forceinline__ void fetch_node(const StagedNodes& n, int node, float4 (&f)[W]) {
+    if (node < n.k) {
+        const float4* p = n.s + W * node;
+#pragma unroll
+        for (int i = 0; i < W; i++) f[i] = p[i];
+    } else fetch_node<W>(n.g, node, f);
+}
+
 // reciprocal direction with the reference's safe epsilon (traverse.cuh:48-50)
 __device__ __forceinline__ float safe_rcp(float x) { const float eps = 1e-20f; return 1.f / (fabsf(x) > eps ? x : copysignf(eps, x)); }
 
@@ -204,11 +223,11 @@ struct TravState<8, ANY, TRI> {
         oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
         cb = im = hm = 0;
     }
-    template <class S>
-    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ tv, S& stack, int& err) {
+    template <class N, class S>
+    __device__ __forceinline__ bool step(const N& nodes, const float4* __restrict__ tv, S& stack, int& err) {
         if (--budget < 0) { err |= kTravBudget; return true; }
-        const float4* nb = nodes + 5 * (size_t)node;
-        const float4 f0 = ld4(nb), f1 = ld4(nb + 1), f2 = ld4(nb + 2), f3_ = ld4(nb + 3), f4_ = ld4(nb + 4);
+        float4 nf[5]; fetch_node<5>(nodes, node, nf);
+        const float4 f0 = nf[0], f1 = nf[1], f2 = nf[2], f3_ = nf[3], f4_ = nf[4];
         const unsigned ew = __float_as_uint(f0.w);
         const float sx = __uint_as_float((ew & 255u) << 23) * idx, sy = __uint_as_float(((ew >> 8) & 255u) << 23) * idy, sz = __uint_as_float(((ew >> 16) & 255u) << 23) * idz;
         const float ox = (f0.x - o.x) * idx, oy = (f0.y - o.y) * idy, oz = (f0.z - o.z) * idz;
@@ -262,8 +281,8 @@ struct TravState<8, ANY, TRI> {
     }
 };
 
-template <bool ANY, int TRI>
-__device__ __forceinline__ bool trav_cwbvh(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
+template <bool ANY, int TRI, class N>
+__device__ __forceinline__ bool trav_cwbvh(const N& nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
                                            float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
     TravState<8, ANY, TRI> r; typename TravState<8, ANY, TRI>::Stack stack; r.begin(o, d, tmin, hitT, root);
     while (!r.step(nodes, tv, stack, err)) {}
@@ -361,11 +380,11 @@ struct TravState<16, ANY, TRI> {
         oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
         cb = im = hm = 0; wt = wt_setup(d);
     }
-    template <class S>
-    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ vt, S& stack, int& err) {
+    template <class N, class S>
+    __device__ __forceinline__ bool step(const N& nodes, const float4* __restrict__ vt, S& stack, int& err) {
         if (--budget < 0) { err |= kTravBudget; return true; }
-        const float4* nb = nodes + 5 * (size_t)node;
-        const float4 f0 = ld4(nb), f1 = ld4(nb + 1), f2 = ld4(nb + 2), f3_ = ld4(nb + 3), f4_ = ld4(nb + 4);
+        float4 nf[5]; fetch_node<5>(nodes, node, nf);
+        const float4 f0 = nf[0], f1 = nf[1], f2 = nf[2], f3_ = nf[3], f4_ = nf[4];
         const unsigned ew = __float_as_uint(f0.w);
         const unsigned imask = ew >> 24, m0 = __float_as_uint(f1.z), m1 = __float_as_uint(f1.w);
         const int childBase = __float_as_int(f1.x), triBase = __float_as_int(f1.y);
@@ -497,18 +516,18 @@ __device__ __forceinline__ bool trav_fp64(const float4* __restrict__ nodes, cons
     }
 }
 
-template <int V, bool ANY, int TRI>
-__device__ __forceinline__ bool trace_ray(const float4* __restrict__ nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
+// nodes: a node pointer, or (CWBVH and the precision form) StagedNodes
+template <int V, bool ANY, int TRI, class N>
+__device__ __forceinline__ bool trace_ray(const N& nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
                                           float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
-    if (V == 2) return trav_bvh2<ANY, TRI>(nodes, tv, o, d, tmin, hitT, hitTri, hu, hv, root, err);
-    if (V == 4) return trav_bvh4<ANY, TRI>(nodes, tv, o, d, tmin, hitT, hitTri, hu, hv, root, err);
-    if (V == 16) {   // precision form: tv = exact corners
+    if constexpr (V == 2) return trav_bvh2<ANY, TRI>(nodes, tv, o, d, tmin, hitT, hitTri, hu, hv, root, err);
+    else if constexpr (V == 4) return trav_bvh4<ANY, TRI>(nodes, tv, o, d, tmin, hitT, hitTri, hu, hv, root, err);
+    else if constexpr (V == 16) {   // precision form: tv = exact corners
         TravState<16, ANY, TRI> r; typename TravState<16, ANY, TRI>::Stack stack; r.begin(o, d, tmin, hitT, root);
         while (!r.step(nodes, tv, stack, err)) {}
         hitT = r.hitT; hitTri = r.hitTri; hu = r.hu; hv = r.hv;
         return hitTri >= 0;
-    }
-    return trav_cwbvh<ANY, TRI>(nodes, tv, o, d, tmin, hitT, hitTri, hu, hv, root, err);
+    } else return trav_cwbvh<ANY, TRI>(nodes, tv, o, d, tmin, hitT, hitTri, hu, hv, root, err);
 }
 
 }  // namespace cwpb

@@ -113,7 +113,7 @@ def fp64_hit(o, d, verts, tri):
     return t, m
 
 
-def explain_differences(o, d, verts, ours, other, any_hit=False, rel=1e-6, graze=16.0):
+def explain_differences(o, d, verts, ours, other, any_hit=False, rel=1e-6, graze=16.0, ids=None):
     """Rays on which this library and another traversal of the same tree disagree, classified in FP64 on the exact
     corners. Closest hit: ours / other are float4 (t, u, v, leaf-order triangle bits) and a ray disagrees when the
     triangles differ; any hit: int32 triangle or -1, and a ray disagrees when one side finds an occluder and the
@@ -124,6 +124,9 @@ def explain_differences(o, d, verts, ours, other, any_hit=False, rel=1e-6, graze
       graze       a triangle that one side reports and the other does not lies within `graze` edge-bound units of one
                   of its edges, inside or out (FP32 rounding decides such rays);
       unexplained anything else.
+    ids (optional): the original mesh triangle of every leaf-order reference (tris[3k].w); with spatial splits one
+    triangle has several references, and two references to the same triangle are the same hit ("same_triangle",
+    counted, not classified).
     Returns (counts, rows), one row per disagreeing ray."""
     if any_hit:
         ia, ib = np.asarray(ours, np.int32), np.asarray(other, np.int32)
@@ -131,7 +134,13 @@ def explain_differences(o, d, verts, ours, other, any_hit=False, rel=1e-6, graze
     else:
         ia, ib = ours[:, 3].view(np.int32), other[:, 3].view(np.int32)
         diff = np.where(ia != ib)[0]
-    counts = {"rays": int(len(o)), "differ": int(len(diff)), "tie": 0, "ours_exact": 0, "graze": 0, "unexplained": 0}
+    counts = {"rays": int(len(o)), "differ": 0, "same_triangle": 0, "tie": 0, "ours_exact": 0, "graze": 0, "unexplained": 0}
+    if ids is not None and not any_hit and len(diff):
+        ids = np.asarray(ids, np.int32)
+        dup = (ia[diff] >= 0) & (ib[diff] >= 0) & (ids[np.maximum(ia[diff], 0)] == ids[np.maximum(ib[diff], 0)])
+        counts["same_triangle"] = int(dup.sum())
+        diff = diff[~dup]
+    counts["differ"] = int(len(diff))
     rows = []
     if not len(diff):
         return counts, rows

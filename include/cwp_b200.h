@@ -75,6 +75,11 @@ typedef struct cwp_build_options {
     float spatial;      /* > 0: spatial splits (SBVH) where the object split's children overlap by more than this
                            fraction of the root's area (1e-5 typical); a spatial split may add at most 30% references
                            to a node. 0: the reference's binned SAH (byte-identical buffers at 16 bins) */
+    int32_t builder;    /* 0: host binned SAH (above); 1: the binary tree built on the GPU by H-PLOC, leaves collapsed
+                           to the SAH optimum on the host, then the same layouts - the reference's --builder hploc
+                           (app/scene_setup.cpp:76-83: hplocBuildHost, hploc.cu:195-209, then treeFromHploc,
+                           bvh_tools.cpp:12-38); bins and spatial do not apply; build_ms is then the GPU build time */
+    int32_t device;     /* builder 1: CUDA device */
 } cwp_build_options;
 
 typedef struct cwp_bvh cwp_bvh;
@@ -165,7 +170,9 @@ typedef struct cwp_render_options {
     int32_t profile;      /* 1: CUDA event pair around every kernel launch (also inside the graph), see cwp_renderer_depth_stats */
     int32_t traversal;    /* 0 auto (refill for CWBVH closest-hit), 1 persistent lanes with dynamic refill everywhere, 2 one 32-ray fetch per warp */
     int32_t sort;         /* continuation rays regrouped before each bounce: 0 off, 1 by direction octant, 2 by octant and a 4x4x4 origin cell */
-    int32_t reserved[2];
+    int32_t stage_levels; /* CWBVH: levels 0..L of the tree copied into every traversal block's shared memory (L = 1..3, at most
+                             512 nodes); -1 none; 0 the library's default */
+    int32_t reserved;
 } cwp_render_options;
 
 typedef struct cwp_frame_stats { double rays, shadow_rays, trace_ms, frame_ms; } cwp_frame_stats;

@@ -27,3 +27,21 @@ extern "C" int ref_gpu_trace(int variant, int any, int tri, const float* nodes, 
 #undef RL
     return (int)cudaGetLastError();
 }
+
+// The reference's GPU BVH construction for a static mesh, as its --builder hploc runs it (app/scene_setup.cpp:76-83):
+// hplocBuildHost (accel/hploc.cu:195-209: upload, one warm-up build, one CUDA-event-timed build, download) on the
+// triangle boxes lo / hi (n float4 each, host), then treeFromHploc (accel/bvh_tools.cpp:12-38: SAH-optimal leaf
+// collapse to leafMax) and sahCost (bvh_tools.cpp:40-44, c_node = c_prim = 1). Returns the SAH cost; *gpu_ms = the
+// timed device build; *n_nodes / *max_depth of the collapsed binary tree.
+#include "accel/hploc.h"
+#include "accel/bvh_tools.h"
+#include <vector>
+extern "C" double ref_hploc_tree(const float* lo, const float* hi, int n, int leafMax, double* gpu_ms, int* n_nodes, int* max_depth) {
+    std::vector<float4> L((size_t)n), H((size_t)n), nodes;
+    for (int i = 0; i < n; i++) { L[i] = make_float4(lo[4 * i], lo[4 * i + 1], lo[4 * i + 2], 0.f); H[i] = make_float4(hi[4 * i], hi[4 * i + 1], hi[4 * i + 2], 0.f); }
+    double ms = 0;
+    const int root = hplocBuildHost(L, H, nodes, ms);
+    BVHBuilder B; treeFromHploc(nodes, n, root, leafMax, B);
+    *gpu_ms = ms; *n_nodes = (int)B.nodes.size(); *max_depth = B.maxDepth;
+    return sahCost(B, 1, 1);
+}

@@ -22,6 +22,8 @@ def run(*args):
     (["--light_sampling", "all"], "--light_sampling must be"),
     (["--integrator", "legacy", "--scene", "s.json"], "does not render scene files"),
     (["--bogus"], "unknown arg"),
+    (["--builder", "lbvh"], "--builder must be sah or hploc"),
+    (["--synthetic", "3", "--scene", "s.json"], "--synthetic and --scene cannot be combined"),
 ])
 def test_refusals(args, msg):
     rc, err = run(*args)
