@@ -36,6 +36,8 @@ int validate_nodes(const float* nodes, int64_t nF4, int stride, int64_t nTris, i
                 if (m & 0x80u) {
                     int64_t first = (int64_t)triBase + (m & 31u), cnt = ((m >> 5) & 3u) + 1;
                     CWPB_CHECK(leafOk(first, cnt), CWP_ERR_INVALID, "CWBVH node %lld slot %d: leaf [%lld, +%lld) out of range", (long long)n, s, (long long)first, (long long)cnt);
+                    // the traversal keeps a node's hit triangles as a 32-bit mask over offsets from triBase
+                    CWPB_CHECK((m & 31u) + cnt <= 32, CWP_ERR_INVALID, "CWBVH node %lld slot %d: leaf offset %u + %lld triangles exceeds 32", (long long)n, s, m & 31u, (long long)cnt);
                 } else if (m) {
                     CWPB_CHECK(imask & (1u << s), CWP_ERR_INVALID, "CWBVH node %lld slot %d: internal child without imask bit", (long long)n, s);
                 }
