@@ -232,20 +232,22 @@ def port_scene(cwp, wl, variant, w=512, h=512, bounces=4):
                            order=bvh.order, n_tris=mesh.n_tris, build_ms=None, stride=bvh.stride)
 
 
-# DRAM bytes per launch of the frame kernels from one full-size ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum, one pass, every launch of one frame; summary and command in profiles/frame512_dram_traffic.txt).
-# Valid only for the configuration it was captured on.
-FRAME512_TRAFFIC = {"k_trace_shade": 2583.8e6, "k_shadow": 531.0e6}
+# DRAM bytes per launch of the frame kernels at the frame512 defaults, from a small-case capture scaled to the full
+# frame: the same frame at 16 spp (batch 16, 4.2 M paths per pass, path state 0.5 GB > L2), dram__bytes_read.sum +
+# dram__bytes_write.sum of every launch of one frame (one pass), per closest ray (k_trace_shade) or shadow ray
+# (k_shadow), times the full frame's rays over its 6 launches (summary and command in profiles/frame512_dram_traffic.txt).
+# Valid only for the configuration it was derived for.
+FRAME512_TRAFFIC = {"k_trace_shade": 1930e6, "k_shadow": 628e6}
 FRAME512_TRAFFIC_BINS = 128   # the build the capture ran on
 
 
 def frame_traffic(args, wl, variant, kernel):
     captured = (args.workload == "frame512" and variant == 8 and args.spatial == 1e-3 and not args.spp and not args.batch and args.sort == 0
-                and args.graph == 1 and args.traversal == 0 and args.bins == FRAME512_TRAFFIC_BINS)
+                and args.graph == 1 and args.traversal == 0 and args.bins == FRAME512_TRAFFIC_BINS and args.stage_levels <= 0)
     if not captured or kernel not in FRAME512_TRAFFIC:
         return {"traffic": None}
     return {"traffic": FRAME512_TRAFFIC[kernel], "traffic_unit": "bytes per launch",
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size capture (profiles/frame512_dram_traffic.txt)"}
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 16-spp frame (one pass, every launch), scaled by rays to the full frame (profiles/frame512_dram_traffic.txt)"}
 
 
 NODE_BYTES = {2: 64, 4: 128, 8: 80}
