@@ -382,7 +382,17 @@ struct cwp_renderer {
 
 namespace {
 
+#ifdef CWPB_L1_CARVEOUT
+template <class K> void prefer_l1(K* k) { cudaFuncSetAttribute((const void*)k, cudaFuncAttributePreferredSharedMemoryCarveout, CWPB_L1_CARVEOUT); }
+#else
+template <class K> void prefer_l1(K*) {}
+#endif
+
 template <int V, int TRI, bool STAGE = false> int occupancy_of(int& bt0, int& bt, int& bs, bool refill = false, size_t smem = 0) {
+    if constexpr (!STAGE) {
+        if constexpr (V != 4) { prefer_l1(k_trace_shade_rf<V, TRI, true>); prefer_l1(k_trace_shade_rf<V, TRI, false>); prefer_l1(k_shadow_rf<V, TRI>); }
+        prefer_l1(k_trace_shade<V, TRI, true>); prefer_l1(k_trace_shade<V, TRI, false>); prefer_l1(k_shadow<V, TRI>);
+    }
     if constexpr (V != 4) {
         if (refill) {
             CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt0, k_trace_shade_rf<V, TRI, true, STAGE>, 128, smem));

@@ -29,6 +29,10 @@ int validate_nodes(const float* nodes, int64_t nF4, int stride, int64_t nTris, i
         for (int64_t n = 0; n < nNodes; n++) {
             const int32_t* q = w + n * 20;
             uint32_t ew = (uint32_t)q[3], imask = ew >> 24; int32_t childBase = q[4], triBase = q[5];
+            // the traversal scales 2^e / d by 2^24: biased exponents up to 164 (quantisation steps up to 2^37, child boxes
+            // up to about 3.5e13 across) keep that finite for |1/d| <= 1e20
+            CWPB_CHECK((ew & 255u) <= 164u && ((ew >> 8) & 255u) <= 164u && ((ew >> 16) & 255u) <= 164u, CWP_ERR_INVALID,
+                       "CWBVH node %lld: quantisation exponent above 164 (child boxes beyond 3.5e13)", (long long)n);
             int nInt = __builtin_popcount(imask);
             CWPB_CHECK(nInt == 0 || (childBase >= 0 && (int64_t)childBase + nInt <= nNodes), CWP_ERR_INVALID, "CWBVH node %lld: children [%d, +%d) out of range", (long long)n, childBase, nInt);
             for (int s = 0; s < 8; s++) {

@@ -211,6 +211,7 @@ struct SharedStack {
 
 
 // ---------------- CWBVH ----------------
+__device__ __forceinline__ __half2 h2_of_bits(unsigned u) { __half2 h; memcpy(&h, &u, 4); return h; }
 __device__ __forceinline__ unsigned byte_of(unsigned w, int s) { return (w >> (8 * (s & 3))) & 255u; }
 // Byte s of w as an exact float without an int->float conversion (those run on the quarter-rate XU pipe): the byte
 // permute builds the bit pattern 0x4B0000bb, which is the float 2^23 + b, and the subtraction is exact.
@@ -235,7 +236,10 @@ struct TravState<8, ANY, TRI> {
         float4 nf[5]; fetch_node<5>(nodes, node, nf);
         const float4 f0 = nf[0], f1 = nf[1], f2 = nf[2], f3_ = nf[3], f4_ = nf[4];
         const unsigned ew = __float_as_uint(f0.w);
-        const float sx = __uint_as_float((ew & 255u) << 23) * idx, sy = __uint_as_float(((ew >> 8) & 255u) << 23) * idy, sz = __uint_as_float(((ew >> 16) & 255u) << 23) * idz;
+        // 2^e / d per axis as the reference computes it, times 2^24 (exact whatever its range; the upload check on the
+        // exponent bytes, at most 164, keeps it finite for |1/d| up to the 1e20 of the safe reciprocal)
+        const float sx24 = (__uint_as_float((ew & 255u) << 23) * idx) * 16777216.f, sy24 = (__uint_as_float(((ew >> 8) & 255u) << 23) * idy) * 16777216.f,
+                    sz24 = (__uint_as_float(((ew >> 16) & 255u) << 23) * idz) * 16777216.f;
         const float ox = (f0.x - o.x) * idx, oy = (f0.y - o.y) * idy, oz = (f0.z - o.z) * idz;
         const unsigned imask = ew >> 24, m0 = __float_as_uint(f1.z), m1 = __float_as_uint(f1.w);
         const int childBase = __float_as_int(f1.x), triBase = __float_as_int(f1.y);
@@ -249,11 +253,26 @@ struct TravState<8, ANY, TRI> {
         const unsigned nz0 = __float_as_uint(fz ? f4_.z : f3_.x), nz1 = __float_as_uint(fz ? f4_.w : f3_.y), pz0 = __float_as_uint(fz ? f3_.x : f4_.z), pz1 = __float_as_uint(fz ? f3_.y : f4_.w);
         // all eight slab tests first (predicated, no branches), then the hit leaves in slot order
         unsigned boxHit = 0;
+        // The quantised planes q (bytes) enter the fused affine map as the f16 subnormals q 2^-24: one byte permute
+        // places two bytes as two halves, and the f16 -> f32 conversions are exact; the per-axis scales carry the
+        // factor 2^24 in their exponents (sx24 = 2^(e + 24) / d, exact), so fmaf(q 2^-24, sx24, ox) is bit for bit
+        // fmaf(q, 2^e / d, ox) - the slab distances of the reference's decode - at one permute per two planes
+        // instead of a permute and a subtraction per plane.
+        float2 pbx, pby, pbz, pcx, pcy, pcz;
 #pragma unroll
         for (int s = 0; s < 8; s++) {
-            const float xn = fmaf(qbyte(s < 4 ? nx0 : nx1, s), sx, ox), xf = fmaf(qbyte(s < 4 ? px0 : px1, s), sx, ox);
-            const float yn = fmaf(qbyte(s < 4 ? ny0 : ny1, s), sy, oy), yf = fmaf(qbyte(s < 4 ? py0 : py1, s), sy, oy);
-            const float zn = fmaf(qbyte(s < 4 ? nz0 : nz1, s), sz, oz), zf = fmaf(qbyte(s < 4 ? pz0 : pz1, s), sz, oz);
+            float2 bx, by, bz, cx, cy, cz;
+            if ((s & 1) == 0) {
+                const unsigned sel = (s & 2) ? 0x4342u : 0x4140u;
+                bx = __half22float2(h2_of_bits(__byte_perm(s < 4 ? nx0 : nx1, 0u, sel))); cx = __half22float2(h2_of_bits(__byte_perm(s < 4 ? px0 : px1, 0u, sel)));
+                by = __half22float2(h2_of_bits(__byte_perm(s < 4 ? ny0 : ny1, 0u, sel))); cy = __half22float2(h2_of_bits(__byte_perm(s < 4 ? py0 : py1, 0u, sel)));
+                bz = __half22float2(h2_of_bits(__byte_perm(s < 4 ? nz0 : nz1, 0u, sel))); cz = __half22float2(h2_of_bits(__byte_perm(s < 4 ? pz0 : pz1, 0u, sel)));
+                pbx = bx; pby = by; pbz = bz; pcx = cx; pcy = cy; pcz = cz;
+            }
+            const bool hi = s & 1;
+            const float xn = fmaf(hi ? pbx.y : pbx.x, sx24, ox), xf = fmaf(hi ? pcx.y : pcx.x, sx24, ox);
+            const float yn = fmaf(hi ? pby.y : pby.x, sy24, oy), yf = fmaf(hi ? pcy.y : pcy.x, sy24, oy);
+            const float zn = fmaf(hi ? pbz.y : pbz.x, sz24, oz), zf = fmaf(hi ? pcz.y : pcz.x, sz24, oz);
             // entry = max(xn, yn, zn, tmin), exit = min(xf, yf, zf, hitT) selected with 3-input integer min/max on the
             // float bits: for values >= +0 the integer order is the float order, entry >= tmin >= +0, and any negative
             // candidate for the exit makes the float comparison below fail whichever negative value is picked - so
@@ -263,8 +282,8 @@ struct TravState<8, ANY, TRI> {
             boxHit |= (tn <= tf ? 1u : 0u) << s;
         }
         // leaf slots: meta bit 7 of each byte
-        const unsigned leafMask = ((m0 >> 7) & 1u) | ((m0 >> 14) & 2u) | ((m0 >> 21) & 4u) | ((m0 >> 28) & 8u) |
-                                  ((m1 >> 3) & 16u) | ((m1 >> 10) & 32u) | ((m1 >> 17) & 64u) | ((m1 >> 24) & 128u);
+        // (bit 7 of each byte, gathered by one multiply: the four products land on bits 28..31 without carries)
+        const unsigned leafMask = ((((m0 >> 7) & 0x01010101u) * 0x10204080u) >> 28) | (((((m1 >> 7) & 0x01010101u) * 0x10204080u) >> 24) & 0xF0u);
         unsigned leafHit = boxHit & leafMask;
         // internal children hit, re-indexed to octant order (slot s -> bit s ^ oct)
         unsigned hits = boxHit & imask;
@@ -354,7 +373,6 @@ __device__ __forceinline__ bool wt_leaf(const float4* __restrict__ vt, int first
     return false;
 }
 
-__device__ __forceinline__ __half2 h2_of_bits(unsigned u) { __half2 h; memcpy(&h, &u, 4); return h; }
 
 // whether an axis's plane distances stay inside the f16 range (see above)
 __device__ __forceinline__ bool h16_ok(float A, float B) {
