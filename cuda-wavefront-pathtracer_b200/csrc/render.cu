@@ -195,7 +195,8 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_trace_shade(const __gr
 }
 
 #ifndef CWPB_REFILL
-#define CWPB_REFILL 12   // a warp refetches rays once this many of its lanes are idle
+#define CWPB_REFILL 24   // a warp refetches rays once this many of its lanes are idle (measured 12..32 on frame512:
+                         // 12 74.6 ms, 16 72.7, 20 71.3, 24 70.8, 28 72.0, 32 76.6)
 #endif
 
 // Persistent traversal with dynamic refill (Aila & Laine 2009): every lane holds one ray's traversal state and

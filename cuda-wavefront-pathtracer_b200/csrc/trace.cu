@@ -162,7 +162,10 @@ __global__ void __launch_bounds__(kBatchBlock) k_trace_any(const float4* __restr
 
 // Persistent variant with dynamic refill: each lane advances its ray one node visit per step and the warp refetches
 // rays (one atomic on *fetch) once kRefillBatch lanes are idle. *fetch must be zero at launch.
-static constexpr int kRefillBatch = 12;
+#ifndef CWPB_BATCH_REFILL
+#define CWPB_BATCH_REFILL 12
+#endif
+static constexpr int kRefillBatch = CWPB_BATCH_REFILL;
 __device__ __forceinline__ unsigned lane_lt() { unsigned m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
 
 template <int V, int TRI, bool ANY>

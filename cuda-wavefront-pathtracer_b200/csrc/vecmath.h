@@ -68,16 +68,18 @@ CWPB_HD void frame_of(float3 n, float3& t, float3& b) {
     float s = n.z >= 0.f ? 1.f : -1.f; float a = -1.f / (s + n.z); float c = n.x * n.y * a;
     t = f3(1.f + s * n.x * n.x * a, s * c, -s * n.x); b = f3(c, s + n.y * n.y * a, -n.y);
 }
+// cos and sin of 2 pi u for u in [0, 1)
+CWPB_HD void turn(float u, float& c, float& s) { const float ph = CWPB_TWO_PI * u; c = cosf(ph); s = sinf(ph); }
 // cosine-weighted hemisphere direction (pdf cos/pi), as core/sampling.h:19-22
 CWPB_HD float3 cosine_dir(float3 n, float u0, float u1) {
-    float r = sqrtf(u0), ph = CWPB_TWO_PI * u1; float3 t, b; frame_of(n, t, b);
-    return normalize(t * (r * cosf(ph)) + b * (r * sinf(ph)) + n * sqrtf(fmaxf(0.f, 1.f - u0)));
+    float r = sqrtf(u0), c, s; turn(u1, c, s); float3 t, b; frame_of(n, t, b);
+    return normalize(t * (r * c) + b * (r * s) + n * sqrtf(fmaxf(0.f, 1.f - u0)));
 }
 // uniform direction in a cone of half-angle acos(cosMax), as core/sampling.h:25-29
 CWPB_HD float3 cone_dir(float3 axis, float cosMax, float u0, float u1) {
-    float cz = 1.f - u0 * (1.f - cosMax); float sz = sqrtf(fmaxf(0.f, 1.f - cz * cz)); float ph = CWPB_TWO_PI * u1;
+    float cz = 1.f - u0 * (1.f - cosMax); float sz = sqrtf(fmaxf(0.f, 1.f - cz * cz)), c, s; turn(u1, c, s);
     float3 t, b; frame_of(axis, t, b);
-    return normalize(axis * cz + t * (sz * cosf(ph)) + b * (sz * sinf(ph)));
+    return normalize(axis * cz + t * (sz * c) + b * (sz * s));
 }
 // piecewise-linear inverse-CDF lookup of n+1 entries, as core/sampling.h:32-34
 CWPB_HD float table_lookup(const float* tab, int n, float u) {
