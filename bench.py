@@ -621,6 +621,9 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
     t0 = time.perf_counter()
     meshes, descs, first, mats, base, boxes = cwp.serving_scenes(n_scenes=wl["scenes"], seed=wl["seed"])
     b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=wl["builder"], tlas_width=args.tlas_width)
+    if args.tuning:
+        blk, wd, fe, sm = (int(x) for x in args.tuning.split(","))
+        b.set_tuning(blk, wd, fe, sm)
     gen_s = time.perf_counter() - t0
     n_req = args.rays if args.rays else wl["requests"]
     streams = {"mix": cwp.serving_requests(n_req, wl["rate"], boxes, seed=wl["seed"] + 1),
@@ -685,7 +688,7 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="override the frame's samples per pixel (profiling cases)")
     ap.add_argument("--rays", type=int, default=0, help="override the batch size of trace16m / rays per scene of batched64 (profiling cases)")
     ap.add_argument("--scenes", type=int, default=0, help="override the scene count of batched64 (profiling cases)")
-    ap.add_argument("--tuning", default="", help="batched64: fixed launch shape block,width,fetch,smem instead of the autotuner (profiling cases)")
+    ap.add_argument("--tuning", default="", help="batched64 / serving: fixed launch shape block,width,fetch,smem (batched64: instead of the autotuner)")
     ap.add_argument("--builder", type=int, default=0, help="batched64: 0 every BLAS on the GPU (H-PLOC, one launch), 1 on the host cores (binned SAH)")
     ap.add_argument("--precision", action="store_true", help="ray-batch workloads: use the precision form")
     ap.add_argument("--traversal", type=int, default=0, help="0 auto (persistent refill for BVH2/CWBVH), 1 refill, 2 one 32-ray fetch per warp")
