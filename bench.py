@@ -647,7 +647,7 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
     if args.slo_sweep:
         sweeps["small"] = slo_sweep(cwp, b, mats, base, descs, first, wl, maxr_c, args, boxes, "small", [25.0, 50.0, 75.0, 100.0, 150.0], 200,
                                     resolutions=[(256, 256), (512, 512)], spps=[1, 4])
-        sweeps["mix"] = slo_sweep(cwp, b, mats, base, descs, first, wl, maxr_c, args, boxes, "mix", [0.25, 0.5, 1.0], 16)
+        sweeps["mix"] = slo_sweep(cwp, b, mats, base, descs, first, wl, maxr_c, args, boxes, "mix", [0.75, 1.5, 3.0], 64)
     info = b.info()
     c, p = res[("mix", "continuous")], res[("mix", "plain")]
     cs, ps = res[("small", "continuous")], res[("small", "plain")]

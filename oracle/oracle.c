@@ -692,12 +692,13 @@ static double hround(double x, int mode) { /* mode 0 nearest-even, -1 toward -in
 }
 static double hfma(double a, double b, double c) { return hround(a * b + c, 0); }
 double orc_half_round(double x, int mode) { return hround(x, mode); }
+static float h16_margin(float A, float B) { return (1.001f * fabsf(A) + 1792.f * fabsf(B)) * (1.f / 2048.f) + 1e-4f; }
 static int h16_ok(float A, float B) {
-    const float m = (fabsf(A) + 2048.f * fabsf(B)) * (1.f / 512.f) + 1e-4f, Ap = A - 1024.f * B;
+    const float m = h16_margin(A, B), Ap = A - 1024.f * B;
     return fabsf(B) * 1279.f < 30000.f && fabsf(Ap) + m < 30000.f;
 }
 static void h16_axis(float A, float B, double* lo, double* hi, double* b) {
-    const float m = (fabsf(A) + 2048.f * fabsf(B)) * (1.f / 512.f) + 1e-4f, Ap = A - 1024.f * B;
+    const float m = h16_margin(A, B), Ap = A - 1024.f * B;
     *lo = hround(Ap - m, -1); *hi = hround(Ap + m, 1); *b = hround(B, 0);
 }
 static void f32_axis(float A, float B, float* lo, float* hi, float* b) {
