@@ -605,7 +605,7 @@ def slo_sweep(cwp, b, mats, base, descs, first, wl, maxr, args, boxes, name, rat
     for rate in rates:
         stream = cwp.serving_requests(n_req, rate, boxes, seed=wl["seed"] + 100 + int(rate * 10), resolutions=resolutions, spps=spps)
         for mode, m in (("continuous", maxr), ("plain", 1)):
-            s = cwp.Server(b, mats, base, max_paths=args.paths or wl["max_paths"], max_requests=m, regroup=bool(args.regroup), policy=args.policy)
+            s = cwp.Server(b, mats, base, max_paths=args.paths or wl["max_paths"], max_requests=m, regroup=bool(args.regroup), policy=args.policy, overlap=bool(args.overlap))
             s.set_scenes(descs, first)
             r = serve_stream(cwp, s, stream)
             pts[mode].append({"rate_req_s": rate, "throughput_req_s": r["throughput_req_s"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"]})
@@ -632,7 +632,7 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
     maxr_c = args.max_requests or wl["max_requests"]
     for name, stream in streams.items():
         for mode, maxr in (("continuous", maxr_c), ("plain", 1)):
-            s = cwp.Server(b, mats, base, max_paths=args.paths or wl["max_paths"], max_requests=maxr, regroup=bool(args.regroup), policy=args.policy)
+            s = cwp.Server(b, mats, base, max_paths=args.paths or wl["max_paths"], max_requests=maxr, regroup=bool(args.regroup), policy=args.policy, overlap=bool(args.overlap))
             s.set_scenes(descs, first)
             barrier()
             clk = Clocks(str(torch.cuda.current_device()))
@@ -657,6 +657,7 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
                config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "blas_builder": ["gpu h-ploc", "host binned SAH"][wl["builder"]],
                        "blas_build_ms": info.blas_build_ms, "scene_generation_s": gen_s, "depth": 8, "max_paths": wl["max_paths"], "max_requests": maxr_c,
                        "tlas_width": args.tlas_width, "regroup": bool(args.regroup), "policy": ["even share", "oldest first with backfill"][args.policy],
+                       "overlap": bool(args.overlap),
                        "materials": "OpenPBR subset: roughness U[0.05,1], metallic Bernoulli(0.3), 10% glass IOR 1.5",
                        "mix": {"requests": n_req, "arrival_rate_req_s": wl["rate"], "resolutions": "256^2, 512^2, 1280x720, 1920x1080", "spp": "1, 4, 16, 64, 256",
                                "continuous": strip(c), "plain": strip(p), "throughput_vs_plain": c["throughput_req_s"] / p["throughput_req_s"],
@@ -699,6 +700,7 @@ def main():
     ap.add_argument("--policy", type=int, default=0, help="serving: new paths by even share (0) or oldest first with backfill (1)")
     ap.add_argument("--slo-sweep", type=int, default=1, help="serving: also sweep arrival rates for throughput at equal p99 (1) or not (0)")
     ap.add_argument("--regroup", type=int, default=1, help="serving: sort each step's continuations by request (1) or not (0)")
+    ap.add_argument("--overlap", type=int, default=1, help="serving: a step returns with its launches queued (1) or waits for them (0)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     ap.add_argument("--stage-levels", type=int, default=0, help="frames (CWBVH): top tree levels staged in shared memory per block (0 library default, -1 none, 1..3)")
     args = ap.parse_args()

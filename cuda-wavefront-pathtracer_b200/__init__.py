@@ -109,7 +109,7 @@ class Material(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("max_paths", C.c_int64), ("max_requests", C.c_int32), ("gd_energy", C.c_int32), ("hbm_reserve", C.c_int64), ("device", C.c_int32),
-                ("regroup", C.c_int32), ("policy", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("regroup", C.c_int32), ("policy", C.c_int32), ("overlap", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class Request(C.Structure):
@@ -749,10 +749,10 @@ class Server:
     form (max_requests = 1)."""
 
     def __init__(self, batch, materials, mesh_mat_base, max_paths=8 << 20, max_requests=64, gd_energy=1, hbm_reserve=1 << 30, device=0,
-                 regroup=True, policy=0):
+                 regroup=True, policy=0, overlap=True):
         self._batch = batch
         M = materials_array(materials); base = np.ascontiguousarray(mesh_mat_base, np.int32)
-        o = ServerOptions(max_paths, max_requests, gd_energy, hbm_reserve, device, 1 if regroup else -1, policy)
+        o = ServerOptions(max_paths, max_requests, gd_energy, hbm_reserve, device, 1 if regroup else -1, policy, 1 if overlap else -1)
         h = C.c_void_p()
         _check(lib().cwp_server_create(batch._h, M, len(M), _iptr(base), C.byref(o), C.byref(h)))
         self._h = h

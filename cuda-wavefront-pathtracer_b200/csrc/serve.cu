@@ -460,6 +460,9 @@ struct ServeRequest {
     int64_t total = 0, issued = 0, finished = 0; double rays = 0, shadow = 0;
     float4* accum = nullptr; bool done = false;
     void* lights = nullptr;   // the request's emissive-triangle tables (pool memory), freed at completion
+    // host data prepared at submission (so that admission, on the step's critical path, only copies): the scene's
+    // instances at the request's frame and its emissive-triangle tables
+    std::vector<cwp_instance> inst; std::vector<float> emT, emC, mlp;
 };
 
 struct cwp_server {
@@ -488,10 +491,13 @@ struct cwp_server {
     std::deque<int64_t> pending; std::map<int64_t, ServeRequest> reqs; std::vector<int64_t> completed;
     int64_t nextId = 1;
     cudaStream_t st = nullptr;
+    cudaStream_t cst = nullptr;   // result copies: completed images, read while the next step runs
     std::chrono::steady_clock::time_point t0;
     std::vector<void*> allocs;
     cudaEvent_t ev[6] = {};   // raygen start, closest start, shade start, shadow start, shadow end, accumulation start
     cwp_server_info info{};
+    bool overlap = true;        // a step returns with its launches queued; the next call takes its results
+    bool inflight = false; int64_t inflightN = 0; double inflightStart = 0;   // the queued step: rays traced, host start time
 };
 
 // one CUDA array and texture object per image: bilinear filtering, wrap addressing, normalised coordinates, 8-bit
@@ -535,7 +541,8 @@ extern "C" double cwp_server_clock_ms(const cwp_server* s) { return s ? now_ms(s
 extern "C" void cwp_server_destroy(cwp_server* s) {
     if (!s) return;
     cudaSetDevice(s->device);
-    if (s->st) cudaStreamSynchronize(s->st);
+    if (s->st) cudaStreamSynchronize(s->st);   // a queued step included
+    if (s->cst) cudaStreamSynchronize(s->cst);
     for (auto& kv : s->reqs) {
         if (kv.second.accum) cudaFreeAsync(kv.second.accum, s->st);
         if (kv.second.lights) cudaFreeAsync(kv.second.lights, s->st);
@@ -551,6 +558,7 @@ extern "C" void cwp_server_destroy(cwp_server* s) {
     if (s->hChunks) cudaFreeHost(s->hChunks);
     for (cudaEvent_t e : s->ev) if (e) cudaEventDestroy(e);
     if (s->st) cudaStreamDestroy(s->st);
+    if (s->cst) cudaStreamDestroy(s->cst);
     delete s;
 }
 
@@ -562,6 +570,7 @@ static int server_create(cwp_batch* b, const cwp_material* mats, int n, const in
     s->O.hbm_reserve = o && o->hbm_reserve > 0 ? o->hbm_reserve : (1ll << 30);
     s->O.regroup = o && o->regroup < 0 ? -1 : 1;
     s->O.policy = o ? o->policy : 0;
+    s->overlap = !(o && o->overlap < 0);
     CWPB_CHECK(s->O.policy == 0 || s->O.policy == 1, CWP_ERR_INVALID, "policy %d is not 0 or 1", s->O.policy);
     CWPB_CHECK(s->O.max_paths < (1ll << 30), CWP_ERR_INVALID, "max_paths %lld above 2^30", (long long)s->O.max_paths);
     CWPB_CHECK(s->O.max_requests <= 1024, CWP_ERR_INVALID, "max_requests %d above 1024", s->O.max_requests);
@@ -572,6 +581,7 @@ static int server_create(cwp_batch* b, const cwp_material* mats, int n, const in
                                            mats[i].transmission >= 0.f && mats[i].transmission <= 1.f, CWP_ERR_INVALID, "material %d out of range", i);
     CWPB_CUDA(cudaSetDevice(s->device));
     CWPB_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+    CWPB_CUDA(cudaStreamCreateWithFlags(&s->cst, cudaStreamNonBlocking));
     for (cudaEvent_t& e : s->ev) CWPB_CUDA(cudaEventCreate(&e));
     auto alloc = [&](void** p, size_t bytes) -> int { CWPB_CUDA(cudaMalloc(p, bytes)); s->allocs.push_back(*p); return CWP_OK; };
     const size_t P = (size_t)s->O.max_paths, R = (size_t)s->O.max_requests;
@@ -748,6 +758,27 @@ extern "C" int cwp_texture_sample_batch(const cwp_texture* tex, int32_t nTex, co
     return CWP_OK;
 }
 
+// A request's host data, prepared at submission: the instances of its scene at its frame, and (unless it samples the
+// BSDF only) the emissive-triangle tables there. Scenes and instance matrices change only while no request is queued,
+// so the data stays valid until admission.
+static int prepare_request(const cwp_server* s, ServeRequest& q) {
+    std::vector<float> xf; std::vector<int> im;
+    q.inst.clear();
+    for (int i = s->sceneFirst[q.r.scene]; i < s->sceneFirst[q.r.scene + 1]; i++) {
+        float m[12]; cwp_instance rec;
+        if (!s->xfCount.empty() && s->xfCount[i] > 0) {   // a matrix per frame, the last one held
+            const float* x = s->xf.data() + 12 * ((size_t)s->xfFirst[i] + std::min(std::max(q.r.frame, 0), s->xfCount[i] - 1));
+            std::copy(x, x + 12, m);
+        } else if (int rc = cwp_xform_animate(&s->desc[i], q.r.frame, m)) return rc;
+        if (int rc = cwp_instance_from_xform(m, s->desc[i].mesh, &rec)) return rc;
+        q.inst.push_back(rec); xf.insert(xf.end(), m, m + 12); im.push_back(s->desc[i].mesh);
+    }
+    q.emT.clear(); q.emC.clear(); q.mlp.clear();
+    if (!s->em.empty() && q.r.light_mode != CWP_LIGHT_BSDF)
+        frame_lights(s->em, xf.data(), im.data(), (int64_t)im.size(), s->hMats.data(), s->nMats, q.emT, q.emC, q.mlp);
+    return CWP_OK;
+}
+
 extern "C" int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* id) {
     CWPB_CHECK(s && r && id, CWP_ERR_INVALID, "NULL argument");
     CWPB_CHECK(!s->sceneFirst.empty(), CWP_ERR_STATE, "no scenes (cwp_server_set_scenes)");
@@ -762,9 +793,12 @@ extern "C" int cwp_server_submit(cwp_server* s, const cwp_request* r, int64_t* i
     CWPB_CHECK(r->cam.w > 0 && r->cam.h > 0 && r->spp > 0 && r->max_depth >= 0 && r->max_depth <= 64, CWP_ERR_INVALID, "bad request size");
     const int64_t total = (int64_t)r->cam.w * r->cam.h * r->spp;
     CWPB_CHECK(total < (1ll << 31), CWP_ERR_INVALID, "%lld paths in one request (limit 2^31)", (long long)total);
-    ServeRequest q; q.r = *r; q.id = s->nextId++; q.submitMs = now_ms(s); q.total = total;
-    s->reqs[q.id] = q; s->pending.push_back(q.id);
-    *id = q.id;
+    ServeRequest q; q.r = *r; q.submitMs = now_ms(s); q.total = total;
+    if (int rc = prepare_request(s, q)) return rc;
+    q.id = s->nextId++;
+    const int64_t qid = q.id;
+    s->reqs[qid] = std::move(q); s->pending.push_back(qid);
+    *id = qid;
     return CWP_OK;
 }
 
@@ -821,22 +855,10 @@ static int admit(cwp_server* s, bool& changed) {
             const cwp_server::EnvMap& E = s->envs[q.r.env];
             P.envTex = E.tex; P.envMarg = E.marg; P.envCond = E.cond; P.envW = E.w; P.envH = E.h; P.envRot = q.r.env_rot_deg * 3.14159265f / 180.f;
         }
-        // the scene's instances at the request's frame, and its emissive triangles there
-        std::vector<cwp_instance>& v = s->slotInst[slot]; v.clear();
-        std::vector<float> xf; std::vector<int> im;
-        for (int i = s->sceneFirst[q.r.scene]; i < s->sceneFirst[q.r.scene + 1]; i++) {
-            float m[12]; cwp_instance rec;
-            if (!s->xfCount.empty() && s->xfCount[i] > 0) {   // a matrix per frame, the last one held
-                const float* x = s->xf.data() + 12 * ((size_t)s->xfFirst[i] + std::min(std::max(q.r.frame, 0), s->xfCount[i] - 1));
-                std::copy(x, x + 12, m);
-            } else if (int rc = cwp_xform_animate(&s->desc[i], q.r.frame, m)) return rc;
-            if (int rc = cwp_instance_from_xform(m, s->desc[i].mesh, &rec)) return rc;
-            v.push_back(rec); xf.insert(xf.end(), m, m + 12); im.push_back(s->desc[i].mesh);
-        }
-        if (!s->em.empty() && q.r.light_mode != CWP_LIGHT_BSDF) {
-            std::vector<float> emT, emC, mlp;
-            frame_lights(s->em, xf.data(), im.data(), (int64_t)im.size(), s->hMats.data(), s->nMats, emT, emC, mlp);
-            if (!emT.empty()) {
+        // the scene's instances at the request's frame, and its emissive triangles there (prepared at submission)
+        if (!q.emT.empty()) {
+            const std::vector<float>& emT = q.emT; const std::vector<float>& emC = q.emC; const std::vector<float>& mlp = q.mlp;
+            {
                 const size_t bT = emT.size() * sizeof(float), bC = (emC.size() * sizeof(float) + 15) & ~(size_t)15, bM = mlp.size() * sizeof(float);
                 const cudaError_t e2 = (int64_t)(bT + bC + bM) <= avail ? cudaMallocFromPoolAsync(&q.lights, bT + bC + bM, s->pool, s->st) : cudaErrorMemoryAllocation;
                 if (e2 == cudaErrorMemoryAllocation) {   // no room for the tables: the request waits with its image freed
@@ -860,6 +882,7 @@ static int admit(cwp_server* s, bool& changed) {
         P.pSun = sunOn ? 1.f / nt : 0.f; P.pTri = triOn ? 1.f / nt : 0.f; P.pEnv = envOn ? 1.f / nt : 0.f;
         P.lightMode = q.r.light_mode; P.rr = q.r.rr; P.rrDepth = q.r.rr_depth; P.envUniform = q.r.env_uniform; P.bumpShadow = q.r.bump_shadow;
         P.nearClip = q.r.near_clip; P.filterBh = q.r.filter_bh;
+        s->slotInst[slot].swap(q.inst); q.inst.clear(); q.inst.shrink_to_fit();
         s->slotsDirty = true;
         CWPB_CUDA(cudaMemsetAsync(s->slotCnt + kSlotCounters * slot, 0, kSlotCounters * sizeof(int), s->st));
         q.slot = slot; q.admitMs = now_ms(s); s->info.admissions++; s->admitted.push_back(slot);
@@ -874,20 +897,42 @@ static int admit(cwp_server* s, bool& changed) {
     return CWP_OK;
 }
 
-extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPending) {
-    CWPB_CHECK(s, CWP_ERR_INVALID, "server is NULL");
-    CWPB_CUDA(cudaSetDevice(s->device));
-    const double stepStart = now_ms(s);
-    bool changed = false;
-    if (int rc = admit(s, changed)) return rc;
-    s->info.admit_ms += now_ms(s) - stepStart;
-    if (changed) {
-        CWPB_CUDA(cudaStreamSynchronize(s->st));
-        const double t = now_ms(s);
-        if (int rc = rebuild_tlas(s)) return rc;
-        s->info.tlas_ms += now_ms(s) - t; s->info.tlas_rebuilds++;
-        cwp_batch_info bi{}; if (cwp_batch_info_of(s->batch, &bi) == CWP_OK) s->info.tlas_device_ms += bi.tlas_build_ms;
+// takes the results of the queued step: waits for its launches (the step's one host round trip), reads the queue
+// lengths and per-request counts, adds its timings and completes the requests whose paths have all finished
+static int finish_step(cwp_server* s) {
+    if (!s->inflight) return CWP_OK;
+    s->inflight = false;
+    const int R = s->O.max_requests; const int64_t n = s->inflightN;
+    CWPB_CUDA(cudaStreamSynchronize(s->st));
+    int64_t nNext = 0, nShadow = 0;
+    if (n > 0) { nNext = s->hcnt[0]; nShadow = s->hcnt[1]; }
+    {
+        float a = 0, b = 0, c = 0, d = 0;
+        CWPB_CUDA(cudaEventElapsedTime(&a, s->ev[0], s->ev[1])); CWPB_CUDA(cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
+        CWPB_CUDA(cudaEventElapsedTime(&c, s->ev[2], s->ev[3])); CWPB_CUDA(cudaEventElapsedTime(&d, s->ev[3], s->ev[4]));
+        float e = 0; CWPB_CUDA(cudaEventElapsedTime(&e, s->ev[5], s->ev[4]));
+        s->info.raygen_ms += a; s->info.closest_ms += b; s->info.shade_ms += c; s->info.shadow_ms += d; s->info.accum_ms += e;
+        s->info.steps++; s->info.rays += n; s->info.shadow_rays += nShadow;
     }
+    if ((s->info.steps & 63) == 0 || nNext == 0) { if (int rc = cwp_batch_status(s->batch)) return rc; }   // traversal bounds: checked every 64 steps and when the queue drains
+    s->cur ^= 1; s->nCur = nNext;
+    const double t = now_ms(s);
+    for (int k = 0; k < R; k++) {
+        if (s->slotReq[k] < 0) continue;
+        ServeRequest& q = s->reqs[s->slotReq[k]];
+        const int* c = s->hcnt + 4 + kSlotCounters * k;
+        q.rays = c[0]; q.shadow = c[1]; q.finished = c[2];
+        if (q.issued == q.total && q.finished == q.total) {
+            q.done = true; q.doneMs = t; s->completed.push_back(q.id); s->slotReq[k] = -1; q.slot = -1;
+            if (q.lights) { CWPB_CUDA(cudaFreeAsync(q.lights, s->st)); q.lights = nullptr; }
+        }
+    }
+    return CWP_OK;
+}
+
+// queues one step's launches: new camera paths, closest hits, shading, regrouping, shadow rays, accumulation, and
+// the copies of the counts the host reads when it takes the step's results
+static int launch_step(cwp_server* s) {
     // new camera paths: free capacity shared evenly by the slots with samples left to issue, oldest first
     const int R = s->O.max_requests;
     std::vector<int> needy;
@@ -912,7 +957,6 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
         CWPB_CUDA(cudaGetLastError());
     }
     const int64_t n = s->nCur + added;
-    int64_t nNext = 0, nShadow = 0;
     CWPB_CUDA(cudaEventRecord(s->ev[1], s->st));
     CWPB_CUDA(cudaEventRecord(s->ev[2], s->st));
     CWPB_CUDA(cudaEventRecord(s->ev[3], s->st));
@@ -947,29 +991,36 @@ extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPendin
     CWPB_CUDA(cudaEventRecord(s->ev[4], s->st));
     if (n > 0) CWPB_CUDA(cudaMemcpyAsync(s->hcnt, s->cnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CWPB_CUDA(cudaMemcpyAsync(s->hcnt + 4, s->slotCnt, (size_t)R * kSlotCounters * sizeof(int), cudaMemcpyDeviceToHost, s->st));
-    CWPB_CUDA(cudaStreamSynchronize(s->st));   // the step's one host round trip: queue lengths and per-request counts
-    if (n > 0) { nNext = s->hcnt[0]; nShadow = s->hcnt[1]; }
-    {
-        float a = 0, b = 0, c = 0, d = 0;
-        CWPB_CUDA(cudaEventElapsedTime(&a, s->ev[0], s->ev[1])); CWPB_CUDA(cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
-        CWPB_CUDA(cudaEventElapsedTime(&c, s->ev[2], s->ev[3])); CWPB_CUDA(cudaEventElapsedTime(&d, s->ev[3], s->ev[4]));
-        float e = 0; CWPB_CUDA(cudaEventElapsedTime(&e, s->ev[5], s->ev[4]));
-        s->info.raygen_ms += a; s->info.closest_ms += b; s->info.shade_ms += c; s->info.shadow_ms += d; s->info.accum_ms += e;
-        s->info.steps++; s->info.rays += n; s->info.shadow_rays += nShadow;
+    s->inflight = true; s->inflightN = n;
+    return CWP_OK;
+}
+
+// One step: the results of the queued step (overlapped form), admissions, the TLAS update for new requests, and
+// the next step's launches; with overlap -1 the call waits for them before returning. In the overlapped form the
+// device runs a step while the caller submits, polls and reads results; admissions still wait for the step before
+// them (free slots are known only then), so the device idles for the admission and TLAS update only.
+extern "C" int cwp_server_step(cwp_server* s, int32_t* nActive, int32_t* nPending) {
+    CWPB_CHECK(s, CWP_ERR_INVALID, "server is NULL");
+    CWPB_CUDA(cudaSetDevice(s->device));
+    const double stepStart = now_ms(s);
+    if (int rc = finish_step(s)) return rc;
+    const double admitStart = now_ms(s);
+    bool changed = false;
+    if (int rc = admit(s, changed)) return rc;
+    s->info.admit_ms += now_ms(s) - admitStart;
+    if (changed) {
+        CWPB_CUDA(cudaStreamSynchronize(s->st));
+        const double t = now_ms(s);
+        if (int rc = rebuild_tlas(s)) return rc;
+        s->info.tlas_ms += now_ms(s) - t; s->info.tlas_rebuilds++;
+        cwp_batch_info bi{}; if (cwp_batch_info_of(s->batch, &bi) == CWP_OK) s->info.tlas_device_ms += bi.tlas_build_ms;
     }
-    if ((s->info.steps & 63) == 0 || nNext == 0) { if (int rc = cwp_batch_status(s->batch)) return rc; }   // traversal bounds: checked every 64 steps and when the queue drains
-    s->cur ^= 1; s->nCur = nNext;
-    // completion
-    const double t = now_ms(s);
-    for (int k = 0; k < R; k++) {
-        if (s->slotReq[k] < 0) continue;
-        ServeRequest& q = s->reqs[s->slotReq[k]];
-        const int* c = s->hcnt + 4 + kSlotCounters * k;
-        q.rays = c[0]; q.shadow = c[1]; q.finished = c[2];
-        if (q.issued == q.total && q.finished == q.total) {
-            q.done = true; q.doneMs = t; s->completed.push_back(q.id); s->slotReq[k] = -1; q.slot = -1;
-            if (q.lights) { CWPB_CUDA(cudaFreeAsync(q.lights, s->st)); q.lights = nullptr; }
-        }
+    const int R = s->O.max_requests;
+    bool any = false;
+    for (int k = 0; k < R; k++) any |= s->slotReq[k] >= 0;
+    if (any) {
+        if (int rc = launch_step(s)) return rc;
+        if (!s->overlap) { if (int rc = finish_step(s)) return rc; }
     }
     s->info.step_ms += now_ms(s) - stepStart;
     if (nActive) { int a = 0; for (int k = 0; k < R; k++) a += s->slotReq[k] >= 0; *nActive = a; }
@@ -993,9 +1044,9 @@ extern "C" int cwp_server_result(cwp_server* s, int64_t id, float* accum, cwp_re
     ServeRequest& q = it->second;
     CWPB_CHECK(q.done, CWP_ERR_STATE, "request %lld is not complete", (long long)id);
     CWPB_CUDA(cudaSetDevice(s->device));
-    if (accum) {
-        CWPB_CUDA(cudaMemcpyAsync(accum, q.accum, (size_t)q.r.cam.w * q.r.cam.h * sizeof(float4), cudaMemcpyDeviceToHost, s->st));
-        CWPB_CUDA(cudaStreamSynchronize(s->st));
+    if (accum) {   // the image's last writes completed before its step's results were taken; a queued step may be running
+        CWPB_CUDA(cudaMemcpyAsync(accum, q.accum, (size_t)q.r.cam.w * q.r.cam.h * sizeof(float4), cudaMemcpyDeviceToHost, s->cst));
+        CWPB_CUDA(cudaStreamSynchronize(s->cst));
     }
     if (st) {
         st->submit_ms = q.submitMs; st->admit_ms = q.admitMs; st->done_ms = q.doneMs; st->rays = q.rays; st->shadow_rays = q.shadow;

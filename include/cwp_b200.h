@@ -359,7 +359,11 @@ typedef struct cwp_server_options {
                               samples left (oldest first, the default); 1 oldest first takes all it can use, the later
                               ones fill what is left (a request's drain no longer idles the GPU, big requests keep the
                               plain form's speed) */
-    int32_t reserved[3];
+    int32_t overlap;       /* 0 (default) or 1: a step returns once its launches are queued, and the next call to
+                              cwp_server_step waits for them and takes their results (completions, queue lengths), so
+                              the caller's work between steps (submissions, results) overlaps the device; -1: every step
+                              waits for its own work before returning */
+    int32_t reserved[2];
 } cwp_server_options;
 
 typedef struct cwp_request {
@@ -436,8 +440,11 @@ int cwp_server_set_textures(cwp_server* s, const cwp_texture* tex, int32_t n_tex
 /* Texture lookups on the device, for tests of the filtering: n (texture, u, v) -> rgba, with the images of tex bound as
  * cwp_server_set_textures binds them. */
 int cwp_texture_sample_batch(const cwp_texture* tex, int32_t n_tex, const int32_t* id, const float* uv, float* rgba, int64_t n);
-/* One step: admission, new camera paths, one bounce of every admitted request (closest hit + shading, sun shadow rays),
- * completion. *n_active / *n_pending: admitted / waiting requests after the step. Synchronous. */
+/* One step: the results of the previous step (completions, queue lengths), admission, new camera paths, one bounce of
+ * every admitted request (closest hit + shading, light-sample shadow rays). With options.overlap (the default) the
+ * call returns once the bounce's launches are queued and its completions appear at the next call; with overlap -1 it
+ * waits for them. *n_active / *n_pending: admitted / waiting requests. A submission prepares the request's host data
+ * (instances at its frame, emissive tables), so the step's admission only copies them to the device. */
 int cwp_server_step(cwp_server* s, int32_t* n_active, int32_t* n_pending);
 /* Completed request ids since the last call (up to cap). */
 int cwp_server_poll(cwp_server* s, int64_t* ids, int32_t cap, int32_t* n);

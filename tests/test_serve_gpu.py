@@ -88,17 +88,19 @@ def _n_inst(b, n_scenes):
 
 def test_alone_equals_in_the_mix(gpu, cwp, serving):
     """Every request's image is the same whether it runs alone (plain form, one request at a time) or among others
-    admitted concurrently, with or without the per-step regrouping of the queue by request, and under either feeding
-    policy: only the order of float atomics differs."""
+    admitted concurrently, with or without the per-step regrouping of the queue by request, under either feeding
+    policy, and whether a step returns with its launches queued or waits for them: only the order of float atomics
+    differs."""
     b, descs, first, mats, base, boxes = serving
     reqs = requests(cwp, boxes, 8, seed=5)
     mix = run_all(server(cwp, serving, max_paths=1 << 15, max_requests=8), reqs)
     mixed_order = run_all(server(cwp, serving, max_paths=1 << 15, max_requests=8, regroup=False), reqs)
     oldest_first = run_all(server(cwp, serving, max_paths=1 << 15, max_requests=8, policy=1), reqs)
+    waiting = run_all(server(cwp, serving, max_paths=1 << 15, max_requests=8, overlap=False), reqs)
     alone = run_all(server(cwp, serving, max_paths=1 << 15, max_requests=1), reqs)
-    for (am, sm), (ao, so), (af, sf), (aa, sa) in zip(mix, mixed_order, oldest_first, alone):
-        assert sm.rays == sa.rays == so.rays == sf.rays and sm.shadow_rays == sa.shadow_rays == so.shadow_rays == sf.shadow_rays
-        assert np.allclose(am, aa, rtol=1e-4, atol=1e-5) and np.allclose(ao, aa, rtol=1e-4, atol=1e-5) and np.allclose(af, aa, rtol=1e-4, atol=1e-5)
+    for (am, sm), (ao, so), (af, sf), (aw, sw), (aa, sa) in zip(mix, mixed_order, oldest_first, waiting, alone):
+        assert sm.rays == sa.rays == so.rays == sf.rays == sw.rays and sm.shadow_rays == sa.shadow_rays == so.shadow_rays == sf.shadow_rays == sw.shadow_rays
+        assert all(np.allclose(x, aa, rtol=1e-4, atol=1e-5) for x in (am, ao, af, aw))
     # in the mix, requests overlapped: some request was admitted before an earlier one finished
     adm = sorted((s.admit_ms, s.done_ms) for _, s in mix)
     assert any(adm[i + 1][0] < adm[i][1] for i in range(len(adm) - 1))
