@@ -480,7 +480,8 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
     t0 = time.perf_counter()
     meshes, xf, mesh_of, first = batched_setup(cwp, wl)
     gen_s = time.perf_counter() - t0
-    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=args.builder, tlas_width=args.tlas_width)
+    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=args.builder, spatial=args.spatial if args.builder == 1 else 0.0,
+                  tlas_width=args.tlas_width)
     inst = cwp.instances(xf, mesh_of)
     b.set_scenes(inst, first)
     info = b.info()
@@ -541,7 +542,7 @@ def bench_batched(args, wl, cwp, torch, ws, rank, barrier, reduce, dev_id, hbm_p
                        "rays": n, "rays_per_scene": per, "hit_rate": hit_rate,
                        "tuning": {"block": tun.block, "width": tun.width, "fetch": tun.fetch, "smem_stack": tun.smem_stack, "sample_ms": tun.ms},
                        "tlas_width": args.tlas_width,
-                       "autotune_s": tune_s, "blas_builder": ["gpu h-ploc (one launch)", "host binned SAH"][args.builder], "blas_build_ms": info.blas_build_ms,
+                       "autotune_s": tune_s, "blas_builder": ["gpu h-ploc (one launch)", "host binned SAH" + (f", spatial splits at {args.spatial:g}" if args.spatial > 0 else "")][args.builder], "blas_build_ms": info.blas_build_ms,
                        "blas_hploc_launches": info.blas_hploc_launches if args.builder == 0 else 0,
                        "tlas_build_ms": info.tlas_build_ms, "node_bytes": {"bvh2": int(info.node_bytes[0]), "bvh4": int(info.node_bytes[1]), "cwbvh": int(info.node_bytes[2])},
                        "scene_generation_s": gen_s, "l2": f"ray queue {n * 36 / 1e9:.1f} GB > L2 (126 MB)",
@@ -620,7 +621,8 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
     import numpy as np
     t0 = time.perf_counter()
     meshes, descs, first, mats, base, boxes = cwp.serving_scenes(n_scenes=wl["scenes"], seed=wl["seed"])
-    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=wl["builder"], tlas_width=args.tlas_width)
+    # BLAS on the host cores, binned SAH (spatial splits only with --serve-spatial: measured 2.3x slower here)
+    b = cwp.Batch(meshes, device=torch.cuda.current_device(), builder=wl["builder"], spatial=args.serve_spatial, tlas_width=args.tlas_width)
     if args.tuning:
         blk, wd, fe, sm = (int(x) for x in args.tuning.split(","))
         b.set_tuning(blk, wd, fe, sm)
@@ -654,7 +656,7 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
     strip = lambda r: {k: v for k, v in r.items() if k != "clocks"}
     out.update(metric=METRIC_SERVING, value=c["job_throughput_req_s"], unit="req/s",
                ms_per_step=1e3 / c["job_throughput_req_s"], higher_is_better=True, dtype="f32",
-               config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "blas_builder": ["gpu h-ploc", "host binned SAH"][wl["builder"]],
+               config={"workload": args.workload, "scenes": wl["scenes"], "blas": info.n_blas, "tris": int(info.n_tris), "blas_builder": ["gpu h-ploc", "host binned SAH, 32 bins" + (f", spatial splits at {args.serve_spatial:g}" if args.serve_spatial > 0 else "")][wl["builder"]],
                        "blas_build_ms": info.blas_build_ms, "scene_generation_s": gen_s, "depth": 8, "max_paths": wl["max_paths"], "max_requests": maxr_c,
                        "tlas_width": args.tlas_width, "regroup": bool(args.regroup), "policy": ["even share", "oldest first with backfill"][args.policy],
                        "overlap": bool(args.overlap),
@@ -700,6 +702,7 @@ def main():
     ap.add_argument("--policy", type=int, default=0, help="serving: new paths by even share (0) or oldest first with backfill (1)")
     ap.add_argument("--slo-sweep", type=int, default=1, help="serving: also sweep arrival rates for throughput at equal p99 (1) or not (0)")
     ap.add_argument("--regroup", type=int, default=1, help="serving: sort each step's continuations by request (1) or not (0)")
+    ap.add_argument("--serve-spatial", type=float, default=0.0, help="serving: spatial-split threshold of the host-built BLAS (0: binned SAH)")
     ap.add_argument("--overlap", type=int, default=1, help="serving: a step returns with its launches queued (1) or waits for them (0)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
     ap.add_argument("--stage-levels", type=int, default=0, help="frames (CWBVH): top tree levels staged in shared memory per block (0 library default, -1 none, 1..3)")

@@ -212,6 +212,12 @@ struct SharedStack {
 
 // ---------------- CWBVH ----------------
 __device__ __forceinline__ __half2 h2_of_bits(unsigned u) { __half2 h; memcpy(&h, &u, 4); return h; }
+__device__ __forceinline__ unsigned bits_of_h2(__half2 h) { unsigned u; memcpy(&u, &h, 4); return u; }
+// CWBVH slots whose meta byte marks a leaf (bit 7 of each of the eight bytes in m0, m1), as an 8-bit mask: the four
+// flag bits of a word, isolated at bits 0, 8, 16, 24, are gathered onto bits 28..31 by one multiply (no carries)
+__device__ __forceinline__ unsigned leaf_slots(unsigned m0, unsigned m1) {
+    return ((((m0 >> 7) & 0x01010101u) * 0x10204080u) >> 28) | (((((m1 >> 7) & 0x01010101u) * 0x10204080u) >> 24) & 0xF0u);
+}
 __device__ __forceinline__ unsigned byte_of(unsigned w, int s) { return (w >> (8 * (s & 3))) & 255u; }
 // Byte s of w as an exact float without an int->float conversion (those run on the quarter-rate XU pipe): the byte
 // permute builds the bit pattern 0x4B0000bb, which is the float 2^23 + b, and the subtraction is exact.
@@ -281,10 +287,7 @@ struct TravState<8, ANY, TRI> {
             const float tf = __int_as_float(__vimin3_s32(__float_as_int(xf), __float_as_int(yf), min(__float_as_int(zf), __float_as_int(hitT))));
             boxHit |= (tn <= tf ? 1u : 0u) << s;
         }
-        // leaf slots: meta bit 7 of each byte
-        // (bit 7 of each byte, gathered by one multiply: the four products land on bits 28..31 without carries)
-        const unsigned leafMask = ((((m0 >> 7) & 0x01010101u) * 0x10204080u) >> 28) | (((((m1 >> 7) & 0x01010101u) * 0x10204080u) >> 24) & 0xF0u);
-        unsigned leafHit = boxHit & leafMask;
+        unsigned leafHit = boxHit & leaf_slots(m0, m1);
         // internal children hit, re-indexed to octant order (slot s -> bit s ^ oct)
         unsigned hits = boxHit & imask;
         if (oct & 1u) hits = ((hits & 0x55u) << 1) | ((hits & 0xAAu) >> 1);
@@ -351,10 +354,10 @@ __device__ __forceinline__ WtRay wt_setup(float3 d) {
     return r;
 }
 
-template <bool ANY>
-__device__ __forceinline__ bool wt_leaf(const float4* __restrict__ vt, int first, int cnt, float3 o, const WtRay& r, float tmin,
-                                        float& hitT, int& hitTri, float& hu, float& hv) {
-    for (int t = first; t < first + cnt; t++) {
+// one watertight test of triangle t; true when it became the closest hit
+__device__ __forceinline__ bool wt_tri(const float4* __restrict__ vt, int t, float3 o, const WtRay& r, float tmin,
+                                       float& hitT, int& hitTri, float& hu, float& hv) {
+    {
         const float3 A = xyz(ld4(vt + 3 * t)) - o, B = xyz(ld4(vt + 3 * t + 1)) - o, C = xyz(ld4(vt + 3 * t + 2)) - o;
         const float Az = comp3(A, r.kz), Bz = comp3(B, r.kz), Cz = comp3(C, r.kz);
         const float Akx = comp3(A, r.kx), Aky = comp3(A, r.ky), Bkx = comp3(B, r.kx), Bky = comp3(B, r.ky), Ckx = comp3(C, r.kx), Cky = comp3(C, r.ky);
@@ -365,16 +368,15 @@ __device__ __forceinline__ bool wt_leaf(const float4* __restrict__ vt, int first
         const float SCx = fabsf(Ckx) + fabsf(pCx), SCy = fabsf(Cky) + fabsf(pCy);
         const float eU = kEdgeRel * (SCx * SBy + SCy * SBx) + kEdgeAbs, eV = kEdgeRel * (SAx * SCy + SAy * SCx) + kEdgeAbs;
         const float eW = kEdgeRel * (SBx * SAy + SBy * SAx) + kEdgeAbs;
-        if ((U < -eU || V < -eV || W < -eW) && (U > eU || V > eV || W > eW)) continue;
+        if ((U < -eU || V < -eV || W < -eW) && (U > eU || V > eV || W > eW)) return false;
         const float det = U + V + W;
-        if (det == 0.f) continue;
+        if (det == 0.f) return false;
         const float T = U * (r.sz * Az) + V * (r.sz * Bz) + W * (r.sz * Cz);
         const float tt = T / det;
-        if (!(tt > tmin && tt < hitT)) continue;
+        if (!(tt > tmin && tt < hitT)) return false;
         hitT = tt; hitTri = t; hu = V / det; hv = W / det;
-        if (ANY) return true;
+        return true;
     }
-    return false;
 }
 
 
@@ -411,13 +413,17 @@ __device__ __forceinline__ void f32_axis(float A, float B, float& lo, float& hi,
 template <bool ANY, int TRI>
 struct TravState<16, ANY, TRI> {
     typedef uint2 Stack[kStack8];
-    float3 o, d; float idx, idy, idz, tmin, hitT, hu, hv; int hitTri, node, sp, budget; unsigned oct, cb, im, hm, tb, tm; WtRay wt;
+    float3 o, d; float idx, idy, idz, tmin, hitT, hu, hv; int hitTri, node, sp, budget; unsigned oct, cb, im, hm, tb, tm, tint; WtRay wt;
 
+    // the f16 interval [tmin rounded down, hitT rounded up], updated when hitT changes (not per node)
+    __device__ __forceinline__ void set_tint() {
+        tint = bits_of_h2(__halves2half2(__float2half_rd(tmin), __float2half_ru(hitT)));
+    }
     __device__ __forceinline__ void begin(float3 o_, float3 d_, float tmin_, float tmax_, int root) {
         o = o_; d = d_; tmin = tmin_; hitT = tmax_; hu = hv = 0.f; hitTri = -1; node = root; sp = 0; budget = kVisitBudget;
         idx = safe_rcp(d.x); idy = safe_rcp(d.y); idz = safe_rcp(d.z);
         oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
-        cb = im = hm = tb = tm = 0; wt = wt_setup(d);
+        cb = im = hm = tb = tm = 0; wt = wt_setup(d); set_tint();
     }
     template <class N, class S>
     __device__ __forceinline__ bool step(const N& nodes, const float4* __restrict__ vt, S& stack, int& err) {
@@ -440,8 +446,7 @@ struct TravState<16, ANY, TRI> {
             if (h16_ok(Ax, Bx) && h16_ok(Ay, By) && h16_ok(Az, Bz)) {
                 __half2 xlo, xhi, xb, ylo, yhi, yb, zlo, zhi, zb;
                 h16_axis(Ax, Bx, xlo, xhi, xb); h16_axis(Ay, By, ylo, yhi, yb); h16_axis(Az, Bz, zlo, zhi, zb);
-                const __half tmn = __float2half_rd(tmin), tmx = __float2half_ru(hitT);
-                const __half2 tmin2 = __halves2half2(tmn, tmn), tmax2 = __halves2half2(tmx, tmx);
+                const __half2 tmin2 = h2_of_bits(__byte_perm(tint, 0u, 0x1010u)), tmax2 = h2_of_bits(__byte_perm(tint, 0u, 0x3232u));
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const unsigned sel = (j & 1) ? 0x4342u : 0x4140u;   // bytes (2j, 2j+1) of the word, each under 0x64: halves 1024 + q
@@ -468,9 +473,7 @@ struct TravState<16, ANY, TRI> {
                     boxHit |= (tn <= tf ? 1u : 0u) << s;
                 }
             }
-            const unsigned leafMask = ((m0 >> 7) & 1u) | ((m0 >> 14) & 2u) | ((m0 >> 21) & 4u) | ((m0 >> 28) & 8u) |
-                                      ((m1 >> 3) & 16u) | ((m1 >> 10) & 32u) | ((m1 >> 17) & 64u) | ((m1 >> 24) & 128u);
-            unsigned leafHit = boxHit & leafMask;
+            unsigned leafHit = boxHit & leaf_slots(m0, m1);
             tb = __float_as_uint(f1.y);
             while (leafHit) {
                 const int s = __ffs(leafHit) - 1; leafHit &= leafHit - 1;
@@ -493,7 +496,7 @@ struct TravState<16, ANY, TRI> {
         }
         if (tm) {
             const int t = (int)tb + __ffs(tm) - 1; tm &= tm - 1;
-            if (wt_leaf<ANY>(vt, t, 1, o, wt, tmin, hitT, hitTri, hu, hv) && ANY) return true;
+            if (wt_tri(vt, t, o, wt, tmin, hitT, hitTri, hu, hv)) { if (ANY) return true; set_tint(); }
         }
         return tm == 0 && node < 0;
     }
