@@ -1,6 +1,7 @@
 // trace.cu - device scene upload/validation and the standalone closest-hit / any-hit ray-batch kernels.
 #include "scene_dev.h"
 #include "trav.cuh"
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -254,8 +255,9 @@ struct cwp_accel {
     int* fetch = nullptr;               // refill kernels' ray cursor (8 bytes)
     int refillGrid = 0;                 // resident blocks of the refill kernels
     bool refill = true;                 // use them (cwp_accel_set_traversal; set at creation by the automatic rule)
-    cudaStream_t st = nullptr;          // stream of the host-buffer entry points
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t st = nullptr, st2 = nullptr;   // streams of the host-buffer entry points (chunks alternate)
+    int* fetch2 = nullptr;              // their refill cursors, one 8-byte counter per stream
+    cudaEvent_t e0 = nullptr, e1 = nullptr, ej = nullptr;
     float4 *bo = nullptr, *bd = nullptr; void* bh = nullptr; size_t cap = 0;   // staging for host-buffer calls
 };
 
@@ -268,6 +270,7 @@ extern "C" int cwp_accel_create(const cwp_scene_buffers* s, int32_t tri, int32_t
     cudaError_t e = cudaMalloc(&a->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(a->err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&a->fetch, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&a->fetch2, 2 * sizeof(unsigned long long));
     if (e == cudaSuccess && a->scene.variant != 4) {
         int nSM = 0, b = 0;
         e = cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, device);
@@ -277,8 +280,10 @@ extern "C" int cwp_accel_create(const cwp_scene_buffers* s, int32_t tri, int32_t
         a->refillGrid = b * nSM;
     }
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&a->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&a->st2, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&a->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&a->e1);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a->ej, cudaEventDisableTiming);
     if (e != cudaSuccess) { cwp_accel_destroy(a); return set_error(CWP_ERR_CUDA, "accel setup: %s", cudaGetErrorString(e)); }
     a->refill = a->scene.variant == 8;
     *out = a;
@@ -289,10 +294,13 @@ extern "C" void cwp_accel_destroy(cwp_accel* a) {
     if (!a) return;
     cudaSetDevice(a->scene.device);
     if (a->st) cudaStreamSynchronize(a->st);
-    cudaFree(a->err); cudaFree(a->fetch); cudaFree(a->bo); cudaFree(a->bd); cudaFree(a->bh);
+    if (a->st2) cudaStreamSynchronize(a->st2);
+    cudaFree(a->err); cudaFree(a->fetch); cudaFree(a->fetch2); cudaFree(a->bo); cudaFree(a->bd); cudaFree(a->bh);
     if (a->st) cudaStreamDestroy(a->st);
+    if (a->st2) cudaStreamDestroy(a->st2);
     if (a->e0) cudaEventDestroy(a->e0);
     if (a->e1) cudaEventDestroy(a->e1);
+    if (a->ej) cudaEventDestroy(a->ej);
     free_scene(a->scene);
     delete a;
 }
@@ -313,6 +321,10 @@ extern "C" int cwp_trace_any(cwp_accel* a, const float* o, const float* d, int32
     return launch_batch<true>(a->scene, (const float4*)o, (const float4*)d, occ, n, a->err, (cudaStream_t)stream, a->refill ? a->fetch : nullptr, a->refillGrid);
 }
 
+// Host-buffer calls pipeline the copies with the traversal: the batch is cut into up to 8 chunks of at least 256k rays
+// that alternate over two streams, so one chunk's rays travel in while the one before it is traced and the results
+// of the one before that travel out (separate copy engines per direction).
+static constexpr int64_t kHostChunkMin = 1 << 18;
 template <bool ANY>
 static int host_call(cwp_accel* a, const float* o, const float* d, void* res, int64_t n, float* ms) {
     CWPB_CHECK(a, CWP_ERR_INVALID, "accel is NULL");
@@ -327,11 +339,21 @@ static int host_call(cwp_accel* a, const float* o, const float* d, void* res, in
         CWPB_CUDA(cudaMalloc(&a->bo, (size_t)n * 16)); CWPB_CUDA(cudaMalloc(&a->bd, (size_t)n * 16)); CWPB_CUDA(cudaMalloc(&a->bh, (size_t)n * 16));
         a->cap = (size_t)n;
     }
+    const int nc = (int)std::max<int64_t>(1, std::min<int64_t>(8, n / kHostChunkMin));
+    const cudaStream_t ss[2] = { a->st, a->st2 };
     CWPB_CUDA(cudaEventRecord(a->e0, a->st));
-    CWPB_CUDA(cudaMemcpyAsync(a->bo, o, (size_t)n * 16, cudaMemcpyHostToDevice, a->st));
-    CWPB_CUDA(cudaMemcpyAsync(a->bd, d, (size_t)n * 16, cudaMemcpyHostToDevice, a->st));
-    if (int rc = launch_batch<ANY>(a->scene, a->bo, a->bd, a->bh, n, a->err, a->st, a->refill ? a->fetch : nullptr, a->refillGrid)) return rc;
-    CWPB_CUDA(cudaMemcpyAsync(res, a->bh, (size_t)n * resBytes, cudaMemcpyDeviceToHost, a->st));
+    CWPB_CUDA(cudaStreamWaitEvent(a->st2, a->e0, 0));
+    for (int c = 0; c < nc; c++) {
+        const int64_t b0 = n * c / nc, m = n * (c + 1) / nc - b0;
+        const cudaStream_t s = ss[c & 1];
+        char* out = (char*)a->bh + (size_t)b0 * resBytes;
+        CWPB_CUDA(cudaMemcpyAsync(a->bo + b0, o + 4 * b0, (size_t)m * 16, cudaMemcpyHostToDevice, s));
+        CWPB_CUDA(cudaMemcpyAsync(a->bd + b0, d + 4 * b0, (size_t)m * 16, cudaMemcpyHostToDevice, s));
+        if (int rc = launch_batch<ANY>(a->scene, a->bo + b0, a->bd + b0, out, m, a->err, s, a->refill ? a->fetch2 + 2 * (c & 1) : nullptr, a->refillGrid)) return rc;
+        CWPB_CUDA(cudaMemcpyAsync((char*)res + (size_t)b0 * resBytes, out, (size_t)m * resBytes, cudaMemcpyDeviceToHost, s));
+    }
+    CWPB_CUDA(cudaEventRecord(a->ej, a->st2));
+    CWPB_CUDA(cudaStreamWaitEvent(a->st, a->ej, 0));
     CWPB_CUDA(cudaEventRecord(a->e1, a->st));
     CWPB_CUDA(cudaEventSynchronize(a->e1));
     if (ms) CWPB_CUDA(cudaEventElapsedTime(ms, a->e0, a->e1));

@@ -119,7 +119,9 @@ void cwp_accel_destroy(cwp_accel* a);
 /* stream: a cudaStream_t or NULL (legacy default stream); asynchronous with respect to the host */
 int cwp_trace_closest(cwp_accel* a, const float* d_o, const float* d_d, float* d_hits, int64_t n, void* stream);
 int cwp_trace_any(cwp_accel* a, const float* d_o, const float* d_d, int32_t* d_occluder, int64_t n, void* stream);
-/* host buffers; copies in, traces, copies out, synchronises; *ms = device time of the whole call (may be NULL) */
+/* host buffers; copies in, traces, copies out, synchronises; *ms = device time of the whole call (may be NULL). Batches
+ * of 512k rays and more are cut into up to 8 chunks over two streams, so copies in, traversal and copies out overlap;
+ * from pinned host memory the copies run asynchronously, from pageable memory the driver stages them. */
 int cwp_trace_closest_host(cwp_accel* a, const float* o, const float* d, float* hits, int64_t n, float* ms);
 int cwp_trace_any_host(cwp_accel* a, const float* o, const float* d, int32_t* occluder, int64_t n, float* ms);
 /* traversal status of the calls since the last query (CWP_OK or CWP_ERR_TRAVERSAL); clears it */

@@ -139,11 +139,14 @@ def test_edge_cases(gpu, cwp, oracle):
     assert h[0, 3].view(np.int32) >= 0 and h[5, 3].view(np.int32) >= 0    # from below the ground: hits its underside
 
 
-def test_host_entry_points_match_device(gpu, cwp):
-    mesh, bvh = cwp.scene("boxes12k", variant=2, bins=16)
+@pytest.mark.parametrize("variant,n", [(2, 5000), (8, 5000), (8, 1_300_001)])
+def test_host_entry_points_match_device(gpu, cwp, variant, n):
+    """The host-buffer calls give the device calls' results bit for bit; 1.3M rays cut into chunks over two streams
+    (an odd count, so the chunks are uneven)."""
+    mesh, bvh = cwp.scene("boxes12k", variant=variant, bins=16)
     acc = cwp.Accel(bvh, tri=1)
     p = cwp.frame_params(mesh, 128, 128)
-    o, d = cwp.camera_rays(p, 5000, seed=2)
+    o, d = cwp.camera_rays(p, n, seed=2)
     hh, ms = acc.trace_closest_host(o, d)
     assert ms > 0
     assert np.array_equal(hh.view(np.uint32), gpu_trace(gpu, acc, o, d).view(np.uint32))
