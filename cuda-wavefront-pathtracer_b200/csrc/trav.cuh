@@ -425,9 +425,11 @@ struct TravState<16, ANY, TRI> {
         oct = (d.x > 0.f ? 1u : 0u) | (d.y > 0.f ? 2u : 0u) | (d.z > 0.f ? 4u : 0u);
         cb = im = hm = tb = tm = 0; wt = wt_setup(d); set_tint();
     }
+    // A node visit: the node's hit leaves become the pending triangles (tm), and the next node is chosen. True when
+    // the ray is finished (no node left and nothing pending, or an error).
     template <class N, class S>
-    __device__ __forceinline__ bool step(const N& nodes, const float4* __restrict__ vt, S& stack, int& err) {
-        if (tm == 0) {
+    __device__ __forceinline__ bool visit(const N& nodes, S& stack, int& err) {
+        {
             if (node < 0) return true;
             if (--budget < 0) { err |= kTravBudget; return true; }
             float4 nf[5]; fetch_node<5>(nodes, node, nf);
@@ -494,11 +496,19 @@ struct TravState<16, ANY, TRI> {
                 node = (int)cb + __popc(im & ((1u << slot) - 1u));
             } else node = -1;
         }
-        if (tm) {
-            const int t = (int)tb + __ffs(tm) - 1; tm &= tm - 1;
-            if (wt_tri(vt, t, o, wt, tmin, hitT, hitTri, hu, hv)) { if (ANY) return true; set_tint(); }
-        }
         return tm == 0 && node < 0;
+    }
+    // One pending triangle test (tm != 0). True when the ray is finished.
+    __device__ __forceinline__ bool tri(const float4* __restrict__ vt) {
+        const int t = (int)tb + __ffs(tm) - 1; tm &= tm - 1;
+        if (wt_tri(vt, t, o, wt, tmin, hitT, hitTri, hu, hv)) { if (ANY) return true; set_tint(); }
+        return tm == 0 && node < 0;
+    }
+    // a visit when nothing is pending, then one pending triangle
+    template <class N, class S>
+    __device__ __forceinline__ bool step(const N& nodes, const float4* __restrict__ vt, S& stack, int& err) {
+        if (tm == 0 && visit(nodes, stack, err)) return true;
+        return tm ? tri(vt) : node < 0;
     }
 };
 
