@@ -63,18 +63,27 @@ struct TwoLevel {
         blas.begin(lo_, ld_, tmin, hitT, root);
         inst = k;
     }
+    // one BLAS node visit of the current instance (inst >= 0); on leaving the instance, its hit is merged and the next
+    // TLAS entry taken. True when the ray is finished.
+    template <class TS, class BS>
+    __device__ __forceinline__ bool step_blas(const BatchArgs& a, TS& tstack, BS& bstack, int& err) {
+        if (!blas.step(a.nodes, a.tris, bstack, err)) return false;
+        if (blas.hitTri >= 0 && blas.hitT < hitT) { hitT = blas.hitT; hitTri = blas.hitTri; hu = blas.hu; hv = blas.hv; hitInst = inst; }
+        inst = -1;
+        if (ANY && hitTri >= 0) return true;
+        if (tsp == 0) return true;
+        next = tstack[--tsp];
+        if (next < 0) { enter(a.inst, a.meshRoot, ~next); return false; }
+        return false;
+    }
     template <class TS, class BS>
     __device__ __forceinline__ bool step(const BatchArgs& a, TS& tstack, BS& bstack, int& err) {
-        if (inst >= 0) {
-            if (!blas.step(a.nodes, a.tris, bstack, err)) return false;
-            if (blas.hitTri >= 0 && blas.hitT < hitT) { hitT = blas.hitT; hitTri = blas.hitTri; hu = blas.hu; hv = blas.hv; hitInst = inst; }
-            inst = -1;
-            if (ANY && hitTri >= 0) return true;
-            if (tsp == 0) return true;
-            next = tstack[--tsp];
-            if (next < 0) { enter(a.inst, a.meshRoot, ~next); return false; }
-            return false;
-        }
+        return inst >= 0 ? step_blas(a, tstack, bstack, err) : step_tlas(a, tstack, err);
+    }
+    // one TLAS node visit (inst < 0): nearer children first, an instance entered when it comes up. True when the ray
+    // is finished.
+    template <class TS>
+    __device__ __forceinline__ bool step_tlas(const BatchArgs& a, TS& tstack, int& err) {
         if (--budget < 0) { err |= kTravBudget; return true; }
         if (a.tlasW == 4) {   // four children, hit ones sorted by entry distance, nearest taken, others pushed far to near
             const float INF = 3.4e38f;
@@ -187,7 +196,7 @@ __global__ void __launch_bounds__(kBatchMaxBlock, 2) k_batch_trace(const BatchAr
                 const bool doB = __popc(inB) >= 2 * __popc(inT);
                 act = act && ((ray.inst >= 0) == doB);
             }
-            if (act) fin = SMEM ? ray.step(a, tstack, sstack, e) : ray.step(a, tstack, lstack, e);
+            if (act) fin = ray.inst >= 0 ? (SMEM ? ray.step_blas(a, tstack, sstack, e) : ray.step_blas(a, tstack, lstack, e)) : ray.step_tlas(a, tstack, e);
             const unsigned busy = __ballot_sync(0xffffffffu, k >= 0 && !fin);
             if (!busy || (!drained && 32 - __popc(busy) >= a.fetch)) break;
         }
