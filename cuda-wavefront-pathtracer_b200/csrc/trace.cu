@@ -205,6 +205,95 @@ __global__ void __launch_bounds__(kBatchBlock, 8) k_trace_rf(const float4* __res
     if (e) atomicOr(err, e);
 }
 
+// Precision form, closest hits: persistent with refill, with the watertight triangle tests shared out over the warp.
+// Each iteration every active lane visits one node (TravState<16>::visit: f16 slab tests; the hit leaves' triangles
+// become its pending mask). Then the warp tests all lanes' pending triangles together, 32 per round: slot i of the
+// warp's concatenated list goes to lane i mod 32, which takes the owning ray's data by shuffles. A lane whose test hits
+// in the owner's interval proposes (t, slot) to the owner by a 64-bit atomic minimum in shared memory, and the owner
+// takes the smallest t, the earliest slot among equal ones. That is the hit the owner's own tests in slot order keep
+// (a later triangle replaces the hit only when strictly closer), so every ray gets the result of the sequential
+// traversal (TravState<16>::step) bit for bit. Rounds of one owner follow one another, each against the interval the
+// previous round left. The watertight test costs several slab tests, and one lane's run of tests no longer holds the
+// warp's other lanes: 8% less time than one test per lane and step on the 1M-ray batch. Any-hit rays keep that form
+// (k_trace_rf<16, 1, true>): they stop at their first hit, and sharing their tests measured 6% slower.
+// The warp refills once 8 lanes are idle (12: +1.5%, 16: +5% time).
+static constexpr int kRefillPrec = 8;
+__device__ __forceinline__ unsigned long long wt_key(float t, int slot) {
+    const unsigned u = __float_as_uint(t);
+    return ((unsigned long long)((u & 0x80000000u) ? ~u : (u | 0x80000000u)) << 32) | (unsigned)slot;   // float order, then slot
+}
+
+__global__ void __launch_bounds__(kBatchBlock, 8) k_trace_prec_rf(const float4* __restrict__ nodes, const float4* __restrict__ vt, const float4* __restrict__ ro,
+                                                                  const float4* __restrict__ rd, float4* __restrict__ hits, long long n, int* fetch, int* err) {
+    __shared__ unsigned long long best[kBatchBlock];   // per lane: the smallest (t, slot) its pending triangles gave this round
+    const int lane = threadIdx.x & 31;
+    unsigned long long* myBest = best + threadIdx.x;
+    int e = 0;
+    TravState<16, false, 1> ray; TravState<16, false, 1>::Stack stack;
+    long long k = -1; bool fin = false, drained = false;
+    for (;;) {
+        if (fin) { __stcs(hits + k, make_float4(ray.hitT, ray.hu, ray.hv, __int_as_float(ray.hitTri))); k = -1; fin = false; }
+        if (!drained) {
+            const bool need = k < 0;
+            const unsigned nm = __ballot_sync(0xffffffffu, need);
+            if (nm) {
+                const int leader = __ffs(nm) - 1;
+                long long base = 0;
+                if (lane == leader) base = atomicAdd((unsigned long long*)fetch, (unsigned long long)__popc(nm));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                const long long kk = base + __popc(nm & lane_lt());
+                if (need && kk < n) { k = kk; const float4 O = __ldcs(ro + k), D = __ldcs(rd + k); ray.begin(xyz(O), xyz(D), O.w, D.w, 0); }
+                drained = __any_sync(0xffffffffu, need && kk >= n);
+            }
+        }
+        if (!__any_sync(0xffffffffu, k >= 0)) break;
+        for (;;) {
+            // one node visit per active ray (true: the ray stopped on a bound; its pending triangles are dropped)
+            if (k >= 0 && !fin && ray.visit(nodes, stack, e)) fin = true;
+            const unsigned pend = (k >= 0 && !fin) ? ray.tm : 0u;
+            ray.tm = 0;
+            // the warp's pending triangles, concatenated in lane order: this lane's are slots [incl - cnt, incl)
+            const int cnt = __popc(pend);
+            int incl = cnt;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, off); if (lane >= off) incl += v; }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int base = 0; base < total; base += 32) {
+                *myBest = ~0ull;
+                __syncwarp();
+                const int slot = base + lane;
+                int owner = 0;   // the first lane whose inclusive count exceeds slot
+#pragma unroll
+                for (int step = 16; step; step >>= 1) if (__shfl_sync(0xffffffffu, incl, owner + step - 1) <= slot) owner += step;
+                const unsigned om = __shfl_sync(0xffffffffu, pend, owner);
+                const int oFirst = __shfl_sync(0xffffffffu, incl - cnt, owner);
+                const int oTb = __shfl_sync(0xffffffffu, (int)ray.tb, owner);
+                const float3 o = make_float3(__shfl_sync(0xffffffffu, ray.o.x, owner), __shfl_sync(0xffffffffu, ray.o.y, owner), __shfl_sync(0xffffffffu, ray.o.z, owner));
+                WtRay w;
+                const int kk = __shfl_sync(0xffffffffu, ray.wt.kx | (ray.wt.ky << 2) | (ray.wt.kz << 4), owner);
+                w.kx = kk & 3; w.ky = (kk >> 2) & 3; w.kz = kk >> 4;
+                w.sx = __shfl_sync(0xffffffffu, ray.wt.sx, owner); w.sy = __shfl_sync(0xffffffffu, ray.wt.sy, owner); w.sz = __shfl_sync(0xffffffffu, ray.wt.sz, owner);
+                const float tmin = __shfl_sync(0xffffffffu, ray.tmin, owner), tmax = __shfl_sync(0xffffffffu, ray.hitT, owner);
+                // the owner's (slot - oFirst)-th pending triangle in bit order (lanes past the list compute an unused index)
+                const int t = oTb + (int)__fns(om, 0, slot - oFirst + 1);
+                float tt = 0.f, u = 0.f, v = 0.f;
+                if (slot < total && wt_test(vt, t, o, w, tmin, tmax, tt, u, v)) atomicMin(best + (threadIdx.x - lane) + owner, wt_key(tt, slot));
+                __syncwarp();
+                const unsigned long long b = *myBest;
+                const int src = b == ~0ull ? lane : (int)(b & 31u);   // the lane that tested this ray's winning slot
+                const float wT = __shfl_sync(0xffffffffu, tt, src), wU = __shfl_sync(0xffffffffu, u, src), wV = __shfl_sync(0xffffffffu, v, src);
+                const int wTri = __shfl_sync(0xffffffffu, t, src);
+                if (b != ~0ull) { ray.hitT = wT; ray.hitTri = wTri; ray.hu = wU; ray.hv = wV; ray.set_tint(); }
+                __syncwarp();
+            }
+            if (k >= 0 && !fin && ray.node < 0) fin = true;
+            const unsigned busy = __ballot_sync(0xffffffffu, k >= 0 && !fin);
+            if (!busy || (!drained && 32 - __popc(busy) >= kRefillPrec)) break;
+        }
+    }
+    if (e) atomicOr(err, e);
+}
+
 template <bool ANY>
 static int launch_batch(const DeviceScene& s, const float4* o, const float4* d, void* out, long long n, int* err, cudaStream_t st, int* fetch, int refillGrid) {
     if (n <= 0) return CWP_OK;
@@ -212,7 +301,10 @@ static int launch_batch(const DeviceScene& s, const float4* o, const float4* d, 
     if (fetch && s.variant != 4) {   // persistent refill kernels (BVH2, CWBVH, precision form)
         CWPB_CUDA(cudaMemsetAsync(fetch, 0, sizeof(unsigned long long), st));
 #define CWPB_R(VV, TT) k_trace_rf<VV, TT, ANY><<<refillGrid, kBatchBlock, 0, st>>>(s.nodes, tv0, o, d, (float4*)out, (int*)out, n, fetch, err)
-        if (s.precise) CWPB_R(16, 1);
+        if (s.precise) {   // closest hits share their triangle tests over the warp; any-hit rays keep their own
+            if (ANY) CWPB_R(16, 1);
+            else k_trace_prec_rf<<<refillGrid, kBatchBlock, 0, st>>>(s.nodes, tv0, o, d, (float4*)out, n, fetch, err);
+        }
         else if (s.variant == 2) { if (s.tri) CWPB_R(2, 1); else CWPB_R(2, 0); }
         else { if (s.tri) CWPB_R(8, 1); else CWPB_R(8, 0); }
 #undef CWPB_R

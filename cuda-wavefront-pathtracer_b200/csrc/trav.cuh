@@ -354,9 +354,10 @@ __device__ __forceinline__ WtRay wt_setup(float3 d) {
     return r;
 }
 
-// one watertight test of triangle t; true when it became the closest hit
-__device__ __forceinline__ bool wt_tri(const float4* __restrict__ vt, int t, float3 o, const WtRay& r, float tmin,
-                                       float& hitT, int& hitTri, float& hu, float& hv) {
+// one watertight test of triangle t against the interval (tmin, tmax); true when it hits there, with its distance and
+// barycentrics in tt, u, v
+__device__ __forceinline__ bool wt_test(const float4* __restrict__ vt, int t, float3 o, const WtRay& r, float tmin, float tmax,
+                                        float& tt, float& u, float& v) {
     {
         const float3 A = xyz(ld4(vt + 3 * t)) - o, B = xyz(ld4(vt + 3 * t + 1)) - o, C = xyz(ld4(vt + 3 * t + 2)) - o;
         const float Az = comp3(A, r.kz), Bz = comp3(B, r.kz), Cz = comp3(C, r.kz);
@@ -372,11 +373,19 @@ __device__ __forceinline__ bool wt_tri(const float4* __restrict__ vt, int t, flo
         const float det = U + V + W;
         if (det == 0.f) return false;
         const float T = U * (r.sz * Az) + V * (r.sz * Bz) + W * (r.sz * Cz);
-        const float tt = T / det;
-        if (!(tt > tmin && tt < hitT)) return false;
-        hitT = tt; hitTri = t; hu = V / det; hv = W / det;
+        tt = T / det;
+        if (!(tt > tmin && tt < tmax)) return false;
+        u = V / det; v = W / det;
         return true;
     }
+}
+// one watertight test of triangle t; true when it became the closest hit
+__device__ __forceinline__ bool wt_tri(const float4* __restrict__ vt, int t, float3 o, const WtRay& r, float tmin,
+                                       float& hitT, int& hitTri, float& hu, float& hv) {
+    float tt, u, v;
+    if (!wt_test(vt, t, o, r, tmin, hitT, tt, u, v)) return false;
+    hitT = tt; hitTri = t; hu = u; hv = v;
+    return true;
 }
 
 
@@ -409,7 +418,8 @@ __device__ __forceinline__ void f32_axis(float A, float B, float& lo, float& hi,
 // slower - its node visits, not its leaf tests, dominate (ncu: thread instructions +8%, active lanes 14.0 -> 13.1).
 // The hit leaves' triangles are kept as a bit mask over the node's triangle range: both encoders here (host collapse,
 // GPU emission) assign a node's leaf ranges in slot order, so ascending bits are slot order, and within a leaf its
-// triangles in order.
+// triangles in order. The closest-hit ray-batch kernel (trace.cu k_trace_prec_rf) calls visit() alone and tests the
+// pending triangles (tb, tm) of all lanes together, with the same per-ray result.
 template <bool ANY, int TRI>
 struct TravState<16, ANY, TRI> {
     typedef uint2 Stack[kStack8];
