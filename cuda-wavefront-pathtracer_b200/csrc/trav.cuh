@@ -399,8 +399,8 @@ __device__ __forceinline__ bool h16_ok(float A, float B) {
 // outward-rounded f16 bases of one axis
 __device__ __forceinline__ void h16_axis(float A, float B, __half2& lo2, __half2& hi2, __half2& b2) {
     const float m = h16_margin(A, B), Ap = A - 1024.f * B;
-    const __half lo = __float2half_rd(Ap - m), hi = __float2half_ru(Ap + m), b = __float2half_rn(B);
-    lo2 = __halves2half2(lo, lo); hi2 = __halves2half2(hi, hi); b2 = __halves2half2(b, b);
+    const __half lo = __float2half_rd(Ap - m), hi = __float2half_ru(Ap + m);
+    lo2 = __halves2half2(lo, lo); hi2 = __halves2half2(hi, hi); b2 = __float2half2_rn(B);   // (one conversion fills both halves)
 }
 // widened FP32 bases of one axis (nodes outside the f16 range)
 __device__ __forceinline__ void f32_axis(float A, float B, float& lo, float& hi, float& b) {
@@ -459,6 +459,7 @@ struct TravState<16, ANY, TRI> {
                 __half2 xlo, xhi, xb, ylo, yhi, yb, zlo, zhi, zb;
                 h16_axis(Ax, Bx, xlo, xhi, xb); h16_axis(Ay, By, ylo, yhi, yb); h16_axis(Az, Bz, zlo, zhi, zb);
                 const __half2 tmin2 = h2_of_bits(__byte_perm(tint, 0u, 0x1010u)), tmax2 = h2_of_bits(__byte_perm(tint, 0u, 0x3232u));
+                unsigned hm2[4];   // per child pair: 0xffff in the low half for slot 2j, in the high half for slot 2j + 1
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const unsigned sel = (j & 1) ? 0x4342u : 0x4140u;   // bytes (2j, 2j+1) of the word, each under 0x64: halves 1024 + q
@@ -470,9 +471,11 @@ struct TravState<16, ANY, TRI> {
                     const __half2 zf = __hfma2(h2_of_bits(__byte_perm(j < 2 ? pz0 : pz1, 0x64646464u, sel)), zb, zhi);
                     const __half2 tn = __hmax2(__hmax2(xn, yn), __hmax2(zn, tmin2));
                     const __half2 tf = __hmin2(__hmin2(xf, yf), __hmin2(zf, tmax2));
-                    const unsigned m = __hle2_mask(tn, tf);
-                    boxHit |= ((m & 1u) << (2 * j)) | (((m >> 16) & 1u) << (2 * j + 1));
+                    hm2[j] = __hle2_mask(tn, tf);
                 }
+                // one byte per slot (the low byte of each half), then the flags gathered onto bits 0..7 as in leaf_slots
+                const unsigned w0 = __byte_perm(hm2[0], hm2[1], 0x6420u), w1 = __byte_perm(hm2[2], hm2[3], 0x6420u);
+                boxHit = (((w0 & 0x01010101u) * 0x10204080u) >> 28) | ((((w1 & 0x01010101u) * 0x10204080u) >> 24) & 0xF0u);
             } else {
                 float xlo, xhi, xb, ylo, yhi, yb, zlo, zhi, zb;
                 f32_axis(Ax, Bx, xlo, xhi, xb); f32_axis(Ay, By, ylo, yhi, yb); f32_axis(Az, Bz, zlo, zhi, zb);
