@@ -18,6 +18,8 @@ A step is one frame (frame*) or one closest + one any-hit pass over the batch (t
 all ranks over the max over ranks of the device-timed steps (CUDA events on the renderer's stream). `e2e` is the same
 metric through the C ABI with host buffers: each frame's accumulation buffer (trace16m: rays in, hits out) crosses
 PCIe inside the timed region. Multi-GPU runs are independent replicas (weak scaling): the path needs no exchange.
+On one GPU the frame workloads also run trace16m and precision1m (config 2's ray batch and config 3) as child
+processes after the frame, and carry their measured lines, shortened, under `companions` (--companions 0: not).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload frame512] [--impl ours|reference]
 """
@@ -694,6 +696,30 @@ def bench_serving(args, wl, cwp, torch, out, barrier=lambda: None, reduce=lambda
                gpu_launches=None)
 
 
+COMPANION_KEYS = ("closest_ms", "any_ms", "references", "rays", "bvh", "lost_hits", "tie_mismatches", "extra_hits", "max_t_error", "plain_grays_s", "vs_plain")
+
+
+def companions(args):
+    """trace16m and precision1m, each in a child process on this GPU (its own context, run after the frame): their
+    JSON lines with the config shortened to the figures that describe the result."""
+    res = {}
+    for name in ("trace16m", "precision1m"):
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", name, "--steps", str(max(args.steps, 3)), "--warmup", str(max(args.warmup, 3)),
+               "--no-cpu-baseline", "--companions", "0"]
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900, env=dict(os.environ))
+            line = [l for l in r.stdout.splitlines() if l.startswith("{")]
+            if r.returncode != 0 or not line:
+                res[name] = {"error": f"exit {r.returncode}: {r.stderr.strip().splitlines()[-1] if r.stderr.strip() else 'no output'}"}
+                continue
+            d = json.loads(line[-1])
+            res[name] = {"metric": d["metric"], "value": d["value"], "unit": d["unit"], "steps": d["steps"], "warmup": d["warmup"], "ms_per_step": d["ms_per_step"],
+                         "e2e": d.get("e2e"), "clocks": d.get("clocks"), "config": {k: d["config"][k] for k in COMPANION_KEYS if k in d["config"]}}
+        except subprocess.TimeoutExpired:
+            res[name] = {"error": "timed out after 900 s"}
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -725,6 +751,7 @@ def main():
     ap.add_argument("--serve-spatial", type=float, default=0.0, help="serving: spatial-split threshold of the host-built BLAS (0: binned SAH)")
     ap.add_argument("--overlap", type=int, default=1, help="serving: a step returns with its launches queued (1) or waits for them (0)")
     ap.add_argument("--sort", type=int, default=0, help="frames: regroup continuation rays before each bounce (0 off, 1 octant, 2 octant + origin cell)")
+    ap.add_argument("--companions", type=int, default=1, help="frames at one GPU: also run trace16m and precision1m in child processes and carry their lines (1) or not (0)")
     ap.add_argument("--stage-levels", type=int, default=0, help="frames (CWBVH): top tree levels staged in shared memory per block (0 library default, -1 none, 1..3)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
@@ -836,6 +863,8 @@ def main():
         r.close()
         if rank == 0 and ws == 1 and args.reference_cuda:
             out["reference_cuda"] = reference_cuda_frame(cwp, wl, mesh, p, max_ms / args.steps, ours_img, local)
+        if rank == 0 and ws == 1 and args.companions:
+            out["companions"] = companions(args)
     else:
         # ------------------------------------------------------------------ ray batches
         n = wl["rays"]
