@@ -230,6 +230,7 @@ __global__ void __launch_bounds__(kBatchBlock, 8) k_trace_prec_rf(const float4* 
     unsigned long long* myBest = best + threadIdx.x;
     int e = 0;
     TravState<16, false, 1> ray; TravState<16, false, 1>::Stack stack;
+    ray.tm = ray.tb = 0u; ray.node = -1;   // (a lane without a ray owns no slot; its fields are shuffled but not used)
     long long k = -1; bool fin = false, drained = false;
     for (;;) {
         if (fin) { __stcs(hits + k, make_float4(ray.hitT, ray.hu, ray.hv, __int_as_float(ray.hitTri))); k = -1; fin = false; }
