@@ -472,8 +472,12 @@ extern "C" int cwp_accel_set_precision(cwp_accel* a, int32_t mode) {
     int nSM = 0, b = 0;
     CWPB_CUDA(cudaSetDevice(a->scene.device));
     CWPB_CUDA(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, a->scene.device));
-    if (mode == 1) CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace_rf<16, 1, false>, kBatchBlock, 0));
-    else CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, a->scene.tri == 1 ? k_trace_rf<8, 1, false> : k_trace_rf<8, 0, false>, kBatchBlock, 0));
+    if (mode == 1) {   // closest hits: the shared-test kernel; any-hit: k_trace_rf<16, 1, true>; one grid fits both
+        int b2 = 0;
+        CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace_prec_rf, kBatchBlock, 0));
+        CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_trace_rf<16, 1, true>, kBatchBlock, 0));
+        b = std::min(b, b2);
+    } else CWPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, a->scene.tri == 1 ? k_trace_rf<8, 1, false> : k_trace_rf<8, 0, false>, kBatchBlock, 0));
     a->scene.precise = mode == 1;
     a->refillGrid = b * nSM;
     return CWP_OK;
