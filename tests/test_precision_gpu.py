@@ -114,6 +114,25 @@ def test_precision_form_matches_host_restatement(gpu, cwp, oracle, scene12k):
         assert np.array_equal(run(gpu, acc, o, d, any_hit=True), oracle.trace_prec(bvh.nodes, bvh.verts, o, d, any_hit=True))
 
 
+def test_precision_form_matches_host_restatement_signed_interval(gpu, cwp, oracle, scene12k):
+    """The closest-hit kernel ranks a warp's shared triangle tests by (t, slot) on the float order of t: rays whose
+    interval starts behind the origin (tmin = -0.5, so hits at negative t count) and ends short (tmax = 5) still give
+    the oracle's restatement bit for bit, through the refill kernel and one ray per thread."""
+    mesh, bvh = scene12k
+    acc = cwp.Accel(bvh, tri=1)
+    p = cwp.frame_params(mesh, 256, 256)
+    o, d = cwp.incoherent_rays(40000, p, bvh.tris, lambda o, d: run(gpu, acc, o, d), seed=37)
+    o[:, 3] = -0.5; d[:, 3] = 5.0
+    acc.set_precision(1)
+    want_h = oracle.trace_prec(bvh.nodes, bvh.verts, o, d)
+    want_o = oracle.trace_prec(bvh.nodes, bvh.verts, o, d, any_hit=True)
+    assert (want_h[:, 0] < 0).sum() > 100   # the batch does hit behind its origins
+    for trav in (1, 2):
+        acc.set_traversal(trav)
+        assert np.array_equal(run(gpu, acc, o, d).view(np.uint32), want_h.view(np.uint32))
+        assert np.array_equal(run(gpu, acc, o, d, any_hit=True), want_o)
+
+
 def test_precision_requires_cwbvh_and_corners(gpu, cwp):
     _, b2 = cwp.scene("boxes12k", variant=2, bins=16)
     acc = cwp.Accel(b2, tri=1)
