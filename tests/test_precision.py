@@ -118,3 +118,46 @@ def test_explain_differences_classes():
     c, rows = explain_differences(o, d, verts, occ_o, occ_x, any_hit=True)
     # ray 1: the other's occluder is inside (we missed it); ray 2: near the edge; ray 3: ours inside
     assert [r["class"] for r in rows] == ["unexplained", "graze", "ours_exact"]
+
+
+def _key(t, slot):
+    """the closest-hit kernel's shared-test key (trace.cu wt_key): the float order of t in the high 32 bits, the slot
+    in the low ones"""
+    u = int(np.float32(t).view(np.uint32))
+    hi = (~u & 0xFFFFFFFF) if u & 0x80000000 else (u | 0x80000000)
+    return (hi << 32) | slot
+
+
+def test_shared_triangle_tests_keep_the_sequential_hit():
+    """A model of the precision form's shared triangle tests: a ray's pending triangles (slot order) are tested in
+    rounds of up to 32 against the interval the previous round left, and the smallest (t, slot) key of each round's
+    hits wins. That is the hit one-by-one testing keeps (a later triangle replaces the hit only when strictly closer),
+    over random distances with repeats (ties), negative t, misses and lists longer than a round."""
+    rng = np.random.default_rng(3)
+    for trial in range(4000):
+        n = int(rng.integers(1, 80))
+        tmin = float(np.float32(rng.choice([0.0, -0.5, 1e-4])))
+        tmax = float(np.float32(rng.choice([1e30, 5.0, 2.0])))
+        pool = np.float32(rng.uniform(-1.0, 6.0, 6))            # few distinct values: many exact ties
+        t = np.float32(rng.choice(pool, n))
+        hit = rng.random(n) < 0.6                                 # the watertight test's verdict on the triangle
+        # sequential: one test at a time, strict tmin < t < hitT
+        hitT, win = tmax, -1
+        for i in range(n):
+            if hit[i] and tmin < t[i] < hitT:
+                hitT, win = float(t[i]), i
+        # shared: rounds of 32 slots, each tested against the interval the previous rounds left
+        hitT2, win2 = tmax, -1
+        # the slot offset within the warp differs from the ray's own index by the lanes before it: keep a random base
+        first = int(rng.integers(0, 32))
+        for base in range(0, first + n, 32):
+            best = None
+            for s in range(max(base, first), min(base + 32, first + n)):
+                i = s - first
+                if hit[i] and tmin < t[i] < hitT2:
+                    k = _key(t[i], s)
+                    best = k if best is None else min(best, k)
+            if best is not None:
+                win2 = (best & 0xFFFFFFFF) - first
+                hitT2 = float(t[win2])
+        assert (win, hitT) == (win2, hitT2), (trial, win, win2, hitT, hitT2)
