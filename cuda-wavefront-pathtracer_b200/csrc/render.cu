@@ -277,7 +277,10 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow_rf(const __grid
     if (err) atomicOr(a.err, err);
 }
 
-template <int V, int TRI, bool STAGE = false>
+// FOCT >= 0 (CWBVH): the launch's shadow rays all point into octant FOCT (the sun's, when its cone stays inside one
+// octant), so their traversal takes the plane choice and child order as constants; a ray outside it (or with a zero
+// direction component) takes the per-ray form. Both visit the same nodes in the same order: the same result.
+template <int V, int TRI, bool STAGE = false, int FOCT = -1>
 __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow(const __grid_constant__ KArgs a) {
     const auto nodes = node_source<STAGE>(a);
     int* const c = a.cnt + 4 * a.depth;
@@ -292,12 +295,26 @@ __global__ void __launch_bounds__(128, CWPB_TRACE_MINB) k_shadow(const __grid_co
         const int k = base + lane;
         if (k < n) {
             const float4 h0 = __ldcs(a.q.h0 + k), h1 = __ldcs(a.q.h1 + k); const float2 h2 = __ldcs(a.q.h2 + k);
-            float t = 1e30f, u, v; int tri = -1;
-            if (!trace_ray<V, true, TRI>(nodes, a.tv, xyz(h0), xyz(h1), 0.f, t, tri, u, v, 0, err))
-                accum_add(a.accum, __float_as_int(h0.w), f3(h1.w, h2.x, h2.y));
+            float t = 1e30f, u, v; int tri = -1; bool hit;
+            if constexpr (V == 8 && FOCT >= 0) {
+                hit = octant_of(xyz(h1)) == FOCT ? trav_cwbvh<true, TRI, FOCT>(nodes, a.tv, xyz(h0), xyz(h1), 0.f, t, tri, u, v, 0, err)
+                                                 : trav_cwbvh<true, TRI>(nodes, a.tv, xyz(h0), xyz(h1), 0.f, t, tri, u, v, 0, err);
+            } else hit = trace_ray<V, true, TRI>(nodes, a.tv, xyz(h0), xyz(h1), 0.f, t, tri, u, v, 0, err);
+            if (!hit) accum_add(a.accum, __float_as_int(h0.w), f3(h1.w, h2.x, h2.y));
         }
     }
     if (err) atomicOr(a.err, err);
+}
+
+// the octant every direction of the sun's cone lies in (all three components of the axis farther from zero than the
+// cone's half-angle, with a factor 2 to spare), or -1
+static int sun_octant(const cwp_params& P) {
+    const float sx = P.sun_to[0], sy = P.sun_to[1], sz = P.sun_to[2];
+    const float len = sqrtf(sx * sx + sy * sy + sz * sz);
+    if (!(len > 0.f) || !(P.sun_cos > 0.f) || P.sun_cos > 1.f) return -1;
+    const float half = acosf(P.sun_cos) * 2.f + 1e-6f;
+    if (fabsf(sx) <= half * len || fabsf(sy) <= half * len || fabsf(sz) <= half * len) return -1;
+    return (sx > 0.f ? 1 : 0) | (sy > 0.f ? 2 : 0) | (sz > 0.f ? 4 : 0);
 }
 
 // ---------------- continuation regrouping (cwp_render_options.sort) ----------------
@@ -435,7 +452,16 @@ template <int V, int TRI, bool STAGE = false> void launch_depth(cwp_renderer* r,
     }
     if (ev) { cudaEventRecordWithFlags(ev[1], r->st, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], r->st, cudaEventRecordExternal); }
     if constexpr (V != 4) { if (rfShadow) k_shadow_rf<V, TRI, STAGE><<<gs, 128, sm, r->st>>>(a); }
-    if (!rfShadow) k_shadow<V, TRI, STAGE><<<gs, 128, sm, r->st>>>(a);
+    if (!rfShadow) {
+        int foct = -1;
+        if constexpr (V == 8 && !STAGE) foct = sun_octant(r->P);
+        switch (foct) {
+#define CWPB_SO(F) case F: if constexpr (V == 8 && !STAGE) k_shadow<8, TRI, false, F><<<gs, 128, sm, r->st>>>(a); break;
+            CWPB_SO(0) CWPB_SO(1) CWPB_SO(2) CWPB_SO(3) CWPB_SO(4) CWPB_SO(5) CWPB_SO(6) CWPB_SO(7)
+#undef CWPB_SO
+            default: k_shadow<V, TRI, STAGE><<<gs, 128, sm, r->st>>>(a);
+        }
+    }
     if (ev) cudaEventRecordWithFlags(ev[3], r->st, cudaEventRecordExternal);
 }
 

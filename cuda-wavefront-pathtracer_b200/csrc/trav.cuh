@@ -225,8 +225,10 @@ __device__ __forceinline__ float qbyte(unsigned w, int s) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | (unsigned)(s & 3))) - 8388608.0f;
 }
 
-template <bool ANY, int TRI>
-struct TravState<8, ANY, TRI> {
+// FOCT >= 0: every ray of the launch has direction octant FOCT and no zero direction component (the caller checks
+// per ray), so the near/far plane choice and the octant order are compile-time constants; -1: taken per ray
+template <bool ANY, int TRI, int FOCT>
+struct CwbvhTrav {
     typedef uint2 Stack[kStack8];
     float3 o, d; float idx, idy, idz, tmin, hitT, hu, hv; int hitTri, node, sp, budget; unsigned oct, cb, im, hm;
 
@@ -252,7 +254,8 @@ struct TravState<8, ANY, TRI> {
         // per axis, the plane a ray enters first: the low bound when the reciprocal is positive, else the high bound.
         // Selecting it replaces the min/max of each (low, high) pair and gives the same values: the fused affine map
         // q * s + o is monotonic in q for either sign of s.
-        const bool fx = idx < 0.f, fy = idy < 0.f, fz = idz < 0.f;
+        const bool fx = FOCT >= 0 ? !(FOCT & 1) : idx < 0.f, fy = FOCT >= 0 ? !(FOCT & 2) : idy < 0.f, fz = FOCT >= 0 ? !(FOCT & 4) : idz < 0.f;
+        const unsigned oc = FOCT >= 0 ? (unsigned)FOCT : oct;
         // quantised bounds: lo x (f2.x, f2.y), lo y (f2.z, f2.w), lo z (f3.x, f3.y), hi x (f3.z, f3.w), hi y (f4.x, f4.y), hi z (f4.z, f4.w)
         const unsigned nx0 = __float_as_uint(fx ? f3_.z : f2.x), nx1 = __float_as_uint(fx ? f3_.w : f2.y), px0 = __float_as_uint(fx ? f2.x : f3_.z), px1 = __float_as_uint(fx ? f2.y : f3_.w);
         const unsigned ny0 = __float_as_uint(fy ? f4_.x : f2.z), ny1 = __float_as_uint(fy ? f4_.y : f2.w), py0 = __float_as_uint(fy ? f2.z : f4_.x), py1 = __float_as_uint(fy ? f2.w : f4_.y);
@@ -290,9 +293,9 @@ struct TravState<8, ANY, TRI> {
         unsigned leafHit = boxHit & leaf_slots(m0, m1);
         // internal children hit, re-indexed to octant order (slot s -> bit s ^ oct)
         unsigned hits = boxHit & imask;
-        if (oct & 1u) hits = ((hits & 0x55u) << 1) | ((hits & 0xAAu) >> 1);
-        if (oct & 2u) hits = ((hits & 0x33u) << 2) | ((hits & 0xCCu) >> 2);
-        if (oct & 4u) hits = ((hits & 0x0Fu) << 4) | ((hits & 0xF0u) >> 4);
+        if (oc & 1u) hits = ((hits & 0x55u) << 1) | ((hits & 0xAAu) >> 1);
+        if (oc & 2u) hits = ((hits & 0x33u) << 2) | ((hits & 0xCCu) >> 2);
+        if (oc & 4u) hits = ((hits & 0x0Fu) << 4) | ((hits & 0xF0u) >> 4);
         while (leafHit) {
             const int s = __ffs(leafHit) - 1; leafHit &= leafHit - 1;
             const unsigned m = byte_of(s < 4 ? m0 : m1, s);
@@ -303,16 +306,24 @@ struct TravState<8, ANY, TRI> {
             cb = (unsigned)childBase; im = imask; hm = hits;
         }
         while (hm == 0) { if (sp == 0) return true; const uint2 e = stack[--sp]; cb = e.x; im = e.y >> 8; hm = e.y & 255u; }
-        const unsigned k = __ffs(hm) - 1; hm &= hm - 1; const unsigned slot = k ^ oct;
+        const unsigned k = __ffs(hm) - 1; hm &= hm - 1; const unsigned slot = k ^ oc;
         node = (int)cb + __popc(im & ((1u << slot) - 1u));
         return false;
     }
 };
 
-template <bool ANY, int TRI, class N>
+template <bool ANY, int TRI> struct TravState<8, ANY, TRI> : CwbvhTrav<ANY, TRI, -1> {};
+
+// direction octant of d (bit i set: component i positive), or -1 when a component is zero (its sign then decides the
+// plane choice, not the octant bit)
+__device__ __forceinline__ int octant_of(float3 d) {
+    return d.x != 0.f && d.y != 0.f && d.z != 0.f ? (d.x > 0.f ? 1 : 0) | (d.y > 0.f ? 2 : 0) | (d.z > 0.f ? 4 : 0) : -1;
+}
+
+template <bool ANY, int TRI, int FOCT = -1, class N>
 __device__ __forceinline__ bool trav_cwbvh(const N& nodes, const float4* __restrict__ tv, float3 o, float3 d, float tmin,
                                            float& hitT, int& hitTri, float& hu, float& hv, int root, int& err) {
-    TravState<8, ANY, TRI> r; typename TravState<8, ANY, TRI>::Stack stack; r.begin(o, d, tmin, hitT, root);
+    CwbvhTrav<ANY, TRI, FOCT> r; typename CwbvhTrav<ANY, TRI, FOCT>::Stack stack; r.begin(o, d, tmin, hitT, root);
     while (!r.step(nodes, tv, stack, err)) {}
     hitT = r.hitT; hitTri = r.hitTri; hu = r.hu; hv = r.hv;
     return hitTri >= 0;
